@@ -1,0 +1,460 @@
+#!/usr/bin/env python
+"""bench.py -- stage throughput of GRotor's routing hot path on B200.
+
+One step is one L-shape routing stage over a whole synthetic design already
+resident in HBM: exact first-fit batching on the GPU, then for every batch the
+incremental cost / prefix refresh, the L-shape DP with layer assignment and the
+demand commit -- in the persistent batched executor (one cooperative kernel per
+part).  ``value`` = nets routed per second (batching + DAG, the reference's
+stage-runtime definition, README.md:139).  The plain per-batch-launch form and
+the CUDA-graph form run on the same GPU afterwards for the comparison the
+metric names, and their routes are checked identical.
+
+``--impl reference`` times the reference's own CPU implementation of the path
+on the host cores instead (its CPU first-fit batching, built from its sources
+into oracle/_ref/, plus the CPU restatement of its DAG code on all cores) on a
+bounded sample of the same workload.
+
+Multi-GPU: the path does not shard (batches depend on each other through
+demand), so ``--gpus N`` runs N independent replicas (seed + rank); timing is
+the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "stage runtime & nets/s on 1 B200: persistent batched vs plain, evaluator-exact"
+WORKLOAD = "persistent_1600x1600x10"
+BATCH_LIMIT = 1000000  # lshape.cuh:62,69
+UNIT = "nets/s"
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="grotor", choices=["grotor", "reference"])
+    ap.add_argument("--workload", default=WORKLOAD)
+    ap.add_argument("--no-compare", action="store_true", help="skip the plain / graph executor comparison")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
+    ap.add_argument("--cpu-nets", type=int, default=0, help="CPU baseline sample size (0: automatic)")
+    return ap.parse_args()
+
+
+# --------------------------------------------------------------------------- helpers
+class Clocks:
+    """Samples SM clock, power and throttle reasons with nvidia-smi while running."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.dev = device_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-i", str(self.dev), "-lms", "200"], stdout=open(self.path, "w"),
+                                         stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        rows = []
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower().startswith("active")})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def measured_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profiled_traffic(kernel: str):
+    """DRAM bytes per launch of `kernel` from the committed ncu summaries
+    (a line 'dram_bytes_per_launch <kernel> <workload> <bytes>'), else None."""
+    d = os.path.join(ROOT, "profiles")
+    if not os.path.isdir(d):
+        return None
+    for f in sorted(os.listdir(d)):
+        if not f.endswith(".md"):
+            continue
+        for line in open(os.path.join(d, f)):
+            parts = line.strip().strip("`").split()
+            if len(parts) == 4 and parts[0] == "dram_bytes_per_launch" and parts[1] == kernel:
+                return float(parts[3])
+    return None
+
+
+def dist_init(n_gpus):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+        pg = dist
+    return rank, world, local, pg
+
+
+def max_over_ranks(pg, value: float, device: str = "cuda") -> float:
+    """Slowest rank's time (every rank calls this with its own value)."""
+    if pg is None:
+        return value
+    import torch
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_params(workload: str, rank: int):
+    """Rank r routes an independent replica of the workload (seed + 1000 r)."""
+    from dataclasses import replace
+
+    from grotor_b200.synth import WORKLOADS
+    base = WORKLOADS[workload]
+    return replace(base, seed=base.seed + 1000 * rank)
+
+
+def barrier(pg):
+    if pg is not None:
+        import torch
+        pg.barrier()
+        torch.cuda.synchronize()
+
+
+def stride_sample(design, target):
+    """Every k-th net of the stage order (sizes representative of the design)."""
+    order = design.order
+    k = max(1, len(order) // max(target, 1))
+    return order[::k][:target]
+
+
+def sub_nets(design, ids):
+    """Topology and geometry of a subset of nets, re-indexed 0..m-1."""
+    from grotor_b200.router import NetArrays
+    n = design.nets
+
+    def csr(off, data, width=1):
+        counts = off[ids + 1] - off[ids]
+        new_off = np.zeros(len(ids) + 1, np.int64)
+        np.cumsum(counts, out=new_off[1:])
+        idx = np.concatenate([np.arange(off[i], off[i + 1]) for i in ids]) if len(ids) else np.zeros(0, np.int64)
+        if width == 1:
+            return new_off.astype(np.int32), data[idx]
+        return new_off.astype(np.int32), data.reshape(-1, width)[idx].reshape(-1)
+
+    no, nodes = csr(n.node_off, n.nodes)
+    _, parents = csr(n.node_off, n.parents)
+    po, points = csr(n.point_off, n.points)
+    ho, hsegs = csr(n.hseg_off, n.hsegs, 2)
+    vo, vsegs = csr(n.vseg_off, n.vsegs, 2)
+    cap = (n.route_off[ids + 1] - n.route_off[ids]).astype(np.int64)
+    ro = np.zeros(len(ids) + 1, np.int64)
+    np.cumsum(cap, out=ro[1:])
+    return NetArrays(no, nodes, parents, ro, po, points, ho, hsegs, vo, vsegs)
+
+
+def cpu_stage(design, n_sample, threads):
+    """The reference's CPU batching (oracle/_ref, its own code) and the CPU
+    restatement of its DAG code on a stride sample; returns (seconds, info)."""
+    import oracle
+    from grotor_b200.router import plan_from_batches
+    g = design.grid
+    ids = np.sort(stride_sample(design, n_sample))  # net ids of the sample
+    # keep the stage order among the sample
+    pos = np.empty(design.n_subnets, np.int64)
+    pos[design.order] = np.arange(design.n_subnets)
+    ids = ids[np.argsort(pos[ids], kind="stable")]
+    sub = sub_nets(design, ids)
+    order = np.arange(len(ids), dtype=np.int32)
+    harness = os.path.join(ROOT, "oracle", "_ref", "ref_harness")
+    kind = "port"
+    t0 = time.perf_counter()
+    if os.path.exists(harness):
+        with tempfile.TemporaryDirectory() as w:
+            np.array([g.L, g.X, g.Y, g.DIR], np.int32).tofile(os.path.join(w, "meta.i32"))
+            order.tofile(os.path.join(w, "order.i32"))
+            for name in ("point_off", "points", "hseg_off", "hsegs", "vseg_off", "vsegs"):
+                np.asarray(getattr(sub, name), np.int32).tofile(os.path.join(w, f"{name}.i32"))
+            res = subprocess.run([harness, "batch", w, str(BATCH_LIMIT), "1"], capture_output=True, text=True,
+                                 check=True)
+            batch_ms = float(res.stdout.split("elapsed_ms=")[1].split()[0])
+            bo = np.fromfile(os.path.join(w, "ref_batch_of.i32"), np.int32)
+        kind = "reference"
+    else:
+        tb = time.perf_counter()
+        bo, _ = oracle.batches(g.X, g.Y, order, sub.point_off, sub.points, sub.hseg_off, sub.hsegs, sub.vseg_off,
+                               sub.vsegs, BATCH_LIMIT, 1)
+        batch_ms = (time.perf_counter() - tb) * 1e3
+    nb = int(bo.max()) + 1 if len(bo) else 0
+    pids, off = plan_from_batches(order, bo, nb)
+    og = oracle.OrcGrid(g.L, g.X, g.Y, g.DIR, g.unit_wire, g.unit_via, g.short_costs, g.x_edge_len, g.y_edge_len,
+                        g.capacity)
+    td = time.perf_counter()
+    r = oracle.lshape_stage(og, pids, off, sub.node_off, sub.nodes, sub.parents, sub.route_off, threads=threads)
+    dag_ms = (time.perf_counter() - td) * 1e3
+    assert r["status"] == 0
+    wall = time.perf_counter() - t0
+    sec = (batch_ms + dag_ms) / 1e3
+    return sec, {"nets": int(len(ids)), "batches": nb, "batching_ms": batch_ms, "dag_ms": dag_ms, "kind": kind,
+                 "wall_s": wall}
+
+
+# --------------------------------------------------------------------------- own arm
+def run_grotor(args):
+    import torch
+
+    from grotor_b200 import Router
+    from grotor_b200.synth import Design
+
+    rank, world, local, pg = dist_init(args.gpus)
+    torch.cuda.set_device(local)
+    params = replica_params(args.workload, rank)
+    t = time.perf_counter()
+    design = Design(params)
+    log(f"[rank {rank}] design {args.workload}: {design.n_subnets} nets prepared in {time.perf_counter() - t:.1f}s")
+    r = Router(design.grid, device=local)
+    r.upload_nets(design.nets)
+    stream = torch.cuda.ExternalStream(r.stream_handle, device=torch.device("cuda", local))
+    order = design.order
+    n_nets = design.n_subnets
+
+    def step(mode):
+        r.reset()
+        r.generate_batches_rsmt(order, BATCH_LIMIT, 1, mode)
+        return r.lshape_route(mode)
+
+    for _ in range(args.warmup):
+        step("persistent")
+    barrier(pg)
+    torch.cuda.synchronize()
+    clocks = Clocks(local)
+    clocks.start()
+    l0 = r.kernel_launches
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    bt, dt = [], []
+    e0.record(stream)
+    for _ in range(args.steps):
+        st = step("persistent")
+        bt.append(st["batching_ms"])
+        dt.append(st["dag_ms"])
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier(pg)
+    clk = clocks.stop()
+    launches = r.kernel_launches - l0
+    ms = e0.elapsed_time(e1)
+    ms_max = max_over_ranks(pg, ms)
+    value = world * args.steps * n_nets / (ms_max / 1e3)
+    ms_step = ms_max / args.steps
+    routes_p = r.read_routes()
+    tables_p = r.read_tables()
+    ids, off = r.plan()
+    stats_p = r.stats()
+
+    # End to end through the public API with host buffers: H2D of the step's
+    # topology and order from pinned memory, batching + stage, D2H of routes.
+    nets = design.nets
+    pinned = {}
+    for name in ("node_off", "nodes", "parents", "route_off", "point_off", "points", "hseg_off", "hsegs",
+                 "vseg_off", "vsegs"):
+        a = np.asarray(getattr(nets, name))
+        tt = torch.empty(a.shape, dtype=getattr(torch, str(a.dtype)), pin_memory=True)
+        tt.numpy()[...] = a
+        pinned[name] = tt
+    from grotor_b200.router import NetArrays
+    host_nets = NetArrays(*[pinned[k].numpy() for k in ("node_off", "nodes", "parents", "route_off", "point_off",
+                                                        "points", "hseg_off", "hsegs", "vseg_off", "vsegs")])
+    order_pin = torch.empty(len(order), dtype=torch.int32, pin_memory=True)
+    order_pin.numpy()[...] = order
+    h2d = sum(v.numel() * v.element_size() for v in pinned.values()) + order_pin.numel() * 4
+    d2h = int(nets.route_off[-1]) * 4 + len(order) * 4 + 16
+    torch.cuda.synchronize()
+    e2 = torch.cuda.Event(enable_timing=True)
+    e3 = torch.cuda.Event(enable_timing=True)
+    e2.record(stream)
+    for _ in range(args.steps):
+        r.upload_nets(host_nets)
+        r.reset()
+        r.generate_batches_rsmt(order_pin.numpy(), BATCH_LIMIT, 1, "persistent")
+        r.lshape_route("persistent")
+        routes_e2e = r.read_routes()
+    e3.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = max_over_ranks(pg, e2.elapsed_time(e3))
+    e2e_value = world * args.steps * n_nets / (e2e_ms / 1e3)
+    assert np.array_equal(routes_e2e, routes_p)
+
+    result = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": args.workload, "grid": [design.grid.X, design.grid.Y, design.grid.L + 1],
+                   "nets": n_nets, "batches": int(stats_p["n_batches"]), "batch_limit": BATCH_LIMIT,
+                   "executor": "persistent", "parallelism": f"replicas{world}",
+                   "l2": "inputs larger than L2 (cost/prefix/demand tables %.0f MB)" % (
+                       design.grid.cells * 32 / 1e6)},
+        "stage": {"batching_ms": float(np.mean(bt)), "dag_ms": float(np.mean(dt)),
+                  "wirelength": stats_p["wirelength"], "vias": stats_p["vias"]},
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
+        "gpu_launches": int(launches),
+        "clocks": clk,
+    }
+
+    # Roofline of the two kernels of the persistent form.
+    lib = r._lib
+    import ctypes as C
+    out = np.zeros(4, np.float64)
+    gs = design.grid.struct()
+    P = lambda a: np.ascontiguousarray(a).ctypes.data_as(C.c_void_p)  # noqa: E731
+    rc = lib.grb_stage_traffic(C.byref(gs), len(off) - 1, P(off), P(ids), P(nets.node_off), P(nets.nodes),
+                               P(nets.parents), P(nets.route_off), P(routes_p), P(nets.point_off), P(nets.hseg_off),
+                               P(nets.hsegs), P(nets.vseg_off), P(nets.vsegs), 1, P(out))
+    assert rc == 0
+    stage_bytes = out[0] + out[1] + out[2]
+    batch_bytes = out[3]
+    peak, peak_kind = measured_peak()
+    stage_ms, batch_ms = float(np.mean(dt)), float(np.mean(bt))
+    kernels = {
+        "k_lshape_persistent": (stage_bytes, stage_ms),
+        "k_batch_persistent": (batch_bytes, batch_ms),
+    }
+    dom = max(kernels, key=lambda k: kernels[k][1])
+    roofs = {}
+    for k, (byt, kms) in kernels.items():
+        ach = byt / (kms / 1e3) / 1e9
+        roofs[k] = {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
+                    "traffic": profiled_traffic(k), "algorithmic_bytes": byt, "ms": kms,
+                    "peak_source": f"{peak_kind} hbm_gbs"}
+    result["roofline"] = dict(roofs[dom], kernel=dom)
+    result["roofline_all"] = roofs
+    result["algorithmic_bytes"] = {"refresh": out[0], "dp": out[1], "commit": out[2], "batching": out[3]}
+
+    if not args.no_compare:
+        comp = {"persistent": {"ms": ms_step, "batching_ms": batch_ms, "dag_ms": stage_ms}}
+        identical = True
+        for mode in ("graph", "plain"):
+            step(mode)  # warm (graph capture)
+            torch.cuda.synchronize()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            st = step(mode)
+            b.record(stream)
+            torch.cuda.synchronize()
+            comp[mode] = {"ms": a.elapsed_time(b), "batching_ms": st["batching_ms"], "dag_ms": st["dag_ms"]}
+            same = np.array_equal(r.read_routes(), routes_p) and np.array_equal(
+                r.read_tables()["demand_half"], tables_p["demand_half"])
+            identical &= bool(same)
+        comp["speedup_persistent_vs_plain"] = comp["plain"]["ms"] / ms_step
+        comp["speedup_persistent_vs_graph"] = comp["graph"]["ms"] / ms_step
+        comp["routes_identical"] = identical
+        result["executors"] = comp
+
+    if rank == 0 and world == 1 and not args.no_cpu:
+        threads = os.cpu_count() or 1
+        target = args.cpu_nets or 60000
+        sec, info = cpu_stage(design, target, threads)
+        result["cpu_baseline"] = {"value": info["nets"] / sec, "unit": UNIT, "cores": threads, "kind": info["kind"],
+                                  "sample": (f"every {max(1, n_nets // target)}-th net of {args.workload} in stage "
+                                             f"order ({info['nets']} nets, {info['batches']} batches): reference "
+                                             f"CPU batching {info['batching_ms']:.0f} ms on 1 core + CPU DAG "
+                                             f"restatement {info['dag_ms']:.0f} ms on {threads} threads")}
+    r.close()
+    if pg is not None:
+        pg.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(result), flush=True)
+
+
+# --------------------------------------------------------------------------- reference arm
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from grotor_b200.synth import WORKLOADS, Design
+    design = Design(WORKLOADS[args.workload])
+    threads = os.cpu_count() or 1
+    target = args.cpu_nets or 30000
+    times, info = [], None
+    for i in range(args.warmup + args.steps):
+        sec, info = cpu_stage(design, target, threads)
+        log(f"reference step {i}: {sec:.2f}s ({info})")
+        if i >= args.warmup:
+            times.append(sec)
+    value = info["nets"] / float(np.mean(times))
+    sample = (f"every {max(1, design.n_subnets // target)}-th net of {args.workload} in stage order "
+              f"({info['nets']} nets, {info['batches']} batches): reference CPU batching (its own code, 1 core) "
+              f"+ CPU restatement of its DAG code on {threads} threads")
+    result = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": int(os.environ.get("WORLD_SIZE", "1")),
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": float(np.mean(times)) * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": args.workload, "grid": [design.grid.X, design.grid.Y, design.grid.L + 1],
+                   "nets": design.n_subnets, "batch_limit": BATCH_LIMIT, "parallelism": "host"},
+        "impl": "reference",
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": info["kind"], "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(result), flush=True)
+
+
+def main():
+    args = parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_grotor(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,228 @@
+// batching.cuh -- exact greedy first-fit net batching on the GPU.
+//
+// Semantics of the reference's CPU batching (generate_batches_cpu.hpp:7-73):
+// nets are taken in the given order; a net joins the first batch that holds
+// fewer than `limit` nets and none of whose marked cells contains one of the
+// net's query points; it then marks its RSMT h-segments (step sparsity*Y),
+// v-segments (step sparsity) and, at every point, the cell itself, its x
+// neighbours and the cell below in y (not above, reference :38).
+//
+// B200 algorithm (replaces the RT-core/OptiX and CPU paths, which produce the
+// same lists):
+//   * cellmask[cell] holds one bit per batch ("colour") already marking the cell;
+//   * nets are processed in chunks of 512 in order; per chunk:
+//       1. every net rasters its marks into a chunk-local bitmask per cell
+//          (bit = its position in the chunk) and ORs cellmask over its points
+//          -> forbidden colours from earlier chunks;
+//       2. every net ORs the chunk-local masks over its points, keeping bits of
+//          earlier chunk nets -> exact intra-chunk predecessors;
+//       3. one CTA solves first-fit inside the chunk by Jacobi iteration over
+//          the predecessor DAG (converges to the unique sequential solution),
+//          then applies batch capacities in order;
+//       4. every net ORs its colour into cellmask over its marks and clears the
+//          chunk-local masks.
+//   The chunks run inside one cooperative kernel with bounded grid barriers
+//   (persistent form) or as one launch per phase (plain form).
+#pragma once
+#include "common.cuh"
+
+namespace grb {
+
+constexpr int kChunk = 512;     // nets per chunk (== threads of the solve CTA)
+constexpr int kChunkWords = kChunk / 32;
+
+struct BatchState {
+    int X, Y, n, limit, sparsity, W;   // W: colour words per cell
+    const int* order;
+    const int* point_off; const int* points;
+    const int* hseg_off; const int* hsegs;
+    const int* vseg_off; const int* vsegs;
+    unsigned* cellmask;    // [X*Y][W]
+    unsigned* localmask;   // [X*Y][kChunkWords]
+    unsigned* fmask;       // [kChunk][W]
+    unsigned* pred;        // [kChunk][kChunkWords]
+    unsigned* fullmask;    // [W]
+    int* count;            // [32*W]
+    int* n_colors;         // [1]
+    int* batch_of;         // [n] colour per order position
+    int* rank;             // [n] position inside its batch
+    int* error;
+    int* error_info;
+};
+
+__device__ __forceinline__ void batch_error(const BatchState& B, int code, int info) {
+    if (atomicCAS(B.error, 0, code) == 0) *B.error_info = info;
+}
+
+// Visit every cell net `id` marks (duplicates allowed), lanes of a warp split
+// the work.
+template <class F>
+__device__ __forceinline__ void for_each_mark(const BatchState& B, int id, int lane, F f) {
+    const int hstep = B.sparsity * B.Y, vstep = B.sparsity;
+    for (int s = B.hseg_off[id]; s < B.hseg_off[id + 1]; ++s) {
+        const int a = B.hsegs[2 * s], b = B.hsegs[2 * s + 1];
+        if (b < a) continue;
+        const int cnt = (b - a) / hstep + 1;
+        for (int k = lane; k < cnt; k += 32) f(a + k * hstep);
+    }
+    for (int s = B.vseg_off[id]; s < B.vseg_off[id + 1]; ++s) {
+        const int a = B.vsegs[2 * s], b = B.vsegs[2 * s + 1];
+        if (b < a) continue;
+        const int cnt = (b - a) / vstep + 1;
+        for (int k = lane; k < cnt; k += 32) f(a + k * vstep);
+    }
+    const int p0 = B.point_off[id], np = B.point_off[id + 1] - p0;
+    for (int k = lane; k < 4 * np; k += 32) {
+        const int p = B.points[p0 + k / 4], x = p / B.Y, y = p - x * B.Y;
+        const int which = k & 3;
+        int cx = x, cy = y;
+        if (which == 0) cx = x - 1;
+        else if (which == 1) cy = y - 1;
+        else if (which == 3) cx = x + 1;
+        if (cx >= 0 && cx < B.X && cy >= 0) f(cx * B.Y + cy);
+    }
+}
+
+// Phase 1 for one net (warp): chunk-local raster and forbidden colours.
+__device__ __forceinline__ void batch_phase1(const BatchState& B, int s, int jj, int lane) {
+    const int id = B.order[s + jj];
+    const unsigned bit = 1u << (jj & 31);
+    const int word = jj >> 5;
+    for_each_mark(B, id, lane, [&](int q) { atomicOr(B.localmask + size_t(q) * kChunkWords + word, bit); });
+    const int p0 = B.point_off[id], p1 = B.point_off[id + 1];
+    for (int w = lane; w < B.W; w += 32) {
+        unsigned acc = 0;
+        for (int k = p0; k < p1; ++k) acc |= B.cellmask[size_t(B.points[k]) * B.W + w];
+        B.fmask[size_t(jj) * B.W + w] = acc;
+    }
+}
+
+// Phase 2 for one net (warp): predecessors inside the chunk.
+__device__ __forceinline__ void batch_phase2(const BatchState& B, int s, int jj, int lane) {
+    const int id = B.order[s + jj];
+    const int p0 = B.point_off[id], p1 = B.point_off[id + 1];
+    if (lane < kChunkWords) {
+        unsigned acc = 0;
+        if (lane * 32 < jj) {
+            for (int k = p0; k < p1; ++k) acc |= B.localmask[size_t(B.points[k]) * kChunkWords + lane];
+            if (lane == (jj >> 5)) acc &= (1u << (jj & 31)) - 1u;
+        }
+        B.pred[jj * kChunkWords + lane] = acc;
+    }
+}
+
+// Phase 4 for one net (warp): publish its colour, clear chunk-local masks.
+__device__ __forceinline__ void batch_phase4(const BatchState& B, int s, int jj, int lane) {
+    const int id = B.order[s + jj];
+    const int c = B.batch_of[s + jj];
+    const unsigned bit = 1u << (c & 31);
+    const int word = c >> 5;
+    for_each_mark(B, id, lane, [&](int q) {
+        atomicOr(B.cellmask + size_t(q) * B.W + word, bit);
+        unsigned* lm = B.localmask + size_t(q) * kChunkWords;
+#pragma unroll
+        for (int w = 0; w < kChunkWords; ++w) lm[w] = 0;
+    });
+}
+
+// Phase 3 (one CTA of kChunk threads): first-fit inside the chunk.
+// smem: F[kChunk][W], P[kChunk][kChunkWords], col[kChunk], cnt[32W], full[W].
+__device__ void batch_phase3(const BatchState& B, int s, unsigned* smem) {
+    const int tid = threadIdx.x;
+    const int m = min(kChunk, B.n - s);
+    const int W = B.W, C = 32 * W;
+    unsigned* F = smem;
+    unsigned* P = F + kChunk * W;
+    int* col = reinterpret_cast<int*>(P + kChunk * kChunkWords);
+    int* cnt = col + kChunk;
+    unsigned* full = reinterpret_cast<unsigned*>(cnt + C);
+    __shared__ int first_bad, overflow;
+    for (int k = tid; k < m * W; k += blockDim.x) F[k] = B.fmask[k];
+    for (int k = tid; k < m * kChunkWords; k += blockDim.x) P[k] = B.pred[k];
+    for (int k = tid; k < C; k += blockDim.x) cnt[k] = B.count[k];
+    for (int k = tid; k < W; k += blockDim.x) full[k] = B.fullmask[k];
+    if (tid < kChunk) col[tid] = -1;
+    if (tid == 0) overflow = 0;
+    __syncthreads();
+    int fixed = 0;  // nets below `fixed` are final
+    while (true) {
+        // Jacobi sweeps until the colouring is a fixed point.
+        while (true) {
+            int mine = tid < m ? col[tid] : -1;
+            if (tid < m && tid >= fixed) {
+                int c = 0;
+                while (true) {
+                    int w = c >> 5;
+                    if (w >= W) { c = C; break; }
+                    unsigned used = F[tid * W + w] | full[w] | ((1u << (c & 31)) - 1u);
+                    while (used == 0xffffffffu) {
+                        if (++w >= W) break;
+                        used = F[tid * W + w] | full[w];
+                    }
+                    if (w >= W) { c = C; break; }
+                    c = w * 32 + __ffs(~used) - 1;
+                    bool hit = false;
+                    for (int pw = 0; pw <= (tid >> 5) && !hit; ++pw) {
+                        unsigned bits = P[tid * kChunkWords + pw];
+                        while (bits) {
+                            const int i = pw * 32 + __ffs(bits) - 1;
+                            bits &= bits - 1;
+                            if (col[i] == c) { hit = true; break; }
+                        }
+                    }
+                    if (!hit) break;
+                    ++c;
+                }
+                if (c >= C) { overflow = 1; c = C - 1; }
+                mine = c;
+            }
+            __syncthreads();
+            const bool changed = tid < m && col[tid] != mine;
+            if (tid < m) col[tid] = mine;
+            if (!__syncthreads_or(changed)) break;
+        }
+        if (overflow) break;
+        // Batch capacities in order: find the first net that would exceed one.
+        if (tid == 0) first_bad = m;
+        __syncthreads();
+        int rank_local = 0;
+        if (tid < m) {
+            const int c = col[tid];
+            for (int i = 0; i < tid; ++i) rank_local += col[i] == c;
+            if (cnt[c] + rank_local >= B.limit) atomicMin(&first_bad, tid);
+        }
+        __syncthreads();
+        const int bad = first_bad;
+        if (bad >= m) {
+            if (tid < m) {
+                B.batch_of[s + tid] = col[tid];
+                B.rank[s + tid] = cnt[col[tid]] + rank_local;
+            }
+            __syncthreads();
+            if (tid < m) atomicAdd(&cnt[col[tid]], 1);
+            __syncthreads();
+            break;
+        }
+        // Net `bad` finds its colour full; so does every later net.
+        const int full_colour = col[bad];
+        __syncthreads();
+        if (tid == 0) full[full_colour >> 5] |= 1u << (full_colour & 31);
+        fixed = bad;
+        __syncthreads();
+    }
+    if (overflow) {
+        if (tid == 0) batch_error(B, kELimit, s);
+        return;
+    }
+    int top = 0;
+    if (tid < m) top = col[tid] + 1;
+    for (int k = tid; k < C; k += blockDim.x) B.count[k] = cnt[k];
+    for (int k = tid; k < W; k += blockDim.x) B.fullmask[k] = full[k];
+    if (top) atomicMax(B.n_colors, top);
+}
+
+__host__ __device__ __forceinline__ size_t phase3_smem_bytes(int W) {
+    return size_t(kChunk) * W * 4 + size_t(kChunk) * kChunkWords * 4 + kChunk * 4 + size_t(32) * W * 4 + W * 4;
+}
+
+}  // namespace grb

@@ -1,0 +1,79 @@
+// commit.cuh -- demand commit and rip-up of routed nets.
+//
+// Semantics of the reference's batch commit (demand.cuh:410-493): wires first
+// (each unit edge gets K, its timestamp becomes the batch stamp, both segment
+// endpoints are stamped), then -- after every wire of the batch is in -- vias:
+// each via layer whose cell was not stamped by a wire of this batch adds K to
+// its single neighbouring edge at a track end, else K/2 to the two edges it
+// lands between.  K = -1 removes a route.  Half-unit integer demand makes every
+// update exact and order-free, so warps may commit in any order.
+#pragma once
+#include "common.cuh"
+
+namespace grb {
+
+__device__ __forceinline__ const int* net_routes(const Plan& P, int id) { return P.routes + P.route_off[id]; }
+
+// One warp commits the wire segments of net `id`; lanes split each segment's
+// unit edges.  Returns nothing; statistics are accumulated atomically.
+__device__ __forceinline__ void commit_net_wires(const Tables& T, const Plan& P, int id, int stamp, int K,
+                                                 int lane, int list) {
+    const int* r = net_routes(P, id);
+    const int words = r[0];
+    double length = 0;
+    for (int i = 1; i < words; i += 2) {
+        const int a = r[i], b = r[i + 1], layer = a / T.XY;
+        if (layer != b / T.XY) continue;
+        const int ra = a - layer * T.XY, rb = b - layer * T.XY;
+        const int x0 = ra / T.Y, y0 = ra - x0 * T.Y, x1 = rb / T.Y, y1 = rb - x1 * T.Y;
+        const bool ay = x0 == x1;
+        const int lo = ay ? min(y0, y1) : min(x0, x1), hi = ay ? max(y0, y1) : max(x0, x1);
+        if (lane == 0) { T.ts[a] = stamp; T.ts[b] = stamp; }
+        for (int pos = lo + lane; pos < hi; pos += 32) {
+            const int c = layer * T.XY + (ay ? x0 * T.Y + pos : pos * T.Y + y0);
+            atomicAdd(T.demand + c, 2 * K);
+            T.ts[c] = stamp;
+            mark_edge_dirty(T, c, list);
+            length += ay ? T.ylen[pos] : T.xlen[pos];
+        }
+    }
+    for (int s = 16; s; s >>= 1) length += __shfl_down_sync(0xffffffffu, length, s);
+    if (lane == 0 && length != 0.0) atomicAdd(T.wirelength, length * K);
+}
+
+__device__ __forceinline__ void add_via_demand(const Tables& T, int c, int half, int list) {
+    atomicAdd(T.demand + c, half);
+    mark_edge_dirty(T, c, list);
+}
+
+// One warp commits the via segments of net `id` (lanes over segments).
+__device__ __forceinline__ void commit_net_vias(const Tables& T, const Plan& P, int id, int stamp, int K,
+                                                int lane, int list) {
+    const int* r = net_routes(P, id);
+    const int words = r[0];
+    long long vias = 0;
+    for (int i = 1 + 2 * lane; i < words; i += 64) {
+        const int a = r[i], b = r[i + 1];
+        const int la = a / T.XY, lb = b / T.XY;
+        const int low = min(la, lb), high = max(la, lb);
+        if (low == high) continue;
+        const int ra = a - la * T.XY, x = ra / T.Y, y = ra - x * T.Y;
+        vias += high - low;
+        for (int layer = low; layer < high; ++layer) {
+            const int c = layer * T.XY + x * T.Y + y;
+            if (T.ts[c] >= stamp) continue;
+            const bool ay = along_y(T, layer);
+            const int pos = ay ? y : x, len = ay ? T.Y : T.X, stride = ay ? 1 : T.Y;
+            if (!pos) add_via_demand(T, c, 2 * K, list);
+            else if (pos == len - 1) add_via_demand(T, c - stride, 2 * K, list);
+            else {
+                add_via_demand(T, c - stride, K, list);
+                add_via_demand(T, c, K, list);
+            }
+        }
+    }
+    for (int s = 16; s; s >>= 1) vias += __shfl_down_sync(0xffffffffu, vias, s);
+    if (lane == 0 && vias) atomicAdd(T.vias, static_cast<unsigned long long>(vias * K));
+}
+
+}  // namespace grb

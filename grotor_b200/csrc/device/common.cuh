@@ -1,0 +1,153 @@
+// common.cuh -- device-side state view and shared helpers for the routing path.
+//
+// Grid layout follows the reference router (router_state.hpp:267):
+// IDX(l,x,y) = (l*X + x)*Y + y, and layer l carries wires along y when
+// ((l & 1) ^ DIR) is 1, along x otherwise.  Demand is int32 half-units: a wire
+// edge adds 2, a split via landing adds 1 to each neighbour (demand.cuh:300-304
+// uses 1.0f and 0.5f), so demand * 0.5f reproduces the reference's float.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace grb {
+
+constexpr double kInf = 1e22;   // router_state.hpp:271
+constexpr int kMaxLayers = 10;  // lshape_warp.cuh:314 asserts L <= 10
+constexpr int kTrackGroup = 32; // tracks per prefix group (one per lane)
+
+enum : int {
+    kOk = 0, kEInval = 1, kENoMem = 2, kECuda = 3, kETimedOut = 4, kELimit = 5,
+};
+
+// Device tables of one routing context.  Copied by value into every kernel.
+struct Tables {
+    int L, X, Y, DIR, XY;
+    int cells;
+    double unit_wire, unit_via, of_scale;
+    const double* short_costs;
+    const int* xlen;
+    const int* ylen;
+    const float* capacity;
+    int* demand;           // half-units
+    int* ts;               // commit timestamps
+    float* wcost;
+    float* vcost;
+    double* presum;
+    unsigned* dirty_wire;  // one bit per cell
+    unsigned* dirty_via;   // one bit per cell
+    // Prefix groups: kTrackGroup adjacent tracks of one layer.
+    int group_base[kMaxLayers + 1];
+    unsigned* group_flag;  // [n_groups]
+    int* group_list[2];    // double-buffered work lists
+    int* group_count;      // [2]
+    int* via_list[2];      // dirty via bitmap words
+    int* via_count;        // [2]
+    int n_groups;
+    double* wirelength;
+    unsigned long long* vias;
+    int* error;            // first error code
+    int* error_info;       // detail (net index, ...)
+};
+
+// Topology of the current plan (device pointers).
+struct Plan {
+    const int* node_off;       // [n_nets+1], indexed by net id
+    const int* nodes;          // l*X*Y + x*Y + y, l == L for Steiner nodes
+    const int* parents;        // parent < child, -1 at the root
+    const long long* route_off;// [n_nets+1] word offsets into routes
+    int* routes;               // [count, a0, b0, ...] per net
+    const int* ids;            // net ids in execution order
+    const int* batch_off;      // [n_batches+1] into ids
+    int n_batches;
+};
+
+__device__ __forceinline__ bool along_y(const Tables& T, int l) { return ((l & 1) ^ T.DIR) != 0; }
+__device__ __forceinline__ int cell_index(const Tables& T, int l, int x, int y) { return (l * T.X + x) * T.Y + y; }
+
+__device__ __forceinline__ void set_error(const Tables& T, int code, int info) {
+    if (atomicCAS(T.error, 0, code) == 0) *T.error_info = info;
+}
+
+__device__ __forceinline__ bool bit_test(const unsigned* bits, int i) { return (bits[i >> 5] >> (i & 31)) & 1u; }
+
+__device__ __forceinline__ int track_length(const Tables& T, int l) { return along_y(T, l) ? T.Y : T.X; }
+
+// Mark the via cost of cell c dirty and queue its bitmap word once.
+__device__ __forceinline__ void mark_via_dirty(const Tables& T, int c, int list) {
+    const unsigned bit = 1u << (c & 31);
+    unsigned* word = T.dirty_via + (c >> 5);
+    if (*reinterpret_cast<volatile unsigned*>(word) & bit) return;
+    if (atomicOr(word, bit) == 0) {
+        const int k = atomicAdd(T.via_count + list, 1);
+        T.via_list[list][k] = c >> 5;
+    }
+}
+
+__device__ __forceinline__ void mark_group_dirty(const Tables& T, int l, int track, int list) {
+    const int g = T.group_base[l] + track / kTrackGroup;
+    if (*reinterpret_cast<volatile unsigned*>(T.group_flag + g)) return;
+    if (atomicOr(T.group_flag + g, 1u) == 0) {
+        const int k = atomicAdd(T.group_count + list, 1);
+        T.group_list[list][k] = g;
+    }
+}
+
+// A demand change on edge cell c invalidates its wire cost, its own via cost
+// and the via cost of the next cell along the track (fenwick.cuh:27-38).
+__device__ __forceinline__ void mark_edge_dirty(const Tables& T, int c, int list) {
+    const int l = c / T.XY, rem = c - l * T.XY, x = rem / T.Y, y = rem - x * T.Y;
+    const bool ay = along_y(T, l);
+    const int pos = ay ? y : x, len = ay ? T.Y : T.X, stride = ay ? 1 : T.Y;
+    const unsigned bit = 1u << (c & 31);
+    unsigned* word = T.dirty_wire + (c >> 5);
+    if (!(*reinterpret_cast<volatile unsigned*>(word) & bit)) atomicOr(word, bit);
+    mark_via_dirty(T, c, list);
+    if (pos + 1 < len) mark_via_dirty(T, c + stride, list);
+    mark_group_dirty(T, l, ay ? x : y, list);
+}
+
+// Grid-wide barrier for cooperative launches.  Every wait is bounded by the
+// global timer; on expiry the kernel records kETimedOut and callers return.
+struct GridSync {
+    unsigned* count;
+    unsigned* generation;
+    unsigned long long timeout_ns;
+};
+
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+__device__ __forceinline__ bool grid_sync(const GridSync& s, const Tables& T) {
+    __shared__ int ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        ok = 1;
+        volatile unsigned* gen = s.generation;
+        const unsigned g = *gen;
+        __threadfence();
+        const unsigned arrived = atomicAdd(s.count, 1u);
+        if (arrived == gridDim.x - 1) {
+            *reinterpret_cast<volatile unsigned*>(s.count) = 0;
+            __threadfence();
+            atomicAdd(s.generation, 1u);
+        } else {
+            const unsigned long long start = global_ns();
+            unsigned spins = 0;
+            while (*gen == g) {
+                if ((++spins & 63) == 0) {
+                    if (global_ns() - start > s.timeout_ns) { set_error(T, kETimedOut, blockIdx.x); ok = 0; break; }
+                    if (*reinterpret_cast<volatile int*>(T.error) == kETimedOut) { ok = 0; break; }
+                }
+                __nanosleep(64);
+            }
+        }
+        __threadfence();
+    }
+    __syncthreads();
+    return ok != 0;
+}
+
+}  // namespace grb

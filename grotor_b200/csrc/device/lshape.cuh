@@ -1,0 +1,255 @@
+// lshape.cuh -- L-shape pattern routing with layer assignment, one warp per net.
+//
+// Semantics are those of the reference's tree DP (lshape_thread.cuh:18-171,
+// lshape_warp.cuh:8-446): per tree node a table dist[low][high] over layer
+// ranges (via stack cost inside the range, INF where a pin's layer falls
+// outside); children are merged into their parent in descending node order;
+// an edge is a straight wire or an L with a via stack at the corner; strict '<'
+// keeps the first minimum in the reference's loop order; the root takes the
+// first minimal range; traceback and segment emission follow node order.
+//
+// B200 mapping: all cost gathers of a net (via stacks at nodes and corners,
+// wire costs of both legs on every layer) are issued up front by the 32 lanes
+// into a per-warp shared-memory arena, so a net pays one memory latency; the
+// DP itself then runs from shared memory with lanes over layers.  The
+// reference keeps 81 doubles per node in global scratch and gathers inside the
+// DP loop.
+#pragma once
+#include "commit.cuh"
+#include "common.cuh"
+
+namespace grb {
+
+__host__ __device__ __forceinline__ int tri_count(int L) { return L * (L + 1) / 2; }
+__device__ __forceinline__ int tri(int L, int lo, int hi) { return lo * L - lo * (lo - 1) / 2 + (hi - lo); }
+
+struct Arena {
+    double* dist;          // [nmax][TT]
+    double* w1;            // [nmax][L] first leg (or straight) wire cost
+    double* w2;            // [nmax][L] second leg wire cost
+    float* vA;             // [nmax][L] via cost at corner (x, py)
+    float* vB;             // [nmax][L] via cost at corner (px, y)
+    float* vN;             // [nmax][L] via cost at the node
+    unsigned short* from;  // [nmax][TT] choice*L*L + curl*L + parl
+    int* range;            // [nmax] chosen range lo*L+hi
+    double* cur;           // [L]
+    double* diag;          // [L]
+    double* mcp;           // [TT]
+    int* cur_from;         // [L]
+    int* pdiag;            // [L]
+};
+
+__host__ __device__ __forceinline__ size_t arena_bytes(int L, int nmax) {
+    const size_t TT = tri_count(L);
+    size_t b = 0;
+    b += nmax * TT * 8 + 2 * size_t(nmax) * L * 8 + 3 * size_t(nmax) * L * 4;
+    b = (b + 7) & ~size_t(7);
+    b += 2 * L * 8 + TT * 8;
+    b += nmax * TT * 2;
+    b = (b + 7) & ~size_t(7);
+    b += nmax * 4 + 2 * L * 4;
+    return (b + 15) & ~size_t(15);
+}
+
+__device__ __forceinline__ Arena carve_arena(char* base, int L, int nmax) {
+    const int TT = tri_count(L);
+    Arena A;
+    char* p = base;
+    A.dist = reinterpret_cast<double*>(p); p += size_t(nmax) * TT * 8;
+    A.w1 = reinterpret_cast<double*>(p); p += size_t(nmax) * L * 8;
+    A.w2 = reinterpret_cast<double*>(p); p += size_t(nmax) * L * 8;
+    A.vA = reinterpret_cast<float*>(p); p += size_t(nmax) * L * 4;
+    A.vB = reinterpret_cast<float*>(p); p += size_t(nmax) * L * 4;
+    A.vN = reinterpret_cast<float*>(p); p += size_t(nmax) * L * 4;
+    p = reinterpret_cast<char*>((reinterpret_cast<uintptr_t>(p) + 7) & ~uintptr_t(7));
+    A.cur = reinterpret_cast<double*>(p); p += L * 8;
+    A.diag = reinterpret_cast<double*>(p); p += L * 8;
+    A.mcp = reinterpret_cast<double*>(p); p += TT * 8;
+    A.from = reinterpret_cast<unsigned short*>(p); p += size_t(nmax) * TT * 2;
+    p = reinterpret_cast<char*>((reinterpret_cast<uintptr_t>(p) + 7) & ~uintptr_t(7));
+    A.range = reinterpret_cast<int*>(p); p += nmax * 4;
+    A.cur_from = reinterpret_cast<int*>(p); p += L * 4;
+    A.pdiag = reinterpret_cast<int*>(p);
+    return A;
+}
+
+__device__ __forceinline__ double wire_cost(const Tables& T, int l, int xmin, int xmax, int ymin, int ymax) {
+    // prefix_scan.cuh:10-40 (wire_segment_cost)
+    return T.presum[cell_index(T, l, xmax, ymax)] - T.presum[cell_index(T, l, xmin, ymin)];
+}
+
+// Route one net.  All 32 lanes of the warp call this with the same id.
+// Returns false (and records kELimit) if the net's route storage is too small.
+__device__ void lshape_net(const Tables& T, const Plan& P, int id, int stamp, const Arena& A, int lane,
+                           bool fuse_wires, int list) {
+    const int L = T.L, Y = T.Y, XY = T.XY, TT = tri_count(L);
+    const int off = P.node_off[id], N = P.node_off[id + 1] - off;
+    const int* nd = P.nodes + off;
+    const int* par = P.parents + off;
+
+    // 1. Gather every cost the DP reads.
+    for (int q = lane; q < N * L; q += 32) {
+        const int i = q / L, l = q - i * L;
+        const int node = nd[i], r = node % XY, x = r / Y, y = r - x * Y;
+        A.vN[q] = T.vcost[l * XY + r];
+        if (i > 0) {
+            const int pr = nd[par[i]] % XY, px = pr / Y, py = pr - px * Y;
+            const int minx = min(x, px), maxx = max(x, px), miny = min(y, py), maxy = max(y, py);
+            const bool ay = along_y(T, l);
+            if (x == px || y == py) {
+                const bool valid = ay ? (x == px) : (y == py);
+                A.w1[q] = valid ? wire_cost(T, l, minx, maxx, miny, maxy) : 0.0;
+            } else {
+                A.w1[q] = ay ? wire_cost(T, l, x, x, miny, maxy) : wire_cost(T, l, minx, maxx, y, y);
+                A.w2[q] = ay ? wire_cost(T, l, px, px, miny, maxy) : wire_cost(T, l, minx, maxx, py, py);
+                A.vA[q] = T.vcost[cell_index(T, l, x, py)];
+                A.vB[q] = T.vcost[cell_index(T, l, px, y)];
+            }
+        }
+    }
+    __syncwarp();
+    // 2. Via stacks at every node (lshape_thread.cuh:40-50).
+    for (int q = lane; q < N * L; q += 32) {
+        const int i = q / L, lo = q - i * L;
+        const int fixed = nd[i] / XY;
+        double acc = 0;
+        for (int hi = lo; hi < L; ++hi) {
+            if (hi > lo) acc = acc + static_cast<double>(A.vN[i * L + hi - 1]);
+            A.dist[i * TT + tri(L, lo, hi)] = (fixed < L && (lo > fixed || hi < fixed)) ? kInf : acc;
+        }
+    }
+    __syncwarp();
+    // 3. Children in descending node order (lshape_thread.cuh:51-115).
+    for (int i = N - 1; i >= 1; --i) {
+        const int p = par[i];
+        const double* di = A.dist + i * TT;
+        if (lane < L) {
+            const int l = lane;
+            double best = kInf;
+            int bf = 0;
+            for (int lo = 0; lo <= l; ++lo)
+                for (int hi = l; hi < L; ++hi) {
+                    const double v = di[tri(L, lo, hi)];
+                    if (v < best) { best = v; bf = lo * L + hi; }
+                }
+            A.cur[l] = best;
+            A.cur_from[l] = bf;
+        }
+        __syncwarp();
+        if (lane < L) {
+            const int pl = lane;
+            const int node = nd[i] % XY, x = node / Y, y = node - x * Y;
+            const int pn = nd[p] % XY, px = pn / Y, py = pn - px * Y;
+            double best = kInf;
+            int pb = 0;
+            if (x == px || y == py) {
+                const bool valid = along_y(T, pl) ? (x == px) : (y == py);
+                if (valid) {
+                    best = A.cur[pl] + A.w1[i * L + pl];
+                    pb = A.cur_from[pl] * L * L + pl * L + pl;
+                }
+            } else {
+                for (int cl = (pl & 1) ^ 1; cl < L; cl += 2) {
+                    const double cost = A.cur[cl] + A.w1[i * L + cl];
+                    double cost2 = 0;
+                    const float* v = along_y(T, cl) ? A.vA + i * L : A.vB + i * L;
+                    for (int l = min(cl, pl) + 1; l < max(cl, pl); ++l) cost2 += static_cast<double>(v[l]);
+                    cost2 += A.w2[i * L + pl];
+                    if (cost + cost2 < best) {
+                        best = cost + cost2;
+                        pb = A.cur_from[cl] * L * L + cl * L + pl;
+                    }
+                }
+            }
+            A.diag[pl] = best;
+            A.pdiag[pl] = pb;
+        }
+        __syncwarp();
+        if (lane < L) {
+            const int lo = lane;
+            double c = A.diag[lo];
+            int path = A.pdiag[lo];
+            for (int hi = lo; hi < L; ++hi) {
+                if (hi > lo && !(c <= A.diag[hi])) { c = A.diag[hi]; path = A.pdiag[hi]; }
+                const int t = tri(L, lo, hi);
+                A.mcp[t] = c;
+                A.from[i * TT + t] = static_cast<unsigned short>(path);
+            }
+        }
+        __syncwarp();
+        for (int t = lane; t < TT; t += 32) A.dist[p * TT + t] += A.mcp[t];
+        __syncwarp();
+    }
+    // 4. Root range and traceback (lshape_thread.cuh:117-127).
+    if (lane == 0) {
+        int choice = 0, best_t = 0;
+        for (int lo = 0; lo < L; ++lo)
+            for (int hi = lo; hi < L; ++hi) {
+                const int t = tri(L, lo, hi);
+                if (A.dist[t] < A.dist[best_t]) { best_t = t; choice = lo * L + hi; }
+            }
+        A.range[0] = choice;
+        if (!(A.dist[best_t] < kInf)) set_error(T, kEInval, id);
+        for (int i = 1; i < N; ++i) {
+            const int pr = A.range[par[i]];
+            A.range[i] = A.from[i * TT + tri(L, pr / L, pr % L)] / (L * L);
+        }
+    }
+    __syncwarp();
+    // 5. Segment emission in node order (lshape_warp.cuh:414-439).
+    int* out = P.routes + P.route_off[id];
+    const long long cap = P.route_off[id + 1] - P.route_off[id];
+    int next = 1;
+    for (int b0 = 0; b0 < N; b0 += 32) {
+        const int i = b0 + lane;
+        int words = 0, x = 0, y = 0, px = 0, py = 0, cl = 0, pl = 0, minl = 0, maxl = 0;
+        if (i < N) {
+            const int node = nd[i] % XY;
+            x = node / Y; y = node - x * Y;
+            minl = A.range[i] / L; maxl = A.range[i] % L;
+            words = minl < maxl ? 2 : 0;
+            if (i) {
+                const int pn = nd[par[i]] % XY;
+                px = pn / Y; py = pn - px * Y;
+                const int pr = A.range[par[i]];
+                const int f = A.from[i * TT + tri(L, pr / L, pr % L)];
+                cl = f / L % L; pl = f % L;
+                words += (x == px || y == py) ? 2 : 6;
+            }
+        }
+        int prefix = words;
+        for (int s = 1; s < 32; s <<= 1) {
+            const int o = __shfl_up_sync(0xffffffffu, prefix, s);
+            if (lane >= s) prefix += o;
+        }
+        const int total = __shfl_sync(0xffffffffu, prefix, 31);
+        if (next + total > cap) {
+            if (lane == 0) set_error(T, kELimit, id);
+            return;
+        }
+        if (i < N) {
+            int* w = out + next + prefix - words;
+            if (minl < maxl) { *w++ = cell_index(T, minl, x, y); *w++ = cell_index(T, maxl, x, y); }
+            if (i) {
+                if (x == px || y == py) {
+                    *w++ = cell_index(T, cl, min(x, px), min(y, py));
+                    *w++ = cell_index(T, cl, max(x, px), max(y, py));
+                } else if (along_y(T, cl)) {
+                    *w++ = cell_index(T, cl, x, y);   *w++ = cell_index(T, cl, x, py);
+                    *w++ = cell_index(T, cl, x, py);  *w++ = cell_index(T, pl, x, py);
+                    *w++ = cell_index(T, pl, x, py);  *w++ = cell_index(T, pl, px, py);
+                } else {
+                    *w++ = cell_index(T, cl, x, y);   *w++ = cell_index(T, cl, px, y);
+                    *w++ = cell_index(T, cl, px, y);  *w++ = cell_index(T, pl, px, y);
+                    *w++ = cell_index(T, pl, px, y);  *w++ = cell_index(T, pl, px, py);
+                }
+            }
+        }
+        next += total;
+    }
+    if (lane == 0) out[0] = next;
+    __syncwarp();
+    if (fuse_wires) commit_net_wires(T, P, id, stamp, 1, lane, list);
+}
+
+}  // namespace grb

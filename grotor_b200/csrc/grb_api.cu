@@ -1,0 +1,1017 @@
+// grb_api.cu -- C ABI, routing context and executors (plain, CUDA graph,
+// persistent) of the B200 routing hot path.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/grb.h"
+#include "device/batching.cuh"
+#include "device/commit.cuh"
+#include "device/common.cuh"
+#include "device/cost.cuh"
+#include "device/lshape.cuh"
+
+using namespace grb;
+
+// ---------------------------------------------------------------------------
+// Kernels
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr int kRefreshThreads = 256;       // refresh_group needs 8 warps
+constexpr int kPersistentThreads = 256;
+constexpr int kDpThreads = 128;
+constexpr unsigned long long kBarrierTimeoutNs = 20ull * 1000 * 1000 * 1000;
+
+__global__ void k_cost_cells(Tables T) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= T.cells) return;
+    const unsigned wbits = T.dirty_wire[c >> 5], vbits = T.dirty_via[c >> 5];
+    const unsigned bit = 1u << (c & 31);
+    if (wbits & bit) T.wcost[c] = wire_cost_at(T, c);
+    if (vbits & bit) T.vcost[c] = via_cost_at(T, c);
+}
+
+__global__ void __launch_bounds__(kRefreshThreads) k_prefix_groups(Tables T) {
+    __shared__ double stack[32 * 16];
+    __shared__ double t3[8 * 32];
+    const int g = blockIdx.x;
+    if (!T.group_flag[g]) return;
+    refresh_group<false>(T, g, stack, t3);
+}
+
+__global__ void k_clear_dirty(Tables T, int words) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < words) { T.dirty_wire[i] = 0; T.dirty_via[i] = 0; }
+    if (i < T.n_groups) T.group_flag[i] = 0;
+    if (i < 2) { T.group_count[i] = 0; T.via_count[i] = 0; }
+}
+
+// Everything dirty: the state of a fresh database (first refresh is full).
+__global__ void k_mark_all_dirty(Tables T, int words, int list) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < words) {
+        const int rem = T.cells - i * 32;
+        const unsigned m = rem >= 32 ? 0xffffffffu : ((1u << rem) - 1u);
+        T.dirty_wire[i] = m;
+        T.dirty_via[i] = m;
+        T.via_list[list][i] = i;
+    }
+    if (i < T.n_groups) { T.group_flag[i] = 1; T.group_list[list][i] = i; }
+    if (i == 0) {
+        T.via_count[list] = words; T.group_count[list] = T.n_groups;
+        T.via_count[list ^ 1] = 0; T.group_count[list ^ 1] = 0;
+    }
+}
+
+__device__ __forceinline__ Arena warp_arena(char* smem, size_t arena_b, int warp, int L, int nmax) {
+    return carve_arena(smem + warp * arena_b, L, nmax);
+}
+
+// Plain DP launch: one warp per net of batch b (routes only).
+__global__ void __launch_bounds__(kDpThreads) k_lshape_batch(Tables T, Plan P, int b, int stamp, int nmax,
+                                                             size_t arena_b, char* gscratch, size_t gslot) {
+    extern __shared__ __align__(16) char smem[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int lo = P.batch_off[b], cnt = P.batch_off[b + 1] - lo;
+    const int k = blockIdx.x * (blockDim.x >> 5) + warp;
+    if (k >= cnt) return;
+    const int id = P.ids[lo + k];
+    const int N = P.node_off[id + 1] - P.node_off[id];
+    Arena A;
+    if (N <= nmax) A = warp_arena(smem, arena_b, warp, T.L, nmax);
+    else if (gscratch) A = carve_arena(gscratch + size_t(blockIdx.x * (blockDim.x >> 5) + warp) * gslot, T.L, N);
+    else { if (lane == 0) set_error(T, kELimit, id); return; }
+    lshape_net(T, P, id, stamp, A, lane, false, 0);
+}
+
+__global__ void k_commit_wires(Tables T, Plan P, int b, int stamp, int K, int list) {
+    const int lane = threadIdx.x & 31;
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, warps = (gridDim.x * blockDim.x) >> 5;
+    const int lo = P.batch_off[b], cnt = P.batch_off[b + 1] - lo;
+    for (int k = warp; k < cnt; k += warps) commit_net_wires(T, P, P.ids[lo + k], stamp, K, lane, list);
+}
+
+__global__ void k_commit_vias(Tables T, Plan P, int b, int stamp, int K, int list) {
+    const int lane = threadIdx.x & 31;
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, warps = (gridDim.x * blockDim.x) >> 5;
+    const int lo = P.batch_off[b], cnt = P.batch_off[b + 1] - lo;
+    for (int k = warp; k < cnt; k += warps) commit_net_vias(T, P, P.ids[lo + k], stamp, K, lane, list);
+}
+
+// Persistent stage: every batch of the plan in one cooperative launch.
+// Per batch: refresh costs from the dirty work lists -> route + commit wires ->
+// commit vias, separated by bounded grid barriers.
+__global__ void __launch_bounds__(kPersistentThreads) k_lshape_persistent(Tables T, Plan P, GridSync S,
+        int stamp0, int parity0, int nmax, size_t arena_b, char* gscratch, size_t gslot, int* work) {
+    extern __shared__ __align__(16) char smem[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int gwarp = blockIdx.x * (blockDim.x >> 5) + warp, nwarps = gridDim.x * (blockDim.x >> 5);
+    double* stack = reinterpret_cast<double*>(smem);
+    double* t3 = stack + 32 * 16;
+    for (int b = 0; b < P.n_batches; ++b) {
+        const int q = (parity0 + b) & 1, nq = q ^ 1;
+        const int stamp = stamp0 + b + 1;
+        // Phase C: incremental cost + prefix refresh.
+        if (blockIdx.x == 0 && threadIdx.x == 0) { T.group_count[nq] = 0; T.via_count[nq] = 0; }
+        const int ng = *reinterpret_cast<volatile int*>(T.group_count + q);
+        const int nv = *reinterpret_cast<volatile int*>(T.via_count + q);
+        for (int k = blockIdx.x; k < ng; k += gridDim.x) {
+            const int g = T.group_list[q][k];
+            refresh_group<true>(T, g, stack, t3);
+            if (threadIdx.x == 0) T.group_flag[g] = 0;
+        }
+        for (int k = gwarp; k < nv; k += nwarps) refresh_via_word(T, T.via_list[q][k], lane);
+        if (!grid_sync(S, T)) return;
+        // Phase A: route every net of the batch and commit its wires.
+        const int lo = P.batch_off[b], cnt = P.batch_off[b + 1] - lo;
+        const Arena A = warp_arena(smem, arena_b, warp, T.L, nmax);
+        while (true) {
+            int k = 0;
+            if (lane == 0) k = atomicAdd(work + b, 1);
+            k = __shfl_sync(0xffffffffu, k, 0);
+            if (k >= cnt) break;
+            const int id = P.ids[lo + k];
+            const int N = P.node_off[id + 1] - P.node_off[id];
+            if (N <= nmax) lshape_net(T, P, id, stamp, A, lane, true, nq);
+            else if (gscratch) lshape_net(T, P, id, stamp, carve_arena(gscratch + size_t(gwarp) * gslot, T.L, N), lane, true, nq);
+            else if (lane == 0) set_error(T, kELimit, id);
+        }
+        if (!grid_sync(S, T)) return;
+        // Phase B: via demand sees every wire timestamp of the batch.
+        for (int k = gwarp; k < cnt; k += nwarps) commit_net_vias(T, P, P.ids[lo + k], stamp, 1, lane, nq);
+        if (!grid_sync(S, T)) return;
+    }
+}
+
+// --- batching kernels -------------------------------------------------------
+__global__ void k_batch_phase1(BatchState B, int s) {
+    const int lane = threadIdx.x & 31, warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int warps = (gridDim.x * blockDim.x) >> 5, m = min(kChunk, B.n - s);
+    for (int j = warp; j < m; j += warps) batch_phase1(B, s, j, lane);
+}
+__global__ void k_batch_phase2(BatchState B, int s) {
+    const int lane = threadIdx.x & 31, warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int warps = (gridDim.x * blockDim.x) >> 5, m = min(kChunk, B.n - s);
+    for (int j = warp; j < m; j += warps) batch_phase2(B, s, j, lane);
+}
+__global__ void __launch_bounds__(kChunk) k_batch_phase3(BatchState B, int s) {
+    extern __shared__ __align__(16) unsigned bsm[];
+    if (*reinterpret_cast<volatile int*>(B.error)) return;
+    batch_phase3(B, s, bsm);
+}
+__global__ void k_batch_phase4(BatchState B, int s) {
+    const int lane = threadIdx.x & 31, warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int warps = (gridDim.x * blockDim.x) >> 5, m = min(kChunk, B.n - s);
+    if (*reinterpret_cast<volatile int*>(B.error)) return;
+    for (int j = warp; j < m; j += warps) batch_phase4(B, s, j, lane);
+}
+
+__global__ void __launch_bounds__(kChunk) k_batch_persistent(BatchState B, GridSync S, Tables T) {
+    extern __shared__ __align__(16) unsigned bsm[];
+    const int lane = threadIdx.x & 31, warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int warps = (gridDim.x * blockDim.x) >> 5;
+    for (int s = 0; s < B.n; s += kChunk) {
+        const int m = min(kChunk, B.n - s);
+        for (int j = warp; j < m; j += warps) batch_phase1(B, s, j, lane);
+        if (!grid_sync(S, T)) return;
+        for (int j = warp; j < m; j += warps) batch_phase2(B, s, j, lane);
+        if (!grid_sync(S, T)) return;
+        if (blockIdx.x == 0) batch_phase3(B, s, bsm);
+        if (!grid_sync(S, T)) return;
+        if (*reinterpret_cast<volatile int*>(B.error)) return;
+        for (int j = warp; j < m; j += warps) batch_phase4(B, s, j, lane);
+        if (!grid_sync(S, T)) return;
+    }
+}
+
+// Batch offsets in execution order (reversed colours) and the flattened ids.
+__global__ void k_plan_offsets(BatchState B, int* batch_off) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    const int nb = *B.n_colors;
+    batch_off[0] = 0;
+    for (int e = 0; e < nb; ++e) batch_off[e + 1] = batch_off[e] + B.count[nb - 1 - e];
+}
+__global__ void k_plan_scatter(BatchState B, const int* batch_off, int* ids) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= B.n) return;
+    const int nb = *B.n_colors, c = B.batch_of[j];
+    ids[batch_off[nb - 1 - c] + B.rank[j]] = B.order[j];
+}
+
+// --- rip-up classification and congestion view -----------------------------
+__global__ void k_mark_overflow(Tables T, int threshold, int* of_sum) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= T.cells) return;
+    const int l = c / T.XY, rem = c - l * T.XY, x = rem / T.Y, y = rem - x * T.Y;
+    const bool edge = along_y(T, l) ? (y + 1 < T.Y) : (x + 1 < T.X);
+    of_sum[c] = (edge && T.capacity[c] + threshold <= static_cast<float>(T.demand[c]) * 0.5f) ? 1 : 0;
+}
+// Exclusive integer prefix along each track (prefix_scan.cuh:42-72; integer
+// sums are order-free).  One thread per track.
+__global__ void k_int_prefix(Tables T, int* v) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    int l = 0, acc = 0;
+    int base = t;
+    for (; l < T.L; ++l) {
+        const int tracks = along_y(T, l) ? T.X : T.Y;
+        if (base < tracks) break;
+        base -= tracks;
+    }
+    if (l >= T.L) return;
+    const bool ay = along_y(T, l);
+    const int len = ay ? T.Y : T.X, stride = ay ? 1 : T.Y;
+    const int c0 = ay ? cell_index(T, l, base, 0) : cell_index(T, l, 0, base);
+    for (int k = 0; k < len; ++k) {
+        const int c = c0 + k * stride, x = v[c];
+        v[c] = acc;
+        acc += x;
+    }
+}
+__global__ void k_overflow_nets(Tables T, Plan P, int n, const int* of_sum, unsigned char* is_of) {
+    const int id = blockIdx.x * blockDim.x + threadIdx.x;
+    if (id >= n) return;
+    const int* r = P.routes + P.route_off[id];
+    int count = 0;
+    unsigned char flag = 0;
+    if (P.route_off[id + 1] > P.route_off[id]) {
+        for (int i = 1; i < r[0]; i += 2) {
+            const int a = r[i], b = r[i + 1], l = a / T.XY, ra = a % T.XY, rb = b % T.XY;
+            const int x0 = ra / T.Y, y0 = ra % T.Y, x1 = rb / T.Y, y1 = rb % T.Y;
+            if (x0 != x1) count += of_sum[cell_index(T, l, max(x0, x1), y0)] - of_sum[cell_index(T, l, min(x0, x1), y0)];
+            if (y0 != y1) count += of_sum[cell_index(T, l, x0, max(y0, y1))] - of_sum[cell_index(T, l, x0, min(y0, y1))];
+            if (count > 10) { flag = 1; break; }
+        }
+    }
+    is_of[id] = flag;
+}
+__global__ void k_congestion(Tables T, unsigned char* cong, float* xsum, float* ysum) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= T.XY) return;
+    double worst = 0.0;
+    for (int l = 0; l < T.L; ++l) {
+        const int e = l * T.XY + i;
+        worst = fmax(worst, static_cast<double>(static_cast<float>(T.demand[e]) * 0.5f - T.capacity[e]));
+    }
+    cong[i] = worst > 0.0;
+    xsum[i] = static_cast<float>(worst);
+    ysum[i] = static_cast<float>(worst);
+}
+// Float prefix of one line in the reference's log-step association
+// (congestion.cuh:81-112), one thread per line.
+__global__ void k_float_line_prefix(float* v, int lines, int len, int line_stride, int elem_stride) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= lines) return;
+    float* a = v + size_t(t) * line_stride;
+    float tot[32];
+    float prev = 0.f;
+    for (int i = 0; i < len; ++i) {
+        const float cur = a[size_t(i) * elem_stride];
+        float acc = i ? prev : 0.f;
+        prev = cur;
+        float fresh[32];
+        fresh[0] = acc;
+        int d = 0;
+        while ((i >> d) & 1) { acc = acc + tot[d]; ++d; fresh[d] = acc; }
+        for (int j = 0; j <= d; ++j) tot[j] = fresh[j];
+        for (int e = d + 1; (i >> e) != 0; ++e)
+            if ((i >> e) & 1) acc = acc + tot[e];
+        a[size_t(i) * elem_stride] = acc;
+    }
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Host context
+// ---------------------------------------------------------------------------
+struct grb_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    int sms = 0;
+    std::string error;
+    Tables T{};
+    std::vector<void*> owned;
+    int words = 0;          // bitmap words
+    int parity = 0;         // list holding pending dirty items
+    int stamp = 0;
+    int64_t launches = 0;
+    // net store
+    int n_nets = 0;
+    int max_nodes = 0;
+    long long route_words = 0;
+    int *node_off = nullptr, *nodes = nullptr, *parents = nullptr;
+    long long* route_off = nullptr;
+    int* routes = nullptr;
+    int *point_off = nullptr, *points = nullptr, *hseg_off = nullptr, *hsegs = nullptr, *vseg_off = nullptr, *vsegs = nullptr;
+    std::vector<void*> net_bufs;
+    long long net_cap[6] = {0, 0, 0, 0, 0, 0};  // nets, nodes, route words, points, hsegs, vsegs
+    // plan
+    int *ids = nullptr, *batch_off = nullptr;
+    int plan_n = 0, n_batches = 0, plan_cap = 0;
+    std::vector<int> h_batch_off;
+    int plan_version = 0;
+    // scratch
+    char* gscratch = nullptr;
+    size_t gscratch_bytes = 0;
+    int* work = nullptr;
+    int work_cap = 0;
+    unsigned* sync = nullptr;   // [count, generation]
+    // batching buffers
+    unsigned *cellmask = nullptr, *localmask = nullptr, *fmask = nullptr, *pred = nullptr, *fullmask = nullptr;
+    int *bcount = nullptr, *ncolors = nullptr, *batch_of = nullptr, *brank = nullptr, *order = nullptr;
+    int bW = 0, bn_cap = 0;
+    // graph cache
+    cudaGraphExec_t graph = nullptr;
+    int graph_version = -1, graph_stamp = -1;
+    int64_t graph_kernels = 0;
+    // timing
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    double batching_ms = 0, dag_ms = 0;
+};
+
+namespace {
+
+int fail(grb_ctx* c, int code, const std::string& msg) {
+    if (c) c->error = msg;
+    return code;
+}
+
+int cuda_fail(grb_ctx* c, cudaError_t e, const char* what) {
+    return fail(c, GRB_ECUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define GRB_CUDA(ctx, expr)                                             \
+    do {                                                                \
+        cudaError_t e_ = (expr);                                        \
+        if (e_ != cudaSuccess) return cuda_fail((ctx), e_, #expr);      \
+    } while (0)
+
+template <class T>
+int dalloc(grb_ctx* c, T** p, size_t count, std::vector<void*>& owner) {
+    void* q = nullptr;
+    const cudaError_t e = cudaMalloc(&q, std::max<size_t>(count, 1) * sizeof(T));
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return fail(c, GRB_ENOMEM, "cudaMalloc of " + std::to_string(count * sizeof(T)) + " bytes failed");
+    }
+    owner.push_back(q);
+    *p = static_cast<T*>(q);
+    return GRB_OK;
+}
+
+void free_all(std::vector<void*>& v) {
+    for (void* p : v) cudaFree(p);
+    v.clear();
+}
+
+int check_device_error(grb_ctx* c) {
+    int err[2] = {0, 0};
+    GRB_CUDA(c, cudaMemcpyAsync(err, c->T.error, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    GRB_CUDA(c, cudaMemcpyAsync(err + 1, c->T.error_info, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    GRB_CUDA(c, cudaStreamSynchronize(c->stream));
+    if (err[0]) {
+        GRB_CUDA(c, cudaMemsetAsync(c->T.error, 0, sizeof(int), c->stream));
+        switch (err[0]) {
+            case kELimit: return fail(c, GRB_ELIMIT, "route storage or colour capacity exceeded (item " + std::to_string(err[1]) + ")");
+            case kETimedOut: return fail(c, GRB_ETIMEDOUT, "bounded device wait expired (block " + std::to_string(err[1]) + ")");
+            default: return fail(c, GRB_EINVAL, "device reported an invalid state (item " + std::to_string(err[1]) + ")");
+        }
+    }
+    return GRB_OK;
+}
+
+Plan make_plan(const grb_ctx* c) {
+    Plan P{};
+    P.node_off = c->node_off; P.nodes = c->nodes; P.parents = c->parents;
+    P.route_off = c->route_off; P.routes = c->routes;
+    P.ids = c->ids; P.batch_off = c->batch_off; P.n_batches = c->n_batches;
+    return P;
+}
+
+int dp_nmax(const grb_ctx* c) { return std::min(c->max_nodes, 16); }
+
+// Global scratch for nets with more nodes than fit a shared-memory arena.
+int ensure_gscratch(grb_ctx* c, int slots) {
+    if (c->max_nodes <= dp_nmax(c)) return GRB_OK;
+    const size_t need = size_t(slots) * arena_bytes(c->T.L, c->max_nodes);
+    if (need <= c->gscratch_bytes) return GRB_OK;
+    if (c->gscratch) cudaFree(c->gscratch);
+    c->gscratch = nullptr;
+    c->gscratch_bytes = 0;
+    if (cudaMalloc(&c->gscratch, need) != cudaSuccess) { cudaGetLastError(); return fail(c, GRB_ENOMEM, "DP scratch allocation failed"); }
+    c->gscratch_bytes = need;
+    return GRB_OK;
+}
+
+int refresh_plain(grb_ctx* c) {
+    Tables& T = c->T;
+    k_cost_cells<<<(T.cells + 255) / 256, 256, 0, c->stream>>>(T);
+    k_prefix_groups<<<T.n_groups, kRefreshThreads, 0, c->stream>>>(T);
+    const int n = std::max(c->words, std::max(T.n_groups, 2));
+    k_clear_dirty<<<(n + 255) / 256, 256, 0, c->stream>>>(T, c->words);
+    c->launches += 3;
+    GRB_CUDA(c, cudaGetLastError());
+    return GRB_OK;
+}
+
+int route_plain(grb_ctx* c, int b, int stamp) {
+    const int cnt = c->h_batch_off[b + 1] - c->h_batch_off[b];
+    if (cnt <= 0) return GRB_OK;
+    const int nmax = dp_nmax(c);
+    const size_t ab = arena_bytes(c->T.L, nmax);
+    const int wpb = kDpThreads / 32;
+    const int blocks = (cnt + wpb - 1) / wpb;
+    const int rc = ensure_gscratch(c, blocks * wpb);
+    if (rc) return rc;
+    const size_t arena_slot = arena_bytes(c->T.L, std::max(c->max_nodes, 1));
+    k_lshape_batch<<<blocks, kDpThreads, ab * wpb, c->stream>>>(c->T, make_plan(c), b, stamp, nmax, ab,
+                                                                 c->gscratch, arena_slot);
+    c->launches += 1;
+    GRB_CUDA(c, cudaGetLastError());
+    return GRB_OK;
+}
+
+int commit_plain(grb_ctx* c, int b, int stamp, int K) {
+    const int cnt = c->h_batch_off[b + 1] - c->h_batch_off[b];
+    if (cnt <= 0) return GRB_OK;
+    const int blocks = std::min((cnt + 3) / 4, 1056);  // demand.cuh:490
+    k_commit_wires<<<blocks, 128, 0, c->stream>>>(c->T, make_plan(c), b, stamp, K, c->parity);
+    k_commit_vias<<<blocks, 128, 0, c->stream>>>(c->T, make_plan(c), b, stamp, K, c->parity);
+    c->launches += 2;
+    GRB_CUDA(c, cudaGetLastError());
+    return GRB_OK;
+}
+
+int stage_plain(grb_ctx* c, int stamp0) {
+    for (int b = 0; b < c->n_batches; ++b) {
+        const int stamp = stamp0 + b + 1;
+        int rc = refresh_plain(c);
+        if (!rc) rc = route_plain(c, b, stamp);
+        if (!rc) rc = commit_plain(c, b, stamp, 1);
+        if (rc) return rc;
+    }
+    return GRB_OK;
+}
+
+int stage_graph(grb_ctx* c, int stamp0) {
+    if (!c->graph || c->graph_version != c->plan_version || c->graph_stamp != stamp0) {
+        if (c->graph) { cudaGraphExecDestroy(c->graph); c->graph = nullptr; }
+        // Scratch must exist before capture (no allocation while capturing).
+        const int wpb = kDpThreads / 32;
+        int maxcnt = 0;
+        for (int b = 0; b < c->n_batches; ++b) maxcnt = std::max(maxcnt, c->h_batch_off[b + 1] - c->h_batch_off[b]);
+        int rc = ensure_gscratch(c, ((maxcnt + wpb - 1) / wpb) * wpb);
+        if (rc) return rc;
+        const int64_t before = c->launches;
+        cudaGraph_t g = nullptr;
+        GRB_CUDA(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+        rc = stage_plain(c, stamp0);
+        const cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+        if (rc) { if (g) cudaGraphDestroy(g); return rc; }
+        if (e != cudaSuccess) return cuda_fail(c, e, "cudaStreamEndCapture");
+        const cudaError_t ei = cudaGraphInstantiate(&c->graph, g, 0);
+        cudaGraphDestroy(g);
+        if (ei != cudaSuccess) return cuda_fail(c, ei, "cudaGraphInstantiate");
+        c->graph_kernels = c->launches - before;
+        c->launches = before;
+        c->graph_version = c->plan_version;
+        c->graph_stamp = stamp0;
+    }
+    GRB_CUDA(c, cudaGraphLaunch(c->graph, c->stream));
+    c->launches += c->graph_kernels;
+    return GRB_OK;
+}
+
+int stage_persistent(grb_ctx* c, int stamp0) {
+    if (c->n_batches == 0) return GRB_OK;
+    const int nmax = dp_nmax(c);
+    const size_t ab = arena_bytes(c->T.L, nmax);
+    const int wpb = kPersistentThreads / 32;
+    const size_t prefix_smem = (32 * 16 + 8 * 32) * sizeof(double);
+    const size_t smem = std::max(ab * wpb, prefix_smem);
+    GRB_CUDA(c, cudaFuncSetAttribute(k_lshape_persistent, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+    int per_sm = 0;
+    GRB_CUDA(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_lshape_persistent, kPersistentThreads, smem));
+    if (per_sm < 1) return fail(c, GRB_EINVAL, "persistent kernel does not fit on an SM");
+    const int blocks = per_sm * c->sms;
+    const size_t slot = arena_bytes(c->T.L, std::max(c->max_nodes, 1));
+    int rc = ensure_gscratch(c, blocks * wpb);
+    if (rc) return rc;
+    if (c->work_cap < c->n_batches) {
+        if (c->work) cudaFree(c->work);
+        c->work = nullptr;
+        if (cudaMalloc(&c->work, sizeof(int) * c->n_batches) != cudaSuccess) { cudaGetLastError(); return fail(c, GRB_ENOMEM, "work counters"); }
+        c->work_cap = c->n_batches;
+    }
+    GRB_CUDA(c, cudaMemsetAsync(c->work, 0, sizeof(int) * c->n_batches, c->stream));
+    GRB_CUDA(c, cudaMemsetAsync(c->sync, 0, 2 * sizeof(unsigned), c->stream));
+    Tables T = c->T;
+    Plan P = make_plan(c);
+    GridSync S{c->sync, c->sync + 1, kBarrierTimeoutNs};
+    int parity = c->parity;
+    char* gs = c->gscratch;
+    void* args[] = {&T, &P, &S, &stamp0, &parity, (void*)&nmax, (void*)&ab, &gs, (void*)&slot, &c->work};
+    GRB_CUDA(c, cudaLaunchCooperativeKernel((void*)k_lshape_persistent, dim3(blocks), dim3(kPersistentThreads), args, smem, c->stream));
+    c->launches += 1;
+    c->parity = (c->parity + c->n_batches) & 1;
+    return GRB_OK;
+}
+
+int ensure_plan_capacity(grb_ctx* c, int n, int nb) {
+    if (c->ids && n <= c->plan_cap && nb + 1 <= c->plan_cap + 1) {
+        return GRB_OK;
+    }
+    if (c->ids) cudaFree(c->ids);
+    if (c->batch_off) cudaFree(c->batch_off);
+    c->ids = nullptr; c->batch_off = nullptr;
+    const int cap = std::max(n, 1);
+    if (cudaMalloc(&c->ids, sizeof(int) * cap) != cudaSuccess ||
+        cudaMalloc(&c->batch_off, sizeof(int) * (size_t(cap) + 1)) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(c, GRB_ENOMEM, "plan allocation failed");
+    }
+    c->plan_cap = cap;
+    return GRB_OK;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+extern "C" {
+
+int grb_create(const grb_grid* g, int32_t device, grb_ctx** out) {
+    if (!out) return GRB_EINVAL;
+    *out = nullptr;
+    if (!g || g->L < 1 || g->L > kMaxLayers || g->X < 2 || g->Y < 2 || !g->capacity ||
+        !g->unit_length_short_costs || !g->x_edge_len || !g->y_edge_len)
+        return GRB_EINVAL;
+    if (size_t(g->L) * g->X * g->Y >= (size_t(1) << 31)) return GRB_EINVAL;
+    auto c = std::make_unique<grb_ctx>();
+    c->device = device;
+    GRB_CUDA(c.get(), cudaSetDevice(device));
+    GRB_CUDA(c.get(), cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    GRB_CUDA(c.get(), cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, device));
+    GRB_CUDA(c.get(), cudaEventCreate(&c->ev0));
+    GRB_CUDA(c.get(), cudaEventCreate(&c->ev1));
+    Tables& T = c->T;
+    T.L = g->L; T.X = g->X; T.Y = g->Y; T.DIR = g->DIR & 1; T.XY = g->X * g->Y;
+    T.cells = T.L * T.XY;
+    T.unit_wire = g->unit_length_wire_cost; T.unit_via = g->unit_via_cost;
+    T.of_scale = g->of_cost_scale;
+    const size_t cells = T.cells;
+    c->words = int((cells + 31) / 32);
+    int ng = 0;
+    for (int l = 0; l < T.L; ++l) {
+        T.group_base[l] = ng;
+        const int tracks = (((l & 1) ^ T.DIR) ? T.X : T.Y);
+        ng += (tracks + kTrackGroup - 1) / kTrackGroup;
+    }
+    T.group_base[T.L] = ng;
+    for (int l = T.L + 1; l <= kMaxLayers; ++l) T.group_base[l] = ng;
+    T.n_groups = ng;
+    grb_ctx* cp = c.get();
+    double* sc; int* xl; int* yl; float* cap;
+    int rc = 0;
+    rc |= dalloc(cp, &sc, T.L, cp->owned);
+    rc |= dalloc(cp, &xl, T.X - 1, cp->owned);
+    rc |= dalloc(cp, &yl, T.Y - 1, cp->owned);
+    rc |= dalloc(cp, &cap, cells, cp->owned);
+    rc |= dalloc(cp, &T.demand, cells, cp->owned);
+    rc |= dalloc(cp, &T.ts, cells, cp->owned);
+    rc |= dalloc(cp, &T.wcost, cells, cp->owned);
+    rc |= dalloc(cp, &T.vcost, cells, cp->owned);
+    rc |= dalloc(cp, &T.presum, cells, cp->owned);
+    rc |= dalloc(cp, &T.dirty_wire, c->words, cp->owned);
+    rc |= dalloc(cp, &T.dirty_via, c->words, cp->owned);
+    rc |= dalloc(cp, &T.group_flag, ng, cp->owned);
+    rc |= dalloc(cp, &T.group_list[0], ng, cp->owned);
+    rc |= dalloc(cp, &T.group_list[1], ng, cp->owned);
+    rc |= dalloc(cp, &T.group_count, 2, cp->owned);
+    rc |= dalloc(cp, &T.via_list[0], c->words, cp->owned);
+    rc |= dalloc(cp, &T.via_list[1], c->words, cp->owned);
+    rc |= dalloc(cp, &T.via_count, 2, cp->owned);
+    rc |= dalloc(cp, &T.wirelength, 1, cp->owned);
+    rc |= dalloc(cp, &T.vias, 1, cp->owned);
+    rc |= dalloc(cp, &T.error, 2, cp->owned);
+    rc |= dalloc(cp, &c->sync, 2, cp->owned);
+    if (rc) { free_all(cp->owned); return GRB_ENOMEM; }
+    T.error_info = T.error + 1;
+    T.short_costs = sc; T.xlen = xl; T.ylen = yl; T.capacity = cap;
+    GRB_CUDA(cp, cudaMemcpy(sc, g->unit_length_short_costs, sizeof(double) * T.L, cudaMemcpyHostToDevice));
+    GRB_CUDA(cp, cudaMemcpy(xl, g->x_edge_len, sizeof(int) * (T.X - 1), cudaMemcpyHostToDevice));
+    GRB_CUDA(cp, cudaMemcpy(yl, g->y_edge_len, sizeof(int) * (T.Y - 1), cudaMemcpyHostToDevice));
+    GRB_CUDA(cp, cudaMemcpy(cap, g->capacity, sizeof(float) * cells, cudaMemcpyHostToDevice));
+    GRB_CUDA(cp, cudaMemset(T.error, 0, 2 * sizeof(int)));
+    GRB_CUDA(cp, cudaFuncSetAttribute(k_batch_phase3, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    GRB_CUDA(cp, cudaFuncSetAttribute(k_batch_persistent, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    GRB_CUDA(cp, cudaFuncSetAttribute(k_lshape_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    const int r = grb_reset(cp);
+    if (r) { const int code = r; free_all(cp->owned); return code; }
+    *out = c.release();
+    return GRB_OK;
+}
+
+void grb_destroy(grb_ctx* c) {
+    if (!c) return;
+    cudaSetDevice(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    if (c->graph) cudaGraphExecDestroy(c->graph);
+    free_all(c->net_bufs);
+    free_all(c->owned);
+    for (void* p : {(void*)c->ids, (void*)c->batch_off, (void*)c->gscratch, (void*)c->work, (void*)c->cellmask,
+                    (void*)c->localmask, (void*)c->fmask, (void*)c->pred, (void*)c->fullmask, (void*)c->bcount,
+                    (void*)c->ncolors, (void*)c->batch_of, (void*)c->brank, (void*)c->order})
+        if (p) cudaFree(p);
+    if (c->ev0) cudaEventDestroy(c->ev0);
+    if (c->ev1) cudaEventDestroy(c->ev1);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+}
+
+const char* grb_last_error(const grb_ctx* c) { return c ? c->error.c_str() : "null context"; }
+
+void* grb_stream(grb_ctx* c) { return c ? static_cast<void*>(c->stream) : nullptr; }
+
+int grb_reset(grb_ctx* c) {
+    if (!c) return GRB_EINVAL;
+    GRB_CUDA(c, cudaSetDevice(c->device));
+    Tables& T = c->T;
+    const size_t cells = T.cells;
+    GRB_CUDA(c, cudaMemsetAsync(T.demand, 0, sizeof(int) * cells, c->stream));
+    GRB_CUDA(c, cudaMemsetAsync(T.ts, 0, sizeof(int) * cells, c->stream));
+    GRB_CUDA(c, cudaMemsetAsync(T.wirelength, 0, sizeof(double), c->stream));
+    GRB_CUDA(c, cudaMemsetAsync(T.vias, 0, sizeof(unsigned long long), c->stream));
+    if (c->routes) GRB_CUDA(c, cudaMemsetAsync(c->routes, 0, sizeof(int) * std::max<long long>(c->route_words, 1), c->stream));
+    c->parity = 0;
+    const int n = std::max(c->words, T.n_groups);
+    k_mark_all_dirty<<<(n + 255) / 256, 256, 0, c->stream>>>(T, c->words, c->parity);
+    c->launches += 1;
+    GRB_CUDA(c, cudaGetLastError());
+    c->stamp = 0;
+    return GRB_OK;
+}
+
+int grb_upload_nets(grb_ctx* c, const grb_nets* nets) {
+    if (!c || !nets || nets->n < 0 || !nets->node_off || !nets->route_off) return c ? fail(c, GRB_EINVAL, "bad nets") : GRB_EINVAL;
+    GRB_CUDA(c, cudaSetDevice(c->device));
+    const int n = nets->n;
+    const int nn = nets->node_off[n];
+    long long maxn = 0;
+    for (int i = 0; i < n; ++i) maxn = std::max<long long>(maxn, nets->node_off[i + 1] - nets->node_off[i]);
+    const long long rw = nets->route_off[n];
+    const int np = nets->point_off ? nets->point_off[n] : 0;
+    const int nh = nets->hseg_off ? nets->hseg_off[n] : 0;
+    const int nv = nets->vseg_off ? nets->vseg_off[n] : 0;
+    // Validate on the host: every index a kernel will dereference is in range.
+    {
+        const int XY = c->T.XY, L = c->T.L;
+        for (int i = 0; i < n; ++i) {
+            const int a = nets->node_off[i], b = nets->node_off[i + 1];
+            if (b < a || nets->route_off[i + 1] < nets->route_off[i]) return fail(c, GRB_EINVAL, "offsets must be non-decreasing");
+            for (int k = a; k < b; ++k) {
+                const int v = nets->nodes[k], p = nets->parents[k];
+                if (v < 0 || v / XY > L) return fail(c, GRB_EINVAL, "tree node outside the grid");
+                if (k == a ? p != -1 : (p < 0 || p >= k - a)) return fail(c, GRB_EINVAL, "parents must precede children");
+            }
+        }
+        auto check_csr = [&](const int* off, const int* data, int width) {
+            if (!off) return true;
+            for (int i = 0; i < n; ++i) if (off[i + 1] < off[i]) return false;
+            for (long long k = 0; k < (long long)off[n] * width; ++k) if (data[k] < 0 || data[k] >= XY) return false;
+            return true;
+        };
+        if (!check_csr(nets->point_off, nets->points, 1) || !check_csr(nets->hseg_off, nets->hsegs, 2) ||
+            !check_csr(nets->vseg_off, nets->vsegs, 2))
+            return fail(c, GRB_EINVAL, "batching geometry outside the grid");
+    }
+    // Reuse the device buffers when every array still fits.
+    const long long need[6] = {n, nn, rw, np, nh, nv};
+    bool fits = !c->net_bufs.empty();
+    for (int k = 0; k < 6 && fits; ++k) fits = need[k] <= c->net_cap[k];
+    if (!fits) {
+        GRB_CUDA(c, cudaStreamSynchronize(c->stream));
+        free_all(c->net_bufs);
+        int rc = 0;
+        rc |= dalloc(c, &c->node_off, n + 1, c->net_bufs);
+        rc |= dalloc(c, &c->nodes, nn, c->net_bufs);
+        rc |= dalloc(c, &c->parents, nn, c->net_bufs);
+        rc |= dalloc(c, &c->route_off, n + 1, c->net_bufs);
+        rc |= dalloc(c, &c->routes, rw, c->net_bufs);
+        rc |= dalloc(c, &c->point_off, n + 1, c->net_bufs);
+        rc |= dalloc(c, &c->points, np, c->net_bufs);
+        rc |= dalloc(c, &c->hseg_off, n + 1, c->net_bufs);
+        rc |= dalloc(c, &c->hsegs, 2 * size_t(nh), c->net_bufs);
+        rc |= dalloc(c, &c->vseg_off, n + 1, c->net_bufs);
+        rc |= dalloc(c, &c->vsegs, 2 * size_t(nv), c->net_bufs);
+        if (rc) { free_all(c->net_bufs); return GRB_ENOMEM; }
+        for (int k = 0; k < 6; ++k) c->net_cap[k] = need[k];
+    }
+    auto h2d = [&](void* dst, const void* src, size_t bytes) {
+        return src && bytes ? cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, c->stream) : cudaSuccess;
+    };
+    GRB_CUDA(c, h2d(c->node_off, nets->node_off, sizeof(int) * (n + 1)));
+    GRB_CUDA(c, h2d(c->nodes, nets->nodes, sizeof(int) * nn));
+    GRB_CUDA(c, h2d(c->parents, nets->parents, sizeof(int) * nn));
+    GRB_CUDA(c, h2d(c->route_off, nets->route_off, sizeof(long long) * (n + 1)));
+    GRB_CUDA(c, cudaMemsetAsync(c->routes, 0, sizeof(int) * std::max<long long>(rw, 1), c->stream));
+    if (nets->point_off) GRB_CUDA(c, h2d(c->point_off, nets->point_off, sizeof(int) * (n + 1)));
+    else GRB_CUDA(c, cudaMemsetAsync(c->point_off, 0, sizeof(int) * (n + 1), c->stream));
+    GRB_CUDA(c, h2d(c->points, nets->points, sizeof(int) * np));
+    if (nets->hseg_off) GRB_CUDA(c, h2d(c->hseg_off, nets->hseg_off, sizeof(int) * (n + 1)));
+    else GRB_CUDA(c, cudaMemsetAsync(c->hseg_off, 0, sizeof(int) * (n + 1), c->stream));
+    GRB_CUDA(c, h2d(c->hsegs, nets->hsegs, sizeof(int) * 2 * nh));
+    if (nets->vseg_off) GRB_CUDA(c, h2d(c->vseg_off, nets->vseg_off, sizeof(int) * (n + 1)));
+    else GRB_CUDA(c, cudaMemsetAsync(c->vseg_off, 0, sizeof(int) * (n + 1), c->stream));
+    GRB_CUDA(c, h2d(c->vsegs, nets->vsegs, sizeof(int) * 2 * nv));
+    // Host buffers may be pageable and short-lived: the copies complete before return.
+    GRB_CUDA(c, cudaStreamSynchronize(c->stream));
+    c->n_nets = n;
+    c->max_nodes = int(maxn);
+    c->route_words = rw;
+    return GRB_OK;
+}
+
+int grb_set_plan(grb_ctx* c, const int32_t* ids, int32_t n, const int32_t* batch_off, int32_t nb) {
+    if (!c || n < 0 || nb < 0 || (n && !ids) || !batch_off) return c ? fail(c, GRB_EINVAL, "bad plan") : GRB_EINVAL;
+    if (batch_off[0] != 0 || batch_off[nb] != n) return fail(c, GRB_EINVAL, "batch offsets must span the ids");
+    for (int i = 0; i < n; ++i)
+        if (ids[i] < 0 || ids[i] >= c->n_nets) return fail(c, GRB_EINVAL, "net id out of range");
+    int rc = ensure_plan_capacity(c, n, nb);
+    if (rc) return rc;
+    if (nb + 1 > c->plan_cap + 1) return fail(c, GRB_EINVAL, "more batches than nets");
+    GRB_CUDA(c, cudaMemcpyAsync(c->ids, ids, sizeof(int) * n, cudaMemcpyHostToDevice, c->stream));
+    GRB_CUDA(c, cudaMemcpyAsync(c->batch_off, batch_off, sizeof(int) * (nb + 1), cudaMemcpyHostToDevice, c->stream));
+    c->h_batch_off.assign(batch_off, batch_off + nb + 1);
+    c->plan_n = n;
+    c->n_batches = nb;
+    ++c->plan_version;
+    GRB_CUDA(c, cudaStreamSynchronize(c->stream));
+    return GRB_OK;
+}
+
+int grb_get_plan(grb_ctx* c, int32_t* ids, int32_t* batch_off, int32_t* n, int32_t* nb) {
+    if (!c) return GRB_EINVAL;
+    if (n) *n = c->plan_n;
+    if (nb) *nb = c->n_batches;
+    if (ids && c->plan_n) GRB_CUDA(c, cudaMemcpyAsync(ids, c->ids, sizeof(int) * c->plan_n, cudaMemcpyDeviceToHost, c->stream));
+    if (batch_off) std::copy(c->h_batch_off.begin(), c->h_batch_off.end(), batch_off);
+    GRB_CUDA(c, cudaStreamSynchronize(c->stream));
+    return GRB_OK;
+}
+
+int grb_plan_batches(grb_ctx* c, const int32_t* order, int32_t n, int32_t limit, int32_t sparsity, int32_t mode,
+                     int32_t* batch_of, int32_t* n_batches) {
+    if (!c || n < 0 || limit < 1 || sparsity < 1 || (n && !order)) return c ? fail(c, GRB_EINVAL, "bad batching arguments") : GRB_EINVAL;
+    GRB_CUDA(c, cudaSetDevice(c->device));
+    for (int i = 0; i < n; ++i)
+        if (order[i] < 0 || order[i] >= c->n_nets) return fail(c, GRB_EINVAL, "net id out of range");
+    const size_t xy = size_t(c->T.XY);
+    int W = std::max(c->bW, 8);
+    int rc = ensure_plan_capacity(c, n, n);
+    if (rc) return rc;
+    if (c->bn_cap < n || !c->order) {
+        for (int** p : {&c->batch_of, &c->brank, &c->order}) { if (*p) cudaFree(*p); *p = nullptr; }
+        const size_t m = std::max(n, 1);
+        if (cudaMalloc(&c->batch_of, 4 * m) || cudaMalloc(&c->brank, 4 * m) || cudaMalloc(&c->order, 4 * m)) {
+            cudaGetLastError();
+            return fail(c, GRB_ENOMEM, "batching buffers");
+        }
+        c->bn_cap = n;
+    }
+    if (!c->localmask) {
+        if (cudaMalloc(&c->localmask, xy * kChunkWords * 4) || cudaMalloc(&c->pred, size_t(kChunk) * kChunkWords * 4) ||
+            cudaMalloc(&c->ncolors, 4)) {
+            cudaGetLastError();
+            return fail(c, GRB_ENOMEM, "batching buffers");
+        }
+        GRB_CUDA(c, cudaMemsetAsync(c->localmask, 0, xy * kChunkWords * 4, c->stream));
+    }
+    GRB_CUDA(c, cudaMemcpyAsync(c->order, order, sizeof(int) * n, cudaMemcpyHostToDevice, c->stream));
+    GRB_CUDA(c, cudaEventRecord(c->ev0, c->stream));
+    for (int attempt = 0; attempt < 6; ++attempt) {
+        if (W != c->bW || !c->cellmask) {
+            for (unsigned** p : {&c->cellmask, &c->fmask, &c->fullmask}) { if (*p) cudaFree(*p); *p = nullptr; }
+            if (c->bcount) cudaFree(c->bcount);
+            c->bcount = nullptr;
+            if (cudaMalloc(&c->cellmask, xy * W * 4) || cudaMalloc(&c->fmask, size_t(kChunk) * W * 4) ||
+                cudaMalloc(&c->fullmask, W * 4) || cudaMalloc(&c->bcount, size_t(32) * W * 4)) {
+                cudaGetLastError();
+                return fail(c, GRB_ENOMEM, "colour masks");
+            }
+            c->bW = W;
+        }
+        GRB_CUDA(c, cudaMemsetAsync(c->cellmask, 0, xy * W * 4, c->stream));
+        GRB_CUDA(c, cudaMemsetAsync(c->fullmask, 0, W * 4, c->stream));
+        GRB_CUDA(c, cudaMemsetAsync(c->bcount, 0, size_t(32) * W * 4, c->stream));
+        GRB_CUDA(c, cudaMemsetAsync(c->ncolors, 0, 4, c->stream));
+        BatchState B{};
+        B.X = c->T.X; B.Y = c->T.Y; B.n = n; B.limit = limit; B.sparsity = sparsity; B.W = W;
+        B.order = c->order;
+        B.point_off = c->point_off; B.points = c->points;
+        B.hseg_off = c->hseg_off; B.hsegs = c->hsegs; B.vseg_off = c->vseg_off; B.vsegs = c->vsegs;
+        B.cellmask = c->cellmask; B.localmask = c->localmask; B.fmask = c->fmask; B.pred = c->pred;
+        B.fullmask = c->fullmask; B.count = c->bcount; B.n_colors = c->ncolors;
+        B.batch_of = c->batch_of; B.rank = c->brank;
+        B.error = c->T.error; B.error_info = c->T.error_info;
+        const size_t smem = phase3_smem_bytes(W);
+        if (smem > 200 * 1024) return fail(c, GRB_ELIMIT, "too many batch colours");
+        if (mode == GRB_MODE_PERSISTENT) {
+            int per_sm = 0;
+            GRB_CUDA(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_persistent, kChunk, smem));
+            if (per_sm < 1) return fail(c, GRB_EINVAL, "batching kernel does not fit on an SM");
+            GRB_CUDA(c, cudaMemsetAsync(c->sync, 0, 2 * sizeof(unsigned), c->stream));
+            GridSync S{c->sync, c->sync + 1, kBarrierTimeoutNs};
+            Tables T = c->T;
+            void* args[] = {&B, &S, &T};
+            GRB_CUDA(c, cudaLaunchCooperativeKernel((void*)k_batch_persistent, dim3(per_sm * c->sms), dim3(kChunk), args, smem, c->stream));
+            c->launches += 1;
+        } else {
+            const int grid = c->sms * 4;
+            for (int s = 0; s < n; s += kChunk) {
+                k_batch_phase1<<<grid, 256, 0, c->stream>>>(B, s);
+                k_batch_phase2<<<grid, 256, 0, c->stream>>>(B, s);
+                k_batch_phase3<<<1, kChunk, smem, c->stream>>>(B, s);
+                k_batch_phase4<<<grid, 256, 0, c->stream>>>(B, s);
+                c->launches += 4;
+            }
+            GRB_CUDA(c, cudaGetLastError());
+        }
+        int err[2] = {0, 0};
+        GRB_CUDA(c, cudaMemcpyAsync(err, c->T.error, 2 * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+        GRB_CUDA(c, cudaStreamSynchronize(c->stream));
+        if (err[0] == kELimit) {
+            // Not enough colour words: clear the chunk-local masks and retry wider.
+            GRB_CUDA(c, cudaMemsetAsync(c->T.error, 0, 2 * sizeof(int), c->stream));
+            GRB_CUDA(c, cudaMemsetAsync(c->localmask, 0, xy * kChunkWords * 4, c->stream));
+            W *= 2;
+            continue;
+        }
+        if (err[0]) return check_device_error(c);
+        int nb = 0;
+        GRB_CUDA(c, cudaMemcpy(&nb, c->ncolors, 4, cudaMemcpyDeviceToHost));
+        k_plan_offsets<<<1, 1, 0, c->stream>>>(B, c->batch_off);
+        k_plan_scatter<<<(n + 255) / 256, 256, 0, c->stream>>>(B, c->batch_off, c->ids);
+        c->launches += 2;
+        GRB_CUDA(c, cudaGetLastError());
+        GRB_CUDA(c, cudaEventRecord(c->ev1, c->stream));
+        c->h_batch_off.assign(nb + 1, 0);
+        GRB_CUDA(c, cudaMemcpyAsync(c->h_batch_off.data(), c->batch_off, sizeof(int) * (nb + 1), cudaMemcpyDeviceToHost, c->stream));
+        if (batch_of) GRB_CUDA(c, cudaMemcpyAsync(batch_of, c->batch_of, sizeof(int) * n, cudaMemcpyDeviceToHost, c->stream));
+        GRB_CUDA(c, cudaStreamSynchronize(c->stream));
+        float ms = 0;
+        GRB_CUDA(c, cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+        c->batching_ms = ms;
+        c->plan_n = n;
+        c->n_batches = nb;
+        ++c->plan_version;
+        if (n_batches) *n_batches = nb;
+        return GRB_OK;
+    }
+    return fail(c, GRB_ELIMIT, "batch colours exceed the supported maximum");
+}
+
+int grb_refresh_cost(grb_ctx* c) {
+    if (!c) return GRB_EINVAL;
+    GRB_CUDA(c, cudaSetDevice(c->device));
+    return refresh_plain(c);
+}
+
+int grb_route_batch(grb_ctx* c, int32_t b, int32_t stamp) {
+    if (!c || b < 0 || b >= c->n_batches) return c ? fail(c, GRB_EINVAL, "batch out of range") : GRB_EINVAL;
+    GRB_CUDA(c, cudaSetDevice(c->device));
+    return route_plain(c, b, stamp);
+}
+
+int grb_commit_batch(grb_ctx* c, int32_t b, int32_t stamp, int32_t K) {
+    if (!c || b < 0 || b >= c->n_batches || (K != 1 && K != -1)) return c ? fail(c, GRB_EINVAL, "bad commit arguments") : GRB_EINVAL;
+    GRB_CUDA(c, cudaSetDevice(c->device));
+    return commit_plain(c, b, stamp, K);
+}
+
+int grb_lshape_stage(grb_ctx* c, int32_t mode, grb_stats* stats) {
+    if (!c) return GRB_EINVAL;
+    if (!c->node_off) return fail(c, GRB_EINVAL, "no nets uploaded");
+    GRB_CUDA(c, cudaSetDevice(c->device));
+    const int stamp0 = c->stamp;
+    GRB_CUDA(c, cudaEventRecord(c->ev0, c->stream));
+    int rc;
+    if (mode == GRB_MODE_PLAIN) rc = stage_plain(c, stamp0);
+    else if (mode == GRB_MODE_GRAPH) rc = stage_graph(c, stamp0);
+    else if (mode == GRB_MODE_PERSISTENT) rc = stage_persistent(c, stamp0);
+    else return fail(c, GRB_EINVAL, "unknown mode");
+    if (rc) return rc;
+    GRB_CUDA(c, cudaEventRecord(c->ev1, c->stream));
+    c->stamp = stamp0 + c->n_batches;
+    rc = check_device_error(c);
+    if (rc) return rc;
+    float ms = 0;
+    GRB_CUDA(c, cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+    c->dag_ms = ms;
+    return stats ? grb_get_stats(c, stats) : GRB_OK;
+}
+
+int grb_ripup_classify(grb_ctx* c, int32_t threshold, uint8_t* is_of) {
+    if (!c || !is_of) return GRB_EINVAL;
+    GRB_CUDA(c, cudaSetDevice(c->device));
+    int* of_sum = nullptr;
+    unsigned char* flags = nullptr;
+    if (cudaMalloc(&of_sum, sizeof(int) * size_t(c->T.cells)) || cudaMalloc(&flags, std::max(c->n_nets, 1))) {
+        cudaGetLastError();
+        if (of_sum) cudaFree(of_sum);
+        return fail(c, GRB_ENOMEM, "rip-up buffers");
+    }
+    int tracks = 0;
+    for (int l = 0; l < c->T.L; ++l) tracks += (((l & 1) ^ c->T.DIR) ? c->T.X : c->T.Y);
+    k_mark_overflow<<<(c->T.cells + 255) / 256, 256, 0, c->stream>>>(c->T, threshold, of_sum);
+    k_int_prefix<<<(tracks + 127) / 128, 128, 0, c->stream>>>(c->T, of_sum);
+    Plan P = make_plan(c);
+    if (c->n_nets) k_overflow_nets<<<(c->n_nets + 255) / 256, 256, 0, c->stream>>>(c->T, P, c->n_nets, of_sum, flags);
+    c->launches += 3;
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemcpyAsync(is_of, flags, c->n_nets, cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    cudaFree(of_sum);
+    cudaFree(flags);
+    if (e != cudaSuccess) return cuda_fail(c, e, "rip-up classification");
+    return GRB_OK;
+}
+
+int grb_congestion_view(grb_ctx* c, uint8_t* congestion, float* xsum, float* ysum) {
+    if (!c || !congestion || !xsum || !ysum) return GRB_EINVAL;
+    GRB_CUDA(c, cudaSetDevice(c->device));
+    const int X = c->T.X, Y = c->T.Y, XY = c->T.XY;
+    unsigned char* d_c = nullptr;
+    float *d_x = nullptr, *d_y = nullptr;
+    if (cudaMalloc(&d_c, XY) || cudaMalloc(&d_x, 4 * size_t(XY)) || cudaMalloc(&d_y, 4 * size_t(XY))) {
+        cudaGetLastError();
+        for (void* p : {(void*)d_c, (void*)d_x, (void*)d_y}) if (p) cudaFree(p);
+        return fail(c, GRB_ENOMEM, "congestion buffers");
+    }
+    k_congestion<<<(XY + 255) / 256, 256, 0, c->stream>>>(c->T, d_c, d_x, d_y);
+    k_float_line_prefix<<<(X + 127) / 128, 128, 0, c->stream>>>(d_y, X, Y, Y, 1);   // per x, along y
+    k_float_line_prefix<<<(Y + 127) / 128, 128, 0, c->stream>>>(d_x, Y, X, 1, Y);   // per y, along x
+    c->launches += 3;
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemcpyAsync(congestion, d_c, XY, cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(xsum, d_x, 4 * size_t(XY), cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(ysum, d_y, 4 * size_t(XY), cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    cudaFree(d_c); cudaFree(d_x); cudaFree(d_y);
+    if (e != cudaSuccess) return cuda_fail(c, e, "congestion view");
+    return GRB_OK;
+}
+
+int grb_read_tables(grb_ctx* c, float* wcost, float* vcost, double* presum, int32_t* demand_half, int32_t* timestamp) {
+    if (!c) return GRB_EINVAL;
+    GRB_CUDA(c, cudaSetDevice(c->device));
+    const size_t cells = c->T.cells;
+    if (wcost) GRB_CUDA(c, cudaMemcpyAsync(wcost, c->T.wcost, 4 * cells, cudaMemcpyDeviceToHost, c->stream));
+    if (vcost) GRB_CUDA(c, cudaMemcpyAsync(vcost, c->T.vcost, 4 * cells, cudaMemcpyDeviceToHost, c->stream));
+    if (presum) GRB_CUDA(c, cudaMemcpyAsync(presum, c->T.presum, 8 * cells, cudaMemcpyDeviceToHost, c->stream));
+    if (demand_half) GRB_CUDA(c, cudaMemcpyAsync(demand_half, c->T.demand, 4 * cells, cudaMemcpyDeviceToHost, c->stream));
+    if (timestamp) GRB_CUDA(c, cudaMemcpyAsync(timestamp, c->T.ts, 4 * cells, cudaMemcpyDeviceToHost, c->stream));
+    GRB_CUDA(c, cudaStreamSynchronize(c->stream));
+    return check_device_error(c);
+}
+
+int grb_read_routes(grb_ctx* c, int32_t* routes) {
+    if (!c || !routes) return GRB_EINVAL;
+    GRB_CUDA(c, cudaSetDevice(c->device));
+    if (c->route_words) GRB_CUDA(c, cudaMemcpyAsync(routes, c->routes, sizeof(int) * c->route_words, cudaMemcpyDeviceToHost, c->stream));
+    GRB_CUDA(c, cudaStreamSynchronize(c->stream));
+    return GRB_OK;
+}
+
+int grb_get_stats(grb_ctx* c, grb_stats* s) {
+    if (!c || !s) return GRB_EINVAL;
+    GRB_CUDA(c, cudaSetDevice(c->device));
+    unsigned long long v = 0;
+    GRB_CUDA(c, cudaMemcpyAsync(&s->total_wirelength, c->T.wirelength, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    GRB_CUDA(c, cudaMemcpyAsync(&v, c->T.vias, sizeof(v), cudaMemcpyDeviceToHost, c->stream));
+    GRB_CUDA(c, cudaStreamSynchronize(c->stream));
+    s->total_via_count = static_cast<int64_t>(v);
+    s->n_batches = c->n_batches;
+    s->stamp = c->stamp;
+    s->batching_ms = c->batching_ms;
+    s->dag_ms = c->dag_ms;
+    return GRB_OK;
+}
+
+int grb_sync(grb_ctx* c) {
+    if (!c) return GRB_EINVAL;
+    GRB_CUDA(c, cudaSetDevice(c->device));
+    GRB_CUDA(c, cudaStreamSynchronize(c->stream));
+    return check_device_error(c);
+}
+
+int64_t grb_kernel_launches(grb_ctx* c) { return c ? c->launches : 0; }
+
+}  // extern "C"

@@ -1,0 +1,242 @@
+"""Host-side mirror of GRotor's routing-path interface over the C ABI.
+
+``Router`` plays the role of ``cudb::RouterState`` (router_state.hpp:182-232)
+and exposes the reference's hot-path seams under their reference names:
+
+* ``generate_batches_rsmt``  -- cudb::generate_batches_rsmt (generate_batches_cpu.hpp:7)
+* ``refresh_cost``           -- graph::refresh_cost (incremental_update.cuh:98)
+* ``route_batch``            -- the Lshape_route_warp launch (lshape.cuh:168)
+* ``commit_batch_demand``    -- graph::commit_batch_demand (demand.cuh:487)
+* ``lshape_route``           -- Lshape_route::Lshape_route's hot loop (lshape.cuh:153-179)
+* ``ripup``                  -- graph::ripup (congestion.cuh:114)
+
+Errors raise ``GrbError`` with the library's message (the reference throws
+std::runtime_error from cuda_check, cuda_memory.hpp:12-15).
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _abi
+
+MODE_PLAIN, MODE_GRAPH, MODE_PERSISTENT = _abi.MODE_PLAIN, _abi.MODE_GRAPH, _abi.MODE_PERSISTENT
+_MODES = {"plain": MODE_PLAIN, "graph": MODE_GRAPH, "persistent": MODE_PERSISTENT}
+
+
+class GrbError(RuntimeError):
+    def __init__(self, code: int, message: str):
+        super().__init__(f"{_abi.ERROR_NAMES.get(code, code)}: {message}")
+        self.code = code
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+def _c(a, dt):
+    return np.ascontiguousarray(a, dtype=dt)
+
+
+def mode_id(mode) -> int:
+    return _MODES[mode] if isinstance(mode, str) else int(mode)
+
+
+@dataclass
+class GridArrays:
+    L: int
+    X: int
+    Y: int
+    DIR: int
+    unit_wire: float
+    unit_via: float
+    short_costs: np.ndarray
+    x_edge_len: np.ndarray
+    y_edge_len: np.ndarray
+    capacity: np.ndarray
+    of_cost_scale: float = 1.0
+
+    @property
+    def cells(self) -> int:
+        return self.L * self.X * self.Y
+
+    def struct(self) -> _abi.GrbGrid:
+        self._keep = [_c(self.short_costs, np.float64), _c(self.x_edge_len, np.int32),
+                      _c(self.y_edge_len, np.int32), _c(self.capacity, np.float32).reshape(-1)]
+        s = _abi.GrbGrid(self.L, self.X, self.Y, self.DIR, self.unit_wire, self.unit_via, self.of_cost_scale,
+                         *[_p(a) for a in self._keep])
+        return s
+
+
+@dataclass
+class NetArrays:
+    node_off: np.ndarray
+    nodes: np.ndarray
+    parents: np.ndarray
+    route_off: np.ndarray
+    point_off: np.ndarray
+    points: np.ndarray
+    hseg_off: np.ndarray
+    hsegs: np.ndarray
+    vseg_off: np.ndarray
+    vsegs: np.ndarray
+
+    @property
+    def n(self) -> int:
+        return len(self.node_off) - 1
+
+    def struct(self) -> _abi.GrbNets:
+        self._keep = [_c(self.node_off, np.int32), _c(self.nodes, np.int32), _c(self.parents, np.int32),
+                      _c(self.route_off, np.int64), _c(self.point_off, np.int32), _c(self.points, np.int32),
+                      _c(self.hseg_off, np.int32), _c(self.hsegs, np.int32), _c(self.vseg_off, np.int32),
+                      _c(self.vsegs, np.int32)]
+        return _abi.GrbNets(self.n, *[_p(a) for a in self._keep])
+
+
+class Router:
+    """One routing context on one GPU (owns device memory and a CUDA stream)."""
+
+    def __init__(self, grid: GridArrays, device: int = 0):
+        self._lib = _abi.load()
+        self.grid = grid
+        self._ctx = C.c_void_p()
+        s = grid.struct()
+        rc = self._lib.grb_create(C.byref(s), int(device), C.byref(self._ctx))
+        if rc:
+            raise GrbError(rc, "grb_create failed")
+        self.nets: NetArrays | None = None
+
+    # -- lifecycle ---------------------------------------------------------
+    def close(self):
+        if self._ctx:
+            self._lib.grb_destroy(self._ctx)
+            self._ctx = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def _check(self, rc: int):
+        if rc:
+            raise GrbError(rc, self._lib.grb_last_error(self._ctx).decode())
+
+    @property
+    def stream_handle(self) -> int:
+        return int(self._lib.grb_stream(self._ctx) or 0)
+
+    @property
+    def kernel_launches(self) -> int:
+        return int(self._lib.grb_kernel_launches(self._ctx))
+
+    def reset(self):
+        self._check(self._lib.grb_reset(self._ctx))
+
+    def upload_nets(self, nets: NetArrays):
+        self.nets = nets
+        s = nets.struct()
+        self._check(self._lib.grb_upload_nets(self._ctx, C.byref(s)))
+
+    # -- batching ------------------------------------------------------------
+    def generate_batches_rsmt(self, order, limit: int = 1000000, sparsity: int = 1, mode="persistent"):
+        """Exact first-fit batching; installs the reversed, flattened plan and
+        returns (batch_of per order position, number of batches)."""
+        order = _c(order, np.int32)
+        out = np.empty(len(order), np.int32)
+        nb = C.c_int32(0)
+        self._check(self._lib.grb_plan_batches(self._ctx, _p(order), len(order), int(limit), int(sparsity),
+                                               mode_id(mode), _p(out), C.byref(nb)))
+        return out, nb.value
+
+    def set_plan(self, ids, batch_off):
+        ids = _c(ids, np.int32)
+        batch_off = _c(batch_off, np.int32)
+        self._check(self._lib.grb_set_plan(self._ctx, _p(ids), len(ids), _p(batch_off), len(batch_off) - 1))
+
+    def plan(self):
+        n, nb = C.c_int32(0), C.c_int32(0)
+        self._check(self._lib.grb_get_plan(self._ctx, None, None, C.byref(n), C.byref(nb)))
+        ids = np.empty(n.value, np.int32)
+        off = np.empty(nb.value + 1, np.int32)
+        self._check(self._lib.grb_get_plan(self._ctx, _p(ids), _p(off), C.byref(n), C.byref(nb)))
+        return ids, off
+
+    # -- per-batch seams -------------------------------------------------------
+    def refresh_cost(self):
+        self._check(self._lib.grb_refresh_cost(self._ctx))
+
+    def route_batch(self, b: int, stamp: int):
+        self._check(self._lib.grb_route_batch(self._ctx, int(b), int(stamp)))
+
+    def commit_batch_demand(self, b: int, stamp: int, K: int = 1):
+        self._check(self._lib.grb_commit_batch(self._ctx, int(b), int(stamp), int(K)))
+
+    # -- stage -------------------------------------------------------------------
+    def lshape_route(self, mode="persistent") -> dict:
+        st = _abi.GrbStats()
+        self._check(self._lib.grb_lshape_stage(self._ctx, mode_id(mode), C.byref(st)))
+        return _stats_dict(st)
+
+    def ripup(self, threshold: int = 0) -> np.ndarray:
+        out = np.zeros(self.nets.n if self.nets else 0, np.uint8)
+        self._check(self._lib.grb_ripup_classify(self._ctx, int(threshold), _p(out)))
+        return out
+
+    def congestion_view(self):
+        xy = self.grid.X * self.grid.Y
+        cong = np.empty(xy, np.uint8)
+        xs = np.empty(xy, np.float32)
+        ys = np.empty(xy, np.float32)
+        self._check(self._lib.grb_congestion_view(self._ctx, _p(cong), _p(xs), _p(ys)))
+        return cong, xs, ys
+
+    # -- readback ----------------------------------------------------------------
+    def read_tables(self) -> dict:
+        n = self.grid.cells
+        out = {"wcost": np.empty(n, np.float32), "vcost": np.empty(n, np.float32),
+               "presum": np.empty(n, np.float64), "demand_half": np.empty(n, np.int32),
+               "timestamp": np.empty(n, np.int32)}
+        self._check(self._lib.grb_read_tables(self._ctx, _p(out["wcost"]), _p(out["vcost"]), _p(out["presum"]),
+                                              _p(out["demand_half"]), _p(out["timestamp"])))
+        return out
+
+    def read_routes(self) -> np.ndarray:
+        words = int(self.nets.route_off[-1]) if self.nets is not None else 0
+        out = np.zeros(words, np.int32)
+        self._check(self._lib.grb_read_routes(self._ctx, _p(out)))
+        return out
+
+    def stats(self) -> dict:
+        st = _abi.GrbStats()
+        self._check(self._lib.grb_get_stats(self._ctx, C.byref(st)))
+        return _stats_dict(st)
+
+    def sync(self):
+        self._check(self._lib.grb_sync(self._ctx))
+
+
+def _stats_dict(st: _abi.GrbStats) -> dict:
+    return {"wirelength": st.total_wirelength, "vias": int(st.total_via_count), "n_batches": st.n_batches,
+            "stamp": st.stamp, "batching_ms": st.batching_ms, "dag_ms": st.dag_ms}
+
+
+def plan_from_batches(order, batch_of, n_batches):
+    """Reverse and flatten a first-fit result into execution order
+    (lshape.cuh:70-77): batch n_batches-1 runs first, nets keep order."""
+    order = np.asarray(order)
+    batch_of = np.asarray(batch_of)
+    ids, off = [], [0]
+    for c in range(n_batches - 1, -1, -1):
+        sel = order[batch_of == c]
+        ids.append(sel)
+        off.append(off[-1] + len(sel))
+    return (np.concatenate(ids).astype(np.int32) if ids else np.zeros(0, np.int32)), np.asarray(off, np.int32)

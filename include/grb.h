@@ -1,0 +1,157 @@
+/*
+ * grb.h -- C ABI of grotor_b200: GRotor's routing hot path on NVIDIA B200.
+ *
+ * The reference router (GRotor) has no plugin or FFI layer; its hot path sits
+ * behind a handful of C++ functions called from its stage drivers.  Each entry
+ * point below replaces one of them (reference file:line, paths relative to the
+ * GRotor project root).  The host pipeline (CAP/NET parsing, net splitting,
+ * RSMT/FLT topology construction, .out writer) stays in the caller.
+ *
+ * Conventions
+ *  - Grid cell index IDX(l,x,y) = (l*X + x)*Y + y over the L routing layers
+ *    (router_state.hpp:267).  Layer l carries wires along y when
+ *    ((l & 1) ^ DIR) == 1, along x otherwise (DIR = direction of CAP layer 1,
+ *    preprocess.hpp:1616).
+ *  - Tree nodes are 3-D cell ids; Steiner nodes use layer L (preprocess.hpp:131).
+ *  - Route words per net: [count, a0, b0, a1, b1, ...] where count is one past
+ *    the last used word, exactly the reference's route record
+ *    (lshape_warp.cuh:414-439); a pair with equal layers is a wire, otherwise a
+ *    via stack.
+ *  - Demand is int32 half-units (wire edge +2, split via landing +1 each side);
+ *    demand_half * 0.5f equals the reference's float demand bit-for-bit.
+ *  - Every call returns GRB_OK or an error code and never throws; the text of
+ *    the last error is available from grb_last_error().  A context owns all of
+ *    its device memory and one CUDA stream; it is not thread-safe.
+ *  - There is no CPU fallback: every compute entry point runs CUDA kernels.
+ */
+#ifndef GRB_H
+#define GRB_H
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GRB_OK 0
+#define GRB_EINVAL 1     /* bad argument or inconsistent input */
+#define GRB_ENOMEM 2     /* device allocation failed */
+#define GRB_ECUDA 3      /* CUDA runtime error */
+#define GRB_ETIMEDOUT 4  /* a bounded device wait expired */
+#define GRB_ELIMIT 5     /* route storage or batch-colour capacity exceeded */
+
+#define GRB_MODE_PLAIN 0       /* one launch sequence per batch (reference structure) */
+#define GRB_MODE_GRAPH 1       /* the plain sequence captured in one CUDA graph */
+#define GRB_MODE_PERSISTENT 2  /* one cooperative kernel runs every batch */
+
+typedef struct grb_ctx grb_ctx;
+
+/* Routing grid and cost model: the device tables built by
+ * build_cuda_database (preprocess.hpp:1625-1786). */
+typedef struct grb_grid {
+    int32_t L, X, Y, DIR;
+    double unit_length_wire_cost;
+    double unit_via_cost;
+    double of_cost_scale;                   /* 1.0 on one GPU (router_state.hpp:37) */
+    const double* unit_length_short_costs;  /* [L] overflow weight per routing layer */
+    const int32_t* x_edge_len;              /* [X-1] */
+    const int32_t* y_edge_len;              /* [Y-1] */
+    const float* capacity;                  /* [L*X*Y] */
+} grb_grid;
+
+/* Per-net topology and batching geometry, indexed by net id (the reference's
+ * net::rsmt DFS order, net::points, rsmt_h_segments, rsmt_v_segments;
+ * lshape.cuh:85-103, preprocess.hpp:88-130). */
+typedef struct grb_nets {
+    int32_t n;
+    const int32_t* node_off;   /* [n+1] */
+    const int32_t* nodes;      /* DFS order, node 0 = root */
+    const int32_t* parents;    /* parent index < child index, -1 at the root */
+    const int64_t* route_off;  /* [n+1] word offsets; route capacity of net i = route_off[i+1]-route_off[i] */
+    const int32_t* point_off;  /* [n+1] */
+    const int32_t* points;     /* 2-D cell ids x*Y+y */
+    const int32_t* hseg_off;   /* [n+1] */
+    const int32_t* hsegs;      /* pairs (first, second), 2-D ids, step Y */
+    const int32_t* vseg_off;   /* [n+1] */
+    const int32_t* vsegs;      /* pairs (first, second), 2-D ids, step 1 */
+} grb_nets;
+
+typedef struct grb_stats {
+    double total_wirelength;   /* RoutingStatistics::total_wirelength (router_state.hpp:17-20) */
+    int64_t total_via_count;   /* RoutingStatistics::total_via_count */
+    int32_t n_batches;
+    int32_t stamp;             /* RouterState::global_timestamp after the call */
+    double batching_ms;        /* device time of the last grb_plan_batches */
+    double dag_ms;             /* device time of the last stage */
+} grb_stats;
+
+/* Create a context on `device` and upload the grid (build_cuda_database,
+ * preprocess.hpp:1625; initialize_incremental_cost, incremental_update.cuh:7). */
+int grb_create(const grb_grid* grid, int32_t device, grb_ctx** out);
+void grb_destroy(grb_ctx* ctx);
+const char* grb_last_error(const grb_ctx* ctx);
+/* The context's CUDA stream (cudaStream_t) for callers that time or order work. */
+void* grb_stream(grb_ctx* ctx);
+
+/* Zero demand, timestamps, statistics and routes; mark every cost dirty
+ * (the state of a freshly built database; lshape_benchmark.cuh:276-290). */
+int grb_reset(grb_ctx* ctx);
+
+/* Upload per-net topology and geometry (host buffers; replaces the uploads in
+ * Lshape_route, lshape.cuh:126-138, and the batching inputs). */
+int grb_upload_nets(grb_ctx* ctx, const grb_nets* nets);
+
+/* Exact first-fit batching of nets `order[0..n)` with at most `limit` nets per
+ * batch (cudb::generate_batches_rsmt, generate_batches_cpu.hpp:7-73, and its
+ * RT-core replacements).  The result becomes the context's plan in execution
+ * order: batches reversed and flattened as in lshape.cuh:70-77.  If batch_of
+ * is not NULL it receives the batch index of every order position. */
+int grb_plan_batches(grb_ctx* ctx, const int32_t* order, int32_t n, int32_t limit, int32_t sparsity,
+                     int32_t mode, int32_t* batch_of, int32_t* n_batches);
+
+/* Set an explicit plan: net ids in execution order and batch offsets. */
+int grb_set_plan(grb_ctx* ctx, const int32_t* ids, int32_t n, const int32_t* batch_off, int32_t n_batches);
+/* Copy the current plan out (ids[n], batch_off[n_batches+1]). */
+int grb_get_plan(grb_ctx* ctx, int32_t* ids, int32_t* batch_off, int32_t* n, int32_t* n_batches);
+
+/* graph::refresh_cost (incremental_update.cuh:98-132): bring wcost, vcost
+ * and the per-track prefix table up to date with demand. */
+int grb_refresh_cost(grb_ctx* ctx);
+
+/* Route batch `b` of the plan with L-shape patterns (Lshape_route_warp,
+ * lshape_warp.cuh:304-446); writes routes only. */
+int grb_route_batch(grb_ctx* ctx, int32_t b, int32_t stamp);
+
+/* graph::commit_batch_demand (demand.cuh:487-493): K = +1 commits, K = -1
+ * rips up the batch's routes. */
+int grb_commit_batch(grb_ctx* ctx, int32_t b, int32_t stamp, int32_t K);
+
+/* Run the whole L-shape stage over the plan: per batch ++stamp, refresh cost,
+ * route, commit (Lshape_route::Lshape_route hot loop, lshape.cuh:153-179). */
+int grb_lshape_stage(grb_ctx* ctx, int32_t mode, grb_stats* stats);
+
+/* Rip-up classification (graph::ripup, congestion.cuh:114-136): is_of[id] = 1
+ * for nets whose route crosses more than 10 edges with demand >= capacity +
+ * threshold. */
+int grb_ripup_classify(grb_ctx* ctx, int32_t threshold, uint8_t* is_of);
+
+/* Congestion view for the FLT topology builder (congestion.cuh:60-112). */
+int grb_congestion_view(grb_ctx* ctx, uint8_t* congestion, float* xsum, float* ysum);
+
+/* Read device tables (any pointer may be NULL). */
+int grb_read_tables(grb_ctx* ctx, float* wcost, float* vcost, double* presum, int32_t* demand_half,
+                    int32_t* timestamp);
+/* Copy all route words (route_off[n] words) to the host. */
+int grb_read_routes(grb_ctx* ctx, int32_t* routes);
+int grb_get_stats(grb_ctx* ctx, grb_stats* stats);
+/* Wait for the context's stream and report any recorded device error. */
+int grb_sync(grb_ctx* ctx);
+
+/* Number of kernels this context has launched so far (graph launches count
+ * every kernel node); used for launch accounting by callers. */
+int64_t grb_kernel_launches(grb_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,538 @@
+// grb_oracle.cpp -- CPU restatement of GRotor's routing hot path (test checker).
+//
+// TEST INFRASTRUCTURE ONLY: loaded by tests/, __graft_entry__.smoke() and the
+// CPU-baseline leg of bench.py, never by the product.  Each routine restates
+// the reference's algorithm; citations are file:line in the GRotor project.
+#include "grb_oracle.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+namespace {
+
+constexpr double kInf = 1e22;  // router_state.hpp:271
+
+struct Grid {
+    const orc_grid* g;
+    int L, X, Y, DIR;
+    explicit Grid(const orc_grid* p) : g(p), L(p->L), X(p->X), Y(p->Y), DIR(p->DIR) {}
+    int idx(int l, int x, int y) const { return (l * X + x) * Y + y; }
+    bool along_y(int l) const { return ((l & 1) ^ DIR) != 0; }
+};
+
+// full_update.cuh:9-14 (of_cost_scaled).  The reference passes capacity and
+// demand as float; the difference is a float subtraction, scaled in double, and
+// the argument of the exponential is narrowed to float.  The host expf stands in
+// for CUDA's __expf (tolerance-level agreement, see header).
+double of_cost_scaled(double scale, float capacity, float demand) {
+    if (capacity > 0.001) {
+        const float diff = demand - capacity;
+        const double a = 0.5 * static_cast<double>(diff);
+        const double b = scale * 0.5 * static_cast<double>(diff);
+        return static_cast<double>(expf(static_cast<float>(std::min(a, b))));
+    }
+    if (demand > 0) {
+        const double a = 1.5 * static_cast<double>(demand);
+        const double b = scale * 1.5 * static_cast<double>(demand);
+        return static_cast<double>(expf(static_cast<float>(std::min(a, b))));
+    }
+    return 0;
+}
+
+// full_update.cuh:23-32 (incremental_of_cost).
+double incremental_of_cost(const Grid& G, const int32_t* demand_half, int l, int x, int y,
+                           double incre, double base) {
+    const int i = G.idx(l, x, y);
+    const float cap = G.g->capacity[i];
+    const float dem = static_cast<float>(demand_half[i]) * 0.5f;
+    const float with = static_cast<float>(static_cast<double>(dem) + incre + base);
+    const float without = static_cast<float>(static_cast<double>(dem) + base);
+    const double delta = (of_cost_scaled(G.g->of_cost_scale, cap, with) -
+                          of_cost_scaled(G.g->of_cost_scale, cap, without)) * G.g->short_costs[l];
+    return std::min(1e12, delta);
+}
+
+// full_update.cuh:34-51 (update_single_wcost_ispd24).  The wire-length term is
+// a multiply feeding an add, which the CUDA compiler contracts to one fma.
+float wire_cost(const Grid& G, const int32_t* demand_half, int l, int x, int y) {
+    float w = static_cast<float>(incremental_of_cost(G, demand_half, l, x, y, 1, 0));
+    if (!G.along_y(l) && x < G.X - 1)
+        w = static_cast<float>(std::fma(G.g->unit_wire, static_cast<double>(G.g->x_edge_len[x]), static_cast<double>(w)));
+    if (G.along_y(l) && y < G.Y - 1)
+        w = static_cast<float>(std::fma(G.g->unit_wire, static_cast<double>(G.g->y_edge_len[y]), static_cast<double>(w)));
+    return w;
+}
+
+// full_update.cuh:58-83 (update_single_vcost_ispd24); cross points are 0 on
+// one GPU (preprocess.hpp:1757).
+float via_cost(const Grid& G, const int32_t* d, int l, int x, int y) {
+    float v;
+    if (G.along_y(l)) {
+        if (y == 0) v = static_cast<float>(incremental_of_cost(G, d, l, x, y, 1, 0));
+        else if (y == G.Y - 1) v = static_cast<float>(incremental_of_cost(G, d, l, x, y - 1, 1, 0));
+        else v = static_cast<float>(incremental_of_cost(G, d, l, x, y, 0.5, 0) + incremental_of_cost(G, d, l, x, y - 1, 0.5, 0));
+    } else {
+        if (x == 0) v = static_cast<float>(incremental_of_cost(G, d, l, x, y, 1, 0));
+        else if (x == G.X - 1) v = static_cast<float>(incremental_of_cost(G, d, l, x - 1, y, 1, 0));
+        else v = static_cast<float>(incremental_of_cost(G, d, l, x, y, 0.5, 0) + incremental_of_cost(G, d, l, x - 1, y, 0.5, 0));
+    }
+    return static_cast<float>(static_cast<double>(v) + G.g->unit_via);
+}
+
+// One track of the prefix: shifted input s[0] = 0, s[i] = w[i-1]; output
+// S(i) = sum_{j<=i} s[j] added exactly as the log-step scan of
+// prefix_scan.cuh:84-95 adds it (equivalently the Fenwick rebuild of
+// fenwick.cuh:146-166): for each set bit d of i, lowest first, add the total of
+// the aligned 2^d block just below.  Block totals are pairwise sums, kept on a
+// stack tot[d] = total of the most recently completed aligned 2^d block.
+template <class T, class Load, class Store>
+void sklansky_track(int n, Load load, Store store) {
+    T tot[32];
+    for (int i = 0; i < n; ++i) {
+        T acc = i ? load(i - 1) : T(0);
+        int d = 0;
+        T fresh[32];
+        fresh[0] = acc;
+        while ((i >> d) & 1) {
+            acc = acc + tot[d];
+            ++d;
+            fresh[d] = acc;
+        }
+        for (int j = 0; j <= d; ++j) tot[j] = fresh[j];
+        for (int e = d + 1; (i >> e) != 0; ++e)
+            if ((i >> e) & 1) acc = acc + tot[e];
+        store(i, acc);
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+void orc_cost_full(const orc_grid* g, const int32_t* demand_half, float* wcost, float* vcost) {
+    Grid G(g);
+    const int cells = G.L * G.X * G.Y;
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < cells; ++i) {
+        const int l = i / (G.X * G.Y), x = i / G.Y % G.X, y = i % G.Y;
+        if (wcost) wcost[i] = wire_cost(G, demand_half, l, x, y);
+        if (vcost) vcost[i] = via_cost(G, demand_half, l, x, y);
+    }
+}
+
+// prefix_scan.cuh:74-114 / fenwick.cuh:129-168: one track per (layer, row or
+// column along the preferred direction).
+void orc_presum(const orc_grid* g, const float* wcost, double* presum) {
+    Grid G(g);
+    for (int l = 0; l < G.L; ++l) {
+        const bool ay = G.along_y(l);
+        const int tracks = ay ? G.X : G.Y, len = ay ? G.Y : G.X, stride = ay ? 1 : G.Y;
+#pragma omp parallel for schedule(static)
+        for (int t = 0; t < tracks; ++t) {
+            const int base = ay ? G.idx(l, t, 0) : G.idx(l, 0, t);
+            sklansky_track<double>(len,
+                [&](int k) { return static_cast<double>(wcost[base + k * stride]); },
+                [&](int k, double v) { presum[base + k * stride] = v; });
+        }
+    }
+}
+
+// Literal log-step loop of prefix_scan.cuh:84-95.
+void orc_presum_logstep(const orc_grid* g, const float* wcost, double* presum) {
+    Grid G(g);
+    std::vector<double> s;
+    for (int l = 0; l < G.L; ++l) {
+        const bool ay = G.along_y(l);
+        const int tracks = ay ? G.X : G.Y, len = ay ? G.Y : G.X, stride = ay ? 1 : G.Y;
+        s.assign(len, 0.0);
+        for (int t = 0; t < tracks; ++t) {
+            const int base = ay ? G.idx(l, t, 0) : G.idx(l, 0, t);
+            s[0] = 0;
+            for (int k = 0; k + 1 < len; ++k) s[k + 1] = wcost[base + k * stride];
+            for (int d = 0; (1 << d) < len; ++d)
+                for (int i = len - 1; i >= 0; --i)  // disjoint reads/writes per level
+                    if ((i >> d) & 1) s[i] += s[((i >> d) << d) - 1];
+            for (int k = 0; k < len; ++k) presum[base + k * stride] = s[k];
+        }
+    }
+}
+
+// lshape_thread.cuh:18-171 (Lshape_route_cuda), one net at a time; the warp
+// kernel lshape_warp.cuh:304-446 is equal to it by construction (children of a
+// parent are merged in descending node order in both).
+int orc_lshape_batch(const orc_grid* g, const float* vcost, const double* presum,
+                     int32_t n, const int32_t* ids, const int32_t* node_off,
+                     const int32_t* nodes, const int32_t* parents,
+                     const int64_t* route_off, int32_t* routes) {
+    Grid G(g);
+    const int L = G.L, X = G.X, Y = G.Y, DIR = G.DIR;
+    int status = 0;
+    auto wire = [&](int l, int xmin, int xmax, int ymin, int ymax) {  // prefix_scan.cuh:10-40
+        return presum[G.idx(l, xmax, ymax)] - presum[G.idx(l, xmin, ymin)];
+    };
+#pragma omp parallel for schedule(dynamic, 16)
+    for (int k = 0; k < n; ++k) {
+        const int id = ids[k];
+        const int N = node_off[id + 1] - node_off[id];
+        const int* nd = nodes + node_off[id];
+        const int* par = parents + node_off[id];
+        std::vector<double> dist(size_t(N) * L * L);
+        std::vector<int> from(size_t(N) * L * L, 0), range(N, 0);
+        for (int i = 0; i < N; ++i) {
+            const int l = nd[i] / X / Y, x = nd[i] / Y % X, y = nd[i] % Y;
+            double* d = dist.data() + size_t(i) * L * L;
+            for (int lo = 0; lo < L; ++lo) {
+                d[lo * L + lo] = 0;
+                for (int hi = lo + 1; hi < L; ++hi)
+                    d[lo * L + hi] = d[lo * L + hi - 1] + static_cast<double>(vcost[G.idx(hi - 1, x, y)]);
+                for (int hi = lo; hi < L; ++hi)
+                    if (l < L && (lo > l || hi < l)) d[lo * L + hi] = kInf;
+            }
+        }
+        for (int i = N - 1; i >= 1; --i) {
+            const int x = nd[i] / Y % X, y = nd[i] % Y;
+            const int p = par[i], px = nd[p] / Y % X, py = nd[p] % Y;
+            const int minx = std::min(x, px), maxx = std::max(x, px), miny = std::min(y, py), maxy = std::max(y, py);
+            const double* nd_dist = dist.data() + size_t(i) * L * L;
+            double* par_dist = dist.data() + size_t(p) * L * L;
+            int* prev = from.data() + size_t(i) * L * L;
+            double cur[10], mcp[100];
+            int cur_from[10] = {0};
+            for (int l = 0; l < L; ++l) {
+                cur[l] = mcp[l * L + l] = kInf;
+                for (int lo = 0; lo <= l; ++lo)
+                    for (int hi = l; hi < L; ++hi)
+                        if (nd_dist[lo * L + hi] < cur[l]) { cur[l] = nd_dist[lo * L + hi]; cur_from[l] = lo * L + hi; }
+            }
+            if (x == px || y == py) {
+                for (int l = 0; l < L; ++l) {
+                    if (((l & 1) ^ DIR) == 0 && y != py) continue;
+                    if (((l & 1) ^ DIR) == 1 && x != px) continue;
+                    mcp[l * L + l] = cur[l] + wire(l, minx, maxx, miny, maxy);
+                    prev[l * L + l] = cur_from[l] * L * L + l * L + l;
+                }
+            } else {
+                for (int cl = 0; cl < L; ++cl) {
+                    double cost = cur[cl];
+                    if ((cl & 1) ^ DIR) cost += wire(cl, x, x, miny, maxy);
+                    else cost += wire(cl, minx, maxx, y, y);
+                    for (int pl = (cl & 1) ^ 1; pl < L; pl += 2) {
+                        double cost2 = 0;
+                        for (int l = std::min(cl, pl) + 1; l < std::max(cl, pl); ++l)
+                            cost2 += ((cl & 1) ^ DIR) ? vcost[G.idx(l, x, py)] : vcost[G.idx(l, px, y)];
+                        if ((pl & 1) ^ DIR) cost2 += wire(pl, px, px, miny, maxy);
+                        else cost2 += wire(pl, minx, maxx, py, py);
+                        if (cost + cost2 < mcp[pl * L + pl]) {
+                            mcp[pl * L + pl] = cost + cost2;
+                            prev[pl * L + pl] = cur_from[cl] * L * L + cl * L + pl;
+                        }
+                    }
+                }
+            }
+            for (int lo = 0; lo < L; ++lo) {
+                for (int hi = lo + 1; hi < L; ++hi) {
+                    if (mcp[lo * L + hi - 1] <= mcp[hi * L + hi]) {
+                        mcp[lo * L + hi] = mcp[lo * L + hi - 1];
+                        prev[lo * L + hi] = prev[lo * L + hi - 1];
+                    } else {
+                        mcp[lo * L + hi] = mcp[hi * L + hi];
+                        prev[lo * L + hi] = prev[hi * L + hi];
+                    }
+                }
+                for (int hi = lo; hi < L; ++hi) par_dist[lo * L + hi] += mcp[lo * L + hi];
+            }
+        }
+        // Root choice and traceback (lshape_thread.cuh:117-170).
+        int32_t* out = routes + route_off[id];
+        const int64_t cap = route_off[id + 1] - route_off[id];
+        int64_t cnt = 1;
+        bool overflow = false;
+        auto emit = [&](int a, int b) {
+            if (cnt + 2 > cap) { overflow = true; return; }
+            out[cnt++] = a; out[cnt++] = b;
+        };
+        range[0] = 0;
+        for (int lo = 0; lo < L; ++lo)
+            for (int hi = lo; hi < L; ++hi)
+                if (dist[lo * L + hi] < dist[range[0]]) range[0] = lo * L + hi;
+        for (int i = 0; i < N; ++i) {
+            const int* prev = from.data() + size_t(i) * L * L;
+            if (i > 0) range[i] = prev[range[par[i]]] / L / L;
+            const int minl = range[i] / L, maxl = range[i] % L, x = nd[i] / Y % X, y = nd[i] % Y;
+            if (minl < maxl) emit(G.idx(minl, x, y), G.idx(maxl, x, y));
+            if (i == 0) continue;
+            const int px = nd[par[i]] / Y % X, py = nd[par[i]] % Y;
+            const int minx = std::min(x, px), maxx = std::max(x, px), miny = std::min(y, py), maxy = std::max(y, py);
+            const int cl = prev[range[par[i]]] / L % L, pl = prev[range[par[i]]] % L;
+            if (px == x || py == y) {
+                emit(G.idx(cl, minx, miny), G.idx(cl, maxx, maxy));
+            } else if ((cl & 1) ^ DIR) {
+                emit(G.idx(cl, x, y), G.idx(cl, x, py));
+                emit(G.idx(cl, x, py), G.idx(pl, x, py));
+                emit(G.idx(pl, x, py), G.idx(pl, px, py));
+            } else {
+                emit(G.idx(cl, x, y), G.idx(cl, px, y));
+                emit(G.idx(cl, px, y), G.idx(pl, px, y));
+                emit(G.idx(pl, px, y), G.idx(pl, px, py));
+            }
+        }
+        if (cap > 0) out[0] = static_cast<int32_t>(cnt);
+        if (overflow) {
+#pragma omp critical
+            if (!status) status = -1 - k;
+        }
+    }
+    return status;
+}
+
+}  // extern "C"
+
+namespace {
+// demand.cuh:410-493 (commit_batch_wires then commit_batch_vias).  `touched`,
+// when given, receives every edge cell whose demand changed.
+void commit_impl(const orc_grid* g, int32_t n, const int32_t* ids,
+                 const int64_t* route_off, const int32_t* routes,
+                 int32_t stamp, int32_t K, int32_t* demand_half, int32_t* timestamp,
+                 double* total_wirelength, int64_t* total_vias, std::vector<int>* touched) {
+    Grid G(g);
+    const int X = G.X, Y = G.Y, XY = X * Y;
+    double length = 0;
+    for (int k = 0; k < n; ++k) {
+        const int32_t* r = routes + route_off[ids[k]];
+        for (int i = 1; i < r[0]; i += 2) {
+            const int a = r[i], b = r[i + 1], layer = a / XY;
+            if (layer != b / XY) continue;
+            const int x0 = a / Y % X, y0 = a % Y, x1 = b / Y % X, y1 = b % Y;
+            const bool ay = x0 == x1;
+            const int lo = ay ? std::min(y0, y1) : std::min(x0, x1);
+            const int hi = ay ? std::max(y0, y1) : std::max(x0, x1);
+            timestamp[a] = timestamp[b] = stamp;
+            for (int pos = lo; pos < hi; ++pos) {
+                const int index = layer * XY + (ay ? x0 * Y + pos : pos * Y + y0);
+                demand_half[index] += 2 * K;
+                timestamp[index] = stamp;
+                if (touched) touched->push_back(index);
+                length += ay ? g->y_edge_len[pos] : g->x_edge_len[pos];
+            }
+        }
+    }
+    int64_t vias = 0;
+    for (int k = 0; k < n; ++k) {
+        const int32_t* r = routes + route_off[ids[k]];
+        for (int i = 1; i < r[0]; i += 2) {
+            const int a = r[i], b = r[i + 1];
+            const int low = std::min(a / XY, b / XY), high = std::max(a / XY, b / XY);
+            if (low == high) continue;
+            const int x = a / Y % X, y = a % Y;
+            vias += high - low;
+            for (int layer = low; layer < high; ++layer) {
+                const int index = layer * XY + x * Y + y;
+                if (timestamp[index] >= stamp) continue;
+                const bool ay = G.along_y(layer);
+                const int position = ay ? y : x, len = ay ? Y : X, stride = ay ? 1 : Y;
+                if (!position) { demand_half[index] += 2 * K; if (touched) touched->push_back(index); }
+                else if (position == len - 1) { demand_half[index - stride] += 2 * K; if (touched) touched->push_back(index - stride); }
+                else {
+                    demand_half[index - stride] += K; demand_half[index] += K;
+                    if (touched) { touched->push_back(index - stride); touched->push_back(index); }
+                }
+            }
+        }
+    }
+    if (total_wirelength) *total_wirelength += length * K;
+    if (total_vias) *total_vias += vias * K;
+}
+}  // namespace
+
+extern "C" {
+
+void orc_commit_batch(const orc_grid* g, int32_t n, const int32_t* ids,
+                      const int64_t* route_off, const int32_t* routes,
+                      int32_t stamp, int32_t K, int32_t* demand_half, int32_t* timestamp,
+                      double* total_wirelength, int64_t* total_vias) {
+    commit_impl(g, n, ids, route_off, routes, stamp, K, demand_half, timestamp, total_wirelength, total_vias, nullptr);
+}
+
+// generate_batches_cpu.hpp:7-73 (generate_batches_rsmt).
+int32_t orc_batches(int32_t X, int32_t Y, int32_t n, const int32_t* order,
+                    const int32_t* point_off, const int32_t* points,
+                    const int32_t* hseg_off, const int32_t* hsegs,
+                    const int32_t* vseg_off, const int32_t* vsegs,
+                    int32_t limit, int32_t sparsity, int32_t* batch_of) {
+    std::vector<std::vector<uint8_t>> vis;
+    std::vector<int32_t> size;
+    for (int k = 0; k < n; ++k) {
+        const int id = order[k];
+        int bid = -1;
+        for (int b = 0; b < static_cast<int>(vis.size()); ++b) {
+            if (size[b] >= limit) continue;
+            bool conflict = false;
+            for (int q = point_off[id]; q < point_off[id + 1] && !conflict; ++q)
+                conflict = vis[b][points[q]] != 0;
+            if (!conflict) { bid = b; break; }
+        }
+        if (bid < 0) {
+            bid = static_cast<int>(vis.size());
+            vis.emplace_back(size_t(X) * Y, 0);
+            size.push_back(0);
+        }
+        ++size[bid];
+        batch_of[k] = bid;
+        auto& v = vis[bid];
+        for (int s = hseg_off[id]; s < hseg_off[id + 1]; ++s)
+            for (int p = hsegs[2 * s]; p <= hsegs[2 * s + 1]; p += sparsity * Y) v[p] = 1;
+        for (int s = vseg_off[id]; s < vseg_off[id + 1]; ++s)
+            for (int p = vsegs[2 * s]; p <= vsegs[2 * s + 1]; p += sparsity) v[p] = 1;
+        for (int q = point_off[id]; q < point_off[id + 1]; ++q) {
+            const int px = points[q] / Y, py = points[q] % Y;
+            for (int x = px - 1; x <= px + 1; ++x) {
+                if (x < 0 || x >= X) continue;
+                for (int y = py - 1; y < py + 1; ++y)  // y + 1 is not marked (reference :38)
+                    if (y >= 0 && y < Y && (x == px || y == py)) v[size_t(x) * Y + y] = 1;
+            }
+        }
+    }
+    return static_cast<int32_t>(vis.size());
+}
+
+// congestion.cuh:8-58 and :114-136.
+void orc_ripup_classify(const orc_grid* g, const int32_t* demand_half, int32_t threshold,
+                        int32_t n_nets, const int64_t* route_off, const int32_t* routes,
+                        uint8_t* is_of) {
+    Grid G(g);
+    const int cells = G.L * G.X * G.Y, X = G.X, Y = G.Y;
+    std::vector<int> sum(cells, 0);
+    for (int i = 0; i < cells; ++i) {
+        const int l = i / (X * Y), x = i / Y % X, y = i % Y;
+        if ((!G.along_y(l) && x + 1 < X) || (G.along_y(l) && y + 1 < Y))
+            sum[i] = (g->capacity[i] + threshold <= static_cast<float>(demand_half[i]) * 0.5f) ? 1 : 0;
+    }
+    for (int l = 0; l < G.L; ++l) {  // prefix_scan.cuh:42-72 (integer scan, order-free)
+        const bool ay = G.along_y(l);
+        const int tracks = ay ? X : Y, len = ay ? Y : X, stride = ay ? 1 : Y;
+        for (int t = 0; t < tracks; ++t) {
+            const int base = ay ? G.idx(l, t, 0) : G.idx(l, 0, t);
+            int acc = 0;
+            for (int k = 0; k < len; ++k) {
+                const int v = sum[base + k * stride];
+                sum[base + k * stride] = acc;
+                acc += v;
+            }
+        }
+    }
+    for (int id = 0; id < n_nets; ++id) {
+        is_of[id] = 0;
+        const int32_t* r = routes + route_off[id];
+        int count = 0;
+        for (int i = 1; i < r[0]; i += 2) {
+            const int l = r[i] / X / Y, x0 = r[i] / Y % X, y0 = r[i] % Y;
+            const int x1 = r[i + 1] / Y % X, y1 = r[i + 1] % Y;
+            if (x0 != x1) count += sum[G.idx(l, std::max(x0, x1), y0)] - sum[G.idx(l, std::min(x0, x1), y0)];
+            if (y0 != y1) count += sum[G.idx(l, x0, std::max(y0, y1))] - sum[G.idx(l, x0, std::min(y0, y1))];
+            if (count > 10) { is_of[id] = 1; break; }
+        }
+    }
+}
+
+// congestion.cuh:60-112.
+void orc_congestion_view(const orc_grid* g, const int32_t* demand_half,
+                         uint8_t* congestion, float* xsum, float* ysum) {
+    Grid G(g);
+    const int X = G.X, Y = G.Y;
+    std::vector<float> worst(size_t(X) * Y);
+    for (int i = 0; i < X * Y; ++i) {
+        double w = 0.0;
+        for (int l = 0; l < G.L; ++l) {
+            const int e = l * X * Y + i;
+            w = std::max(w, static_cast<double>(static_cast<float>(demand_half[e]) * 0.5f - g->capacity[e]));
+        }
+        congestion[i] = w > 0.0;
+        worst[i] = static_cast<float>(w);
+    }
+    for (int x = 0; x < X; ++x)  // extract_congestionView_ysum: per x, scan over y
+        sklansky_track<float>(Y, [&](int k) { return worst[size_t(x) * Y + k]; },
+                              [&](int k, float v) { ysum[size_t(x) * Y + k] = v; });
+    for (int y = 0; y < Y; ++y)  // extract_congestionView_xsum: per y, scan over x
+        sklansky_track<float>(X, [&](int k) { return worst[size_t(k) * Y + y]; },
+                              [&](int k, float v) { xsum[size_t(k) * Y + y] = v; });
+}
+
+int orc_lshape_stage(const orc_grid* g, int32_t n_batches, const int32_t* batch_off,
+                     const int32_t* ids, const int32_t* node_off, const int32_t* nodes,
+                     const int32_t* parents, const int64_t* route_off, int32_t* routes,
+                     int32_t* demand_half, int32_t* timestamp, int32_t* stamp,
+                     double* total_wirelength, int64_t* total_vias, int32_t nthreads) {
+#ifdef _OPENMP
+    if (nthreads > 0) omp_set_num_threads(nthreads);
+#endif
+    Grid G(g);
+    const size_t cells = size_t(g->L) * g->X * g->Y;
+    std::vector<float> wcost(cells), vcost(cells);
+    std::vector<double> presum(cells);
+    std::vector<int> touched;
+    std::vector<uint8_t> wire_dirty(cells, 0), via_dirty(cells, 0);
+    int status = 0;
+    for (int b = 0; b < n_batches; ++b) {
+        const int32_t s = ++*stamp;  // lshape.cuh:161
+        // refresh_cost (incremental_update.cuh:98-132): the first refresh is
+        // full; later ones recompute the cells the previous commit changed and
+        // rescan their tracks (values identical to a full recompute).
+        if (b == 0) {
+            orc_cost_full(g, demand_half, wcost.data(), vcost.data());
+            orc_presum(g, wcost.data(), presum.data());
+        } else {
+            std::vector<int> wlist, vlist;
+            std::vector<int> tracks;
+            for (int c : touched) {
+                const int l = c / (G.X * G.Y), x = c / G.Y % G.X, y = c % G.Y;
+                const bool ay = G.along_y(l);
+                const int pos = ay ? y : x, len = ay ? G.Y : G.X, stride = ay ? 1 : G.Y;
+                if (!wire_dirty[c]) { wire_dirty[c] = 1; wlist.push_back(c); }
+                if (!via_dirty[c]) { via_dirty[c] = 1; vlist.push_back(c); }
+                if (pos + 1 < len && !via_dirty[c + stride]) { via_dirty[c + stride] = 1; vlist.push_back(c + stride); }
+            }
+#pragma omp parallel for schedule(static)
+            for (size_t k = 0; k < wlist.size(); ++k) {
+                const int c = wlist[k];
+                wcost[c] = wire_cost(G, demand_half, c / (G.X * G.Y), c / G.Y % G.X, c % G.Y);
+            }
+#pragma omp parallel for schedule(static)
+            for (size_t k = 0; k < vlist.size(); ++k) {
+                const int c = vlist[k];
+                vcost[c] = via_cost(G, demand_half, c / (G.X * G.Y), c / G.Y % G.X, c % G.Y);
+            }
+            for (int c : wlist) {
+                const int l = c / (G.X * G.Y), x = c / G.Y % G.X, y = c % G.Y;
+                tracks.push_back(G.along_y(l) ? G.idx(l, x, 0) : G.idx(l, 0, y));
+                wire_dirty[c] = 0;
+            }
+            for (int c : vlist) via_dirty[c] = 0;
+            std::sort(tracks.begin(), tracks.end());
+            tracks.erase(std::unique(tracks.begin(), tracks.end()), tracks.end());
+#pragma omp parallel for schedule(dynamic, 4)
+            for (size_t k = 0; k < tracks.size(); ++k) {
+                const int base = tracks[k], l = base / (G.X * G.Y);
+                const bool ay = G.along_y(l);
+                const int len = ay ? G.Y : G.X, stride = ay ? 1 : G.Y;
+                sklansky_track<double>(len,
+                    [&](int q) { return static_cast<double>(wcost[base + q * stride]); },
+                    [&](int q, double v) { presum[base + q * stride] = v; });
+            }
+        }
+        touched.clear();
+        const int n = batch_off[b + 1] - batch_off[b];
+        const int rc = orc_lshape_batch(g, vcost.data(), presum.data(), n, ids + batch_off[b],
+                                        node_off, nodes, parents, route_off, routes);
+        if (rc && !status) status = rc;
+        commit_impl(g, n, ids + batch_off[b], route_off, routes, s, 1, demand_half,
+                    timestamp, total_wirelength, total_vias, &touched);
+    }
+    return status;
+}
+
+}  // extern "C"

@@ -1,0 +1,97 @@
+/*
+ * grb_oracle.h -- CPU restatement of GRotor's routing hot path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This library is the checker for the CUDA path in
+ * grotor_b200/: only tests/, __graft_entry__.smoke() and the cpu_baseline /
+ * --impl reference leg of bench.py may load it.  The product never links it and
+ * has no CPU fallback.
+ *
+ * Every function restates the reference's algorithm from its source (file:line
+ * cited at each definition, paths relative to the GRotor project root).  Cost
+ * values use the host's expf where the reference uses CUDA's __expf, so costs
+ * agree with the GPU within 1e-6 relative; every other step (prefix addition
+ * order, DP comparisons, tie-breaks, demand, batching) is exact.  Parity of the
+ * restatement is pinned against outputs of the reference itself (see
+ * tests/golden/ and oracle/ref_harness.cu).
+ *
+ * Grid layout: IDX(l,x,y) = (l*X + x)*Y + y; layer l carries wires along y when
+ * ((l & 1) ^ DIR) is 1, along x otherwise (router_state.hpp:267,
+ * full_update.cuh:43).  Demand is kept in int32 half-units (a wire edge adds 2,
+ * a split via landing adds 1), which is exact and converts to the reference's
+ * float demand bit-for-bit (demand = half * 0.5f).
+ */
+#ifndef GRB_ORACLE_H
+#define GRB_ORACLE_H
+#include <stdint.h>
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct orc_grid {
+    int32_t L, X, Y, DIR;
+    double unit_wire, unit_via, of_cost_scale;
+    const double* short_costs;   /* [L] overflow weight per routing layer */
+    const int32_t* x_edge_len;   /* [X-1] */
+    const int32_t* y_edge_len;   /* [Y-1] */
+    const float* capacity;       /* [L*X*Y] */
+} orc_grid;
+
+/* Full cost recompute: wcost/vcost from capacity and demand. */
+void orc_cost_full(const orc_grid* g, const int32_t* demand_half, float* wcost, float* vcost);
+
+/* Per-track double prefix of wcost in the reference's addition order. */
+void orc_presum(const orc_grid* g, const float* wcost, double* presum);
+
+/* Same prefix computed by the literal log-step (Sklansky) loop of the full scan;
+ * used by the tests to prove orc_presum's single-pass form adds in the same order. */
+void orc_presum_logstep(const orc_grid* g, const float* wcost, double* presum);
+
+/* L-shape tree DP for the nets of one batch (thread-per-net semantics).
+ * node_off is the CSR over all nets of the plan (global); nets are ids[0..n).
+ * Writes routes[route_off[id] ...] = [count, a0, b0, a1, b1, ...].
+ * Returns 0, or -1-i if net i's output would exceed its route capacity. */
+int orc_lshape_batch(const orc_grid* g, const float* vcost, const double* presum,
+                     int32_t n, const int32_t* ids, const int32_t* node_off,
+                     const int32_t* nodes, const int32_t* parents,
+                     const int64_t* route_off, int32_t* routes);
+
+/* Wire then via demand commit of one batch (K = +1 commit, -1 rip-up). */
+void orc_commit_batch(const orc_grid* g, int32_t n, const int32_t* ids,
+                      const int64_t* route_off, const int32_t* routes,
+                      int32_t stamp, int32_t K, int32_t* demand_half, int32_t* timestamp,
+                      double* total_wirelength, int64_t* total_vias);
+
+/* Exact greedy first-fit batching.  order[0..n) are net ids; geometry CSRs are
+ * indexed by net id.  Writes batch_of[i] for order position i and returns the
+ * number of batches. */
+int32_t orc_batches(int32_t X, int32_t Y, int32_t n, const int32_t* order,
+                    const int32_t* point_off, const int32_t* points,
+                    const int32_t* hseg_off, const int32_t* hsegs,
+                    const int32_t* vseg_off, const int32_t* vsegs,
+                    int32_t limit, int32_t sparsity, int32_t* batch_of);
+
+/* Rip-up classification: is_of[id] = route of net crosses > 10 overflowed edges
+ * (demand >= capacity + threshold). routes_of_net: route_off per net id. */
+void orc_ripup_classify(const orc_grid* g, const int32_t* demand_half, int32_t threshold,
+                        int32_t n_nets, const int64_t* route_off, const int32_t* routes,
+                        uint8_t* is_of);
+
+/* Congestion view: worst (demand - capacity) over layers per (x,y), flag and
+ * row/column float prefix sums. */
+void orc_congestion_view(const orc_grid* g, const int32_t* demand_half,
+                         uint8_t* congestion, float* xsum, float* ysum);
+
+/* Whole L-shape stage over an explicit batch plan: for each batch, ++stamp,
+ * full cost refresh, DP, commit.  ids/batch_off describe the plan in execution
+ * order.  nthreads > 1 solves the nets of a batch on that many host threads
+ * (results are independent of the thread count). */
+int orc_lshape_stage(const orc_grid* g, int32_t n_batches, const int32_t* batch_off,
+                     const int32_t* ids, const int32_t* node_off, const int32_t* nodes,
+                     const int32_t* parents, const int64_t* route_off, int32_t* routes,
+                     int32_t* demand_half, int32_t* timestamp, int32_t* stamp,
+                     double* total_wirelength, int64_t* total_vias, int32_t nthreads);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,189 @@
+"""ctypes bindings of liboracle.so (CPU restatement; test infrastructure only)."""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = os.path.join(_HERE, "liboracle.so")
+
+__all__ = [
+    "build", "load", "OrcGrid", "cost_full", "presum", "presum_logstep", "lshape_batch",
+    "commit_batch", "batches", "ripup_classify", "congestion_view", "lshape_stage",
+]
+
+
+def build() -> None:
+    """Compile liboracle.so in place (g++, no GPU needed)."""
+    subprocess.run(["make", "-s", "-C", _HERE, "liboracle.so"], check=True)
+
+
+_lib = None
+
+
+def load():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB):
+            build()
+        _lib = C.CDLL(_LIB)
+        _declare(_lib)
+    return _lib
+
+
+class _COrcGrid(C.Structure):
+    _fields_ = [
+        ("L", C.c_int32), ("X", C.c_int32), ("Y", C.c_int32), ("DIR", C.c_int32),
+        ("unit_wire", C.c_double), ("unit_via", C.c_double), ("of_cost_scale", C.c_double),
+        ("short_costs", C.c_void_p), ("x_edge_len", C.c_void_p), ("y_edge_len", C.c_void_p),
+        ("capacity", C.c_void_p),
+    ]
+
+
+P = C.c_void_p
+
+
+def _declare(lib):
+    lib.orc_cost_full.argtypes = [P, P, P, P]
+    lib.orc_presum.argtypes = [P, P, P]
+    lib.orc_presum_logstep.argtypes = [P, P, P]
+    lib.orc_lshape_batch.argtypes = [P, P, P, C.c_int32, P, P, P, P, P, P]
+    lib.orc_lshape_batch.restype = C.c_int
+    lib.orc_commit_batch.argtypes = [P, C.c_int32, P, P, P, C.c_int32, C.c_int32, P, P, P, P]
+    lib.orc_batches.argtypes = [C.c_int32, C.c_int32, C.c_int32, P, P, P, P, P, P, P, C.c_int32, C.c_int32, P]
+    lib.orc_batches.restype = C.c_int32
+    lib.orc_ripup_classify.argtypes = [P, P, C.c_int32, C.c_int32, P, P, P]
+    lib.orc_congestion_view.argtypes = [P, P, P, P, P]
+    lib.orc_lshape_stage.argtypes = [P, C.c_int32, P, P, P, P, P, P, P, P, P, P, P, P, C.c_int32]
+    lib.orc_lshape_stage.restype = C.c_int
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+def _c(a, dt):
+    return np.ascontiguousarray(a, dtype=dt)
+
+
+class OrcGrid:
+    """Grid arrays in the oracle's layout (keeps the numpy buffers alive)."""
+
+    def __init__(self, L, X, Y, DIR, unit_wire, unit_via, short_costs, x_edge_len, y_edge_len, capacity,
+                 of_cost_scale=1.0):
+        self.L, self.X, self.Y, self.DIR = int(L), int(X), int(Y), int(DIR)
+        self.short_costs = _c(short_costs, np.float64)
+        self.x_edge_len = _c(x_edge_len, np.int32)
+        self.y_edge_len = _c(y_edge_len, np.int32)
+        self.capacity = _c(capacity, np.float32).reshape(-1)
+        self.unit_wire, self.unit_via, self.of_cost_scale = float(unit_wire), float(unit_via), float(of_cost_scale)
+        self._s = _COrcGrid(self.L, self.X, self.Y, self.DIR, self.unit_wire, self.unit_via, self.of_cost_scale,
+                            _p(self.short_costs), _p(self.x_edge_len), _p(self.y_edge_len), _p(self.capacity))
+
+    @property
+    def cells(self):
+        return self.L * self.X * self.Y
+
+    @property
+    def ref(self):
+        return C.byref(self._s)
+
+
+def cost_full(g: OrcGrid, demand_half):
+    lib = load()
+    d = _c(demand_half, np.int32)
+    w = np.empty(g.cells, np.float32)
+    v = np.empty(g.cells, np.float32)
+    lib.orc_cost_full(g.ref, _p(d), _p(w), _p(v))
+    return w, v
+
+
+def presum(g: OrcGrid, wcost):
+    lib = load()
+    w = _c(wcost, np.float32)
+    out = np.empty(g.cells, np.float64)
+    lib.orc_presum(g.ref, _p(w), _p(out))
+    return out
+
+
+def presum_logstep(g: OrcGrid, wcost):
+    lib = load()
+    w = _c(wcost, np.float32)
+    out = np.empty(g.cells, np.float64)
+    lib.orc_presum_logstep(g.ref, _p(w), _p(out))
+    return out
+
+
+def lshape_batch(g: OrcGrid, vcost, presum_, ids, node_off, nodes, parents, route_off, routes):
+    """Route nets `ids` into `routes` (modified in place); returns status."""
+    lib = load()
+    ids = _c(ids, np.int32)
+    return lib.orc_lshape_batch(g.ref, _p(_c(vcost, np.float32)), _p(_c(presum_, np.float64)), len(ids), _p(ids),
+                                _p(_c(node_off, np.int32)), _p(_c(nodes, np.int32)), _p(_c(parents, np.int32)),
+                                _p(_c(route_off, np.int64)), _p(routes))
+
+
+def commit_batch(g: OrcGrid, ids, route_off, routes, stamp, K, demand_half, timestamp, stats=None):
+    """Wire then via commit; demand_half/timestamp are int32 arrays modified in place.
+    stats: optional dict with 'wirelength' and 'vias' accumulated in place."""
+    lib = load()
+    ids = _c(ids, np.int32)
+    wl = C.c_double(stats["wirelength"] if stats else 0.0)
+    vi = C.c_int64(stats["vias"] if stats else 0)
+    lib.orc_commit_batch(g.ref, len(ids), _p(ids), _p(_c(route_off, np.int64)), _p(_c(routes, np.int32)),
+                         int(stamp), int(K), _p(demand_half), _p(timestamp), C.byref(wl), C.byref(vi))
+    if stats is not None:
+        stats["wirelength"], stats["vias"] = wl.value, vi.value
+
+
+def batches(X, Y, order, point_off, points, hseg_off, hsegs, vseg_off, vsegs, limit, sparsity=1):
+    lib = load()
+    order = _c(order, np.int32)
+    out = np.empty(len(order), np.int32)
+    nb = lib.orc_batches(int(X), int(Y), len(order), _p(order), _p(_c(point_off, np.int32)), _p(_c(points, np.int32)),
+                         _p(_c(hseg_off, np.int32)), _p(_c(hsegs, np.int32)), _p(_c(vseg_off, np.int32)),
+                         _p(_c(vsegs, np.int32)), int(limit), int(sparsity), _p(out))
+    return out, int(nb)
+
+
+def ripup_classify(g: OrcGrid, demand_half, threshold, route_off, routes):
+    lib = load()
+    n = len(route_off) - 1
+    out = np.zeros(n, np.uint8)
+    lib.orc_ripup_classify(g.ref, _p(_c(demand_half, np.int32)), int(threshold), n, _p(_c(route_off, np.int64)),
+                           _p(_c(routes, np.int32)), _p(out))
+    return out
+
+
+def congestion_view(g: OrcGrid, demand_half):
+    lib = load()
+    xy = g.X * g.Y
+    cong = np.empty(xy, np.uint8)
+    xs = np.empty(xy, np.float32)
+    ys = np.empty(xy, np.float32)
+    lib.orc_congestion_view(g.ref, _p(_c(demand_half, np.int32)), _p(cong), _p(xs), _p(ys))
+    return cong, xs, ys
+
+
+def lshape_stage(g: OrcGrid, ids, batch_off, node_off, nodes, parents, route_off, threads=0,
+                 demand_half=None, timestamp=None, stamp=0):
+    """Full L-shape stage on the CPU; returns dict with routes, demand, timestamps, stats."""
+    lib = load()
+    ids = _c(ids, np.int32)
+    batch_off = _c(batch_off, np.int32)
+    route_off = _c(route_off, np.int64)
+    routes = np.zeros(int(route_off[-1]), np.int32)
+    demand = np.zeros(g.cells, np.int32) if demand_half is None else _c(demand_half, np.int32).copy()
+    ts = np.zeros(g.cells, np.int32) if timestamp is None else _c(timestamp, np.int32).copy()
+    st = C.c_int32(stamp)
+    wl = C.c_double(0)
+    vi = C.c_int64(0)
+    rc = lib.orc_lshape_stage(g.ref, len(batch_off) - 1, _p(batch_off), _p(ids), _p(_c(node_off, np.int32)),
+                              _p(_c(nodes, np.int32)), _p(_c(parents, np.int32)), _p(route_off), _p(routes),
+                              _p(demand), _p(ts), C.byref(st), C.byref(wl), C.byref(vi), int(threads))
+    return {"status": rc, "routes": routes, "demand_half": demand, "timestamp": ts, "stamp": st.value,
+            "wirelength": wl.value, "vias": vi.value}
+

@@ -1,0 +1,28 @@
+# Builds the reference router's own code, from its sources where they lie,
+# into oracle/_ref/ (git-ignored; travels to the GPU box with the snapshot):
+#   ref_harness  -- oracle/ref_harness.cu compiled against the reference headers
+#   evaluator    -- the reference's scoring program (resources/evaluator.cpp)
+#   POWV9.dat, POST9.dat -- FLUTE lookup tables the reference reads at run time
+# Usage: make -C oracle -f ref.mk [REF=/path/to/GRotor]
+REF ?= /root/reference
+NVCC ?= nvcc
+HOSTCXX ?= /usr/bin/g++
+OUT := _ref
+
+all: $(OUT)/ref_harness $(OUT)/evaluator $(OUT)/POWV9.dat $(OUT)/POST9.dat
+
+$(OUT):
+	mkdir -p $(OUT)
+
+$(OUT)/ref_harness: ref_harness.cu | $(OUT)
+	$(NVCC) -ccbin $(HOSTCXX) -std=c++17 -O3 -UNDEBUG -gencode arch=compute_100a,code=sm_100a \
+	  -Xcompiler -fopenmp -I$(REF)/include -I$(REF)/src -I$(REF)/third_party \
+	  -DG_ROTOR_RESOURCE_DIR=\"$(OUT)\" -x cu ref_harness.cu -o $@
+
+$(OUT)/evaluator: $(REF)/resources/evaluator.cpp | $(OUT)
+	$(HOSTCXX) -O3 -UNDEBUG -std=c++17 $< -o $@
+
+$(OUT)/%.dat: $(REF)/resources/flute/%.dat | $(OUT)
+	cp $< $@
+
+.PHONY: all

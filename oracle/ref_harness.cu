@@ -1,0 +1,337 @@
+// ref_harness.cu -- drives the reference router's own code on a CAP/NET design
+// and dumps its intermediate and final results for the parity tests.
+//
+// TEST INFRASTRUCTURE ONLY.  Built by oracle/ref.mk from the reference sources
+// where they lie (include path only, nothing copied); the binary lands in
+// oracle/_ref/.  Modes:
+//   topo  <cap> <net> <dir> <lut>   CPU: subnets, FLUTE trees (DFS order as in
+//                                   Lshape_route), batching geometry, HPWL order,
+//                                   CPU first-fit batches, grid tables.
+//   route <cap> <net> <dir> <lut> <out>
+//                                   GPU: the reference L-shape stage
+//                                   (build_cuda_database, Lshape_route), routes,
+//                                   demand, statistics, refreshed cost tables and
+//                                   the .out file written by the reference writer.
+//   snap  <cap> <net> <dir> <lut> <k>
+//                                   GPU: reference per-batch kernels over the dumped
+//                                   plan; cost tables before batch k, routes after.
+//   batch <dir> <limit> <sparsity>  CPU: time generate_batches_rsmt on a dumped
+//                                   geometry (X, Y, order, points, segments).
+//   write <cap> <net> <dir> <lut> <routes> <out>
+//                                   CPU: write a .out with the reference writer from
+//                                   route words produced elsewhere.
+// Every array is written as raw little-endian data, <dir>/<name>.<i32|i64|f32|f64>.
+#include "pipeline.hpp"
+
+#include <filesystem>
+#include <fstream>
+#include <numeric>
+
+namespace {
+
+template <class T>
+void dump(const std::string& dir, const std::string& name, const T* data, size_t count) {
+    const char* ext = std::is_same_v<T, int> ? ".i32" : std::is_same_v<T, long long> ? ".i64"
+                    : std::is_same_v<T, float> ? ".f32" : ".f64";
+    std::ofstream f(dir + "/" + name + ext, std::ios::binary);
+    f.write(reinterpret_cast<const char*>(data), sizeof(T) * count);
+}
+template <class T>
+void dump(const std::string& dir, const std::string& name, const std::vector<T>& v) { dump(dir, name, v.data(), v.size()); }
+
+template <class T>
+std::vector<T> load(const std::string& path) {
+    std::ifstream f(path, std::ios::binary | std::ios::ate);
+    if (!f) throw std::runtime_error("cannot read " + path);
+    const size_t bytes = f.tellg();
+    f.seekg(0);
+    std::vector<T> v(bytes / sizeof(T));
+    f.read(reinterpret_cast<char*>(v.data()), bytes);
+    return v;
+}
+
+void read_design(const std::string& cap, const std::string& net, const std::string& lut) {
+    std::string c = cap, n = net;
+    db::read(c.data(), n.data());
+    const auto cwd = std::filesystem::current_path();
+    std::filesystem::current_path(lut);
+    flute::readLUT();
+    std::filesystem::current_path(cwd);
+}
+
+void dump_grid(const std::string& dir, cudb::RouterState& state) {
+    const int L = state.device.L, X = state.device.X, Y = state.device.Y;
+    std::vector<int> meta{L, X, Y, state.device.DIR};
+    dump(dir, "meta", meta);
+    std::vector<double> sc(L), units{db::unit_length_wire_cost, db::unit_via_cost};
+    for (int l = 0; l < L; ++l) sc[l] = db::unit_length_short_costs[l + 1];
+    dump(dir, "short_costs", sc);
+    dump(dir, "unit_costs", units);
+    dump(dir, "x_edge_len", db::x_edge_len);
+    dump(dir, "y_edge_len", db::y_edge_len);
+    std::vector<float> cap(size_t(L) * X * Y);
+    for (int l = 0; l < L; ++l)
+        for (int x = 0; x < X; ++x)
+            for (int y = 0; y < Y; ++y) cap[(size_t(l) * X + x) * Y + y] = float(db::capacity[l + 1][x][y]);
+    dump(dir, "capacity", cap);
+}
+
+int run_topo(const std::string& cap, const std::string& net, const std::string& dir, const std::string& lut) {
+    read_design(cap, net, lut);
+    cudb::RouterState state;
+    state.batch_sparsity_override = 1;
+    cudb::prepare_routing_nets(state);
+    auto& nets = state.nets;
+    const int n = nets.size();
+    std::vector<int> all(n);
+    std::iota(all.begin(), all.end(), 0);
+#pragma omp parallel for num_threads(8)
+    for (int i = 0; i < n; ++i) nets[i].construct_rsmt(state, false);  // lshape.cuh:33-36
+    std::vector<int> order = all;
+    std::sort(order.begin(), order.end(), [&](int l, int r) { return nets[l].hpwl > nets[r].hpwl; });  // lshape.cuh:53-55
+    std::vector<int> sorted = order;
+    auto batches = cudb::generate_batches_rsmt(state, sorted, 1000000, 1);
+    std::vector<int> batch_of(n, -1), pos(n);
+    for (int i = 0; i < n; ++i) pos[order[i]] = i;
+    for (size_t b = 0; b < batches.size(); ++b)
+        for (int id : batches[b]) batch_of[pos[id]] = int(b);
+    std::reverse(batches.begin(), batches.end());  // lshape.cuh:70
+    std::vector<int> ids, batch_off{0};
+    for (auto& b : batches) { ids.insert(ids.end(), b.begin(), b.end()); batch_off.push_back(ids.size()); }
+    // Per-net DFS flattening exactly as lshape.cuh:85-103.
+    std::vector<int> node_off{0}, nodes, parents, point_off{0}, points, hseg_off{0}, hsegs, vseg_off{0}, vsegs;
+    std::vector<int> hpwl(n), original(n), pin_count(n);
+    for (int id = 0; id < n; ++id) {
+        auto& graph = nets[id].rsmt;
+        const size_t base = nodes.size();
+        nodes.resize(base + graph.back().size());
+        parents.resize(base + graph.back().size());
+        int cnt = 0;
+        std::function<void(int, int, int)> dfs = [&](int x, int par, int par_node) {
+            const int idx = cnt++;
+            nodes[base + idx] = graph.back()[x];
+            parents[base + idx] = par_node;
+            for (int e : graph[x]) if (e != par) dfs(e, x, idx);
+        };
+        dfs(0, -1, -1);
+        node_off.push_back(nodes.size());
+        for (int p : nets[id].points) points.push_back(p);
+        point_off.push_back(points.size());
+        for (auto& s : nets[id].rsmt_h_segments) { hsegs.push_back(s.first); hsegs.push_back(s.second); }
+        hseg_off.push_back(hsegs.size() / 2);
+        for (auto& s : nets[id].rsmt_v_segments) { vsegs.push_back(s.first); vsegs.push_back(s.second); }
+        vseg_off.push_back(vsegs.size() / 2);
+        hpwl[id] = nets[id].hpwl;
+        original[id] = nets[id].original_net_id;
+        pin_count[id] = nets[id].pins.size();
+    }
+    dump_grid(dir, state);
+    dump(dir, "pin_acc_num", state.pin_cnt_sum_cpu);
+    dump(dir, "node_off", node_off); dump(dir, "nodes", nodes); dump(dir, "parents", parents);
+    dump(dir, "point_off", point_off); dump(dir, "points", points);
+    dump(dir, "hseg_off", hseg_off); dump(dir, "hsegs", hsegs);
+    dump(dir, "vseg_off", vseg_off); dump(dir, "vsegs", vsegs);
+    dump(dir, "hpwl", hpwl); dump(dir, "original", original); dump(dir, "pin_count", pin_count);
+    dump(dir, "order", order); dump(dir, "batch_of", batch_of);
+    dump(dir, "ids", ids); dump(dir, "batch_off", batch_off);
+    printf("REF_TOPO nets=%d batches=%zu nodes=%zu\n", n, batches.size(), nodes.size());
+    return 0;
+}
+
+int run_route(const std::string& cap, const std::string& net, const std::string& dir, const std::string& lut,
+              const std::string& out) {
+    read_design(cap, net, lut);
+    out_file = fopen(out.c_str(), "w");
+    if (!out_file) throw std::runtime_error("cannot open " + out);
+    setvbuf(out_file, nullptr, _IONBF, 0);
+    std::vector<int> ids, words;
+    {
+        cudb::RouterState state;
+        state.batch_sparsity_override = 1;
+        state.report_score = false;
+        // pipeline.hpp:247-276, stage one only.
+        cudb::build_cuda_database(state);
+        graph::initialize_incremental_cost(state);
+        auto& view = state.device;
+        for (int i = 0; i < int(db::nets.size()); ++i)
+            if (db::nets[i].pins.size() == 1) nets2output.push(i);
+        grotor::cuda_check(cudaFuncSetAttribute(graph::compute_presum,
+                   cudaFuncAttributeMaxDynamicSharedMemorySize, sizeof(double) * view.XY), "prefix shared memory");
+        std::vector<int> all(state.nets.size());
+        std::iota(all.begin(), all.end(), 0);
+        Lshape_route::Lshape_route(state, all);
+        grotor::cuda_check(cudaDeviceSynchronize(), "L-shape stage");
+        state.download_routes(false);
+        const size_t cells = size_t(view.L) * view.X * view.Y;
+        std::vector<float> demand(cells), wcost(cells), vcost(cells);
+        std::vector<double> presum(cells);
+        cudaMemcpy(demand.data(), view.demand, cells * 4, cudaMemcpyDeviceToHost);
+        cudb::RoutingStatistics stats;
+        cudaMemcpy(&stats, view.statistics, sizeof(stats), cudaMemcpyDeviceToHost);
+        graph::refresh_cost(state);  // costs of the final demand
+        grotor::cuda_check(cudaDeviceSynchronize(), "final refresh");
+        cudaMemcpy(wcost.data(), view.wcost, cells * 4, cudaMemcpyDeviceToHost);
+        cudaMemcpy(vcost.data(), view.vcost, cells * 4, cudaMemcpyDeviceToHost);
+        cudaMemcpy(presum.data(), view.presum, cells * 8, cudaMemcpyDeviceToHost);
+        const size_t count = view.ROUTE_PER_PIN * view.PIN_NUM + 1;
+        dump(dir, "ref_routes", state.routes_cpu.get(), count);
+        dump(dir, "ref_demand", demand); dump(dir, "ref_wcost", wcost); dump(dir, "ref_vcost", vcost);
+        dump(dir, "ref_presum", presum);
+        std::vector<double> st{stats.total_wirelength, double(stats.total_via_count)};
+        dump(dir, "ref_stats", st);
+        graph::finish_nets(state, all);  // pipeline.hpp:283-291
+        auto records = graph::collect_output_nets(std::move(nets2output));
+        nets2output = {};
+        graph::output_nets(state, std::move(records));
+        state.release_workspaces();
+    }
+    fclose(out_file);
+    out_file = nullptr;
+    printf("REF_ROUTE done\n");
+    return 0;
+}
+
+// GPU: the reference's per-batch kernels (graph::refresh_cost,
+// Lshape_route_warp, graph::commit_batch_demand) driven in the order of
+// lshape.cuh:153-179 over the dumped plan; before batch `snap` the cost tables
+// are saved, after it the batch's routes.  Lets the CPU tests feed the
+// reference's own tables to the oracle's DP.
+int run_snap(const std::string& cap, const std::string& net, const std::string& dir, const std::string& lut,
+             int snap) {
+    read_design(cap, net, lut);
+    cudb::RouterState state;
+    state.batch_sparsity_override = 1;
+    cudb::build_cuda_database(state);
+    graph::initialize_incremental_cost(state);
+    auto& view = state.device;
+    const auto ids = load<int>(dir + "/ids.i32"), batch_off = load<int>(dir + "/batch_off.i32");
+    const auto node_off_id = load<int>(dir + "/node_off.i32"), nodes_id = load<int>(dir + "/nodes.i32");
+    const auto parents_id = load<int>(dir + "/parents.i32");
+    const int n = ids.size(), nb = batch_off.size() - 1, L = view.L;
+    if (snap < 0) snap += nb;
+    // Flatten per execution position (lshape.cuh:80-103 layout).
+    std::vector<int> node_cnt_sum{0}, nodes, par_nodes;
+    for (int id : ids) {
+        for (int k = node_off_id[id]; k < node_off_id[id + 1]; ++k) {
+            nodes.push_back(nodes_id[k]);
+            par_nodes.push_back(parents_id[k]);
+        }
+        node_cnt_sum.push_back(nodes.size());
+    }
+    int max_nodes = 0;
+    for (int b = 0; b < nb; ++b) max_nodes = std::max(max_nodes, node_cnt_sum[batch_off[b + 1]] - node_cnt_sum[batch_off[b]]);
+    int *d_ncs, *d_nodes, *d_par, *d_from, *d_range;
+    double* d_dist;
+    cudaMalloc(&d_ncs, node_cnt_sum.size() * 4); cudaMalloc(&d_nodes, nodes.size() * 4);
+    cudaMalloc(&d_par, nodes.size() * 4); cudaMalloc(&d_range, nodes.size() * 4);
+    cudaMalloc(&d_dist, size_t(max_nodes) * L * L * 8); cudaMalloc(&d_from, size_t(max_nodes) * L * L * 4);
+    cudaMemcpy(d_ncs, node_cnt_sum.data(), node_cnt_sum.size() * 4, cudaMemcpyHostToDevice);
+    cudaMemcpy(d_nodes, nodes.data(), nodes.size() * 4, cudaMemcpyHostToDevice);
+    cudaMemcpy(d_par, par_nodes.data(), nodes.size() * 4, cudaMemcpyHostToDevice);
+    cudaMemcpy(view.net_ids, ids.data(), n * 4, cudaMemcpyHostToDevice);
+    grotor::cuda_check(cudaFuncSetAttribute(graph::compute_presum,
+               cudaFuncAttributeMaxDynamicSharedMemorySize, sizeof(double) * view.XY), "prefix shared memory");
+    auto routing_view = state.device;
+    routing_view.pre_demand = nullptr;
+    const size_t cells = size_t(L) * view.X * view.Y;
+    for (int b = 0; b <= snap; ++b) {
+        ++state.global_timestamp;
+        graph::refresh_cost(state);
+        if (b == snap) {
+            grotor::cuda_check(cudaDeviceSynchronize(), "snapshot");
+            std::vector<float> wcost(cells), vcost(cells), demand(cells);
+            std::vector<double> presum(cells);
+            cudaMemcpy(wcost.data(), view.wcost, cells * 4, cudaMemcpyDeviceToHost);
+            cudaMemcpy(vcost.data(), view.vcost, cells * 4, cudaMemcpyDeviceToHost);
+            cudaMemcpy(presum.data(), view.presum, cells * 8, cudaMemcpyDeviceToHost);
+            cudaMemcpy(demand.data(), view.demand, cells * 4, cudaMemcpyDeviceToHost);
+            dump(dir, "snap_wcost", wcost); dump(dir, "snap_vcost", vcost);
+            dump(dir, "snap_presum", presum); dump(dir, "snap_demand", demand);
+        }
+        const int cnt = batch_off[b + 1] - batch_off[b];
+        Lshape_route::Lshape_route_warp<<<(cnt + 3) / 4, 128>>>(routing_view, cnt, batch_off[b], d_ncs, d_nodes, d_par,
+                                                               d_dist, d_from, d_range, state.global_timestamp);
+        graph::commit_batch_demand(state.device, cnt, batch_off[b], state.global_timestamp);
+    }
+    grotor::cuda_check(cudaDeviceSynchronize(), "snap stage");
+    state.download_routes(false);
+    dump(dir, "snap_routes", state.routes_cpu.get(), view.ROUTE_PER_PIN * view.PIN_NUM + 1);
+    std::vector<int> meta{snap};
+    dump(dir, "snap_batch", meta);
+    printf("REF_SNAP batch=%d of %d\n", snap, nb);
+    return 0;
+}
+
+int run_batch(const std::string& dir, int limit, int sparsity) {
+    const auto meta = load<int>(dir + "/meta.i32");
+    const auto order = load<int>(dir + "/order.i32");
+    const auto point_off = load<int>(dir + "/point_off.i32"), points = load<int>(dir + "/points.i32");
+    const auto hseg_off = load<int>(dir + "/hseg_off.i32"), hsegs = load<int>(dir + "/hsegs.i32");
+    const auto vseg_off = load<int>(dir + "/vseg_off.i32"), vsegs = load<int>(dir + "/vsegs.i32");
+    cudb::RouterState state;
+    state.device.X = meta[1];
+    state.device.Y = meta[2];
+    const int n = point_off.size() - 1;
+    state.nets.resize(n);
+    for (int i = 0; i < n; ++i) {
+        auto& net = state.nets[i];
+        net.points.assign(points.begin() + point_off[i], points.begin() + point_off[i + 1]);
+        for (int s = hseg_off[i]; s < hseg_off[i + 1]; ++s) net.rsmt_h_segments.emplace_back(hsegs[2 * s], hsegs[2 * s + 1]);
+        for (int s = vseg_off[i]; s < vseg_off[i + 1]; ++s) net.rsmt_v_segments.emplace_back(vsegs[2 * s], vsegs[2 * s + 1]);
+    }
+    std::vector<int> sorted = order;
+    const auto start = std::chrono::steady_clock::now();
+    auto batches = cudb::generate_batches_rsmt(state, sorted, limit, sparsity);
+    const double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - start).count();
+    std::vector<int> batch_of(order.size(), -1), pos(n, -1);
+    for (size_t i = 0; i < order.size(); ++i) pos[order[i]] = i;
+    for (size_t b = 0; b < batches.size(); ++b)
+        for (int id : batches[b]) batch_of[pos[id]] = int(b);
+    dump(dir, "ref_batch_of", batch_of);
+    printf("REF_BATCH nets=%zu batches=%zu elapsed_ms=%.6f\n", order.size(), batches.size(), ms);
+    return 0;
+}
+
+int run_write(const std::string& cap, const std::string& net, const std::string& dir, const std::string& lut,
+              const std::string& routes_path, const std::string& out) {
+    read_design(cap, net, lut);
+    cudb::RouterState state;
+    cudb::prepare_routing_nets(state);
+    const auto words = load<int>(routes_path);
+    state.routes_cpu.reset(new int[words.size()]);
+    std::copy(words.begin(), words.end(), state.routes_cpu.get());
+    for (int i = 0; i < int(db::nets.size()); ++i)
+        if (db::nets[i].pins.size() == 1) nets2output.push(i);
+    std::vector<int> all(state.nets.size());
+    std::iota(all.begin(), all.end(), 0);
+    out_file = fopen(out.c_str(), "w");
+    if (!out_file) throw std::runtime_error("cannot open " + out);
+    setvbuf(out_file, nullptr, _IONBF, 0);
+    graph::finish_nets(state, all);
+    auto records = graph::collect_output_nets(std::move(nets2output));
+    nets2output = {};
+    graph::output_nets(state, std::move(records));
+    fclose(out_file);
+    out_file = nullptr;
+    (void)dir;
+    return 0;
+}
+
+}  // namespace
+
+int main(int argc, char** argv) {
+    try {
+        program_start = std::chrono::high_resolution_clock::now();
+        const std::string mode = argc > 1 ? argv[1] : "";
+        if (mode == "topo" && argc == 6) return run_topo(argv[2], argv[3], argv[4], argv[5]);
+        if (mode == "route" && argc == 7) return run_route(argv[2], argv[3], argv[4], argv[5], argv[6]);
+        if (mode == "snap" && argc == 7) return run_snap(argv[2], argv[3], argv[4], argv[5], std::stoi(argv[6]));
+        if (mode == "batch" && argc == 5) return run_batch(argv[2], std::stoi(argv[3]), std::stoi(argv[4]));
+        if (mode == "write" && argc == 8) return run_write(argv[2], argv[3], argv[4], argv[5], argv[6], argv[7]);
+        fprintf(stderr, "usage: ref_harness topo|route|snap|batch|write ...\n");
+        return 2;
+    } catch (const std::exception& e) {
+        fprintf(stderr, "ref_harness error: %s\n", e.what());
+        return 1;
+    }
+}
