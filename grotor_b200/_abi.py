@@ -72,8 +72,11 @@ SIGNATURES = {
     "grb_read_tables": (C.c_int, [P, P, P, P, P, P]),
     "grb_read_routes": (C.c_int, [P, P]),
     "grb_get_stats": (C.c_int, [P, C.POINTER(GrbStats)]),
+    "grb_set_stats": (C.c_int, [P, C.c_double, C.c_int64]),
     "grb_sync": (C.c_int, [P]),
     "grb_kernel_launches": (C.c_int64, [P]),
+    "grb_set_profiling": (C.c_int, [P, C.c_int32]),
+    "grb_phase_times": (C.c_int, [P, P, C.c_int32, C.c_int32]),
     # grb_synth.h
     "grb_synth_generate": (P, [C.POINTER(GrbSynthParams)]),
     "grb_design_free": (None, [P]),

@@ -112,6 +112,7 @@ struct GridSync {
     unsigned* count;
     unsigned* generation;
     unsigned long long timeout_ns;
+    unsigned long long* phase_ns;  // optional per-phase time accumulators
 };
 
 __device__ __forceinline__ unsigned long long global_ns() {
@@ -149,5 +150,21 @@ __device__ __forceinline__ bool grid_sync(const GridSync& s, const Tables& T) {
     __syncthreads();
     return ok != 0;
 }
+
+// Per-phase timing of a cooperative kernel: block 0 / thread 0 adds the time
+// since its previous mark (a grid barrier has just completed) to slot k.
+struct PhaseClock {
+    unsigned long long last = 0;
+    __device__ __forceinline__ void start(const GridSync& s) {
+        if (s.phase_ns && blockIdx.x == 0 && threadIdx.x == 0) last = global_ns();
+    }
+    __device__ __forceinline__ void mark(const GridSync& s, int k) {
+        if (s.phase_ns && blockIdx.x == 0 && threadIdx.x == 0) {
+            const unsigned long long now = global_ns();
+            s.phase_ns[k] += now - last;
+            last = now;
+        }
+    }
+};
 
 }  // namespace grb

@@ -114,6 +114,8 @@ __global__ void __launch_bounds__(kPersistentThreads) k_lshape_persistent(Tables
     const int gwarp = blockIdx.x * (blockDim.x >> 5) + warp, nwarps = gridDim.x * (blockDim.x >> 5);
     double* stack = reinterpret_cast<double*>(smem);
     double* t3 = stack + 32 * 16;
+    PhaseClock clk;
+    clk.start(S);
     for (int b = 0; b < P.n_batches; ++b) {
         const int q = (parity0 + b) & 1, nq = q ^ 1;
         const int stamp = stamp0 + b + 1;
@@ -128,6 +130,7 @@ __global__ void __launch_bounds__(kPersistentThreads) k_lshape_persistent(Tables
         }
         for (int k = gwarp; k < nv; k += nwarps) refresh_via_word(T, T.via_list[q][k], lane);
         if (!grid_sync(S, T)) return;
+        clk.mark(S, 4);
         // Phase A: route every net of the batch and commit its wires.
         const int lo = P.batch_off[b], cnt = P.batch_off[b + 1] - lo;
         const Arena A = warp_arena(smem, arena_b, warp, T.L, nmax);
@@ -143,9 +146,11 @@ __global__ void __launch_bounds__(kPersistentThreads) k_lshape_persistent(Tables
             else if (lane == 0) set_error(T, kELimit, id);
         }
         if (!grid_sync(S, T)) return;
+        clk.mark(S, 5);
         // Phase B: via demand sees every wire timestamp of the batch.
         for (int k = gwarp; k < cnt; k += nwarps) commit_net_vias(T, P, P.ids[lo + k], stamp, 1, lane, nq);
         if (!grid_sync(S, T)) return;
+        clk.mark(S, 6);
     }
 }
 
@@ -176,17 +181,23 @@ __global__ void __launch_bounds__(kChunk) k_batch_persistent(BatchState B, GridS
     extern __shared__ __align__(16) unsigned bsm[];
     const int lane = threadIdx.x & 31, warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int warps = (gridDim.x * blockDim.x) >> 5;
+    PhaseClock clk;
+    clk.start(S);
     for (int s = 0; s < B.n; s += kChunk) {
         const int m = min(kChunk, B.n - s);
         for (int j = warp; j < m; j += warps) batch_phase1(B, s, j, lane);
         if (!grid_sync(S, T)) return;
+        clk.mark(S, 0);
         for (int j = warp; j < m; j += warps) batch_phase2(B, s, j, lane);
         if (!grid_sync(S, T)) return;
+        clk.mark(S, 1);
         if (blockIdx.x == 0) batch_phase3(B, s, bsm);
         if (!grid_sync(S, T)) return;
+        clk.mark(S, 2);
         if (*reinterpret_cast<volatile int*>(B.error)) return;
         for (int j = warp; j < m; j += warps) batch_phase4(B, s, j, lane);
         if (!grid_sync(S, T)) return;
+        clk.mark(S, 3);
     }
 }
 
@@ -332,6 +343,12 @@ struct grb_ctx {
     int64_t graph_kernels = 0;
     // timing
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    bool profiling = false;
+    unsigned long long* d_phase = nullptr;     // [8] persistent-kernel phase clocks
+    double phase_ms[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev_pool;
+    std::vector<int> ev_slot;                  // phase slot of each recorded pair
+    size_t ev_used = 0;
     double batching_ms = 0, dag_ms = 0;
 };
 
@@ -409,12 +426,54 @@ int ensure_gscratch(grb_ctx* c, int slots) {
     return GRB_OK;
 }
 
+// Plain-form profiling: an event pair around each launch group, resolved later.
+int prof_begin(grb_ctx* c, int slot, cudaEvent_t* end) {
+    *end = nullptr;
+    if (!c->profiling) return GRB_OK;
+    if (c->ev_used == c->ev_pool.size()) {
+        cudaEvent_t a, b;
+        GRB_CUDA(c, cudaEventCreate(&a));
+        GRB_CUDA(c, cudaEventCreate(&b));
+        c->ev_pool.push_back({a, b});
+        c->ev_slot.push_back(slot);
+    }
+    c->ev_slot[c->ev_used] = slot;
+    GRB_CUDA(c, cudaEventRecord(c->ev_pool[c->ev_used].first, c->stream));
+    *end = c->ev_pool[c->ev_used].second;
+    ++c->ev_used;
+    return GRB_OK;
+}
+void prof_end(grb_ctx* c, cudaEvent_t end) {
+    if (end) cudaEventRecord(end, c->stream);
+}
+int prof_collect(grb_ctx* c) {
+    if (!c->profiling) return GRB_OK;
+    GRB_CUDA(c, cudaStreamSynchronize(c->stream));
+    for (size_t k = 0; k < c->ev_used; ++k) {
+        float ms = 0;
+        GRB_CUDA(c, cudaEventElapsedTime(&ms, c->ev_pool[k].first, c->ev_pool[k].second));
+        c->phase_ms[c->ev_slot[k]] += ms;
+    }
+    c->ev_used = 0;
+    if (c->d_phase) {
+        unsigned long long ns[8];
+        GRB_CUDA(c, cudaMemcpy(ns, c->d_phase, sizeof(ns), cudaMemcpyDeviceToHost));
+        for (int k = 0; k < 8; ++k) c->phase_ms[k] += ns[k] * 1e-6;
+        GRB_CUDA(c, cudaMemset(c->d_phase, 0, sizeof(ns)));
+    }
+    return GRB_OK;
+}
+
 int refresh_plain(grb_ctx* c) {
     Tables& T = c->T;
+    cudaEvent_t e;
+    int rc = prof_begin(c, 4, &e);
+    if (rc) return rc;
     k_cost_cells<<<(T.cells + 255) / 256, 256, 0, c->stream>>>(T);
     k_prefix_groups<<<T.n_groups, kRefreshThreads, 0, c->stream>>>(T);
     const int n = std::max(c->words, std::max(T.n_groups, 2));
     k_clear_dirty<<<(n + 255) / 256, 256, 0, c->stream>>>(T, c->words);
+    prof_end(c, e);
     c->launches += 3;
     GRB_CUDA(c, cudaGetLastError());
     return GRB_OK;
@@ -430,8 +489,12 @@ int route_plain(grb_ctx* c, int b, int stamp) {
     const int rc = ensure_gscratch(c, blocks * wpb);
     if (rc) return rc;
     const size_t arena_slot = arena_bytes(c->T.L, std::max(c->max_nodes, 1));
+    cudaEvent_t e;
+    const int prc = prof_begin(c, 5, &e);
+    if (prc) return prc;
     k_lshape_batch<<<blocks, kDpThreads, ab * wpb, c->stream>>>(c->T, make_plan(c), b, stamp, nmax, ab,
                                                                  c->gscratch, arena_slot);
+    prof_end(c, e);
     c->launches += 1;
     GRB_CUDA(c, cudaGetLastError());
     return GRB_OK;
@@ -441,8 +504,12 @@ int commit_plain(grb_ctx* c, int b, int stamp, int K) {
     const int cnt = c->h_batch_off[b + 1] - c->h_batch_off[b];
     if (cnt <= 0) return GRB_OK;
     const int blocks = std::min((cnt + 3) / 4, 1056);  // demand.cuh:490
+    cudaEvent_t e;
+    const int prc = prof_begin(c, 6, &e);
+    if (prc) return prc;
     k_commit_wires<<<blocks, 128, 0, c->stream>>>(c->T, make_plan(c), b, stamp, K, c->parity);
     k_commit_vias<<<blocks, 128, 0, c->stream>>>(c->T, make_plan(c), b, stamp, K, c->parity);
+    prof_end(c, e);
     c->launches += 2;
     GRB_CUDA(c, cudaGetLastError());
     return GRB_OK;
@@ -469,10 +536,13 @@ int stage_graph(grb_ctx* c, int stamp0) {
         int rc = ensure_gscratch(c, ((maxcnt + wpb - 1) / wpb) * wpb);
         if (rc) return rc;
         const int64_t before = c->launches;
+        const bool prof = c->profiling;
+        c->profiling = false;
         cudaGraph_t g = nullptr;
         GRB_CUDA(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
         rc = stage_plain(c, stamp0);
         const cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+        c->profiling = prof;
         if (rc) { if (g) cudaGraphDestroy(g); return rc; }
         if (e != cudaSuccess) return cuda_fail(c, e, "cudaStreamEndCapture");
         const cudaError_t ei = cudaGraphInstantiate(&c->graph, g, 0);
@@ -513,7 +583,7 @@ int stage_persistent(grb_ctx* c, int stamp0) {
     GRB_CUDA(c, cudaMemsetAsync(c->sync, 0, 2 * sizeof(unsigned), c->stream));
     Tables T = c->T;
     Plan P = make_plan(c);
-    GridSync S{c->sync, c->sync + 1, kBarrierTimeoutNs};
+    GridSync S{c->sync, c->sync + 1, kBarrierTimeoutNs, c->profiling ? c->d_phase : nullptr};
     int parity = c->parity;
     char* gs = c->gscratch;
     void* args[] = {&T, &P, &S, &stamp0, &parity, (void*)&nmax, (void*)&ab, &gs, (void*)&slot, &c->work};
@@ -828,7 +898,7 @@ int grb_plan_batches(grb_ctx* c, const int32_t* order, int32_t n, int32_t limit,
             GRB_CUDA(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_persistent, kChunk, smem));
             if (per_sm < 1) return fail(c, GRB_EINVAL, "batching kernel does not fit on an SM");
             GRB_CUDA(c, cudaMemsetAsync(c->sync, 0, 2 * sizeof(unsigned), c->stream));
-            GridSync S{c->sync, c->sync + 1, kBarrierTimeoutNs};
+            GridSync S{c->sync, c->sync + 1, kBarrierTimeoutNs, c->profiling ? c->d_phase : nullptr};
             Tables T = c->T;
             void* args[] = {&B, &S, &T};
             GRB_CUDA(c, cudaLaunchCooperativeKernel((void*)k_batch_persistent, dim3(per_sm * c->sms), dim3(kChunk), args, smem, c->stream));
@@ -836,10 +906,19 @@ int grb_plan_batches(grb_ctx* c, const int32_t* order, int32_t n, int32_t limit,
         } else {
             const int grid = c->sms * 4;
             for (int s = 0; s < n; s += kChunk) {
+                cudaEvent_t e;
+                if ((rc = prof_begin(c, 0, &e))) return rc;
                 k_batch_phase1<<<grid, 256, 0, c->stream>>>(B, s);
+                prof_end(c, e);
+                if ((rc = prof_begin(c, 1, &e))) return rc;
                 k_batch_phase2<<<grid, 256, 0, c->stream>>>(B, s);
+                prof_end(c, e);
+                if ((rc = prof_begin(c, 2, &e))) return rc;
                 k_batch_phase3<<<1, kChunk, smem, c->stream>>>(B, s);
+                prof_end(c, e);
+                if ((rc = prof_begin(c, 3, &e))) return rc;
                 k_batch_phase4<<<grid, 256, 0, c->stream>>>(B, s);
+                prof_end(c, e);
                 c->launches += 4;
             }
             GRB_CUDA(c, cudaGetLastError());
@@ -858,8 +937,8 @@ int grb_plan_batches(grb_ctx* c, const int32_t* order, int32_t n, int32_t limit,
         int nb = 0;
         GRB_CUDA(c, cudaMemcpy(&nb, c->ncolors, 4, cudaMemcpyDeviceToHost));
         k_plan_offsets<<<1, 1, 0, c->stream>>>(B, c->batch_off);
-        k_plan_scatter<<<(n + 255) / 256, 256, 0, c->stream>>>(B, c->batch_off, c->ids);
-        c->launches += 2;
+        if (n) k_plan_scatter<<<(n + 255) / 256, 256, 0, c->stream>>>(B, c->batch_off, c->ids);
+        c->launches += n ? 2 : 1;
         GRB_CUDA(c, cudaGetLastError());
         GRB_CUDA(c, cudaEventRecord(c->ev1, c->stream));
         c->h_batch_off.assign(nb + 1, 0);
@@ -869,6 +948,7 @@ int grb_plan_batches(grb_ctx* c, const int32_t* order, int32_t n, int32_t limit,
         float ms = 0;
         GRB_CUDA(c, cudaEventElapsedTime(&ms, c->ev0, c->ev1));
         c->batching_ms = ms;
+        if ((rc = prof_collect(c))) return rc;
         c->plan_n = n;
         c->n_batches = nb;
         ++c->plan_version;
@@ -915,6 +995,7 @@ int grb_lshape_stage(grb_ctx* c, int32_t mode, grb_stats* stats) {
     float ms = 0;
     GRB_CUDA(c, cudaEventElapsedTime(&ms, c->ev0, c->ev1));
     c->dag_ms = ms;
+    if ((rc = prof_collect(c))) return rc;
     return stats ? grb_get_stats(c, stats) : GRB_OK;
 }
 
@@ -1005,6 +1086,16 @@ int grb_get_stats(grb_ctx* c, grb_stats* s) {
     return GRB_OK;
 }
 
+int grb_set_stats(grb_ctx* c, double wirelength, int64_t vias) {
+    if (!c) return GRB_EINVAL;
+    GRB_CUDA(c, cudaSetDevice(c->device));
+    const unsigned long long v = static_cast<unsigned long long>(vias);
+    GRB_CUDA(c, cudaMemcpyAsync(c->T.wirelength, &wirelength, sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    GRB_CUDA(c, cudaMemcpyAsync(c->T.vias, &v, sizeof(v), cudaMemcpyHostToDevice, c->stream));
+    GRB_CUDA(c, cudaStreamSynchronize(c->stream));
+    return GRB_OK;
+}
+
 int grb_sync(grb_ctx* c) {
     if (!c) return GRB_EINVAL;
     GRB_CUDA(c, cudaSetDevice(c->device));
@@ -1013,5 +1104,26 @@ int grb_sync(grb_ctx* c) {
 }
 
 int64_t grb_kernel_launches(grb_ctx* c) { return c ? c->launches : 0; }
+
+int grb_set_profiling(grb_ctx* c, int32_t on) {
+    if (!c) return GRB_EINVAL;
+    GRB_CUDA(c, cudaSetDevice(c->device));
+    if (on && !c->d_phase) {
+        if (cudaMalloc(&c->d_phase, 8 * sizeof(unsigned long long)) != cudaSuccess) {
+            cudaGetLastError();
+            return fail(c, GRB_ENOMEM, "profiling buffer");
+        }
+        GRB_CUDA(c, cudaMemset(c->d_phase, 0, 8 * sizeof(unsigned long long)));
+    }
+    c->profiling = on != 0;
+    return GRB_OK;
+}
+
+int grb_phase_times(grb_ctx* c, double* ms, int32_t n, int32_t reset) {
+    if (!c || !ms || n < 0) return GRB_EINVAL;
+    for (int k = 0; k < n && k < 8; ++k) ms[k] = c->phase_ms[k];
+    if (reset) for (double& v : c->phase_ms) v = 0;
+    return GRB_OK;
+}
 
 }  // extern "C"

@@ -215,10 +215,23 @@ class Router:
         self._check(self._lib.grb_read_routes(self._ctx, _p(out)))
         return out
 
+    def set_stats(self, wirelength: float = 0.0, vias: int = 0):
+        self._check(self._lib.grb_set_stats(self._ctx, float(wirelength), int(vias)))
+
     def stats(self) -> dict:
         st = _abi.GrbStats()
         self._check(self._lib.grb_get_stats(self._ctx, C.byref(st)))
         return _stats_dict(st)
+
+    PHASES = ("batch_forbid_raster", "batch_preds", "batch_solve", "batch_publish", "refresh", "dp", "commit")
+
+    def set_profiling(self, on: bool = True):
+        self._check(self._lib.grb_set_profiling(self._ctx, int(bool(on))))
+
+    def phase_times(self, reset: bool = True) -> dict:
+        out = np.zeros(8, np.float64)
+        self._check(self._lib.grb_phase_times(self._ctx, _p(out), 8, int(reset)))
+        return dict(zip(self.PHASES, out.tolist()))
 
     def sync(self):
         self._check(self._lib.grb_sync(self._ctx))

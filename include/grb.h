@@ -144,12 +144,27 @@ int grb_read_tables(grb_ctx* ctx, float* wcost, float* vcost, double* presum, in
 /* Copy all route words (route_off[n] words) to the host. */
 int grb_read_routes(grb_ctx* ctx, int32_t* routes);
 int grb_get_stats(grb_ctx* ctx, grb_stats* stats);
+/* Set the statistics counters (the reference uploads RouterState::statistics,
+ * whose via count starts at the number of metal1 pins, preprocess.hpp:1716-1718
+ * and :1780). */
+int grb_set_stats(grb_ctx* ctx, double total_wirelength, int64_t total_via_count);
 /* Wait for the context's stream and report any recorded device error. */
 int grb_sync(grb_ctx* ctx);
 
 /* Number of kernels this context has launched so far (graph launches count
  * every kernel node); used for launch accounting by callers. */
 int64_t grb_kernel_launches(grb_ctx* ctx);
+
+/* Profiling (off by default).  When on, the plain form brackets each launch
+ * group with CUDA events and the persistent kernels time each phase between
+ * grid barriers (block 0, global timer).  grb_phase_times returns accumulated
+ * milliseconds per phase: [0] batching forbidden colours + chunk raster,
+ * [1] batching predecessors, [2] batching in-chunk solve, [3] batching
+ * publish, [4] cost refresh, [5] DP (persistent: + wire commit), [6] commit
+ * (persistent: vias).  The reference prints its stage timings as
+ * BATCH_TIMING / DAG_TIMING records (router_state.hpp:259-264). */
+int grb_set_profiling(grb_ctx* ctx, int32_t on);
+int grb_phase_times(grb_ctx* ctx, double* ms, int32_t n, int32_t reset);
 
 #ifdef __cplusplus
 }

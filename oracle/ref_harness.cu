@@ -127,6 +127,11 @@ int run_topo(const std::string& cap, const std::string& net, const std::string& 
     }
     dump_grid(dir, state);
     dump(dir, "pin_acc_num", state.pin_cnt_sum_cpu);
+    // Initial via statistic: one via per metal1 pin (preprocess.hpp:1716-1718).
+    std::vector<int> pin_vias{0};
+    for (auto& dbnet : db::nets)
+        for (int pin : dbnet.pins) pin_vias[0] += pin < state.device.X * state.device.Y;
+    dump(dir, "pin_vias", pin_vias);
     dump(dir, "node_off", node_off); dump(dir, "nodes", nodes); dump(dir, "parents", parents);
     dump(dir, "point_off", point_off); dump(dir, "points", points);
     dump(dir, "hseg_off", hseg_off); dump(dir, "hsegs", hsegs);

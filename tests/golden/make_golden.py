@@ -40,7 +40,7 @@ FIXTURES = {
 }
 TOPO_KEYS = ["meta", "short_costs", "unit_costs", "x_edge_len", "y_edge_len", "capacity", "pin_acc_num",
              "node_off", "nodes", "parents", "point_off", "points", "hseg_off", "hsegs", "vseg_off", "vsegs",
-             "hpwl", "original", "pin_count", "order", "batch_of", "ids", "batch_off"]
+             "hpwl", "original", "pin_count", "order", "batch_of", "ids", "batch_off", "pin_vias"]
 EXT = {"i32": np.int32, "i64": np.int64, "f32": np.float32, "f64": np.float64}
 
 
@@ -101,7 +101,8 @@ def main():
                 data.update(read_dir(w, TOPO_KEYS))
             if args.route:
                 for k in TOPO_KEYS:  # the GPU passes read the committed plan
-                    data[k].tofile(os.path.join(w, f"{k}.{_ext(data[k])}"))
+                    if k in data:
+                        data[k].tofile(os.path.join(w, f"{k}.{_ext(data[k])}"))
                 out = os.path.join(w, "ref.out")
                 subprocess.run([HARNESS, "route", cap, net, w, REF, out], check=True, stdout=subprocess.DEVNULL)
                 nb = len(data["batch_off"]) - 1

@@ -34,6 +34,7 @@ def _route(g, mode):
     r = Router(golden_grid(g))
     r.upload_nets(golden_nets(g))
     r.set_plan(g["ids"], g["batch_off"])
+    r.set_stats(0.0, int(g["pin_vias"][0]))  # build_cuda_database seeds the via count
     st = r.lshape_route(mode)
     out = r.read_routes(), r.read_tables(), st
     r.close()
@@ -97,4 +98,12 @@ def test_out_file_byte_identical_and_scores(name):
         assert hashlib.sha256(blob).digest() == bytes(g["ref_out_sha256"])
         if os.path.exists(EVALUATOR):
             res = subprocess.run([EVALUATOR, cap, net, out], capture_output=True, text=True)
-            assert (res.stdout + res.stderr) == bytes(g["ref_eval_text"]).decode()
+            assert _scores(res.stdout + res.stderr) == _scores(bytes(g["ref_eval_text"]).decode())
+
+
+def _scores(text):
+    """Evaluator report lines (costs, open / incomplete nets), timing excluded."""
+    keep = ("overflow cost", "open nets", "incompleted nets", "wirelength cost", "via cost", "total cost", "FOR_STAT")
+    lines = [ln.strip() for ln in text.splitlines() if any(k in ln for k in keep) and "time" not in ln.lower()]
+    assert len(lines) >= 6, text
+    return lines
