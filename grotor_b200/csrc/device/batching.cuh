@@ -54,25 +54,25 @@ __device__ __forceinline__ void batch_error(const BatchState& B, int code, int i
     if (atomicCAS(B.error, 0, code) == 0) *B.error_info = info;
 }
 
-// Visit every cell net `id` marks (duplicates allowed), lanes of a warp split
+// Visit every cell net `id` marks (duplicates allowed); threads t of n split
 // the work.
 template <class F>
-__device__ __forceinline__ void for_each_mark(const BatchState& B, int id, int lane, F f) {
+__device__ __forceinline__ void for_each_mark(const BatchState& B, int id, int t, int n, F f) {
     const int hstep = B.sparsity * B.Y, vstep = B.sparsity;
     for (int s = B.hseg_off[id]; s < B.hseg_off[id + 1]; ++s) {
         const int a = B.hsegs[2 * s], b = B.hsegs[2 * s + 1];
         if (b < a) continue;
         const int cnt = (b - a) / hstep + 1;
-        for (int k = lane; k < cnt; k += 32) f(a + k * hstep);
+        for (int k = t; k < cnt; k += n) f(a + k * hstep);
     }
     for (int s = B.vseg_off[id]; s < B.vseg_off[id + 1]; ++s) {
         const int a = B.vsegs[2 * s], b = B.vsegs[2 * s + 1];
         if (b < a) continue;
         const int cnt = (b - a) / vstep + 1;
-        for (int k = lane; k < cnt; k += 32) f(a + k * vstep);
+        for (int k = t; k < cnt; k += n) f(a + k * vstep);
     }
     const int p0 = B.point_off[id], np = B.point_off[id + 1] - p0;
-    for (int k = lane; k < 4 * np; k += 32) {
+    for (int k = t; k < 4 * np; k += n) {
         const int p = B.points[p0 + k / 4], x = p / B.Y, y = p - x * B.Y;
         const int which = k & 3;
         int cx = x, cy = y;
@@ -83,45 +83,61 @@ __device__ __forceinline__ void for_each_mark(const BatchState& B, int id, int l
     }
 }
 
-// Phase 1 for one net (warp): chunk-local raster and forbidden colours.
-__device__ __forceinline__ void batch_phase1(const BatchState& B, int s, int jj, int lane) {
+// The per-net phases run one net per CTA (all its threads share the net's
+// marks and points); `acc` is CTA shared memory of at least max(W, 16) words.
+// Phase 1: chunk-local raster and forbidden colours from earlier chunks.
+__device__ __forceinline__ void batch_phase1(const BatchState& B, int s, int jj, unsigned* acc) {
     const int id = B.order[s + jj];
     const unsigned bit = 1u << (jj & 31);
     const int word = jj >> 5;
-    for_each_mark(B, id, lane, [&](int q) { atomicOr(B.localmask + size_t(q) * kChunkWords + word, bit); });
-    const int p0 = B.point_off[id], p1 = B.point_off[id + 1];
-    for (int w = lane; w < B.W; w += 32) {
-        unsigned acc = 0;
-        for (int k = p0; k < p1; ++k) acc |= B.cellmask[size_t(B.points[k]) * B.W + w];
-        B.fmask[size_t(jj) * B.W + w] = acc;
+    const int t = threadIdx.x, n = blockDim.x;
+    for (int w = t; w < B.W; w += n) acc[w] = 0u;
+    __syncthreads();
+    for_each_mark(B, id, t, n, [&](int q) { atomicOr(B.localmask + size_t(q) * kChunkWords + word, bit); });
+    const int p0 = B.point_off[id], np = B.point_off[id + 1] - p0;
+    for (int k = t; k < np * B.W; k += n) {
+        const int w = k % B.W;
+        const unsigned v = B.cellmask[size_t(B.points[p0 + k / B.W]) * B.W + w];
+        if (v) atomicOr(acc + w, v);
     }
+    __syncthreads();
+    for (int w = t; w < B.W; w += n) B.fmask[size_t(jj) * B.W + w] = acc[w];
+    __syncthreads();
 }
 
-// Phase 2 for one net (warp): predecessors inside the chunk.
-__device__ __forceinline__ void batch_phase2(const BatchState& B, int s, int jj, int lane) {
+// Phase 2: predecessors inside the chunk.
+__device__ __forceinline__ void batch_phase2(const BatchState& B, int s, int jj, unsigned* acc) {
     const int id = B.order[s + jj];
-    const int p0 = B.point_off[id], p1 = B.point_off[id + 1];
-    if (lane < kChunkWords) {
-        unsigned acc = 0;
-        if (lane * 32 < jj) {
-            for (int k = p0; k < p1; ++k) acc |= B.localmask[size_t(B.points[k]) * kChunkWords + lane];
-            if (lane == (jj >> 5)) acc &= (1u << (jj & 31)) - 1u;
-        }
-        B.pred[jj * kChunkWords + lane] = acc;
+    const int t = threadIdx.x, n = blockDim.x;
+    const int words = (jj >> 5) + 1;  // only bits of earlier chunk nets matter
+    for (int w = t; w < kChunkWords; w += n) acc[w] = 0u;
+    __syncthreads();
+    const int p0 = B.point_off[id], np = B.point_off[id + 1] - p0;
+    for (int k = t; k < np * words; k += n) {
+        const int w = k % words;
+        const unsigned v = B.localmask[size_t(B.points[p0 + k / words]) * kChunkWords + w];
+        if (v) atomicOr(acc + w, v);
     }
+    __syncthreads();
+    for (int w = t; w < kChunkWords; w += n) {
+        unsigned v = w < words ? acc[w] : 0u;
+        if (w == (jj >> 5)) v &= (1u << (jj & 31)) - 1u;
+        B.pred[jj * kChunkWords + w] = v;
+    }
+    __syncthreads();
 }
 
-// Phase 4 for one net (warp): publish its colour, clear chunk-local masks.
-__device__ __forceinline__ void batch_phase4(const BatchState& B, int s, int jj, int lane) {
+// Phase 4: publish the net's colour over its marks and clear its chunk-local
+// word (every net of the chunk clears the word holding its own bit, so all
+// words touched by the chunk end up zero).
+__device__ __forceinline__ void batch_phase4(const BatchState& B, int s, int jj) {
     const int id = B.order[s + jj];
     const int c = B.batch_of[s + jj];
     const unsigned bit = 1u << (c & 31);
-    const int word = c >> 5;
-    for_each_mark(B, id, lane, [&](int q) {
+    const int word = c >> 5, lword = jj >> 5;
+    for_each_mark(B, id, threadIdx.x, blockDim.x, [&](int q) {
         atomicOr(B.cellmask + size_t(q) * B.W + word, bit);
-        unsigned* lm = B.localmask + size_t(q) * kChunkWords;
-#pragma unroll
-        for (int w = 0; w < kChunkWords; ++w) lm[w] = 0;
+        B.localmask[size_t(q) * kChunkWords + lword] = 0u;
     });
 }
 

@@ -15,9 +15,10 @@ namespace grb {
 __device__ __forceinline__ const int* net_routes(const Plan& P, int id) { return P.routes + P.route_off[id]; }
 
 // One warp commits the wire segments of net `id`; lanes split each segment's
-// unit edges.  Returns nothing; statistics are accumulated atomically.
+// unit edges.  Along-y segments cover consecutive cells, so their dirty bits
+// are set a bitmap word at a time (fenwick.cuh:51-78).
 __device__ __forceinline__ void commit_net_wires(const Tables& T, const Plan& P, int id, int stamp, int K,
-                                                 int lane, int list) {
+                                                 int lane) {
     const int* r = net_routes(P, id);
     const int words = r[0];
     double length = 0;
@@ -28,12 +29,27 @@ __device__ __forceinline__ void commit_net_wires(const Tables& T, const Plan& P,
         const int x0 = ra / T.Y, y0 = ra - x0 * T.Y, x1 = rb / T.Y, y1 = rb - x1 * T.Y;
         const bool ay = x0 == x1;
         const int lo = ay ? min(y0, y1) : min(x0, x1), hi = ay ? max(y0, y1) : max(x0, x1);
-        if (lane == 0) { T.ts[a] = stamp; T.ts[b] = stamp; }
+        if (lane == 0) {
+            T.ts[a] = stamp;
+            T.ts[b] = stamp;
+            if (hi > lo) {
+                mark_group_dirty(T, layer, ay ? x0 : y0);
+                if (ay) {
+                    const int first = layer * T.XY + x0 * T.Y + lo;
+                    mark_range(T.dirty_wire, first, first + (hi - lo) - 1);
+                    mark_range(T.dirty_via, first, first + (hi - lo));
+                }
+            }
+        }
         for (int pos = lo + lane; pos < hi; pos += 32) {
             const int c = layer * T.XY + (ay ? x0 * T.Y + pos : pos * T.Y + y0);
             atomicAdd(T.demand + c, 2 * K);
             T.ts[c] = stamp;
-            mark_edge_dirty(T, c, list);
+            if (!ay) {
+                set_bits(T.dirty_wire, c >> 5, 1u << (c & 31));
+                set_bits(T.dirty_via, c >> 5, 1u << (c & 31));
+                if (pos + 1 < T.X) set_bits(T.dirty_via, (c + T.Y) >> 5, 1u << ((c + T.Y) & 31));
+            }
             length += ay ? T.ylen[pos] : T.xlen[pos];
         }
     }
@@ -41,14 +57,14 @@ __device__ __forceinline__ void commit_net_wires(const Tables& T, const Plan& P,
     if (lane == 0 && length != 0.0) atomicAdd(T.wirelength, length * K);
 }
 
-__device__ __forceinline__ void add_via_demand(const Tables& T, int c, int half, int list) {
+__device__ __forceinline__ void add_via_demand(const Tables& T, int c, int half) {
     atomicAdd(T.demand + c, half);
-    mark_edge_dirty(T, c, list);
+    mark_edge_dirty(T, c);
 }
 
 // One warp commits the via segments of net `id` (lanes over segments).
 __device__ __forceinline__ void commit_net_vias(const Tables& T, const Plan& P, int id, int stamp, int K,
-                                                int lane, int list) {
+                                                int lane) {
     const int* r = net_routes(P, id);
     const int words = r[0];
     long long vias = 0;
@@ -64,11 +80,11 @@ __device__ __forceinline__ void commit_net_vias(const Tables& T, const Plan& P, 
             if (T.ts[c] >= stamp) continue;
             const bool ay = along_y(T, layer);
             const int pos = ay ? y : x, len = ay ? T.Y : T.X, stride = ay ? 1 : T.Y;
-            if (!pos) add_via_demand(T, c, 2 * K, list);
-            else if (pos == len - 1) add_via_demand(T, c - stride, 2 * K, list);
+            if (!pos) add_via_demand(T, c, 2 * K);
+            else if (pos == len - 1) add_via_demand(T, c - stride, 2 * K);
             else {
-                add_via_demand(T, c - stride, K, list);
-                add_via_demand(T, c, K, list);
+                add_via_demand(T, c - stride, K);
+                add_via_demand(T, c, K);
             }
         }
     }

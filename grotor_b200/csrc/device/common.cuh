@@ -35,13 +35,10 @@ struct Tables {
     double* presum;
     unsigned* dirty_wire;  // one bit per cell
     unsigned* dirty_via;   // one bit per cell
+    int words;             // bitmap words
     // Prefix groups: kTrackGroup adjacent tracks of one layer.
     int group_base[kMaxLayers + 1];
-    unsigned* group_flag;  // [n_groups]
-    int* group_list[2];    // double-buffered work lists
-    int* group_count;      // [2]
-    int* via_list[2];      // dirty via bitmap words
-    int* via_count;        // [2]
+    unsigned* group_flag;  // [n_groups], nonzero = some track of the group changed
     int n_groups;
     double* wirelength;
     unsigned long long* vias;
@@ -72,38 +69,38 @@ __device__ __forceinline__ bool bit_test(const unsigned* bits, int i) { return (
 
 __device__ __forceinline__ int track_length(const Tables& T, int l) { return along_y(T, l) ? T.Y : T.X; }
 
-// Mark the via cost of cell c dirty and queue its bitmap word once.
-__device__ __forceinline__ void mark_via_dirty(const Tables& T, int c, int list) {
-    const unsigned bit = 1u << (c & 31);
-    unsigned* word = T.dirty_via + (c >> 5);
-    if (*reinterpret_cast<volatile unsigned*>(word) & bit) return;
-    if (atomicOr(word, bit) == 0) {
-        const int k = atomicAdd(T.via_count + list, 1);
-        T.via_list[list][k] = c >> 5;
-    }
+// Dirty marking uses fire-and-forget atomics (no return value): the refresh
+// finds the work by scanning the bitmaps, which are small (one bit per cell).
+__device__ __forceinline__ void set_bits(unsigned* bits, int word, unsigned mask) {
+    if (mask) atomicOr(bits + word, mask);
 }
 
-__device__ __forceinline__ void mark_group_dirty(const Tables& T, int l, int track, int list) {
-    const int g = T.group_base[l] + track / kTrackGroup;
-    if (*reinterpret_cast<volatile unsigned*>(T.group_flag + g)) return;
-    if (atomicOr(T.group_flag + g, 1u) == 0) {
-        const int k = atomicAdd(T.group_count + list, 1);
-        T.group_list[list][k] = g;
-    }
+__device__ __forceinline__ void mark_group_dirty(const Tables& T, int l, int track) {
+    T.group_flag[T.group_base[l] + track / kTrackGroup] = 1u;
 }
 
 // A demand change on edge cell c invalidates its wire cost, its own via cost
 // and the via cost of the next cell along the track (fenwick.cuh:27-38).
-__device__ __forceinline__ void mark_edge_dirty(const Tables& T, int c, int list) {
+__device__ __forceinline__ void mark_edge_dirty(const Tables& T, int c) {
     const int l = c / T.XY, rem = c - l * T.XY, x = rem / T.Y, y = rem - x * T.Y;
     const bool ay = along_y(T, l);
     const int pos = ay ? y : x, len = ay ? T.Y : T.X, stride = ay ? 1 : T.Y;
-    const unsigned bit = 1u << (c & 31);
-    unsigned* word = T.dirty_wire + (c >> 5);
-    if (!(*reinterpret_cast<volatile unsigned*>(word) & bit)) atomicOr(word, bit);
-    mark_via_dirty(T, c, list);
-    if (pos + 1 < len) mark_via_dirty(T, c + stride, list);
-    mark_group_dirty(T, l, ay ? x : y, list);
+    set_bits(T.dirty_wire, c >> 5, 1u << (c & 31));
+    set_bits(T.dirty_via, c >> 5, 1u << (c & 31));
+    if (pos + 1 < len) set_bits(T.dirty_via, (c + stride) >> 5, 1u << ((c + stride) & 31));
+    mark_group_dirty(T, l, ay ? x : y);
+}
+
+// Mark cells [first, last] of a bitmap with one atomic per word
+// (fenwick.cuh:40-49).
+__device__ __forceinline__ void mark_range(unsigned* bits, int first, int last) {
+    const int a = first >> 5, b = last >> 5;
+    for (int w = a; w <= b; ++w) {
+        unsigned m = ~0u;
+        if (w == a) m &= ~0u << (first & 31);
+        if (w == b) m &= ~0u >> (31 - (last & 31));
+        set_bits(bits, w, m);
+    }
 }
 
 // Grid-wide barrier for cooperative launches.  Every wait is bounded by the

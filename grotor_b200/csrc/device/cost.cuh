@@ -65,113 +65,155 @@ __device__ __forceinline__ float via_cost_at(const Tables& T, int c) {
     return static_cast<float>(static_cast<double>(v) + T.unit_via);
 }
 
-// Recompute the via costs of one dirty bitmap word (32 consecutive cells);
-// one warp, one lane per cell.  The word is cleared afterwards.
-__device__ __forceinline__ void refresh_via_word(const Tables& T, int w, int lane) {
-    const unsigned bits = T.dirty_via[w];
-    const int c = w * 32 + lane;
-    if (((bits >> lane) & 1u) && c < T.cells) T.vcost[c] = via_cost_at(T, c);
-    __syncwarp();
-    if (lane == 0) T.dirty_via[w] = 0;
+// Recompute every dirty cell: warps scan 32 bitmap words at a time and spend
+// all lanes (one per bit) on each nonzero word; wire costs where the wire bit
+// is set, via costs where the via bit is set (a wire-dirty cell is always
+// via-dirty).  Both words are cleared.  `warp`/`nwarps` number the calling
+// warps across the launch.
+__device__ __forceinline__ void refresh_dirty_cells(const Tables& T, int warp, int nwarps, int lane) {
+    for (int base = warp * 32; base < T.words; base += nwarps * 32) {
+        const int w = base + lane;
+        const unsigned vb = w < T.words ? T.dirty_via[w] : 0u;
+        const unsigned wb = w < T.words ? T.dirty_wire[w] : 0u;
+        unsigned nz = __ballot_sync(0xffffffffu, vb != 0u);
+        while (nz) {
+            const int k = __ffs(nz) - 1;
+            nz &= nz - 1;
+            const unsigned v = __shfl_sync(0xffffffffu, vb, k), x = __shfl_sync(0xffffffffu, wb, k);
+            const int c = (base + k) * 32 + lane;
+            if (c < T.cells) {
+                if ((x >> lane) & 1u) T.wcost[c] = wire_cost_at(T, c);
+                if ((v >> lane) & 1u) T.vcost[c] = via_cost_at(T, c);
+            }
+        }
+        if (vb) T.dirty_via[w] = 0u;
+        if (wb) T.dirty_wire[w] = 0u;
+    }
 }
 
-// Rebuild the prefix of one group (CTA-wide, blockDim.x == 256).  When
-// `recompute` is set, dirty wire cells read on the way are recomputed first
-// (the persistent executor fuses the cost update into the scan).
-template <bool recompute>
-__device__ void refresh_group(const Tables& T, int g, double* stack /* smem [32][16] */,
-                              double* t3 /* smem [8][32] */) {
+// Prefix rebuild of one group: 32 adjacent tracks (one per lane) of one layer,
+// CTA of 8 warps.  Positions are cut into aligned 32-position chunks; warps take
+// chunks round-robin.
+//   pass 1: each lane runs the reference association over its chunk (stack of
+//           aligned block totals, fully unrolled so it lives in registers) and
+//           keeps only the chunk total;
+//   tree:   totals of aligned 2^e-chunk blocks, pairwise, in shared memory;
+//   pass 2: each lane re-runs its chunk, and every element adds, lowest bit
+//           first, the totals of the aligned blocks below it at levels >= 5.
+// The result equals the reference's per-track scan bit for bit.  Wire costs
+// must be current (refresh_dirty_cells runs first).
+constexpr int kChunkPos = 32;
+
+__host__ __device__ __forceinline__ int prefix_tree_entries(int len) {
+    const int nch = (len + kChunkPos - 1) / kChunkPos;
+    return 2 * nch + 1;
+}
+__host__ __device__ __forceinline__ size_t prefix_smem_bytes(int max_len) {
+    return size_t(prefix_tree_entries(max_len)) * 32 * sizeof(double);
+}
+
+__device__ void refresh_group(const Tables& T, int g, double* tree /* smem [entries][32] */) {
     int l = 0;
     while (l + 1 <= T.L && g >= T.group_base[l + 1]) ++l;
     const bool ay = along_y(T, l);
     const int tracks = ay ? T.X : T.Y, len = ay ? T.Y : T.X;
     const int track0 = (g - T.group_base[l]) * kTrackGroup;
-    const int lane = threadIdx.x & 31, sub = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
     const int track = track0 + lane;
     const bool live = track < tracks;
-    const int base = ay ? cell_index(T, l, track < tracks ? track : 0, 0) : cell_index(T, l, 0, track < tracks ? track : 0);
+    const int base = ay ? cell_index(T, l, live ? track : 0, 0) : cell_index(T, l, 0, live ? track : 0);
     const int stride = ay ? 1 : T.Y;
-    double* my_stack = stack + lane * 16;
-    for (int p0 = 0; p0 < len; p0 += 64) {
-        const int i0 = p0 + sub * 8;
-        double v[8];
+    const int nch = (len + kChunkPos - 1) / kChunkPos;
+
+    // Loads the shifted input s[i] = w[i-1] of chunk c (0 outside the track).
+    auto load_chunk = [&](int c, double (&x)[kChunkPos]) {
+        const int i0 = c * kChunkPos;
 #pragma unroll
-        for (int k = 0; k < 8; ++k) {
+        for (int k = 0; k < kChunkPos; ++k) {
             const int i = i0 + k;
-            double x = 0.0;
-            if (live && i > 0 && i < len) {
-                const int c = base + (i - 1) * stride;
-                float w;
-                if (recompute && bit_test(T.dirty_wire, c)) {
-                    w = wire_cost_at(T, c);
-                    T.wcost[c] = w;
-                    atomicAnd(T.dirty_wire + (c >> 5), ~(1u << (c & 31)));
-                } else {
-                    w = T.wcost[c];
-                }
-                x = static_cast<double>(w);
-            }
-            v[k] = x;
+            x[k] = (live && i > 0 && i < len) ? static_cast<double>(T.wcost[base + (i - 1) * stride]) : 0.0;
         }
-        if (recompute && live && i0 <= len - 1 && len - 1 < i0 + 8) {
-            // The last cell of a track feeds no prefix entry but keeps its cost current.
-            const int c = base + (len - 1) * stride;
-            if (bit_test(T.dirty_wire, c)) {
-                T.wcost[c] = wire_cost_at(T, c);
-                atomicAnd(T.dirty_wire + (c >> 5), ~(1u << (c & 31)));
-            }
-        }
-        // Levels 0..2 inside the aligned 8-run (sum[i] += sum[(i>>d<<d)-1]).
-        v[1] = v[1] + v[0]; v[3] = v[3] + v[2]; v[5] = v[5] + v[4]; v[7] = v[7] + v[6];
-        v[2] = v[2] + v[1]; v[3] = v[3] + v[1]; v[6] = v[6] + v[5]; v[7] = v[7] + v[5];
-        v[4] = v[4] + v[3]; v[5] = v[5] + v[3]; v[6] = v[6] + v[3]; v[7] = v[7] + v[3];
-        t3[sub * 32 + lane] = v[7];
-        __syncthreads();
-        // Levels 3..5: totals of aligned 8-, 16- and 32-runs below this run.
-        double add3 = 0, add4 = 0, add5 = 0;
-        if (sub & 1) add3 = t3[(sub - 1) * 32 + lane];
-        if (sub & 2) {
-            const int q = (sub >> 1) - 1;  // 16-run index below
-            add4 = t3[(2 * q + 1) * 32 + lane] + t3[(2 * q) * 32 + lane];
-        }
-        if (sub & 4) {
-            const double up = t3[3 * 32 + lane] + t3[2 * 32 + lane];
-            const double lo = t3[1 * 32 + lane] + t3[0 * 32 + lane];
-            add5 = up + lo;
-        }
-        // Levels >= 6: completed 64-aligned blocks below this chunk.
-        const int chunk = p0 >> 6;
+    };
+
+    // Pass 1: chunk totals (level 0 of the tree).
+    for (int c = warp; c < nch; c += nwarp) {
+        double x[kChunkPos];
+        load_chunk(c, x);
+        double tot[6];
 #pragma unroll
-        for (int k = 0; k < 8; ++k) {
-            double acc = v[k];
-            if (sub & 1) acc = acc + add3;
-            if (sub & 2) acc = acc + add4;
-            if (sub & 4) acc = acc + add5;
-            for (int e = 0; (chunk >> e) != 0; ++e)
-                if ((chunk >> e) & 1) acc = acc + my_stack[e];
+        for (int k = 0; k < kChunkPos; ++k) {
+            double acc = x[k];
+            double fresh[6];
+            fresh[0] = acc;
+#pragma unroll
+            for (int d = 0; d < 5; ++d) {
+                if (((k >> d) & 1) && ((k & ((1 << d) - 1)) == (1 << d) - 1)) {
+                    acc = acc + tot[d];
+                    fresh[d + 1] = acc;
+                }
+            }
+            int t = 0;
+            while (t < 5 && ((k >> t) & 1)) ++t;
+#pragma unroll
+            for (int d = 0; d < 6; ++d) if (d <= t) tot[d] = fresh[d];
+            if (k == kChunkPos - 1) tree[c * 32 + lane] = acc;  // 31 = all ones: acc is the chunk total
+        }
+    }
+    __syncthreads();
+    // Tree of aligned block totals: level e entry b = level e-1 entries 2b+1 + 2b.
+    {
+        int off = 0, cnt = nch;
+        while (cnt > 1) {
+            const int up = cnt >> 1;
+            for (int b = warp; b < up; b += nwarp)
+                tree[(off + cnt + b) * 32 + lane] = tree[(off + 2 * b + 1) * 32 + lane] + tree[(off + 2 * b) * 32 + lane];
+            __syncthreads();
+            off += cnt;
+            cnt = up;
+        }
+    }
+    // Pass 2: final prefix values.
+    for (int c = warp; c < nch; c += nwarp) {
+        double add[8];
+        {
+            int off = 0, cnt = nch;
+#pragma unroll
+            for (int e = 0; e < 8; ++e) {
+                add[e] = 0.0;
+                if (cnt >= 1 && ((c >> e) & 1)) add[e] = tree[(off + (c >> e) - 1) * 32 + lane];
+                off += cnt;
+                cnt >>= 1;
+            }
+        }
+        double x[kChunkPos];
+        load_chunk(c, x);
+        double tot[6];
+        const int i0 = c * kChunkPos;
+#pragma unroll
+        for (int k = 0; k < kChunkPos; ++k) {
+            double acc = x[k];
+            double fresh[6];
+            fresh[0] = acc;
+            int t = 0;
+#pragma unroll
+            for (int d = 0; d < 5; ++d) {
+                if (((k >> d) & 1) && ((k & ((1 << d) - 1)) == (1 << d) - 1)) {
+                    acc = acc + tot[d];
+                    fresh[d + 1] = acc;
+                    t = d + 1;
+                }
+            }
+#pragma unroll
+            for (int d = 0; d < 6; ++d) if (d <= t) tot[d] = fresh[d];
+#pragma unroll
+            for (int e = 0; e < 5; ++e)
+                if (e > t && ((k >> e) & 1)) acc = acc + tot[e];
+#pragma unroll
+            for (int e = 0; e < 8; ++e)
+                if ((c >> e) & 1) acc = acc + add[e];
             const int i = i0 + k;
             if (live && i < len) T.presum[base + i * stride] = acc;
-            v[k] = acc;
         }
-        __syncthreads();
-        // Push this chunk's total (element 63 before the high levels) onto the
-        // per-track stack of completed block totals.
-        if (sub == 7) {
-            double up = t3[7 * 32 + lane] + t3[6 * 32 + lane];
-            up = up + (t3[5 * 32 + lane] + t3[4 * 32 + lane]);
-            const double lo = (t3[3 * 32 + lane] + t3[2 * 32 + lane]) + (t3[1 * 32 + lane] + t3[0 * 32 + lane]);
-            double total = up + lo;
-            double fresh[16];
-            fresh[0] = total;
-            int d = 0;
-            while ((chunk >> d) & 1) {
-                total = total + my_stack[d];
-                ++d;
-                fresh[d] = total;
-            }
-            for (int j = 0; j <= d; ++j) my_stack[j] = fresh[j];
-        }
-        __syncthreads();
     }
 }
 

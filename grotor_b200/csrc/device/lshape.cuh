@@ -81,7 +81,7 @@ __device__ __forceinline__ double wire_cost(const Tables& T, int l, int xmin, in
 // Route one net.  All 32 lanes of the warp call this with the same id.
 // Returns false (and records kELimit) if the net's route storage is too small.
 __device__ void lshape_net(const Tables& T, const Plan& P, int id, int stamp, const Arena& A, int lane,
-                           bool fuse_wires, int list) {
+                           bool fuse_wires) {
     const int L = T.L, Y = T.Y, XY = T.XY, TT = tri_count(L);
     const int off = P.node_off[id], N = P.node_off[id + 1] - off;
     const int* nd = P.nodes + off;
@@ -249,7 +249,7 @@ __device__ void lshape_net(const Tables& T, const Plan& P, int id, int stamp, co
     }
     if (lane == 0) out[0] = next;
     __syncwarp();
-    if (fuse_wires) commit_net_wires(T, P, id, stamp, 1, lane, list);
+    if (fuse_wires) commit_net_wires(T, P, id, stamp, 1, lane);
 }
 
 }  // namespace grb

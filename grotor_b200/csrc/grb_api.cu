@@ -28,45 +28,31 @@ constexpr int kPersistentThreads = 256;
 constexpr int kDpThreads = 128;
 constexpr unsigned long long kBarrierTimeoutNs = 20ull * 1000 * 1000 * 1000;
 
-__global__ void k_cost_cells(Tables T) {
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= T.cells) return;
-    const unsigned wbits = T.dirty_wire[c >> 5], vbits = T.dirty_via[c >> 5];
-    const unsigned bit = 1u << (c & 31);
-    if (wbits & bit) T.wcost[c] = wire_cost_at(T, c);
-    if (vbits & bit) T.vcost[c] = via_cost_at(T, c);
+// update_dirty_costs (incremental_update.cuh:62-96): recompute dirty cells.
+__global__ void k_refresh_cells(Tables T) {
+    const int lane = threadIdx.x & 31;
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nwarps = (gridDim.x * blockDim.x) >> 5;
+    refresh_dirty_cells(T, warp, nwarps, lane);
 }
 
 __global__ void __launch_bounds__(kRefreshThreads) k_prefix_groups(Tables T) {
-    __shared__ double stack[32 * 16];
-    __shared__ double t3[8 * 32];
+    extern __shared__ __align__(16) double tree[];
     const int g = blockIdx.x;
     if (!T.group_flag[g]) return;
-    refresh_group<false>(T, g, stack, t3);
-}
-
-__global__ void k_clear_dirty(Tables T, int words) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < words) { T.dirty_wire[i] = 0; T.dirty_via[i] = 0; }
-    if (i < T.n_groups) T.group_flag[i] = 0;
-    if (i < 2) { T.group_count[i] = 0; T.via_count[i] = 0; }
+    refresh_group(T, g, tree);
+    if (threadIdx.x == 0) T.group_flag[g] = 0u;
 }
 
 // Everything dirty: the state of a fresh database (first refresh is full).
-__global__ void k_mark_all_dirty(Tables T, int words, int list) {
+__global__ void k_mark_all_dirty(Tables T) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < words) {
+    if (i < T.words) {
         const int rem = T.cells - i * 32;
         const unsigned m = rem >= 32 ? 0xffffffffu : ((1u << rem) - 1u);
         T.dirty_wire[i] = m;
         T.dirty_via[i] = m;
-        T.via_list[list][i] = i;
     }
-    if (i < T.n_groups) { T.group_flag[i] = 1; T.group_list[list][i] = i; }
-    if (i == 0) {
-        T.via_count[list] = words; T.group_count[list] = T.n_groups;
-        T.via_count[list ^ 1] = 0; T.group_count[list ^ 1] = 0;
-    }
+    if (i < T.n_groups) T.group_flag[i] = 1u;
 }
 
 __device__ __forceinline__ Arena warp_arena(char* smem, size_t arena_b, int warp, int L, int nmax) {
@@ -87,51 +73,48 @@ __global__ void __launch_bounds__(kDpThreads) k_lshape_batch(Tables T, Plan P, i
     if (N <= nmax) A = warp_arena(smem, arena_b, warp, T.L, nmax);
     else if (gscratch) A = carve_arena(gscratch + size_t(blockIdx.x * (blockDim.x >> 5) + warp) * gslot, T.L, N);
     else { if (lane == 0) set_error(T, kELimit, id); return; }
-    lshape_net(T, P, id, stamp, A, lane, false, 0);
+    lshape_net(T, P, id, stamp, A, lane, false);
 }
 
-__global__ void k_commit_wires(Tables T, Plan P, int b, int stamp, int K, int list) {
+__global__ void k_commit_wires(Tables T, Plan P, int b, int stamp, int K) {
     const int lane = threadIdx.x & 31;
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, warps = (gridDim.x * blockDim.x) >> 5;
     const int lo = P.batch_off[b], cnt = P.batch_off[b + 1] - lo;
-    for (int k = warp; k < cnt; k += warps) commit_net_wires(T, P, P.ids[lo + k], stamp, K, lane, list);
+    for (int k = warp; k < cnt; k += warps) commit_net_wires(T, P, P.ids[lo + k], stamp, K, lane);
 }
 
-__global__ void k_commit_vias(Tables T, Plan P, int b, int stamp, int K, int list) {
+__global__ void k_commit_vias(Tables T, Plan P, int b, int stamp, int K) {
     const int lane = threadIdx.x & 31;
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, warps = (gridDim.x * blockDim.x) >> 5;
     const int lo = P.batch_off[b], cnt = P.batch_off[b + 1] - lo;
-    for (int k = warp; k < cnt; k += warps) commit_net_vias(T, P, P.ids[lo + k], stamp, K, lane, list);
+    for (int k = warp; k < cnt; k += warps) commit_net_vias(T, P, P.ids[lo + k], stamp, K, lane);
 }
 
 // Persistent stage: every batch of the plan in one cooperative launch.
-// Per batch: refresh costs from the dirty work lists -> route + commit wires ->
-// commit vias, separated by bounded grid barriers.
+// Per batch: recompute dirty cells -> rebuild dirty prefix groups -> route and
+// commit wires -> commit vias, separated by bounded grid barriers.
 __global__ void __launch_bounds__(kPersistentThreads) k_lshape_persistent(Tables T, Plan P, GridSync S,
-        int stamp0, int parity0, int nmax, size_t arena_b, char* gscratch, size_t gslot, int* work) {
+        int stamp0, int nmax, size_t arena_b, char* gscratch, size_t gslot, int* work) {
     extern __shared__ __align__(16) char smem[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int gwarp = blockIdx.x * (blockDim.x >> 5) + warp, nwarps = gridDim.x * (blockDim.x >> 5);
-    double* stack = reinterpret_cast<double*>(smem);
-    double* t3 = stack + 32 * 16;
+    const int gwarp = warp * gridDim.x + blockIdx.x, nwarps = gridDim.x * (blockDim.x >> 5);
+    double* tree = reinterpret_cast<double*>(smem);
     PhaseClock clk;
     clk.start(S);
     for (int b = 0; b < P.n_batches; ++b) {
-        const int q = (parity0 + b) & 1, nq = q ^ 1;
         const int stamp = stamp0 + b + 1;
-        // Phase C: incremental cost + prefix refresh.
-        if (blockIdx.x == 0 && threadIdx.x == 0) { T.group_count[nq] = 0; T.via_count[nq] = 0; }
-        const int ng = *reinterpret_cast<volatile int*>(T.group_count + q);
-        const int nv = *reinterpret_cast<volatile int*>(T.via_count + q);
-        for (int k = blockIdx.x; k < ng; k += gridDim.x) {
-            const int g = T.group_list[q][k];
-            refresh_group<true>(T, g, stack, t3);
-            if (threadIdx.x == 0) T.group_flag[g] = 0;
+        // refresh_cost (incremental_update.cuh:98-132): dirty cells, then the
+        // prefix of every group with a changed wire cost.
+        refresh_dirty_cells(T, gwarp, nwarps, lane);
+        if (!grid_sync(S, T)) return;
+        for (int g = blockIdx.x; g < T.n_groups; g += gridDim.x) {
+            if (!*reinterpret_cast<volatile unsigned*>(T.group_flag + g)) continue;
+            refresh_group(T, g, tree);
+            if (threadIdx.x == 0) T.group_flag[g] = 0u;
         }
-        for (int k = gwarp; k < nv; k += nwarps) refresh_via_word(T, T.via_list[q][k], lane);
         if (!grid_sync(S, T)) return;
         clk.mark(S, 4);
-        // Phase A: route every net of the batch and commit its wires.
+        // Route every net of the batch and commit its wires.
         const int lo = P.batch_off[b], cnt = P.batch_off[b + 1] - lo;
         const Arena A = warp_arena(smem, arena_b, warp, T.L, nmax);
         while (true) {
@@ -141,29 +124,30 @@ __global__ void __launch_bounds__(kPersistentThreads) k_lshape_persistent(Tables
             if (k >= cnt) break;
             const int id = P.ids[lo + k];
             const int N = P.node_off[id + 1] - P.node_off[id];
-            if (N <= nmax) lshape_net(T, P, id, stamp, A, lane, true, nq);
-            else if (gscratch) lshape_net(T, P, id, stamp, carve_arena(gscratch + size_t(gwarp) * gslot, T.L, N), lane, true, nq);
+            if (N <= nmax) lshape_net(T, P, id, stamp, A, lane, true);
+            else if (gscratch) lshape_net(T, P, id, stamp, carve_arena(gscratch + size_t(gwarp) * gslot, T.L, N), lane, true);
             else if (lane == 0) set_error(T, kELimit, id);
         }
         if (!grid_sync(S, T)) return;
         clk.mark(S, 5);
-        // Phase B: via demand sees every wire timestamp of the batch.
-        for (int k = gwarp; k < cnt; k += nwarps) commit_net_vias(T, P, P.ids[lo + k], stamp, 1, lane, nq);
+        // Via demand sees every wire timestamp of the batch.
+        for (int k = gwarp; k < cnt; k += nwarps) commit_net_vias(T, P, P.ids[lo + k], stamp, 1, lane);
         if (!grid_sync(S, T)) return;
         clk.mark(S, 6);
     }
 }
 
 // --- batching kernels -------------------------------------------------------
+// One net per CTA in the per-net phases (a chunk's nets spread over the grid).
 __global__ void k_batch_phase1(BatchState B, int s) {
-    const int lane = threadIdx.x & 31, warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int warps = (gridDim.x * blockDim.x) >> 5, m = min(kChunk, B.n - s);
-    for (int j = warp; j < m; j += warps) batch_phase1(B, s, j, lane);
+    __shared__ unsigned acc[64];
+    const int m = min(kChunk, B.n - s);
+    for (int j = blockIdx.x; j < m; j += gridDim.x) batch_phase1(B, s, j, acc);
 }
 __global__ void k_batch_phase2(BatchState B, int s) {
-    const int lane = threadIdx.x & 31, warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int warps = (gridDim.x * blockDim.x) >> 5, m = min(kChunk, B.n - s);
-    for (int j = warp; j < m; j += warps) batch_phase2(B, s, j, lane);
+    __shared__ unsigned acc[kChunkWords];
+    const int m = min(kChunk, B.n - s);
+    for (int j = blockIdx.x; j < m; j += gridDim.x) batch_phase2(B, s, j, acc);
 }
 __global__ void __launch_bounds__(kChunk) k_batch_phase3(BatchState B, int s) {
     extern __shared__ __align__(16) unsigned bsm[];
@@ -171,31 +155,29 @@ __global__ void __launch_bounds__(kChunk) k_batch_phase3(BatchState B, int s) {
     batch_phase3(B, s, bsm);
 }
 __global__ void k_batch_phase4(BatchState B, int s) {
-    const int lane = threadIdx.x & 31, warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int warps = (gridDim.x * blockDim.x) >> 5, m = min(kChunk, B.n - s);
+    const int m = min(kChunk, B.n - s);
     if (*reinterpret_cast<volatile int*>(B.error)) return;
-    for (int j = warp; j < m; j += warps) batch_phase4(B, s, j, lane);
+    for (int j = blockIdx.x; j < m; j += gridDim.x) batch_phase4(B, s, j);
 }
 
 __global__ void __launch_bounds__(kChunk) k_batch_persistent(BatchState B, GridSync S, Tables T) {
     extern __shared__ __align__(16) unsigned bsm[];
-    const int lane = threadIdx.x & 31, warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int warps = (gridDim.x * blockDim.x) >> 5;
+    __shared__ unsigned acc[64];
     PhaseClock clk;
     clk.start(S);
     for (int s = 0; s < B.n; s += kChunk) {
         const int m = min(kChunk, B.n - s);
-        for (int j = warp; j < m; j += warps) batch_phase1(B, s, j, lane);
+        for (int j = blockIdx.x; j < m; j += gridDim.x) batch_phase1(B, s, j, acc);
         if (!grid_sync(S, T)) return;
         clk.mark(S, 0);
-        for (int j = warp; j < m; j += warps) batch_phase2(B, s, j, lane);
+        for (int j = blockIdx.x; j < m; j += gridDim.x) batch_phase2(B, s, j, acc);
         if (!grid_sync(S, T)) return;
         clk.mark(S, 1);
         if (blockIdx.x == 0) batch_phase3(B, s, bsm);
         if (!grid_sync(S, T)) return;
         clk.mark(S, 2);
         if (*reinterpret_cast<volatile int*>(B.error)) return;
-        for (int j = warp; j < m; j += warps) batch_phase4(B, s, j, lane);
+        for (int j = blockIdx.x; j < m; j += gridDim.x) batch_phase4(B, s, j);
         if (!grid_sync(S, T)) return;
         clk.mark(S, 3);
     }
@@ -309,7 +291,6 @@ struct grb_ctx {
     Tables T{};
     std::vector<void*> owned;
     int words = 0;          // bitmap words
-    int parity = 0;         // list holding pending dirty items
     int stamp = 0;
     int64_t launches = 0;
     // net store
@@ -469,12 +450,10 @@ int refresh_plain(grb_ctx* c) {
     cudaEvent_t e;
     int rc = prof_begin(c, 4, &e);
     if (rc) return rc;
-    k_cost_cells<<<(T.cells + 255) / 256, 256, 0, c->stream>>>(T);
-    k_prefix_groups<<<T.n_groups, kRefreshThreads, 0, c->stream>>>(T);
-    const int n = std::max(c->words, std::max(T.n_groups, 2));
-    k_clear_dirty<<<(n + 255) / 256, 256, 0, c->stream>>>(T, c->words);
+    k_refresh_cells<<<c->sms * 8, 256, 0, c->stream>>>(T);
+    k_prefix_groups<<<T.n_groups, kRefreshThreads, prefix_smem_bytes(std::max(T.X, T.Y)), c->stream>>>(T);
     prof_end(c, e);
-    c->launches += 3;
+    c->launches += 2;
     GRB_CUDA(c, cudaGetLastError());
     return GRB_OK;
 }
@@ -507,8 +486,8 @@ int commit_plain(grb_ctx* c, int b, int stamp, int K) {
     cudaEvent_t e;
     const int prc = prof_begin(c, 6, &e);
     if (prc) return prc;
-    k_commit_wires<<<blocks, 128, 0, c->stream>>>(c->T, make_plan(c), b, stamp, K, c->parity);
-    k_commit_vias<<<blocks, 128, 0, c->stream>>>(c->T, make_plan(c), b, stamp, K, c->parity);
+    k_commit_wires<<<blocks, 128, 0, c->stream>>>(c->T, make_plan(c), b, stamp, K);
+    k_commit_vias<<<blocks, 128, 0, c->stream>>>(c->T, make_plan(c), b, stamp, K);
     prof_end(c, e);
     c->launches += 2;
     GRB_CUDA(c, cudaGetLastError());
@@ -563,7 +542,7 @@ int stage_persistent(grb_ctx* c, int stamp0) {
     const int nmax = dp_nmax(c);
     const size_t ab = arena_bytes(c->T.L, nmax);
     const int wpb = kPersistentThreads / 32;
-    const size_t prefix_smem = (32 * 16 + 8 * 32) * sizeof(double);
+    const size_t prefix_smem = prefix_smem_bytes(std::max(c->T.X, c->T.Y));
     const size_t smem = std::max(ab * wpb, prefix_smem);
     GRB_CUDA(c, cudaFuncSetAttribute(k_lshape_persistent, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
     int per_sm = 0;
@@ -584,12 +563,10 @@ int stage_persistent(grb_ctx* c, int stamp0) {
     Tables T = c->T;
     Plan P = make_plan(c);
     GridSync S{c->sync, c->sync + 1, kBarrierTimeoutNs, c->profiling ? c->d_phase : nullptr};
-    int parity = c->parity;
     char* gs = c->gscratch;
-    void* args[] = {&T, &P, &S, &stamp0, &parity, (void*)&nmax, (void*)&ab, &gs, (void*)&slot, &c->work};
+    void* args[] = {&T, &P, &S, &stamp0, (void*)&nmax, (void*)&ab, &gs, (void*)&slot, &c->work};
     GRB_CUDA(c, cudaLaunchCooperativeKernel((void*)k_lshape_persistent, dim3(blocks), dim3(kPersistentThreads), args, smem, c->stream));
     c->launches += 1;
-    c->parity = (c->parity + c->n_batches) & 1;
     return GRB_OK;
 }
 
@@ -624,6 +601,7 @@ int grb_create(const grb_grid* g, int32_t device, grb_ctx** out) {
         !g->unit_length_short_costs || !g->x_edge_len || !g->y_edge_len)
         return GRB_EINVAL;
     if (size_t(g->L) * g->X * g->Y >= (size_t(1) << 31)) return GRB_EINVAL;
+    if (std::max(g->X, g->Y) > 8192) return GRB_EINVAL;  // prefix tree depth (kChunkPos << 8)
     auto c = std::make_unique<grb_ctx>();
     c->device = device;
     GRB_CUDA(c.get(), cudaSetDevice(device));
@@ -638,6 +616,7 @@ int grb_create(const grb_grid* g, int32_t device, grb_ctx** out) {
     T.of_scale = g->of_cost_scale;
     const size_t cells = T.cells;
     c->words = int((cells + 31) / 32);
+    T.words = c->words;
     int ng = 0;
     for (int l = 0; l < T.L; ++l) {
         T.group_base[l] = ng;
@@ -662,12 +641,6 @@ int grb_create(const grb_grid* g, int32_t device, grb_ctx** out) {
     rc |= dalloc(cp, &T.dirty_wire, c->words, cp->owned);
     rc |= dalloc(cp, &T.dirty_via, c->words, cp->owned);
     rc |= dalloc(cp, &T.group_flag, ng, cp->owned);
-    rc |= dalloc(cp, &T.group_list[0], ng, cp->owned);
-    rc |= dalloc(cp, &T.group_list[1], ng, cp->owned);
-    rc |= dalloc(cp, &T.group_count, 2, cp->owned);
-    rc |= dalloc(cp, &T.via_list[0], c->words, cp->owned);
-    rc |= dalloc(cp, &T.via_list[1], c->words, cp->owned);
-    rc |= dalloc(cp, &T.via_count, 2, cp->owned);
     rc |= dalloc(cp, &T.wirelength, 1, cp->owned);
     rc |= dalloc(cp, &T.vias, 1, cp->owned);
     rc |= dalloc(cp, &T.error, 2, cp->owned);
@@ -683,6 +656,8 @@ int grb_create(const grb_grid* g, int32_t device, grb_ctx** out) {
     GRB_CUDA(cp, cudaFuncSetAttribute(k_batch_phase3, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
     GRB_CUDA(cp, cudaFuncSetAttribute(k_batch_persistent, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
     GRB_CUDA(cp, cudaFuncSetAttribute(k_lshape_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    GRB_CUDA(cp, cudaFuncSetAttribute(k_prefix_groups, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      int(prefix_smem_bytes(std::max(T.X, T.Y)))));
     const int r = grb_reset(cp);
     if (r) { const int code = r; free_all(cp->owned); return code; }
     *out = c.release();
@@ -720,9 +695,8 @@ int grb_reset(grb_ctx* c) {
     GRB_CUDA(c, cudaMemsetAsync(T.wirelength, 0, sizeof(double), c->stream));
     GRB_CUDA(c, cudaMemsetAsync(T.vias, 0, sizeof(unsigned long long), c->stream));
     if (c->routes) GRB_CUDA(c, cudaMemsetAsync(c->routes, 0, sizeof(int) * std::max<long long>(c->route_words, 1), c->stream));
-    c->parity = 0;
     const int n = std::max(c->words, T.n_groups);
-    k_mark_all_dirty<<<(n + 255) / 256, 256, 0, c->stream>>>(T, c->words, c->parity);
+    k_mark_all_dirty<<<(n + 255) / 256, 256, 0, c->stream>>>(T);
     c->launches += 1;
     GRB_CUDA(c, cudaGetLastError());
     c->stamp = 0;

@@ -87,6 +87,7 @@ def main():
     ap.add_argument("--route", action="store_true")
     ap.add_argument("--only", default=None)
     ap.add_argument("--outdir", default=HERE, help="where to write the .npz files")
+    ap.add_argument("--keep-out", action="store_true", help="also copy the reference .out into --outdir")
     args = ap.parse_args()
     for name in FIXTURES:
         if args.only and name != args.only:
@@ -116,6 +117,9 @@ def main():
                               "snap_demand"):
                         data.pop(k)
                 blob = open(out, "rb").read()
+                if args.keep_out:
+                    with open(os.path.join(args.outdir, name + ".ref.out"), "wb") as f:
+                        f.write(blob)
                 data["ref_out_sha256"] = np.frombuffer(hashlib.sha256(blob).digest(), np.uint8)
                 data["ref_out_bytes"] = np.array([len(blob)], np.int64)
                 scores = evaluate(cap, net, out)
