@@ -83,16 +83,26 @@ __device__ __forceinline__ void for_each_mark(const BatchState& B, int id, int t
     }
 }
 
-// The per-net phases run one net per CTA (all its threads share the net's
-// marks and points); `acc` is CTA shared memory of at least max(W, 16) words.
+// A group of threads that works on one net: a whole CTA, or half of one
+// synchronised with a named barrier.
+struct NetGroup {
+    int t, n, bar;  // thread rank, group size, named barrier id (0: the CTA)
+    __device__ __forceinline__ void sync() const {
+        if (bar == 0) __syncthreads();
+        else asm volatile("bar.sync %0, %1;" ::"r"(bar), "r"(n) : "memory");
+    }
+};
+
+// The per-net phases run one net per group (its threads share the net's marks
+// and points); `acc` is group shared memory of at least max(W, 16) words.
 // Phase 1: chunk-local raster and forbidden colours from earlier chunks.
-__device__ __forceinline__ void batch_phase1(const BatchState& B, int s, int jj, unsigned* acc) {
+__device__ __forceinline__ void batch_phase1(const BatchState& B, int s, int jj, unsigned* acc, const NetGroup& G) {
     const int id = B.order[s + jj];
     const unsigned bit = 1u << (jj & 31);
     const int word = jj >> 5;
-    const int t = threadIdx.x, n = blockDim.x;
+    const int t = G.t, n = G.n;
     for (int w = t; w < B.W; w += n) acc[w] = 0u;
-    __syncthreads();
+    G.sync();
     for_each_mark(B, id, t, n, [&](int q) { atomicOr(B.localmask + size_t(q) * kChunkWords + word, bit); });
     const int p0 = B.point_off[id], np = B.point_off[id + 1] - p0;
     for (int k = t; k < np * B.W; k += n) {
@@ -100,42 +110,42 @@ __device__ __forceinline__ void batch_phase1(const BatchState& B, int s, int jj,
         const unsigned v = B.cellmask[size_t(B.points[p0 + k / B.W]) * B.W + w];
         if (v) atomicOr(acc + w, v);
     }
-    __syncthreads();
+    G.sync();
     for (int w = t; w < B.W; w += n) B.fmask[size_t(jj) * B.W + w] = acc[w];
-    __syncthreads();
+    G.sync();
 }
 
 // Phase 2: predecessors inside the chunk.
-__device__ __forceinline__ void batch_phase2(const BatchState& B, int s, int jj, unsigned* acc) {
+__device__ __forceinline__ void batch_phase2(const BatchState& B, int s, int jj, unsigned* acc, const NetGroup& G) {
     const int id = B.order[s + jj];
-    const int t = threadIdx.x, n = blockDim.x;
+    const int t = G.t, n = G.n;
     const int words = (jj >> 5) + 1;  // only bits of earlier chunk nets matter
     for (int w = t; w < kChunkWords; w += n) acc[w] = 0u;
-    __syncthreads();
+    G.sync();
     const int p0 = B.point_off[id], np = B.point_off[id + 1] - p0;
     for (int k = t; k < np * words; k += n) {
         const int w = k % words;
         const unsigned v = B.localmask[size_t(B.points[p0 + k / words]) * kChunkWords + w];
         if (v) atomicOr(acc + w, v);
     }
-    __syncthreads();
+    G.sync();
     for (int w = t; w < kChunkWords; w += n) {
         unsigned v = w < words ? acc[w] : 0u;
         if (w == (jj >> 5)) v &= (1u << (jj & 31)) - 1u;
         B.pred[jj * kChunkWords + w] = v;
     }
-    __syncthreads();
+    G.sync();
 }
 
 // Phase 4: publish the net's colour over its marks and clear its chunk-local
 // word (every net of the chunk clears the word holding its own bit, so all
 // words touched by the chunk end up zero).
-__device__ __forceinline__ void batch_phase4(const BatchState& B, int s, int jj) {
+__device__ __forceinline__ void batch_phase4(const BatchState& B, int s, int jj, const NetGroup& G) {
     const int id = B.order[s + jj];
     const int c = B.batch_of[s + jj];
     const unsigned bit = 1u << (c & 31);
     const int word = c >> 5, lword = jj >> 5;
-    for_each_mark(B, id, threadIdx.x, blockDim.x, [&](int q) {
+    for_each_mark(B, id, G.t, G.n, [&](int q) {
         atomicOr(B.cellmask + size_t(q) * B.W + word, bit);
         B.localmask[size_t(q) * kChunkWords + lword] = 0u;
     });

@@ -65,25 +65,47 @@ __device__ __forceinline__ float via_cost_at(const Tables& T, int c) {
     return static_cast<float>(static_cast<double>(v) + T.unit_via);
 }
 
-// Recompute every dirty cell: warps scan 32 bitmap words at a time and spend
-// all lanes (one per bit) on each nonzero word; wire costs where the wire bit
-// is set, via costs where the via bit is set (a wire-dirty cell is always
-// via-dirty).  Both words are cleared.  `warp`/`nwarps` number the calling
-// warps across the launch.
+// Recompute every dirty cell.  A warp loads 32 bitmap words at a time, ranks
+// their dirty cells with a warp prefix sum and computes them 32 at a time, one
+// cell per lane (a dirty word typically holds only a few dirty cells).  Wire
+// costs where the wire bit is set, via costs where the via bit is set (a
+// wire-dirty cell is always via-dirty).  Both words are cleared.
+// `warp`/`nwarps` number the calling warps across the launch.
 __device__ __forceinline__ void refresh_dirty_cells(const Tables& T, int warp, int nwarps, int lane) {
     for (int base = warp * 32; base < T.words; base += nwarps * 32) {
         const int w = base + lane;
         const unsigned vb = w < T.words ? T.dirty_via[w] : 0u;
         const unsigned wb = w < T.words ? T.dirty_wire[w] : 0u;
-        unsigned nz = __ballot_sync(0xffffffffu, vb != 0u);
-        while (nz) {
-            const int k = __ffs(nz) - 1;
-            nz &= nz - 1;
-            const unsigned v = __shfl_sync(0xffffffffu, vb, k), x = __shfl_sync(0xffffffffu, wb, k);
-            const int c = (base + k) * 32 + lane;
-            if (c < T.cells) {
-                if ((x >> lane) & 1u) T.wcost[c] = wire_cost_at(T, c);
-                if ((v >> lane) & 1u) T.vcost[c] = via_cost_at(T, c);
+        const int n = __popc(vb);
+        int incl = n;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const int o = __shfl_up_sync(0xffffffffu, incl, d);
+            if (lane >= d) incl += o;
+        }
+        const int total = __shfl_sync(0xffffffffu, incl, 31);
+        for (int r = 0; r < total; r += 32) {
+            const int k = r + lane;
+            // Owner lane: first lane whose inclusive count exceeds k.
+            int lo = 0;
+#pragma unroll
+            for (int step = 16; step; step >>= 1) {
+                const int v = __shfl_sync(0xffffffffu, incl, lo + step - 1);
+                if (v <= k) lo += step;
+            }
+            const int owner_incl = __shfl_sync(0xffffffffu, incl, lo);
+            const int owner_n = __shfl_sync(0xffffffffu, n, lo);
+            const unsigned ov = __shfl_sync(0xffffffffu, vb, lo), ow = __shfl_sync(0xffffffffu, wb, lo);
+            if (k < total) {
+                const int nth = k - (owner_incl - owner_n);  // 0-based rank inside the owner's word
+                unsigned m = ov;
+                for (int q = 0; q < nth; ++q) m &= m - 1;  // drop the nth lowest set bits
+                const int bit = __ffs(m) - 1;
+                const int c = (base + lo) * 32 + bit;
+                if (c < T.cells) {
+                    if ((ow >> bit) & 1u) T.wcost[c] = wire_cost_at(T, c);
+                    T.vcost[c] = via_cost_at(T, c);
+                }
             }
         }
         if (vb) T.dirty_via[w] = 0u;

@@ -107,13 +107,14 @@ __global__ void __launch_bounds__(kPersistentThreads) k_lshape_persistent(Tables
         // prefix of every group with a changed wire cost.
         refresh_dirty_cells(T, gwarp, nwarps, lane);
         if (!grid_sync(S, T)) return;
+        clk.mark(S, 4);
         for (int g = blockIdx.x; g < T.n_groups; g += gridDim.x) {
             if (!*reinterpret_cast<volatile unsigned*>(T.group_flag + g)) continue;
             refresh_group(T, g, tree);
             if (threadIdx.x == 0) T.group_flag[g] = 0u;
         }
         if (!grid_sync(S, T)) return;
-        clk.mark(S, 4);
+        clk.mark(S, 7);
         // Route every net of the batch and commit its wires.
         const int lo = P.batch_off[b], cnt = P.batch_off[b + 1] - lo;
         const Arena A = warp_arena(smem, arena_b, warp, T.L, nmax);
@@ -141,13 +142,15 @@ __global__ void __launch_bounds__(kPersistentThreads) k_lshape_persistent(Tables
 // One net per CTA in the per-net phases (a chunk's nets spread over the grid).
 __global__ void k_batch_phase1(BatchState B, int s) {
     __shared__ unsigned acc[64];
+    const NetGroup G{int(threadIdx.x), int(blockDim.x), 0};
     const int m = min(kChunk, B.n - s);
-    for (int j = blockIdx.x; j < m; j += gridDim.x) batch_phase1(B, s, j, acc);
+    for (int j = blockIdx.x; j < m; j += gridDim.x) batch_phase1(B, s, j, acc, G);
 }
 __global__ void k_batch_phase2(BatchState B, int s) {
     __shared__ unsigned acc[kChunkWords];
+    const NetGroup G{int(threadIdx.x), int(blockDim.x), 0};
     const int m = min(kChunk, B.n - s);
-    for (int j = blockIdx.x; j < m; j += gridDim.x) batch_phase2(B, s, j, acc);
+    for (int j = blockIdx.x; j < m; j += gridDim.x) batch_phase2(B, s, j, acc, G);
 }
 __global__ void __launch_bounds__(kChunk) k_batch_phase3(BatchState B, int s) {
     extern __shared__ __align__(16) unsigned bsm[];
@@ -155,29 +158,37 @@ __global__ void __launch_bounds__(kChunk) k_batch_phase3(BatchState B, int s) {
     batch_phase3(B, s, bsm);
 }
 __global__ void k_batch_phase4(BatchState B, int s) {
+    const NetGroup G{int(threadIdx.x), int(blockDim.x), 0};
     const int m = min(kChunk, B.n - s);
     if (*reinterpret_cast<volatile int*>(B.error)) return;
-    for (int j = blockIdx.x; j < m; j += gridDim.x) batch_phase4(B, s, j);
+    for (int j = blockIdx.x; j < m; j += gridDim.x) batch_phase4(B, s, j, G);
 }
 
+// Persistent batching: CTAs of kChunk threads (the in-chunk solve needs one
+// thread per net); the per-net phases use each half CTA as a net group so a
+// chunk's nets fit in one wave.
 __global__ void __launch_bounds__(kChunk) k_batch_persistent(BatchState B, GridSync S, Tables T) {
     extern __shared__ __align__(16) unsigned bsm[];
-    __shared__ unsigned acc[64];
+    __shared__ unsigned acc[2][64];
+    constexpr int kHalf = kChunk / 2;
+    const int half = threadIdx.x / kHalf;
+    const NetGroup G{int(threadIdx.x % kHalf), kHalf, 1 + half};
+    const int gi = half * gridDim.x + blockIdx.x, ng = 2 * gridDim.x;
     PhaseClock clk;
     clk.start(S);
     for (int s = 0; s < B.n; s += kChunk) {
         const int m = min(kChunk, B.n - s);
-        for (int j = blockIdx.x; j < m; j += gridDim.x) batch_phase1(B, s, j, acc);
+        for (int j = gi; j < m; j += ng) batch_phase1(B, s, j, acc[half], G);
         if (!grid_sync(S, T)) return;
         clk.mark(S, 0);
-        for (int j = blockIdx.x; j < m; j += gridDim.x) batch_phase2(B, s, j, acc);
+        for (int j = gi; j < m; j += ng) batch_phase2(B, s, j, acc[half], G);
         if (!grid_sync(S, T)) return;
         clk.mark(S, 1);
         if (blockIdx.x == 0) batch_phase3(B, s, bsm);
         if (!grid_sync(S, T)) return;
         clk.mark(S, 2);
         if (*reinterpret_cast<volatile int*>(B.error)) return;
-        for (int j = blockIdx.x; j < m; j += gridDim.x) batch_phase4(B, s, j);
+        for (int j = gi; j < m; j += ng) batch_phase4(B, s, j, G);
         if (!grid_sync(S, T)) return;
         clk.mark(S, 3);
     }
@@ -451,6 +462,8 @@ int refresh_plain(grb_ctx* c) {
     int rc = prof_begin(c, 4, &e);
     if (rc) return rc;
     k_refresh_cells<<<c->sms * 8, 256, 0, c->stream>>>(T);
+    prof_end(c, e);
+    if ((rc = prof_begin(c, 7, &e))) return rc;
     k_prefix_groups<<<T.n_groups, kRefreshThreads, prefix_smem_bytes(std::max(T.X, T.Y)), c->stream>>>(T);
     prof_end(c, e);
     c->launches += 2;

@@ -223,7 +223,8 @@ class Router:
         self._check(self._lib.grb_get_stats(self._ctx, C.byref(st)))
         return _stats_dict(st)
 
-    PHASES = ("batch_forbid_raster", "batch_preds", "batch_solve", "batch_publish", "refresh", "dp", "commit")
+    PHASES = ("batch_forbid_raster", "batch_preds", "batch_solve", "batch_publish", "refresh_cells", "dp", "commit",
+              "refresh_prefix")
 
     def set_profiling(self, on: bool = True):
         self._check(self._lib.grb_set_profiling(self._ctx, int(bool(on))))

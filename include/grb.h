@@ -160,8 +160,8 @@ int64_t grb_kernel_launches(grb_ctx* ctx);
  * grid barriers (block 0, global timer).  grb_phase_times returns accumulated
  * milliseconds per phase: [0] batching forbidden colours + chunk raster,
  * [1] batching predecessors, [2] batching in-chunk solve, [3] batching
- * publish, [4] cost refresh, [5] DP (persistent: + wire commit), [6] commit
- * (persistent: vias).  The reference prints its stage timings as
+ * publish, [4] dirty-cell cost recompute, [5] DP (persistent: + wire commit),
+ * [6] commit (persistent: vias), [7] prefix-table rebuild.  The reference prints its stage timings as
  * BATCH_TIMING / DAG_TIMING records (router_state.hpp:259-264). */
 int grb_set_profiling(grb_ctx* ctx, int32_t on);
 int grb_phase_times(grb_ctx* ctx, double* ms, int32_t n, int32_t reset);

@@ -19,7 +19,8 @@
 //                                   geometry (X, Y, order, points, segments).
 //   write <cap> <net> <dir> <lut> <routes> <out>
 //                                   CPU: write a .out with the reference writer from
-//                                   route words produced elsewhere.
+//                                   route words produced elsewhere (nets published
+//                                   in the plan order <dir>/ids.i32 when present).
 // Every array is written as raw little-endian data, <dir>/<name>.<i32|i64|f32|f64>.
 #include "pipeline.hpp"
 
@@ -307,8 +308,11 @@ int run_write(const std::string& cap, const std::string& net, const std::string&
     std::copy(words.begin(), words.end(), state.routes_cpu.get());
     for (int i = 0; i < int(db::nets.size()); ++i)
         if (db::nets[i].pins.size() == 1) nets2output.push(i);
+    // Lshape_route leaves nets2route in plan order and finish_nets publishes in
+    // that order (lshape.cuh:70-77, pipeline.hpp:286): use the plan if given.
     std::vector<int> all(state.nets.size());
     std::iota(all.begin(), all.end(), 0);
+    if (std::filesystem::exists(dir + "/ids.i32")) all = load<int>(dir + "/ids.i32");
     out_file = fopen(out.c_str(), "w");
     if (!out_file) throw std::runtime_error("cannot open " + out);
     setvbuf(out_file, nullptr, _IONBF, 0);
@@ -318,7 +322,6 @@ int run_write(const std::string& cap, const std::string& net, const std::string&
     graph::output_nets(state, std::move(records));
     fclose(out_file);
     out_file = nullptr;
-    (void)dir;
     return 0;
 }
 

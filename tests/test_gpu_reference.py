@@ -91,6 +91,7 @@ def test_out_file_byte_identical_and_scores(name):
         words = np.concatenate([routes, np.zeros(1, np.int32)])
         rp = os.path.join(w, "routes.i32")
         words.tofile(rp)
+        np.asarray(g["ids"], np.int32).tofile(os.path.join(w, "ids.i32"))  # publication order
         out = os.path.join(w, "mine.out")
         subprocess.run([HARNESS, "write", cap, net, w, os.path.dirname(HARNESS), rp, out], check=True,
                        stdout=subprocess.DEVNULL)
