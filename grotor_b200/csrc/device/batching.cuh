@@ -152,27 +152,32 @@ __device__ __forceinline__ void batch_phase4(const BatchState& B, int s, int jj,
 }
 
 // Phase 3 (one CTA of kChunk threads): first-fit inside the chunk.
-// smem: F[kChunk][W], P[kChunk][kChunkWords], col[kChunk], cnt[32W], full[W].
+// smem (word-major so a warp reads 32 consecutive words): F[W][kChunk],
+// P[kChunkWords][kChunk], col[kChunk], cnt[32W], run[32W], full[W].
 __device__ void batch_phase3(const BatchState& B, int s, unsigned* smem) {
-    const int tid = threadIdx.x;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int m = min(kChunk, B.n - s);
     const int W = B.W, C = 32 * W;
     unsigned* F = smem;
     unsigned* P = F + kChunk * W;
     int* col = reinterpret_cast<int*>(P + kChunk * kChunkWords);
     int* cnt = col + kChunk;
-    unsigned* full = reinterpret_cast<unsigned*>(cnt + C);
+    int* run = cnt + C;
+    unsigned* full = reinterpret_cast<unsigned*>(run + C);
     __shared__ int first_bad, overflow;
-    for (int k = tid; k < m * W; k += blockDim.x) F[k] = B.fmask[k];
-    for (int k = tid; k < m * kChunkWords; k += blockDim.x) P[k] = B.pred[k];
+    for (int k = tid; k < m * W; k += blockDim.x) F[(k % W) * kChunk + k / W] = B.fmask[k];
+    for (int k = tid; k < m * kChunkWords; k += blockDim.x) P[(k % kChunkWords) * kChunk + k / kChunkWords] = B.pred[k];
     for (int k = tid; k < C; k += blockDim.x) cnt[k] = B.count[k];
     for (int k = tid; k < W; k += blockDim.x) full[k] = B.fullmask[k];
     if (tid < kChunk) col[tid] = -1;
     if (tid == 0) overflow = 0;
     __syncthreads();
     int fixed = 0;  // nets below `fixed` are final
+    int rank = 0;
     while (true) {
-        // Jacobi sweeps until the colouring is a fixed point.
+        // Jacobi sweeps until the colouring is a fixed point: a net's colour is
+        // the first one neither forbidden by earlier chunks, nor full, nor held
+        // by one of its predecessors in the chunk.
         while (true) {
             int mine = tid < m ? col[tid] : -1;
             if (tid < m && tid >= fixed) {
@@ -180,16 +185,16 @@ __device__ void batch_phase3(const BatchState& B, int s, unsigned* smem) {
                 while (true) {
                     int w = c >> 5;
                     if (w >= W) { c = C; break; }
-                    unsigned used = F[tid * W + w] | full[w] | ((1u << (c & 31)) - 1u);
+                    unsigned used = F[w * kChunk + tid] | full[w] | ((1u << (c & 31)) - 1u);
                     while (used == 0xffffffffu) {
                         if (++w >= W) break;
-                        used = F[tid * W + w] | full[w];
+                        used = F[w * kChunk + tid] | full[w];
                     }
                     if (w >= W) { c = C; break; }
                     c = w * 32 + __ffs(~used) - 1;
                     bool hit = false;
                     for (int pw = 0; pw <= (tid >> 5) && !hit; ++pw) {
-                        unsigned bits = P[tid * kChunkWords + pw];
+                        unsigned bits = P[pw * kChunk + tid];
                         while (bits) {
                             const int i = pw * 32 + __ffs(bits) - 1;
                             bits &= bits - 1;
@@ -208,24 +213,29 @@ __device__ void batch_phase3(const BatchState& B, int s, unsigned* smem) {
             if (!__syncthreads_or(changed)) break;
         }
         if (overflow) break;
-        // Batch capacities in order: find the first net that would exceed one.
+        // Position of every net inside its batch, in chunk order: warps in turn
+        // add their per-colour group sizes to a running count.
+        for (int k = tid; k < C; k += blockDim.x) run[k] = cnt[k];
         if (tid == 0) first_bad = m;
         __syncthreads();
-        int rank_local = 0;
-        if (tid < m) {
-            const int c = col[tid];
-            for (int i = 0; i < tid; ++i) rank_local += col[i] == c;
-            if (cnt[c] + rank_local >= B.limit) atomicMin(&first_bad, tid);
+        const int c = tid < m ? col[tid] : -1 - lane;  // distinct dummies for idle lanes
+        const unsigned peers = __match_any_sync(0xffffffffu, c);
+        const int within = __popc(peers & ((1u << lane) - 1u));
+        for (int w = 0; w < (m + 31) / 32; ++w) {
+            if (warp == w && tid < m) {
+                rank = run[c] + within;
+                if (lane == __ffs(peers) - 1) run[c] += __popc(peers);
+                if (rank >= B.limit) atomicMin(&first_bad, tid);
+            }
+            __syncthreads();
         }
-        __syncthreads();
         const int bad = first_bad;
         if (bad >= m) {
             if (tid < m) {
                 B.batch_of[s + tid] = col[tid];
-                B.rank[s + tid] = cnt[col[tid]] + rank_local;
+                B.rank[s + tid] = rank;
             }
-            __syncthreads();
-            if (tid < m) atomicAdd(&cnt[col[tid]], 1);
+            for (int k = tid; k < C; k += blockDim.x) cnt[k] = run[k];
             __syncthreads();
             break;
         }
@@ -248,7 +258,7 @@ __device__ void batch_phase3(const BatchState& B, int s, unsigned* smem) {
 }
 
 __host__ __device__ __forceinline__ size_t phase3_smem_bytes(int W) {
-    return size_t(kChunk) * W * 4 + size_t(kChunk) * kChunkWords * 4 + kChunk * 4 + size_t(32) * W * 4 + W * 4;
+    return size_t(kChunk) * W * 4 + size_t(kChunk) * kChunkWords * 4 + kChunk * 4 + size_t(64) * W * 4 + W * 4;
 }
 
 }  // namespace grb

@@ -148,23 +148,23 @@ __device__ void refresh_group(const Tables& T, int g, double* tree /* smem [entr
     const int nch = (len + kChunkPos - 1) / kChunkPos;
 
     // Loads the shifted input s[i] = w[i-1] of chunk c (0 outside the track).
-    auto load_chunk = [&](int c, double (&x)[kChunkPos]) {
+    auto load_chunk = [&](int c, float (&x)[kChunkPos]) {  // wire costs are floats
         const int i0 = c * kChunkPos;
 #pragma unroll
         for (int k = 0; k < kChunkPos; ++k) {
             const int i = i0 + k;
-            x[k] = (live && i > 0 && i < len) ? static_cast<double>(T.wcost[base + (i - 1) * stride]) : 0.0;
+            x[k] = (live && i > 0 && i < len) ? T.wcost[base + (i - 1) * stride] : 0.0f;
         }
     };
 
     // Pass 1: chunk totals (level 0 of the tree).
     for (int c = warp; c < nch; c += nwarp) {
-        double x[kChunkPos];
+        float x[kChunkPos];
         load_chunk(c, x);
         double tot[6];
 #pragma unroll
         for (int k = 0; k < kChunkPos; ++k) {
-            double acc = x[k];
+            double acc = static_cast<double>(x[k]);
             double fresh[6];
             fresh[0] = acc;
 #pragma unroll
@@ -207,13 +207,13 @@ __device__ void refresh_group(const Tables& T, int g, double* tree /* smem [entr
                 cnt >>= 1;
             }
         }
-        double x[kChunkPos];
+        float x[kChunkPos];
         load_chunk(c, x);
         double tot[6];
         const int i0 = c * kChunkPos;
 #pragma unroll
         for (int k = 0; k < kChunkPos; ++k) {
-            double acc = x[k];
+            double acc = static_cast<double>(x[k]);
             double fresh[6];
             fresh[0] = acc;
             int t = 0;

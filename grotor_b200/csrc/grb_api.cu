@@ -35,7 +35,7 @@ __global__ void k_refresh_cells(Tables T) {
     refresh_dirty_cells(T, warp, nwarps, lane);
 }
 
-__global__ void __launch_bounds__(kRefreshThreads) k_prefix_groups(Tables T) {
+__global__ void __launch_bounds__(kRefreshThreads, 2) k_prefix_groups(Tables T) {
     extern __shared__ __align__(16) double tree[];
     const int g = blockIdx.x;
     if (!T.group_flag[g]) return;
@@ -93,7 +93,7 @@ __global__ void k_commit_vias(Tables T, Plan P, int b, int stamp, int K) {
 // Persistent stage: every batch of the plan in one cooperative launch.
 // Per batch: recompute dirty cells -> rebuild dirty prefix groups -> route and
 // commit wires -> commit vias, separated by bounded grid barriers.
-__global__ void __launch_bounds__(kPersistentThreads) k_lshape_persistent(Tables T, Plan P, GridSync S,
+__global__ void __launch_bounds__(kPersistentThreads, 2) k_lshape_persistent(Tables T, Plan P, GridSync S,
         int stamp0, int nmax, size_t arena_b, char* gscratch, size_t gslot, int* work) {
     extern __shared__ __align__(16) char smem[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
