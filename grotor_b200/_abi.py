@@ -68,6 +68,7 @@ SIGNATURES = {
     "grb_commit_batch": (C.c_int, [P, C.c_int32, C.c_int32, C.c_int32]),
     "grb_lshape_stage": (C.c_int, [P, C.c_int32, C.POINTER(GrbStats)]),
     "grb_ripup_classify": (C.c_int, [P, C.c_int32, P]),
+    "grb_ripup_classify_noalloc": (C.c_int, [P, C.c_int32, P]),
     "grb_congestion_view": (C.c_int, [P, P, P, P]),
     "grb_read_tables": (C.c_int, [P, P, P, P, P, P]),
     "grb_read_routes": (C.c_int, [P, P]),

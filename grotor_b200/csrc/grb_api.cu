@@ -6,6 +6,7 @@
 #include <cstdio>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -290,6 +291,18 @@ __global__ void k_float_line_prefix(float* v, int lines, int len, int line_strid
 }
 
 }  // namespace
+
+// ---------------------------------------------------------------------------
+// Fixed scratch for grb_ripup_classify_noalloc
+// ---------------------------------------------------------------------------
+// The rip-up classification needs one int per grid cell (overflow marks, then
+// their prefix along each track) and one flag per net.  For callers that must
+// not allocate device memory this scratch lives in one file-scope array that
+// every GPU loading the library holds until the process exits (about 20 MiB).
+constexpr int kNoAllocCells = 4 << 20;  // at most 4,194,304 grid cells (L*X*Y)
+constexpr int kNoAllocNets = 1 << 20;   // at most 1,048,576 nets
+constexpr int kNoAllocWords = kNoAllocCells + kNoAllocNets / 4;
+static __device__ __align__(256) int g_noalloc_scratch[kNoAllocWords];
 
 // ---------------------------------------------------------------------------
 // Host context
@@ -1009,6 +1022,54 @@ int grb_ripup_classify(grb_ctx* c, int32_t threshold, uint8_t* is_of) {
     cudaFree(of_sum);
     cudaFree(flags);
     if (e != cudaSuccess) return cuda_fail(c, e, "rip-up classification");
+    return GRB_OK;
+}
+
+// Device address of g_noalloc_scratch on the current device.  Host code only
+// holds a host-side stand-in for the array's name, so the address is looked up
+// once per device, with that device current, and cached.
+static int noalloc_scratch(grb_ctx* c, int** out) {
+    static std::mutex lock;
+    static std::vector<int*> cache;
+    std::lock_guard<std::mutex> guard(lock);
+    if (c->device >= int(cache.size())) cache.resize(c->device + 1, nullptr);
+    if (!cache[c->device]) {
+        void* p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess) return cuda_fail(c, e, "cudaGetSymbolAddress(g_noalloc_scratch)");
+        cache[c->device] = static_cast<int*>(p);
+    }
+    *out = cache[c->device];
+    return GRB_OK;
+}
+
+int grb_ripup_classify_noalloc(grb_ctx* c, int32_t threshold, uint8_t* is_of) {
+    if (!c || !is_of) return c ? fail(c, GRB_EINVAL, "is_of must not be NULL") : GRB_EINVAL;
+    if (c->T.cells > kNoAllocCells)
+        return fail(c, GRB_ELIMIT, "grid has " + std::to_string(c->T.cells) + " cells; the allocation-free "
+                    "classification supports at most " + std::to_string(kNoAllocCells));
+    if (c->n_nets > kNoAllocNets)
+        return fail(c, GRB_ELIMIT, "design has " + std::to_string(c->n_nets) + " nets; the allocation-free "
+                    "classification supports at most " + std::to_string(kNoAllocNets));
+    if (!c->node_off) return fail(c, GRB_EINVAL, "no nets uploaded");
+    GRB_CUDA(c, cudaSetDevice(c->device));
+    int* scratch = nullptr;
+    const int rc = noalloc_scratch(c, &scratch);
+    if (rc) return rc;
+    // Every scratch word used below is written before it is read (one overflow
+    // mark per cell, one flag per net), so nothing has to be cleared first.
+    int* of_sum = scratch;
+    unsigned char* flags = reinterpret_cast<unsigned char*>(scratch + kNoAllocCells);
+    int tracks = 0;
+    for (int l = 0; l < c->T.L; ++l) tracks += (((l & 1) ^ c->T.DIR) ? c->T.X : c->T.Y);
+    k_mark_overflow<<<(c->T.cells + 255) / 256, 256, 0, c->stream>>>(c->T, threshold, of_sum);
+    k_int_prefix<<<(tracks + 127) / 128, 128, 0, c->stream>>>(c->T, of_sum);
+    Plan P = make_plan(c);
+    if (c->n_nets) k_overflow_nets<<<(c->n_nets + 255) / 256, 256, 0, c->stream>>>(c->T, P, c->n_nets, of_sum, flags);
+    c->launches += c->n_nets ? 3 : 2;
+    GRB_CUDA(c, cudaGetLastError());
+    if (c->n_nets) GRB_CUDA(c, cudaMemcpyAsync(is_of, flags, c->n_nets, cudaMemcpyDeviceToHost, c->stream));
+    GRB_CUDA(c, cudaStreamSynchronize(c->stream));
     return GRB_OK;
 }
 

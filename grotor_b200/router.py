@@ -191,6 +191,15 @@ class Router:
         self._check(self._lib.grb_ripup_classify(self._ctx, int(threshold), _p(out)))
         return out
 
+    def ripup_noalloc(self, threshold: int = 0) -> np.ndarray:
+        """Same result as ``ripup``, computed without allocating device memory
+        (for callers under a fixed device-memory budget or in loops that must
+        not allocate); see grb_ripup_classify_noalloc in include/grb.h for the
+        size limits and the rule that overlapping calls race."""
+        out = np.zeros(self.nets.n if self.nets else 0, np.uint8)
+        self._check(self._lib.grb_ripup_classify_noalloc(self._ctx, int(threshold), _p(out)))
+        return out
+
     def congestion_view(self):
         xy = self.grid.X * self.grid.Y
         cong = np.empty(xy, np.uint8)

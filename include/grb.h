@@ -135,6 +135,22 @@ int grb_lshape_stage(grb_ctx* ctx, int32_t mode, grb_stats* stats);
  * threshold. */
 int grb_ripup_classify(grb_ctx* ctx, int32_t threshold, uint8_t* is_of);
 
+/* Allocation-free variant of grb_ripup_classify (no counterpart in the
+ * reference).  Some callers cannot allocate device memory while they route:
+ * processes that run under a fixed device-memory budget shared with another
+ * framework's caching allocator, or steady-state loops that must not pay the
+ * device-wide synchronisation cudaMalloc/cudaFree bring.  This entry point
+ * allocates nothing: its scratch (one int per grid cell, one flag per net) is a
+ * fixed array inside the library that every GPU loading the library holds until
+ * the process exits (about 20 MiB).  Limits: at most 4,194,304 grid cells
+ * (L*X*Y) and 1,048,576 nets; larger designs get GRB_ELIMIT.  The first call on
+ * a device looks up the array's device address with that device current, so it
+ * should come before any stream capture.  All calls share the one array (its
+ * contents are those of the last call, and every word is rewritten before use),
+ * so calls that overlap on the GPU -- two contexts or streams on the same
+ * device at once -- race; serialise them.  Results equal grb_ripup_classify's. */
+int grb_ripup_classify_noalloc(grb_ctx* ctx, int32_t threshold, uint8_t* is_of);
+
 /* Congestion view for the FLT topology builder (congestion.cuh:60-112). */
 int grb_congestion_view(grb_ctx* ctx, uint8_t* congestion, float* xsum, float* ysum);
 
