@@ -40,6 +40,11 @@ struct Tables {
     int group_base[kMaxLayers + 1];
     unsigned* group_flag;  // [n_groups], nonzero = some track of the group changed
     int n_groups;
+    int* group_list;       // [n_groups] dirty groups of the current refresh
+    int* group_count;      // [1]
+    double* ptree;         // [n_groups][tree_stride][32] prefix block totals
+    int tree_stride;       // entries per group (2 * tree_chunks + 1)
+    int tree_chunks;       // 32-position chunks of the longest track
     double* wirelength;
     unsigned long long* vias;
     int* error;            // first error code

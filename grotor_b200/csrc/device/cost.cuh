@@ -113,130 +113,181 @@ __device__ __forceinline__ void refresh_dirty_cells(const Tables& T, int warp, i
     }
 }
 
-// Prefix rebuild of one group: 32 adjacent tracks (one per lane) of one layer,
-// CTA of 8 warps.  Positions are cut into aligned 32-position chunks; warps take
-// chunks round-robin.
+// Prefix rebuild.  A group is 32 adjacent tracks of one layer (one per lane);
+// positions are cut into aligned 32-position chunks.  Work items are (group,
+// chunk) pairs, one warp each, spread over the whole GPU:
 //   pass 1: each lane runs the reference association over its chunk (stack of
-//           aligned block totals, fully unrolled so it lives in registers) and
-//           keeps only the chunk total;
-//   tree:   totals of aligned 2^e-chunk blocks, pairwise, in shared memory;
+//           aligned block totals, fully unrolled into registers) and stores the
+//           chunk total (level 0 of the group's tree, global memory);
+//   tree:   one CTA per group builds the totals of aligned 2^e-chunk blocks,
+//           pairwise (level e entry b = level e-1 entries 2b+1 + 2b);
 //   pass 2: each lane re-runs its chunk, and every element adds, lowest bit
 //           first, the totals of the aligned blocks below it at levels >= 5.
 // The result equals the reference's per-track scan bit for bit.  Wire costs
 // must be current (refresh_dirty_cells runs first).
 constexpr int kChunkPos = 32;
 
-__host__ __device__ __forceinline__ int prefix_tree_entries(int len) {
-    const int nch = (len + kChunkPos - 1) / kChunkPos;
-    return 2 * nch + 1;
-}
+__host__ __device__ __forceinline__ int prefix_chunks(int len) { return (len + kChunkPos - 1) / kChunkPos; }
+__host__ __device__ __forceinline__ int prefix_tree_entries(int len) { return 2 * prefix_chunks(len) + 1; }
 __host__ __device__ __forceinline__ size_t prefix_smem_bytes(int max_len) {
     return size_t(prefix_tree_entries(max_len)) * 32 * sizeof(double);
 }
 
-__device__ void refresh_group(const Tables& T, int g, double* tree /* smem [entries][32] */) {
+struct GroupGeom {
+    int l, len, nch, base, stride;
+    bool live;
+};
+
+__device__ __forceinline__ GroupGeom group_geom(const Tables& T, int g, int lane) {
+    GroupGeom G;
     int l = 0;
     while (l + 1 <= T.L && g >= T.group_base[l + 1]) ++l;
     const bool ay = along_y(T, l);
-    const int tracks = ay ? T.X : T.Y, len = ay ? T.Y : T.X;
-    const int track0 = (g - T.group_base[l]) * kTrackGroup;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
-    const int track = track0 + lane;
-    const bool live = track < tracks;
-    const int base = ay ? cell_index(T, l, live ? track : 0, 0) : cell_index(T, l, 0, live ? track : 0);
-    const int stride = ay ? 1 : T.Y;
-    const int nch = (len + kChunkPos - 1) / kChunkPos;
+    const int tracks = ay ? T.X : T.Y;
+    const int track = (g - T.group_base[l]) * kTrackGroup + lane;
+    G.l = l;
+    G.len = ay ? T.Y : T.X;
+    G.nch = prefix_chunks(G.len);
+    G.live = track < tracks;
+    G.base = ay ? cell_index(T, l, G.live ? track : 0, 0) : cell_index(T, l, 0, G.live ? track : 0);
+    G.stride = ay ? 1 : T.Y;
+    return G;
+}
 
-    // Loads the shifted input s[i] = w[i-1] of chunk c (0 outside the track).
-    auto load_chunk = [&](int c, float (&x)[kChunkPos]) {  // wire costs are floats
-        const int i0 = c * kChunkPos;
+// The shifted input s[i] = w[i-1] of chunk c (0 outside the track); wire
+// costs are floats, widened when used.
+__device__ __forceinline__ void load_chunk(const Tables& T, const GroupGeom& G, int c, float (&x)[kChunkPos]) {
+    const int i0 = c * kChunkPos;
 #pragma unroll
-        for (int k = 0; k < kChunkPos; ++k) {
-            const int i = i0 + k;
-            x[k] = (live && i > 0 && i < len) ? T.wcost[base + (i - 1) * stride] : 0.0f;
-        }
-    };
+    for (int k = 0; k < kChunkPos; ++k) {
+        const int i = i0 + k;
+        x[k] = (G.live && i > 0 && i < G.len) ? T.wcost[G.base + (i - 1) * G.stride] : 0.0f;
+    }
+}
 
-    // Pass 1: chunk totals (level 0 of the tree).
-    for (int c = warp; c < nch; c += nwarp) {
-        float x[kChunkPos];
-        load_chunk(c, x);
-        double tot[6];
+// Pass 1 for work item (g, c): the chunk total of every lane's track.
+__device__ __forceinline__ void prefix_pass1(const Tables& T, int g, int c, int lane) {
+    const GroupGeom G = group_geom(T, g, lane);
+    float x[kChunkPos];
+    load_chunk(T, G, c, x);
+    double tot[6];
+    double acc = 0;
 #pragma unroll
-        for (int k = 0; k < kChunkPos; ++k) {
-            double acc = static_cast<double>(x[k]);
-            double fresh[6];
-            fresh[0] = acc;
+    for (int k = 0; k < kChunkPos; ++k) {
+        acc = static_cast<double>(x[k]);
+        double fresh[6];
+        fresh[0] = acc;
+        int t = 0;
 #pragma unroll
-            for (int d = 0; d < 5; ++d) {
-                if (((k >> d) & 1) && ((k & ((1 << d) - 1)) == (1 << d) - 1)) {
-                    acc = acc + tot[d];
-                    fresh[d + 1] = acc;
-                }
+        for (int d = 0; d < 5; ++d) {
+            if (((k >> d) & 1) && ((k & ((1 << d) - 1)) == (1 << d) - 1)) {
+                acc = acc + tot[d];
+                fresh[d + 1] = acc;
+                t = d + 1;
             }
-            int t = 0;
-            while (t < 5 && ((k >> t) & 1)) ++t;
+        }
 #pragma unroll
-            for (int d = 0; d < 6; ++d) if (d <= t) tot[d] = fresh[d];
-            if (k == kChunkPos - 1) tree[c * 32 + lane] = acc;  // 31 = all ones: acc is the chunk total
+        for (int d = 0; d < 6; ++d) if (d <= t) tot[d] = fresh[d];
+    }
+    // k = 31 has all five low bits set: acc is the pairwise total of the chunk.
+    T.ptree[(size_t(g) * T.tree_stride + c) * 32 + lane] = acc;
+}
+
+// Tree of aligned block totals for group g (one CTA, `tree` = shared memory
+// of prefix_smem_bytes): level 0 from global, higher levels built here, the
+// whole tree written back.
+__device__ __forceinline__ void prefix_tree(const Tables& T, int g, double* tree) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+    const GroupGeom G = group_geom(T, g, lane);
+    double* gt = T.ptree + size_t(g) * T.tree_stride * 32;
+    for (int c = warp; c < G.nch; c += nwarp) tree[c * 32 + lane] = gt[c * 32 + lane];
+    __syncthreads();
+    int off = 0, cnt = G.nch;
+    while (cnt > 1) {
+        const int up = cnt >> 1;
+        for (int b = warp; b < up; b += nwarp) {
+            const double v = tree[(off + 2 * b + 1) * 32 + lane] + tree[(off + 2 * b) * 32 + lane];
+            tree[(off + cnt + b) * 32 + lane] = v;
+            gt[(off + cnt + b) * 32 + lane] = v;
+        }
+        __syncthreads();
+        off += cnt;
+        cnt = up;
+    }
+}
+
+// Pass 2 for work item (g, c): final prefix values of the chunk.
+__device__ __forceinline__ void prefix_pass2(const Tables& T, int g, int c, int lane) {
+    const GroupGeom G = group_geom(T, g, lane);
+    const double* gt = T.ptree + size_t(g) * T.tree_stride * 32;
+    double add[8];
+    {
+        int off = 0, cnt = G.nch;
+#pragma unroll
+        for (int e = 0; e < 8; ++e) {
+            add[e] = 0.0;
+            if (cnt >= 1 && ((c >> e) & 1)) add[e] = gt[(off + (c >> e) - 1) * 32 + lane];
+            off += cnt;
+            cnt >>= 1;
+        }
+    }
+    float x[kChunkPos];
+    load_chunk(T, G, c, x);
+    double tot[6];
+    const int i0 = c * kChunkPos;
+#pragma unroll
+    for (int k = 0; k < kChunkPos; ++k) {
+        double acc = static_cast<double>(x[k]);
+        double fresh[6];
+        fresh[0] = acc;
+        int t = 0;
+#pragma unroll
+        for (int d = 0; d < 5; ++d) {
+            if (((k >> d) & 1) && ((k & ((1 << d) - 1)) == (1 << d) - 1)) {
+                acc = acc + tot[d];
+                fresh[d + 1] = acc;
+                t = d + 1;
+            }
+        }
+#pragma unroll
+        for (int d = 0; d < 6; ++d) if (d <= t) tot[d] = fresh[d];
+#pragma unroll
+        for (int e = 0; e < 5; ++e)
+            if (e > t && ((k >> e) & 1)) acc = acc + tot[e];
+#pragma unroll
+        for (int e = 0; e < 8; ++e)
+            if ((c >> e) & 1) acc = acc + add[e];
+        const int i = i0 + k;
+        if (G.live && i < G.len) T.presum[G.base + i * G.stride] = acc;
+    }
+}
+
+// Move the dirty-group flags into group_list and clear them (one CTA).  The
+// commits that follow mark the flags again for the next refresh.
+__device__ __forceinline__ void collect_dirty_groups(const Tables& T) {
+    __shared__ int count;
+    if (threadIdx.x == 0) count = 0;
+    __syncthreads();
+    for (int g = threadIdx.x; g < T.n_groups; g += blockDim.x) {
+        if (T.group_flag[g]) {
+            T.group_list[atomicAdd(&count, 1)] = g;
+            T.group_flag[g] = 0u;
         }
     }
     __syncthreads();
-    // Tree of aligned block totals: level e entry b = level e-1 entries 2b+1 + 2b.
-    {
-        int off = 0, cnt = nch;
-        while (cnt > 1) {
-            const int up = cnt >> 1;
-            for (int b = warp; b < up; b += nwarp)
-                tree[(off + cnt + b) * 32 + lane] = tree[(off + 2 * b + 1) * 32 + lane] + tree[(off + 2 * b) * 32 + lane];
-            __syncthreads();
-            off += cnt;
-            cnt = up;
-        }
-    }
-    // Pass 2: final prefix values.
-    for (int c = warp; c < nch; c += nwarp) {
-        double add[8];
-        {
-            int off = 0, cnt = nch;
-#pragma unroll
-            for (int e = 0; e < 8; ++e) {
-                add[e] = 0.0;
-                if (cnt >= 1 && ((c >> e) & 1)) add[e] = tree[(off + (c >> e) - 1) * 32 + lane];
-                off += cnt;
-                cnt >>= 1;
-            }
-        }
-        float x[kChunkPos];
-        load_chunk(c, x);
-        double tot[6];
-        const int i0 = c * kChunkPos;
-#pragma unroll
-        for (int k = 0; k < kChunkPos; ++k) {
-            double acc = static_cast<double>(x[k]);
-            double fresh[6];
-            fresh[0] = acc;
-            int t = 0;
-#pragma unroll
-            for (int d = 0; d < 5; ++d) {
-                if (((k >> d) & 1) && ((k & ((1 << d) - 1)) == (1 << d) - 1)) {
-                    acc = acc + tot[d];
-                    fresh[d + 1] = acc;
-                    t = d + 1;
-                }
-            }
-#pragma unroll
-            for (int d = 0; d < 6; ++d) if (d <= t) tot[d] = fresh[d];
-#pragma unroll
-            for (int e = 0; e < 5; ++e)
-                if (e > t && ((k >> e) & 1)) acc = acc + tot[e];
-#pragma unroll
-            for (int e = 0; e < 8; ++e)
-                if ((c >> e) & 1) acc = acc + add[e];
-            const int i = i0 + k;
-            if (live && i < len) T.presum[base + i * stride] = acc;
-        }
-    }
+    if (threadIdx.x == 0) *T.group_count = count;
+}
+
+// Work items (k, c): chunk c of the k-th dirty group, enumerated as
+// k * tree_chunks + c.
+__device__ __forceinline__ bool prefix_item(const Tables& T, int item, int& g, int& c) {
+    const int k = item / T.tree_chunks;
+    c = item - k * T.tree_chunks;
+    if (k >= *reinterpret_cast<const volatile int*>(T.group_count)) return false;
+    g = T.group_list[k];
+    int l = 0;
+    while (l + 1 <= T.L && g >= T.group_base[l + 1]) ++l;
+    return c < prefix_chunks(along_y(T, l) ? T.Y : T.X);
 }
 
 }  // namespace grb

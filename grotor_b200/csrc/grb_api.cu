@@ -36,12 +36,30 @@ __global__ void k_refresh_cells(Tables T) {
     refresh_dirty_cells(T, warp, nwarps, lane);
 }
 
-__global__ void __launch_bounds__(kRefreshThreads, 2) k_prefix_groups(Tables T) {
+// Prefix rebuild of dirty groups: pass 1 and pass 2 over (group, chunk) work
+// items, one warp each; the tree with one CTA per group.
+__global__ void k_collect_groups(Tables T) { collect_dirty_groups(T); }
+__global__ void __launch_bounds__(256, 2) k_prefix_pass1(Tables T) {
+    const int lane = threadIdx.x & 31;
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nwarps = (gridDim.x * blockDim.x) >> 5;
+    const int items = *T.group_count * T.tree_chunks;
+    for (int item = warp; item < items; item += nwarps) {
+        int g, c;
+        if (prefix_item(T, item, g, c)) prefix_pass1(T, g, c, lane);
+    }
+}
+__global__ void __launch_bounds__(kRefreshThreads) k_prefix_tree(Tables T) {
     extern __shared__ __align__(16) double tree[];
-    const int g = blockIdx.x;
-    if (!T.group_flag[g]) return;
-    refresh_group(T, g, tree);
-    if (threadIdx.x == 0) T.group_flag[g] = 0u;
+    for (int k = blockIdx.x; k < *T.group_count; k += gridDim.x) prefix_tree(T, T.group_list[k], tree);
+}
+__global__ void __launch_bounds__(256, 2) k_prefix_pass2(Tables T) {
+    const int lane = threadIdx.x & 31;
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nwarps = (gridDim.x * blockDim.x) >> 5;
+    const int items = *T.group_count * T.tree_chunks;
+    for (int item = warp; item < items; item += nwarps) {
+        int g, c;
+        if (prefix_item(T, item, g, c)) prefix_pass2(T, g, c, lane);
+    }
 }
 
 // Everything dirty: the state of a fresh database (first refresh is full).
@@ -92,8 +110,9 @@ __global__ void k_commit_vias(Tables T, Plan P, int b, int stamp, int K) {
 }
 
 // Persistent stage: every batch of the plan in one cooperative launch.
-// Per batch: recompute dirty cells -> rebuild dirty prefix groups -> route and
-// commit wires -> commit vias, separated by bounded grid barriers.
+// Per batch: recompute dirty cells (block 0 also lists the dirty prefix
+// groups) -> prefix pass 1 -> prefix trees -> prefix pass 2 -> route and commit
+// wires -> commit vias, separated by bounded grid barriers.
 __global__ void __launch_bounds__(kPersistentThreads, 2) k_lshape_persistent(Tables T, Plan P, GridSync S,
         int stamp0, int nmax, size_t arena_b, char* gscratch, size_t gslot, int* work) {
     extern __shared__ __align__(16) char smem[];
@@ -104,15 +123,23 @@ __global__ void __launch_bounds__(kPersistentThreads, 2) k_lshape_persistent(Tab
     clk.start(S);
     for (int b = 0; b < P.n_batches; ++b) {
         const int stamp = stamp0 + b + 1;
-        // refresh_cost (incremental_update.cuh:98-132): dirty cells, then the
-        // prefix of every group with a changed wire cost.
+        // refresh_cost (incremental_update.cuh:98-132).
+        if (blockIdx.x == 0) collect_dirty_groups(T);
         refresh_dirty_cells(T, gwarp, nwarps, lane);
         if (!grid_sync(S, T)) return;
         clk.mark(S, 4);
-        for (int g = blockIdx.x; g < T.n_groups; g += gridDim.x) {
-            if (!*reinterpret_cast<volatile unsigned*>(T.group_flag + g)) continue;
-            refresh_group(T, g, tree);
-            if (threadIdx.x == 0) T.group_flag[g] = 0u;
+        const int items = *reinterpret_cast<volatile int*>(T.group_count) * T.tree_chunks;
+        for (int item = gwarp; item < items; item += nwarps) {
+            int g, c;
+            if (prefix_item(T, item, g, c)) prefix_pass1(T, g, c, lane);
+        }
+        if (!grid_sync(S, T)) return;
+        for (int k = blockIdx.x; k < *reinterpret_cast<volatile int*>(T.group_count); k += gridDim.x)
+            prefix_tree(T, T.group_list[k], tree);
+        if (!grid_sync(S, T)) return;
+        for (int item = gwarp; item < items; item += nwarps) {
+            int g, c;
+            if (prefix_item(T, item, g, c)) prefix_pass2(T, g, c, lane);
         }
         if (!grid_sync(S, T)) return;
         clk.mark(S, 7);
@@ -470,16 +497,19 @@ int prof_collect(grb_ctx* c) {
 }
 
 int refresh_plain(grb_ctx* c) {
-    Tables& T = c->T;
+    const Tables T = c->T;
     cudaEvent_t e;
     int rc = prof_begin(c, 4, &e);
     if (rc) return rc;
+    k_collect_groups<<<1, 256, 0, c->stream>>>(T);
     k_refresh_cells<<<c->sms * 8, 256, 0, c->stream>>>(T);
     prof_end(c, e);
     if ((rc = prof_begin(c, 7, &e))) return rc;
-    k_prefix_groups<<<T.n_groups, kRefreshThreads, prefix_smem_bytes(std::max(T.X, T.Y)), c->stream>>>(T);
+    k_prefix_pass1<<<c->sms * 8, 256, 0, c->stream>>>(T);
+    k_prefix_tree<<<c->sms * 2, kRefreshThreads, prefix_smem_bytes(std::max(T.X, T.Y)), c->stream>>>(T);
+    k_prefix_pass2<<<c->sms * 8, 256, 0, c->stream>>>(T);
     prof_end(c, e);
-    c->launches += 2;
+    c->launches += 5;
     GRB_CUDA(c, cudaGetLastError());
     return GRB_OK;
 }
@@ -568,7 +598,7 @@ int stage_persistent(grb_ctx* c, int stamp0) {
     const int nmax = dp_nmax(c);
     const size_t ab = arena_bytes(c->T.L, nmax);
     const int wpb = kPersistentThreads / 32;
-    const size_t prefix_smem = prefix_smem_bytes(std::max(c->T.X, c->T.Y));
+    const size_t prefix_smem = prefix_smem_bytes(std::max(c->T.X, c->T.Y));  // prefix_tree
     const size_t smem = std::max(ab * wpb, prefix_smem);
     GRB_CUDA(c, cudaFuncSetAttribute(k_lshape_persistent, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
     int per_sm = 0;
@@ -667,6 +697,11 @@ int grb_create(const grb_grid* g, int32_t device, grb_ctx** out) {
     rc |= dalloc(cp, &T.dirty_wire, c->words, cp->owned);
     rc |= dalloc(cp, &T.dirty_via, c->words, cp->owned);
     rc |= dalloc(cp, &T.group_flag, ng, cp->owned);
+    rc |= dalloc(cp, &T.group_list, ng, cp->owned);
+    rc |= dalloc(cp, &T.group_count, 1, cp->owned);
+    T.tree_chunks = prefix_chunks(std::max(T.X, T.Y));
+    T.tree_stride = prefix_tree_entries(std::max(T.X, T.Y));
+    rc |= dalloc(cp, &T.ptree, size_t(ng) * T.tree_stride * 32, cp->owned);
     rc |= dalloc(cp, &T.wirelength, 1, cp->owned);
     rc |= dalloc(cp, &T.vias, 1, cp->owned);
     rc |= dalloc(cp, &T.error, 2, cp->owned);
@@ -682,7 +717,7 @@ int grb_create(const grb_grid* g, int32_t device, grb_ctx** out) {
     GRB_CUDA(cp, cudaFuncSetAttribute(k_batch_phase3, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
     GRB_CUDA(cp, cudaFuncSetAttribute(k_batch_persistent, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
     GRB_CUDA(cp, cudaFuncSetAttribute(k_lshape_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
-    GRB_CUDA(cp, cudaFuncSetAttribute(k_prefix_groups, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    GRB_CUDA(cp, cudaFuncSetAttribute(k_prefix_tree, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       int(prefix_smem_bytes(std::max(T.X, T.Y)))));
     const int r = grb_reset(cp);
     if (r) { const int code = r; free_all(cp->owned); return code; }
