@@ -113,9 +113,9 @@ def measured_peak():
     return 6650.0, "fallback"
 
 
-def profiled_traffic(kernel: str):
-    """DRAM bytes per launch of `kernel` from the committed ncu summaries
-    (a line 'dram_bytes_per_launch <kernel> <workload> <bytes>'), else None."""
+def profiled_traffic(kernel: str, workload: str):
+    """DRAM bytes per launch of `kernel` on `workload` from the committed ncu
+    summaries (a line 'dram_bytes_per_launch <kernel> <workload> <bytes>'), else None."""
     d = os.path.join(ROOT, "profiles")
     if not os.path.isdir(d):
         return None
@@ -124,7 +124,8 @@ def profiled_traffic(kernel: str):
             continue
         for line in open(os.path.join(d, f)):
             parts = line.strip().strip("`").split()
-            if len(parts) == 4 and parts[0] == "dram_bytes_per_launch" and parts[1] == kernel:
+            if len(parts) == 4 and parts[0] == "dram_bytes_per_launch" and parts[1] == kernel \
+                    and parts[2] == workload:
                 return float(parts[3])
     return None
 
@@ -374,7 +375,7 @@ def run_grotor(args):
     for k, (byt, kms) in kernels.items():
         ach = byt / (kms / 1e3) / 1e9
         roofs[k] = {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
-                    "traffic": profiled_traffic(k), "algorithmic_bytes": byt, "ms": kms,
+                    "traffic": profiled_traffic(k, args.workload), "algorithmic_bytes": byt, "ms": kms,
                     "peak_source": f"{peak_kind} hbm_gbs"}
     result["roofline"] = dict(roofs[dom], kernel=dom)
     result["roofline_all"] = roofs
