@@ -40,6 +40,11 @@ class GrbStats(C.Structure):
     ]
 
 
+class GrbFltDags(C.Structure):
+    _fields_ = [(k, P) for k in ("node_off", "coord", "depth", "children", "parent_end", "edge_off", "edge_parent",
+                                 "edge_source_slot", "route2_off")]
+
+
 class GrbSynthParams(C.Structure):
     _fields_ = [
         ("X", C.c_int32), ("Y", C.c_int32), ("cap_layers", C.c_int32), ("n_nets", C.c_int32),
@@ -69,6 +74,10 @@ SIGNATURES = {
     "grb_lshape_stage": (C.c_int, [P, C.c_int32, C.POINTER(GrbStats)]),
     "grb_ripup_classify": (C.c_int, [P, C.c_int32, P]),
     "grb_ripup_classify_noalloc": (C.c_int, [P, C.c_int32, P]),
+    "grb_upload_geometry": (C.c_int, [P, P, P, P, P, P, P]),
+    "grb_upload_flt": (C.c_int, [P, C.POINTER(GrbFltDags)]),
+    "grb_flt_stage": (C.c_int, [P, C.c_int32, C.c_int32, C.POINTER(GrbStats)]),
+    "grb_read_routes2": (C.c_int, [P, P]),
     "grb_congestion_view": (C.c_int, [P, P, P, P]),
     "grb_read_tables": (C.c_int, [P, P, P, P, P, P]),
     "grb_read_routes": (C.c_int, [P, P]),

@@ -15,6 +15,7 @@
 #include "device/commit.cuh"
 #include "device/common.cuh"
 #include "device/cost.cuh"
+#include "device/flt.cuh"
 #include "device/lshape.cuh"
 
 using namespace grb;
@@ -161,6 +162,72 @@ __global__ void __launch_bounds__(kPersistentThreads, 2) k_lshape_persistent(Tab
         clk.mark(S, 5);
         // Via demand sees every wire timestamp of the batch.
         for (int k = gwarp; k < cnt; k += nwarps) commit_net_vias(T, P, P.ids[lo + k], stamp, 1, lane);
+        if (!grid_sync(S, T)) return;
+        clk.mark(S, 6);
+    }
+}
+
+// --- FLT stage kernels (flt.cuh) --------------------------------------------
+constexpr int kFltThreads = 128;
+
+// One warp per net of batch b: layer-change tables, solve, trace, wires.
+__global__ void __launch_bounds__(kFltThreads) k_flt_batch(Tables T, Flt F, Plan P2, int b, int stamp) {
+    const int lane = threadIdx.x & 31;
+    const int k = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lo = P2.batch_off[b], cnt = P2.batch_off[b + 1] - lo;
+    if (k < cnt) flt_net(T, F, P2, P2.ids[lo + k], stamp, lane, true);
+}
+
+// Persistent FLT stage: per batch, [remove stage-one wires -> remove their
+// vias ->] refresh cells -> prefix pass 1 -> trees -> pass 2 -> FLT nets and
+// wires -> vias, separated by bounded grid barriers (flt.cuh:141-168 order).
+__global__ void __launch_bounds__(kPersistentThreads, 2) k_flt_persistent(Tables T, Flt F, Plan P1, Plan P2,
+        GridSync S, int stamp0, int remove, int* work) {
+    extern __shared__ __align__(16) char smem[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int gwarp = warp * gridDim.x + blockIdx.x, nwarps = gridDim.x * (blockDim.x >> 5);
+    double* tree = reinterpret_cast<double*>(smem);
+    PhaseClock clk;
+    clk.start(S);
+    for (int b = 0; b < P2.n_batches; ++b) {
+        const int lo = P2.batch_off[b], cnt = P2.batch_off[b + 1] - lo;
+        const int stamp = stamp0 + (remove ? 2 * b + 2 : b + 1);
+        if (remove) {
+            for (int k = gwarp; k < cnt; k += nwarps) commit_net_wires(T, P1, P2.ids[lo + k], stamp - 1, -1, lane);
+            if (!grid_sync(S, T)) return;
+            for (int k = gwarp; k < cnt; k += nwarps) commit_net_vias(T, P1, P2.ids[lo + k], stamp - 1, -1, lane);
+            if (!grid_sync(S, T)) return;
+            clk.mark(S, 6);
+        }
+        if (blockIdx.x == 0) collect_dirty_groups(T);
+        refresh_dirty_cells(T, gwarp, nwarps, lane);
+        if (!grid_sync(S, T)) return;
+        clk.mark(S, 4);
+        const int items = *reinterpret_cast<volatile int*>(T.group_count) * T.tree_chunks;
+        for (int item = gwarp; item < items; item += nwarps) {
+            int g, c;
+            if (prefix_item(T, item, g, c)) prefix_pass1(T, g, c, lane);
+        }
+        if (!grid_sync(S, T)) return;
+        for (int k = blockIdx.x; k < *reinterpret_cast<volatile int*>(T.group_count); k += gridDim.x)
+            prefix_tree(T, T.group_list[k], tree);
+        if (!grid_sync(S, T)) return;
+        for (int item = gwarp; item < items; item += nwarps) {
+            int g, c;
+            if (prefix_item(T, item, g, c)) prefix_pass2(T, g, c, lane);
+        }
+        if (!grid_sync(S, T)) return;
+        clk.mark(S, 7);
+        while (true) {
+            int k = 0;
+            if (lane == 0) k = atomicAdd(work + b, 1);
+            k = __shfl_sync(0xffffffffu, k, 0);
+            if (k >= cnt) break;
+            flt_net(T, F, P2, P2.ids[lo + k], stamp, lane, true);
+        }
+        if (!grid_sync(S, T)) return;
+        clk.mark(S, 5);
+        for (int k = gwarp; k < cnt; k += nwarps) commit_net_vias(T, P2, P2.ids[lo + k], stamp, 1, lane);
         if (!grid_sync(S, T)) return;
         clk.mark(S, 6);
     }
@@ -369,6 +436,18 @@ struct grb_ctx {
     unsigned *cellmask = nullptr, *localmask = nullptr, *fmask = nullptr, *pred = nullptr, *fullmask = nullptr;
     int *bcount = nullptr, *ncolors = nullptr, *batch_of = nullptr, *brank = nullptr, *order = nullptr;
     int bW = 0, bn_cap = 0;
+    // FLT stage (grb_upload_geometry / grb_upload_flt)
+    std::vector<void*> geom_bufs;     // batching geometry replacing the uploaded one
+    std::vector<void*> flt_bufs;
+    Flt F{};
+    long long route2_words = 0;
+    int flt_n = -1;                   // nets covered by the uploaded DAGs
+    std::vector<int> h_flt_node_off;
+    std::vector<long long> h_route2_off;
+    int flt_version = 0;
+    cudaGraphExec_t flt_graph = nullptr;
+    long long flt_graph_key[4] = {-1, -1, -1, -1};
+    int64_t flt_graph_kernels = 0;
     // graph cache
     cudaGraphExec_t graph = nullptr;
     int graph_version = -1, graph_stamp = -1;
@@ -440,6 +519,14 @@ Plan make_plan(const grb_ctx* c) {
     P.node_off = c->node_off; P.nodes = c->nodes; P.parents = c->parents;
     P.route_off = c->route_off; P.routes = c->routes;
     P.ids = c->ids; P.batch_off = c->batch_off; P.n_batches = c->n_batches;
+    return P;
+}
+
+// The plan with the phase-two routes of the FLT stage.
+Plan make_plan2(const grb_ctx* c) {
+    Plan P = make_plan(c);
+    P.route_off = c->F.route2_off;
+    P.routes = c->F.routes2;
     return P;
 }
 
@@ -558,6 +645,97 @@ int stage_plain(grb_ctx* c, int stamp0) {
         if (!rc) rc = commit_plain(c, b, stamp, 1);
         if (rc) return rc;
     }
+    return GRB_OK;
+}
+
+// --- FLT stage executors ---------------------------------------------------
+int flt_stamps(const grb_ctx* c, int remove) { return c->n_batches * (remove ? 2 : 1); }
+
+int flt_stage_plain(grb_ctx* c, int stamp0, int remove) {
+    const Plan P1 = make_plan(c), P2 = make_plan2(c);
+    for (int b = 0; b < c->n_batches; ++b) {
+        const int cnt = c->h_batch_off[b + 1] - c->h_batch_off[b];
+        if (cnt <= 0) continue;
+        const int stamp = stamp0 + (remove ? 2 * b + 2 : b + 1);
+        const int cblocks = std::min((cnt + 3) / 4, 1056);  // demand.cuh:316
+        int rc;
+        cudaEvent_t e;
+        if (remove) {  // flt.cuh:143-150
+            if ((rc = prof_begin(c, 6, &e))) return rc;
+            k_commit_wires<<<cblocks, 128, 0, c->stream>>>(c->T, P1, b, stamp - 1, -1);
+            k_commit_vias<<<cblocks, 128, 0, c->stream>>>(c->T, P1, b, stamp - 1, -1);
+            prof_end(c, e);
+            c->launches += 2;
+        }
+        if ((rc = refresh_plain(c))) return rc;
+        if ((rc = prof_begin(c, 5, &e))) return rc;
+        k_flt_batch<<<(cnt + kFltThreads / 32 - 1) / (kFltThreads / 32), kFltThreads, 0, c->stream>>>(c->T, c->F, P2, b,
+                                                                                                      stamp);
+        prof_end(c, e);
+        if ((rc = prof_begin(c, 6, &e))) return rc;
+        k_commit_vias<<<cblocks, 128, 0, c->stream>>>(c->T, P2, b, stamp, 1);
+        prof_end(c, e);
+        c->launches += 2;
+        GRB_CUDA(c, cudaGetLastError());
+    }
+    return GRB_OK;
+}
+
+int flt_stage_graph(grb_ctx* c, int stamp0, int remove) {
+    const long long key[4] = {c->plan_version, c->flt_version, stamp0, remove};
+    if (!c->flt_graph || !std::equal(key, key + 4, c->flt_graph_key)) {
+        if (c->flt_graph) { cudaGraphExecDestroy(c->flt_graph); c->flt_graph = nullptr; }
+        const int64_t before = c->launches;
+        const bool prof = c->profiling;
+        c->profiling = false;
+        cudaGraph_t g = nullptr;
+        GRB_CUDA(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+        const int rc = flt_stage_plain(c, stamp0, remove);
+        const cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+        c->profiling = prof;
+        if (rc) { if (g) cudaGraphDestroy(g); return rc; }
+        if (e != cudaSuccess) return cuda_fail(c, e, "cudaStreamEndCapture");
+        const cudaError_t ei = cudaGraphInstantiate(&c->flt_graph, g, 0);
+        cudaGraphDestroy(g);
+        if (ei != cudaSuccess) return cuda_fail(c, ei, "cudaGraphInstantiate");
+        c->flt_graph_kernels = c->launches - before;
+        c->launches = before;
+        std::copy(key, key + 4, c->flt_graph_key);
+    }
+    GRB_CUDA(c, cudaGraphLaunch(c->flt_graph, c->stream));
+    c->launches += c->flt_graph_kernels;
+    return GRB_OK;
+}
+
+int ensure_work(grb_ctx* c) {
+    if (c->work_cap < c->n_batches) {
+        if (c->work) cudaFree(c->work);
+        c->work = nullptr;
+        if (cudaMalloc(&c->work, sizeof(int) * c->n_batches) != cudaSuccess) { cudaGetLastError(); return fail(c, GRB_ENOMEM, "work counters"); }
+        c->work_cap = c->n_batches;
+    }
+    GRB_CUDA(c, cudaMemsetAsync(c->work, 0, sizeof(int) * std::max(c->n_batches, 1), c->stream));
+    return GRB_OK;
+}
+
+int flt_stage_persistent(grb_ctx* c, int stamp0, int remove) {
+    if (c->n_batches == 0) return GRB_OK;
+    const size_t smem = prefix_smem_bytes(std::max(c->T.X, c->T.Y));
+    GRB_CUDA(c, cudaFuncSetAttribute(k_flt_persistent, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+    int per_sm = 0;
+    GRB_CUDA(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_flt_persistent, kPersistentThreads, smem));
+    if (per_sm < 1) return fail(c, GRB_EINVAL, "persistent FLT kernel does not fit on an SM");
+    int rc = ensure_work(c);
+    if (rc) return rc;
+    GRB_CUDA(c, cudaMemsetAsync(c->sync, 0, 2 * sizeof(unsigned), c->stream));
+    Tables T = c->T;
+    Flt F = c->F;
+    Plan P1 = make_plan(c), P2 = make_plan2(c);
+    GridSync S{c->sync, c->sync + 1, kBarrierTimeoutNs, c->profiling ? c->d_phase : nullptr};
+    void* args[] = {&T, &F, &P1, &P2, &S, &stamp0, &remove, &c->work};
+    GRB_CUDA(c, cudaLaunchCooperativeKernel((void*)k_flt_persistent, dim3(per_sm * c->sms), dim3(kPersistentThreads),
+                                            args, smem, c->stream));
+    c->launches += 1;
     return GRB_OK;
 }
 
@@ -730,7 +908,10 @@ void grb_destroy(grb_ctx* c) {
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
     if (c->graph) cudaGraphExecDestroy(c->graph);
+    if (c->flt_graph) cudaGraphExecDestroy(c->flt_graph);
     free_all(c->net_bufs);
+    free_all(c->geom_bufs);
+    free_all(c->flt_bufs);
     free_all(c->owned);
     for (void* p : {(void*)c->ids, (void*)c->batch_off, (void*)c->gscratch, (void*)c->work, (void*)c->cellmask,
                     (void*)c->localmask, (void*)c->fmask, (void*)c->pred, (void*)c->fullmask, (void*)c->bcount,
@@ -799,11 +980,14 @@ int grb_upload_nets(grb_ctx* c, const grb_nets* nets) {
     }
     // Reuse the device buffers when every array still fits.
     const long long need[6] = {n, nn, rw, np, nh, nv};
-    bool fits = !c->net_bufs.empty();
+    bool fits = !c->net_bufs.empty() && c->geom_bufs.empty();
     for (int k = 0; k < 6 && fits; ++k) fits = need[k] <= c->net_cap[k];
     if (!fits) {
         GRB_CUDA(c, cudaStreamSynchronize(c->stream));
         free_all(c->net_bufs);
+        free_all(c->geom_bufs);
+        free_all(c->flt_bufs);
+        c->flt_n = -1;
         int rc = 0;
         rc |= dalloc(c, &c->node_off, n + 1, c->net_bufs);
         rc |= dalloc(c, &c->nodes, nn, c->net_bufs);
@@ -841,6 +1025,167 @@ int grb_upload_nets(grb_ctx* c, const grb_nets* nets) {
     c->n_nets = n;
     c->max_nodes = int(maxn);
     c->route_words = rw;
+    c->flt_n = -1;  // FLT DAGs refer to the previous nets
+    return GRB_OK;
+}
+
+int grb_upload_geometry(grb_ctx* c, const int32_t* point_off, const int32_t* points, const int32_t* hseg_off,
+                        const int32_t* hsegs, const int32_t* vseg_off, const int32_t* vsegs) {
+    if (!c) return GRB_EINVAL;
+    if (!c->node_off) return fail(c, GRB_EINVAL, "no nets uploaded");
+    if (!point_off || !hseg_off || !vseg_off) return fail(c, GRB_EINVAL, "geometry offsets missing");
+    GRB_CUDA(c, cudaSetDevice(c->device));
+    const int n = c->n_nets, XY = c->T.XY;
+    const int* offs[3] = {point_off, hseg_off, vseg_off};
+    const int* data[3] = {points, hsegs, vsegs};
+    const int width[3] = {1, 2, 2};
+    for (int k = 0; k < 3; ++k) {
+        if (offs[k][0] != 0) return fail(c, GRB_EINVAL, "geometry offsets must start at 0");
+        for (int i = 0; i < n; ++i) if (offs[k][i + 1] < offs[k][i]) return fail(c, GRB_EINVAL, "geometry offsets must be non-decreasing");
+        if (offs[k][n] && !data[k]) return fail(c, GRB_EINVAL, "geometry data missing");
+        for (long long q = 0; q < (long long)offs[k][n] * width[k]; ++q)
+            if (data[k][q] < 0 || data[k][q] >= XY) return fail(c, GRB_EINVAL, "batching geometry outside the grid");
+    }
+    GRB_CUDA(c, cudaStreamSynchronize(c->stream));
+    free_all(c->geom_bufs);
+    int* d[6];
+    int rc = 0;
+    rc |= dalloc(c, &d[0], n + 1, c->geom_bufs);
+    rc |= dalloc(c, &d[1], point_off[n], c->geom_bufs);
+    rc |= dalloc(c, &d[2], n + 1, c->geom_bufs);
+    rc |= dalloc(c, &d[3], 2 * size_t(hseg_off[n]), c->geom_bufs);
+    rc |= dalloc(c, &d[4], n + 1, c->geom_bufs);
+    rc |= dalloc(c, &d[5], 2 * size_t(vseg_off[n]), c->geom_bufs);
+    if (rc) { free_all(c->geom_bufs); return GRB_ENOMEM; }
+    for (int k = 0; k < 3; ++k) {
+        GRB_CUDA(c, cudaMemcpyAsync(d[2 * k], offs[k], sizeof(int) * (n + 1), cudaMemcpyHostToDevice, c->stream));
+        if (offs[k][n])
+            GRB_CUDA(c, cudaMemcpyAsync(d[2 * k + 1], data[k], sizeof(int) * width[k] * size_t(offs[k][n]),
+                                        cudaMemcpyHostToDevice, c->stream));
+    }
+    GRB_CUDA(c, cudaStreamSynchronize(c->stream));
+    c->point_off = d[0]; c->points = d[1]; c->hseg_off = d[2]; c->hsegs = d[3]; c->vseg_off = d[4]; c->vsegs = d[5];
+    return GRB_OK;
+}
+
+int grb_upload_flt(grb_ctx* c, const grb_flt_dags* d) {
+    if (!c) return GRB_EINVAL;
+    if (!c->node_off) return fail(c, GRB_EINVAL, "no nets uploaded");
+    if (!d || !d->node_off || !d->edge_off || !d->route2_off) return fail(c, GRB_EINVAL, "FLT DAG offsets missing");
+    if (c->T.L != kFltLayers - 1) return fail(c, GRB_EINVAL, "the FLT stage needs 9 routing layers (MAX_LAYER 10)");
+    GRB_CUDA(c, cudaSetDevice(c->device));
+    const Tables& T = c->T;
+    const int n = c->n_nets, XY = T.XY;
+    if (d->node_off[0] != 0 || d->edge_off[0] != 0 || d->route2_off[0] != 0) return fail(c, GRB_EINVAL, "FLT offsets must start at 0");
+    for (int i = 0; i < n; ++i)
+        if (d->node_off[i + 1] < d->node_off[i] || d->edge_off[i + 1] < d->edge_off[i] || d->route2_off[i + 1] < d->route2_off[i])
+            return fail(c, GRB_EINVAL, "FLT offsets must be non-decreasing");
+    const long long nn = d->node_off[n], ne = d->edge_off[n];
+    if ((nn && (!d->coord || !d->depth || !d->children || !d->parent_end)) || (ne && (!d->edge_parent || !d->edge_source_slot)))
+        return fail(c, GRB_EINVAL, "FLT DAG arrays missing");
+    // Host validation (every index the kernels dereference) and the derived
+    // per-node arrays: global child offsets, depth-sorted order, level offsets.
+    std::vector<int> child_off(size_t(nn) + 1), order(nn), eslot(ne), lvl_off(n + 1, 0), level;
+    long long children = 0;
+    for (int id = 0; id < n; ++id) {
+        const int nb = d->node_off[id], N = d->node_off[id + 1] - nb;
+        const int eb = d->edge_off[id], E = d->edge_off[id + 1] - eb;
+        lvl_off[id] = int(level.size());
+        if (N == 0) {
+            if (E) return fail(c, GRB_EINVAL, "FLT edges without nodes");
+            continue;
+        }
+        if (N >= (1ll << 31) / 100 - 1) return fail(c, GRB_EINVAL, "FLT DAG too large for packed candidate ids");
+        int maxd = 0;
+        for (int i = 0; i < N; ++i) {
+            const int g = nb + i;
+            const int cd = d->coord[g], dp = d->depth[g], ch = d->children[g];
+            if (cd < 0 || cd / XY > kFltLayers - 1) return fail(c, GRB_EINVAL, "FLT node outside the grid");
+            if (dp < 0 || dp >= 5000) return fail(c, GRB_EINVAL, "FLT depth out of range");  // flt_topology.hpp:58
+            if (ch < 0 || ch > kFltMaxChildren) return fail(c, GRB_EINVAL, "FLT node with more than 6 child slots");
+            const int pb = i ? d->parent_end[g - 1] : 0, pe = d->parent_end[g];
+            if (pe < pb || pe > E) return fail(c, GRB_EINVAL, "FLT parent ranges inconsistent");
+            child_off[g] = int(children);
+            children += ch;
+            maxd = std::max(maxd, dp);
+        }
+        if (d->parent_end[nb + N - 1] != E) return fail(c, GRB_EINVAL, "FLT parent ranges do not cover the edges");
+        for (int i = 0; i < N; ++i) {
+            const int g = nb + i;
+            const int pb = i ? d->parent_end[g - 1] : 0, pe = d->parent_end[g];
+            const int cx = d->coord[g] % XY / T.Y, cy = d->coord[g] % T.Y;
+            for (int e = eb + pb; e < eb + pe; ++e) {
+                const int p = d->edge_parent[e], src = d->edge_source_slot[e];
+                if (p < 0 || p >= N || src < 0 || src / 10 != i) return fail(c, GRB_EINVAL, "FLT edge endpoints inconsistent");
+                if (d->depth[nb + p] >= d->depth[g]) return fail(c, GRB_EINVAL, "FLT parent not shallower than child");
+                if (src % 10 >= d->children[nb + p]) return fail(c, GRB_EINVAL, "FLT child slot out of range");
+                const int px = d->coord[nb + p] % XY / T.Y, py = d->coord[nb + p] % T.Y;
+                if (px != cx && py != cy) return fail(c, GRB_EINVAL, "FLT edge is not straight");
+                eslot[e] = src;
+            }
+        }
+        std::vector<int> cnt(maxd + 2, 0);
+        for (int i = 0; i < N; ++i) ++cnt[d->depth[nb + i] + 1];
+        for (int q = 0; q <= maxd; ++q) cnt[q + 1] += cnt[q];
+        for (int q = 0; q <= maxd + 1; ++q) level.push_back(cnt[q]);
+        for (int i = 0; i < N; ++i) order[nb + cnt[d->depth[nb + i]]++] = i;  // stable by index
+    }
+    lvl_off[n] = int(level.size());
+    if (children >= (1ll << 31) / kFltLayers) return fail(c, GRB_EINVAL, "too many FLT child slots");
+    child_off[nn] = int(children);
+    for (int i = 0; i < n; ++i) {
+        if (d->node_off[i + 1] > d->node_off[i] && d->route2_off[i + 1] - d->route2_off[i] < 1)
+            return fail(c, GRB_EINVAL, "FLT net without phase-two route storage");
+    }
+    const long long rw = d->route2_off[n];
+    GRB_CUDA(c, cudaStreamSynchronize(c->stream));
+    free_all(c->flt_bufs);
+    c->flt_n = -1;
+    Flt F{};
+    int *node_off, *edge_off, *lvl, *levelp, *coord, *ch, *coff, *pend, *ord, *epar, *es, *lo, *bc, *r2;
+    long long* r2off;
+    double *costs, *ce;
+    unsigned long long *packed, *best;
+    int rc = 0;
+    std::vector<void*>& B = c->flt_bufs;
+    rc |= dalloc(c, &node_off, n + 1, B); rc |= dalloc(c, &edge_off, n + 1, B);
+    rc |= dalloc(c, &lvl, n + 1, B); rc |= dalloc(c, &levelp, level.size(), B);
+    rc |= dalloc(c, &r2off, n + 1, B); rc |= dalloc(c, &r2, std::max<long long>(rw, 1), B);
+    rc |= dalloc(c, &coord, nn, B); rc |= dalloc(c, &ch, nn, B); rc |= dalloc(c, &coff, nn + 1, B);
+    rc |= dalloc(c, &pend, nn, B); rc |= dalloc(c, &ord, nn, B); rc |= dalloc(c, &lo, nn, B);
+    rc |= dalloc(c, &epar, ne, B); rc |= dalloc(c, &es, ne, B);
+    rc |= dalloc(c, &costs, size_t(nn) * kFltLayers, B);
+    rc |= dalloc(c, &packed, size_t(children) * kFltLayers, B);
+    rc |= dalloc(c, &best, size_t(children) * kFltLayers, B);
+    rc |= dalloc(c, &ce, size_t(ne) * 81, B); rc |= dalloc(c, &bc, size_t(ne) * 81, B);
+    if (rc) { free_all(B); return GRB_ENOMEM; }
+    auto h2d = [&](void* dst, const void* src, size_t bytes) {
+        return bytes ? cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, c->stream) : cudaSuccess;
+    };
+    GRB_CUDA(c, h2d(node_off, d->node_off, 4 * (n + 1)));
+    GRB_CUDA(c, h2d(edge_off, d->edge_off, 4 * (n + 1)));
+    GRB_CUDA(c, h2d(lvl, lvl_off.data(), 4 * (n + 1)));
+    GRB_CUDA(c, h2d(levelp, level.data(), 4 * level.size()));
+    GRB_CUDA(c, h2d(r2off, d->route2_off, 8 * (n + 1)));
+    GRB_CUDA(c, cudaMemsetAsync(r2, 0, 4 * std::max<long long>(rw, 1), c->stream));
+    GRB_CUDA(c, h2d(coord, d->coord, 4 * nn));
+    GRB_CUDA(c, h2d(ch, d->children, 4 * nn));
+    GRB_CUDA(c, h2d(coff, child_off.data(), 4 * (nn + 1)));
+    GRB_CUDA(c, h2d(pend, d->parent_end, 4 * nn));
+    GRB_CUDA(c, h2d(ord, order.data(), 4 * nn));
+    GRB_CUDA(c, h2d(epar, d->edge_parent, 4 * ne));
+    GRB_CUDA(c, h2d(es, eslot.data(), 4 * ne));
+    GRB_CUDA(c, cudaStreamSynchronize(c->stream));
+    F.node_off = node_off; F.edge_off = edge_off; F.lvl_off = lvl; F.level = levelp; F.route2_off = r2off;
+    F.coord = coord; F.children = ch; F.child_off = coff; F.pend = pend; F.order = ord;
+    F.eparent = epar; F.eslot = es; F.costs = costs; F.packed = packed; F.best = best; F.lo = lo;
+    F.ce = ce; F.bc = bc; F.routes2 = r2;
+    c->F = F;
+    c->route2_words = rw;
+    c->flt_n = n;
+    c->h_flt_node_off.assign(d->node_off, d->node_off + n + 1);
+    c->h_route2_off.assign(d->route2_off, d->route2_off + n + 1);
+    ++c->flt_version;
     return GRB_OK;
 }
 
@@ -1032,6 +1377,47 @@ int grb_lshape_stage(grb_ctx* c, int32_t mode, grb_stats* stats) {
     c->dag_ms = ms;
     if ((rc = prof_collect(c))) return rc;
     return stats ? grb_get_stats(c, stats) : GRB_OK;
+}
+
+int grb_flt_stage(grb_ctx* c, int32_t remove_phase_one, int32_t mode, grb_stats* stats) {
+    if (!c) return GRB_EINVAL;
+    if (c->flt_n != c->n_nets || c->flt_n < 0) return fail(c, GRB_EINVAL, "no FLT DAGs uploaded for the current nets");
+    GRB_CUDA(c, cudaSetDevice(c->device));
+    std::vector<int> ids(c->plan_n);
+    if (c->plan_n) {
+        GRB_CUDA(c, cudaMemcpyAsync(ids.data(), c->ids, sizeof(int) * c->plan_n, cudaMemcpyDeviceToHost, c->stream));
+        GRB_CUDA(c, cudaStreamSynchronize(c->stream));
+    }
+    for (int id : ids)
+        if (c->h_flt_node_off[id + 1] == c->h_flt_node_off[id]) return fail(c, GRB_EINVAL, "plan net " + std::to_string(id) + " has no FLT DAG");
+    const int remove = remove_phase_one ? 1 : 0;
+    const int stamp0 = c->stamp;
+    GRB_CUDA(c, cudaEventRecord(c->ev0, c->stream));
+    int rc;
+    if (mode == GRB_MODE_PLAIN) rc = flt_stage_plain(c, stamp0, remove);
+    else if (mode == GRB_MODE_GRAPH) rc = flt_stage_graph(c, stamp0, remove);
+    else if (mode == GRB_MODE_PERSISTENT) rc = flt_stage_persistent(c, stamp0, remove);
+    else return fail(c, GRB_EINVAL, "unknown mode");
+    if (rc) return rc;
+    GRB_CUDA(c, cudaEventRecord(c->ev1, c->stream));
+    c->stamp = stamp0 + flt_stamps(c, remove);
+    rc = check_device_error(c);
+    if (rc) return rc;
+    float ms = 0;
+    GRB_CUDA(c, cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+    c->dag_ms = ms;
+    if ((rc = prof_collect(c))) return rc;
+    return stats ? grb_get_stats(c, stats) : GRB_OK;
+}
+
+int grb_read_routes2(grb_ctx* c, int32_t* routes2) {
+    if (!c || !routes2) return GRB_EINVAL;
+    if (c->flt_n < 0) return fail(c, GRB_EINVAL, "no FLT DAGs uploaded");
+    GRB_CUDA(c, cudaSetDevice(c->device));
+    if (c->route2_words)
+        GRB_CUDA(c, cudaMemcpyAsync(routes2, c->F.routes2, sizeof(int) * c->route2_words, cudaMemcpyDeviceToHost, c->stream));
+    GRB_CUDA(c, cudaStreamSynchronize(c->stream));
+    return GRB_OK;
 }
 
 int grb_ripup_classify(grb_ctx* c, int32_t threshold, uint8_t* is_of) {

@@ -186,6 +186,35 @@ class Router:
         self._check(self._lib.grb_lshape_stage(self._ctx, mode_id(mode), C.byref(st)))
         return _stats_dict(st)
 
+    # ---- FLT stage ----------------------------------------------------------
+    def upload_geometry(self, point_off, points, hseg_off, hsegs, vseg_off, vsegs):
+        """Replace the batching geometry (net::points and RSMT segments after the
+        FLT DAG builder) so that ``generate_batches_rsmt`` batches the FLT stage."""
+        a = [_c(v, np.int32) for v in (point_off, points, hseg_off, hsegs, vseg_off, vsegs)]
+        self._check(self._lib.grb_upload_geometry(self._ctx, *[_p(v) for v in a]))
+
+    def upload_flt(self, dags: dict, route2_off):
+        """Upload FLT DAGs (CSR by net id: node_off, coord, depth, children,
+        parent_end, edge_off, edge_parent, edge_source_slot) and the phase-two
+        route offsets (int64, n+1)."""
+        keep = {k: _c(dags[k], np.int32) for k in ("node_off", "coord", "depth", "children", "parent_end",
+                                                    "edge_off", "edge_parent", "edge_source_slot")}
+        keep["route2_off"] = _c(route2_off, np.int64)
+        d = _abi.GrbFltDags(**{k: v.ctypes.data for k, v in keep.items()})
+        self._check(self._lib.grb_upload_flt(self._ctx, C.byref(d)))
+        self._route2_words = int(keep["route2_off"][-1])
+
+    def flt_route(self, mode="persistent", remove_phase_one: bool = True) -> dict:
+        """route_prepared_topology's batch loop over the current plan."""
+        st = _abi.GrbStats()
+        self._check(self._lib.grb_flt_stage(self._ctx, int(bool(remove_phase_one)), mode_id(mode), C.byref(st)))
+        return _stats_dict(st)
+
+    def read_routes2(self) -> np.ndarray:
+        out = np.zeros(getattr(self, "_route2_words", 0), np.int32)
+        self._check(self._lib.grb_read_routes2(self._ctx, _p(out)))
+        return out
+
     def ripup(self, threshold: int = 0) -> np.ndarray:
         out = np.zeros(self.nets.n if self.nets else 0, np.uint8)
         self._check(self._lib.grb_ripup_classify(self._ctx, int(threshold), _p(out)))

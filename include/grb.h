@@ -151,6 +151,53 @@ int grb_ripup_classify(grb_ctx* ctx, int32_t threshold, uint8_t* is_of);
  * device at once -- race; serialise them.  Results equal grb_ripup_classify's. */
 int grb_ripup_classify_noalloc(grb_ctx* ctx, int32_t threshold, uint8_t* is_of);
 
+/* ---- FLT stage (stage two of the default pipeline, flt.cuh:75-182) ------ */
+
+/* Replace the batching geometry of the uploaded nets (net::points and
+ * rsmt_h/v_segments after the FLT DAG builder has added its detour points,
+ * preprocess.hpp:1002-1019) so that grb_plan_batches batches the FLT stage
+ * (flt.cuh:92, limit 300000).  CSR by net id over the uploaded nets. */
+int grb_upload_geometry(grb_ctx* ctx, const int32_t* point_off, const int32_t* points,
+                        const int32_t* hseg_off, const int32_t* hsegs,
+                        const int32_t* vseg_off, const int32_t* vsegs);
+
+/* FLT DAGs of the stage's nets, CSR by net id over the uploaded nets (nets
+ * outside the stage have empty ranges).  Exactly the reference's compact
+ * topology (flt::Topology::emit, flt_topology.hpp:52-70; flt::Node/Edge,
+ * :15-16): per node its 3-D coordinate (layer 9 = no pin layer), depth,
+ * child-slot count and cumulative parent-edge count within the net; per edge,
+ * grouped by child node, the parent (net-local) and the source slot
+ * child * 10 + slot index at the parent.  route2_off gives each net's
+ * phase-two route words (the reference reserves 100 per pin,
+ * router_state.hpp:33, at pin_acc_num_phase2). */
+typedef struct grb_flt_dags {
+    const int32_t* node_off;     /* [n+1] */
+    const int32_t* coord;
+    const int32_t* depth;
+    const int32_t* children;     /* <= 6 (flt_block.cuh:31-32) */
+    const int32_t* parent_end;
+    const int32_t* edge_off;     /* [n+1] */
+    const int32_t* edge_parent;
+    const int32_t* edge_source_slot;
+    const int64_t* route2_off;   /* [n+1] */
+} grb_flt_dags;
+
+/* Upload FLT DAGs (host buffers; replaces flt::Workspace upload/assemble,
+ * flt_workspace.cuh:156-224, and its CUB scan and depth sort).  Needs L == 9
+ * routing layers (MAX_LAYER 10, flt_cost.cuh:14). */
+int grb_upload_flt(grb_ctx* ctx, const grb_flt_dags* dags);
+
+/* Run the FLT stage over the current plan (route_prepared_topology's batch
+ * loop, flt.cuh:141-168): per batch, when remove_phase_one, remove the nets'
+ * stage-one routes (commit with K = -1 under its own stamp), then ++stamp,
+ * refresh_cost, layer-change tables (precompute_cost_edge), DAG solve and
+ * trace (route_flt_block) into the phase-two routes, and commit of the
+ * phase-two routes.  mode: GRB_MODE_PLAIN, GRAPH or PERSISTENT. */
+int grb_flt_stage(grb_ctx* ctx, int32_t remove_phase_one, int32_t mode, grb_stats* stats);
+
+/* Copy all phase-two route words (route2_off[n] words) to the host. */
+int grb_read_routes2(grb_ctx* ctx, int32_t* routes2);
+
 /* Congestion view for the FLT topology builder (congestion.cuh:60-112). */
 int grb_congestion_view(grb_ctx* ctx, uint8_t* congestion, float* xsum, float* ysum);
 

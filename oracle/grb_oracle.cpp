@@ -536,3 +536,290 @@ int orc_lshape_stage(const orc_grid* g, int32_t n_batches, const int32_t* batch_
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// FLT stage (flt.cuh:75-182, flt_cost.cuh:25-130, flt_block.cuh:6-355).
+namespace {
+
+constexpr int kFltLayers = 10;                         // MAX_LAYER, flt_cost.cuh:14
+constexpr uint64_t kFltInit = 7208259049189261824ULL;  // init_cost_with_road, flt_cost.cuh:48
+constexpr int kStraight = 82;                          // "no layer change" choice, flt_block.cuh:109
+
+// flt_cost.cuh:25-46: a float cost in an order-preserving int32 in the high
+// word, the candidate id in the low word.
+int32_t flt_ordered(float f) {
+    int32_t i;
+    std::memcpy(&i, &f, 4);
+    return i >= 0 ? i : i ^ 0x7FFFFFFF;
+}
+uint64_t flt_pack(float cost, int id) {
+    return (uint64_t(uint32_t(flt_ordered(cost))) << 32) | uint32_t(id);
+}
+double flt_unpack_cost(uint64_t p) {
+    int32_t i = int32_t(p >> 32);
+    i = i >= 0 ? i : i ^ 0x7FFFFFFF;
+    float f;
+    std::memcpy(&f, &i, 4);
+    return double(f);
+}
+
+// One net: layer-change tables, solve (deepest level first), trace (root
+// first).  Nodes of one depth are visited in ascending node index, the order
+// of the reference's stable depth sort (flt_workspace.cuh:216-217); the
+// reference appends segments with atomics, so its order within a level may
+// differ while the segment multiset is the same.
+int flt_net(const Grid& G, const orc_flt* D, const float* vcost, const double* presum, int id,
+            int32_t* r, int64_t cap) {
+    const int nb = D->node_off[id], N = D->node_off[id + 1] - nb;
+    const int eb = D->edge_off[id], E = D->edge_off[id + 1] - eb;
+    if (N <= 0) return 0;
+    const int X = G.X, Y = G.Y, XY = X * Y, L = G.L;
+    const int* crd = D->coord + nb;
+    const int* dep = D->depth + nb;
+    const int* nch = D->children + nb;
+    const int* pend = D->parent_end + nb;
+    const int* epar = D->edge_parent + eb;
+    const int* eslot = D->edge_slot + eb;
+    auto wire = [&](int l, int xmin, int xmax, int ymin, int ymax) {  // prefix_scan.cuh:10-40
+        return presum[G.idx(l, xmax, ymax)] - presum[G.idx(l, xmin, ymin)];
+    };
+    auto pbeg = [&](int i) { return i ? pend[i - 1] : 0; };
+    std::vector<int> coff(N + 1, 0);
+    int maxd = 0;
+    for (int i = 0; i < N; ++i) { coff[i + 1] = coff[i] + nch[i]; maxd = std::max(maxd, dep[i]); }
+    std::vector<int> lvl_off(maxd + 2, 0), order(N);
+    for (int i = 0; i < N; ++i) ++lvl_off[dep[i] + 1];
+    for (int d = 0; d <= maxd; ++d) lvl_off[d + 1] += lvl_off[d];
+    {
+        std::vector<int> fill(lvl_off.begin(), lvl_off.end() - 1);
+        for (int i = 0; i < N; ++i) order[fill[dep[i]]++] = i;
+    }
+    // precompute_cost_edge (flt_cost.cuh:50-130): per edge and from-layer, the
+    // best of <= 19 sampled change positions per same-parity to-layer.
+    std::vector<double> ce(size_t(E) * 81, kInf);
+    std::vector<int> bc(size_t(E) * 81, -1);
+    for (int e = 0; e < E; ++e) {
+        const int from = eslot[e] / 10, to = epar[e];
+        const int tox = crd[to] / Y % X, toy = crd[to] % Y, fromx = crd[from] / Y % X, fromy = crd[from] % Y;
+        for (int fl = 0; fl < 9; ++fl) {
+            const bool ay = ((fl & 1) ^ G.DIR) != 0;
+            if ((!ay && fromy != toy) || (ay && fromx != tox)) continue;  // rows stay INF
+            const int distance = std::abs(tox - fromx) + std::abs(toy - fromy);
+            if (!distance) continue;
+            const int dd = distance / std::min(distance, 20);
+            const bool vertical = fromx == tox;
+            const int start = vertical ? std::min(fromy, toy) : std::min(fromx, tox);
+            const int end = vertical ? std::max(fromy, toy) : std::max(fromx, tox);
+            for (int tl = 0; tl < 9; ++tl) {
+                if ((tl % 2) != (fl % 2)) continue;
+                double best = kInf;
+                int pos = -1;
+                for (int sp = start + dd; sp < end; sp += dd) {
+                    const int sx = vertical ? fromx : sp, sy = vertical ? sp : fromy;
+                    double via = 0;
+                    for (int ll = std::min(fl, tl); ll < std::max(fl, tl); ++ll) via += vcost[G.idx(ll, sx, sy)];
+                    double c = via;
+                    if (vertical)
+                        c += (wire(fl, fromx, fromx, std::min(fromy, sy), std::max(fromy, sy)) +
+                              wire(tl, tox, tox, std::min(toy, sy), std::max(toy, sy)));
+                    else
+                        c += (wire(fl, std::min(fromx, sx), std::max(fromx, sx), fromy, fromy) +
+                              wire(tl, std::min(tox, sx), std::max(tox, sx), toy, toy));
+                    if (c < best) { best = c; pos = sp; }
+                }
+                ce[size_t(e) * 81 + fl * 9 + tl] = best;
+                bc[size_t(e) * 81 + fl * 9 + tl] = pos;
+            }
+        }
+    }
+    // solve_flt_node (flt_block.cuh:6-142).
+    std::vector<double> costs(size_t(N) * kFltLayers, kInf);
+    std::vector<uint64_t> packed(size_t(coff[N]) * kFltLayers, kFltInit), best(size_t(coff[N]) * kFltLayers, 0);
+    for (int d = maxd; d >= 0; --d) {
+        for (int k = lvl_off[d]; k < lvl_off[d + 1]; ++k) {
+            const int node = order[k];
+            const int flow = 1 + crd[node] / XY, x = crd[node] / Y % X, y = crd[node] % Y;
+            const int fhigh = flow == kFltLayers ? 0 : flow;
+            const int nc = nch[node];
+            uint64_t* cbp = best.data() + size_t(coff[node]) * kFltLayers;
+            const uint64_t* cpk = packed.data() + size_t(coff[node]) * kFltLayers;
+            double* cst = costs.data() + size_t(node) * kFltLayers;
+            double mcc[6];
+            uint64_t bp[6] = {0, 0, 0, 0, 0, 0};
+            for (int low = 1; low <= flow; ++low) {
+                for (int c = 0; c < nc; ++c) mcc[c] = kInf;
+                double via = 0;
+                for (int li = low; li < L + 1; ++li) {
+                    if (li > low) via += vcost[G.idx(li - 2, x, y)];
+                    for (int c = 0; c < nc; ++c) {
+                        const uint64_t pv = cpk[c * kFltLayers + li];
+                        const double cc = flt_unpack_cost(pv);
+                        if (cc < mcc[c]) { mcc[c] = cc; bp[c] = uint64_t(uint32_t(pv)) * kFltLayers + li; }
+                    }
+                    if (li >= fhigh) {
+                        double cost = via;
+                        for (int c = 0; c < nc; ++c) cost += mcc[c];
+                        if (cost < kInf && cost < cst[li]) {
+                            cst[li] = cost;
+                            for (int c = 0; c < nc; ++c) cbp[c * kFltLayers + li] = bp[c];
+                        }
+                    }
+                }
+                for (int li = L - 1; li >= low; --li) {
+                    if (cst[li + 1] < cst[li]) {
+                        cst[li] = cst[li + 1];
+                        for (int c = 0; c < nc; ++c) cbp[c * kFltLayers + li] = cbp[c * kFltLayers + li + 1];
+                    }
+                }
+            }
+            const int P = pend[node] - pbeg(node);
+            for (int pi = 0; pi < P; ++pi) {
+                const int e = pbeg(node) + pi, par = epar[e], slot = eslot[e] % 10;
+                uint64_t* ppk = packed.data() + size_t(coff[par]) * kFltLayers;
+                const int px = crd[par] / Y % X, py = crd[par] % Y;
+                const int minx = std::min(x, px), maxx = std::max(x, px), miny = std::min(y, py), maxy = std::max(y, py);
+                uint64_t cache[kFltLayers];
+                for (int t = 0; t < kFltLayers; ++t) cache[t] = kFltInit;
+                for (int layer = 1; layer < kFltLayers; ++layer) {
+                    const bool ay = ((layer & 1) ^ G.DIR) == 1;  // 1-based layer index
+                    if (ay && y != py) continue;
+                    if (!ay && x != px) continue;
+                    const double cb = cst[layer];
+                    for (int tl = 1 + (1 - layer % 2); tl < kFltLayers; tl += 2) {
+                        double c2;
+                        int choice = kStraight;
+                        if (tl == layer) c2 = cb + wire(layer - 1, minx, maxx, miny, maxy);
+                        else if (std::abs(x - px) + std::abs(y - py) > 4) {
+                            const int seq = (layer - 1) * 9 + (tl - 1);
+                            const double c_e = ce[size_t(e) * 81 + seq];
+                            if (!(c_e < kInf)) continue;
+                            c2 = cb + c_e;
+                            choice = seq;
+                        } else continue;
+                        const uint64_t v = flt_pack(static_cast<float>(c2), node * 100 + choice);
+                        if (v < cache[tl]) cache[tl] = v;
+                    }
+                }
+                for (int tl = 1; tl < kFltLayers; ++tl)
+                    ppk[slot * kFltLayers + tl] = std::min(ppk[slot * kFltLayers + tl], cache[tl]);
+            }
+        }
+    }
+    // trace_flt_node (flt_block.cuh:144-331).
+    std::vector<int> lo(N, -1);
+    int status = 0;
+    r[0] = 1;
+    auto emit = [&](int a, int b) {
+        if (r[0] + 2 > cap) { status = 3; return; }
+        r[r[0]] = a;
+        r[r[0] + 1] = b;
+        r[0] += 2;
+    };
+    for (int d = 0; d <= maxd; ++d) {
+        for (int k = lvl_off[d]; k < lvl_off[d + 1]; ++k) {
+            const int node = order[k];
+            const int cx = crd[node] / Y % X, cy = crd[node] % Y, l = crd[node] / XY;
+            const int P = pend[node] - pbeg(node);
+            if (P == 0) {
+                int ml = 0;
+                double mc = costs[size_t(node) * kFltLayers];
+                for (int layer = 1; layer < kFltLayers; ++layer)
+                    if (costs[size_t(node) * kFltLayers + layer] < mc) { mc = costs[size_t(node) * kFltLayers + layer]; ml = layer; }
+                lo[node] = ml;
+            } else {
+                int par_layer = -1, par_idx = -1, par_seq = -1;
+                for (int pi = 0; pi < P; ++pi) {
+                    const int e = pbeg(node) + pi, pn = epar[e];
+                    if (lo[pn] <= 0) continue;
+                    par_idx = pn; par_seq = pi; par_layer = lo[pn];
+                    const uint64_t path = best[size_t(coff[pn]) * kFltLayers + (eslot[e] % 10) * kFltLayers + par_layer];
+                    const uint64_t cidx = path / kFltLayers / 100, choice = (path / kFltLayers) % 100;
+                    if (cidx != uint64_t(node)) { lo[node] = -1; continue; }
+                    lo[node] = choice == kStraight ? int(path % kFltLayers) : int(choice / 9 + 1);
+                    const int px = crd[pn] / Y % X, py = crd[pn] % Y;
+                    const bool vert = px == cx && cy != py, horz = py == cy && cx != px;
+                    if (vert || horz) {
+                        if (choice == kStraight) {
+                            const int ll = lo[node] - 1;
+                            if (vert) emit(G.idx(ll, px, std::min(py, cy)), G.idx(ll, px, std::max(py, cy)));
+                            else emit(G.idx(ll, std::min(px, cx), py), G.idx(ll, std::max(px, cx), py));
+                        } else {
+                            const int fl = int(choice / 9), tl = int(choice % 9);
+                            const int cp = bc[size_t(e) * 81 + fl * 9 + tl];
+                            if (vert) {
+                                emit(G.idx(fl, cx, std::min(cy, cp)), G.idx(fl, cx, std::max(cy, cp)));
+                                emit(G.idx(std::min(fl, tl), cx, cp), G.idx(std::max(fl, tl), cx, cp));
+                                emit(G.idx(tl, cx, std::min(py, cp)), G.idx(tl, cx, std::max(py, cp)));
+                            } else {
+                                emit(G.idx(fl, std::min(cx, cp), cy), G.idx(fl, std::max(cx, cp), cy));
+                                emit(G.idx(std::min(fl, tl), cp, cy), G.idx(std::max(fl, tl), cp, cy));
+                                emit(G.idx(tl, std::min(px, cp), cy), G.idx(tl, std::max(px, cp), cy));
+                            }
+                        }
+                    }
+                    break;
+                }
+                if (par_layer == -1) { lo[node] = -1; continue; }
+                const int e = pbeg(node) + par_seq;
+                const uint64_t path = best[size_t(coff[par_idx]) * kFltLayers + (eslot[e] % 10) * kFltLayers + par_layer];
+                if (path / kFltLayers / 100 != uint64_t(node)) { lo[node] = -1; continue; }
+            }
+            int minl = l + 1, maxl = (l + 1) == kFltLayers ? 1 : minl;
+            minl = std::min(minl, lo[node]);
+            maxl = std::max(maxl, lo[node]);
+            for (int c = 0; c < nch[node]; ++c) {
+                const int lc = int(best[size_t(coff[node]) * kFltLayers + c * kFltLayers + lo[node]] % kFltLayers);
+                minl = std::min(lc, minl);
+                maxl = std::max(lc, maxl);
+            }
+            if (minl < 1) { if (!status) status = 4; continue; }
+            if (minl < maxl) emit(G.idx(minl - 1, cx, cy), G.idx(maxl - 1, cx, cy));
+        }
+    }
+    (void)L;
+    return status;
+}
+
+}  // namespace
+
+extern "C" {
+
+int orc_flt_stage(const orc_grid* g, const orc_flt* dags, int32_t n_batches, const int32_t* batch_off,
+                  const int32_t* ids, const int64_t* route_off, const int32_t* routes,
+                  const int64_t* route2_off, int32_t* routes2, int32_t remove_phase_one,
+                  int32_t* demand_half, int32_t* timestamp, int32_t* stamp,
+                  double* total_wirelength, int64_t* total_vias, int32_t nthreads) {
+#ifdef _OPENMP
+    if (nthreads > 0) omp_set_num_threads(nthreads);
+#endif
+    Grid G(g);
+    const size_t cells = size_t(g->L) * g->X * g->Y;
+    std::vector<float> wcost(cells), vcost(cells);
+    std::vector<double> presum(cells);
+    int status = 0;
+    for (int b = 0; b < n_batches; ++b) {
+        const int n = batch_off[b + 1] - batch_off[b];
+        const int32_t* bid = ids + batch_off[b];
+        if (remove_phase_one)  // flt.cuh:143-150
+            commit_impl(g, n, bid, route_off, routes, ++*stamp, -1, demand_half, timestamp, total_wirelength,
+                        total_vias, nullptr);
+        const int32_t s = ++*stamp;  // flt.cuh:151
+        orc_cost_full(g, demand_half, wcost.data(), vcost.data());  // refresh_cost: same values as incremental
+        orc_presum(g, wcost.data(), presum.data());
+#pragma omp parallel for schedule(dynamic, 4)
+        for (int k = 0; k < n; ++k) {
+            const int id = bid[k];
+            const int rc = flt_net(G, dags, vcost.data(), presum.data(), id, routes2 + route2_off[id],
+                                   route2_off[id + 1] - route2_off[id]);
+            if (rc) {
+#pragma omp critical
+                if (!status) status = rc;
+            }
+        }
+        commit_impl(g, n, bid, route2_off, routes2, s, 1, demand_half, timestamp, total_wirelength, total_vias,
+                    nullptr);
+    }
+    return status;
+}
+
+}  // extern "C"

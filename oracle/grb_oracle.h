@@ -91,6 +91,34 @@ int orc_lshape_stage(const orc_grid* g, int32_t n_batches, const int32_t* batch_
                      int32_t* demand_half, int32_t* timestamp, int32_t* stamp,
                      double* total_wirelength, int64_t* total_vias, int32_t nthreads);
 
+/* FLT DAGs of a stage's nets, CSR by net id (nets outside the stage have empty
+ * ranges).  Per node: 3-D coordinate (layer 9 marks a node with no pin layer),
+ * depth, child-slot count, cumulative parent-edge count within the net.  Per
+ * edge, grouped by child node: parent node (net-local) and source slot
+ * child * 10 + slot index at the parent (flt_topology.hpp:15-16, 52-70). */
+typedef struct orc_flt {
+    const int32_t* node_off;
+    const int32_t* coord;
+    const int32_t* depth;
+    const int32_t* children;
+    const int32_t* parent_end;
+    const int32_t* edge_off;
+    const int32_t* edge_parent;
+    const int32_t* edge_slot;
+} orc_flt;
+
+/* FLT stage (flt.cuh:141-168) over an explicit batch plan in execution order:
+ * per batch, optionally remove the nets' phase-one routes (K = -1, own stamp),
+ * ++stamp, full cost refresh, mid-edge layer-change tables, bottom-up solve,
+ * top-down trace into the phase-two routes (routes2 at route2_off[id], count
+ * word first), commit of the phase-two routes.  Returns 0, or 3 when a net's
+ * route storage overflows, or 4 for an unroutable net. */
+int orc_flt_stage(const orc_grid* g, const orc_flt* dags, int32_t n_batches, const int32_t* batch_off,
+                  const int32_t* ids, const int64_t* route_off, const int32_t* routes,
+                  const int64_t* route2_off, int32_t* routes2, int32_t remove_phase_one,
+                  int32_t* demand_half, int32_t* timestamp, int32_t* stamp,
+                  double* total_wirelength, int64_t* total_vias, int32_t nthreads);
+
 #ifdef __cplusplus
 }
 #endif

@@ -12,7 +12,7 @@ _LIB = os.path.join(_HERE, "liboracle.so")
 
 __all__ = [
     "build", "load", "OrcGrid", "cost_full", "presum", "presum_logstep", "lshape_batch",
-    "commit_batch", "batches", "ripup_classify", "congestion_view", "lshape_stage",
+    "commit_batch", "batches", "ripup_classify", "congestion_view", "lshape_stage", "flt_stage",
 ]
 
 
@@ -59,6 +59,13 @@ def _declare(lib):
     lib.orc_congestion_view.argtypes = [P, P, P, P, P]
     lib.orc_lshape_stage.argtypes = [P, C.c_int32, P, P, P, P, P, P, P, P, P, P, P, P, C.c_int32]
     lib.orc_lshape_stage.restype = C.c_int
+    lib.orc_flt_stage.argtypes = [P, P, C.c_int32, P, P, P, P, P, P, C.c_int32, P, P, P, P, P, C.c_int32]
+    lib.orc_flt_stage.restype = C.c_int
+
+
+class _COrcFlt(C.Structure):
+    _fields_ = [(k, C.c_void_p) for k in ("node_off", "coord", "depth", "children", "parent_end", "edge_off",
+                                          "edge_parent", "edge_slot")]
 
 
 def _p(a):
@@ -187,3 +194,26 @@ def lshape_stage(g: OrcGrid, ids, batch_off, node_off, nodes, parents, route_off
     return {"status": rc, "routes": routes, "demand_half": demand, "timestamp": ts, "stamp": st.value,
             "wirelength": wl.value, "vias": vi.value}
 
+
+
+def flt_stage(g: OrcGrid, dags: dict, ids, batch_off, route_off, routes, route2_off, demand_half, timestamp, stamp,
+              remove_phase_one=True, threads=0, wirelength=0.0, vias=0):
+    """FLT stage on the CPU.  `dags` holds the CSR arrays by net id (node_off,
+    coord, depth, children, parent_end, edge_off, edge_parent, edge_slot)."""
+    lib = load()
+    keep = {k: _c(dags[k], np.int32) for k, _ in _COrcFlt._fields_}
+    d = _COrcFlt(**{k: v.ctypes.data for k, v in keep.items()})
+    ids = _c(ids, np.int32)
+    batch_off = _c(batch_off, np.int32)
+    route2_off = _c(route2_off, np.int64)
+    routes2 = np.zeros(int(route2_off[-1]), np.int32)
+    demand = _c(demand_half, np.int32).copy()
+    ts = _c(timestamp, np.int32).copy()
+    st = C.c_int32(stamp)
+    wl = C.c_double(wirelength)
+    vi = C.c_int64(vias)
+    rc = lib.orc_flt_stage(g.ref, C.byref(d), len(batch_off) - 1, _p(batch_off), _p(ids), _p(_c(route_off, np.int64)),
+                           _p(_c(routes, np.int32)), _p(route2_off), _p(routes2), int(bool(remove_phase_one)),
+                           _p(demand), _p(ts), C.byref(st), C.byref(wl), C.byref(vi), int(threads))
+    return {"status": rc, "routes2": routes2, "demand_half": demand, "timestamp": ts, "stamp": st.value,
+            "wirelength": wl.value, "vias": vi.value}

@@ -17,6 +17,13 @@
 //                                   plan; cost tables before batch k, routes after.
 //   batch <dir> <limit> <sparsity>  CPU: time generate_batches_rsmt on a dumped
 //                                   geometry (X, Y, order, points, segments).
+//   flt   <cap> <net> <dir> <lut>   GPU: the reference default pipeline up to and
+//                                   through its FLT stage (pipeline.hpp:263-305):
+//                                   L-shape, congestion view, rip-up, the host FLT
+//                                   DAG builder; dumps the DAGs, the FLT batching
+//                                   geometry and batches and the state before the
+//                                   stage, runs route_prepared_topology and dumps
+//                                   phase-two routes, demand and statistics.
 //   write <cap> <net> <dir> <lut> <routes> <out>
 //                                   CPU: write a .out with the reference writer from
 //                                   route words produced elsewhere (nets published
@@ -268,6 +275,110 @@ int run_snap(const std::string& cap, const std::string& net, const std::string& 
     return 0;
 }
 
+int run_flt(const std::string& cap, const std::string& net, const std::string& dir, const std::string& lut) {
+    read_design(cap, net, lut);
+    cudb::RouterState state;
+    state.batch_sparsity_override = 1;
+    state.report_score = false;
+    cudb::build_cuda_database(state);
+    graph::initialize_incremental_cost(state);
+    auto& view = state.device;
+    grotor::cuda_check(cudaFuncSetAttribute(graph::compute_presum,
+               cudaFuncAttributeMaxDynamicSharedMemorySize, sizeof(double) * view.XY), "prefix shared memory");
+    grotor::cuda_check(cudaFuncSetAttribute(graph::compute_presum_general,
+               cudaFuncAttributeMaxDynamicSharedMemorySize, sizeof(int) * view.XY), "demand shared memory");
+    std::vector<int> all(state.nets.size());
+    std::iota(all.begin(), all.end(), 0);
+    Lshape_route::Lshape_route(state, all);
+    grotor::cuda_check(cudaDeviceSynchronize(), "L-shape stage");
+    const size_t cells = size_t(view.L) * view.X * view.Y;
+    auto dump_state = [&](const std::string& tag) {
+        std::vector<float> demand(cells);
+        cudaMemcpy(demand.data(), view.demand, cells * 4, cudaMemcpyDeviceToHost);
+        cudb::RoutingStatistics stats;
+        cudaMemcpy(&stats, view.statistics, sizeof(stats), cudaMemcpyDeviceToHost);
+        dump(dir, tag + "_demand", demand);
+        std::vector<double> st{stats.total_wirelength, double(stats.total_via_count), double(state.global_timestamp)};
+        dump(dir, tag + "_stats", st);
+    };
+    dump_state("flt_before");
+    // pipeline.hpp:263-285: mode, congestion view, rip-up, phase-two offsets.
+    if (state.nets.size() > 5000000) mode = 1;
+    if (state.nets.size() > 20000000) mode = 2;
+    graph::extract_congestionView<<<BLOCK_NUM(view.X * view.Y), THREAD_NUM>>>(view);
+    graph::extract_congestionView_xsum<<<view.Y, THREAD_NUM, sizeof(float) * view.X>>>(view);
+    graph::extract_congestionView_ysum<<<view.X, THREAD_NUM, sizeof(float) * view.Y>>>(view);
+    auto overflow_nets = graph::ripup(state, 0);
+    dump(dir, "flt_of_nets", overflow_nets.first);
+    int pin_count = 0;
+    for (auto net_id : overflow_nets.first) {
+        state.pin_cnt_sum_phase2_cpu[net_id] = pin_count;
+        pin_count += state.nets[net_id].pins.size();
+        state.ripup_flag_cpu[net_id] = 1;
+    }
+    view.PIN_NUM_PHASE2 = pin_count;
+    state.memory.allocate(&view.routes_phase2, (view.ROUTE_PER_PIN_PHASE2 * pin_count + 1) * sizeof(int));
+    cudaMemcpy(view.ripup_flag, state.ripup_flag_cpu.data(), (1 + view.NET_NUM) * sizeof(int), cudaMemcpyHostToDevice);
+    cudaMemcpy(view.pin_acc_num_phase2, state.pin_cnt_sum_phase2_cpu.data(), (1 + view.NET_NUM) * sizeof(int),
+               cudaMemcpyHostToDevice);
+    dump(dir, "flt_pin_acc2", state.pin_cnt_sum_phase2_cpu);
+    std::vector<int> nets2route = overflow_nets.first;
+    // flt.cuh:48-73: sort by HPWL, host DAG builder, batching geometry.
+    Lshape_route_detour::prepare_detour_topology(state, nets2route);
+    dump(dir, "flt_nets", nets2route);
+    auto& topo = state.flt_topology;
+    std::vector<int> node_off{0}, coord, depth, children, parent_end, edge_off{0}, edge_parent, edge_slot;
+    std::vector<int> point_off{0}, points, hseg_off{0}, hsegs, vseg_off{0}, vsegs;
+    for (size_t slot = 0; slot < nets2route.size(); ++slot) {
+        const auto& span = topo.spans[slot];
+        const auto& arena = topo.arenas[span.lane];
+        for (int i = 0; i < span.nodes; ++i) {
+            const auto& nd = arena.nodes[span.node_begin + i];
+            coord.push_back(nd.coordinate); depth.push_back(nd.depth);
+            children.push_back(nd.children); parent_end.push_back(nd.parent_end);
+        }
+        for (int i = 0; i < span.edges; ++i) {
+            const auto& e = arena.edges[span.edge_begin + i];
+            edge_parent.push_back(e.parent); edge_slot.push_back(e.source_slot);
+        }
+        node_off.push_back(coord.size()); edge_off.push_back(edge_parent.size());
+        const auto& n = state.nets[nets2route[slot]];
+        for (int p : n.points) points.push_back(p);
+        point_off.push_back(points.size());
+        for (auto& sg : n.rsmt_h_segments) { hsegs.push_back(sg.first); hsegs.push_back(sg.second); }
+        hseg_off.push_back(hsegs.size() / 2);
+        for (auto& sg : n.rsmt_v_segments) { vsegs.push_back(sg.first); vsegs.push_back(sg.second); }
+        vseg_off.push_back(vsegs.size() / 2);
+    }
+    dump(dir, "flt_node_off", node_off); dump(dir, "flt_coord", coord); dump(dir, "flt_depth", depth);
+    dump(dir, "flt_children", children); dump(dir, "flt_parent_end", parent_end);
+    dump(dir, "flt_edge_off", edge_off); dump(dir, "flt_edge_parent", edge_parent); dump(dir, "flt_edge_slot", edge_slot);
+    dump(dir, "flt_point_off", point_off); dump(dir, "flt_points", points);
+    dump(dir, "flt_hseg_off", hseg_off); dump(dir, "flt_hsegs", hsegs);
+    dump(dir, "flt_vseg_off", vseg_off); dump(dir, "flt_vsegs", vsegs);
+    // The stage's batches (flt.cuh:92, executed in reverse, flt_topology.hpp:101).
+    std::vector<int> sorted = nets2route;
+    auto batches = cudb::generate_batches_rsmt(state, sorted, 300000, state.batch_sparsity_override);
+    std::vector<int> batch_ids, batch_off{0};
+    for (auto it = batches.rbegin(); it != batches.rend(); ++it) {
+        if (it->empty()) continue;
+        batch_ids.insert(batch_ids.end(), it->begin(), it->end());
+        batch_off.push_back(batch_ids.size());
+    }
+    dump(dir, "flt_batch_ids", batch_ids); dump(dir, "flt_batch_off", batch_off);
+    Lshape_route_detour::route_prepared_topology(state, nets2route, "detour", true);
+    grotor::cuda_check(cudaDeviceSynchronize(), "FLT stage");
+    dump_state("flt_after");
+    state.download_routes(true);
+    dump(dir, "flt_routes2", state.routes_phase2_cpu.get(), view.ROUTE_PER_PIN_PHASE2 * view.PIN_NUM_PHASE2 + 1);
+    state.download_routes(false);
+    dump(dir, "flt_routes1", state.routes_cpu.get(), view.ROUTE_PER_PIN * view.PIN_NUM + 1);
+    printf("REF_FLT nets=%zu batches=%zu nodes=%zu edges=%zu\n", nets2route.size(), batch_off.size() - 1,
+           coord.size(), edge_parent.size());
+    state.release_workspaces();
+    return 0;
+}
+
 int run_batch(const std::string& dir, int limit, int sparsity) {
     const auto meta = load<int>(dir + "/meta.i32");
     const auto order = load<int>(dir + "/order.i32");
@@ -334,9 +445,10 @@ int main(int argc, char** argv) {
         if (mode == "topo" && argc == 6) return run_topo(argv[2], argv[3], argv[4], argv[5]);
         if (mode == "route" && argc == 7) return run_route(argv[2], argv[3], argv[4], argv[5], argv[6]);
         if (mode == "snap" && argc == 7) return run_snap(argv[2], argv[3], argv[4], argv[5], std::stoi(argv[6]));
+        if (mode == "flt" && argc == 6) return run_flt(argv[2], argv[3], argv[4], argv[5]);
         if (mode == "batch" && argc == 5) return run_batch(argv[2], std::stoi(argv[3]), std::stoi(argv[4]));
         if (mode == "write" && argc == 8) return run_write(argv[2], argv[3], argv[4], argv[5], argv[6], argv[7]);
-        fprintf(stderr, "usage: ref_harness topo|route|snap|batch|write ...\n");
+        fprintf(stderr, "usage: ref_harness topo|route|snap|flt|batch|write ...\n");
         return 2;
     } catch (const std::exception& e) {
         fprintf(stderr, "ref_harness error: %s\n", e.what());

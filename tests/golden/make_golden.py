@@ -8,10 +8,15 @@ sources by ``oracle/ref.mk``):
   geometry, HPWL order and the reference CPU first-fit batches, grid tables;
 * ``route`` and ``snap`` (GPU): routes, demand and statistics of the reference
   L-shape stage, cost tables after the stage, the .out file (SHA-256 and
-  evaluator scores), and the cost tables before / routes after one batch.
+  evaluator scores), and the cost tables before / routes after one batch;
+* ``flt`` (GPU, FLT fixtures): the reference default pipeline through its FLT
+  stage -- demand and statistics before the stage, the rip-up set, the DAGs of
+  the reference's host FLT builder, the FLT batching geometry and batches, and
+  phase-two routes, demand and statistics after the stage.
 
-Usage:  python tests/golden/make_golden.py --topo      (here, no GPU)
+Usage:  python tests/golden/make_golden.py --topo      (no GPU needed)
         python tests/golden/make_golden.py --route     (on a GPU box)
+        python tests/golden/make_golden.py --flt       (on a GPU box)
 The two passes update the same ``<name>.npz``.
 """
 from __future__ import annotations
@@ -37,7 +42,11 @@ EVALUATOR = os.path.join(REF, "evaluator")
 FIXTURES = {
     "ref_64x64x10_2k": ("small_64x64x5", dict(n_nets=2000, cap_layers=10, seed=11)),
     "ref_32x32x10_400": ("small_64x64x5", dict(n_nets=400, cap_layers=10, seed=12, X=32, Y=32)),
+    # congested (capacity 1..4) so that the L-shape stage leaves overflow nets for FLT
+    "ref_flt_48x48x10_1500": ("small_64x64x5", dict(n_nets=1500, cap_layers=10, seed=13, X=48, Y=48, cap_lo=1,
+                                                    cap_hi=4)),
 }
+FLT_FIXTURES = {"ref_flt_48x48x10_1500"}
 TOPO_KEYS = ["meta", "short_costs", "unit_costs", "x_edge_len", "y_edge_len", "capacity", "pin_acc_num",
              "node_off", "nodes", "parents", "point_off", "points", "hseg_off", "hsegs", "vseg_off", "vsegs",
              "hpwl", "original", "pin_count", "order", "batch_of", "ids", "batch_off", "pin_vias"]
@@ -85,6 +94,7 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--topo", action="store_true")
     ap.add_argument("--route", action="store_true")
+    ap.add_argument("--flt", action="store_true")
     ap.add_argument("--only", default=None)
     ap.add_argument("--outdir", default=HERE, help="where to write the .npz files")
     ap.add_argument("--keep-out", action="store_true", help="also copy the reference .out into --outdir")
@@ -100,7 +110,11 @@ def main():
             if args.topo:
                 subprocess.run([HARNESS, "topo", cap, net, w, REF], check=True, stdout=subprocess.DEVNULL)
                 data.update(read_dir(w, TOPO_KEYS))
-            if args.route:
+            if args.flt and name in FLT_FIXTURES:
+                subprocess.run([HARNESS, "flt", cap, net, w, REF], check=True, stdout=subprocess.DEVNULL)
+                got = read_dir(w)
+                data.update({k: v for k, v in got.items() if k.startswith("flt_")})
+            if args.route and name not in FLT_FIXTURES:
                 for k in TOPO_KEYS:  # the GPU passes read the committed plan
                     if k in data:
                         data[k].tofile(os.path.join(w, f"{k}.{_ext(data[k])}"))

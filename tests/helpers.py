@@ -97,3 +97,85 @@ def check_connected(routes, route_off, node_off, nodes, X, Y, L, ids):
         if parent:
             comps = {find(c) for c in list(parent)}
             assert len(comps) == 1, f"net {i}: route has {len(comps)} components"
+
+
+# ---- FLT stage fixtures (tests/golden/make_golden.py --flt) -----------------
+ROUTE_PER_PIN_PHASE2 = 100  # router_state.hpp:33
+FLT_DAG_KEYS = ("node_off", "coord", "depth", "children", "parent_end", "edge_off", "edge_parent", "edge_slot")
+
+
+def flt_by_net(g: dict):
+    """FLT inputs of a fixture re-indexed by net id: DAG CSR (empty for nets
+    outside the stage), batching geometry (FLT geometry for stage nets, the
+    stage-one geometry otherwise) and phase-two route offsets (100 words per
+    pin for stage nets)."""
+    n = len(g["node_off"]) - 1
+    slot_of = np.full(n, -1, np.int64)
+    slot_of[g["flt_nets"]] = np.arange(len(g["flt_nets"]))
+
+    def csr(off_key, data_keys, default_off=None, default_data=None, width=1):
+        off = [0]
+        data = {k: [] for k in data_keys}
+        for i in range(n):
+            s = slot_of[i]
+            if s >= 0:
+                a, b = g[off_key][s], g[off_key][s + 1]
+                for k in data_keys:
+                    data[k].append(g[k][a * width:b * width])
+                off.append(off[-1] + b - a)
+            elif default_off is not None:
+                a, b = default_off[i], default_off[i + 1]
+                for k, dk in zip(data_keys, default_data):
+                    data[k].append(dk[a * width:b * width])
+                off.append(off[-1] + b - a)
+            else:
+                off.append(off[-1])
+        cat = {k: (np.concatenate(v) if v else np.zeros(0, np.int32)).astype(np.int32) for k, v in data.items()}
+        return np.asarray(off, np.int32), cat
+
+    node_off, nd = csr("flt_node_off", ["flt_coord", "flt_depth", "flt_children", "flt_parent_end"])
+    edge_off, ed = csr("flt_edge_off", ["flt_edge_parent", "flt_edge_slot"])
+    dags = {"node_off": node_off, "coord": nd["flt_coord"], "depth": nd["flt_depth"],
+            "children": nd["flt_children"], "parent_end": nd["flt_parent_end"], "edge_off": edge_off,
+            "edge_parent": ed["flt_edge_parent"], "edge_slot": ed["flt_edge_slot"]}
+    dags["edge_source_slot"] = dags["edge_slot"]
+    point_off, pd = csr("flt_point_off", ["flt_points"], g["point_off"], [g["points"]])
+    hseg_off, hd = csr("flt_hseg_off", ["flt_hsegs"], g["hseg_off"], [g["hsegs"]], width=2)
+    vseg_off, vd = csr("flt_vseg_off", ["flt_vsegs"], g["vseg_off"], [g["vsegs"]], width=2)
+    geom = (point_off, pd["flt_points"], hseg_off, hd["flt_hsegs"], vseg_off, vd["flt_vsegs"])
+    words = np.where(slot_of >= 0, g["pin_count"].astype(np.int64) * ROUTE_PER_PIN_PHASE2, 0)
+    route2_off = np.concatenate([[0], np.cumsum(words)]).astype(np.int64)
+    return dags, geom, route2_off
+
+
+def segment_multiset(r: np.ndarray):
+    """Sorted (a, b) pairs of one route record [count, a0, b0, ...]."""
+    if len(r) == 0 or r[0] <= 1:
+        return []
+    w = r[1:r[0]].reshape(-1, 2)
+    return sorted(map(tuple, w.tolist()))
+
+
+def ref_routes2_of(g: dict, net: int) -> np.ndarray:
+    base = int(g["flt_pin_acc2"][net]) * ROUTE_PER_PIN_PHASE2
+    return g["flt_routes2"][base:base + int(g["pin_count"][net]) * ROUTE_PER_PIN_PHASE2]
+
+
+def route_geometry(r: np.ndarray, X: int, Y: int):
+    """Canonical geometry of one route record: sorted unit wire edges
+    (cell ids) and via stacks.  Two records with the same geometry put the
+    same demand on the grid and score the same; they may still split a
+    straight run into different segments."""
+    XY = X * Y
+    edges, vias = [], []
+    for a, b in segment_multiset(r):
+        if a // XY != b // XY:
+            vias.append((a, b))
+            continue
+        l = a // XY
+        xa, ya, xb, yb = a % XY // Y, a % Y, b % XY // Y, b % Y
+        if xa == xb:
+            edges += [l * XY + xa * Y + y for y in range(min(ya, yb), max(ya, yb))]
+        else:
+            edges += [l * XY + x * Y + ya for x in range(min(xa, xb), max(xa, xb))]
+    return sorted(edges), sorted(vias)
