@@ -1,6 +1,8 @@
 # Builds the reference router's own code, from its sources where they lie,
 # into oracle/_ref/ (git-ignored; travels to the GPU box with the snapshot):
 #   ref_harness  -- oracle/ref_harness.cu compiled against the reference headers
+#   ref_harness_ggr -- the same with GROTOR_GGR_ROUTING (integer wire costs and
+#                   the Z-shape pipeline of the reference's grotor_ggr build)
 #   evaluator    -- the reference's scoring program (resources/evaluator.cpp)
 #   POWV9.dat, POST9.dat -- FLUTE lookup tables the reference reads at run time
 # Usage: make -C oracle -f ref.mk [REF=/path/to/GRotor]
@@ -9,7 +11,7 @@ NVCC ?= nvcc
 HOSTCXX ?= /usr/bin/g++
 OUT := _ref
 
-all: $(OUT)/ref_harness $(OUT)/evaluator $(OUT)/POWV9.dat $(OUT)/POST9.dat
+all: $(OUT)/ref_harness $(OUT)/ref_harness_ggr $(OUT)/evaluator $(OUT)/POWV9.dat $(OUT)/POST9.dat
 
 $(OUT):
 	mkdir -p $(OUT)
@@ -17,6 +19,11 @@ $(OUT):
 $(OUT)/ref_harness: ref_harness.cu | $(OUT)
 	$(NVCC) -ccbin $(HOSTCXX) -std=c++17 -O3 -UNDEBUG -gencode arch=compute_100a,code=sm_100a \
 	  -Xcompiler -fopenmp -I$(REF)/include -I$(REF)/src -I$(REF)/third_party \
+	  -DG_ROTOR_RESOURCE_DIR=\"$(OUT)\" -x cu ref_harness.cu -o $@
+
+$(OUT)/ref_harness_ggr: ref_harness.cu | $(OUT)
+	$(NVCC) -ccbin $(HOSTCXX) -std=c++17 -O3 -UNDEBUG -gencode arch=compute_100a,code=sm_100a \
+	  -Xcompiler -fopenmp -I$(REF)/include -I$(REF)/src -I$(REF)/third_party -DGROTOR_GGR_ROUTING=1 \
 	  -DG_ROTOR_RESOURCE_DIR=\"$(OUT)\" -x cu ref_harness.cu -o $@
 
 $(OUT)/evaluator: $(REF)/resources/evaluator.cpp | $(OUT)

@@ -24,12 +24,22 @@
 //                                   geometry and batches and the state before the
 //                                   stage, runs route_prepared_topology and dumps
 //                                   phase-two routes, demand and statistics.
+//   zshape <cap> <net> <dir> <lut>  GPU, GGR build only (ref_harness_ggr, compiled with
+//                                   GROTOR_GGR_ROUTING): the reference Z-shape
+//                                   pipeline (pipeline_ggr.hpp:8-144) -- order,
+//                                   first-fit groups, bbox batches, the encoded
+//                                   trees and net boxes, then routes, demand and
+//                                   statistics after the stage, before the host
+//                                   post-processing (:145-151).
 //   write <cap> <net> <dir> <lut> <routes> <out>
 //                                   CPU: write a .out with the reference writer from
 //                                   route words produced elsewhere (nets published
 //                                   in the plan order <dir>/ids.i32 when present).
 // Every array is written as raw little-endian data, <dir>/<name>.<i32|i64|f32|f64>.
 #include "pipeline.hpp"
+#ifdef GROTOR_GGR_ROUTING
+#include "pipeline_ggr.hpp"
+#endif
 
 #include <filesystem>
 #include <fstream>
@@ -379,6 +389,142 @@ int run_flt(const std::string& cap, const std::string& net, const std::string& d
     return 0;
 }
 
+#ifdef GROTOR_GGR_ROUTING
+int run_zshape(const std::string& cap, const std::string& net, const std::string& dir, const std::string& lut) {
+    read_design(cap, net, lut);
+    cudb::RouterState state;
+    state.batch_sparsity_override = 1;
+    state.report_score = false;
+    // pipeline_ggr.hpp:9-71.
+    state.device.ROUTE_PER_PIN = 256;
+    cudb::build_cuda_database(state);
+    graph::initialize_incremental_cost(state);
+    auto& view = state.device;
+    grotor::cuda_check(cudaFuncSetAttribute(graph::compute_presum,
+               cudaFuncAttributeMaxDynamicSharedMemorySize, sizeof(double) * view.XY), "prefix shared memory");
+    const int n = std::max(view.X, view.Y), layers = view.L + 1;
+    const size_t grid = size_t(layers) * n * n;
+    std::vector<int> order(state.nets.size());
+    std::iota(order.begin(), order.end(), 0);
+#pragma omp parallel for num_threads(8)
+    for (int i = 0; i < int(order.size()); ++i) state.nets[i].construct_rsmt(state, false);
+    std::sort(order.begin(), order.end(), [&](int a, int b) {
+        return state.nets[a].hpwl == state.nets[b].hpwl ? a > b : state.nets[a].hpwl > state.nets[b].hpwl;
+    });
+    auto groups = cudb::generate_batches_rsmt(state, order, 1000000, 1);
+    std::vector<std::vector<int>> batches;
+    for (const auto& group : groups) {
+        auto refined = grotor::zshape::generate_bbox_batches(group, state.nets, view.X, view.Y);
+        for (auto& batch : refined) batches.emplace_back(std::move(batch));
+    }
+    std::reverse(batches.begin(), batches.end());
+    std::vector<int> group_ids, group_off{0}, zb_ids, zb_off{0};
+    for (auto& g : groups) { group_ids.insert(group_ids.end(), g.begin(), g.end()); group_off.push_back(group_ids.size()); }
+    for (auto& b : batches) { zb_ids.insert(zb_ids.end(), b.begin(), b.end()); zb_off.push_back(zb_ids.size()); }
+    dump_grid(dir, state);
+    dump(dir, "pin_acc_num", state.pin_cnt_sum_cpu);
+    dump(dir, "z_order", order); dump(dir, "z_group_ids", group_ids); dump(dir, "z_group_off", group_off);
+    dump(dir, "z_batch_ids", zb_ids); dump(dir, "z_batch_off", zb_off);
+    // Per-net trees in the encoding of zshape::encode_batch (zshape_topology.hpp:59-121),
+    // with 3-D coordinates, and the net boxes used by generate_bbox_batches.
+    std::vector<int> node_off{0}, coord, child, bbox;
+    std::vector<int> zero_offsets(state.nets.size(), 0);
+    for (int id = 0; id < int(state.nets.size()); ++id) {
+        const auto& nt = state.nets[id];
+        bbox.push_back(nt.minx); bbox.push_back(nt.maxx); bbox.push_back(nt.miny); bbox.push_back(nt.maxy);
+        auto enc = grotor::zshape::encode_batch({id}, state.nets, zero_offsets, view.X, view.Y, view.L);
+        const int* rec = enc.points.data() + enc.points[0];
+        const int cnt = rec[1];
+        // Recover each preorder node's 3-D coordinate from the tree (the
+        // encoding keeps only its 2-D position and pin layer range).
+        const auto& graph = nt.rsmt;
+        const int node_count = int(graph.size()) - 1;
+        int root = 0;
+        for (int i = 0; i < node_count; ++i) if (graph[i].size() == 1) { root = i; break; }
+        std::vector<int> ord, parent(node_count, -1), stack{root};
+        while (!stack.empty()) {
+            const int v = stack.back(); stack.pop_back(); ord.push_back(v);
+            for (auto it = graph[v].rbegin(); it != graph[v].rend(); ++it) {
+                if (*it == parent[v]) continue;
+                parent[*it] = v; stack.push_back(*it);
+            }
+        }
+        for (int k = 0; k < cnt; ++k) {
+            coord.push_back(graph.back()[ord[k]]);
+            for (int j = 0; j < 3; ++j) child.push_back(rec[2 + 6 * k + 3 + j] < 0 ? -1 : rec[2 + 6 * k + 3 + j] / 6);
+        }
+        node_off.push_back(coord.size());
+    }
+    dump(dir, "z_node_off", node_off); dump(dir, "z_coord", coord); dump(dir, "z_child", child); dump(dir, "z_bbox", bbox);
+    // pipeline_ggr.hpp:72-134: the batch loop, in the reference's structure.
+    struct Span { size_t points, gbpoints, offsets, ids; int count, point_count, gb_count, raw_words; };
+    std::vector<Span> spans;
+    std::vector<int> points, gbpoints, offsets, ids, route_offsets(order.size());
+    size_t max_points = 1, max_gb = 1, max_raw = 1;
+    for (const auto& batch : batches) {
+        int raw_words = 0;
+        const size_t offset_begin = offsets.size();
+        for (int id : batch) {
+            route_offsets[id] = raw_words;
+            offsets.push_back(raw_words);
+            raw_words += int(state.nets[id].pins.size()) * 256;
+        }
+        auto encoded = grotor::zshape::encode_batch(batch, state.nets, route_offsets, view.X, view.Y, view.L);
+        spans.push_back({points.size(), gbpoints.size(), offset_begin, ids.size(), int(batch.size()),
+            int(encoded.points.size()), int(encoded.gbpoints.size()), raw_words});
+        points.insert(points.end(), encoded.points.begin(), encoded.points.end());
+        gbpoints.insert(gbpoints.end(), encoded.gbpoints.begin(), encoded.gbpoints.end());
+        ids.insert(ids.end(), batch.begin(), batch.end());
+        max_points = std::max(max_points, encoded.points.size());
+        max_gb = std::max(max_gb, encoded.gbpoints.size());
+        max_raw = std::max(max_raw, size_t(raw_words));
+    }
+    grotor::DeviceMemory memory;
+    int *map = nullptr, *prev = nullptr, *raw = nullptr, *d_points = nullptr, *d_gb = nullptr, *d_offsets = nullptr, *error = nullptr;
+    memory.allocate(&map, 6 * grid * sizeof(int));
+    memory.allocate(&prev, 16 * grid * sizeof(int));
+    memory.allocate(&raw, max_raw * sizeof(int));
+    memory.allocate(&d_points, max_points * sizeof(int));
+    memory.allocate(&d_gb, max_gb * sizeof(int));
+    memory.allocate(&d_offsets, 251 * sizeof(int));
+    memory.allocate(&error, sizeof(int));
+    cudaMemset(error, 0, sizeof(int));
+    for (const auto& batch : spans) {
+        graph::refresh_cost(state);
+        cudaMemcpy(d_points, points.data() + batch.points, batch.point_count * 4, cudaMemcpyHostToDevice);
+        cudaMemcpy(d_gb, gbpoints.data() + batch.gbpoints, batch.gb_count * 4, cudaMemcpyHostToDevice);
+        cudaMemcpy(d_offsets, offsets.data() + batch.offsets, batch.count * 4, cudaMemcpyHostToDevice);
+        cudaMemcpy(view.net_ids, ids.data() + batch.ids, batch.count * 4, cudaMemcpyHostToDevice);
+        grotor::zshape::reset_nodes<<<batch.count, 128>>>(map, d_points, layers, n, view.DIR ^ 1, batch.count);
+        grotor::zshape::solve<4><<<(batch.count + 3) / 4, 128>>>(map, d_points, {view, n}, {view, n}, prev,
+            prev + 10 * grid, raw, d_gb, nullptr, layers, n, view.DIR ^ 1, batch.count);
+        grotor::zshape::convert_routes<<<BLOCK_NUM(batch.count), THREAD_NUM>>>(batch.count, view.net_ids,
+            d_offsets, raw, n, view.L, view.X, view.Y, view.DIR, view.ROUTE_PER_PIN, view.pin_acc_num, view.routes, error);
+        const int stamp = ++state.global_timestamp;
+        graph::commit_wire_demand<<<BLOCK_NUM(batch.count), THREAD_NUM>>>(view, batch.count, 0, stamp);
+        graph::commit_via_demand<<<BLOCK_NUM(batch.count), THREAD_NUM>>>(view, batch.count, 0, stamp);
+    }
+    grotor::cuda_check(cudaDeviceSynchronize(), "Z-shape stage");
+    int status = 0;
+    cudaMemcpy(&status, error, sizeof(int), cudaMemcpyDeviceToHost);
+    const size_t cells = size_t(view.L) * view.X * view.Y;
+    std::vector<float> demand(cells);
+    cudaMemcpy(demand.data(), view.demand, cells * 4, cudaMemcpyDeviceToHost);
+    cudb::RoutingStatistics stats;
+    cudaMemcpy(&stats, view.statistics, sizeof(stats), cudaMemcpyDeviceToHost);
+    state.download_routes(false);
+    dump(dir, "z_routes", state.routes_cpu.get(), view.ROUTE_PER_PIN * view.PIN_NUM + 1);
+    dump(dir, "z_demand", demand);
+    std::vector<double> st{stats.total_wirelength, double(stats.total_via_count), double(state.global_timestamp),
+                           double(status)};
+    dump(dir, "z_stats", st);
+    printf("REF_ZSHAPE nets=%zu groups=%zu batches=%zu status=%d\n", order.size(), groups.size(), batches.size(), status);
+    memory.clear();
+    state.release_workspaces();
+    return 0;
+}
+#endif
+
 int run_batch(const std::string& dir, int limit, int sparsity) {
     const auto meta = load<int>(dir + "/meta.i32");
     const auto order = load<int>(dir + "/order.i32");
@@ -446,9 +592,12 @@ int main(int argc, char** argv) {
         if (mode == "route" && argc == 7) return run_route(argv[2], argv[3], argv[4], argv[5], argv[6]);
         if (mode == "snap" && argc == 7) return run_snap(argv[2], argv[3], argv[4], argv[5], std::stoi(argv[6]));
         if (mode == "flt" && argc == 6) return run_flt(argv[2], argv[3], argv[4], argv[5]);
+#ifdef GROTOR_GGR_ROUTING
+        if (mode == "zshape" && argc == 6) return run_zshape(argv[2], argv[3], argv[4], argv[5]);
+#endif
         if (mode == "batch" && argc == 5) return run_batch(argv[2], std::stoi(argv[3]), std::stoi(argv[4]));
         if (mode == "write" && argc == 8) return run_write(argv[2], argv[3], argv[4], argv[5], argv[6], argv[7]);
-        fprintf(stderr, "usage: ref_harness topo|route|snap|flt|batch|write ...\n");
+        fprintf(stderr, "usage: ref_harness topo|route|snap|flt|zshape|batch|write ...\n");
         return 2;
     } catch (const std::exception& e) {
         fprintf(stderr, "ref_harness error: %s\n", e.what());

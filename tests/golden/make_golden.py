@@ -9,6 +9,9 @@ sources by ``oracle/ref.mk``):
 * ``route`` and ``snap`` (GPU): routes, demand and statistics of the reference
   L-shape stage, cost tables after the stage, the .out file (SHA-256 and
   evaluator scores), and the cost tables before / routes after one batch;
+* ``zshape`` (GPU, Z-shape fixtures, reference GGR build ``ref_harness_ggr``):
+  the reference Z-shape pipeline -- order, first-fit groups, bbox batches,
+  encoded trees and net boxes, routes, demand and statistics after the stage;
 * ``flt`` (GPU, FLT fixtures): the reference default pipeline through its FLT
   stage -- demand and statistics before the stage, the rip-up set, the DAGs of
   the reference's host FLT builder, the FLT batching geometry and batches, and
@@ -17,6 +20,7 @@ sources by ``oracle/ref.mk``):
 Usage:  python tests/golden/make_golden.py --topo      (no GPU needed)
         python tests/golden/make_golden.py --route     (on a GPU box)
         python tests/golden/make_golden.py --flt       (on a GPU box)
+        python tests/golden/make_golden.py --zshape    (on a GPU box)
 The two passes update the same ``<name>.npz``.
 """
 from __future__ import annotations
@@ -47,6 +51,10 @@ FIXTURES = {
                                                     cap_hi=4)),
 }
 FLT_FIXTURES = {"ref_flt_48x48x10_1500"}
+FIXTURES["ref_z_48x48x10_1500"] = FIXTURES["ref_flt_48x48x10_1500"]
+FIXTURES["ref_z_40x56x10_800"] = ("small_64x64x5", dict(n_nets=800, cap_layers=10, seed=14, X=40, Y=56))
+Z_FIXTURES = {"ref_z_48x48x10_1500", "ref_z_40x56x10_800"}
+HARNESS_GGR = os.path.join(REF, "ref_harness_ggr")
 TOPO_KEYS = ["meta", "short_costs", "unit_costs", "x_edge_len", "y_edge_len", "capacity", "pin_acc_num",
              "node_off", "nodes", "parents", "point_off", "points", "hseg_off", "hsegs", "vseg_off", "vsegs",
              "hpwl", "original", "pin_count", "order", "batch_of", "ids", "batch_off", "pin_vias"]
@@ -95,6 +103,7 @@ def main():
     ap.add_argument("--topo", action="store_true")
     ap.add_argument("--route", action="store_true")
     ap.add_argument("--flt", action="store_true")
+    ap.add_argument("--zshape", action="store_true")
     ap.add_argument("--only", default=None)
     ap.add_argument("--outdir", default=HERE, help="where to write the .npz files")
     ap.add_argument("--keep-out", action="store_true", help="also copy the reference .out into --outdir")
@@ -107,14 +116,20 @@ def main():
         data = dict(np.load(src)) if os.path.exists(src) else {}
         with tempfile.TemporaryDirectory() as w:
             cap, net = design_files(name, w)
-            if args.topo:
+            if args.topo and name not in Z_FIXTURES:
                 subprocess.run([HARNESS, "topo", cap, net, w, REF], check=True, stdout=subprocess.DEVNULL)
                 data.update(read_dir(w, TOPO_KEYS))
+            if args.zshape and name in Z_FIXTURES:
+                subprocess.run([HARNESS_GGR, "zshape", cap, net, w, REF], check=True, stdout=subprocess.DEVNULL)
+                got = read_dir(w)
+                data.update({k: v for k, v in got.items()
+                             if k.startswith("z_") or k in ("meta", "short_costs", "unit_costs", "x_edge_len",
+                                                            "y_edge_len", "capacity", "pin_acc_num")})
             if args.flt and name in FLT_FIXTURES:
                 subprocess.run([HARNESS, "flt", cap, net, w, REF], check=True, stdout=subprocess.DEVNULL)
                 got = read_dir(w)
                 data.update({k: v for k, v in got.items() if k.startswith("flt_")})
-            if args.route and name not in FLT_FIXTURES:
+            if args.route and name not in FLT_FIXTURES and name not in Z_FIXTURES:
                 for k in TOPO_KEYS:  # the GPU passes read the committed plan
                     if k in data:
                         data[k].tofile(os.path.join(w, f"{k}.{_ext(data[k])}"))
