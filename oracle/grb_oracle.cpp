@@ -65,6 +65,7 @@ float wire_cost(const Grid& G, const int32_t* demand_half, int l, int x, int y) 
         w = static_cast<float>(std::fma(G.g->unit_wire, static_cast<double>(G.g->x_edge_len[x]), static_cast<double>(w)));
     if (G.along_y(l) && y < G.Y - 1)
         w = static_cast<float>(std::fma(G.g->unit_wire, static_cast<double>(G.g->y_edge_len[y]), static_cast<double>(w)));
+    if (G.g->integer_wire) w = static_cast<float>(static_cast<int64_t>(std::fmin(std::fmax(w, 0.f), 1.e7f)));
     return w;
 }
 
@@ -820,6 +821,378 @@ int orc_flt_stage(const orc_grid* g, const orc_flt* dags, int32_t n_batches, con
                     nullptr);
     }
     return status;
+}
+
+}  // extern "C"
+
+
+// ---------------------------------------------------------------------------
+// Z-shape stage (pipeline_ggr.hpp:72-134, zshape.cuh:5-404,
+// zshape_topology.hpp:7-57 and 249-290, demand.cuh:129-232).
+namespace {
+
+constexpr int kZInf = 1000000000;  // zshape.cuh:6
+
+// 32-bit integer addition with wrap-around, as the device code computes it.
+inline int zadd(int a, int b) { return static_cast<int>(static_cast<uint32_t>(a) + static_cast<uint32_t>(b)); }
+
+struct ZPlanes {
+    int LAYER, N, D, L, X, Y;
+    size_t NN, LNN;
+    std::vector<int> map, prev;   // 6 and 16 planes of LAYER*N*N (pipeline_ggr.hpp:105-106)
+    const double* presum;
+    const float* vcost;
+    int DIR;
+    int pidx(int i, int x, int y) const { return int(i * NN + (((i & 1) ^ D) ? x * N + y : y * N + x)); }
+    // WireCosts / ViaCosts (zshape.cuh:8-31): a plane index names (layer + 1, a, b).
+    double wsum(int index) const {
+        const int layer = index / int(NN) - 1;
+        if (layer < 0 || layer >= L) return 0;
+        const int a = index / N % N, b = index % N;
+        const bool ay = ((layer & 1) ^ DIR) != 0;
+        const int x = ay ? a : b, y = ay ? b : a;
+        return presum[(size_t(layer) * X + x) * Y + y];
+    }
+    int vc(int index) const {
+        const int layer = index / int(NN) - 1;
+        if (layer < 0 || layer >= L) return kZInf;
+        const int a = index / N % N, b = index % N;
+        const bool ay = ((layer & 1) ^ DIR) != 0;
+        const int x = ay ? a : b, y = ay ? b : a;
+        return int(std::fmin(std::fmax(vcost[(size_t(layer) * X + x) * Y + y], 1.f), 1.e6f));
+    }
+    int wc(int a, int b) const { return int(std::fmin(std::fabs(wsum(a) - wsum(b)), double(kZInf / 2))); }
+    int* M(int k) { return map.data() + k * LNN; }
+    int* P(int k) { return prev.data() + k * LNN; }
+    // viaSweep (zshape.cuh:42-61) on plane 4 at 2-D position (x, y).
+    void via_sweep(int x, int y) {
+        int* m = M(4);
+        int* p = P(4);
+        int* p5 = P(5);
+        for (int i = 1; i < LAYER; ++i) {
+            const int cur = int(i * NN + (((i & 1) ^ D) ? x * N + y : y * N + x));
+            p5[cur] = cur;
+        }
+        for (int i = 2; i < LAYER; ++i) {
+            const int cur = int(i * NN + (((i & 1) ^ D) ? x * N + y : y * N + x));
+            const int last = int((i - 1) * NN + (((i & 1) ^ D) ? y * N + x : x * N + y));
+            if (m[cur] > zadd(m[last], vc(last))) { m[cur] = zadd(m[last], vc(last)); p[cur] = p[last]; p5[cur] = last; }
+        }
+        for (int i = LAYER - 2; i >= 1; --i) {
+            const int cur = int(i * NN + (((i & 1) ^ D) ? x * N + y : y * N + x));
+            const int last = int((i + 1) * NN + (((i & 1) ^ D) ? y * N + x : x * N + y));
+            if (m[cur] > zadd(m[last], vc(cur))) { m[cur] = zadd(m[last], vc(cur)); p[cur] = p[last]; p5[cur] = last; }
+        }
+    }
+};
+
+struct ZNode { int pos, minl, maxl, child[3]; };
+
+// solve<4> (zshape.cuh:62-388) for one net, sequentially; `raw` receives the
+// reference's route encoding: [count, (start, length | -1)...].
+void zshape_net(ZPlanes& Z, const std::vector<ZNode>& nd, std::vector<int>& raw) {
+    const int LAYER = Z.LAYER, N = Z.N, D = Z.D;
+    raw.assign(1, 1);
+    const int cnt = int(nd.size());
+    int* map0 = Z.M(0);
+    int* prev0 = Z.P(0);
+    int* m4 = Z.M(4);
+    int* p4 = Z.P(4);
+    int* p5 = Z.P(5);
+    int* m5 = Z.M(5);
+    // reset_nodes (zshape.cuh:392-404).
+    for (const auto& v : nd)
+        for (int l = 0; l < LAYER; ++l)
+            for (int plane = 0; plane < 4; ++plane) Z.M(plane)[Z.pidx(l, v.pos / N, v.pos % N)] = kZInf;
+    for (int t = cnt - 1; t >= 0; --t) {
+        const int tox = nd[t].pos / N, toy = nd[t].pos % N, minlayer = nd[t].minl, maxlayer = nd[t].maxl;
+        for (int j = 1; j <= 3; ++j) {
+            if (nd[t].child[j - 1] == -1) continue;
+            int* mj = Z.M(j);
+            int* pj = Z.P(j);
+            int* p2j = Z.P(10 + j);
+            const int cp = nd[nd[t].child[j - 1]].pos, fromx = cp / N, fromy = cp % N;
+            const int minx = std::min(fromx, tox), maxx = std::max(fromx, tox);
+            const int miny = std::min(fromy, toy), maxy = std::max(fromy, toy);
+            if (fromx != tox && fromy != toy) {
+                for (int a = minx; a <= maxx; ++a)
+                    for (int i = 1; i < LAYER; ++i) {
+                        if ((i & 1) ^ D) { m4[i * Z.NN + a * N + toy] = kZInf; m4[i * Z.NN + a * N + fromy] = kZInf; }
+                        else { m4[i * Z.NN + toy * N + a] = kZInf; m4[i * Z.NN + fromy * N + a] = kZInf; }
+                    }
+                for (int b = miny; b <= maxy; ++b)
+                    for (int i = 1; i < LAYER; ++i) {
+                        if ((i & 1) ^ D) { m4[i * Z.NN + tox * N + b] = kZInf; m4[i * Z.NN + fromx * N + b] = kZInf; }
+                        else { m4[i * Z.NN + b * N + tox] = kZInf; m4[i * Z.NN + b * N + fromx] = kZInf; }
+                    }
+                for (int i = 1; i < LAYER; ++i) {
+                    if ((i & 1) ^ D) {
+                        const int last = int(i * Z.NN + fromx * N + fromy);
+                        for (int b = miny; b <= maxy; ++b) {
+                            if (b == fromy) continue;
+                            const int cur = int(i * Z.NN + fromx * N + b);
+                            m4[cur] = zadd(map0[last], Z.wc(last, cur));
+                            p4[cur] = last;
+                        }
+                    } else {
+                        const int last = int(i * Z.NN + fromy * N + fromx);
+                        for (int b = minx; b <= maxx; ++b) {
+                            if (b == fromx) continue;
+                            const int cur = int(i * Z.NN + fromy * N + b);
+                            m4[cur] = zadd(map0[last], Z.wc(last, cur));
+                            p4[cur] = last;
+                        }
+                    }
+                }
+                for (int b = miny; b <= maxy; ++b) if (b != fromy) Z.via_sweep(fromx, b);
+                for (int b = minx; b <= maxx; ++b) if (b != fromx) Z.via_sweep(b, fromy);
+                for (int i = 1; i < LAYER; ++i) {
+                    if ((i & 1) ^ D) {
+                        for (int b = minx; b <= maxx; ++b) {
+                            const int last = int(i * Z.NN + b * N + fromy), cur = int(i * Z.NN + b * N + toy);
+                            const int c = Z.wc(last, cur);
+                            if (zadd(m4[last], c) < m4[cur]) { m4[cur] = zadd(m4[last], c); p4[cur] = p4[last]; }
+                        }
+                    } else {
+                        for (int b = miny; b <= maxy; ++b) {
+                            const int last = int(i * Z.NN + b * N + fromx), cur = int(i * Z.NN + b * N + tox);
+                            const int c = Z.wc(last, cur);
+                            if (zadd(m4[last], c) < m4[cur]) { m4[cur] = zadd(m4[last], c); p4[cur] = p4[last]; }
+                        }
+                    }
+                }
+                for (int b = miny; b <= maxy; ++b) if (b != toy) Z.via_sweep(tox, b);
+                for (int b = minx; b <= maxx; ++b) if (b != tox) Z.via_sweep(b, toy);
+                for (int i = 1; i < LAYER; ++i) {
+                    if ((i & 1) ^ D) {
+                        const int cur = int(i * Z.NN + tox * N + toy);
+                        for (int b = miny; b <= maxy; ++b) {
+                            if (b == toy) continue;
+                            const int last = int(i * Z.NN + tox * N + b);
+                            const int c = Z.wc(last, cur);
+                            if (zadd(m4[last], c) < mj[cur]) { mj[cur] = zadd(m4[last], c); pj[cur] = p4[last]; p2j[cur] = p5[last]; }
+                        }
+                    } else {
+                        const int cur = int(i * Z.NN + toy * N + tox);
+                        for (int b = minx; b <= maxx; ++b) {
+                            if (b == tox) continue;
+                            const int last = int(i * Z.NN + toy * N + b);
+                            const int c = Z.wc(last, cur);
+                            if (zadd(m4[last], c) < mj[cur]) { mj[cur] = zadd(m4[last], c); pj[cur] = p4[last]; p2j[cur] = p5[last]; }
+                        }
+                    }
+                }
+            } else if (fromx == tox) {
+                for (int i = 1; i < LAYER; ++i) {
+                    if ((i & 1) ^ D) {
+                        const int last = int(i * Z.NN + fromx * N + fromy), cur = int(i * Z.NN + tox * N + toy);
+                        const int c = Z.wc(last, cur);
+                        if (mj[cur] > zadd(map0[last], c)) { mj[cur] = zadd(map0[last], c); pj[cur] = last; }
+                    } else {
+                        mj[i * Z.NN + toy * N + tox] = kZInf;
+                    }
+                }
+            } else if (fromy == toy) {
+                for (int i = 1; i < LAYER; ++i) {
+                    if ((!(i & 1)) ^ D) {
+                        const int last = int(i * Z.NN + fromy * N + fromx), cur = int(i * Z.NN + toy * N + tox);
+                        const int c = Z.wc(last, cur);
+                        if (mj[cur] > zadd(map0[last], c)) { mj[cur] = zadd(map0[last], c); pj[cur] = last; }
+                    } else {
+                        mj[i * Z.NN + tox * N + toy] = kZInf;
+                    }
+                }
+            }
+        }
+        // Layer-range DP at the node (zshape.cuh:241-267).
+        for (int lower = 0; lower < LAYER; ++lower) {
+            int viaSum = 0, minCost = kZInf, bestpos[3] = {0, 0, 0};
+            int costs[3] = {nd[t].child[0] == -1 ? 0 : kZInf, nd[t].child[1] == -1 ? 0 : kZInf,
+                            nd[t].child[2] == -1 ? 0 : kZInf};
+            for (int upper = lower; upper < LAYER; ++upper) {
+                const int idx = Z.pidx(upper, tox, toy);
+                for (int j = 0; j < 3; ++j)
+                    if (nd[t].child[j] != -1 && Z.M(j + 1)[idx] < costs[j]) { costs[j] = Z.M(j + 1)[idx]; bestpos[j] = upper; }
+                if (1LL * costs[0] + costs[1] + costs[2] < minCost) minCost = costs[0] + costs[1] + costs[2];
+                if (minlayer == -1 || (lower <= minlayer && maxlayer <= upper)) {
+                    for (int i = lower; i <= upper; ++i) {
+                        const int index = Z.pidx(i, tox, toy);
+                        if (map0[index] > zadd(minCost, viaSum)) {
+                            map0[index] = zadd(minCost, viaSum);
+                            prev0[index] = (((lower * LAYER + upper) * LAYER + bestpos[2]) * LAYER + bestpos[1]) * LAYER + bestpos[0];
+                        }
+                    }
+                }
+                viaSum = zadd(viaSum, Z.vc(idx));
+            }
+        }
+    }
+    // Traceback (zshape.cuh:271-386).
+    auto emit = [&](int a, int b) { raw.push_back(a); raw.push_back(b); raw[0] += 2; };
+    int minTotal = kZInf;
+    {
+        const int x = nd[0].pos / N, y = nd[0].pos % N;
+        for (int i = 0; i < LAYER; ++i) {
+            const int idx = Z.pidx(i, x, y);
+            if (map0[idx] < minTotal) { minTotal = map0[idx]; m5[nd[0].pos] = i; }
+        }
+    }
+    if (minTotal == kZInf || minTotal < 0) { raw[0] = -1; return; }
+    for (int t = 0; t < cnt; ++t) {
+        const int x = nd[t].pos / N, y = nd[t].pos % N, layer = m5[nd[t].pos];
+        const int idx = Z.pidx(layer, x, y);
+        const int minl = prev0[idx] / LAYER / LAYER / LAYER / LAYER, maxl = prev0[idx] / LAYER / LAYER / LAYER % LAYER;
+        for (int i = minl; i < maxl; ++i) emit(Z.pidx(i, x, y), -1);
+        int bestpos = prev0[idx];
+        for (int j = 0; j < 3; ++j) {
+            if (nd[t].child[j] == -1) break;
+            const int child = nd[nd[t].child[j]].pos;
+            const int entrylayer = bestpos % LAYER, entry = Z.pidx(entrylayer, x, y);
+            bestpos /= LAYER;
+            const int last = Z.P(j + 1)[entry];
+            const int lastlayer = last / int(Z.NN);
+            int lastx = last / N % N, lasty = last % N;
+            if ((!(lastlayer & 1)) ^ D) std::swap(lastx, lasty);
+            if (lastx != x && lasty != y) {
+                const int mid = Z.P(11 + j)[entry];
+                const int midlayer = mid / int(Z.NN);
+                int midx = mid / N % N, midy = mid % N;
+                if ((!(midlayer & 1)) ^ D) std::swap(midx, midy);
+                const int p1 = ((entrylayer & 1) ^ D) ? entry - y + midy : entry - x + midx;
+                const int p3 = ((midlayer & 1) ^ D) ? mid - midy + lasty : mid - midx + lastx;
+                const int p4 = ((lastlayer & 1) ^ D) ? last - lasty + midy : last - lastx + midx;
+                if (entry != p1) emit(std::min(entry, p1), std::max(entry, p1) - std::min(entry, p1));
+                if (p1 != mid)
+                    for (int i = std::min(entrylayer, midlayer); i < std::max(entrylayer, midlayer); ++i) emit(Z.pidx(i, midx, midy), -1);
+                if (mid != p3) emit(std::min(mid, p3), std::max(mid, p3) - std::min(mid, p3));
+                if (p3 != p4) {
+                    int tx = p3 / N % N, ty = p3 % N;
+                    if ((!((p3 / int(Z.NN)) & 1)) ^ D) std::swap(tx, ty);
+                    for (int i = std::min(midlayer, lastlayer); i < std::max(midlayer, lastlayer); ++i) emit(Z.pidx(i, tx, ty), -1);
+                }
+                if (p4 != last) emit(std::min(p4, last), std::max(p4, last) - std::min(p4, last));
+            } else {
+                emit(std::min(last, entry), std::max(last, entry) - std::min(last, entry));
+            }
+            m5[child] = lastlayer;
+        }
+    }
+}
+
+// convert_routes (zshape_topology.hpp:249-290).
+int zshape_convert(const ZPlanes& Z, const std::vector<int>& src, int32_t* dst, int64_t cap) {
+    int status = 0;
+    const int n = Z.N, XY = Z.X * Z.Y;
+    int out = 1;
+    for (size_t p = 1; p + 1 < size_t(std::max(src[0], 0)); p += 2) {
+        const int start = src[p], len = src[p + 1];
+        const int layer = start / (n * n) - 1;
+        const int a = start / n % n, b = start % n;
+        const bool ay = ((layer & 1) ^ Z.DIR) != 0;
+        const int x = ay ? a : b, y = ay ? b : a;
+        if (layer < 0 || layer >= Z.L || x >= Z.X || y >= Z.Y) { status = 3; continue; }
+        const int pos0 = layer * XY + x * Z.Y + y;
+        int pos1 = pos0;
+        if (len == -1) {
+            if (layer + 1 >= Z.L) { status = 3; continue; }
+            pos1 += XY;
+        } else {
+            const int end = start + len, ea = end / n % n, eb = end % n;
+            const int ex = ay ? ea : eb, ey = ay ? eb : ea;
+            if (ex >= Z.X || ey >= Z.Y) { status = 3; continue; }
+            pos1 = layer * XY + ex * Z.Y + ey;
+        }
+        if (out + 1 < cap) { dst[out++] = pos0; dst[out++] = pos1; }
+        else status = 1;
+    }
+    if (src[0] <= 0) status = 2;
+    dst[0] = out;
+    return status;
+}
+
+}  // namespace
+
+extern "C" {
+
+int orc_zshape_stage(const orc_grid* g, const orc_ztrees* trees, int32_t n_batches, const int32_t* batch_off,
+                     const int32_t* ids, const int64_t* route_off, int32_t* routes, int32_t* demand_half,
+                     int32_t* timestamp, int32_t* stamp, double* total_wirelength, int64_t* total_vias) {
+    Grid G(g);
+    ZPlanes Z;
+    Z.L = g->L; Z.X = g->X; Z.Y = g->Y; Z.DIR = g->DIR;
+    Z.LAYER = g->L + 1; Z.N = std::max(g->X, g->Y); Z.D = g->DIR ^ 1;
+    Z.NN = size_t(Z.N) * Z.N; Z.LNN = Z.LAYER * Z.NN;
+    Z.map.assign(6 * Z.LNN, 0);
+    Z.prev.assign(16 * Z.LNN, 0);
+    const size_t cells = size_t(g->L) * g->X * g->Y;
+    std::vector<float> wcost(cells), vcost(cells);
+    std::vector<double> presum(cells);
+    Z.presum = presum.data();
+    Z.vcost = vcost.data();
+    int status = 0;
+    std::vector<int> raw;
+    std::vector<ZNode> nd;
+    for (int b = 0; b < n_batches; ++b) {
+        orc_cost_full(g, demand_half, wcost.data(), vcost.data());
+        orc_presum(g, wcost.data(), presum.data());
+        const int n = batch_off[b + 1] - batch_off[b];
+        const int32_t* bid = ids + batch_off[b];
+        for (int k = 0; k < n; ++k) {
+            const int id = bid[k];
+            const int nb = trees->node_off[id], cnt = trees->node_off[id + 1] - nb;
+            nd.assign(cnt, ZNode{});
+            for (int i = 0; i < cnt; ++i) {  // encode_batch (zshape_topology.hpp:100-116)
+                const int c = trees->coord[nb + i], l = c / (g->X * g->Y), p2 = c % (g->X * g->Y);
+                nd[i].pos = (p2 / g->Y) * Z.N + p2 % g->Y;
+                nd[i].minl = nd[i].maxl = l < g->L ? l + 1 : -1;
+                for (int j = 0; j < 3; ++j) nd[i].child[j] = trees->child[3 * (nb + i) + j];
+            }
+            if (cnt) zshape_net(Z, nd, raw);
+            else raw.assign(1, 1);
+            const int rc = zshape_convert(Z, raw, routes + route_off[id], route_off[id + 1] - route_off[id]);
+            if (rc) status = rc;
+        }
+        const int32_t s = ++*stamp;
+        commit_impl(g, n, bid, route_off, routes, s, 1, demand_half, timestamp, total_wirelength, total_vias, nullptr);
+    }
+    (void)G;
+    return status;
+}
+
+int32_t orc_bbox_batches(int32_t X, int32_t Y, int32_t n, const int32_t* group, const int32_t* bbox,
+                         int32_t max_batch, int32_t* ids, int32_t* off) {
+    std::vector<int> pending(group, group + n);
+    auto area = [&](int id) {
+        return int64_t(bbox[4 * id + 1] - bbox[4 * id] + 1) * (bbox[4 * id + 3] - bbox[4 * id + 2] + 1);
+    };
+    std::sort(pending.begin(), pending.end(), [&](int l, int r) {
+        return area(l) == area(r) ? l > r : area(l) > area(r);
+    });
+    std::vector<unsigned char> occupied(size_t(X) * Y, 0);
+    int nb = 0, out = 0, routed = 0;
+    off[0] = 0;
+    while (routed < n) {
+        std::fill(occupied.begin(), occupied.end(), 0);
+        int count = 0;
+        for (int& id : pending) {
+            if (id < 0) continue;
+            const int* bb = bbox + 4 * id;
+            bool conflict = false;
+            for (int x = bb[0]; x <= bb[1] && !conflict; ++x)
+                for (int y = bb[2]; y <= bb[3]; ++y)
+                    if (occupied[size_t(x) * Y + y]) { conflict = true; break; }
+            if (conflict) continue;
+            for (int x = bb[0]; x <= bb[1]; ++x)
+                for (int y = bb[2]; y <= bb[3]; ++y) occupied[size_t(x) * Y + y] = 1;
+            ids[out++] = id;
+            id = -1;
+            ++routed;
+            if (++count == max_batch) break;
+        }
+        if (!count) break;
+        off[++nb] = out;
+    }
+    return nb;
 }
 
 }  // extern "C"

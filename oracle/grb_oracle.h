@@ -34,6 +34,7 @@ typedef struct orc_grid {
     const int32_t* x_edge_len;   /* [X-1] */
     const int32_t* y_edge_len;   /* [Y-1] */
     const float* capacity;       /* [L*X*Y] */
+    int32_t integer_wire;        /* 1: GGR build's wire costs, clamped to [0, 1e7] and truncated (full_update.cuh:47-50) */
 } orc_grid;
 
 /* Full cost recompute: wcost/vcost from capacity and demand. */
@@ -118,6 +119,34 @@ int orc_flt_stage(const orc_grid* g, const orc_flt* dags, int32_t n_batches, con
                   const int64_t* route2_off, int32_t* routes2, int32_t remove_phase_one,
                   int32_t* demand_half, int32_t* timestamp, int32_t* stamp,
                   double* total_wirelength, int64_t* total_vias, int32_t nthreads);
+
+/* Z-shape trees in the reference's encoding (zshape::encode_batch,
+ * zshape_topology.hpp:59-121), CSR by net id: nodes in preorder from the
+ * first leaf, 3-D coordinate (layer L = Steiner point) and up to three child
+ * preorder indices per node (-1 = none). */
+typedef struct orc_ztrees {
+    const int32_t* node_off;
+    const int32_t* coord;
+    const int32_t* child;   /* [3 per node] */
+} orc_ztrees;
+
+/* Z-shape stage (pipeline_ggr.hpp:119-134) over an explicit batch plan in
+ * execution order: per batch, full cost refresh, Z-shape DP and traceback per
+ * net (zshape.cuh:42-388), conversion to route words (zshape_topology.hpp:
+ * 249-290) at route_off[id], ++stamp, thread-per-net wire then via commit
+ * (demand.cuh:129-232).  Returns the reference's status: 0, 1 (route storage),
+ * 2 (no finite route), 3 (segment outside the grid). */
+int orc_zshape_stage(const orc_grid* g, const orc_ztrees* trees, int32_t n_batches, const int32_t* batch_off,
+                     const int32_t* ids, const int64_t* route_off, int32_t* routes, int32_t* demand_half,
+                     int32_t* timestamp, int32_t* stamp, double* total_wirelength, int64_t* total_vias);
+
+/* Bounding-box refinement of one first-fit group (zshape::generate_bbox_batches,
+ * zshape_topology.hpp:7-57): nets sorted by box area (descending, larger id
+ * first on ties), greedy rounds of at most max_batch nets with disjoint boxes.
+ * bbox is [minx, maxx, miny, maxy] per net id.  Writes the refined batches
+ * (ids, off) and returns their number. */
+int32_t orc_bbox_batches(int32_t X, int32_t Y, int32_t n, const int32_t* group, const int32_t* bbox,
+                         int32_t max_batch, int32_t* ids, int32_t* off);
 
 #ifdef __cplusplus
 }

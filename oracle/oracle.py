@@ -12,7 +12,8 @@ _LIB = os.path.join(_HERE, "liboracle.so")
 
 __all__ = [
     "build", "load", "OrcGrid", "cost_full", "presum", "presum_logstep", "lshape_batch",
-    "commit_batch", "batches", "ripup_classify", "congestion_view", "lshape_stage", "flt_stage",
+    "commit_batch", "batches", "ripup_classify", "congestion_view", "lshape_stage", "flt_stage", "zshape_stage",
+    "bbox_batches",
 ]
 
 
@@ -39,7 +40,7 @@ class _COrcGrid(C.Structure):
         ("L", C.c_int32), ("X", C.c_int32), ("Y", C.c_int32), ("DIR", C.c_int32),
         ("unit_wire", C.c_double), ("unit_via", C.c_double), ("of_cost_scale", C.c_double),
         ("short_costs", C.c_void_p), ("x_edge_len", C.c_void_p), ("y_edge_len", C.c_void_p),
-        ("capacity", C.c_void_p),
+        ("capacity", C.c_void_p), ("integer_wire", C.c_int32),
     ]
 
 
@@ -61,6 +62,10 @@ def _declare(lib):
     lib.orc_lshape_stage.restype = C.c_int
     lib.orc_flt_stage.argtypes = [P, P, C.c_int32, P, P, P, P, P, P, C.c_int32, P, P, P, P, P, C.c_int32]
     lib.orc_flt_stage.restype = C.c_int
+    lib.orc_zshape_stage.argtypes = [P, P, C.c_int32, P, P, P, P, P, P, P, P, P]
+    lib.orc_zshape_stage.restype = C.c_int
+    lib.orc_bbox_batches.argtypes = [C.c_int32, C.c_int32, C.c_int32, P, P, C.c_int32, P, P]
+    lib.orc_bbox_batches.restype = C.c_int32
 
 
 class _COrcFlt(C.Structure):
@@ -80,7 +85,7 @@ class OrcGrid:
     """Grid arrays in the oracle's layout (keeps the numpy buffers alive)."""
 
     def __init__(self, L, X, Y, DIR, unit_wire, unit_via, short_costs, x_edge_len, y_edge_len, capacity,
-                 of_cost_scale=1.0):
+                 of_cost_scale=1.0, integer_wire=False):
         self.L, self.X, self.Y, self.DIR = int(L), int(X), int(Y), int(DIR)
         self.short_costs = _c(short_costs, np.float64)
         self.x_edge_len = _c(x_edge_len, np.int32)
@@ -88,7 +93,8 @@ class OrcGrid:
         self.capacity = _c(capacity, np.float32).reshape(-1)
         self.unit_wire, self.unit_via, self.of_cost_scale = float(unit_wire), float(unit_via), float(of_cost_scale)
         self._s = _COrcGrid(self.L, self.X, self.Y, self.DIR, self.unit_wire, self.unit_via, self.of_cost_scale,
-                            _p(self.short_costs), _p(self.x_edge_len), _p(self.y_edge_len), _p(self.capacity))
+                            _p(self.short_costs), _p(self.x_edge_len), _p(self.y_edge_len), _p(self.capacity),
+                            int(bool(integer_wire)))
 
     @property
     def cells(self):
@@ -217,3 +223,40 @@ def flt_stage(g: OrcGrid, dags: dict, ids, batch_off, route_off, routes, route2_
                            _p(demand), _p(ts), C.byref(st), C.byref(wl), C.byref(vi), int(threads))
     return {"status": rc, "routes2": routes2, "demand_half": demand, "timestamp": ts, "stamp": st.value,
             "wirelength": wl.value, "vias": vi.value}
+
+
+class _COrcZTrees(C.Structure):
+    _fields_ = [(k, C.c_void_p) for k in ("node_off", "coord", "child")]
+
+
+def zshape_stage(g: OrcGrid, trees: dict, ids, batch_off, route_off, demand_half=None, timestamp=None, stamp=0,
+                 wirelength=0.0, vias=0):
+    """Z-shape stage on the CPU (g built with integer_wire=True for the
+    reference's GGR cost mode).  `trees`: node_off, coord, child (3 per node)."""
+    lib = load()
+    keep = {k: _c(trees[k], np.int32) for k, _ in _COrcZTrees._fields_}
+    t = _COrcZTrees(**{k: v.ctypes.data for k, v in keep.items()})
+    ids = _c(ids, np.int32)
+    batch_off = _c(batch_off, np.int32)
+    route_off = _c(route_off, np.int64)
+    routes = np.zeros(int(route_off[-1]), np.int32)
+    demand = np.zeros(g.cells, np.int32) if demand_half is None else _c(demand_half, np.int32).copy()
+    ts = np.zeros(g.cells, np.int32) if timestamp is None else _c(timestamp, np.int32).copy()
+    st = C.c_int32(stamp)
+    wl = C.c_double(wirelength)
+    vi = C.c_int64(vias)
+    rc = lib.orc_zshape_stage(g.ref, C.byref(t), len(batch_off) - 1, _p(batch_off), _p(ids), _p(route_off),
+                              _p(routes), _p(demand), _p(ts), C.byref(st), C.byref(wl), C.byref(vi))
+    return {"status": rc, "routes": routes, "demand_half": demand, "timestamp": ts, "stamp": st.value,
+            "wirelength": wl.value, "vias": vi.value}
+
+
+def bbox_batches(X, Y, group, bbox, max_batch=250):
+    """Bounding-box refinement of one first-fit group: list of batches."""
+    lib = load()
+    group = _c(group, np.int32)
+    ids = np.empty(len(group), np.int32)
+    off = np.empty(len(group) + 1, np.int32)
+    nb = lib.orc_bbox_batches(int(X), int(Y), len(group), _p(group), _p(_c(bbox, np.int32)), int(max_batch),
+                              _p(ids), _p(off))
+    return [ids[off[k]:off[k + 1]].tolist() for k in range(nb)]

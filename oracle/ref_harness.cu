@@ -423,6 +423,10 @@ int run_zshape(const std::string& cap, const std::string& net, const std::string
     for (auto& b : batches) { zb_ids.insert(zb_ids.end(), b.begin(), b.end()); zb_off.push_back(zb_ids.size()); }
     dump_grid(dir, state);
     dump(dir, "pin_acc_num", state.pin_cnt_sum_cpu);
+    std::vector<int> pin_vias{0};  // initial via statistic (preprocess.hpp:1716-1718)
+    for (auto& dbnet : db::nets)
+        for (int pin : dbnet.pins) pin_vias[0] += pin < view.X * view.Y;
+    dump(dir, "pin_vias", pin_vias);
     dump(dir, "z_order", order); dump(dir, "z_group_ids", group_ids); dump(dir, "z_group_off", group_off);
     dump(dir, "z_batch_ids", zb_ids); dump(dir, "z_batch_off", zb_off);
     // Per-net trees in the encoding of zshape::encode_batch (zshape_topology.hpp:59-121),

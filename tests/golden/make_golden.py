@@ -124,7 +124,7 @@ def main():
                 got = read_dir(w)
                 data.update({k: v for k, v in got.items()
                              if k.startswith("z_") or k in ("meta", "short_costs", "unit_costs", "x_edge_len",
-                                                            "y_edge_len", "capacity", "pin_acc_num")})
+                                                            "y_edge_len", "capacity", "pin_acc_num", "pin_vias")})
             if args.flt and name in FLT_FIXTURES:
                 subprocess.run([HARNESS, "flt", cap, net, w, REF], check=True, stdout=subprocess.DEVNULL)
                 got = read_dir(w)
