@@ -45,6 +45,10 @@ class GrbFltDags(C.Structure):
                                  "edge_source_slot", "route2_off")]
 
 
+class GrbZshapeTrees(C.Structure):
+    _fields_ = [(k, P) for k in ("node_off", "coord", "child")]
+
+
 class GrbSynthParams(C.Structure):
     _fields_ = [
         ("X", C.c_int32), ("Y", C.c_int32), ("cap_layers", C.c_int32), ("n_nets", C.c_int32),
@@ -78,6 +82,10 @@ SIGNATURES = {
     "grb_upload_flt": (C.c_int, [P, C.POINTER(GrbFltDags)]),
     "grb_flt_stage": (C.c_int, [P, C.c_int32, C.c_int32, C.POINTER(GrbStats)]),
     "grb_read_routes2": (C.c_int, [P, P]),
+    "grb_set_wire_cost_mode": (C.c_int, [P, C.c_int32]),
+    "grb_upload_zshape": (C.c_int, [P, C.POINTER(GrbZshapeTrees)]),
+    "grb_plan_bbox_batches": (C.c_int, [P, P, C.c_int32, C.POINTER(C.c_int32)]),
+    "grb_zshape_stage": (C.c_int, [P, C.c_int32, C.POINTER(GrbStats)]),
     "grb_congestion_view": (C.c_int, [P, P, P, P]),
     "grb_read_tables": (C.c_int, [P, P, P, P, P, P]),
     "grb_read_routes": (C.c_int, [P, P]),

@@ -92,4 +92,71 @@ __device__ __forceinline__ void commit_net_vias(const Tables& T, const Plan& P, 
     if (lane == 0 && vias) atomicAdd(T.vias, static_cast<unsigned long long>(vias * K));
 }
 
+// Thread-per-net forms (commit_wire_demand / commit_via_demand,
+// demand.cuh:129-232), used where the reference commits one net per thread
+// (the Z-shape stage).  Same demand, timestamps, dirty marks and statistics as
+// the warp forms above.
+__device__ __forceinline__ void commit_thread_wires(const Tables& T, const Plan& P, int id, int stamp, int K) {
+    const int* r = net_routes(P, id);
+    const int words = r[0];
+    double length = 0;
+    for (int i = 1; i < words; i += 2) {
+        const int a = r[i], b = r[i + 1], layer = a / T.XY;
+        if (layer != b / T.XY) continue;
+        const int ra = a - layer * T.XY, rb = b - layer * T.XY;
+        const int x0 = ra / T.Y, y0 = ra - x0 * T.Y, x1 = rb / T.Y, y1 = rb - x1 * T.Y;
+        const bool ay = x0 == x1;
+        const int lo = ay ? min(y0, y1) : min(x0, x1), hi = ay ? max(y0, y1) : max(x0, x1);
+        T.ts[a] = stamp;
+        T.ts[b] = stamp;
+        if (hi > lo) {
+            mark_group_dirty(T, layer, ay ? x0 : y0);
+            if (ay) {
+                const int first = layer * T.XY + x0 * T.Y + lo;
+                mark_range(T.dirty_wire, first, first + (hi - lo) - 1);
+                mark_range(T.dirty_via, first, first + (hi - lo));
+            }
+        }
+        for (int pos = lo; pos < hi; ++pos) {
+            const int c = layer * T.XY + (ay ? x0 * T.Y + pos : pos * T.Y + y0);
+            atomicAdd(T.demand + c, 2 * K);
+            T.ts[c] = stamp;
+            if (!ay) {
+                set_bits(T.dirty_wire, c >> 5, 1u << (c & 31));
+                set_bits(T.dirty_via, c >> 5, 1u << (c & 31));
+                if (pos + 1 < T.X) set_bits(T.dirty_via, (c + T.Y) >> 5, 1u << ((c + T.Y) & 31));
+            }
+            length += ay ? T.ylen[pos] : T.xlen[pos];
+        }
+    }
+    if (length != 0.0) atomicAdd(T.wirelength, length * K);
+}
+
+__device__ __forceinline__ void commit_thread_vias(const Tables& T, const Plan& P, int id, int stamp, int K) {
+    const int* r = net_routes(P, id);
+    const int words = r[0];
+    long long vias = 0;
+    for (int i = 1; i < words; i += 2) {
+        const int a = r[i], b = r[i + 1];
+        const int la = a / T.XY, lb = b / T.XY;
+        const int low = min(la, lb), high = max(la, lb);
+        if (low == high) continue;
+        const int ra = a - la * T.XY, x = ra / T.Y, y = ra - x * T.Y;
+        vias += high - low;
+        for (int layer = low; layer < high; ++layer) {
+            const int c = layer * T.XY + x * T.Y + y;
+            if (T.ts[c] >= stamp) continue;
+            const bool ay = along_y(T, layer);
+            const int pos = ay ? y : x, len = ay ? T.Y : T.X, stride = ay ? 1 : T.Y;
+            if (!pos) add_via_demand(T, c, 2 * K);
+            else if (pos == len - 1) add_via_demand(T, c - stride, 2 * K);
+            else {
+                add_via_demand(T, c - stride, K);
+                add_via_demand(T, c, K);
+            }
+        }
+    }
+    if (vias) atomicAdd(T.vias, static_cast<unsigned long long>(vias * K));
+}
+
 }  // namespace grb

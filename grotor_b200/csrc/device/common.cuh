@@ -36,6 +36,7 @@ struct Tables {
     unsigned* dirty_wire;  // one bit per cell
     unsigned* dirty_via;   // one bit per cell
     int words;             // bitmap words
+    int int_wire;          // 1: wire costs clamped to [0, 1e7] and truncated (GGR build)
     // Prefix groups: kTrackGroup adjacent tracks of one layer.
     int group_base[kMaxLayers + 1];
     unsigned* group_flag;  // [n_groups], nonzero = some track of the group changed

@@ -45,6 +45,9 @@ __device__ __forceinline__ float wire_cost_at(const Tables& T, int c) {
     float w = static_cast<float>(incremental_of_cost(T, c, l, 1.0));
     if (!along_y(T, l) && x < T.X - 1) w = static_cast<float>(fma(T.unit_wire, static_cast<double>(T.xlen[x]), static_cast<double>(w)));
     if (along_y(T, l) && y < T.Y - 1) w = static_cast<float>(fma(T.unit_wire, static_cast<double>(T.ylen[y]), static_cast<double>(w)));
+    // The GGR build keeps integer DP edges non-negative and below its sentinel
+    // (full_update.cuh:47-50).
+    if (T.int_wire) w = static_cast<float>(static_cast<long long>(fminf(fmaxf(w, 0.f), 1.e7f)));
     return w;
 }
 

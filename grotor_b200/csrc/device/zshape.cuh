@@ -1,0 +1,378 @@
+// zshape.cuh -- Z-shape stage: two-bend candidates on projection planes,
+// layer-range DP per tree node and traceback; bounding-box batch refinement.
+//
+// Semantics of the reference's Z-shape pipeline (zshape.cuh:5-404,
+// zshape_topology.hpp:7-57 and 249-290).  All costs are int32: a wire costs
+// |presum[a] - presum[b]| clamped to 5e8, a via clamp(vcost, 1, 1e6), with 1e9
+// as infinity; sums wrap as 32-bit integers exactly as the device code does.
+// Planes of LAYER = L+1 layers of N x N (N = max(X, Y)) hold, per 2-D position
+// and layer: map 0 = node DP, 1..3 = best arrival of child slot j, 4 = the
+// current edge's candidate rows and columns, 5 = chosen layer per node; prev
+// 0..5 the matching back-pointers, prev 11..13 the turn cells of slot j.
+// A position on GGR layer i sits at i*N*N + (x*N + y) when ((i & 1) ^ D) is 1,
+// at i*N*N + (y*N + x) otherwise, D = DIR ^ 1; GGR layer i is routing layer
+// i-1 (layer 0 carries no wires and costs an infinite via).
+//
+// B200 form: one warp per net (as the reference); the nets of a batch have
+// disjoint bounding boxes, so their plane cells never overlap.  Lanes split
+// each row/column relaxation and the via sweeps; the node DP and the
+// traceback run on lane 0 in the reference's order.  The traceback converts
+// each segment straight into route words (convert_routes).
+#pragma once
+#include "commit.cuh"
+#include "common.cuh"
+
+namespace grb {
+
+constexpr int kZInf = 1000000000;  // zshape.cuh:6
+
+struct ZTrees {
+    const int* node_off;  // [n+1] by net id
+    const int* pos;       // per node: x*N + y
+    const int* pin;       // per node: pin layer + 1, -1 for Steiner points
+    const int* child;     // [3 per node] net-local preorder index, -1 = none
+    int* map;             // 6 planes
+    int* prev;            // 16 planes
+    int N, LAYER, D;
+    long long NN, LNN;
+};
+
+__device__ __forceinline__ int zadd(int a, int b) {
+    return static_cast<int>(static_cast<unsigned>(a) + static_cast<unsigned>(b));
+}
+__device__ __forceinline__ int zidx(const ZTrees& Z, int i, int x, int y) {
+    return static_cast<int>(i * Z.NN + (((i & 1) ^ Z.D) ? x * Z.N + y : y * Z.N + x));
+}
+// WireCosts (zshape.cuh:8-19): prefix value at a plane index.
+__device__ __forceinline__ double zsum(const Tables& T, const ZTrees& Z, int index) {
+    const int layer = static_cast<int>(index / Z.NN) - 1;
+    if (layer < 0 || layer >= T.L) return 0;
+    const int a = index / Z.N % Z.N, b = index % Z.N;
+    const bool ay = along_y(T, layer);
+    return T.presum[cell_index(T, layer, ay ? a : b, ay ? b : a)];
+}
+// ViaCosts (zshape.cuh:20-31).
+__device__ __forceinline__ int zvia(const Tables& T, const ZTrees& Z, int index) {
+    const int layer = static_cast<int>(index / Z.NN) - 1;
+    if (layer < 0 || layer >= T.L) return kZInf;
+    const int a = index / Z.N % Z.N, b = index % Z.N;
+    const bool ay = along_y(T, layer);
+    return static_cast<int>(fminf(fmaxf(T.vcost[cell_index(T, layer, ay ? a : b, ay ? b : a)], 1.f), 1.e6f));
+}
+// boundedWireCost (zshape.cuh:32-35).
+__device__ __forceinline__ int zwire(const Tables& T, const ZTrees& Z, int a, int b) {
+    return static_cast<int>(fmin(fabs(zsum(T, Z, a) - zsum(T, Z, b)), static_cast<double>(kZInf / 2)));
+}
+
+// viaSweep (zshape.cuh:42-61) on plane 4 at 2-D position (x, y): up, then down.
+__device__ __forceinline__ void zvia_sweep(const Tables& T, const ZTrees& Z, int x, int y) {
+    int* m = Z.map + 4 * Z.LNN;
+    int* p = Z.prev + 4 * Z.LNN;
+    int* p5 = Z.prev + 5 * Z.LNN;
+    for (int i = 1; i < Z.LAYER; ++i) {
+        const int cur = zidx(Z, i, x, y);
+        p5[cur] = cur;
+    }
+    for (int i = 2; i < Z.LAYER; ++i) {
+        const int cur = zidx(Z, i, x, y), last = zidx(Z, i - 1, x, y);
+        const int v = zadd(m[last], zvia(T, Z, last));
+        if (m[cur] > v) { m[cur] = v; p[cur] = p[last]; p5[cur] = last; }
+    }
+    for (int i = Z.LAYER - 2; i >= 1; --i) {
+        const int cur = zidx(Z, i, x, y), last = zidx(Z, i + 1, x, y);
+        const int v = zadd(m[last], zvia(T, Z, cur));
+        if (m[cur] > v) { m[cur] = v; p[cur] = p[last]; p5[cur] = last; }
+    }
+}
+
+// Child slot j (1..3) of node (tox, toy): fill plane j at the node from the
+// child at (fromx, fromy) (zshape.cuh:87-237).
+__device__ __forceinline__ void zedge(const Tables& T, const ZTrees& Z, int j, int fromx, int fromy, int tox, int toy,
+                                      int lane) {
+    const int LAYER = Z.LAYER, D = Z.D;
+    const long long NN = Z.NN;
+    int* map0 = Z.map;
+    int* m4 = Z.map + 4 * Z.LNN;
+    int* p4 = Z.prev + 4 * Z.LNN;
+    int* p5 = Z.prev + 5 * Z.LNN;
+    int* mj = Z.map + j * Z.LNN;
+    int* pj = Z.prev + j * Z.LNN;
+    int* p2j = Z.prev + (10 + j) * Z.LNN;
+    const int minx = min(fromx, tox), maxx = max(fromx, tox), miny = min(fromy, toy), maxy = max(fromy, toy);
+    if (fromx != tox && fromy != toy) {
+        // Clear the candidate rows and columns of the edge's box.
+        for (int a = minx + lane; a <= maxx; a += 32)
+            for (int i = 1; i < LAYER; ++i) {
+                if ((i & 1) ^ D) { m4[i * NN + a * Z.N + toy] = kZInf; m4[i * NN + a * Z.N + fromy] = kZInf; }
+                else { m4[i * NN + toy * Z.N + a] = kZInf; m4[i * NN + fromy * Z.N + a] = kZInf; }
+            }
+        for (int b = miny + lane; b <= maxy; b += 32)
+            for (int i = 1; i < LAYER; ++i) {
+                if ((i & 1) ^ D) { m4[i * NN + tox * Z.N + b] = kZInf; m4[i * NN + fromx * Z.N + b] = kZInf; }
+                else { m4[i * NN + b * Z.N + tox] = kZInf; m4[i * NN + b * Z.N + fromx] = kZInf; }
+            }
+        __syncwarp();
+        // Straight runs out of the child along each layer's direction.
+        for (int i = 1; i < LAYER; ++i) {
+            if ((i & 1) ^ D) {
+                const int last = static_cast<int>(i * NN + fromx * Z.N + fromy);
+                for (int b = miny + lane; b <= maxy; b += 32) {
+                    if (b == fromy) continue;
+                    const int cur = static_cast<int>(i * NN + fromx * Z.N + b);
+                    m4[cur] = zadd(map0[last], zwire(T, Z, last, cur));
+                    p4[cur] = last;
+                }
+            } else {
+                const int last = static_cast<int>(i * NN + fromy * Z.N + fromx);
+                for (int b = minx + lane; b <= maxx; b += 32) {
+                    if (b == fromx) continue;
+                    const int cur = static_cast<int>(i * NN + fromy * Z.N + b);
+                    m4[cur] = zadd(map0[last], zwire(T, Z, last, cur));
+                    p4[cur] = last;
+                }
+            }
+        }
+        __syncwarp();
+        // Layer changes on the child's column and row (distinct positions).
+        {
+            const int ncol = maxy - miny + 1;
+            for (int k = lane; k < ncol + (maxx - minx + 1); k += 32) {
+                if (k < ncol) { const int b = miny + k; if (b != fromy) zvia_sweep(T, Z, fromx, b); }
+                else { const int b = minx + (k - ncol); if (b != fromx) zvia_sweep(T, Z, b, fromy); }
+            }
+        }
+        __syncwarp();
+        // Cross the box to the node's row / column.
+        for (int i = 1; i < LAYER; ++i) {
+            if ((i & 1) ^ D) {
+                for (int b = minx + lane; b <= maxx; b += 32) {
+                    const int last = static_cast<int>(i * NN + b * Z.N + fromy), cur = static_cast<int>(i * NN + b * Z.N + toy);
+                    const int v = zadd(m4[last], zwire(T, Z, last, cur));
+                    if (v < m4[cur]) { m4[cur] = v; p4[cur] = p4[last]; }
+                }
+            } else {
+                for (int b = miny + lane; b <= maxy; b += 32) {
+                    const int last = static_cast<int>(i * NN + b * Z.N + fromx), cur = static_cast<int>(i * NN + b * Z.N + tox);
+                    const int v = zadd(m4[last], zwire(T, Z, last, cur));
+                    if (v < m4[cur]) { m4[cur] = v; p4[cur] = p4[last]; }
+                }
+            }
+        }
+        __syncwarp();
+        {
+            const int ncol = maxy - miny + 1;
+            for (int k = lane; k < ncol + (maxx - minx + 1); k += 32) {
+                if (k < ncol) { const int b = miny + k; if (b != toy) zvia_sweep(T, Z, tox, b); }
+                else { const int b = minx + (k - ncol); if (b != tox) zvia_sweep(T, Z, b, toy); }
+            }
+        }
+        __syncwarp();
+        // Last run into the node, one lane per layer, positions in order.
+        for (int i = 1 + lane; i < LAYER; i += 32) {
+            if ((i & 1) ^ D) {
+                const int cur = static_cast<int>(i * NN + tox * Z.N + toy);
+                for (int b = miny; b <= maxy; ++b) {
+                    if (b == toy) continue;
+                    const int last = static_cast<int>(i * NN + tox * Z.N + b);
+                    const int v = zadd(m4[last], zwire(T, Z, last, cur));
+                    if (v < mj[cur]) { mj[cur] = v; pj[cur] = p4[last]; p2j[cur] = p5[last]; }
+                }
+            } else {
+                const int cur = static_cast<int>(i * NN + toy * Z.N + tox);
+                for (int b = minx; b <= maxx; ++b) {
+                    if (b == tox) continue;
+                    const int last = static_cast<int>(i * NN + toy * Z.N + b);
+                    const int v = zadd(m4[last], zwire(T, Z, last, cur));
+                    if (v < mj[cur]) { mj[cur] = v; pj[cur] = p4[last]; p2j[cur] = p5[last]; }
+                }
+            }
+        }
+    } else if (fromx == tox) {
+        for (int i = 1 + lane; i < LAYER; i += 32) {
+            if ((i & 1) ^ D) {
+                const int last = static_cast<int>(i * NN + fromx * Z.N + fromy), cur = static_cast<int>(i * NN + tox * Z.N + toy);
+                const int v = zadd(map0[last], zwire(T, Z, last, cur));
+                if (mj[cur] > v) { mj[cur] = v; pj[cur] = last; }
+            } else {
+                mj[i * NN + toy * Z.N + tox] = kZInf;
+            }
+        }
+    } else {  // fromy == toy
+        for (int i = 1 + lane; i < LAYER; i += 32) {
+            if ((!(i & 1)) ^ D) {
+                const int last = static_cast<int>(i * NN + fromy * Z.N + fromx), cur = static_cast<int>(i * NN + toy * Z.N + tox);
+                const int v = zadd(map0[last], zwire(T, Z, last, cur));
+                if (mj[cur] > v) { mj[cur] = v; pj[cur] = last; }
+            } else {
+                mj[i * NN + tox * Z.N + toy] = kZInf;
+            }
+        }
+    }
+    __syncwarp();
+}
+
+// Layer-range DP of one node (zshape.cuh:241-267), lane 0.
+__device__ __forceinline__ void znode_dp(const Tables& T, const ZTrees& Z, int tox, int toy, int pin,
+                                         const int* ch) {
+    const int LAYER = Z.LAYER;
+    int* map0 = Z.map;
+    int* prev0 = Z.prev;
+    for (int lower = 0; lower < LAYER; ++lower) {
+        int viaSum = 0, minCost = kZInf, bestpos[3] = {0, 0, 0};
+        int costs[3] = {ch[0] == -1 ? 0 : kZInf, ch[1] == -1 ? 0 : kZInf, ch[2] == -1 ? 0 : kZInf};
+        for (int upper = lower; upper < LAYER; ++upper) {
+            const int idx = zidx(Z, upper, tox, toy);
+            for (int j = 0; j < 3; ++j) {
+                if (ch[j] == -1) continue;
+                const int v = Z.map[(j + 1) * Z.LNN + idx];
+                if (v < costs[j]) { costs[j] = v; bestpos[j] = upper; }
+            }
+            if (1LL * costs[0] + costs[1] + costs[2] < minCost) minCost = costs[0] + costs[1] + costs[2];
+            if (pin == -1 || (lower <= pin && pin <= upper)) {
+                const int v = zadd(minCost, viaSum);
+                const int code = (((lower * LAYER + upper) * LAYER + bestpos[2]) * LAYER + bestpos[1]) * LAYER + bestpos[0];
+                for (int i = lower; i <= upper; ++i) {
+                    const int index = zidx(Z, i, tox, toy);
+                    if (map0[index] > v) { map0[index] = v; prev0[index] = code; }
+                }
+            }
+            viaSum = zadd(viaSum, zvia(T, Z, idx));
+        }
+    }
+}
+
+// convert_routes (zshape_topology.hpp:249-290) of one (start, length | -1)
+// pair straight into route words; returns a reference status on failure.
+__device__ __forceinline__ int zemit(const Tables& T, const ZTrees& Z, int start, int len, int* r, int& out,
+                                     long long cap) {
+    const int n = Z.N;
+    const int layer = start / (n * n) - 1;
+    const int a = start / n % n, b = start % n;
+    const bool ay = ((layer & 1) ^ T.DIR) != 0;
+    const int x = ay ? a : b, y = ay ? b : a;
+    if (layer < 0 || layer >= T.L || x >= T.X || y >= T.Y) return 3;
+    const int pos0 = cell_index(T, layer, x, y);
+    int pos1;
+    if (len == -1) {
+        if (layer + 1 >= T.L) return 3;
+        pos1 = pos0 + T.XY;
+    } else {
+        const int end = start + len, ea = end / n % n, eb = end % n;
+        const int ex = ay ? ea : eb, ey = ay ? eb : ea;
+        if (ex >= T.X || ey >= T.Y) return 3;
+        pos1 = cell_index(T, layer, ex, ey);
+    }
+    if (out + 1 < cap) { r[out++] = pos0; r[out++] = pos1; return 0; }
+    return 1;
+}
+
+// Traceback (zshape.cuh:271-386) of one net on lane 0, converted into the
+// net's route record.  Returns 0 or the reference's status (1 storage, 2 no
+// finite route, 3 segment outside the grid).
+__device__ __forceinline__ int ztrace(const Tables& T, const ZTrees& Z, int nb, int cnt, int* r, long long cap) {
+    const int LAYER = Z.LAYER, N = Z.N, D = Z.D;
+    int* map0 = Z.map;
+    int* m5 = Z.map + 5 * Z.LNN;
+    int out = 1, status = 0;
+    auto emit = [&](int a, int b) { const int s = zemit(T, Z, a, b, r, out, cap); if (s) status = s; };
+    int minTotal = kZInf;
+    const int p0 = Z.pos[nb];
+    for (int i = 0; i < LAYER; ++i) {
+        const int idx = zidx(Z, i, p0 / N, p0 % N);
+        if (map0[idx] < minTotal) { minTotal = map0[idx]; m5[p0] = i; }
+    }
+    if (minTotal == kZInf || minTotal < 0) { r[0] = 1; return 2; }
+    for (int t = 0; t < cnt; ++t) {
+        const int pt = Z.pos[nb + t], x = pt / N, y = pt % N, layer = m5[pt];
+        const int idx = zidx(Z, layer, x, y);
+        const int code = Z.prev[idx];
+        const int minl = code / LAYER / LAYER / LAYER / LAYER, maxl = code / LAYER / LAYER / LAYER % LAYER;
+        for (int i = minl; i < maxl; ++i) emit(zidx(Z, i, x, y), -1);
+        int bestpos = code;
+        for (int j = 0; j < 3; ++j) {
+            const int c = Z.child[3 * (nb + t) + j];
+            if (c == -1) break;
+            const int child = Z.pos[nb + c];
+            const int entrylayer = bestpos % LAYER, entry = zidx(Z, entrylayer, x, y);
+            bestpos /= LAYER;
+            const int last = Z.prev[(j + 1) * Z.LNN + entry];
+            const int lastlayer = static_cast<int>(last / Z.NN);
+            int lastx = last / N % N, lasty = last % N;
+            if ((!(lastlayer & 1)) ^ D) { const int s = lastx; lastx = lasty; lasty = s; }
+            if (lastx != x && lasty != y) {
+                const int mid = Z.prev[(11 + j) * Z.LNN + entry];
+                const int midlayer = static_cast<int>(mid / Z.NN);
+                int midx = mid / N % N, midy = mid % N;
+                if ((!(midlayer & 1)) ^ D) { const int s = midx; midx = midy; midy = s; }
+                const int q1 = ((entrylayer & 1) ^ D) ? entry - y + midy : entry - x + midx;
+                const int q3 = ((midlayer & 1) ^ D) ? mid - midy + lasty : mid - midx + lastx;
+                const int q4 = ((lastlayer & 1) ^ D) ? last - lasty + midy : last - lastx + midx;
+                if (entry != q1) emit(min(entry, q1), max(entry, q1) - min(entry, q1));
+                if (q1 != mid)
+                    for (int i = min(entrylayer, midlayer); i < max(entrylayer, midlayer); ++i) emit(zidx(Z, i, midx, midy), -1);
+                if (mid != q3) emit(min(mid, q3), max(mid, q3) - min(mid, q3));
+                if (q3 != q4) {
+                    int tx = q3 / N % N, ty = q3 % N;
+                    if ((!(static_cast<int>(q3 / Z.NN) & 1)) ^ D) { const int s = tx; tx = ty; ty = s; }
+                    for (int i = min(midlayer, lastlayer); i < max(midlayer, lastlayer); ++i) emit(zidx(Z, i, tx, ty), -1);
+                }
+                if (q4 != last) emit(min(q4, last), max(q4, last) - min(q4, last));
+            } else {
+                emit(min(last, entry), max(last, entry) - min(last, entry));
+            }
+            m5[child] = lastlayer;
+        }
+    }
+    r[0] = out;
+    return status;
+}
+
+// Route net `id` with one warp; with `commit`, also its wire demand.
+__device__ __forceinline__ void zshape_net(const Tables& T, const ZTrees& Z, const Plan& P, int id, int stamp,
+                                           int lane, bool commit) {
+    const int nb = Z.node_off[id], cnt = Z.node_off[id + 1] - nb;
+    int* r = P.routes + P.route_off[id];
+    const long long cap = P.route_off[id + 1] - P.route_off[id];
+    if (cnt <= 0) {
+        if (lane == 0 && cap > 0) r[0] = 1;
+        return;
+    }
+    // reset_nodes (zshape.cuh:392-404).
+    for (int k = lane; k < cnt * Z.LAYER; k += 32) {
+        const int pt = Z.pos[nb + k / Z.LAYER];
+        const int idx = zidx(Z, k % Z.LAYER, pt / Z.N, pt % Z.N);
+        for (int plane = 0; plane < 4; ++plane) Z.map[plane * Z.LNN + idx] = kZInf;
+    }
+    __syncwarp();
+    for (int t = cnt - 1; t >= 0; --t) {
+        const int pt = Z.pos[nb + t], tox = pt / Z.N, toy = pt % Z.N;
+        const int* ch = Z.child + 3 * (nb + t);
+        for (int j = 1; j <= 3; ++j) {
+            const int c = ch[j - 1];
+            if (c == -1) continue;
+            const int cp = Z.pos[nb + c];
+            zedge(T, Z, j, cp / Z.N, cp % Z.N, tox, toy, lane);
+        }
+        if (lane == 0) znode_dp(T, Z, tox, toy, Z.pin[nb + t], ch);
+        __syncwarp();
+    }
+    int status = 0;
+    if (lane == 0) {
+        status = ztrace(T, Z, nb, cnt, r, cap);
+        if (status) set_error(T, status == 1 ? kELimit : kEInval, id);
+    }
+    status = __shfl_sync(0xffffffffu, status, 0);
+    __syncwarp();
+    if (commit && !status) commit_net_wires(T, P, id, stamp, 1, lane);
+}
+
+// --- bounding-box batch refinement (zshape_topology.hpp:7-57) --------------
+// Within one first-fit group, nets sorted by box area (descending, larger id
+// first on ties) form greedy rounds of at most `max_batch` nets with pairwise
+// disjoint boxes; this is first-fit colouring with box-intersection conflicts.
+__device__ __forceinline__ bool boxes_meet(int4 a, int4 b) {
+    // int4 = (minx, maxx, miny, maxy)
+    return !(a.y < b.x || b.y < a.x || a.w < b.z || b.w < a.z);
+}
+
+}  // namespace grb

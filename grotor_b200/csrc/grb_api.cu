@@ -17,6 +17,7 @@
 #include "device/cost.cuh"
 #include "device/flt.cuh"
 #include "device/lshape.cuh"
+#include "device/zshape.cuh"
 
 using namespace grb;
 
@@ -230,6 +231,190 @@ __global__ void __launch_bounds__(kPersistentThreads, 2) k_flt_persistent(Tables
         for (int k = gwarp; k < cnt; k += nwarps) commit_net_vias(T, P2, P2.ids[lo + k], stamp, 1, lane);
         if (!grid_sync(S, T)) return;
         clk.mark(S, 6);
+    }
+}
+
+// --- Z-shape stage kernels (zshape.cuh) -------------------------------------
+constexpr int kZThreads = 128;
+constexpr int kBoxThreads = 256;
+constexpr int kMaxBoxBatch = 256;
+
+// One warp per net of batch b (solve<4>, zshape.cuh:62-388, with the route
+// conversion of convert_routes fused into the traceback).
+__global__ void __launch_bounds__(kZThreads) k_zshape_batch(Tables T, ZTrees Z, Plan P, int b) {
+    const int lane = threadIdx.x & 31;
+    const int k = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lo = P.batch_off[b], cnt = P.batch_off[b + 1] - lo;
+    if (k < cnt) zshape_net(T, Z, P, P.ids[lo + k], 0, lane, false);
+}
+// Thread-per-net commit (commit_wire_demand / commit_via_demand,
+// demand.cuh:129-232), the Z-shape pipeline's form (pipeline_ggr.hpp:132-133).
+__global__ void k_commit_thread_wires(Tables T, Plan P, int b, int stamp) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int lo = P.batch_off[b], cnt = P.batch_off[b + 1] - lo;
+    if (i < cnt) commit_thread_wires(T, P, P.ids[lo + i], stamp, 1);
+}
+__global__ void k_commit_thread_vias(Tables T, Plan P, int b, int stamp) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int lo = P.batch_off[b], cnt = P.batch_off[b + 1] - lo;
+    if (i < cnt) commit_thread_vias(T, P, P.ids[lo + i], stamp, 1);
+}
+
+// Persistent Z-shape stage: per batch, refresh cells -> prefix pass 1 ->
+// trees -> pass 2 -> Z-shape nets and their wires -> vias.
+__global__ void __launch_bounds__(kPersistentThreads, 2) k_zshape_persistent(Tables T, ZTrees Z, Plan P, GridSync S,
+                                                                              int stamp0, int* work) {
+    extern __shared__ __align__(16) char smem[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int gwarp = warp * gridDim.x + blockIdx.x, nwarps = gridDim.x * (blockDim.x >> 5);
+    double* tree = reinterpret_cast<double*>(smem);
+    PhaseClock clk;
+    clk.start(S);
+    for (int b = 0; b < P.n_batches; ++b) {
+        const int lo = P.batch_off[b], cnt = P.batch_off[b + 1] - lo;
+        const int stamp = stamp0 + b + 1;
+        if (blockIdx.x == 0) collect_dirty_groups(T);
+        refresh_dirty_cells(T, gwarp, nwarps, lane);
+        if (!grid_sync(S, T)) return;
+        clk.mark(S, 4);
+        const int items = *reinterpret_cast<volatile int*>(T.group_count) * T.tree_chunks;
+        for (int item = gwarp; item < items; item += nwarps) {
+            int g, c;
+            if (prefix_item(T, item, g, c)) prefix_pass1(T, g, c, lane);
+        }
+        if (!grid_sync(S, T)) return;
+        for (int k = blockIdx.x; k < *reinterpret_cast<volatile int*>(T.group_count); k += gridDim.x)
+            prefix_tree(T, T.group_list[k], tree);
+        if (!grid_sync(S, T)) return;
+        for (int item = gwarp; item < items; item += nwarps) {
+            int g, c;
+            if (prefix_item(T, item, g, c)) prefix_pass2(T, g, c, lane);
+        }
+        if (!grid_sync(S, T)) return;
+        clk.mark(S, 7);
+        while (true) {
+            int k = 0;
+            if (lane == 0) k = atomicAdd(work + b, 1);
+            k = __shfl_sync(0xffffffffu, k, 0);
+            if (k >= cnt) break;
+            zshape_net(T, Z, P, P.ids[lo + k], stamp, lane, true);
+        }
+        if (!grid_sync(S, T)) return;
+        clk.mark(S, 5);
+        for (int k = gwarp; k < cnt; k += nwarps) commit_net_vias(T, P, P.ids[lo + k], stamp, 1, lane);
+        if (!grid_sync(S, T)) return;
+        clk.mark(S, 6);
+    }
+}
+
+// Bounding-box refinement of every group (current plan batch) at once, one
+// CTA per group: keys (area, id) merge-sorted descending by the CTA, then
+// warp 0 forms the greedy rounds (zshape_topology.hpp:7-57) with the round's
+// boxes in shared memory, 32 pending nets fetched per memory round trip.
+// Writes the rounds in order into tmp (the group's own id range), their sizes
+// into bsize and their number into rounds[g].
+__global__ void __launch_bounds__(kBoxThreads) k_bbox_refine(const int* ids, const int* batch_off, const int4* box,
+        unsigned long long* ka, unsigned long long* kb, int* pend, int* tmp, int* bsize, int* rounds, int max_batch) {
+    __shared__ int4 rect[kMaxBoxBatch];
+    const int g = blockIdx.x, tid = threadIdx.x;
+    const int lo = batch_off[g], n = batch_off[g + 1] - lo;
+    for (int k = tid; k < n; k += blockDim.x) {
+        const int id = ids[lo + k];
+        const int4 bb = box[id];
+        const unsigned long long area = static_cast<unsigned long long>(bb.y - bb.x + 1) * (bb.w - bb.z + 1);
+        ka[lo + k] = (area << 32) | static_cast<unsigned>(id);
+    }
+    __syncthreads();
+    unsigned long long* src = ka + lo;
+    unsigned long long* dst = kb + lo;
+    for (int w = 1; w < n; w <<= 1) {
+        for (int k = tid; k < n; k += blockDim.x) {
+            const int start = (k / (2 * w)) * (2 * w), mid = min(start + w, n), end = min(start + 2 * w, n);
+            const unsigned long long key = src[k];
+            int a = k < mid ? mid : start, e = k < mid ? end : mid;
+            const int base = k < mid ? k - start : k - mid;
+            const int first = a;
+            while (a < e) {  // elements of the other run that sort before `key` (keys are distinct)
+                const int m = (a + e) >> 1;
+                if (src[m] > key) a = m + 1;
+                else e = m;
+            }
+            dst[start + base + (a - first)] = key;
+        }
+        __syncthreads();
+        unsigned long long* t = src; src = dst; dst = t;
+    }
+    for (int k = tid; k < n; k += blockDim.x) pend[lo + k] = static_cast<int>(src[k] & 0xffffffffu);
+    __syncthreads();
+    if (tid >= 32) return;
+    const int lane = tid;
+    int remaining = n, r = 0, out = 0;
+    while (remaining > 0) {
+        int count = 0;
+        bool full = false;
+        for (int base = 0; base < remaining && !full; base += 32) {
+            const int myid = base + lane < remaining ? pend[lo + base + lane] : -1;
+            const int4 mb = myid >= 0 ? box[myid] : make_int4(0, -1, 0, -1);
+            const int lim = min(32, remaining - base);
+            for (int q = 0; q < lim; ++q) {
+                const int id = __shfl_sync(0xffffffffu, myid, q);
+                int4 bb;
+                bb.x = __shfl_sync(0xffffffffu, mb.x, q);
+                bb.y = __shfl_sync(0xffffffffu, mb.y, q);
+                bb.z = __shfl_sync(0xffffffffu, mb.z, q);
+                bb.w = __shfl_sync(0xffffffffu, mb.w, q);
+                bool hit = false;
+                for (int m = lane; m < count; m += 32) hit |= boxes_meet(rect[m], bb);
+                if (__any_sync(0xffffffffu, hit)) continue;
+                if (lane == 0) {
+                    rect[count] = bb;
+                    tmp[lo + out] = id;
+                    pend[lo + base + q] = -1;
+                }
+                __syncwarp();
+                ++count;
+                ++out;
+                if (count == max_batch) { full = true; break; }
+            }
+        }
+        if (lane == 0) bsize[lo + r] = count;
+        ++r;
+        __syncwarp();
+        // Stable in-place compaction of the nets still pending.
+        int kept = 0;
+        for (int base = 0; base < remaining; base += 32) {
+            const int v = base + lane < remaining ? pend[lo + base + lane] : -1;
+            const unsigned keep = __ballot_sync(0xffffffffu, v >= 0);
+            __syncwarp();
+            if (v >= 0) pend[lo + kept + __popc(keep & ((1u << lane) - 1u))] = v;
+            kept += __popc(keep);
+            __syncwarp();
+        }
+        remaining = kept;
+    }
+    if (lane == 0) rounds[g] = r;
+}
+
+// Lay the rounds of group g out in reverse order (the stage runs the refined
+// batch list reversed, pipeline_ggr.hpp:55): ids and new batch offsets.
+__global__ void k_bbox_scatter(const int* batch_off, const int* tmp, const int* bsize, const int* rounds,
+                               const int* first_batch, int* bofs, int* ids_out, int* off_out) {
+    const int g = blockIdx.x, tid = threadIdx.x;
+    const int lo = batch_off[g], n = batch_off[g + 1] - lo, R = rounds[g], B = first_batch[g];
+    if (tid == 0) {
+        int o = 0;
+        for (int r = 0; r < R; ++r) {
+            bofs[lo + r] = o;
+            off_out[B + (R - 1 - r)] = lo + n - o - bsize[lo + r];
+            o += bsize[lo + r];
+        }
+    }
+    __syncthreads();
+    const int warp = tid >> 5, lane = tid & 31, nw = blockDim.x >> 5;
+    for (int r = warp; r < R; r += nw) {
+        const int o = bofs[lo + r], sz = bsize[lo + r];
+        const int dst = lo + n - o - sz;
+        for (int k = lane; k < sz; k += 32) ids_out[dst + k] = tmp[lo + o + k];
     }
 }
 
@@ -448,6 +633,16 @@ struct grb_ctx {
     cudaGraphExec_t flt_graph = nullptr;
     long long flt_graph_key[4] = {-1, -1, -1, -1};
     int64_t flt_graph_kernels = 0;
+    // Z-shape stage (grb_upload_zshape)
+    std::vector<void*> z_bufs;
+    ZTrees Z{};
+    int4* z_box = nullptr;            // per net (minx, maxx, miny, maxy)
+    int z_n = -1;
+    std::vector<int> h_z_node_off;
+    int z_version = 0;
+    cudaGraphExec_t z_graph = nullptr;
+    long long z_graph_key[3] = {-1, -1, -1};
+    int64_t z_graph_kernels = 0;
     // graph cache
     cudaGraphExec_t graph = nullptr;
     int graph_version = -1, graph_stamp = -1;
@@ -645,6 +840,78 @@ int stage_plain(grb_ctx* c, int stamp0) {
         if (!rc) rc = commit_plain(c, b, stamp, 1);
         if (rc) return rc;
     }
+    return GRB_OK;
+}
+
+// --- Z-shape stage executors (pipeline_ggr.hpp:119-134) ---------------------
+int z_stage_plain(grb_ctx* c, int stamp0) {
+    const Plan P = make_plan(c);
+    for (int b = 0; b < c->n_batches; ++b) {
+        const int cnt = c->h_batch_off[b + 1] - c->h_batch_off[b];
+        if (cnt <= 0) continue;
+        const int stamp = stamp0 + b + 1;
+        int rc;
+        if ((rc = refresh_plain(c))) return rc;
+        cudaEvent_t e;
+        if ((rc = prof_begin(c, 5, &e))) return rc;
+        k_zshape_batch<<<(cnt + kZThreads / 32 - 1) / (kZThreads / 32), kZThreads, 0, c->stream>>>(c->T, c->Z, P, b);
+        prof_end(c, e);
+        if ((rc = prof_begin(c, 6, &e))) return rc;
+        k_commit_thread_wires<<<(cnt + 255) / 256, 256, 0, c->stream>>>(c->T, P, b, stamp);
+        k_commit_thread_vias<<<(cnt + 255) / 256, 256, 0, c->stream>>>(c->T, P, b, stamp);
+        prof_end(c, e);
+        c->launches += 3;
+        GRB_CUDA(c, cudaGetLastError());
+    }
+    return GRB_OK;
+}
+
+int z_stage_graph(grb_ctx* c, int stamp0) {
+    const long long key[3] = {c->plan_version, c->z_version, stamp0};
+    if (!c->z_graph || !std::equal(key, key + 3, c->z_graph_key)) {
+        if (c->z_graph) { cudaGraphExecDestroy(c->z_graph); c->z_graph = nullptr; }
+        const int64_t before = c->launches;
+        const bool prof = c->profiling;
+        c->profiling = false;
+        cudaGraph_t g = nullptr;
+        GRB_CUDA(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+        const int rc = z_stage_plain(c, stamp0);
+        const cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+        c->profiling = prof;
+        if (rc) { if (g) cudaGraphDestroy(g); return rc; }
+        if (e != cudaSuccess) return cuda_fail(c, e, "cudaStreamEndCapture");
+        const cudaError_t ei = cudaGraphInstantiate(&c->z_graph, g, 0);
+        cudaGraphDestroy(g);
+        if (ei != cudaSuccess) return cuda_fail(c, ei, "cudaGraphInstantiate");
+        c->z_graph_kernels = c->launches - before;
+        c->launches = before;
+        std::copy(key, key + 3, c->z_graph_key);
+    }
+    GRB_CUDA(c, cudaGraphLaunch(c->z_graph, c->stream));
+    c->launches += c->z_graph_kernels;
+    return GRB_OK;
+}
+
+int ensure_work(grb_ctx* c);
+
+int z_stage_persistent(grb_ctx* c, int stamp0) {
+    if (c->n_batches == 0) return GRB_OK;
+    const size_t smem = prefix_smem_bytes(std::max(c->T.X, c->T.Y));
+    GRB_CUDA(c, cudaFuncSetAttribute(k_zshape_persistent, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+    int per_sm = 0;
+    GRB_CUDA(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_zshape_persistent, kPersistentThreads, smem));
+    if (per_sm < 1) return fail(c, GRB_EINVAL, "persistent Z-shape kernel does not fit on an SM");
+    int rc = ensure_work(c);
+    if (rc) return rc;
+    GRB_CUDA(c, cudaMemsetAsync(c->sync, 0, 2 * sizeof(unsigned), c->stream));
+    Tables T = c->T;
+    ZTrees Z = c->Z;
+    Plan P = make_plan(c);
+    GridSync S{c->sync, c->sync + 1, kBarrierTimeoutNs, c->profiling ? c->d_phase : nullptr};
+    void* args[] = {&T, &Z, &P, &S, &stamp0, &c->work};
+    GRB_CUDA(c, cudaLaunchCooperativeKernel((void*)k_zshape_persistent, dim3(per_sm * c->sms), dim3(kPersistentThreads),
+                                            args, smem, c->stream));
+    c->launches += 1;
     return GRB_OK;
 }
 
@@ -909,6 +1176,8 @@ void grb_destroy(grb_ctx* c) {
     if (c->stream) cudaStreamSynchronize(c->stream);
     if (c->graph) cudaGraphExecDestroy(c->graph);
     if (c->flt_graph) cudaGraphExecDestroy(c->flt_graph);
+    if (c->z_graph) cudaGraphExecDestroy(c->z_graph);
+    free_all(c->z_bufs);
     free_all(c->net_bufs);
     free_all(c->geom_bufs);
     free_all(c->flt_bufs);
@@ -1025,8 +1294,165 @@ int grb_upload_nets(grb_ctx* c, const grb_nets* nets) {
     c->n_nets = n;
     c->max_nodes = int(maxn);
     c->route_words = rw;
-    c->flt_n = -1;  // FLT DAGs refer to the previous nets
+    c->flt_n = -1;  // FLT DAGs and Z-shape trees refer to the previous nets
+    c->z_n = -1;
     return GRB_OK;
+}
+
+int grb_set_wire_cost_mode(grb_ctx* c, int32_t integer_wire) {
+    if (!c) return GRB_EINVAL;
+    GRB_CUDA(c, cudaSetDevice(c->device));
+    c->T.int_wire = integer_wire ? 1 : 0;
+    // Every wire cost changes: the next refresh recomputes all cells and tracks.
+    const int n = std::max(c->words, c->T.n_groups);
+    k_mark_all_dirty<<<(n + 255) / 256, 256, 0, c->stream>>>(c->T);
+    c->launches += 1;
+    GRB_CUDA(c, cudaGetLastError());
+    GRB_CUDA(c, cudaStreamSynchronize(c->stream));
+    return GRB_OK;
+}
+
+int grb_upload_zshape(grb_ctx* c, const grb_zshape_trees* t) {
+    if (!c) return GRB_EINVAL;
+    if (!c->node_off) return fail(c, GRB_EINVAL, "no nets uploaded");
+    if (!t || !t->node_off) return fail(c, GRB_EINVAL, "Z-shape tree offsets missing");
+    GRB_CUDA(c, cudaSetDevice(c->device));
+    const Tables& T = c->T;
+    const int n = c->n_nets, XY = T.XY;
+    const int N = std::max(T.X, T.Y), LAYER = T.L + 1;
+    const long long NN = (long long)N * N, LNN = LAYER * NN;
+    if (16 * LNN >= (1ll << 31)) return fail(c, GRB_EINVAL, "Z-shape planes exceed 32-bit indexing");
+    if (t->node_off[0] != 0) return fail(c, GRB_EINVAL, "Z-shape offsets must start at 0");
+    for (int i = 0; i < n; ++i) if (t->node_off[i + 1] < t->node_off[i]) return fail(c, GRB_EINVAL, "Z-shape offsets must be non-decreasing");
+    const long long nn = t->node_off[n];
+    if (nn && (!t->coord || !t->child)) return fail(c, GRB_EINVAL, "Z-shape tree arrays missing");
+    std::vector<int> pos(nn), pin(nn);
+    std::vector<int4> box(std::max(n, 1));
+    for (int id = 0; id < n; ++id) {
+        const int nb = t->node_off[id], cnt = t->node_off[id + 1] - nb;
+        int4 bb = make_int4(T.X, 0, T.Y, 0);
+        for (int i = 0; i < cnt; ++i) {
+            const int cd = t->coord[nb + i];
+            if (cd < 0 || cd / XY > T.L) return fail(c, GRB_EINVAL, "Z-shape node outside the grid");
+            const int l = cd / XY, x = cd % XY / T.Y, y = cd % T.Y;
+            pos[nb + i] = x * N + y;                 // zshape_topology.hpp:105
+            pin[nb + i] = l < T.L ? l + 1 : -1;      // :106-109
+            bb.x = std::min(bb.x, x); bb.y = std::max(bb.y, x);
+            bb.z = std::min(bb.z, y); bb.w = std::max(bb.w, y);
+            for (int j = 0; j < 3; ++j) {
+                const int ch = t->child[3 * (size_t(nb) + i) + j];
+                if (ch != -1 && (ch <= i || ch >= cnt)) return fail(c, GRB_EINVAL, "Z-shape children must follow their parent in preorder");
+            }
+        }
+        if (!cnt) bb = make_int4(0, 0, 0, 0);
+        box[id] = bb;
+    }
+    GRB_CUDA(c, cudaStreamSynchronize(c->stream));
+    const bool planes = c->Z.map != nullptr && c->Z.LNN == LNN;
+    std::vector<void*> keep;
+    if (planes) {  // keep the (large) planes, replace the per-node arrays
+        for (void* p : c->z_bufs)
+            if (p == c->Z.map || p == c->Z.prev) keep.push_back(p);
+            else cudaFree(p);
+        c->z_bufs = keep;
+    } else {
+        free_all(c->z_bufs);
+    }
+    ZTrees Z = c->Z;
+    int *noff, *dpos, *dpin, *dch;
+    int4* dbox;
+    int rc = 0;
+    rc |= dalloc(c, &noff, n + 1, c->z_bufs);
+    rc |= dalloc(c, &dpos, nn, c->z_bufs);
+    rc |= dalloc(c, &dpin, nn, c->z_bufs);
+    rc |= dalloc(c, &dch, 3 * nn, c->z_bufs);
+    rc |= dalloc(c, &dbox, std::max(n, 1), c->z_bufs);
+    if (!planes) {
+        rc |= dalloc(c, &Z.map, size_t(6) * LNN, c->z_bufs);
+        rc |= dalloc(c, &Z.prev, size_t(16) * LNN, c->z_bufs);
+    }
+    if (rc) { free_all(c->z_bufs); c->Z = ZTrees{}; c->z_n = -1; return GRB_ENOMEM; }
+    auto h2d = [&](void* dst, const void* src, size_t bytes) {
+        return bytes ? cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, c->stream) : cudaSuccess;
+    };
+    GRB_CUDA(c, h2d(noff, t->node_off, 4 * size_t(n + 1)));
+    GRB_CUDA(c, h2d(dpos, pos.data(), 4 * size_t(nn)));
+    GRB_CUDA(c, h2d(dpin, pin.data(), 4 * size_t(nn)));
+    GRB_CUDA(c, h2d(dch, t->child, 12 * size_t(nn)));
+    GRB_CUDA(c, h2d(dbox, box.data(), sizeof(int4) * box.size()));
+    if (!planes) {
+        GRB_CUDA(c, cudaMemsetAsync(Z.map, 0, sizeof(int) * 6 * LNN, c->stream));
+        GRB_CUDA(c, cudaMemsetAsync(Z.prev, 0, sizeof(int) * 16 * LNN, c->stream));
+    }
+    GRB_CUDA(c, cudaStreamSynchronize(c->stream));
+    Z.node_off = noff; Z.pos = dpos; Z.pin = dpin; Z.child = dch;
+    Z.N = N; Z.LAYER = LAYER; Z.D = T.DIR ^ 1; Z.NN = NN; Z.LNN = LNN;
+    c->Z = Z;
+    c->z_box = dbox;
+    c->z_n = n;
+    c->h_z_node_off.assign(t->node_off, t->node_off + n + 1);
+    ++c->z_version;
+    return GRB_OK;
+}
+
+int grb_plan_bbox_batches(grb_ctx* c, const int32_t* bbox, int32_t max_batch, int32_t* n_batches) {
+    if (!c) return GRB_EINVAL;
+    if (max_batch < 1 || max_batch > kMaxBoxBatch) return fail(c, GRB_EINVAL, "max_batch must be in [1, 256]");
+    if (!bbox && c->z_n != c->n_nets) return fail(c, GRB_EINVAL, "no boxes given and no Z-shape trees uploaded");
+    GRB_CUDA(c, cudaSetDevice(c->device));
+    const int n = c->plan_n, G = c->n_batches;
+    if (n == 0) { if (n_batches) *n_batches = 0; return GRB_OK; }
+    std::vector<void*> tmpb;
+    int4* box = c->z_box;
+    if (bbox) {
+        for (int i = 0; i < c->n_nets; ++i) {
+            const int* b = bbox + 4 * size_t(i);
+            if (b[0] < 0 || b[0] > b[1] || b[1] >= c->T.X || b[2] < 0 || b[2] > b[3] || b[3] >= c->T.Y)
+                return fail(c, GRB_EINVAL, "net box outside the grid");
+        }
+        if (dalloc(c, &box, c->n_nets, tmpb)) return GRB_ENOMEM;
+        GRB_CUDA(c, cudaMemcpyAsync(box, bbox, sizeof(int4) * c->n_nets, cudaMemcpyHostToDevice, c->stream));
+    }
+    unsigned long long *ka, *kb;
+    int *pend, *tmp, *bsize, *bofs, *rounds, *first, *off_new;
+    int rc = 0;
+    rc |= dalloc(c, &ka, n, tmpb); rc |= dalloc(c, &kb, n, tmpb);
+    rc |= dalloc(c, &pend, n, tmpb); rc |= dalloc(c, &tmp, n, tmpb);
+    rc |= dalloc(c, &bsize, n, tmpb); rc |= dalloc(c, &bofs, n, tmpb);
+    rc |= dalloc(c, &rounds, G, tmpb); rc |= dalloc(c, &first, G, tmpb);
+    rc |= dalloc(c, &off_new, n + 1, tmpb);
+    if (rc) { free_all(tmpb); return GRB_ENOMEM; }
+    auto run = [&]() -> int {
+        k_bbox_refine<<<G, kBoxThreads, 0, c->stream>>>(c->ids, c->batch_off, box, ka, kb, pend, tmp, bsize, rounds,
+                                                        max_batch);
+        c->launches += 1;
+        GRB_CUDA(c, cudaGetLastError());
+        std::vector<int> hr(G), hf(G);
+        GRB_CUDA(c, cudaMemcpyAsync(hr.data(), rounds, 4 * size_t(G), cudaMemcpyDeviceToHost, c->stream));
+        GRB_CUDA(c, cudaStreamSynchronize(c->stream));
+        int total = 0;
+        for (int g = 0; g < G; ++g) { hf[g] = total; total += hr[g]; }
+        GRB_CUDA(c, cudaMemcpyAsync(first, hf.data(), 4 * size_t(G), cudaMemcpyHostToDevice, c->stream));
+        k_bbox_scatter<<<G, kBoxThreads, 0, c->stream>>>(c->batch_off, tmp, bsize, rounds, first, bofs, c->ids, off_new);
+        c->launches += 1;
+        GRB_CUDA(c, cudaGetLastError());
+        std::vector<int> h(total + 1);
+        GRB_CUDA(c, cudaMemcpyAsync(h.data(), off_new, 4 * size_t(total), cudaMemcpyDeviceToHost, c->stream));
+        GRB_CUDA(c, cudaStreamSynchronize(c->stream));
+        h[total] = n;
+        if (total > c->plan_cap) return fail(c, GRB_EINVAL, "more batches than plan capacity");
+        GRB_CUDA(c, cudaMemcpyAsync(c->batch_off, h.data(), 4 * size_t(total + 1), cudaMemcpyHostToDevice, c->stream));
+        GRB_CUDA(c, cudaStreamSynchronize(c->stream));
+        c->h_batch_off = h;
+        c->n_batches = total;
+        ++c->plan_version;
+        if (n_batches) *n_batches = total;
+        return GRB_OK;
+    };
+    const int r = run();
+    cudaStreamSynchronize(c->stream);
+    free_all(tmpb);
+    return r;
 }
 
 int grb_upload_geometry(grb_ctx* c, const int32_t* point_off, const int32_t* points, const int32_t* hseg_off,
@@ -1401,6 +1827,29 @@ int grb_flt_stage(grb_ctx* c, int32_t remove_phase_one, int32_t mode, grb_stats*
     if (rc) return rc;
     GRB_CUDA(c, cudaEventRecord(c->ev1, c->stream));
     c->stamp = stamp0 + flt_stamps(c, remove);
+    rc = check_device_error(c);
+    if (rc) return rc;
+    float ms = 0;
+    GRB_CUDA(c, cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+    c->dag_ms = ms;
+    if ((rc = prof_collect(c))) return rc;
+    return stats ? grb_get_stats(c, stats) : GRB_OK;
+}
+
+int grb_zshape_stage(grb_ctx* c, int32_t mode, grb_stats* stats) {
+    if (!c) return GRB_EINVAL;
+    if (c->z_n != c->n_nets || c->z_n < 0) return fail(c, GRB_EINVAL, "no Z-shape trees uploaded for the current nets");
+    GRB_CUDA(c, cudaSetDevice(c->device));
+    const int stamp0 = c->stamp;
+    GRB_CUDA(c, cudaEventRecord(c->ev0, c->stream));
+    int rc;
+    if (mode == GRB_MODE_PLAIN) rc = z_stage_plain(c, stamp0);
+    else if (mode == GRB_MODE_GRAPH) rc = z_stage_graph(c, stamp0);
+    else if (mode == GRB_MODE_PERSISTENT) rc = z_stage_persistent(c, stamp0);
+    else return fail(c, GRB_EINVAL, "unknown mode");
+    if (rc) return rc;
+    GRB_CUDA(c, cudaEventRecord(c->ev1, c->stream));
+    c->stamp = stamp0 + c->n_batches;
     rc = check_device_error(c);
     if (rc) return rc;
     float ms = 0;

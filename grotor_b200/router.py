@@ -215,6 +215,30 @@ class Router:
         self._check(self._lib.grb_read_routes2(self._ctx, _p(out)))
         return out
 
+    # ---- Z-shape stage (GGR pipeline) ----------------------------------------
+    def set_wire_cost_mode(self, integer_wire: bool):
+        """True selects the GGR build's integer wire costs (clamped, truncated)."""
+        self._check(self._lib.grb_set_wire_cost_mode(self._ctx, int(bool(integer_wire))))
+
+    def upload_zshape(self, trees: dict):
+        """Upload Z-shape trees (CSR by net id: node_off, coord, child[3 per node])."""
+        keep = {k: _c(trees[k], np.int32) for k in ("node_off", "coord", "child")}
+        t = _abi.GrbZshapeTrees(**{k: v.ctypes.data for k, v in keep.items()})
+        self._check(self._lib.grb_upload_zshape(self._ctx, C.byref(t)))
+
+    def plan_bbox_batches(self, max_batch: int = 250, bbox=None) -> int:
+        """zshape::generate_bbox_batches over every batch of the current plan."""
+        nb = C.c_int32(0)
+        b = None if bbox is None else _c(bbox, np.int32)
+        self._check(self._lib.grb_plan_bbox_batches(self._ctx, _p(b) if b is not None else None, int(max_batch),
+                                                    C.byref(nb)))
+        return nb.value
+
+    def zshape_route(self, mode="persistent") -> dict:
+        st = _abi.GrbStats()
+        self._check(self._lib.grb_zshape_stage(self._ctx, mode_id(mode), C.byref(st)))
+        return _stats_dict(st)
+
     def ripup(self, threshold: int = 0) -> np.ndarray:
         out = np.zeros(self.nets.n if self.nets else 0, np.uint8)
         self._check(self._lib.grb_ripup_classify(self._ctx, int(threshold), _p(out)))

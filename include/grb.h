@@ -198,6 +198,45 @@ int grb_flt_stage(grb_ctx* ctx, int32_t remove_phase_one, int32_t mode, grb_stat
 /* Copy all phase-two route words (route2_off[n] words) to the host. */
 int grb_read_routes2(grb_ctx* ctx, int32_t* routes2);
 
+/* ---- Z-shape stage (the reference's GGR pipeline, pipeline_ggr.hpp:8-144) */
+
+/* Wire-cost mode of the cost tables: 0 = default; 1 = the GGR build's integer
+ * wire costs, clamped to [0, 1e7] and truncated (full_update.cuh:47-50),
+ * which the Z-shape stage's integer DP expects.  Takes effect at the next
+ * cost refresh (every cell is recomputed). */
+int grb_set_wire_cost_mode(grb_ctx* ctx, int32_t integer_wire);
+
+/* Z-shape trees, CSR by net id over the uploaded nets, in the reference's
+ * encoding (zshape::encode_batch, zshape_topology.hpp:59-121): nodes in
+ * preorder from the tree's first leaf; per node its 3-D coordinate (layer L =
+ * Steiner point) and up to three child preorder indices (-1 = none). */
+typedef struct grb_zshape_trees {
+    const int32_t* node_off;   /* [n+1] */
+    const int32_t* coord;
+    const int32_t* child;      /* [3 per node] */
+} grb_zshape_trees;
+
+/* Upload Z-shape trees (host buffers); also derives every net's bounding box
+ * and allocates the DP planes (22 int planes of (L+1) * max(X,Y)^2). */
+int grb_upload_zshape(grb_ctx* ctx, const grb_zshape_trees* trees);
+
+/* Refine every batch of the current plan into bounding-box batches
+ * (zshape::generate_bbox_batches, zshape_topology.hpp:7-57: box area
+ * descending, rounds of at most max_batch nets with disjoint boxes) and make
+ * the reversed list the plan (pipeline_ggr.hpp:51-55).  The current plan must
+ * hold the first-fit groups in execution order (as grb_plan_batches leaves
+ * it).  bbox: [minx, maxx, miny, maxy] per net id, or NULL for the boxes of
+ * the uploaded Z-shape trees.  max_batch <= 256 (the reference uses 250). */
+int grb_plan_bbox_batches(grb_ctx* ctx, const int32_t* bbox, int32_t max_batch, int32_t* n_batches);
+
+/* Run the Z-shape stage over the current plan (pipeline_ggr.hpp:119-134): per
+ * batch refresh_cost, Z-shape DP and traceback (zshape::solve, reset_nodes,
+ * convert_routes) into the route words, ++stamp, thread-per-net wire then via
+ * commit (commit_wire_demand / commit_via_demand, demand.cuh:129-232).  The
+ * reference's host post-processing (promote_congested_segments,
+ * canonicalize_routes) stays with the caller. */
+int grb_zshape_stage(grb_ctx* ctx, int32_t mode, grb_stats* stats);
+
 /* Congestion view for the FLT topology builder (congestion.cuh:60-112). */
 int grb_congestion_view(grb_ctx* ctx, uint8_t* congestion, float* xsum, float* ysum);
 
