@@ -83,6 +83,9 @@ SIGNATURES = {
     "grb_flt_stage": (C.c_int, [P, C.c_int32, C.c_int32, C.POINTER(GrbStats)]),
     "grb_read_routes2": (C.c_int, [P, P]),
     "grb_set_wire_cost_mode": (C.c_int, [P, C.c_int32]),
+    "grb_softmin_forward": (C.c_int, [P, C.c_int32, C.c_double, P, P, C.c_double, P, C.POINTER(C.c_double)]),
+    "grb_softmin_backward": (C.c_int, [P, C.c_int32, C.c_double, P, P, C.c_double, C.c_double, P, P,
+                                       C.POINTER(C.c_double)]),
     "grb_upload_zshape": (C.c_int, [P, C.POINTER(GrbZshapeTrees)]),
     "grb_plan_bbox_batches": (C.c_int, [P, P, C.c_int32, C.POINTER(C.c_int32)]),
     "grb_zshape_stage": (C.c_int, [P, C.c_int32, C.POINTER(GrbStats)]),

@@ -17,6 +17,7 @@
 #include "device/cost.cuh"
 #include "device/flt.cuh"
 #include "device/lshape.cuh"
+#include "device/softmin.cuh"
 #include "device/zshape.cuh"
 
 using namespace grb;
@@ -418,6 +419,94 @@ __global__ void k_bbox_scatter(const int* batch_off, const int* tmp, const int* 
     }
 }
 
+// --- soft-min DAG and adjoint (softmin.cuh) ---------------------------------
+constexpr int kSoftThreads = 128;
+
+template <class T>
+__global__ void k_soft_tables(Tables Tb, Soft<T> S) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c < Tb.cells) soft_tables_cell<T>(Tb, S, c);
+}
+// Track k of layer l (one thread each): first cell, stride and length.
+__device__ __forceinline__ bool soft_track(const Tables& Tb, int t, int& base, int& stride, int& len) {
+    const int M = max(Tb.X, Tb.Y), l = t / M, k = t - l * M;
+    if (l >= Tb.L) return false;
+    if (along_y(Tb, l)) {
+        if (k >= Tb.X) return false;
+        base = cell_index(Tb, l, k, 0); stride = 1; len = Tb.Y;
+    } else {
+        if (k >= Tb.Y) return false;
+        base = cell_index(Tb, l, 0, k); stride = Tb.Y; len = Tb.X;
+    }
+    return true;
+}
+template <class T>
+__global__ void k_soft_prefix(Tables Tb, Soft<T> S) {
+    int base, stride, len;
+    if (!soft_track(Tb, blockIdx.x * blockDim.x + threadIdx.x, base, stride, len)) return;
+    T acc = 0;
+    for (int q = 0; q < len; ++q) {
+        S.P[base + q * stride] = acc;
+        acc += S.wc[base + q * stride];
+    }
+}
+template <class T>
+__global__ void __launch_bounds__(kSoftThreads) k_soft_forward(Tables Tb, Soft<T> S, Plan P, int n) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x, nt = gridDim.x * blockDim.x;
+    T* dist = S.slot + size_t(t) * 2 * S.slot_nodes * Tb.L * Tb.L;
+    for (int id = t; id < n; id += nt)
+        S.net_cost[id] = P.node_off[id + 1] > P.node_off[id] ? soft_net_forward<T>(Tb, S, P, id, dist) : T(0);
+}
+template <class T>
+__global__ void __launch_bounds__(kSoftThreads) k_soft_backward(Tables Tb, Soft<T> S, Plan P, int n, T g) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x, nt = gridDim.x * blockDim.x;
+    T* dist = S.slot + size_t(t) * 2 * S.slot_nodes * Tb.L * Tb.L;
+    T* gd = dist + size_t(S.slot_nodes) * Tb.L * Tb.L;
+    for (int id = t; id < n; id += nt)
+        if (P.node_off[id + 1] > P.node_off[id]) soft_net_backward<T>(Tb, S, P, id, dist, gd, g);
+}
+// dwc[j] = sum over later track positions of dP (presum[i] = sum_{j<i} wc[j]).
+template <class T>
+__global__ void k_soft_suffix(Tables Tb, Soft<T> S, T* dwc) {
+    int base, stride, len;
+    if (!soft_track(Tb, blockIdx.x * blockDim.x + threadIdx.x, base, stride, len)) return;
+    T acc = 0;
+    for (int q = len - 1; q >= 0; --q) {
+        dwc[base + q * stride] = acc;
+        acc += S.dP[base + q * stride];
+    }
+}
+// Chain rule to capacity and the per-edge unit wire cost.
+template <class T>
+__global__ void k_soft_chain(Tables Tb, Soft<T> S, const T* dwc, T* dcap, T* duw) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= Tb.cells) return;
+    const int l = c / Tb.XY, rem = c - l * Tb.XY, x = rem / Tb.Y, y = rem - x * Tb.Y;
+    const bool ay = along_y(Tb, l);
+    const int pos = ay ? y : x, len = ay ? Tb.Y : Tb.X, stride = ay ? 1 : Tb.Y;
+    T g = dwc[c] * soft_incr_dcap<T>(Tb, S, c, l, 1);
+    if (pos == 0) g += S.dvc[c] * soft_incr_dcap<T>(Tb, S, c, l, 1);
+    else if (pos < len - 1) g += S.dvc[c] * soft_incr_dcap<T>(Tb, S, c, l, static_cast<T>(0.5));
+    if (pos + 1 == len - 1) g += S.dvc[c + stride] * soft_incr_dcap<T>(Tb, S, c, l, 1);
+    else if (pos + 1 < len - 1) g += S.dvc[c + stride] * soft_incr_dcap<T>(Tb, S, c, l, static_cast<T>(0.5));
+    dcap[c] = g;
+    duw[c] = dwc[c] * static_cast<T>(soft_edge_len(Tb, l, x, y));
+}
+// Deterministic sum of v[0..n) into *out (one CTA).
+template <class T>
+__global__ void __launch_bounds__(1024) k_soft_sum(const T* v, int n, double* out) {
+    __shared__ double part[1024];
+    double acc = 0;
+    for (int k = threadIdx.x; k < n; k += blockDim.x) acc += static_cast<double>(v[k]);
+    part[threadIdx.x] = acc;
+    __syncthreads();
+    for (int w = blockDim.x / 2; w; w >>= 1) {
+        if (threadIdx.x < w) part[threadIdx.x] += part[threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *out = part[0];
+}
+
 // --- batching kernels -------------------------------------------------------
 // One net per CTA in the per-net phases (a chunk's nets spread over the grid).
 __global__ void k_batch_phase1(BatchState B, int s) {
@@ -643,6 +732,12 @@ struct grb_ctx {
     cudaGraphExec_t z_graph = nullptr;
     long long z_graph_key[3] = {-1, -1, -1};
     int64_t z_graph_kernels = 0;
+    // soft-min workspace (grb_softmin_forward / backward)
+    std::vector<void*> soft_bufs;
+    char* soft_cells = nullptr;       // 6 arrays of cells doubles
+    char* soft_slot = nullptr;
+    size_t soft_slot_bytes = 0;
+    double* soft_scalar = nullptr;
     // graph cache
     cudaGraphExec_t graph = nullptr;
     int graph_version = -1, graph_stamp = -1;
@@ -915,6 +1010,85 @@ int z_stage_persistent(grb_ctx* c, int stamp0) {
     return GRB_OK;
 }
 
+// --- soft-min executors ------------------------------------------------------
+int soft_threads(const grb_ctx* c) { return c->sms * kSoftThreads; }
+
+int soft_workspace(grb_ctx* c) {
+    const size_t cells = c->T.cells;
+    const int nodes = std::max(c->max_nodes, 1);
+    const size_t slot = size_t(soft_threads(c)) * 2 * nodes * c->T.L * c->T.L * sizeof(double);
+    if (c->soft_cells && c->soft_slot_bytes >= slot) return GRB_OK;
+    GRB_CUDA(c, cudaStreamSynchronize(c->stream));
+    free_all(c->soft_bufs);
+    int rc = 0;
+    rc |= dalloc(c, &c->soft_cells, 6 * cells * sizeof(double), c->soft_bufs);
+    rc |= dalloc(c, &c->soft_slot, slot, c->soft_bufs);
+    rc |= dalloc(c, &c->soft_scalar, 2, c->soft_bufs);
+    if (rc) { free_all(c->soft_bufs); c->soft_cells = nullptr; return GRB_ENOMEM; }
+    c->soft_slot_bytes = slot;
+    return GRB_OK;
+}
+
+template <class T>
+Soft<T> soft_view(grb_ctx* c, double tau, const void* cap, const void* uw, double uv, T* net_cost) {
+    const size_t cells = c->T.cells;
+    T* a = reinterpret_cast<T*>(c->soft_cells);
+    Soft<T> S{};
+    S.cap = static_cast<const T*>(cap);
+    S.uw = static_cast<const T*>(uw);
+    S.uv = static_cast<T>(uv);
+    S.tau = static_cast<T>(tau);
+    S.wc = a; S.vc = a + cells; S.P = a + 2 * cells; S.dP = a + 3 * cells; S.dvc = a + 4 * cells;
+    S.slot = reinterpret_cast<T*>(c->soft_slot);
+    S.slot_nodes = std::max(c->max_nodes, 1);
+    S.net_cost = net_cost;
+    return S;
+}
+
+template <class T>
+int soft_forward(grb_ctx* c, double tau, const void* cap, const void* uw, double uv, T* net_cost, double* total) {
+    const Tables& Tb = c->T;
+    const int n = c->n_nets;
+    Soft<T> S = soft_view<T>(c, tau, cap, uw, uv, net_cost);
+    const int M = std::max(Tb.X, Tb.Y);
+    k_soft_tables<T><<<(Tb.cells + 255) / 256, 256, 0, c->stream>>>(Tb, S);
+    k_soft_prefix<T><<<(Tb.L * M + 127) / 128, 128, 0, c->stream>>>(Tb, S);
+    const int th = std::min(soft_threads(c), std::max(n, 1));
+    k_soft_forward<T><<<(th + kSoftThreads - 1) / kSoftThreads, kSoftThreads, 0, c->stream>>>(Tb, S, make_plan(c), n);
+    k_soft_sum<T><<<1, 1024, 0, c->stream>>>(net_cost, n, c->soft_scalar);
+    c->launches += 4;
+    GRB_CUDA(c, cudaGetLastError());
+    GRB_CUDA(c, cudaMemcpyAsync(total, c->soft_scalar, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    GRB_CUDA(c, cudaStreamSynchronize(c->stream));
+    return GRB_OK;
+}
+
+template <class T>
+int soft_backward(grb_ctx* c, double tau, const void* cap, const void* uw, double uv, double g, T* dcap, T* duw,
+                  double* duv) {
+    const Tables& Tb = c->T;
+    const int n = c->n_nets;
+    const size_t cells = Tb.cells;
+    Soft<T> S = soft_view<T>(c, tau, cap, uw, uv, nullptr);
+    T* dwc = reinterpret_cast<T*>(c->soft_cells) + 5 * cells;
+    const int M = std::max(Tb.X, Tb.Y);
+    k_soft_tables<T><<<(Tb.cells + 255) / 256, 256, 0, c->stream>>>(Tb, S);
+    k_soft_prefix<T><<<(Tb.L * M + 127) / 128, 128, 0, c->stream>>>(Tb, S);
+    GRB_CUDA(c, cudaMemsetAsync(S.dP, 0, sizeof(T) * cells, c->stream));
+    GRB_CUDA(c, cudaMemsetAsync(S.dvc, 0, sizeof(T) * cells, c->stream));
+    const int th = std::min(soft_threads(c), std::max(n, 1));
+    k_soft_backward<T><<<(th + kSoftThreads - 1) / kSoftThreads, kSoftThreads, 0, c->stream>>>(Tb, S, make_plan(c), n,
+                                                                                              static_cast<T>(g));
+    k_soft_suffix<T><<<(Tb.L * M + 127) / 128, 128, 0, c->stream>>>(Tb, S, dwc);
+    k_soft_chain<T><<<(Tb.cells + 255) / 256, 256, 0, c->stream>>>(Tb, S, dwc, dcap, duw);
+    k_soft_sum<T><<<1, 1024, 0, c->stream>>>(S.dvc, int(cells), c->soft_scalar + 1);
+    c->launches += 6;
+    GRB_CUDA(c, cudaGetLastError());
+    GRB_CUDA(c, cudaMemcpyAsync(duv, c->soft_scalar + 1, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    GRB_CUDA(c, cudaStreamSynchronize(c->stream));
+    return GRB_OK;
+}
+
 // --- FLT stage executors ---------------------------------------------------
 int flt_stamps(const grb_ctx* c, int remove) { return c->n_batches * (remove ? 2 : 1); }
 
@@ -1177,6 +1351,7 @@ void grb_destroy(grb_ctx* c) {
     if (c->graph) cudaGraphExecDestroy(c->graph);
     if (c->flt_graph) cudaGraphExecDestroy(c->flt_graph);
     if (c->z_graph) cudaGraphExecDestroy(c->z_graph);
+    free_all(c->soft_bufs);
     free_all(c->z_bufs);
     free_all(c->net_bufs);
     free_all(c->geom_bufs);
@@ -1834,6 +2009,42 @@ int grb_flt_stage(grb_ctx* c, int32_t remove_phase_one, int32_t mode, grb_stats*
     c->dag_ms = ms;
     if ((rc = prof_collect(c))) return rc;
     return stats ? grb_get_stats(c, stats) : GRB_OK;
+}
+
+int grb_softmin_forward(grb_ctx* c, int32_t dtype, double tau, const void* capacity, const void* unit_wire,
+                        double unit_via, void* net_cost, double* total) {
+    if (!c) return GRB_EINVAL;
+    if (!c->node_off) return fail(c, GRB_EINVAL, "no nets uploaded");
+    if (!(tau > 0) || !capacity || !unit_wire || !net_cost || !total) return fail(c, GRB_EINVAL, "bad soft-min arguments");
+    if (dtype != GRB_F32 && dtype != GRB_F64) return fail(c, GRB_EINVAL, "dtype must be GRB_F32 or GRB_F64");
+    GRB_CUDA(c, cudaSetDevice(c->device));
+    int rc = soft_workspace(c);
+    if (rc) return rc;
+    if (dtype == GRB_F64)
+        return soft_forward<double>(c, tau, capacity, unit_wire, unit_via, static_cast<double*>(net_cost), total);
+    return soft_forward<float>(c, tau, capacity, unit_wire, unit_via, static_cast<float*>(net_cost), total);
+}
+
+int grb_softmin_backward(grb_ctx* c, int32_t dtype, double tau, const void* capacity, const void* unit_wire,
+                         double unit_via, double grad_total, void* dcap, void* dunit_wire, double* dunit_via) {
+    if (!c) return GRB_EINVAL;
+    if (!c->node_off) return fail(c, GRB_EINVAL, "no nets uploaded");
+    if (!(tau > 0) || !capacity || !unit_wire || !dcap || !dunit_wire || !dunit_via)
+        return fail(c, GRB_EINVAL, "bad soft-min arguments");
+    if (dtype != GRB_F32 && dtype != GRB_F64) return fail(c, GRB_EINVAL, "dtype must be GRB_F32 or GRB_F64");
+    GRB_CUDA(c, cudaSetDevice(c->device));
+    int rc = soft_workspace(c);
+    if (rc) return rc;
+    double duv = 0;
+    if (dtype == GRB_F64)
+        rc = soft_backward<double>(c, tau, capacity, unit_wire, unit_via, grad_total, static_cast<double*>(dcap),
+                                   static_cast<double*>(dunit_wire), &duv);
+    else
+        rc = soft_backward<float>(c, tau, capacity, unit_wire, unit_via, grad_total, static_cast<float*>(dcap),
+                                  static_cast<float*>(dunit_wire), &duv);
+    if (rc) return rc;
+    *dunit_via = duv;  // the adjoint already carries grad_total
+    return GRB_OK;
 }
 
 int grb_zshape_stage(grb_ctx* c, int32_t mode, grb_stats* stats) {

@@ -237,6 +237,29 @@ int grb_plan_bbox_batches(grb_ctx* ctx, const int32_t* bbox, int32_t max_batch, 
  * canonicalize_routes) stays with the caller. */
 int grb_zshape_stage(grb_ctx* ctx, int32_t mode, grb_stats* stats);
 
+/* ---- Differentiable routing cost (no counterpart in the reference) ------- */
+#define GRB_F32 0
+#define GRB_F64 1
+
+/* Soft-min L-shape DAG: the DP of Lshape_route (lshape_thread.cuh:18-171)
+ * over every uploaded net with each min replaced by
+ * smin(v) = -tau * log(sum exp(-v / tau)), on cost tables computed in the
+ * working precision from `capacity` and the per-edge `unit_wire` cost
+ * (device arrays of L*X*Y floats or doubles, per dtype) at the context's
+ * current demand (full_update.cuh:9-83 without float narrowing).  Writes each
+ * net's soft cost to net_cost (device, n values) and their sum to *total.
+ * As tau -> 0 the value tends to the hard DP's optimum. */
+int grb_softmin_forward(grb_ctx* ctx, int32_t dtype, double tau, const void* capacity, const void* unit_wire,
+                        double unit_via, void* net_cost, double* total);
+/* Hand-written adjoint of grb_softmin_forward: grad_total * d(total)/d(capacity)
+ * into dcap, d(total)/d(unit_wire) per edge into dunit_wire (device arrays
+ * like the inputs) and d(total)/d(unit_via) into *dunit_via.  Each net's DP
+ * tables are recomputed in a per-thread slot (memory bounded by the threads
+ * in flight, not by the nets); as tau -> 0 the gradient tends to the
+ * indicator of the chosen routes. */
+int grb_softmin_backward(grb_ctx* ctx, int32_t dtype, double tau, const void* capacity, const void* unit_wire,
+                         double unit_via, double grad_total, void* dcap, void* dunit_wire, double* dunit_via);
+
 /* Congestion view for the FLT topology builder (congestion.cuh:60-112). */
 int grb_congestion_view(grb_ctx* ctx, uint8_t* congestion, float* xsum, float* ysum);
 
