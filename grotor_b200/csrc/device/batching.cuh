@@ -54,23 +54,33 @@ __device__ __forceinline__ void batch_error(const BatchState& B, int code, int i
     if (atomicCAS(B.error, 0, code) == 0) *B.error_info = info;
 }
 
+// Cells of the segments [s0, s1) of `segs` with step `step`; threads t of n
+// split each segment's cells.  Every warp of the group fetches 32 segment
+// endpoints per memory round trip and broadcasts them by shuffle, so a net
+// with many short segments does not wait one load latency per segment.
+// All 32 lanes of each warp of the group must call this.
+template <class F>
+__device__ __forceinline__ void for_each_segment_cell(const int* segs, int s0, int s1, int step, int t, int n, F f) {
+    const int lane = t & 31;
+    for (int base = s0; base < s1; base += 32) {
+        int a = 0, b = -1;
+        if (base + lane < s1) { a = segs[2 * (base + lane)]; b = segs[2 * (base + lane) + 1]; }
+        const int m = min(32, s1 - base);
+        for (int q = 0; q < m; ++q) {
+            const int aq = __shfl_sync(0xffffffffu, a, q), bq = __shfl_sync(0xffffffffu, b, q);
+            if (bq < aq) continue;
+            const int cnt = (bq - aq) / step + 1;
+            for (int k = t; k < cnt; k += n) f(aq + k * step);
+        }
+    }
+}
+
 // Visit every cell net `id` marks (duplicates allowed); threads t of n split
 // the work.
 template <class F>
 __device__ __forceinline__ void for_each_mark(const BatchState& B, int id, int t, int n, F f) {
-    const int hstep = B.sparsity * B.Y, vstep = B.sparsity;
-    for (int s = B.hseg_off[id]; s < B.hseg_off[id + 1]; ++s) {
-        const int a = B.hsegs[2 * s], b = B.hsegs[2 * s + 1];
-        if (b < a) continue;
-        const int cnt = (b - a) / hstep + 1;
-        for (int k = t; k < cnt; k += n) f(a + k * hstep);
-    }
-    for (int s = B.vseg_off[id]; s < B.vseg_off[id + 1]; ++s) {
-        const int a = B.vsegs[2 * s], b = B.vsegs[2 * s + 1];
-        if (b < a) continue;
-        const int cnt = (b - a) / vstep + 1;
-        for (int k = t; k < cnt; k += n) f(a + k * vstep);
-    }
+    for_each_segment_cell(B.hsegs, B.hseg_off[id], B.hseg_off[id + 1], B.sparsity * B.Y, t, n, f);
+    for_each_segment_cell(B.vsegs, B.vseg_off[id], B.vseg_off[id + 1], B.sparsity, t, n, f);
     const int p0 = B.point_off[id], np = B.point_off[id + 1] - p0;
     for (int k = t; k < 4 * np; k += n) {
         const int p = B.points[p0 + k / 4], x = p / B.Y, y = p - x * B.Y;
@@ -103,7 +113,7 @@ __device__ __forceinline__ void batch_phase1(const BatchState& B, int s, int jj,
     const int t = G.t, n = G.n;
     for (int w = t; w < B.W; w += n) acc[w] = 0u;
     G.sync();
-    for_each_mark(B, id, t, n, [&](int q) { atomicOr(B.localmask + size_t(q) * kChunkWords + word, bit); });
+    for_each_mark(B, id, t, n, [&](int q) { red_or(B.localmask + size_t(q) * kChunkWords + word, bit); });
     const int p0 = B.point_off[id], np = B.point_off[id + 1] - p0;
     for (int k = t; k < np * B.W; k += n) {
         const int w = k % B.W;
@@ -146,7 +156,7 @@ __device__ __forceinline__ void batch_phase4(const BatchState& B, int s, int jj,
     const unsigned bit = 1u << (c & 31);
     const int word = c >> 5, lword = jj >> 5;
     for_each_mark(B, id, G.t, G.n, [&](int q) {
-        atomicOr(B.cellmask + size_t(q) * B.W + word, bit);
+        red_or(B.cellmask + size_t(q) * B.W + word, bit);
         B.localmask[size_t(q) * kChunkWords + lword] = 0u;
     });
 }

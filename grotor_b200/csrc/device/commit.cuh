@@ -43,7 +43,7 @@ __device__ __forceinline__ void commit_net_wires(const Tables& T, const Plan& P,
         }
         for (int pos = lo + lane; pos < hi; pos += 32) {
             const int c = layer * T.XY + (ay ? x0 * T.Y + pos : pos * T.Y + y0);
-            atomicAdd(T.demand + c, 2 * K);
+            red_add(T.demand + c, 2 * K);
             T.ts[c] = stamp;
             if (!ay) {
                 set_bits(T.dirty_wire, c >> 5, 1u << (c & 31));
@@ -58,7 +58,7 @@ __device__ __forceinline__ void commit_net_wires(const Tables& T, const Plan& P,
 }
 
 __device__ __forceinline__ void add_via_demand(const Tables& T, int c, int half) {
-    atomicAdd(T.demand + c, half);
+    red_add(T.demand + c, half);
     mark_edge_dirty(T, c);
 }
 
@@ -119,7 +119,7 @@ __device__ __forceinline__ void commit_thread_wires(const Tables& T, const Plan&
         }
         for (int pos = lo; pos < hi; ++pos) {
             const int c = layer * T.XY + (ay ? x0 * T.Y + pos : pos * T.Y + y0);
-            atomicAdd(T.demand + c, 2 * K);
+            red_add(T.demand + c, 2 * K);
             T.ts[c] = stamp;
             if (!ay) {
                 set_bits(T.dirty_wire, c >> 5, 1u << (c & 31));

@@ -77,8 +77,17 @@ __device__ __forceinline__ int track_length(const Tables& T, int l) { return alo
 
 // Dirty marking uses fire-and-forget atomics (no return value): the refresh
 // finds the work by scanning the bitmaps, which are small (one bit per cell).
+// Fire-and-forget reductions: the result is never read, so the instruction
+// carries no return value and the issuing thread does not wait for L2.
+__device__ __forceinline__ void red_or(unsigned* p, unsigned v) {
+    asm volatile("red.relaxed.gpu.global.or.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ void red_add(int* p, int v) {
+    asm volatile("red.relaxed.gpu.global.add.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
 __device__ __forceinline__ void set_bits(unsigned* bits, int word, unsigned mask) {
-    if (mask) atomicOr(bits + word, mask);
+    if (mask) red_or(bits + word, mask);
 }
 
 __device__ __forceinline__ void mark_group_dirty(const Tables& T, int l, int track) {

@@ -536,7 +536,7 @@ __global__ void k_batch_phase4(BatchState B, int s) {
 // Persistent batching: CTAs of kChunk threads (the in-chunk solve needs one
 // thread per net); the per-net phases use each half CTA as a net group so a
 // chunk's nets fit in one wave.
-__global__ void __launch_bounds__(kChunk) k_batch_persistent(BatchState B, GridSync S, Tables T) {
+__global__ void __launch_bounds__(kChunk, 2) k_batch_persistent(BatchState B, GridSync S, Tables T) {
     extern __shared__ __align__(16) unsigned bsm[];
     __shared__ unsigned acc[2][64];
     constexpr int kHalf = kChunk / 2;
