@@ -22,7 +22,11 @@
 //       4. every net ORs its colour into cellmask over its marks and clears the
 //          chunk-local masks.
 //   The chunks run inside one cooperative kernel with bounded grid barriers
-//   (persistent form) or as one launch per phase (plain form).
+//   (persistent form) or as one launch per phase (plain form).  The chunk-local
+//   masks are double-buffered by chunk parity, so the persistent form rasters
+//   chunk k+1 on every other CTA while one CTA solves chunk k, and reads the
+//   forbidden colours (step 1's second half) together with the predecessors
+//   after chunk k-1 is published.
 #pragma once
 #include "common.cuh"
 
@@ -38,7 +42,8 @@ struct BatchState {
     const int* hseg_off; const int* hsegs;
     const int* vseg_off; const int* vsegs;
     unsigned* cellmask;    // [X*Y][W]
-    unsigned* localmask;   // [X*Y][kChunkWords]
+    unsigned* localmask;   // [X*Y][kChunkWords], chunks of even index
+    unsigned* localmask2;  // [X*Y][kChunkWords], chunks of odd index
     unsigned* fmask;       // [kChunk][W]
     unsigned* pred;        // [kChunk][kChunkWords]
     unsigned* fullmask;    // [W]
@@ -103,44 +108,48 @@ struct NetGroup {
     }
 };
 
-// The per-net phases run one net per group (its threads share the net's marks
-// and points); `acc` is group shared memory of at least max(W, 16) words.
-// Phase 1: chunk-local raster and forbidden colours from earlier chunks.
-__device__ __forceinline__ void batch_phase1(const BatchState& B, int s, int jj, unsigned* acc, const NetGroup& G) {
+// Chunk-local mask buffer of the chunk starting at order position s.
+__device__ __forceinline__ unsigned* chunk_mask(const BatchState& B, int s) {
+    return ((s / kChunk) & 1) ? B.localmask2 : B.localmask;
+}
+
+// The per-net steps run one net per group (its threads share the net's marks
+// and points).
+// Step 1a: chunk-local raster.
+__device__ __forceinline__ void batch_raster(const BatchState& B, int s, int jj, const NetGroup& G) {
     const int id = B.order[s + jj];
     const unsigned bit = 1u << (jj & 31);
     const int word = jj >> 5;
-    const int t = G.t, n = G.n;
-    for (int w = t; w < B.W; w += n) acc[w] = 0u;
-    G.sync();
-    for_each_mark(B, id, t, n, [&](int q) { red_or(B.localmask + size_t(q) * kChunkWords + word, bit); });
-    const int p0 = B.point_off[id], np = B.point_off[id + 1] - p0;
-    for (int k = t; k < np * B.W; k += n) {
-        const int w = k % B.W;
-        const unsigned v = B.cellmask[size_t(B.points[p0 + k / B.W]) * B.W + w];
-        if (v) atomicOr(acc + w, v);
-    }
-    G.sync();
-    for (int w = t; w < B.W; w += n) B.fmask[size_t(jj) * B.W + w] = acc[w];
-    G.sync();
+    unsigned* lm = chunk_mask(B, s);
+    for_each_mark(B, id, G.t, G.n, [&](int q) { red_or(lm + size_t(q) * kChunkWords + word, bit); });
 }
 
-// Phase 2: predecessors inside the chunk.
-__device__ __forceinline__ void batch_phase2(const BatchState& B, int s, int jj, unsigned* acc, const NetGroup& G) {
+// Step 1b + 2: forbidden colours from earlier (published) chunks and the
+// predecessors inside the chunk, both ORed over the net's query points.
+// `acc` is group shared memory of W + kChunkWords words.
+__device__ __forceinline__ void batch_forbid_preds(const BatchState& B, int s, int jj, unsigned* acc, const NetGroup& G) {
     const int id = B.order[s + jj];
     const int t = G.t, n = G.n;
+    const int W = B.W;
     const int words = (jj >> 5) + 1;  // only bits of earlier chunk nets matter
-    for (int w = t; w < kChunkWords; w += n) acc[w] = 0u;
+    const unsigned* lm = chunk_mask(B, s);
+    for (int w = t; w < W + kChunkWords; w += n) acc[w] = 0u;
     G.sync();
     const int p0 = B.point_off[id], np = B.point_off[id + 1] - p0;
-    for (int k = t; k < np * words; k += n) {
-        const int w = k % words;
-        const unsigned v = B.localmask[size_t(B.points[p0 + k / words]) * kChunkWords + w];
+    for (int k = t; k < np * W; k += n) {
+        const int w = k % W;
+        const unsigned v = B.cellmask[size_t(B.points[p0 + k / W]) * W + w];
         if (v) atomicOr(acc + w, v);
     }
+    for (int k = t; k < np * words; k += n) {
+        const int w = k % words;
+        const unsigned v = lm[size_t(B.points[p0 + k / words]) * kChunkWords + w];
+        if (v) atomicOr(acc + W + w, v);
+    }
     G.sync();
+    for (int w = t; w < W; w += n) B.fmask[size_t(jj) * W + w] = acc[w];
     for (int w = t; w < kChunkWords; w += n) {
-        unsigned v = w < words ? acc[w] : 0u;
+        unsigned v = w < words ? acc[W + w] : 0u;
         if (w == (jj >> 5)) v &= (1u << (jj & 31)) - 1u;
         B.pred[jj * kChunkWords + w] = v;
     }
@@ -155,9 +164,10 @@ __device__ __forceinline__ void batch_phase4(const BatchState& B, int s, int jj,
     const int c = B.batch_of[s + jj];
     const unsigned bit = 1u << (c & 31);
     const int word = c >> 5, lword = jj >> 5;
+    unsigned* lm = chunk_mask(B, s);
     for_each_mark(B, id, G.t, G.n, [&](int q) {
         red_or(B.cellmask + size_t(q) * B.W + word, bit);
-        B.localmask[size_t(q) * kChunkWords + lword] = 0u;
+        lm[size_t(q) * kChunkWords + lword] = 0u;
     });
 }
 

@@ -33,7 +33,7 @@ __device__ __forceinline__ void commit_net_wires(const Tables& T, const Plan& P,
             T.ts[a] = stamp;
             T.ts[b] = stamp;
             if (hi > lo) {
-                mark_group_dirty(T, layer, ay ? x0 : y0);
+                mark_group_dirty(T, layer, ay ? x0 : y0, lo);
                 if (ay) {
                     const int first = layer * T.XY + x0 * T.Y + lo;
                     mark_range(T.dirty_wire, first, first + (hi - lo) - 1);
@@ -110,7 +110,7 @@ __device__ __forceinline__ void commit_thread_wires(const Tables& T, const Plan&
         T.ts[a] = stamp;
         T.ts[b] = stamp;
         if (hi > lo) {
-            mark_group_dirty(T, layer, ay ? x0 : y0);
+            mark_group_dirty(T, layer, ay ? x0 : y0, lo);
             if (ay) {
                 const int first = layer * T.XY + x0 * T.Y + lo;
                 mark_range(T.dirty_wire, first, first + (hi - lo) - 1);

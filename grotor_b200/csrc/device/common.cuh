@@ -40,6 +40,8 @@ struct Tables {
     // Prefix groups: kTrackGroup adjacent tracks of one layer.
     int group_base[kMaxLayers + 1];
     unsigned* group_flag;  // [n_groups], nonzero = some track of the group changed
+    int* group_first;      // [n_groups] first 32-position chunk whose wire cost changed (INT_MAX: none)
+    int* first_list;       // [n_groups] group_first of each listed dirty group
     int n_groups;
     int* group_list;       // [n_groups] dirty groups of the current refresh
     int* group_count;      // [1]
@@ -90,8 +92,16 @@ __device__ __forceinline__ void set_bits(unsigned* bits, int word, unsigned mask
     if (mask) red_or(bits + word, mask);
 }
 
-__device__ __forceinline__ void mark_group_dirty(const Tables& T, int l, int track) {
-    T.group_flag[T.group_base[l] + track / kTrackGroup] = 1u;
+__device__ __forceinline__ void red_min(int* p, int v) {
+    asm volatile("red.relaxed.gpu.global.min.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// A wire cost of track `track` at position `pos` changed: the group's prefix
+// must be rebuilt from that position's 32-position chunk on.
+__device__ __forceinline__ void mark_group_dirty(const Tables& T, int l, int track, int pos) {
+    const int g = T.group_base[l] + track / kTrackGroup;
+    T.group_flag[g] = 1u;
+    red_min(T.group_first + g, pos >> 5);
 }
 
 // A demand change on edge cell c invalidates its wire cost, its own via cost
@@ -103,7 +113,7 @@ __device__ __forceinline__ void mark_edge_dirty(const Tables& T, int c) {
     set_bits(T.dirty_wire, c >> 5, 1u << (c & 31));
     set_bits(T.dirty_via, c >> 5, 1u << (c & 31));
     if (pos + 1 < len) set_bits(T.dirty_via, (c + stride) >> 5, 1u << ((c + stride) & 31));
-    mark_group_dirty(T, l, ay ? x : y);
+    mark_group_dirty(T, l, ay ? x : y, pos);
 }
 
 // Mark cells [first, last] of a bitmap with one atomic per word
@@ -118,13 +128,18 @@ __device__ __forceinline__ void mark_range(unsigned* bits, int first, int last) 
     }
 }
 
-// Grid-wide barrier for cooperative launches.  Every wait is bounded by the
-// global timer; on expiry the kernel records kETimedOut and callers return.
+// Grid-wide barrier for cooperative launches: one monotone arrival counter
+// (zeroed before the launch).  Barrier k of a launch completes when the
+// counter reaches k * gridDim.x, so no reset or generation word is needed and
+// a barrier costs one acquire-release atomic plus acquire polls.  Every wait
+// is bounded by the global timer; on expiry the kernel records kETimedOut and
+// callers return.  `epoch` counts this block's barriers (a kernel-local copy).
 struct GridSync {
     unsigned* count;
-    unsigned* generation;
+    unsigned* generation;          // unused by the counter barrier
     unsigned long long timeout_ns;
     unsigned long long* phase_ns;  // optional per-phase time accumulators
+    unsigned epoch;
 };
 
 __device__ __forceinline__ unsigned long long global_ns() {
@@ -133,38 +148,37 @@ __device__ __forceinline__ unsigned long long global_ns() {
     return t;
 }
 
-__device__ __forceinline__ bool grid_sync(const GridSync& s, const Tables& T) {
+__device__ __forceinline__ bool grid_sync(GridSync& s, const Tables& T) {
     __shared__ int ok;
+    const unsigned target = (++s.epoch) * gridDim.x;
     __syncthreads();
     if (threadIdx.x == 0) {
         ok = 1;
-        volatile unsigned* gen = s.generation;
-        const unsigned g = *gen;
+        unsigned v;
         __threadfence();
-        const unsigned arrived = atomicAdd(s.count, 1u);
-        if (arrived == gridDim.x - 1) {
-            *reinterpret_cast<volatile unsigned*>(s.count) = 0;
-            __threadfence();
-            atomicAdd(s.generation, 1u);
-        } else {
+        asm volatile("atom.add.acq_rel.gpu.u32 %0, [%1], 1;" : "=r"(v) : "l"(s.count) : "memory");
+        v += 1;
+        if (v < target) {
             const unsigned long long start = global_ns();
             unsigned spins = 0;
-            while (*gen == g) {
+            while (v < target) {
                 if ((++spins & 63) == 0) {
                     if (global_ns() - start > s.timeout_ns) { set_error(T, kETimedOut, blockIdx.x); ok = 0; break; }
                     if (*reinterpret_cast<volatile int*>(T.error) == kETimedOut) { ok = 0; break; }
                 }
-                __nanosleep(64);
+                // Relaxed polls (an acquire load per poll would invalidate the
+                // SM's L1 under the warps still working), backing off after the
+                // first polls so long waits do not flood the counter's L2 slice.
+                if (spins > 16) __nanosleep(spins > 256 ? 128 : 32);
+                asm volatile("ld.relaxed.gpu.u32 %0, [%1];" : "=r"(v) : "l"(s.count) : "memory");
             }
         }
-        __threadfence();
+        __threadfence();  // acquire: later reads see every block's writes
     }
     __syncthreads();
     return ok != 0;
 }
 
-// Per-phase timing of a cooperative kernel: block 0 / thread 0 adds the time
-// since its previous mark (a grid barrier has just completed) to slot k.
 struct PhaseClock {
     unsigned long long last = 0;
     __device__ __forceinline__ void start(const GridSync& s) {

@@ -75,10 +75,16 @@ __device__ __forceinline__ float via_cost_at(const Tables& T, int c) {
 // wire-dirty cell is always via-dirty).  Both words are cleared.
 // `warp`/`nwarps` number the calling warps across the launch.
 __device__ __forceinline__ void refresh_dirty_cells(const Tables& T, int warp, int nwarps, int lane) {
+    // The next window's bitmap words are loaded while this one is processed.
+    int nw = warp * 32 + lane;
+    unsigned nvb = nw < T.words ? T.dirty_via[nw] : 0u;
+    unsigned nwb = nw < T.words ? T.dirty_wire[nw] : 0u;
     for (int base = warp * 32; base < T.words; base += nwarps * 32) {
         const int w = base + lane;
-        const unsigned vb = w < T.words ? T.dirty_via[w] : 0u;
-        const unsigned wb = w < T.words ? T.dirty_wire[w] : 0u;
+        const unsigned vb = nvb, wb = nwb;
+        nw = w + nwarps * 32;
+        nvb = nw < T.words ? T.dirty_via[nw] : 0u;
+        nwb = nw < T.words ? T.dirty_wire[nw] : 0u;
         const int n = __popc(vb);
         int incl = n;
 #pragma unroll
@@ -273,8 +279,11 @@ __device__ __forceinline__ void collect_dirty_groups(const Tables& T) {
     __syncthreads();
     for (int g = threadIdx.x; g < T.n_groups; g += blockDim.x) {
         if (T.group_flag[g]) {
-            T.group_list[atomicAdd(&count, 1)] = g;
+            const int k = atomicAdd(&count, 1);
+            T.group_list[k] = g;
+            T.first_list[k] = T.group_first[g];
             T.group_flag[g] = 0u;
+            T.group_first[g] = 0x7fffffff;
         }
     }
     __syncthreads();
@@ -282,11 +291,13 @@ __device__ __forceinline__ void collect_dirty_groups(const Tables& T) {
 }
 
 // Work items (k, c): chunk c of the k-th dirty group, enumerated as
-// k * tree_chunks + c.
+// k * tree_chunks + c.  Chunks before the group's first changed chunk keep
+// their prefix values and their level-0 totals from the previous rebuild.
 __device__ __forceinline__ bool prefix_item(const Tables& T, int item, int& g, int& c) {
     const int k = item / T.tree_chunks;
     c = item - k * T.tree_chunks;
     if (k >= *reinterpret_cast<const volatile int*>(T.group_count)) return false;
+    if (c < T.first_list[k]) return false;
     g = T.group_list[k];
     int l = 0;
     while (l + 1 <= T.L && g >= T.group_base[l + 1]) ++l;

@@ -74,7 +74,7 @@ __global__ void k_mark_all_dirty(Tables T) {
         T.dirty_wire[i] = m;
         T.dirty_via[i] = m;
     }
-    if (i < T.n_groups) T.group_flag[i] = 1u;
+    if (i < T.n_groups) { T.group_flag[i] = 1u; T.group_first[i] = 0; }
 }
 
 __device__ __forceinline__ Arena warp_arena(char* smem, size_t arena_b, int warp, int L, int nmax) {
@@ -508,18 +508,18 @@ __global__ void __launch_bounds__(1024) k_soft_sum(const T* v, int n, double* ou
 }
 
 // --- batching kernels -------------------------------------------------------
-// One net per CTA in the per-net phases (a chunk's nets spread over the grid).
-__global__ void k_batch_phase1(BatchState B, int s) {
-    __shared__ unsigned acc[64];
+// One net per CTA in the per-net steps (a chunk's nets spread over the grid).
+constexpr int kBatchAcc = 96;  // >= W + kChunkWords for every W phase 3 admits
+__global__ void k_batch_raster(BatchState B, int s) {
     const NetGroup G{int(threadIdx.x), int(blockDim.x), 0};
     const int m = min(kChunk, B.n - s);
-    for (int j = blockIdx.x; j < m; j += gridDim.x) batch_phase1(B, s, j, acc, G);
+    for (int j = blockIdx.x; j < m; j += gridDim.x) batch_raster(B, s, j, G);
 }
-__global__ void k_batch_phase2(BatchState B, int s) {
-    __shared__ unsigned acc[kChunkWords];
+__global__ void k_batch_forbid_preds(BatchState B, int s) {
+    __shared__ unsigned acc[kBatchAcc];
     const NetGroup G{int(threadIdx.x), int(blockDim.x), 0};
     const int m = min(kChunk, B.n - s);
-    for (int j = blockIdx.x; j < m; j += gridDim.x) batch_phase2(B, s, j, acc, G);
+    for (int j = blockIdx.x; j < m; j += gridDim.x) batch_forbid_preds(B, s, j, acc, G);
 }
 __global__ void __launch_bounds__(kChunk) k_batch_phase3(BatchState B, int s) {
     extern __shared__ __align__(16) unsigned bsm[];
@@ -534,26 +534,35 @@ __global__ void k_batch_phase4(BatchState B, int s) {
 }
 
 // Persistent batching: CTAs of kChunk threads (the in-chunk solve needs one
-// thread per net); the per-net phases use each half CTA as a net group so a
-// chunk's nets fit in one wave.
+// thread per net); the per-net steps use each half CTA as a net group so a
+// chunk's nets fit in one wave.  Per chunk k, three barriers:
+//   forbidden colours + predecessors of k (all groups) |
+//   solve k on CTA 0 while the other CTAs raster chunk k+1 (other buffer) |
+//   publish k (all groups).
 __global__ void __launch_bounds__(kChunk, 2) k_batch_persistent(BatchState B, GridSync S, Tables T) {
     extern __shared__ __align__(16) unsigned bsm[];
-    __shared__ unsigned acc[2][64];
+    __shared__ unsigned acc[2][kBatchAcc];
     constexpr int kHalf = kChunk / 2;
     const int half = threadIdx.x / kHalf;
     const NetGroup G{int(threadIdx.x % kHalf), kHalf, 1 + half};
     const int gi = half * gridDim.x + blockIdx.x, ng = 2 * gridDim.x;
+    // Raster groups of the overlapped step: every CTA but the solving one.
+    const bool solo = gridDim.x == 1;
+    const int rgi = solo ? gi : half * (gridDim.x - 1) + blockIdx.x - 1, rng = solo ? ng : 2 * (gridDim.x - 1);
     PhaseClock clk;
     clk.start(S);
+    for (int j = gi; j < min(kChunk, B.n); j += ng) batch_raster(B, 0, j, G);
+    if (!grid_sync(S, T)) return;
+    clk.mark(S, 0);
     for (int s = 0; s < B.n; s += kChunk) {
         const int m = min(kChunk, B.n - s);
-        for (int j = gi; j < m; j += ng) batch_phase1(B, s, j, acc[half], G);
-        if (!grid_sync(S, T)) return;
-        clk.mark(S, 0);
-        for (int j = gi; j < m; j += ng) batch_phase2(B, s, j, acc[half], G);
+        for (int j = gi; j < m; j += ng) batch_forbid_preds(B, s, j, acc[half], G);
         if (!grid_sync(S, T)) return;
         clk.mark(S, 1);
+        const int s2 = s + kChunk, m2 = s2 < B.n ? min(kChunk, B.n - s2) : 0;
         if (blockIdx.x == 0) batch_phase3(B, s, bsm);
+        if (blockIdx.x != 0 || solo)
+            for (int j = rgi; j < m2; j += rng) batch_raster(B, s2, j, G);
         if (!grid_sync(S, T)) return;
         clk.mark(S, 2);
         if (*reinterpret_cast<volatile int*>(B.error)) return;
@@ -707,7 +716,8 @@ struct grb_ctx {
     int work_cap = 0;
     unsigned* sync = nullptr;   // [count, generation]
     // batching buffers
-    unsigned *cellmask = nullptr, *localmask = nullptr, *fmask = nullptr, *pred = nullptr, *fullmask = nullptr;
+    unsigned *cellmask = nullptr, *localmask = nullptr, *localmask2 = nullptr, *fmask = nullptr, *pred = nullptr,
+             *fullmask = nullptr;
     int *bcount = nullptr, *ncolors = nullptr, *batch_of = nullptr, *brank = nullptr, *order = nullptr;
     int bW = 0, bn_cap = 0;
     // FLT stage (grb_upload_geometry / grb_upload_flt)
@@ -1316,6 +1326,8 @@ int grb_create(const grb_grid* g, int32_t device, grb_ctx** out) {
     rc |= dalloc(cp, &T.dirty_wire, c->words, cp->owned);
     rc |= dalloc(cp, &T.dirty_via, c->words, cp->owned);
     rc |= dalloc(cp, &T.group_flag, ng, cp->owned);
+    rc |= dalloc(cp, &T.group_first, ng, cp->owned);
+    rc |= dalloc(cp, &T.first_list, ng, cp->owned);
     rc |= dalloc(cp, &T.group_list, ng, cp->owned);
     rc |= dalloc(cp, &T.group_count, 1, cp->owned);
     T.tree_chunks = prefix_chunks(std::max(T.X, T.Y));
@@ -1358,7 +1370,7 @@ void grb_destroy(grb_ctx* c) {
     free_all(c->flt_bufs);
     free_all(c->owned);
     for (void* p : {(void*)c->ids, (void*)c->batch_off, (void*)c->gscratch, (void*)c->work, (void*)c->cellmask,
-                    (void*)c->localmask, (void*)c->fmask, (void*)c->pred, (void*)c->fullmask, (void*)c->bcount,
+                    (void*)c->localmask, (void*)c->localmask2, (void*)c->fmask, (void*)c->pred, (void*)c->fullmask, (void*)c->bcount,
                     (void*)c->ncolors, (void*)c->batch_of, (void*)c->brank, (void*)c->order})
         if (p) cudaFree(p);
     if (c->ev0) cudaEventDestroy(c->ev0);
@@ -1838,12 +1850,14 @@ int grb_plan_batches(grb_ctx* c, const int32_t* order, int32_t n, int32_t limit,
         c->bn_cap = n;
     }
     if (!c->localmask) {
-        if (cudaMalloc(&c->localmask, xy * kChunkWords * 4) || cudaMalloc(&c->pred, size_t(kChunk) * kChunkWords * 4) ||
+        if (cudaMalloc(&c->localmask, xy * kChunkWords * 4) || cudaMalloc(&c->localmask2, xy * kChunkWords * 4) ||
+            cudaMalloc(&c->pred, size_t(kChunk) * kChunkWords * 4) ||
             cudaMalloc(&c->ncolors, 4)) {
             cudaGetLastError();
             return fail(c, GRB_ENOMEM, "batching buffers");
         }
         GRB_CUDA(c, cudaMemsetAsync(c->localmask, 0, xy * kChunkWords * 4, c->stream));
+        GRB_CUDA(c, cudaMemsetAsync(c->localmask2, 0, xy * kChunkWords * 4, c->stream));
     }
     GRB_CUDA(c, cudaMemcpyAsync(c->order, order, sizeof(int) * n, cudaMemcpyHostToDevice, c->stream));
     GRB_CUDA(c, cudaEventRecord(c->ev0, c->stream));
@@ -1868,12 +1882,13 @@ int grb_plan_batches(grb_ctx* c, const int32_t* order, int32_t n, int32_t limit,
         B.order = c->order;
         B.point_off = c->point_off; B.points = c->points;
         B.hseg_off = c->hseg_off; B.hsegs = c->hsegs; B.vseg_off = c->vseg_off; B.vsegs = c->vsegs;
-        B.cellmask = c->cellmask; B.localmask = c->localmask; B.fmask = c->fmask; B.pred = c->pred;
+        B.cellmask = c->cellmask; B.localmask = c->localmask; B.localmask2 = c->localmask2;
+        B.fmask = c->fmask; B.pred = c->pred;
         B.fullmask = c->fullmask; B.count = c->bcount; B.n_colors = c->ncolors;
         B.batch_of = c->batch_of; B.rank = c->brank;
         B.error = c->T.error; B.error_info = c->T.error_info;
         const size_t smem = phase3_smem_bytes(W);
-        if (smem > 200 * 1024) return fail(c, GRB_ELIMIT, "too many batch colours");
+        if (smem > 200 * 1024 || W + kChunkWords > kBatchAcc) return fail(c, GRB_ELIMIT, "too many batch colours");
         if (mode == GRB_MODE_PERSISTENT) {
             int per_sm = 0;
             GRB_CUDA(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_persistent, kChunk, smem));
@@ -1889,10 +1904,10 @@ int grb_plan_batches(grb_ctx* c, const int32_t* order, int32_t n, int32_t limit,
             for (int s = 0; s < n; s += kChunk) {
                 cudaEvent_t e;
                 if ((rc = prof_begin(c, 0, &e))) return rc;
-                k_batch_phase1<<<grid, 256, 0, c->stream>>>(B, s);
+                k_batch_raster<<<grid, 256, 0, c->stream>>>(B, s);
                 prof_end(c, e);
                 if ((rc = prof_begin(c, 1, &e))) return rc;
-                k_batch_phase2<<<grid, 256, 0, c->stream>>>(B, s);
+                k_batch_forbid_preds<<<grid, 256, 0, c->stream>>>(B, s);
                 prof_end(c, e);
                 if ((rc = prof_begin(c, 2, &e))) return rc;
                 k_batch_phase3<<<1, kChunk, smem, c->stream>>>(B, s);
@@ -1911,6 +1926,7 @@ int grb_plan_batches(grb_ctx* c, const int32_t* order, int32_t n, int32_t limit,
             // Not enough colour words: clear the chunk-local masks and retry wider.
             GRB_CUDA(c, cudaMemsetAsync(c->T.error, 0, 2 * sizeof(int), c->stream));
             GRB_CUDA(c, cudaMemsetAsync(c->localmask, 0, xy * kChunkWords * 4, c->stream));
+            GRB_CUDA(c, cudaMemsetAsync(c->localmask2, 0, xy * kChunkWords * 4, c->stream));
             W *= 2;
             continue;
         }
