@@ -83,6 +83,7 @@ SIGNATURES = {
     "grb_flt_stage": (C.c_int, [P, C.c_int32, C.c_int32, C.POINTER(GrbStats)]),
     "grb_read_routes2": (C.c_int, [P, P]),
     "grb_set_wire_cost_mode": (C.c_int, [P, C.c_int32]),
+    "grb_autotune": (C.c_int, [P, C.c_int32, P, P]),
     "grb_softmin_forward": (C.c_int, [P, C.c_int32, C.c_double, P, P, C.c_double, P, C.POINTER(C.c_double)]),
     "grb_softmin_backward": (C.c_int, [P, C.c_int32, C.c_double, P, P, C.c_double, C.c_double, P, P,
                                        C.POINTER(C.c_double)]),

@@ -64,6 +64,24 @@ struct Plan {
     const int* ids;            // net ids in execution order
     const int* batch_off;      // [n_batches+1] into ids
     int n_batches;
+    // The same plan with each batch's nets grouped by size bucket
+    // (kDpBuckets): bucket_ids, and per batch kDpBuckets+1 offsets into it.
+    const int* bucket_ids;
+    const int* bucket_off;
+};
+
+// Size buckets of the routing DP: tree nodes <= 4, <= 8, <= 16, more.
+constexpr int kDpBuckets = 4;
+__host__ __device__ __forceinline__ int dp_bucket(int nodes) {
+    return nodes <= 4 ? 0 : nodes <= 8 ? 1 : nodes <= 16 ? 2 : 3;
+}
+__host__ __device__ __forceinline__ int dp_bucket_nodes(int b) { return b == 0 ? 4 : b == 1 ? 8 : 16; }
+
+// Launch shape chosen per size bucket (grb_autotune): nets per CTA of the
+// per-batch DP launch, nets taken per work-queue grab in the persistent form.
+struct DpTune {
+    int per_cta[kDpBuckets];
+    int per_grab[kDpBuckets];
 };
 
 __device__ __forceinline__ bool along_y(const Tables& T, int l) { return ((l & 1) ^ T.DIR) != 0; }

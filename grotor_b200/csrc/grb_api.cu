@@ -98,6 +98,63 @@ __global__ void __launch_bounds__(kDpThreads) k_lshape_batch(Tables T, Plan P, i
     lshape_net(T, P, id, stamp, A, lane, false);
 }
 
+// Per-batch DP launch over every size bucket of batch b at once: CTA ranges
+// [block_off[k], block_off[k+1]) serve bucket k with per_cta[k] nets per CTA
+// (warps beyond it return) and an arena of nmax[k] nodes per warp (global
+// scratch where nmax is 0).
+struct BucketLaunch {
+    int block_off[kDpBuckets + 1];
+    int per[kDpBuckets];
+    int nmax[kDpBuckets];
+    int arena[kDpBuckets];
+};
+__global__ void k_lshape_bucketed(Tables T, Plan P, int b, int stamp, BucketLaunch BL, char* gscratch,
+                                  size_t gslot) {
+    extern __shared__ __align__(16) char smem[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    int bk = 0;
+    while (bk + 1 < kDpBuckets && int(blockIdx.x) >= BL.block_off[bk + 1]) ++bk;
+    if (warp >= BL.per[bk]) return;
+    const int lo = P.bucket_off[b * (kDpBuckets + 1) + bk], hi = P.bucket_off[b * (kDpBuckets + 1) + bk + 1];
+    const int k = (int(blockIdx.x) - BL.block_off[bk]) * BL.per[bk] + warp;
+    if (lo + k >= hi) return;
+    const int id = P.bucket_ids[lo + k];
+    const int N = P.node_off[id + 1] - P.node_off[id];
+    const int nmax = BL.nmax[bk];
+    Arena A;
+    if (N <= nmax) A = warp_arena(smem, BL.arena[bk], warp, T.L, nmax);
+    else if (gscratch) A = carve_arena(gscratch + size_t(k) * gslot, T.L, N);
+    else { if (lane == 0) set_error(T, kELimit, id); return; }
+    lshape_net(T, P, id, stamp, A, lane, false);
+}
+
+// Group each batch's nets by size bucket (one CTA per batch).
+__global__ void k_plan_buckets(Plan P, int* bucket_ids, int* bucket_off) {
+    __shared__ int cnt[kDpBuckets], cur[kDpBuckets];
+    const int b = blockIdx.x, lo = P.batch_off[b], hi = P.batch_off[b + 1];
+    if (threadIdx.x < kDpBuckets) cnt[threadIdx.x] = 0;
+    __syncthreads();
+    for (int k = lo + threadIdx.x; k < hi; k += blockDim.x) {
+        const int id = P.ids[k];
+        atomicAdd(&cnt[dp_bucket(P.node_off[id + 1] - P.node_off[id])], 1);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int acc = lo;
+        for (int q = 0; q < kDpBuckets; ++q) {
+            bucket_off[b * (kDpBuckets + 1) + q] = acc;
+            cur[q] = acc;
+            acc += cnt[q];
+        }
+        bucket_off[b * (kDpBuckets + 1) + kDpBuckets] = hi;
+    }
+    __syncthreads();
+    for (int k = lo + threadIdx.x; k < hi; k += blockDim.x) {
+        const int id = P.ids[k];
+        bucket_ids[atomicAdd(&cur[dp_bucket(P.node_off[id + 1] - P.node_off[id])], 1)] = id;
+    }
+}
+
 __global__ void k_commit_wires(Tables T, Plan P, int b, int stamp, int K) {
     const int lane = threadIdx.x & 31;
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, warps = (gridDim.x * blockDim.x) >> 5;
@@ -117,7 +174,7 @@ __global__ void k_commit_vias(Tables T, Plan P, int b, int stamp, int K) {
 // groups) -> prefix pass 1 -> prefix trees -> prefix pass 2 -> route and commit
 // wires -> commit vias, separated by bounded grid barriers.
 __global__ void __launch_bounds__(kPersistentThreads, 2) k_lshape_persistent(Tables T, Plan P, GridSync S,
-        int stamp0, int nmax, size_t arena_b, char* gscratch, size_t gslot, int* work) {
+        int stamp0, int nmax, size_t arena_b, char* gscratch, size_t gslot, int* work, DpTune tune) {
     extern __shared__ __align__(16) char smem[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int gwarp = warp * gridDim.x + blockIdx.x, nwarps = gridDim.x * (blockDim.x >> 5);
@@ -146,19 +203,27 @@ __global__ void __launch_bounds__(kPersistentThreads, 2) k_lshape_persistent(Tab
         }
         if (!grid_sync(S, T)) return;
         clk.mark(S, 7);
-        // Route every net of the batch and commit its wires.
+        // Route every net of the batch and commit its wires: size buckets from
+        // the largest down (long nets start first), nets taken from the
+        // bucket's work queue `per_grab` at a time.
         const int lo = P.batch_off[b], cnt = P.batch_off[b + 1] - lo;
         const Arena A = warp_arena(smem, arena_b, warp, T.L, nmax);
-        while (true) {
-            int k = 0;
-            if (lane == 0) k = atomicAdd(work + b, 1);
-            k = __shfl_sync(0xffffffffu, k, 0);
-            if (k >= cnt) break;
-            const int id = P.ids[lo + k];
-            const int N = P.node_off[id + 1] - P.node_off[id];
-            if (N <= nmax) lshape_net(T, P, id, stamp, A, lane, true);
-            else if (gscratch) lshape_net(T, P, id, stamp, carve_arena(gscratch + size_t(gwarp) * gslot, T.L, N), lane, true);
-            else if (lane == 0) set_error(T, kELimit, id);
+        for (int bk = kDpBuckets - 1; bk >= 0; --bk) {
+            const int blo = P.bucket_off[b * (kDpBuckets + 1) + bk], bhi = P.bucket_off[b * (kDpBuckets + 1) + bk + 1];
+            const int g = tune.per_grab[bk];
+            while (true) {
+                int k = 0;
+                if (lane == 0) k = atomicAdd(work + b * kDpBuckets + bk, g);
+                k = __shfl_sync(0xffffffffu, k, 0);
+                if (blo + k >= bhi) break;
+                for (int q = blo + k; q < min(blo + k + g, bhi); ++q) {
+                    const int id = P.bucket_ids[q];
+                    const int N = P.node_off[id + 1] - P.node_off[id];
+                    if (N <= nmax) lshape_net(T, P, id, stamp, A, lane, true);
+                    else if (gscratch) lshape_net(T, P, id, stamp, carve_arena(gscratch + size_t(gwarp) * gslot, T.L, N), lane, true);
+                    else if (lane == 0) set_error(T, kELimit, id);
+                }
+            }
         }
         if (!grid_sync(S, T)) return;
         clk.mark(S, 5);
@@ -748,6 +813,12 @@ struct grb_ctx {
     char* soft_slot = nullptr;
     size_t soft_slot_bytes = 0;
     double* soft_scalar = nullptr;
+    // size-bucketed plan and tuned launch shapes
+    int* bucket_ids = nullptr;
+    int* bucket_off = nullptr;
+    int bucket_cap = 0, bucket_batches = 0, bucket_version = -1;
+    std::vector<int> h_bucket_off;  // [n_batches][kDpBuckets+1]
+    DpTune tune{{4, 4, 4, 4}, {1, 1, 1, 1}};
     // graph cache
     cudaGraphExec_t graph = nullptr;
     int graph_version = -1, graph_stamp = -1;
@@ -819,7 +890,38 @@ Plan make_plan(const grb_ctx* c) {
     P.node_off = c->node_off; P.nodes = c->nodes; P.parents = c->parents;
     P.route_off = c->route_off; P.routes = c->routes;
     P.ids = c->ids; P.batch_off = c->batch_off; P.n_batches = c->n_batches;
+    P.bucket_ids = c->bucket_ids; P.bucket_off = c->bucket_off;
     return P;
+}
+
+// The plan grouped by size bucket, rebuilt when the plan changes (one launch).
+int ensure_buckets(grb_ctx* c) {
+    if (c->bucket_version == c->plan_version && c->bucket_ids) return GRB_OK;
+    if (c->bucket_cap < c->plan_n || c->bucket_batches < c->n_batches || !c->bucket_ids) {
+        if (c->bucket_ids) cudaFree(c->bucket_ids);
+        if (c->bucket_off) cudaFree(c->bucket_off);
+        c->bucket_ids = nullptr; c->bucket_off = nullptr;
+        const int cap = std::max(c->plan_n, 1), nb = std::max(c->n_batches, 1);
+        if (cudaMalloc(&c->bucket_ids, sizeof(int) * cap) != cudaSuccess ||
+            cudaMalloc(&c->bucket_off, sizeof(int) * size_t(nb) * (kDpBuckets + 1)) != cudaSuccess) {
+            cudaGetLastError();
+            return fail(c, GRB_ENOMEM, "bucketed plan");
+        }
+        c->bucket_cap = cap;
+        c->bucket_batches = nb;
+    }
+    c->h_bucket_off.assign(size_t(c->n_batches) * (kDpBuckets + 1), 0);
+    if (c->n_batches) {
+        k_plan_buckets<<<c->n_batches, 256, 0, c->stream>>>(make_plan(c), c->bucket_ids, c->bucket_off);
+        c->launches += 1;
+        GRB_CUDA(c, cudaGetLastError());
+        // The per-batch launches are sized from the bucket counts.
+        GRB_CUDA(c, cudaMemcpyAsync(c->h_bucket_off.data(), c->bucket_off, sizeof(int) * c->h_bucket_off.size(),
+                                    cudaMemcpyDeviceToHost, c->stream));
+        GRB_CUDA(c, cudaStreamSynchronize(c->stream));
+    }
+    c->bucket_version = c->plan_version;
+    return GRB_OK;
 }
 
 // The plan with the phase-two routes of the FLT stage.
@@ -901,25 +1003,51 @@ int refresh_plain(grb_ctx* c) {
     return GRB_OK;
 }
 
-int route_plain(grb_ctx* c, int b, int stamp) {
-    const int cnt = c->h_batch_off[b + 1] - c->h_batch_off[b];
-    if (cnt <= 0) return GRB_OK;
-    const int nmax = dp_nmax(c);
-    const size_t ab = arena_bytes(c->T.L, nmax);
-    const int wpb = kDpThreads / 32;
-    const int blocks = (cnt + wpb - 1) / wpb;
-    const int rc = ensure_gscratch(c, blocks * wpb);
-    if (rc) return rc;
+// Batch b in the per-batch DP form: one launch for all its size buckets (or
+// only bucket `only` when only >= 0), each bucket with its tuned nets per CTA
+// and an arena sized to the bucket.
+int launch_buckets(grb_ctx* c, int b, int stamp, int only) {
+    const int* bo = c->h_bucket_off.data() + size_t(b) * (kDpBuckets + 1);
+    BucketLaunch BL{};
+    int blocks = 0, threads = 32;
+    size_t smem = 0;
+    int gslots = 0;
+    for (int bk = 0; bk < kDpBuckets; ++bk) {
+        BL.block_off[bk] = blocks;
+        const int cnt = (only < 0 || only == bk) ? bo[bk + 1] - bo[bk] : 0;
+        BL.per[bk] = c->tune.per_cta[bk];
+        BL.nmax[bk] = bk < kDpBuckets - 1 ? std::min(dp_bucket_nodes(bk), std::max(c->max_nodes, 1)) : 0;
+        BL.arena[bk] = BL.nmax[bk] ? int(arena_bytes(c->T.L, BL.nmax[bk])) : 0;
+        if (cnt <= 0) continue;
+        const int nb = (cnt + BL.per[bk] - 1) / BL.per[bk];
+        blocks += nb;
+        threads = std::max(threads, 32 * BL.per[bk]);
+        smem = std::max(smem, size_t(BL.per[bk]) * BL.arena[bk]);
+        if (!BL.nmax[bk]) gslots = nb * BL.per[bk];
+    }
+    BL.block_off[kDpBuckets] = blocks;
+    if (!blocks) return GRB_OK;
+    if (gslots) {
+        const int rc = ensure_gscratch(c, gslots);
+        if (rc) return rc;
+    }
     const size_t arena_slot = arena_bytes(c->T.L, std::max(c->max_nodes, 1));
-    cudaEvent_t e;
-    const int prc = prof_begin(c, 5, &e);
-    if (prc) return prc;
-    k_lshape_batch<<<blocks, kDpThreads, ab * wpb, c->stream>>>(c->T, make_plan(c), b, stamp, nmax, ab,
-                                                                 c->gscratch, arena_slot);
-    prof_end(c, e);
+    k_lshape_bucketed<<<blocks, threads, smem, c->stream>>>(c->T, make_plan(c), b, stamp, BL, c->gscratch, arena_slot);
     c->launches += 1;
     GRB_CUDA(c, cudaGetLastError());
     return GRB_OK;
+}
+
+// Per-batch DP launch.
+int route_plain(grb_ctx* c, int b, int stamp) {
+    if (c->h_batch_off[b + 1] <= c->h_batch_off[b]) return GRB_OK;
+    int rc = ensure_buckets(c);
+    if (rc) return rc;
+    cudaEvent_t e;
+    if ((rc = prof_begin(c, 5, &e))) return rc;
+    rc = launch_buckets(c, b, stamp, -1);
+    prof_end(c, e);
+    return rc;
 }
 
 int commit_plain(grb_ctx* c, int b, int stamp, int K) {
@@ -1194,10 +1322,10 @@ int stage_graph(grb_ctx* c, int stamp0) {
     if (!c->graph || c->graph_version != c->plan_version || c->graph_stamp != stamp0) {
         if (c->graph) { cudaGraphExecDestroy(c->graph); c->graph = nullptr; }
         // Scratch must exist before capture (no allocation while capturing).
-        const int wpb = kDpThreads / 32;
         int maxcnt = 0;
         for (int b = 0; b < c->n_batches; ++b) maxcnt = std::max(maxcnt, c->h_batch_off[b + 1] - c->h_batch_off[b]);
-        int rc = ensure_gscratch(c, ((maxcnt + wpb - 1) / wpb) * wpb);
+        int rc = ensure_gscratch(c, maxcnt + 8);
+        if (!rc) rc = ensure_buckets(c);
         if (rc) return rc;
         const int64_t before = c->launches;
         const bool prof = c->profiling;
@@ -1237,19 +1365,22 @@ int stage_persistent(grb_ctx* c, int stamp0) {
     const size_t slot = arena_bytes(c->T.L, std::max(c->max_nodes, 1));
     int rc = ensure_gscratch(c, blocks * wpb);
     if (rc) return rc;
-    if (c->work_cap < c->n_batches) {
+    if ((rc = ensure_buckets(c))) return rc;
+    const int counters = c->n_batches * kDpBuckets;
+    if (c->work_cap < counters) {
         if (c->work) cudaFree(c->work);
         c->work = nullptr;
-        if (cudaMalloc(&c->work, sizeof(int) * c->n_batches) != cudaSuccess) { cudaGetLastError(); return fail(c, GRB_ENOMEM, "work counters"); }
-        c->work_cap = c->n_batches;
+        if (cudaMalloc(&c->work, sizeof(int) * counters) != cudaSuccess) { cudaGetLastError(); return fail(c, GRB_ENOMEM, "work counters"); }
+        c->work_cap = counters;
     }
-    GRB_CUDA(c, cudaMemsetAsync(c->work, 0, sizeof(int) * c->n_batches, c->stream));
+    GRB_CUDA(c, cudaMemsetAsync(c->work, 0, sizeof(int) * counters, c->stream));
     GRB_CUDA(c, cudaMemsetAsync(c->sync, 0, 2 * sizeof(unsigned), c->stream));
     Tables T = c->T;
     Plan P = make_plan(c);
     GridSync S{c->sync, c->sync + 1, kBarrierTimeoutNs, c->profiling ? c->d_phase : nullptr};
     char* gs = c->gscratch;
-    void* args[] = {&T, &P, &S, &stamp0, (void*)&nmax, (void*)&ab, &gs, (void*)&slot, &c->work};
+    DpTune tune = c->tune;
+    void* args[] = {&T, &P, &S, &stamp0, (void*)&nmax, (void*)&ab, &gs, (void*)&slot, &c->work, &tune};
     GRB_CUDA(c, cudaLaunchCooperativeKernel((void*)k_lshape_persistent, dim3(blocks), dim3(kPersistentThreads), args, smem, c->stream));
     c->launches += 1;
     return GRB_OK;
@@ -1348,6 +1479,7 @@ int grb_create(const grb_grid* g, int32_t device, grb_ctx** out) {
     GRB_CUDA(cp, cudaFuncSetAttribute(k_batch_phase3, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
     GRB_CUDA(cp, cudaFuncSetAttribute(k_batch_persistent, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
     GRB_CUDA(cp, cudaFuncSetAttribute(k_lshape_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    GRB_CUDA(cp, cudaFuncSetAttribute(k_lshape_bucketed, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
     GRB_CUDA(cp, cudaFuncSetAttribute(k_prefix_tree, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       int(prefix_smem_bytes(std::max(T.X, T.Y)))));
     const int r = grb_reset(cp);
@@ -1369,7 +1501,7 @@ void grb_destroy(grb_ctx* c) {
     free_all(c->geom_bufs);
     free_all(c->flt_bufs);
     free_all(c->owned);
-    for (void* p : {(void*)c->ids, (void*)c->batch_off, (void*)c->gscratch, (void*)c->work, (void*)c->cellmask,
+    for (void* p : {(void*)c->bucket_ids, (void*)c->bucket_off, (void*)c->ids, (void*)c->batch_off, (void*)c->gscratch, (void*)c->work, (void*)c->cellmask,
                     (void*)c->localmask, (void*)c->localmask2, (void*)c->fmask, (void*)c->pred, (void*)c->fullmask, (void*)c->bcount,
                     (void*)c->ncolors, (void*)c->batch_of, (void*)c->brank, (void*)c->order})
         if (p) cudaFree(p);
@@ -2093,6 +2225,78 @@ int grb_read_routes2(grb_ctx* c, int32_t* routes2) {
     if (c->route2_words)
         GRB_CUDA(c, cudaMemcpyAsync(routes2, c->F.routes2, sizeof(int) * c->route2_words, cudaMemcpyDeviceToHost, c->stream));
     GRB_CUDA(c, cudaStreamSynchronize(c->stream));
+    return GRB_OK;
+}
+
+int grb_autotune(grb_ctx* c, int32_t what, int32_t* per_cta, int32_t* per_grab) {
+    if (!c) return GRB_EINVAL;
+    if (!c->node_off) return fail(c, GRB_EINVAL, "no nets uploaded");
+    if (!c->n_batches) return fail(c, GRB_EINVAL, "no plan to tune on");
+    GRB_CUDA(c, cudaSetDevice(c->device));
+    int rc = ensure_buckets(c);
+    if (rc) return rc;
+    const bool prof = c->profiling;
+    c->profiling = false;
+    if (what & 1) {
+        // Per-batch DP form: coordinate descent over the buckets -- for each
+        // bucket in turn, time the whole per-batch launch of the three largest
+        // batches with each nets-per-CTA choice (DP only, on refreshed tables).
+        if ((rc = refresh_plain(c))) { c->profiling = prof; return rc; }
+        std::vector<int> order(c->n_batches);
+        for (int b = 0; b < c->n_batches; ++b) order[b] = b;
+        std::sort(order.begin(), order.end(), [&](int a, int b) {
+            return c->h_batch_off[a + 1] - c->h_batch_off[a] > c->h_batch_off[b + 1] - c->h_batch_off[b];
+        });
+        const int samples = std::min<int>(3, order.size());
+        for (int bk = 0; bk < kDpBuckets; ++bk) {
+            float best = 1e30f;
+            int choice = c->tune.per_cta[bk];
+            for (int per : {1, 2, 4, 8}) {
+                c->tune.per_cta[bk] = per;
+                float ms = 1e30f;
+                for (int rep = 0; rep < 3 && !rc; ++rep) {
+                    GRB_CUDA(c, cudaEventRecord(c->ev0, c->stream));
+                    for (int q = 0; q < samples && !rc; ++q) rc = launch_buckets(c, order[q], c->stamp + 1, -1);
+                    GRB_CUDA(c, cudaEventRecord(c->ev1, c->stream));
+                    GRB_CUDA(c, cudaEventSynchronize(c->ev1));
+                    float t = 0;
+                    GRB_CUDA(c, cudaEventElapsedTime(&t, c->ev0, c->ev1));
+                    ms = std::min(ms, t);
+                }
+                if (rc) { c->profiling = prof; return rc; }
+                if (ms < best) { best = ms; choice = per; }
+            }
+            c->tune.per_cta[bk] = choice;
+        }
+        if ((rc = check_device_error(c))) { c->profiling = prof; return rc; }
+    }
+    if (what & 2) {
+        // Persistent form: whole-stage runs from a reset state for each
+        // candidate set of nets per grab (small buckets take more per grab).
+        const int cands[4][kDpBuckets] = {{1, 1, 1, 1}, {2, 1, 1, 1}, {4, 2, 1, 1}, {8, 4, 2, 1}};
+        float best = 1e30f;
+        int pick = 0;
+        for (int k = 0; k < 4; ++k) {
+            for (int q = 0; q < kDpBuckets; ++q) c->tune.per_grab[q] = cands[k][q];
+            if ((rc = grb_reset(c))) { c->profiling = prof; return rc; }
+            GRB_CUDA(c, cudaEventRecord(c->ev0, c->stream));
+            if ((rc = stage_persistent(c, 0))) { c->profiling = prof; return rc; }
+            GRB_CUDA(c, cudaEventRecord(c->ev1, c->stream));
+            GRB_CUDA(c, cudaEventSynchronize(c->ev1));
+            float t = 0;
+            GRB_CUDA(c, cudaEventElapsedTime(&t, c->ev0, c->ev1));
+            if ((rc = check_device_error(c))) { c->profiling = prof; return rc; }
+            if (t < best) { best = t; pick = k; }
+        }
+        for (int q = 0; q < kDpBuckets; ++q) c->tune.per_grab[q] = cands[pick][q];
+    }
+    c->profiling = prof;
+    c->graph_version = -1;  // a captured per-batch sequence bakes in the launch shapes
+    if ((rc = grb_reset(c))) return rc;
+    for (int q = 0; q < kDpBuckets; ++q) {
+        if (per_cta) per_cta[q] = c->tune.per_cta[q];
+        if (per_grab) per_grab[q] = c->tune.per_grab[q];
+    }
     return GRB_OK;
 }
 

@@ -215,6 +215,16 @@ class Router:
         self._check(self._lib.grb_read_routes2(self._ctx, _p(out)))
         return out
 
+    def autotune(self, plain: bool = True, persistent: bool = True) -> dict:
+        """Pick nets-per-CTA (per-batch DP launch) and nets-per-grab (persistent
+        work queue) by size bucket (<= 4, <= 8, <= 16, > 16 tree nodes) on the
+        current plan; leaves the context reset."""
+        per_cta = np.zeros(4, np.int32)
+        per_grab = np.zeros(4, np.int32)
+        what = (1 if plain else 0) | (2 if persistent else 0)
+        self._check(self._lib.grb_autotune(self._ctx, what, _p(per_cta), _p(per_grab)))
+        return {"nets_per_cta": per_cta.tolist(), "nets_per_grab": per_grab.tolist()}
+
     # ---- Z-shape stage (GGR pipeline) ----------------------------------------
     def set_wire_cost_mode(self, integer_wire: bool):
         """True selects the GGR build's integer wire costs (clamped, truncated)."""

@@ -151,6 +151,17 @@ int grb_ripup_classify(grb_ctx* ctx, int32_t threshold, uint8_t* is_of);
  * device at once -- race; serialise them.  Results equal grb_ripup_classify's. */
 int grb_ripup_classify_noalloc(grb_ctx* ctx, int32_t threshold, uint8_t* is_of);
 
+/* Autotuner (no counterpart in the reference).  Nets of every batch are
+ * scheduled by size bucket (tree nodes <= 4, <= 8, <= 16, more; the
+ * persistent form takes the largest bucket first).  what & 1 times the
+ * per-batch DP launch of each bucket on the plan's largest batches for 1, 2,
+ * 4 and 8 nets per CTA (arena sized to the bucket); what & 2 runs the
+ * persistent stage from a reset state for candidate nets-per-grab sets of its
+ * work queue.  The choices stay in the context (and are copied to the
+ * optional per_cta[4] / per_grab[4]).  Needs nets and a plan; leaves the
+ * context reset (grb_reset).  Routes do not depend on the choices. */
+int grb_autotune(grb_ctx* ctx, int32_t what, int32_t* per_cta, int32_t* per_grab);
+
 /* ---- FLT stage (stage two of the default pipeline, flt.cuh:75-182) ------ */
 
 /* Replace the batching geometry of the uploaded nets (net::points and
