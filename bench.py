@@ -55,6 +55,11 @@ def parse_args():
     ap.add_argument("--no-compare", action="store_true", help="skip the plain / graph executor comparison")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
     ap.add_argument("--cpu-nets", type=int, default=0, help="CPU baseline sample size (0: automatic)")
+    ap.add_argument("--no-tune", action="store_true", help="skip grb_autotune (default launch shapes)")
+    ap.add_argument("--executor", default="persistent", choices=["persistent", "plain", "graph"],
+                    help="executor of the timed step (the headline is the persistent one)")
+    ap.add_argument("--no-extra", action="store_true",
+                    help="skip the Z-shape and soft-min stage measurements (other workloads)")
     return ap.parse_args()
 
 
@@ -275,8 +280,12 @@ def run_grotor(args):
         r.generate_batches_rsmt(order, BATCH_LIMIT, 1, mode)
         return r.lshape_route(mode)
 
+    tune = None
+    if not args.no_tune:  # launch shapes by size bucket, chosen on this plan (untimed)
+        r.generate_batches_rsmt(order, BATCH_LIMIT, 1, "persistent")
+        tune = r.autotune()
     for _ in range(args.warmup):
-        step("persistent")
+        step(args.executor)
     barrier(pg)
     torch.cuda.synchronize()
     clocks = Clocks(local)
@@ -286,7 +295,7 @@ def run_grotor(args):
     bt, dt = [], []
     e0.record(stream)
     for _ in range(args.steps):
-        st = step("persistent")
+        st = step(args.executor)
         bt.append(st["batching_ms"])
         dt.append(st["dag_ms"])
     e1.record(stream)
@@ -327,8 +336,8 @@ def run_grotor(args):
     for _ in range(args.steps):
         r.upload_nets(host_nets)
         r.reset()
-        r.generate_batches_rsmt(order_pin.numpy(), BATCH_LIMIT, 1, "persistent")
-        r.lshape_route("persistent")
+        r.generate_batches_rsmt(order_pin.numpy(), BATCH_LIMIT, 1, "plain" if args.executor != "persistent" else "persistent")
+        r.lshape_route(args.executor)
         routes_e2e = r.read_routes()
     e3.record(stream)
     torch.cuda.synchronize()
@@ -342,7 +351,7 @@ def run_grotor(args):
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": args.workload, "grid": [design.grid.X, design.grid.Y, design.grid.L + 1],
                    "nets": n_nets, "batches": int(stats_p["n_batches"]), "batch_limit": BATCH_LIMIT,
-                   "executor": "persistent", "parallelism": f"replicas{world}",
+                   "executor": args.executor, "parallelism": f"replicas{world}",
                    "l2": "inputs larger than L2 (cost/prefix/demand tables %.0f MB)" % (
                        design.grid.cells * 32 / 1e6)},
         "stage": {"batching_ms": float(np.mean(bt)), "dag_ms": float(np.mean(dt)),
@@ -401,6 +410,12 @@ def run_grotor(args):
         comp["routes_identical"] = identical
         result["executors"] = comp
 
+    result["config"]["autotune"] = tune
+    if rank == 0 and world == 1 and not args.no_extra:
+        r.close()
+        r = None
+        result["zshape"] = zshape_measure(args)
+        result["softmin"] = softmin_measure(args)
     if rank == 0 and world == 1 and not args.no_cpu:
         threads = os.cpu_count() or 1
         target = args.cpu_nets or 60000
@@ -410,11 +425,107 @@ def run_grotor(args):
                                              f"order ({info['nets']} nets, {info['batches']} batches): reference "
                                              f"CPU batching {info['batching_ms']:.0f} ms on 1 core + CPU DAG "
                                              f"restatement {info['dag_ms']:.0f} ms on {threads} threads")}
-    r.close()
+    if r is not None:
+        r.close()
     if pg is not None:
         pg.destroy_process_group()
     if rank == 0:
         print(json.dumps(result), flush=True)
+
+
+# --------------------------------------------------------------------------- other stages
+def _stream(r):
+    import torch
+    return torch.cuda.ExternalStream(r.stream_handle, device=torch.device("cuda", torch.cuda.current_device()))
+
+
+def zshape_measure(args, workload="large_800x800x10", steps=3, warmup=2):
+    """Z-shape stage (the GGR pipeline, configuration 'large' 800x800x10 with
+    900K nets) on the generator's trees: first-fit groups, bounding-box
+    batches and the Z-shape stage per step, persistent and plain executors."""
+    import torch
+
+    from grotor_b200 import Router
+    from grotor_b200.router import GrbError, NetArrays
+    from grotor_b200.synth import WORKLOADS, Design
+    d = Design(WORKLOADS[workload])
+    z = d.zshape_trees()
+    n = d.nets
+    zn = np.diff(z["node_off"]).astype(np.int64)
+    route_off = np.concatenate([[0], np.cumsum(1 + 64 * zn)]).astype(np.int64)
+    r = Router(d.grid)
+    r.upload_nets(NetArrays(n.node_off, n.nodes, n.parents, route_off, n.point_off, n.points, n.hseg_off, n.hsegs,
+                            n.vseg_off, n.vsegs))
+    r.upload_zshape(z)
+    r.set_wire_cost_mode(True)
+    stream = _stream(r)
+    out = {"workload": workload, "nets": int(n.n), "batch_limit": 250}
+    for mode in ("persistent", "plain"):
+        times, dag, first = [], [], []
+        for k in range(warmup + steps):
+            torch.cuda.synchronize()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            r.reset()
+            r.generate_batches_rsmt(d.order, BATCH_LIMIT, 1, mode)
+            fb = r.stats()["batching_ms"]
+            nb = r.plan_bbox_batches(250)
+            try:
+                st = r.zshape_route(mode)
+                status = "ok"
+            except GrbError as e:  # the reference's "Z-shape DP failure": the stage still ran to the end
+                st = r.stats()
+                status = str(e)
+            b.record(stream)
+            torch.cuda.synchronize()
+            if k >= warmup:
+                times.append(a.elapsed_time(b))
+                dag.append(st["dag_ms"])
+                first.append(fb)
+        out[mode] = {"ms_per_step": float(np.mean(times)), "nets_per_s": n.n / (np.mean(times) / 1e3),
+                     "first_fit_ms": float(np.mean(first)), "dag_ms": float(np.mean(dag)), "batches": int(nb),
+                     "wirelength": st["wirelength"], "vias": st["vias"], "status": status}
+    out["speedup_persistent_vs_plain"] = out["plain"]["ms_per_step"] / out["persistent"]["ms_per_step"]
+    r.close()
+    return out
+
+
+def softmin_measure(args, workload="softmin_320x320x10", taus=(1.0, 0.1, 0.01), reps=3):
+    """Soft-min DAG forward and adjoint (configuration 'soft-min', 320x320x10,
+    120K nets) in fp32, at the demand of the exact L-shape stage."""
+    import torch
+
+    from grotor_b200 import Router
+    from grotor_b200.softmin import routing_cost
+    from grotor_b200.synth import WORKLOADS, Design
+    d = Design(WORKLOADS[workload])
+    r = Router(d.grid)
+    r.upload_nets(d.nets)
+    r.generate_batches_rsmt(d.order, BATCH_LIMIT, 1, "persistent")
+    r.lshape_route("persistent")
+    g = d.grid
+    out = {"workload": workload, "nets": int(d.n_subnets), "dtype": "f32"}
+    for tau in taus:
+        cap = torch.tensor(np.asarray(g.capacity, np.float32), device="cuda").requires_grad_(True)
+        uw = torch.full_like(cap, float(g.unit_wire)).requires_grad_(True)
+        uv = torch.tensor(float(g.unit_via), device="cuda", requires_grad=True)
+        fw, bw = [], []
+        for k in range(reps + 1):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            F = routing_cost(r, cap, uw, uv, tau)
+            t1 = time.perf_counter()
+            F.backward()
+            torch.cuda.synchronize()
+            t2 = time.perf_counter()
+            cap.grad = uw.grad = uv.grad = None
+            if k:
+                fw.append((t1 - t0) * 1e3)
+                bw.append((t2 - t1) * 1e3)
+        out[f"tau_{tau:g}"] = {"forward_ms": float(np.mean(fw)), "backward_ms": float(np.mean(bw)),
+                               "total_cost": float(F.item())}
+    r.close()
+    return out
 
 
 # --------------------------------------------------------------------------- reference arm

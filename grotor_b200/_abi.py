@@ -107,6 +107,7 @@ SIGNATURES = {
     "grb_design_write": (C.c_int, [P, C.c_char_p, C.c_char_p]),
     "grb_design_build_topology": (C.c_int, [P, C.c_int32, C.c_int32]),
     "grb_design_nets": (C.c_int, [P, C.POINTER(GrbNets)]),
+    "grb_design_zshape_trees": (C.c_int, [P, C.POINTER(P), C.POINTER(P), C.POINTER(P)]),
     "grb_design_subnet_info": (C.c_int, [P, C.POINTER(P), C.POINTER(P), C.POINTER(P)]),
     "grb_design_order": (C.c_int, [P, P]),
     "grb_design_pins": (C.c_int, [P, C.POINTER(P), C.POINTER(P), C.POINTER(C.c_int32)]),

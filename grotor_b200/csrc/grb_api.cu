@@ -2209,11 +2209,15 @@ int grb_zshape_stage(grb_ctx* c, int32_t mode, grb_stats* stats) {
     if (rc) return rc;
     GRB_CUDA(c, cudaEventRecord(c->ev1, c->stream));
     c->stamp = stamp0 + c->n_batches;
-    rc = check_device_error(c);
-    if (rc) return rc;
+    GRB_CUDA(c, cudaEventSynchronize(c->ev1));
     float ms = 0;
     GRB_CUDA(c, cudaEventElapsedTime(&ms, c->ev0, c->ev1));
     c->dag_ms = ms;
+    // As the reference (pipeline_ggr.hpp:136-138), a net without a finite
+    // route or with a segment off the grid is reported after the whole stage
+    // has run; its route record is left empty.
+    rc = check_device_error(c);
+    if (rc) return rc;
     if ((rc = prof_collect(c))) return rc;
     return stats ? grb_get_stats(c, stats) : GRB_OK;
 }

@@ -25,6 +25,8 @@ struct grb_design {
     std::vector<int32_t> node_off, nodes, parents, point_off, points, hseg_off, hsegs, vseg_off, vsegs;
     std::vector<int64_t> route_off;
     std::vector<int32_t> hpwl, original, pin_count;
+    // Z-shape encoding of the same trees (built on request)
+    std::vector<int32_t> z_node_off, z_coord, z_child;
 };
 
 namespace {
@@ -474,6 +476,73 @@ int grb_design_order(const grb_design* d, int32_t* order) {
     const int m = int(d->hpwl.size());
     std::iota(order, order + m, 0);
     std::stable_sort(order, order + m, [&](int a, int b) { return d->hpwl[a] > d->hpwl[b]; });
+    return GRB_OK;
+}
+
+int grb_design_zshape_trees(grb_design* d, const int32_t** node_off, const int32_t** coord, const int32_t** child) {
+    if (!d || d->node_off.empty()) return GRB_EINVAL;
+    if (d->z_node_off.empty()) {
+        const int m = int(d->node_off.size()) - 1;
+        d->z_node_off.assign(1, 0);
+        d->z_coord.reserve(d->nodes.size());
+        d->z_child.reserve(3 * d->nodes.size());
+        std::vector<std::vector<int>> adj, kids;
+        std::vector<int> crd, order, pre, stack;
+        for (int k = 0; k < m; ++k) {
+            const int a = d->node_off[k], n = d->node_off[k + 1] - a;
+            adj.assign(n, {});
+            for (int i = 1; i < n; ++i) {
+                const int p = d->parents[a + i];
+                adj[i].push_back(p);
+                adj[p].push_back(i);
+            }
+            for (auto& v : adj) std::sort(v.begin(), v.end());
+            int root = 0;  // the first leaf, as zshape_topology.hpp:80-82
+            for (int i = 0; i < n; ++i) if (adj[i].size() == 1) { root = i; break; }
+            // Rooted children lists.  A node with more than three children
+            // hands the extra ones to the nearest node of its first child's
+            // subtree that has room (the Z-shape DP keeps one plane cell per
+            // 2-D position, so no two tree nodes may share a position).
+            kids.assign(n, {});
+            crd.assign(n, 0);
+            for (int i = 0; i < n; ++i) crd[i] = d->nodes[a + i];
+            std::vector<int> par(n, -1);
+            stack.assign(1, root);
+            par[root] = root;
+            while (!stack.empty()) {
+                const int v = stack.back(); stack.pop_back();
+                for (int w : adj[v]) if (par[w] == -1) { par[w] = v; kids[v].push_back(w); stack.push_back(w); }
+            }
+            for (int v = 0; v < n; ++v) {
+                while (kids[v].size() > 3) {
+                    const int extra = kids[v].back();
+                    kids[v].pop_back();
+                    std::vector<int> queue{kids[v][0]};
+                    for (size_t h = 0; h < queue.size(); ++h) {
+                        const int w = queue[h];
+                        if (kids[w].size() < 3) { kids[w].push_back(extra); break; }
+                        for (int x : kids[w]) queue.push_back(x);
+                    }
+                }
+            }
+            const int nn = int(kids.size());
+            order.clear(); pre.assign(nn, -1); stack.assign(1, root);
+            while (!stack.empty()) {
+                const int v = stack.back(); stack.pop_back();
+                pre[v] = int(order.size());
+                order.push_back(v);
+                for (auto it = kids[v].rbegin(); it != kids[v].rend(); ++it) stack.push_back(*it);
+            }
+            for (int v : order) {
+                d->z_coord.push_back(crd[v]);
+                for (int j = 0; j < 3; ++j) d->z_child.push_back(j < int(kids[v].size()) ? pre[kids[v][j]] : -1);
+            }
+            d->z_node_off.push_back(int32_t(d->z_coord.size()));
+        }
+    }
+    if (node_off) *node_off = d->z_node_off.data();
+    if (coord) *coord = d->z_coord.data();
+    if (child) *child = d->z_child.data();
     return GRB_OK;
 }
 

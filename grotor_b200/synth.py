@@ -111,6 +111,15 @@ class Design:
     def n_subnets(self) -> int:
         return self.nets.n
 
+    def zshape_trees(self) -> dict:
+        """The same trees in the Z-shape encoding (upload with Router.upload_zshape)."""
+        off, crd, ch = C.c_void_p(), C.c_void_p(), C.c_void_p()
+        if self._lib.grb_design_zshape_trees(self._d, C.byref(off), C.byref(crd), C.byref(ch)):
+            raise ValueError(self._lib.grb_design_error(self._d).decode())
+        m = self.nets.n
+        o = _arr(off, C.c_int32, m + 1).copy()
+        return {"node_off": o, "coord": _arr(crd, C.c_int32, o[-1]).copy(), "child": _arr(ch, C.c_int32, 3 * o[-1]).copy()}
+
     def pins(self):
         off, pins, n = C.c_void_p(), C.c_void_p(), C.c_int32()
         self._lib.grb_design_pins(self._d, C.byref(off), C.byref(pins), C.byref(n))

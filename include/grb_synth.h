@@ -57,6 +57,11 @@ int grb_design_write(const grb_design* d, const char* cap_path, const char* net_
 int grb_design_build_topology(grb_design* d, int32_t max_subnet_pins, int32_t threads);
 /* Topology arrays (owned by the design, valid until the next build or free). */
 int grb_design_nets(const grb_design* d, grb_nets* out);
+/* The same trees in the Z-shape encoding (grb_zshape_trees): preorder from
+ * each tree's first leaf, children in ascending node order; a node with more
+ * than three children hands the extra ones to the nearest node with room in
+ * its first child's subtree (built on the first call; owned by the design). */
+int grb_design_zshape_trees(grb_design* d, const int32_t** node_off, const int32_t** coord, const int32_t** child);
 /* Per-subnet HPWL, original net id and pin count (arrays of n entries). */
 int grb_design_subnet_info(const grb_design* d, const int32_t** hpwl, const int32_t** original,
                            const int32_t** pin_count);

@@ -69,3 +69,55 @@ def test_zshape_stage_equals_reference(name, mode):
     if "pin_vias" in g:
         assert st["vias"] == int(g["z_stats"][1])
     r.close()
+
+
+def test_zshape_synthetic_design_equals_oracle():
+    """On a seeded 320x320x10 design (trees from the workload generator): GPU
+    first-fit + bounding-box batches equal the oracle's refinement of the
+    same groups, and the Z-shape stage's routes, demand and statistics equal
+    the oracle's."""
+    import oracle
+    from grotor_b200 import Router
+    from grotor_b200.router import NetArrays
+    from grotor_b200.synth import WORKLOADS, Design
+    from helpers import orc_grid
+    d = Design(WORKLOADS["medium_320x320x10"].scaled(6000, seed=47))
+    z = d.zshape_trees()
+    n = d.nets
+    zn = np.diff(z["node_off"]).astype(np.int64)
+    route_off = np.concatenate([[0], np.cumsum(1 + 64 * zn)]).astype(np.int64)
+    nets = NetArrays(n.node_off, n.nodes, n.parents, route_off, n.point_off, n.points, n.hseg_off, n.hsegs,
+                     n.vseg_off, n.vsegs)
+    r = Router(d.grid)
+    r.upload_nets(nets)
+    r.upload_zshape(z)
+    r.set_wire_cost_mode(True)
+    r.generate_batches_rsmt(d.order, 1000000)
+    gids, goff = r.plan()
+    # oracle refinement of the same groups (execution order: groups reversed)
+    bbox = np.zeros((n.n, 4), np.int32)
+    for i in range(n.n):
+        c = z["coord"][z["node_off"][i]:z["node_off"][i + 1]] % (d.grid.X * d.grid.Y)
+        xs, ys = c // d.grid.Y, c % d.grid.Y
+        bbox[i] = (xs.min(), xs.max(), ys.min(), ys.max())
+    groups = [gids[goff[k]:goff[k + 1]] for k in range(len(goff) - 1)][::-1]
+    ref = []
+    for grp in groups:
+        ref += oracle.bbox_batches(d.grid.X, d.grid.Y, grp, bbox.reshape(-1))
+    ref = ref[::-1]
+    nb = r.plan_bbox_batches(250)
+    ids, off = r.plan()
+    assert nb == len(ref)
+    np.testing.assert_array_equal(ids, np.concatenate([np.asarray(b, np.int32) for b in ref]))
+    og = orc_grid(d.grid)
+    og2 = oracle.OrcGrid(og.L, og.X, og.Y, og.DIR, og.unit_wire, og.unit_via, og.short_costs, og.x_edge_len,
+                         og.y_edge_len, og.capacity, og.of_cost_scale, integer_wire=True)
+    out = oracle.zshape_stage(og2, z, ids, off, route_off)
+    assert out["status"] == 0
+    for mode in ("persistent", "plain"):
+        r.reset()
+        st = r.zshape_route(mode)
+        np.testing.assert_array_equal(r.read_routes(), out["routes"])
+        np.testing.assert_array_equal(r.read_tables()["demand_half"], out["demand_half"])
+        assert st["wirelength"] == out["wirelength"] and st["vias"] == out["vias"]
+    r.close()
