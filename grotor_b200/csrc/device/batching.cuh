@@ -44,8 +44,8 @@ struct BatchState {
     unsigned* cellmask;    // [X*Y][W]
     unsigned* localmask;   // [X*Y][kChunkWords], chunks of even index
     unsigned* localmask2;  // [X*Y][kChunkWords], chunks of odd index
-    unsigned* fmask;       // [kChunk][W]
-    unsigned* pred;        // [kChunk][kChunkWords]
+    unsigned* fmask;       // [W][kChunk] (word-major: the solve copies it as is)
+    unsigned* pred;        // [kChunkWords][kChunk]
     unsigned* fullmask;    // [W]
     int* count;            // [32*W]
     int* n_colors;         // [1]
@@ -147,11 +147,11 @@ __device__ __forceinline__ void batch_forbid_preds(const BatchState& B, int s, i
         if (v) atomicOr(acc + W + w, v);
     }
     G.sync();
-    for (int w = t; w < W; w += n) B.fmask[size_t(jj) * W + w] = acc[w];
+    for (int w = t; w < W; w += n) B.fmask[size_t(w) * kChunk + jj] = acc[w];
     for (int w = t; w < kChunkWords; w += n) {
         unsigned v = w < words ? acc[W + w] : 0u;
         if (w == (jj >> 5)) v &= (1u << (jj & 31)) - 1u;
-        B.pred[jj * kChunkWords + w] = v;
+        B.pred[w * kChunk + jj] = v;
     }
     G.sync();
 }
@@ -185,8 +185,18 @@ __device__ void batch_phase3(const BatchState& B, int s, unsigned* smem) {
     int* run = cnt + C;
     unsigned* full = reinterpret_cast<unsigned*>(run + C);
     __shared__ int first_bad, overflow;
-    for (int k = tid; k < m * W; k += blockDim.x) F[(k % W) * kChunk + k / W] = B.fmask[k];
-    for (int k = tid; k < m * kChunkWords; k += blockDim.x) P[(k % kChunkWords) * kChunk + k / kChunkWords] = B.pred[k];
+    // Both tables are word-major in global memory already: 16-byte copies.
+    {
+        const uint4* f4 = reinterpret_cast<const uint4*>(B.fmask);
+        const uint4* p4 = reinterpret_cast<const uint4*>(B.pred);
+        uint4* F4 = reinterpret_cast<uint4*>(F);
+        uint4* P4 = reinterpret_cast<uint4*>(P);
+        const int nf = W * kChunk / 4, np = kChunkWords * kChunk / 4;
+        for (int k = tid; k < nf + np; k += blockDim.x) {
+            if (k < nf) F4[k] = f4[k];
+            else P4[k - nf] = p4[k - nf];
+        }
+    }
     for (int k = tid; k < C; k += blockDim.x) cnt[k] = B.count[k];
     for (int k = tid; k < W; k += blockDim.x) full[k] = B.fullmask[k];
     if (tid < kChunk) col[tid] = -1;

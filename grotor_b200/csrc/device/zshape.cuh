@@ -15,9 +15,10 @@
 //
 // B200 form: one warp per net (as the reference); the nets of a batch have
 // disjoint bounding boxes, so their plane cells never overlap.  Lanes split
-// each row/column relaxation and the via sweeps; the node DP and the
-// traceback run on lane 0 in the reference's order.  The traceback converts
-// each segment straight into route words (convert_routes).
+// each row/column relaxation, the via sweeps and the node DP; the traceback
+// runs on lane 0 in the reference's order.  The traceback converts
+// each segment straight into route words (convert_routes).  The node DP is
+// split across lanes (one lane per lower layer, then one per layer).
 #pragma once
 #include "commit.cuh"
 #include "common.cuh"
@@ -211,34 +212,51 @@ __device__ __forceinline__ void zedge(const Tables& T, const ZTrees& Z, int j, i
     __syncwarp();
 }
 
-// Layer-range DP of one node (zshape.cuh:241-267), lane 0.
-__device__ __forceinline__ void znode_dp(const Tables& T, const ZTrees& Z, int tox, int toy, int pin,
-                                         const int* ch) {
+// Layer-range DP of one node (zshape.cuh:241-267) with the warp: lane
+// `lower` walks its uppers (the
+// child and via values of every layer come by shuffle) and writes each
+// range's value and code to shared memory `cand` (2 * LAYER * LAYER ints);
+// then lane i takes, over the allowed ranges containing layer i in the
+// sequential (lower, upper) order, the first strict minimum -- exactly the
+// value and code the sequential loop leaves at layer i.
+__device__ __forceinline__ void znode_dp_warp(const Tables& T, const ZTrees& Z, int tox, int toy, int pin,
+                                              const int* ch, int lane, int* cand) {
     const int LAYER = Z.LAYER;
-    int* map0 = Z.map;
-    int* prev0 = Z.prev;
-    for (int lower = 0; lower < LAYER; ++lower) {
-        int viaSum = 0, minCost = kZInf, bestpos[3] = {0, 0, 0};
-        int costs[3] = {ch[0] == -1 ? 0 : kZInf, ch[1] == -1 ? 0 : kZInf, ch[2] == -1 ? 0 : kZInf};
-        for (int upper = lower; upper < LAYER; ++upper) {
-            const int idx = zidx(Z, upper, tox, toy);
-            for (int j = 0; j < 3; ++j) {
-                if (ch[j] == -1) continue;
-                const int v = Z.map[(j + 1) * Z.LNN + idx];
-                if (v < costs[j]) { costs[j] = v; bestpos[j] = upper; }
-            }
-            if (1LL * costs[0] + costs[1] + costs[2] < minCost) minCost = costs[0] + costs[1] + costs[2];
-            if (pin == -1 || (lower <= pin && pin <= upper)) {
-                const int v = zadd(minCost, viaSum);
-                const int code = (((lower * LAYER + upper) * LAYER + bestpos[2]) * LAYER + bestpos[1]) * LAYER + bestpos[0];
-                for (int i = lower; i <= upper; ++i) {
-                    const int index = zidx(Z, i, tox, toy);
-                    if (map0[index] > v) { map0[index] = v; prev0[index] = code; }
-                }
-            }
-            viaSum = zadd(viaSum, zvia(T, Z, idx));
-        }
+    const int idx_l = lane < LAYER ? zidx(Z, lane, tox, toy) : 0;
+    int pv[3];
+    for (int j = 0; j < 3; ++j) pv[j] = (lane < LAYER && ch[j] != -1) ? Z.map[(j + 1) * Z.LNN + idx_l] : 0;
+    const int vc = lane < LAYER ? zvia(T, Z, idx_l) : 0;
+    const int lower = lane;
+    int viaSum = 0, minCost = kZInf, bestpos[3] = {0, 0, 0};
+    int costs[3] = {ch[0] == -1 ? 0 : kZInf, ch[1] == -1 ? 0 : kZInf, ch[2] == -1 ? 0 : kZInf};
+    for (int upper = 0; upper < LAYER; ++upper) {
+        int v[3];
+        for (int j = 0; j < 3; ++j) v[j] = __shfl_sync(0xffffffffu, pv[j], upper);
+        const int vu = __shfl_sync(0xffffffffu, vc, upper);
+        if (lower >= LAYER || upper < lower) continue;
+        for (int j = 0; j < 3; ++j)
+            if (ch[j] != -1 && v[j] < costs[j]) { costs[j] = v[j]; bestpos[j] = upper; }
+        if (1LL * costs[0] + costs[1] + costs[2] < minCost) minCost = costs[0] + costs[1] + costs[2];
+        const bool allowed = pin == -1 || (lower <= pin && pin <= upper);
+        cand[lower * LAYER + upper] = zadd(minCost, viaSum);
+        cand[LAYER * LAYER + lower * LAYER + upper] =
+            allowed ? (((lower * LAYER + upper) * LAYER + bestpos[2]) * LAYER + bestpos[1]) * LAYER + bestpos[0] : -1;
+        viaSum = zadd(viaSum, vu);
     }
+    __syncwarp();
+    if (lane < LAYER) {
+        const int i = lane;
+        int best = Z.map[idx_l], code = Z.prev[idx_l];
+        bool changed = false;
+        for (int lo = 0; lo <= i; ++lo)
+            for (int up = i; up < LAYER; ++up) {
+                const int c = cand[LAYER * LAYER + lo * LAYER + up];
+                const int val = cand[lo * LAYER + up];
+                if (c >= 0 && best > val) { best = val; code = c; changed = true; }
+            }
+        if (changed) { Z.map[idx_l] = best; Z.prev[idx_l] = code; }
+    }
+    __syncwarp();
 }
 
 // convert_routes (zshape_topology.hpp:249-290) of one (start, length | -1)
@@ -328,8 +346,9 @@ __device__ __forceinline__ int ztrace(const Tables& T, const ZTrees& Z, int nb, 
 }
 
 // Route net `id` with one warp; with `commit`, also its wire demand.
+// `cand`: the calling warp's 2 * LAYER * LAYER ints of shared memory.
 __device__ __forceinline__ void zshape_net(const Tables& T, const ZTrees& Z, const Plan& P, int id, int stamp,
-                                           int lane, bool commit) {
+                                           int lane, bool commit, int* cand) {
     const int nb = Z.node_off[id], cnt = Z.node_off[id + 1] - nb;
     int* r = P.routes + P.route_off[id];
     const long long cap = P.route_off[id + 1] - P.route_off[id];
@@ -353,8 +372,7 @@ __device__ __forceinline__ void zshape_net(const Tables& T, const ZTrees& Z, con
             const int cp = Z.pos[nb + c];
             zedge(T, Z, j, cp / Z.N, cp % Z.N, tox, toy, lane);
         }
-        if (lane == 0) znode_dp(T, Z, tox, toy, Z.pin[nb + t], ch);
-        __syncwarp();
+        znode_dp_warp(T, Z, tox, toy, Z.pin[nb + t], ch, lane, cand);
     }
     int status = 0;
     if (lane == 0) {

@@ -307,11 +307,13 @@ constexpr int kMaxBoxBatch = 256;
 
 // One warp per net of batch b (solve<4>, zshape.cuh:62-388, with the route
 // conversion of convert_routes fused into the traceback).
+constexpr int kZCand = 2 * (kMaxLayers + 1) * (kMaxLayers + 1);  // node-DP ranges per warp
 __global__ void __launch_bounds__(kZThreads) k_zshape_batch(Tables T, ZTrees Z, Plan P, int b) {
+    __shared__ int cand[kZThreads / 32][kZCand];
     const int lane = threadIdx.x & 31;
     const int k = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lo = P.batch_off[b], cnt = P.batch_off[b + 1] - lo;
-    if (k < cnt) zshape_net(T, Z, P, P.ids[lo + k], 0, lane, false);
+    if (k < cnt) zshape_net(T, Z, P, P.ids[lo + k], 0, lane, false, cand[threadIdx.x >> 5]);
 }
 // Thread-per-net commit (commit_wire_demand / commit_via_demand,
 // demand.cuh:129-232), the Z-shape pipeline's form (pipeline_ggr.hpp:132-133).
@@ -334,6 +336,7 @@ __global__ void __launch_bounds__(kPersistentThreads, 2) k_zshape_persistent(Tab
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int gwarp = warp * gridDim.x + blockIdx.x, nwarps = gridDim.x * (blockDim.x >> 5);
     double* tree = reinterpret_cast<double*>(smem);
+    __shared__ int cand[kPersistentThreads / 32][kZCand];
     PhaseClock clk;
     clk.start(S);
     for (int b = 0; b < P.n_batches; ++b) {
@@ -363,7 +366,7 @@ __global__ void __launch_bounds__(kPersistentThreads, 2) k_zshape_persistent(Tab
             if (lane == 0) k = atomicAdd(work + b, 1);
             k = __shfl_sync(0xffffffffu, k, 0);
             if (k >= cnt) break;
-            zshape_net(T, Z, P, P.ids[lo + k], stamp, lane, true);
+            zshape_net(T, Z, P, P.ids[lo + k], stamp, lane, true, cand[warp]);
         }
         if (!grid_sync(S, T)) return;
         clk.mark(S, 5);
