@@ -13,12 +13,13 @@
 // at i*N*N + (y*N + x) otherwise, D = DIR ^ 1; GGR layer i is routing layer
 // i-1 (layer 0 carries no wires and costs an infinite via).
 //
-// B200 form: one warp per net (as the reference); the nets of a batch have
-// disjoint bounding boxes, so their plane cells never overlap.  Lanes split
-// each row/column relaxation, the via sweeps and the node DP; the traceback
-// runs on lane 0 in the reference's order.  The traceback converts
-// each segment straight into route words (convert_routes).  The node DP is
-// split across lanes (one lane per lower layer, then one per layer).
+// B200 form: one CTA per net (the reference uses one warp); a bounding-box
+// batch holds at most 250 nets, so a whole CTA per net keeps the GPU busy and
+// splits a long edge's row/column relaxations and via sweeps over all its
+// threads.  The nets of a batch have disjoint bounding boxes, so their plane
+// cells never overlap.  Warp 0 runs the node DP (one lane per lower layer,
+// then one per layer); thread 0 runs the traceback in the reference's order
+// and converts each segment straight into route words (convert_routes).
 #pragma once
 #include "commit.cuh"
 #include "common.cuh"
@@ -89,7 +90,7 @@ __device__ __forceinline__ void zvia_sweep(const Tables& T, const ZTrees& Z, int
 // Child slot j (1..3) of node (tox, toy): fill plane j at the node from the
 // child at (fromx, fromy) (zshape.cuh:87-237).
 __device__ __forceinline__ void zedge(const Tables& T, const ZTrees& Z, int j, int fromx, int fromy, int tox, int toy,
-                                      int lane) {
+                                      int lane, int nth) {
     const int LAYER = Z.LAYER, D = Z.D;
     const long long NN = Z.NN;
     int* map0 = Z.map;
@@ -102,22 +103,22 @@ __device__ __forceinline__ void zedge(const Tables& T, const ZTrees& Z, int j, i
     const int minx = min(fromx, tox), maxx = max(fromx, tox), miny = min(fromy, toy), maxy = max(fromy, toy);
     if (fromx != tox && fromy != toy) {
         // Clear the candidate rows and columns of the edge's box.
-        for (int a = minx + lane; a <= maxx; a += 32)
+        for (int a = minx + lane; a <= maxx; a += nth)
             for (int i = 1; i < LAYER; ++i) {
                 if ((i & 1) ^ D) { m4[i * NN + a * Z.N + toy] = kZInf; m4[i * NN + a * Z.N + fromy] = kZInf; }
                 else { m4[i * NN + toy * Z.N + a] = kZInf; m4[i * NN + fromy * Z.N + a] = kZInf; }
             }
-        for (int b = miny + lane; b <= maxy; b += 32)
+        for (int b = miny + lane; b <= maxy; b += nth)
             for (int i = 1; i < LAYER; ++i) {
                 if ((i & 1) ^ D) { m4[i * NN + tox * Z.N + b] = kZInf; m4[i * NN + fromx * Z.N + b] = kZInf; }
                 else { m4[i * NN + b * Z.N + tox] = kZInf; m4[i * NN + b * Z.N + fromx] = kZInf; }
             }
-        __syncwarp();
+        __syncthreads();
         // Straight runs out of the child along each layer's direction.
         for (int i = 1; i < LAYER; ++i) {
             if ((i & 1) ^ D) {
                 const int last = static_cast<int>(i * NN + fromx * Z.N + fromy);
-                for (int b = miny + lane; b <= maxy; b += 32) {
+                for (int b = miny + lane; b <= maxy; b += nth) {
                     if (b == fromy) continue;
                     const int cur = static_cast<int>(i * NN + fromx * Z.N + b);
                     m4[cur] = zadd(map0[last], zwire(T, Z, last, cur));
@@ -125,7 +126,7 @@ __device__ __forceinline__ void zedge(const Tables& T, const ZTrees& Z, int j, i
                 }
             } else {
                 const int last = static_cast<int>(i * NN + fromy * Z.N + fromx);
-                for (int b = minx + lane; b <= maxx; b += 32) {
+                for (int b = minx + lane; b <= maxx; b += nth) {
                     if (b == fromx) continue;
                     const int cur = static_cast<int>(i * NN + fromy * Z.N + b);
                     m4[cur] = zadd(map0[last], zwire(T, Z, last, cur));
@@ -133,43 +134,43 @@ __device__ __forceinline__ void zedge(const Tables& T, const ZTrees& Z, int j, i
                 }
             }
         }
-        __syncwarp();
+        __syncthreads();
         // Layer changes on the child's column and row (distinct positions).
         {
             const int ncol = maxy - miny + 1;
-            for (int k = lane; k < ncol + (maxx - minx + 1); k += 32) {
+            for (int k = lane; k < ncol + (maxx - minx + 1); k += nth) {
                 if (k < ncol) { const int b = miny + k; if (b != fromy) zvia_sweep(T, Z, fromx, b); }
                 else { const int b = minx + (k - ncol); if (b != fromx) zvia_sweep(T, Z, b, fromy); }
             }
         }
-        __syncwarp();
+        __syncthreads();
         // Cross the box to the node's row / column.
         for (int i = 1; i < LAYER; ++i) {
             if ((i & 1) ^ D) {
-                for (int b = minx + lane; b <= maxx; b += 32) {
+                for (int b = minx + lane; b <= maxx; b += nth) {
                     const int last = static_cast<int>(i * NN + b * Z.N + fromy), cur = static_cast<int>(i * NN + b * Z.N + toy);
                     const int v = zadd(m4[last], zwire(T, Z, last, cur));
                     if (v < m4[cur]) { m4[cur] = v; p4[cur] = p4[last]; }
                 }
             } else {
-                for (int b = miny + lane; b <= maxy; b += 32) {
+                for (int b = miny + lane; b <= maxy; b += nth) {
                     const int last = static_cast<int>(i * NN + b * Z.N + fromx), cur = static_cast<int>(i * NN + b * Z.N + tox);
                     const int v = zadd(m4[last], zwire(T, Z, last, cur));
                     if (v < m4[cur]) { m4[cur] = v; p4[cur] = p4[last]; }
                 }
             }
         }
-        __syncwarp();
+        __syncthreads();
         {
             const int ncol = maxy - miny + 1;
-            for (int k = lane; k < ncol + (maxx - minx + 1); k += 32) {
+            for (int k = lane; k < ncol + (maxx - minx + 1); k += nth) {
                 if (k < ncol) { const int b = miny + k; if (b != toy) zvia_sweep(T, Z, tox, b); }
                 else { const int b = minx + (k - ncol); if (b != tox) zvia_sweep(T, Z, b, toy); }
             }
         }
-        __syncwarp();
+        __syncthreads();
         // Last run into the node, one lane per layer, positions in order.
-        for (int i = 1 + lane; i < LAYER; i += 32) {
+        for (int i = 1 + lane; i < LAYER; i += nth) {
             if ((i & 1) ^ D) {
                 const int cur = static_cast<int>(i * NN + tox * Z.N + toy);
                 for (int b = miny; b <= maxy; ++b) {
@@ -189,7 +190,7 @@ __device__ __forceinline__ void zedge(const Tables& T, const ZTrees& Z, int j, i
             }
         }
     } else if (fromx == tox) {
-        for (int i = 1 + lane; i < LAYER; i += 32) {
+        for (int i = 1 + lane; i < LAYER; i += nth) {
             if ((i & 1) ^ D) {
                 const int last = static_cast<int>(i * NN + fromx * Z.N + fromy), cur = static_cast<int>(i * NN + tox * Z.N + toy);
                 const int v = zadd(map0[last], zwire(T, Z, last, cur));
@@ -199,7 +200,7 @@ __device__ __forceinline__ void zedge(const Tables& T, const ZTrees& Z, int j, i
             }
         }
     } else {  // fromy == toy
-        for (int i = 1 + lane; i < LAYER; i += 32) {
+        for (int i = 1 + lane; i < LAYER; i += nth) {
             if ((!(i & 1)) ^ D) {
                 const int last = static_cast<int>(i * NN + fromy * Z.N + fromx), cur = static_cast<int>(i * NN + toy * Z.N + tox);
                 const int v = zadd(map0[last], zwire(T, Z, last, cur));
@@ -209,7 +210,7 @@ __device__ __forceinline__ void zedge(const Tables& T, const ZTrees& Z, int j, i
             }
         }
     }
-    __syncwarp();
+    __syncthreads();
 }
 
 // Layer-range DP of one node (zshape.cuh:241-267) with the warp: lane
@@ -346,42 +347,46 @@ __device__ __forceinline__ int ztrace(const Tables& T, const ZTrees& Z, int nb, 
 }
 
 // Route net `id` with one warp; with `commit`, also its wire demand.
-// `cand`: the calling warp's 2 * LAYER * LAYER ints of shared memory.
+// Route net `id` with the whole CTA (thread t of nth); with `commit`, also its
+// wire demand (warp 0).  `cand`: 2 * LAYER * LAYER ints of shared memory.
 __device__ __forceinline__ void zshape_net(const Tables& T, const ZTrees& Z, const Plan& P, int id, int stamp,
-                                           int lane, bool commit, int* cand) {
+                                           int t, int nth, bool commit, int* cand) {
+    __shared__ int zstatus;
+    const int lane = t;
     const int nb = Z.node_off[id], cnt = Z.node_off[id + 1] - nb;
     int* r = P.routes + P.route_off[id];
     const long long cap = P.route_off[id + 1] - P.route_off[id];
     if (cnt <= 0) {
-        if (lane == 0 && cap > 0) r[0] = 1;
+        if (t == 0 && cap > 0) r[0] = 1;
         return;
     }
     // reset_nodes (zshape.cuh:392-404).
-    for (int k = lane; k < cnt * Z.LAYER; k += 32) {
+    for (int k = t; k < cnt * Z.LAYER; k += nth) {
         const int pt = Z.pos[nb + k / Z.LAYER];
         const int idx = zidx(Z, k % Z.LAYER, pt / Z.N, pt % Z.N);
         for (int plane = 0; plane < 4; ++plane) Z.map[plane * Z.LNN + idx] = kZInf;
     }
-    __syncwarp();
-    for (int t = cnt - 1; t >= 0; --t) {
-        const int pt = Z.pos[nb + t], tox = pt / Z.N, toy = pt % Z.N;
-        const int* ch = Z.child + 3 * (nb + t);
+    __syncthreads();
+    for (int v = cnt - 1; v >= 0; --v) {
+        const int pt = Z.pos[nb + v], tox = pt / Z.N, toy = pt % Z.N;
+        const int* ch = Z.child + 3 * (nb + v);
         for (int j = 1; j <= 3; ++j) {
             const int c = ch[j - 1];
             if (c == -1) continue;
             const int cp = Z.pos[nb + c];
-            zedge(T, Z, j, cp / Z.N, cp % Z.N, tox, toy, lane);
+            zedge(T, Z, j, cp / Z.N, cp % Z.N, tox, toy, lane, nth);
         }
-        znode_dp_warp(T, Z, tox, toy, Z.pin[nb + t], ch, lane, cand);
+        if (t < 32) znode_dp_warp(T, Z, tox, toy, Z.pin[nb + v], ch, lane, cand);
+        __syncthreads();
     }
-    int status = 0;
-    if (lane == 0) {
-        status = ztrace(T, Z, nb, cnt, r, cap);
-        if (status) set_error(T, status == 1 ? kELimit : kEInval, id);
+    if (t == 0) {
+        zstatus = ztrace(T, Z, nb, cnt, r, cap);
+        if (zstatus) set_error(T, zstatus == 1 ? kELimit : kEInval, id);
     }
-    status = __shfl_sync(0xffffffffu, status, 0);
-    __syncwarp();
-    if (commit && !status) commit_net_wires(T, P, id, stamp, 1, lane);
+    __syncthreads();
+    const int status = zstatus;
+    if (commit && !status && t < 32) commit_net_wires(T, P, id, stamp, 1, lane);
+    __syncthreads();
 }
 
 // --- bounding-box batch refinement (zshape_topology.hpp:7-57) --------------

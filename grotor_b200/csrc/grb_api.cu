@@ -301,19 +301,17 @@ __global__ void __launch_bounds__(kPersistentThreads, 2) k_flt_persistent(Tables
 }
 
 // --- Z-shape stage kernels (zshape.cuh) -------------------------------------
-constexpr int kZThreads = 128;
+constexpr int kZThreads = 256;
 constexpr int kBoxThreads = 256;
 constexpr int kMaxBoxBatch = 256;
 
-// One warp per net of batch b (solve<4>, zshape.cuh:62-388, with the route
-// conversion of convert_routes fused into the traceback).
 constexpr int kZCand = 2 * (kMaxLayers + 1) * (kMaxLayers + 1);  // node-DP ranges per warp
+// One CTA per net of batch b (solve<4>, zshape.cuh:62-388, with the route
+// conversion of convert_routes fused into the traceback).
 __global__ void __launch_bounds__(kZThreads) k_zshape_batch(Tables T, ZTrees Z, Plan P, int b) {
-    __shared__ int cand[kZThreads / 32][kZCand];
-    const int lane = threadIdx.x & 31;
-    const int k = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int lo = P.batch_off[b], cnt = P.batch_off[b + 1] - lo;
-    if (k < cnt) zshape_net(T, Z, P, P.ids[lo + k], 0, lane, false, cand[threadIdx.x >> 5]);
+    __shared__ int cand[kZCand];
+    const int lo = P.batch_off[b];
+    zshape_net(T, Z, P, P.ids[lo + blockIdx.x], 0, threadIdx.x, blockDim.x, false, cand);
 }
 // Thread-per-net commit (commit_wire_demand / commit_via_demand,
 // demand.cuh:129-232), the Z-shape pipeline's form (pipeline_ggr.hpp:132-133).
@@ -336,7 +334,8 @@ __global__ void __launch_bounds__(kPersistentThreads, 2) k_zshape_persistent(Tab
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int gwarp = warp * gridDim.x + blockIdx.x, nwarps = gridDim.x * (blockDim.x >> 5);
     double* tree = reinterpret_cast<double*>(smem);
-    __shared__ int cand[kPersistentThreads / 32][kZCand];
+    __shared__ int cand[kZCand];
+    __shared__ int znet;
     PhaseClock clk;
     clk.start(S);
     for (int b = 0; b < P.n_batches; ++b) {
@@ -361,12 +360,13 @@ __global__ void __launch_bounds__(kPersistentThreads, 2) k_zshape_persistent(Tab
         }
         if (!grid_sync(S, T)) return;
         clk.mark(S, 7);
-        while (true) {
-            int k = 0;
-            if (lane == 0) k = atomicAdd(work + b, 1);
-            k = __shfl_sync(0xffffffffu, k, 0);
+        while (true) {  // one CTA per net
+            if (threadIdx.x == 0) znet = atomicAdd(work + b, 1);
+            __syncthreads();
+            const int k = znet;
+            __syncthreads();
             if (k >= cnt) break;
-            zshape_net(T, Z, P, P.ids[lo + k], stamp, lane, true, cand[warp]);
+            zshape_net(T, Z, P, P.ids[lo + k], stamp, threadIdx.x, blockDim.x, true, cand);
         }
         if (!grid_sync(S, T)) return;
         clk.mark(S, 5);
@@ -1090,7 +1090,7 @@ int z_stage_plain(grb_ctx* c, int stamp0) {
         if ((rc = refresh_plain(c))) return rc;
         cudaEvent_t e;
         if ((rc = prof_begin(c, 5, &e))) return rc;
-        k_zshape_batch<<<(cnt + kZThreads / 32 - 1) / (kZThreads / 32), kZThreads, 0, c->stream>>>(c->T, c->Z, P, b);
+        k_zshape_batch<<<cnt, kZThreads, 0, c->stream>>>(c->T, c->Z, P, b);
         prof_end(c, e);
         if ((rc = prof_begin(c, 6, &e))) return rc;
         k_commit_thread_wires<<<(cnt + 255) / 256, 256, 0, c->stream>>>(c->T, P, b, stamp);
