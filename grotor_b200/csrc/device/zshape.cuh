@@ -66,24 +66,47 @@ __device__ __forceinline__ int zwire(const Tables& T, const ZTrees& Z, int a, in
     return static_cast<int>(fmin(fabs(zsum(T, Z, a) - zsum(T, Z, b)), static_cast<double>(kZInf / 2)));
 }
 
-// viaSweep (zshape.cuh:42-61) on plane 4 at 2-D position (x, y): up, then down.
-__device__ __forceinline__ void zvia_sweep(const Tables& T, const ZTrees& Z, int x, int y) {
+// viaSweep (zshape.cuh:42-61) on plane 4 at 2-D position (x, y): up, then
+// down.  The position's layer column is loaded into registers first, so the
+// two dependent chains run without a memory round trip per layer.
+__device__ __noinline__ void zvia_sweep(const Tables& T, const ZTrees& Z, int x, int y) {
+    constexpr int K = kMaxLayers + 1;
     int* m = Z.map + 4 * Z.LNN;
     int* p = Z.prev + 4 * Z.LNN;
     int* p5 = Z.prev + 5 * Z.LNN;
-    for (int i = 1; i < Z.LAYER; ++i) {
-        const int cur = zidx(Z, i, x, y);
-        p5[cur] = cur;
+    int mv[K], pv[K], vc[K], q[K];  // q: layer of the cell the value came from
+#pragma unroll
+    for (int i = 1; i < K; ++i) {
+        if (i < Z.LAYER) {
+            const int c = zidx(Z, i, x, y);
+            mv[i] = m[c];
+            pv[i] = p[c];
+            vc[i] = zvia(T, Z, c);
+            q[i] = i;
+        }
     }
-    for (int i = 2; i < Z.LAYER; ++i) {
-        const int cur = zidx(Z, i, x, y), last = zidx(Z, i - 1, x, y);
-        const int v = zadd(m[last], zvia(T, Z, last));
-        if (m[cur] > v) { m[cur] = v; p[cur] = p[last]; p5[cur] = last; }
+#pragma unroll
+    for (int i = 2; i < K; ++i) {
+        if (i < Z.LAYER) {
+            const int v = zadd(mv[i - 1], vc[i - 1]);
+            if (mv[i] > v) { mv[i] = v; pv[i] = pv[i - 1]; q[i] = i - 1; }
+        }
     }
-    for (int i = Z.LAYER - 2; i >= 1; --i) {
-        const int cur = zidx(Z, i, x, y), last = zidx(Z, i + 1, x, y);
-        const int v = zadd(m[last], zvia(T, Z, cur));
-        if (m[cur] > v) { m[cur] = v; p[cur] = p[last]; p5[cur] = last; }
+#pragma unroll
+    for (int i = K - 2; i >= 1; --i) {
+        if (i <= Z.LAYER - 2) {
+            const int v = zadd(mv[i + 1], vc[i]);
+            if (mv[i] > v) { mv[i] = v; pv[i] = pv[i + 1]; q[i] = i + 1; }
+        }
+    }
+#pragma unroll
+    for (int i = 1; i < K; ++i) {
+        if (i < Z.LAYER) {
+            const int c = zidx(Z, i, x, y);
+            m[c] = mv[i];
+            p[c] = pv[i];
+            p5[c] = zidx(Z, q[i], x, y);
+        }
     }
 }
 
@@ -169,25 +192,39 @@ __device__ __forceinline__ void zedge(const Tables& T, const ZTrees& Z, int j, i
             }
         }
         __syncthreads();
-        // Last run into the node, one lane per layer, positions in order.
-        for (int i = 1 + lane; i < LAYER; i += nth) {
-            if ((i & 1) ^ D) {
-                const int cur = static_cast<int>(i * NN + tox * Z.N + toy);
-                for (int b = miny; b <= maxy; ++b) {
-                    if (b == toy) continue;
-                    const int last = static_cast<int>(i * NN + tox * Z.N + b);
-                    const int v = zadd(m4[last], zwire(T, Z, last, cur));
-                    if (v < mj[cur]) { mj[cur] = v; pj[cur] = p4[last]; p2j[cur] = p5[last]; }
+        // Last run into the node: per layer, the first minimum over the
+        // positions of the node's row/column (the reference scans them in
+        // order keeping strict improvements), found by a block reduction of
+        // (value, position) pairs.
+        __shared__ int red_v[32], red_b[32];
+        for (int i = 1; i < LAYER; ++i) {
+            const bool ay = ((i & 1) ^ D) != 0;
+            const int cur = static_cast<int>(ay ? i * NN + tox * Z.N + toy : i * NN + toy * Z.N + tox);
+            const int lo = ay ? miny : minx, hi = ay ? maxy : maxx, skip = ay ? toy : tox;
+            int bv = 0, bb = -1;
+            for (int b = lo + lane; b <= hi; b += nth) {
+                if (b == skip) continue;
+                const int last = static_cast<int>(ay ? i * NN + tox * Z.N + b : i * NN + toy * Z.N + b);
+                const int v = zadd(m4[last], zwire(T, Z, last, cur));
+                if (bb < 0 || v < bv) { bv = v; bb = b; }
+            }
+            for (int o = 16; o; o >>= 1) {
+                const int ov = __shfl_down_sync(0xffffffffu, bv, o), ob = __shfl_down_sync(0xffffffffu, bb, o);
+                if (ob >= 0 && (bb < 0 || ov < bv || (ov == bv && ob < bb))) { bv = ov; bb = ob; }
+            }
+            if ((lane & 31) == 0) { red_v[lane >> 5] = bv; red_b[lane >> 5] = bb; }
+            __syncthreads();
+            if (lane == 0) {
+                for (int w = 1; w < (nth + 31) / 32; ++w) {
+                    const int ov = red_v[w], ob = red_b[w];
+                    if (ob >= 0 && (bb < 0 || ov < bv || (ov == bv && ob < bb))) { bv = ov; bb = ob; }
                 }
-            } else {
-                const int cur = static_cast<int>(i * NN + toy * Z.N + tox);
-                for (int b = minx; b <= maxx; ++b) {
-                    if (b == tox) continue;
-                    const int last = static_cast<int>(i * NN + toy * Z.N + b);
-                    const int v = zadd(m4[last], zwire(T, Z, last, cur));
-                    if (v < mj[cur]) { mj[cur] = v; pj[cur] = p4[last]; p2j[cur] = p5[last]; }
+                if (bb >= 0 && bv < mj[cur]) {
+                    const int last = static_cast<int>(ay ? i * NN + tox * Z.N + bb : i * NN + toy * Z.N + bb);
+                    mj[cur] = bv; pj[cur] = p4[last]; p2j[cur] = p5[last];
                 }
             }
+            __syncthreads();
         }
     } else if (fromx == tox) {
         for (int i = 1 + lane; i < LAYER; i += nth) {
