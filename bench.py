@@ -328,6 +328,7 @@ def run_grotor(args):
     order_pin = torch.empty(len(order), dtype=torch.int32, pin_memory=True)
     order_pin.numpy()[...] = order
     h2d = sum(v.numel() * v.element_size() for v in pinned.values()) + order_pin.numel() * 4
+    routes_pin = torch.empty(int(nets.route_off[-1]), dtype=torch.int32, pin_memory=True)
     d2h = int(nets.route_off[-1]) * 4 + len(order) * 4 + 16
     torch.cuda.synchronize()
     e2 = torch.cuda.Event(enable_timing=True)
@@ -338,7 +339,7 @@ def run_grotor(args):
         r.reset()
         r.generate_batches_rsmt(order_pin.numpy(), BATCH_LIMIT, 1, "plain" if args.executor != "persistent" else "persistent")
         r.lshape_route(args.executor)
-        routes_e2e = r.read_routes()
+        routes_e2e = r.read_routes(out=routes_pin.numpy())
     e3.record(stream)
     torch.cuda.synchronize()
     e2e_ms = max_over_ranks(pg, e2.elapsed_time(e3))

@@ -575,6 +575,47 @@ __global__ void __launch_bounds__(1024) k_soft_sum(const T* v, int n, double* ou
     if (threadIdx.x == 0) *out = part[0];
 }
 
+// --- input validation ------------------------------------------------------
+// Every index a stage kernel will dereference is checked on the device after
+// the upload (one thread per net, then one per geometry element); the first
+// violation is recorded as (code, item) and the largest tree size kept.
+struct NetCheck {
+    const int* node_off; const int* nodes; const int* parents; const long long* route_off;
+    const int* point_off; const int* points; const int* hseg_off; const int* hsegs;
+    const int* vseg_off; const int* vsegs;
+    int n, nn, np, nh, nv, XY, L;
+    long long rw;
+    int* status;  // [0] code (1 offsets, 2 node, 3 parent, 4 geometry), [1] item, [2] max nodes
+};
+__device__ __forceinline__ void check_fail(const NetCheck& C, int code, int item) {
+    if (atomicCAS(C.status, 0, code) == 0) C.status[1] = item;
+}
+__global__ void k_validate_nets(NetCheck C) {
+    const int nt = gridDim.x * blockDim.x;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < C.n; i += nt) {
+        const int a = C.node_off[i], b = C.node_off[i + 1];
+        const bool geo = (C.point_off[i] <= C.point_off[i + 1] && C.point_off[i] >= 0 && C.point_off[i + 1] <= C.np) &&
+                         (C.hseg_off[i] <= C.hseg_off[i + 1] && C.hseg_off[i] >= 0 && C.hseg_off[i + 1] <= C.nh) &&
+                         (C.vseg_off[i] <= C.vseg_off[i + 1] && C.vseg_off[i] >= 0 && C.vseg_off[i + 1] <= C.nv);
+        if (a < 0 || b < a || b > C.nn || C.route_off[i] < 0 || C.route_off[i + 1] < C.route_off[i] ||
+            C.route_off[i + 1] > C.rw || !geo) {
+            check_fail(C, 1, i);
+            continue;
+        }
+        atomicMax(C.status + 2, b - a);
+        for (int k = a; k < b; ++k) {
+            const int v = C.nodes[k], p = C.parents[k];
+            if (v < 0 || v / C.XY > C.L) { check_fail(C, 2, i); break; }
+            if (k == a ? p != -1 : (p < 0 || p >= k - a)) { check_fail(C, 3, i); break; }
+        }
+    }
+    const long long total = (long long)C.np + 2ll * C.nh + 2ll * C.nv;
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < total; k += nt) {
+        const int v = k < C.np ? C.points[k] : k < C.np + 2ll * C.nh ? C.hsegs[k - C.np] : C.vsegs[k - C.np - 2ll * C.nh];
+        if (v < 0 || v >= C.XY) check_fail(C, 4, int(k));
+    }
+}
+
 // --- batching kernels -------------------------------------------------------
 // One net per CTA in the per-net steps (a chunk's nets spread over the grid).
 constexpr int kBatchAcc = 96;  // >= W + kChunkWords for every W phase 3 admits
@@ -816,6 +857,7 @@ struct grb_ctx {
     char* soft_slot = nullptr;
     size_t soft_slot_bytes = 0;
     double* soft_scalar = nullptr;
+    int* check = nullptr;             // [3] upload validation status
     // size-bucketed plan and tuned launch shapes
     int* bucket_ids = nullptr;
     int* bucket_off = nullptr;
@@ -1504,7 +1546,7 @@ void grb_destroy(grb_ctx* c) {
     free_all(c->geom_bufs);
     free_all(c->flt_bufs);
     free_all(c->owned);
-    for (void* p : {(void*)c->bucket_ids, (void*)c->bucket_off, (void*)c->ids, (void*)c->batch_off, (void*)c->gscratch, (void*)c->work, (void*)c->cellmask,
+    for (void* p : {(void*)c->check, (void*)c->bucket_ids, (void*)c->bucket_off, (void*)c->ids, (void*)c->batch_off, (void*)c->gscratch, (void*)c->work, (void*)c->cellmask,
                     (void*)c->localmask, (void*)c->localmask2, (void*)c->fmask, (void*)c->pred, (void*)c->fullmask, (void*)c->bcount,
                     (void*)c->ncolors, (void*)c->batch_of, (void*)c->brank, (void*)c->order})
         if (p) cudaFree(p);
@@ -1540,35 +1582,19 @@ int grb_upload_nets(grb_ctx* c, const grb_nets* nets) {
     if (!c || !nets || nets->n < 0 || !nets->node_off || !nets->route_off) return c ? fail(c, GRB_EINVAL, "bad nets") : GRB_EINVAL;
     GRB_CUDA(c, cudaSetDevice(c->device));
     const int n = nets->n;
+    // Only the totals are read on the host (they size the buffers); every
+    // element is checked on the device after the upload.
+    if (nets->node_off[0] != 0 || nets->route_off[0] != 0 || (nets->point_off && nets->point_off[0] != 0) ||
+        (nets->hseg_off && nets->hseg_off[0] != 0) || (nets->vseg_off && nets->vseg_off[0] != 0))
+        return fail(c, GRB_EINVAL, "offsets must start at 0");
     const int nn = nets->node_off[n];
-    long long maxn = 0;
-    for (int i = 0; i < n; ++i) maxn = std::max<long long>(maxn, nets->node_off[i + 1] - nets->node_off[i]);
     const long long rw = nets->route_off[n];
     const int np = nets->point_off ? nets->point_off[n] : 0;
     const int nh = nets->hseg_off ? nets->hseg_off[n] : 0;
     const int nv = nets->vseg_off ? nets->vseg_off[n] : 0;
-    // Validate on the host: every index a kernel will dereference is in range.
-    {
-        const int XY = c->T.XY, L = c->T.L;
-        for (int i = 0; i < n; ++i) {
-            const int a = nets->node_off[i], b = nets->node_off[i + 1];
-            if (b < a || nets->route_off[i + 1] < nets->route_off[i]) return fail(c, GRB_EINVAL, "offsets must be non-decreasing");
-            for (int k = a; k < b; ++k) {
-                const int v = nets->nodes[k], p = nets->parents[k];
-                if (v < 0 || v / XY > L) return fail(c, GRB_EINVAL, "tree node outside the grid");
-                if (k == a ? p != -1 : (p < 0 || p >= k - a)) return fail(c, GRB_EINVAL, "parents must precede children");
-            }
-        }
-        auto check_csr = [&](const int* off, const int* data, int width) {
-            if (!off) return true;
-            for (int i = 0; i < n; ++i) if (off[i + 1] < off[i]) return false;
-            for (long long k = 0; k < (long long)off[n] * width; ++k) if (data[k] < 0 || data[k] >= XY) return false;
-            return true;
-        };
-        if (!check_csr(nets->point_off, nets->points, 1) || !check_csr(nets->hseg_off, nets->hsegs, 2) ||
-            !check_csr(nets->vseg_off, nets->vsegs, 2))
-            return fail(c, GRB_EINVAL, "batching geometry outside the grid");
-    }
+    if (nn < 0 || rw < 0 || np < 0 || nh < 0 || nv < 0) return fail(c, GRB_EINVAL, "negative totals");
+    if ((nn && (!nets->nodes || !nets->parents)) || (np && !nets->points) || (nh && !nets->hsegs) || (nv && !nets->vsegs))
+        return fail(c, GRB_EINVAL, "net arrays missing");
     // Reuse the device buffers when every array still fits.
     const long long need[6] = {n, nn, rw, np, nh, nv};
     bool fits = !c->net_bufs.empty() && c->geom_bufs.empty();
@@ -1611,8 +1637,29 @@ int grb_upload_nets(grb_ctx* c, const grb_nets* nets) {
     if (nets->vseg_off) GRB_CUDA(c, h2d(c->vseg_off, nets->vseg_off, sizeof(int) * (n + 1)));
     else GRB_CUDA(c, cudaMemsetAsync(c->vseg_off, 0, sizeof(int) * (n + 1), c->stream));
     GRB_CUDA(c, h2d(c->vsegs, nets->vsegs, sizeof(int) * 2 * nv));
-    // Host buffers may be pageable and short-lived: the copies complete before return.
+    // Device-side validation; host buffers may be pageable and short-lived: the
+    // copies complete before return.
+    int status[3] = {0, 0, 0};
+    if (!c->check) {
+        if (cudaMalloc(&c->check, 3 * sizeof(int)) != cudaSuccess) { cudaGetLastError(); return fail(c, GRB_ENOMEM, "validation status"); }
+    }
+    GRB_CUDA(c, cudaMemsetAsync(c->check, 0, 3 * sizeof(int), c->stream));
+    NetCheck C{c->node_off, c->nodes, c->parents, c->route_off, c->point_off, c->points, c->hseg_off, c->hsegs,
+               c->vseg_off, c->vsegs, n, nn, np, nh, nv, c->T.XY, c->T.L, rw, c->check};
+    k_validate_nets<<<c->sms * 4, 256, 0, c->stream>>>(C);
+    c->launches += 1;
+    GRB_CUDA(c, cudaGetLastError());
+    GRB_CUDA(c, cudaMemcpyAsync(status, c->check, 3 * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
     GRB_CUDA(c, cudaStreamSynchronize(c->stream));
+    if (status[0]) {
+        static const char* what[] = {"", "offsets must be non-decreasing and within the arrays", "tree node outside the grid",
+                                     "parents must precede children", "batching geometry outside the grid"};
+        c->n_nets = 0;  // no net id is accepted until a valid upload
+        c->flt_n = -1;
+        c->z_n = -1;
+        return fail(c, GRB_EINVAL, std::string(what[status[0]]) + " (item " + std::to_string(status[1]) + ")");
+    }
+    const long long maxn = status[2];
     c->n_nets = n;
     c->max_nodes = int(maxn);
     c->route_words = rw;

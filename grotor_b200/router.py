@@ -142,9 +142,9 @@ class Router:
         self._check(self._lib.grb_reset(self._ctx))
 
     def upload_nets(self, nets: NetArrays):
-        self.nets = nets
         s = nets.struct()
         self._check(self._lib.grb_upload_nets(self._ctx, C.byref(s)))
+        self.nets = nets
 
     # -- batching ------------------------------------------------------------
     def generate_batches_rsmt(self, order, limit: int = 1000000, sparsity: int = 1, mode="persistent"):
@@ -281,9 +281,15 @@ class Router:
                                               _p(out["demand_half"]), _p(out["timestamp"])))
         return out
 
-    def read_routes(self) -> np.ndarray:
+    def read_routes(self, out=None) -> np.ndarray:
+        """All route words (route_off order).  ``out`` may be a caller-owned
+        int32 buffer of at least that many words (pinned host memory makes the
+        copy run at full PCIe rate)."""
         words = int(self.nets.route_off[-1]) if self.nets is not None else 0
-        out = np.zeros(words, np.int32)
+        if out is None:
+            out = np.zeros(words, np.int32)
+        elif out.dtype != np.int32 or not out.flags.c_contiguous or out.size < words:
+            raise ValueError(f"out must be a contiguous int32 array of at least {words} words")
         self._check(self._lib.grb_read_routes(self._ctx, _p(out)))
         return out
 
