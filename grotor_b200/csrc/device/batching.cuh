@@ -9,24 +9,31 @@
 //
 // B200 algorithm (replaces the RT-core/OptiX and CPU paths, which produce the
 // same lists):
+//   * once per run, every net's marked cells and query points are written to
+//     flat lists in order-position order (k_flat_*), tagged with the net's
+//     position inside its chunk of kChunk nets, so each per-chunk step below is
+//     one balanced, coalesced pass over a contiguous range;
 //   * cellmask[cell] holds one bit per batch ("colour") already marking the cell;
-//   * nets are processed in chunks of 512 in order; per chunk:
-//       1. every net rasters its marks into a chunk-local bitmask per cell
-//          (bit = its position in the chunk) and ORs cellmask over its points
-//          -> forbidden colours from earlier chunks;
-//       2. every net ORs the chunk-local masks over its points, keeping bits of
-//          earlier chunk nets -> exact intra-chunk predecessors;
-//       3. one CTA solves first-fit inside the chunk by Jacobi iteration over
-//          the predecessor DAG (converges to the unique sequential solution),
-//          then applies batch capacities in order;
-//       4. every net ORs its colour into cellmask over its marks and clears the
-//          chunk-local masks.
-//   The chunks run inside one cooperative kernel with bounded grid barriers
-//   (persistent form) or as one launch per phase (plain form).  The chunk-local
-//   masks are double-buffered by chunk parity, so the persistent form rasters
-//   chunk k+1 on every other CTA while one CTA solves chunk k, and reads the
-//   forbidden colours (step 1's second half) together with the predecessors
-//   after chunk k-1 is published.
+//   * nets are processed in chunks of kChunk in order; per chunk:
+//       1. raster: every mark ORs its net's bit into the chunk-local mask of
+//          the cell (triple-buffered by chunk index);
+//       2. gather: every query point ORs, into its net's column of the chunk
+//          tables, the cell's colours (forbidden batches of earlier chunks),
+//          the chunk-local bits of earlier nets of the chunk (predecessors),
+//          and -- in the lookback form -- the bits of the previous chunk's nets;
+//       3. solve: one CTA solves first-fit inside the chunk by Jacobi
+//          iteration over the predecessor DAG (converges to the unique
+//          sequential solution), then applies batch capacities in order;
+//       4. publish: every mark ORs its net's colour into cellmask and clears
+//          the chunk-local mask.
+//   Plain form: one launch per step per chunk.  Persistent form: one
+//   cooperative kernel in which CTA 0 solves chunk r while the other CTAs
+//   publish chunk r-1, raster chunk r+1 and gather chunk r+1; the gather
+//   reads cellmask as of chunk r-1 and takes chunk r's colours through the
+//   previous-chunk bits, which the solver resolves from the colours it keeps
+//   in shared memory.  The solver and the other CTAs hand chunks over through
+//   two monotone counters (bounded waits), so the solve never waits for a
+//   publish.
 #pragma once
 #include "common.cuh"
 
@@ -41,16 +48,24 @@ struct BatchState {
     const int* point_off; const int* points;
     const int* hseg_off; const int* hsegs;
     const int* vseg_off; const int* vsegs;
-    unsigned* cellmask;    // [X*Y][W]
-    unsigned* localmask;   // [X*Y][kChunkWords], chunks of even index
-    unsigned* localmask2;  // [X*Y][kChunkWords], chunks of odd index
-    unsigned* fmask;       // [W][kChunk] (word-major: the solve copies it as is)
-    unsigned* pred;        // [kChunkWords][kChunk]
-    unsigned* fullmask;    // [W]
-    int* count;            // [32*W]
-    int* n_colors;         // [1]
-    int* batch_of;         // [n] colour per order position
-    int* rank;             // [n] position inside its batch
+    // Flat lists by order position (k_flat_*).
+    long long* mark_off;        // [n+1]
+    unsigned* mark_cell;        // cells marked by the nets (duplicates allowed)
+    unsigned short* mark_jj;    // position of the marking net inside its chunk
+    long long* pt_off;          // [n+1]
+    unsigned* pt_cell;          // query points
+    unsigned short* pt_jj;
+    unsigned* cellmask;         // [X*Y][W]
+    unsigned* localmask[3];     // [X*Y][kChunkWords], chunk k in buffer k % 3
+    unsigned* fmask;            // [2][W][kChunk] forbidden colours, by chunk parity
+    unsigned* pred;             // [2][kChunkWords][kChunk] predecessors inside the chunk
+    unsigned* prevp;            // [2][kChunkWords][kChunk] marking nets of the previous chunk
+    unsigned* fullmask;         // [W]
+    int* count;                 // [32*W]
+    int* n_colors;              // [1]
+    int* batch_of;              // [n] colour per order position
+    int* rank;                  // [n] position inside its batch
+    unsigned* solved;           // [1] chunks solved (persistent form)
     int* error;
     int* error_info;
 };
@@ -59,14 +74,13 @@ __device__ __forceinline__ void batch_error(const BatchState& B, int code, int i
     if (atomicCAS(B.error, 0, code) == 0) *B.error_info = info;
 }
 
-// Cells of the segments [s0, s1) of `segs` with step `step`; threads t of n
-// split each segment's cells.  Every warp of the group fetches 32 segment
-// endpoints per memory round trip and broadcasts them by shuffle, so a net
-// with many short segments does not wait one load latency per segment.
-// All 32 lanes of each warp of the group must call this.
-template <class F>
-__device__ __forceinline__ void for_each_segment_cell(const int* segs, int s0, int s1, int step, int t, int n, F f) {
-    const int lane = t & 31;
+// Cells of the segments [s0, s1) of `segs` with step `step`, visited by the 32
+// lanes of a warp: lanes fetch 32 segment endpoints per memory round trip and
+// broadcast them by shuffle.  f(cell, k, cnt) gets each cell with its index
+// k < cnt inside the segment; done(cnt) runs on every lane after a segment.
+template <class F, class D>
+__device__ __forceinline__ void warp_segment_cells(const int* segs, int s0, int s1, int step, F f, D done) {
+    const int lane = threadIdx.x & 31;
     for (int base = s0; base < s1; base += 32) {
         int a = 0, b = -1;
         if (base + lane < s1) { a = segs[2 * (base + lane)]; b = segs[2 * (base + lane) + 1]; }
@@ -75,220 +89,357 @@ __device__ __forceinline__ void for_each_segment_cell(const int* segs, int s0, i
             const int aq = __shfl_sync(0xffffffffu, a, q), bq = __shfl_sync(0xffffffffu, b, q);
             if (bq < aq) continue;
             const int cnt = (bq - aq) / step + 1;
-            for (int k = t; k < cnt; k += n) f(aq + k * step);
+            for (int k = lane; k < cnt; k += 32) f(aq + k * step, k, cnt);
+            done(cnt);
         }
     }
 }
 
-// Visit every cell net `id` marks (duplicates allowed); threads t of n split
-// the work.
-template <class F>
-__device__ __forceinline__ void for_each_mark(const BatchState& B, int id, int t, int n, F f) {
-    for_each_segment_cell(B.hsegs, B.hseg_off[id], B.hseg_off[id + 1], B.sparsity * B.Y, t, n, f);
-    for_each_segment_cell(B.vsegs, B.vseg_off[id], B.vseg_off[id + 1], B.sparsity, t, n, f);
+// The (up to) four cells a query point marks: left, below, itself, right.
+__device__ __forceinline__ bool point_mark(const BatchState& B, int p, int which, int* cell) {
+    const int x = p / B.Y, y = p - x * B.Y;
+    int cx = x, cy = y;
+    if (which == 0) cx = x - 1;
+    else if (which == 1) cy = y - 1;
+    else if (which == 3) cx = x + 1;
+    *cell = cx * B.Y + cy;
+    return cx >= 0 && cx < B.X && cy >= 0;
+}
+
+// Warp per order position: number of marks and query points of its net.
+__device__ __forceinline__ void flat_count(const BatchState& B, int p) {
+    const int lane = threadIdx.x & 31;
+    const int id = B.order[p];
+    long long marks = 0;
+    warp_segment_cells(B.hsegs, B.hseg_off[id], B.hseg_off[id + 1], B.sparsity * B.Y, [](int, int, int) {},
+                       [&](int cnt) { marks += cnt; });
+    warp_segment_cells(B.vsegs, B.vseg_off[id], B.vseg_off[id + 1], B.sparsity, [](int, int, int) {},
+                       [&](int cnt) { marks += cnt; });
     const int p0 = B.point_off[id], np = B.point_off[id + 1] - p0;
-    for (int k = t; k < 4 * np; k += n) {
-        const int p = B.points[p0 + k / 4], x = p / B.Y, y = p - x * B.Y;
-        const int which = k & 3;
-        int cx = x, cy = y;
-        if (which == 0) cx = x - 1;
-        else if (which == 1) cy = y - 1;
-        else if (which == 3) cx = x + 1;
-        if (cx >= 0 && cx < B.X && cy >= 0) f(cx * B.Y + cy);
+    int own = 0;
+    for (int k = lane; k < 4 * np; k += 32) {
+        int cell;
+        own += point_mark(B, B.points[p0 + k / 4], k & 3, &cell) ? 1 : 0;
+    }
+    for (int o = 16; o; o >>= 1) own += __shfl_xor_sync(0xffffffffu, own, o);
+    if (lane == 0) {
+        B.mark_off[p] = marks + own;
+        B.pt_off[p] = np;
     }
 }
 
-// A group of threads that works on one net: a whole CTA, or half of one
-// synchronised with a named barrier.
-struct NetGroup {
-    int t, n, bar;  // thread rank, group size, named barrier id (0: the CTA)
-    __device__ __forceinline__ void sync() const {
-        if (bar == 0) __syncthreads();
-        else asm volatile("bar.sync %0, %1;" ::"r"(bar), "r"(n) : "memory");
+// Warp per order position: writes its net's marks and query points at the
+// (scanned) offsets.
+__device__ __forceinline__ void flat_fill(const BatchState& B, int p) {
+    const int lane = threadIdx.x & 31;
+    const int id = B.order[p];
+    const unsigned short jj = static_cast<unsigned short>(p % kChunk);
+    long long o = B.mark_off[p];
+    auto put = [&](int cell, int k, int) {
+        B.mark_cell[o + k] = static_cast<unsigned>(cell);
+        B.mark_jj[o + k] = jj;
+    };
+    auto advance = [&](int cnt) { o += cnt; };
+    warp_segment_cells(B.hsegs, B.hseg_off[id], B.hseg_off[id + 1], B.sparsity * B.Y, put, advance);
+    warp_segment_cells(B.vsegs, B.vseg_off[id], B.vseg_off[id + 1], B.sparsity, put, advance);
+    const int p0 = B.point_off[id], np = B.point_off[id + 1] - p0;
+    for (int base = 0; base < 4 * np; base += 32) {
+        const int k = base + lane;
+        int cell = 0;
+        const bool ok = k < 4 * np && point_mark(B, B.points[p0 + k / 4], k & 3, &cell);
+        const unsigned ball = __ballot_sync(0xffffffffu, ok);
+        if (ok) {
+            const long long at = o + __popc(ball & ((1u << lane) - 1u));
+            B.mark_cell[at] = static_cast<unsigned>(cell);
+            B.mark_jj[at] = jj;
+        }
+        o += __popc(ball);
     }
+    const long long q = B.pt_off[p];
+    for (int k = lane; k < np; k += 32) {
+        B.pt_cell[q + k] = static_cast<unsigned>(B.points[p0 + k]);
+        B.pt_jj[q + k] = jj;
+    }
+}
+
+__device__ __forceinline__ unsigned* chunk_mask(const BatchState& B, int chunk) { return B.localmask[chunk % 3]; }
+
+// Step 1: the chunk at order position s rasters its marks.  Threads t of nt.
+__device__ __forceinline__ void batch_raster(const BatchState& B, int s, long long t, long long nt) {
+    const int m = min(kChunk, B.n - s);
+    unsigned* lm = chunk_mask(B, s / kChunk);
+    const long long a = B.mark_off[s], b = B.mark_off[s + m];
+    for (long long k = a + t; k < b; k += nt) {
+        const unsigned q = __ldg(B.mark_cell + k);
+        const int jj = __ldg(B.mark_jj + k);
+        red_or(lm + size_t(q) * kChunkWords + (jj >> 5), 1u << (jj & 31));
+    }
+}
+
+// Step 2: per query point, OR the cell's colours, the earlier nets' bits of
+// this chunk and (lookback) the previous chunk's bits into the net's column.
+__device__ __forceinline__ void batch_gather(const BatchState& B, int s, bool lookback, long long t, long long nt) {
+    const int chunk = s / kChunk, m = min(kChunk, B.n - s), W = B.W;
+    const unsigned* lm = chunk_mask(B, chunk);
+    const unsigned* lp = lookback ? chunk_mask(B, chunk - 1) : nullptr;
+    unsigned* F = B.fmask + size_t(chunk & 1) * W * kChunk;
+    unsigned* P = B.pred + size_t(chunk & 1) * kChunkWords * kChunk;
+    unsigned* Q = B.prevp + size_t(chunk & 1) * kChunkWords * kChunk;
+    const int per = W + kChunkWords * (lookback ? 2 : 1);
+    const long long a = B.pt_off[s], b = B.pt_off[s + m];
+    const long long items = (b - a) * per;
+    for (long long k = t; k < items; k += nt) {
+        const long long pi = k / per;
+        const int w = int(k - pi * per);
+        const unsigned q = __ldg(B.pt_cell + a + pi);
+        const int jj = __ldg(B.pt_jj + a + pi);
+        unsigned v;
+        unsigned* dst;
+        if (w < W) {
+            v = __ldcg(B.cellmask + size_t(q) * W + w);
+            dst = F + size_t(w) * kChunk + jj;
+        } else if (w < W + kChunkWords) {
+            const int pw = w - W;
+            if (pw > (jj >> 5)) continue;
+            v = __ldcg(lm + size_t(q) * kChunkWords + pw);
+            if (pw == (jj >> 5)) v &= (1u << (jj & 31)) - 1u;
+            dst = P + pw * kChunk + jj;
+        } else {
+            const int qw = w - W - kChunkWords;
+            v = __ldcg(lp + size_t(q) * kChunkWords + qw);
+            dst = Q + qw * kChunk + jj;
+        }
+        if (v) red_or(dst, v);
+    }
+}
+
+// Step 4: the chunk at s publishes its colours and clears its chunk-local mask.
+__device__ __forceinline__ void batch_publish(const BatchState& B, int s, long long t, long long nt) {
+    const int m = min(kChunk, B.n - s);
+    unsigned* lm = chunk_mask(B, s / kChunk);
+    const long long a = B.mark_off[s], b = B.mark_off[s + m];
+    for (long long k = a + t; k < b; k += nt) {
+        const unsigned q = __ldg(B.mark_cell + k);
+        const int jj = __ldg(B.mark_jj + k);
+        const int c = __ldcg(B.batch_of + s + jj);
+        red_or(B.cellmask + size_t(q) * B.W + (c >> 5), 1u << (c & 31));
+        lm[size_t(q) * kChunkWords + (jj >> 5)] = 0u;
+    }
+}
+
+// Shared memory of the solving CTA (kept across chunks in the persistent form).
+struct SolveSmem {
+    unsigned* U;     // [W][kChunk] colours a net may not take (published, full, previous chunk)
+    unsigned* P;     // [kChunkWords][kChunk] predecessor bits
+    int* col;        // [kChunk] colour of each net of the chunk
+    int* colp;       // [kChunk] colours of the previous chunk
+    int* cnt;        // [32W] nets per colour so far
+    int* wh;         // [kChunk/32][32W] per-warp colour counts (zero between uses), or
+                     // for W > kWarpCountWords a [32W] running count
+    bool per_warp;   // wh holds per-warp counts
+    unsigned* full;  // [W] colours whose batch is full
 };
 
-// Chunk-local mask buffer of the chunk starting at order position s.
-__device__ __forceinline__ unsigned* chunk_mask(const BatchState& B, int s) {
-    return ((s / kChunk) & 1) ? B.localmask2 : B.localmask;
+// Up to this many colour words the ranks use per-warp colour counts (three
+// barriers); beyond it, warps add their counts in turn (one barrier per warp).
+constexpr int kWarpCountWords = 32;
+
+__host__ __device__ __forceinline__ size_t solve_smem_bytes(int W) {
+    const size_t C = 32 * size_t(W);
+    const size_t wh = W <= kWarpCountWords ? (kChunk / 32) * C : C;
+    return size_t(kChunk) * W * 4 + size_t(kChunk) * kChunkWords * 4 + 2 * size_t(kChunk) * 4 + C * 4 + wh * 4 +
+           size_t(W) * 4;
 }
 
-// The per-net steps run one net per group (its threads share the net's marks
-// and points).
-// Step 1a: chunk-local raster.
-__device__ __forceinline__ void batch_raster(const BatchState& B, int s, int jj, const NetGroup& G) {
-    const int id = B.order[s + jj];
-    const unsigned bit = 1u << (jj & 31);
-    const int word = jj >> 5;
-    unsigned* lm = chunk_mask(B, s);
-    for_each_mark(B, id, G.t, G.n, [&](int q) { red_or(lm + size_t(q) * kChunkWords + word, bit); });
+__device__ __forceinline__ SolveSmem solve_smem(unsigned* base, int W) {
+    const int C = 32 * W;
+    SolveSmem S;
+    S.U = base;
+    S.P = S.U + size_t(kChunk) * W;
+    S.col = reinterpret_cast<int*>(S.P + size_t(kChunk) * kChunkWords);
+    S.colp = S.col + kChunk;
+    S.cnt = S.colp + kChunk;
+    S.wh = S.cnt + C;
+    S.per_warp = W <= kWarpCountWords;
+    S.full = reinterpret_cast<unsigned*>(S.wh + (S.per_warp ? (kChunk / 32) * C : C));
+    return S;
 }
 
-// Step 1b + 2: forbidden colours from earlier (published) chunks and the
-// predecessors inside the chunk, both ORed over the net's query points.
-// `acc` is group shared memory of W + kChunkWords words.
-__device__ __forceinline__ void batch_forbid_preds(const BatchState& B, int s, int jj, unsigned* acc, const NetGroup& G) {
-    const int id = B.order[s + jj];
-    const int t = G.t, n = G.n;
-    const int W = B.W;
-    const int words = (jj >> 5) + 1;  // only bits of earlier chunk nets matter
-    const unsigned* lm = chunk_mask(B, s);
-    for (int w = t; w < W + kChunkWords; w += n) acc[w] = 0u;
-    G.sync();
-    const int p0 = B.point_off[id], np = B.point_off[id + 1] - p0;
-    for (int k = t; k < np * W; k += n) {
-        const int w = k % W;
-        const unsigned v = B.cellmask[size_t(B.points[p0 + k / W]) * W + w];
-        if (v) atomicOr(acc + w, v);
-    }
-    for (int k = t; k < np * words; k += n) {
-        const int w = k % words;
-        const unsigned v = lm[size_t(B.points[p0 + k / words]) * kChunkWords + w];
-        if (v) atomicOr(acc + W + w, v);
-    }
-    G.sync();
-    for (int w = t; w < W; w += n) B.fmask[size_t(w) * kChunk + jj] = acc[w];
-    for (int w = t; w < kChunkWords; w += n) {
-        unsigned v = w < words ? acc[W + w] : 0u;
-        if (w == (jj >> 5)) v &= (1u << (jj & 31)) - 1u;
-        B.pred[w * kChunk + jj] = v;
-    }
-    G.sync();
-}
-
-// Phase 4: publish the net's colour over its marks and clear its chunk-local
-// word (every net of the chunk clears the word holding its own bit, so all
-// words touched by the chunk end up zero).
-__device__ __forceinline__ void batch_phase4(const BatchState& B, int s, int jj, const NetGroup& G) {
-    const int id = B.order[s + jj];
-    const int c = B.batch_of[s + jj];
-    const unsigned bit = 1u << (c & 31);
-    const int word = c >> 5, lword = jj >> 5;
-    unsigned* lm = chunk_mask(B, s);
-    for_each_mark(B, id, G.t, G.n, [&](int q) {
-        red_or(B.cellmask + size_t(q) * B.W + word, bit);
-        lm[size_t(q) * kChunkWords + lword] = 0u;
-    });
-}
-
-// Phase 3 (one CTA of kChunk threads): first-fit inside the chunk.
-// smem (word-major so a warp reads 32 consecutive words): F[W][kChunk],
-// P[kChunkWords][kChunk], col[kChunk], cnt[32W], run[32W], full[W].
-__device__ void batch_phase3(const BatchState& B, int s, unsigned* smem) {
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int m = min(kChunk, B.n - s);
-    const int W = B.W, C = 32 * W;
-    unsigned* F = smem;
-    unsigned* P = F + kChunk * W;
-    int* col = reinterpret_cast<int*>(P + kChunk * kChunkWords);
-    int* cnt = col + kChunk;
-    int* run = cnt + C;
-    unsigned* full = reinterpret_cast<unsigned*>(run + C);
-    __shared__ int first_bad, overflow;
-    // Both tables are word-major in global memory already: 16-byte copies.
-    {
-        const uint4* f4 = reinterpret_cast<const uint4*>(B.fmask);
-        const uint4* p4 = reinterpret_cast<const uint4*>(B.pred);
-        uint4* F4 = reinterpret_cast<uint4*>(F);
-        uint4* P4 = reinterpret_cast<uint4*>(P);
-        const int nf = W * kChunk / 4, np = kChunkWords * kChunk / 4;
-        for (int k = tid; k < nf + np; k += blockDim.x) {
-            if (k < nf) F4[k] = f4[k];
-            else P4[k - nf] = p4[k - nf];
+// The smallest colour c >= c0 net `tid` may take: not in U, not held by a
+// predecessor (pmask: which predecessor words are nonzero).  C if none.
+__device__ __forceinline__ int first_fit(const SolveSmem& S, int tid, int W, unsigned pmask, int c0) {
+    int c = c0;
+    while (true) {
+        int w = c >> 5;
+        if (w >= W) return 32 * W;
+        unsigned used = S.U[w * kChunk + tid] | ((1u << (c & 31)) - 1u);
+        while (used == 0xffffffffu) {
+            if (++w >= W) return 32 * W;
+            used = S.U[w * kChunk + tid];
         }
+        c = w * 32 + __ffs(~used) - 1;
+        bool hit = false;
+        for (unsigned pm = pmask; pm && !hit; pm &= pm - 1) {
+            const int pw = __ffs(pm) - 1;
+            unsigned bits = S.P[pw * kChunk + tid];
+            while (bits) {
+                const int i = pw * 32 + __ffs(bits) - 1;
+                bits &= bits - 1;
+                if (S.col[i] == c) { hit = true; break; }
+            }
+        }
+        if (!hit) return c;
+        ++c;
     }
-    for (int k = tid; k < C; k += blockDim.x) cnt[k] = B.count[k];
-    for (int k = tid; k < W; k += blockDim.x) full[k] = B.fullmask[k];
-    if (tid < kChunk) col[tid] = -1;
+}
+
+// The solve runs on threads 0..kChunk-1 of its CTA and synchronises them
+// with named barrier 1 (the CTA may hold more threads, which do not take part).
+__device__ __forceinline__ void solve_sync() { asm volatile("bar.sync 1, %0;" ::"n"(kChunk) : "memory"); }
+__device__ __forceinline__ bool solve_sync_or(bool v) {
+    int r;
+    asm volatile(
+        "{\n .reg .pred p, q;\n setp.ne.s32 p, %1, 0;\n bar.red.or.pred q, 1, %2, p;\n selp.s32 %0, 1, 0, q;\n}"
+        : "=r"(r) : "r"(int(v)), "n"(kChunk) : "memory");
+    return r != 0;
+}
+
+// Step 3 (threads 0..kChunk-1 of a CTA): first-fit of the chunk at order
+// position s.  S.cnt and S.full hold the state of the chunks before it;
+// with `lookback`, S.colp holds the previous chunk's colours.  The chunk's
+// tables are read once and cleared for reuse by chunk s + 2 * kChunk.
+// Returns false on colour overflow (kELimit recorded).
+__device__ __forceinline__ bool batch_solve(const BatchState& B, int s, bool lookback, const SolveSmem& S) {
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int chunk = s / kChunk, m = min(kChunk, B.n - s);
+    const int W = B.W, C = 32 * W;
+    unsigned* Fg = B.fmask + size_t(chunk & 1) * W * kChunk;
+    unsigned* Pg = B.pred + size_t(chunk & 1) * kChunkWords * kChunk;
+    unsigned* Qg = B.prevp + size_t(chunk & 1) * kChunkWords * kChunk;
+    __shared__ int first_bad, overflow;
     if (tid == 0) overflow = 0;
-    __syncthreads();
+    unsigned pmask = 0;
+    int c0 = 0;  // first colour not in U
+    if (tid < m) {
+        // Every load of a group is issued before its stores, so the round
+        // trips overlap (the tables were just written by other SMs).
+        for (int w0 = 0; w0 < W; w0 += 8) {
+            unsigned v[8];
+#pragma unroll
+            for (int k = 0; k < 8; ++k) v[k] = w0 + k < W ? __ldcg(Fg + size_t(w0 + k) * kChunk + tid) : 0u;
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+                if (w0 + k >= W) break;
+                if (v[k]) Fg[size_t(w0 + k) * kChunk + tid] = 0u;
+                S.U[(w0 + k) * kChunk + tid] = v[k] | S.full[w0 + k];
+            }
+        }
+        {
+            unsigned v[kChunkWords];
+#pragma unroll
+            for (int w = 0; w < kChunkWords; ++w) v[w] = w <= (tid >> 5) ? __ldcg(Pg + w * kChunk + tid) : 0u;
+#pragma unroll
+            for (int w = 0; w < kChunkWords; ++w) {
+                S.P[w * kChunk + tid] = v[w];
+                if (v[w]) { Pg[w * kChunk + tid] = 0u; pmask |= 1u << w; }
+            }
+        }
+        if (lookback) {
+            unsigned v[kChunkWords];
+#pragma unroll
+            for (int w = 0; w < kChunkWords; ++w) v[w] = __ldcg(Qg + w * kChunk + tid);
+#pragma unroll
+            for (int w = 0; w < kChunkWords; ++w) {
+                unsigned bits = v[w];
+                if (bits) Qg[w * kChunk + tid] = 0u;
+                while (bits) {
+                    const int c = S.colp[w * 32 + __ffs(bits) - 1];
+                    bits &= bits - 1;
+                    S.U[(c >> 5) * kChunk + tid] |= 1u << (c & 31);
+                }
+            }
+        }
+        c0 = first_fit(S, tid, W, 0u, 0);
+    }
+    S.col[tid] = -1;
+    solve_sync();
     int fixed = 0;  // nets below `fixed` are final
     int rank = 0;
     while (true) {
-        // Jacobi sweeps until the colouring is a fixed point: a net's colour is
-        // the first one neither forbidden by earlier chunks, nor full, nor held
-        // by one of its predecessors in the chunk.
+        // Jacobi sweeps until the colouring is a fixed point.
         while (true) {
-            int mine = tid < m ? col[tid] : -1;
+            int mine = tid < m ? S.col[tid] : -1;
             if (tid < m && tid >= fixed) {
-                int c = 0;
-                while (true) {
-                    int w = c >> 5;
-                    if (w >= W) { c = C; break; }
-                    unsigned used = F[w * kChunk + tid] | full[w] | ((1u << (c & 31)) - 1u);
-                    while (used == 0xffffffffu) {
-                        if (++w >= W) break;
-                        used = F[w * kChunk + tid] | full[w];
-                    }
-                    if (w >= W) { c = C; break; }
-                    c = w * 32 + __ffs(~used) - 1;
-                    bool hit = false;
-                    for (int pw = 0; pw <= (tid >> 5) && !hit; ++pw) {
-                        unsigned bits = P[pw * kChunk + tid];
-                        while (bits) {
-                            const int i = pw * 32 + __ffs(bits) - 1;
-                            bits &= bits - 1;
-                            if (col[i] == c) { hit = true; break; }
-                        }
-                    }
-                    if (!hit) break;
-                    ++c;
-                }
-                if (c >= C) { overflow = 1; c = C - 1; }
-                mine = c;
+                mine = first_fit(S, tid, W, pmask, c0);
+                if (mine >= C) { overflow = 1; mine = C - 1; }
             }
-            __syncthreads();
-            const bool changed = tid < m && col[tid] != mine;
-            if (tid < m) col[tid] = mine;
-            if (!__syncthreads_or(changed)) break;
+            solve_sync();
+            const bool changed = tid < m && S.col[tid] != mine;
+            if (tid < m) S.col[tid] = mine;
+            if (!solve_sync_or(changed)) break;
         }
         if (overflow) break;
-        // Position of every net inside its batch, in chunk order: warps in turn
-        // add their per-colour group sizes to a running count.
-        for (int k = tid; k < C; k += blockDim.x) run[k] = cnt[k];
+        // Position of every net inside its batch, in chunk order: colour
+        // counts of the earlier warps plus the rank inside the own warp.
         if (tid == 0) first_bad = m;
-        __syncthreads();
-        const int c = tid < m ? col[tid] : -1 - lane;  // distinct dummies for idle lanes
+        const int c = tid < m ? S.col[tid] : -1 - lane;  // distinct dummies for idle lanes
         const unsigned peers = __match_any_sync(0xffffffffu, c);
+        const bool leader = tid < m && lane == __ffs(peers) - 1;
         const int within = __popc(peers & ((1u << lane) - 1u));
-        for (int w = 0; w < (m + 31) / 32; ++w) {
-            if (warp == w && tid < m) {
-                rank = run[c] + within;
-                if (lane == __ffs(peers) - 1) run[c] += __popc(peers);
-                if (rank >= B.limit) atomicMin(&first_bad, tid);
+        if (S.per_warp) {
+            if (leader) S.wh[warp * C + c] = __popc(peers);
+            solve_sync();
+            if (tid < m) {
+                int r = S.cnt[c] + within;
+                for (int w = 0; w < warp; ++w) r += S.wh[w * C + c];
+                rank = r;
+                if (r >= B.limit) atomicMin(&first_bad, tid);
             }
-            __syncthreads();
+            solve_sync();
+            if (leader) S.wh[warp * C + c] = 0;
+        } else {
+            for (int k = tid; k < C; k += kChunk) S.wh[k] = S.cnt[k];
+            solve_sync();
+            for (int w = 0; w < (m + 31) / 32; ++w) {
+                if (warp == w && tid < m) {
+                    rank = S.wh[c] + within;
+                    if (leader) S.wh[c] += __popc(peers);
+                    if (rank >= B.limit) atomicMin(&first_bad, tid);
+                }
+                solve_sync();
+            }
         }
         const int bad = first_bad;
         if (bad >= m) {
-            if (tid < m) {
-                B.batch_of[s + tid] = col[tid];
-                B.rank[s + tid] = rank;
-            }
-            for (int k = tid; k < C; k += blockDim.x) cnt[k] = run[k];
-            __syncthreads();
+            if (leader) atomicAdd(S.cnt + c, __popc(peers));
             break;
         }
         // Net `bad` finds its colour full; so does every later net.
-        const int full_colour = col[bad];
-        __syncthreads();
-        if (tid == 0) full[full_colour >> 5] |= 1u << (full_colour & 31);
+        const int fc = S.col[bad];
+        if (tid == 0) S.full[fc >> 5] |= 1u << (fc & 31);
+        if (tid >= bad && tid < m) {
+            S.U[(fc >> 5) * kChunk + tid] |= 1u << (fc & 31);
+            c0 = first_fit(S, tid, W, 0u, c0);
+        }
         fixed = bad;
-        __syncthreads();
+        solve_sync();
     }
     if (overflow) {
         if (tid == 0) batch_error(B, kELimit, s);
-        return;
+        return false;
     }
     int top = 0;
-    if (tid < m) top = col[tid] + 1;
-    for (int k = tid; k < C; k += blockDim.x) B.count[k] = cnt[k];
-    for (int k = tid; k < W; k += blockDim.x) B.fullmask[k] = full[k];
-    if (top) atomicMax(B.n_colors, top);
-}
-
-__host__ __device__ __forceinline__ size_t phase3_smem_bytes(int W) {
-    return size_t(kChunk) * W * 4 + size_t(kChunk) * kChunkWords * 4 + kChunk * 4 + size_t(64) * W * 4 + W * 4;
+    if (tid < m) {
+        const int c = S.col[tid];
+        B.batch_of[s + tid] = c;
+        B.rank[s + tid] = rank;
+        S.colp[tid] = c;
+        top = c + 1;
+    }
+    for (int o = 16; o; o >>= 1) top = max(top, __shfl_xor_sync(0xffffffffu, top, o));
+    if (lane == 0 && top) atomicMax(B.n_colors, top);
+    solve_sync();
+    return true;
 }
 
 }  // namespace grb

@@ -166,44 +166,60 @@ __device__ __forceinline__ unsigned long long global_ns() {
     return t;
 }
 
-__device__ __forceinline__ bool grid_sync(GridSync& s, const Tables& T) {
+// Thread 0 waits until *p >= target: relaxed polls (an acquire load per poll
+// would invalidate the SM's L1 under the warps still working), backing off
+// after the first polls so long waits do not flood the word's L2 slice, then
+// one fence so later reads see the writes that preceded the producers'
+// releases.  Gives up, recording kETimedOut, after timeout_ns; also returns
+// false as soon as any error is recorded when `any_error` is set (the
+// producer may have stopped), else only on a timeout elsewhere.
+__device__ __forceinline__ bool wait_at_least(const unsigned* p, unsigned target, unsigned long long timeout_ns,
+                                              const Tables& T, bool any_error) {
+    unsigned v;
+    asm volatile("ld.relaxed.gpu.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    if (v < target) {
+        const unsigned long long start = global_ns();
+        unsigned spins = 0;
+        while (v < target) {
+            if ((++spins & 63) == 0) {
+                if (global_ns() - start > timeout_ns) { set_error(T, kETimedOut, blockIdx.x); return false; }
+                const int e = *reinterpret_cast<volatile int*>(T.error);
+                if (any_error ? e != 0 : e == kETimedOut) return false;
+            }
+            if (spins > 16) __nanosleep(spins > 256 ? 128 : 32);
+            asm volatile("ld.relaxed.gpu.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+        }
+    }
+    __threadfence();  // acquire: later reads see every producer's writes
+    return true;
+}
+
+// Barrier of `members` blocks (every block of the grid, or a subset that
+// shares the counter); barrier k completes at k * members arrivals.
+__device__ __forceinline__ bool grid_sync_of(GridSync& s, const Tables& T, unsigned members) {
     __shared__ int ok;
-    const unsigned target = (++s.epoch) * gridDim.x;
+    const unsigned target = (++s.epoch) * members;
     __syncthreads();
     if (threadIdx.x == 0) {
-        ok = 1;
         unsigned v;
         __threadfence();
         asm volatile("atom.add.acq_rel.gpu.u32 %0, [%1], 1;" : "=r"(v) : "l"(s.count) : "memory");
-        v += 1;
-        if (v < target) {
-            const unsigned long long start = global_ns();
-            unsigned spins = 0;
-            while (v < target) {
-                if ((++spins & 63) == 0) {
-                    if (global_ns() - start > s.timeout_ns) { set_error(T, kETimedOut, blockIdx.x); ok = 0; break; }
-                    if (*reinterpret_cast<volatile int*>(T.error) == kETimedOut) { ok = 0; break; }
-                }
-                // Relaxed polls (an acquire load per poll would invalidate the
-                // SM's L1 under the warps still working), backing off after the
-                // first polls so long waits do not flood the counter's L2 slice.
-                if (spins > 16) __nanosleep(spins > 256 ? 128 : 32);
-                asm volatile("ld.relaxed.gpu.u32 %0, [%1];" : "=r"(v) : "l"(s.count) : "memory");
-            }
-        }
-        __threadfence();  // acquire: later reads see every block's writes
+        ok = v + 1 >= target ? 1 : wait_at_least(s.count, target, s.timeout_ns, T, false);
+        if (v + 1 >= target) __threadfence();
     }
     __syncthreads();
     return ok != 0;
 }
+__device__ __forceinline__ bool grid_sync(GridSync& s, const Tables& T) { return grid_sync_of(s, T, gridDim.x); }
 
 struct PhaseClock {
     unsigned long long last = 0;
+    int owner = 0;  // the block whose thread 0 records
     __device__ __forceinline__ void start(const GridSync& s) {
-        if (s.phase_ns && blockIdx.x == 0 && threadIdx.x == 0) last = global_ns();
+        if (s.phase_ns && blockIdx.x == owner && threadIdx.x == 0) last = global_ns();
     }
     __device__ __forceinline__ void mark(const GridSync& s, int k) {
-        if (s.phase_ns && blockIdx.x == 0 && threadIdx.x == 0) {
+        if (s.phase_ns && blockIdx.x == owner && threadIdx.x == 0) {
             const unsigned long long now = global_ns();
             s.phase_ns[k] += now - last;
             last = now;

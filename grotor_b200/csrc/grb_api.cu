@@ -31,6 +31,7 @@ constexpr int kRefreshThreads = 256;       // refresh_group needs 8 warps
 constexpr int kPersistentThreads = 256;
 constexpr int kDpThreads = 128;
 constexpr unsigned long long kBarrierTimeoutNs = 20ull * 1000 * 1000 * 1000;
+constexpr int kPhaseSlots = 12;  // grb_phase_times entries
 
 // update_dirty_costs (incremental_update.cuh:62-96): recompute dirty cells.
 __global__ void k_refresh_cells(Tables T) {
@@ -617,67 +618,182 @@ __global__ void k_validate_nets(NetCheck C) {
 }
 
 // --- batching kernels -------------------------------------------------------
-// One net per CTA in the per-net steps (a chunk's nets spread over the grid).
-constexpr int kBatchAcc = 96;  // >= W + kChunkWords for every W phase 3 admits
-__global__ void k_batch_raster(BatchState B, int s) {
-    const NetGroup G{int(threadIdx.x), int(blockDim.x), 0};
-    const int m = min(kChunk, B.n - s);
-    for (int j = blockIdx.x; j < m; j += gridDim.x) batch_raster(B, s, j, G);
+// Flat lists: per-position counts (warp per position), exclusive scans, fill.
+__global__ void k_flat_count(BatchState B, int n_nets) {
+    const int warps = gridDim.x * blockDim.x / 32;
+    for (int p = (blockIdx.x * blockDim.x + threadIdx.x) / 32; p < B.n; p += warps) {
+        const int id = B.order[p];
+        if (id < 0 || id >= n_nets) {  // refused on the host after the scan
+            if ((threadIdx.x & 31) == 0) { batch_error(B, kEInval, p); B.mark_off[p] = 0; B.pt_off[p] = 0; }
+            continue;
+        }
+        flat_count(B, p);
+    }
 }
-__global__ void k_batch_forbid_preds(BatchState B, int s) {
-    __shared__ unsigned acc[kBatchAcc];
-    const NetGroup G{int(threadIdx.x), int(blockDim.x), 0};
-    const int m = min(kChunk, B.n - s);
-    for (int j = blockIdx.x; j < m; j += gridDim.x) batch_forbid_preds(B, s, j, acc, G);
-}
-__global__ void __launch_bounds__(kChunk) k_batch_phase3(BatchState B, int s) {
-    extern __shared__ __align__(16) unsigned bsm[];
-    if (*reinterpret_cast<volatile int*>(B.error)) return;
-    batch_phase3(B, s, bsm);
-}
-__global__ void k_batch_phase4(BatchState B, int s) {
-    const NetGroup G{int(threadIdx.x), int(blockDim.x), 0};
-    const int m = min(kChunk, B.n - s);
-    if (*reinterpret_cast<volatile int*>(B.error)) return;
-    for (int j = blockIdx.x; j < m; j += gridDim.x) batch_phase4(B, s, j, G);
+__global__ void k_flat_fill(BatchState B) {
+    const int warps = gridDim.x * blockDim.x / 32;
+    for (int p = (blockIdx.x * blockDim.x + threadIdx.x) / 32; p < B.n; p += warps) flat_fill(B, p);
 }
 
-// Persistent batching: CTAs of kChunk threads (the in-chunk solve needs one
-// thread per net); the per-net steps use each half CTA as a net group so a
-// chunk's nets fit in one wave.  Per chunk k, three barriers:
-//   forbidden colours + predecessors of k (all groups) |
-//   solve k on CTA 0 while the other CTAs raster chunk k+1 (other buffer) |
-//   publish k (all groups).
-__global__ void __launch_bounds__(kChunk, 2) k_batch_persistent(BatchState B, GridSync S, Tables T) {
+// Exclusive scan of a[0..n) in place with the total at a[n]: tiles of
+// kScanTile, a scan of the tile totals, then the tile offsets added.
+constexpr int kScanTile = 1024;  // 256 threads x 4 elements
+__device__ __forceinline__ long long block_incl_scan(long long v, long long* ws) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (int o = 1; o < 32; o <<= 1) {
+        const long long u = __shfl_up_sync(0xffffffffu, v, o);
+        if (lane >= o) v += u;
+    }
+    if (lane == 31) ws[warp] = v;
+    __syncthreads();
+    if (warp == 0) {
+        long long w = lane < nw ? ws[lane] : 0;
+        for (int o = 1; o < 32; o <<= 1) {
+            const long long u = __shfl_up_sync(0xffffffffu, w, o);
+            if (lane >= o) w += u;
+        }
+        if (lane < nw) ws[lane] = w;
+    }
+    __syncthreads();
+    const long long r = v + (warp ? ws[warp - 1] : 0);
+    __syncthreads();  // ws is reused by the next call
+    return r;
+}
+__global__ void __launch_bounds__(256) k_scan_tiles(long long* a, int n, long long* sums) {
+    __shared__ long long ws[32];
+    const long long base = blockIdx.x * (long long)kScanTile + threadIdx.x * 4;
+    long long v[4], t = 0;
+    for (int k = 0; k < 4; ++k) {
+        v[k] = base + k < n ? a[base + k] : 0;
+        t += v[k];
+    }
+    long long run = block_incl_scan(t, ws) - t;
+    for (int k = 0; k < 4; ++k) {
+        if (base + k < n) a[base + k] = run;
+        run += v[k];
+    }
+    if (threadIdx.x == blockDim.x - 1) sums[blockIdx.x] = run;
+}
+__global__ void __launch_bounds__(1024) k_scan_sums(long long* sums, int tiles) {
+    __shared__ long long ws[32];
+    __shared__ long long total;
+    long long carry = 0;
+    for (int base = 0; base < tiles; base += blockDim.x) {
+        const int i = base + threadIdx.x;
+        const long long v = i < tiles ? sums[i] : 0;
+        const long long incl = block_incl_scan(v, ws);
+        if (i < tiles) sums[i] = carry + incl - v;
+        if (threadIdx.x == blockDim.x - 1) total = incl;
+        __syncthreads();
+        carry += total;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) sums[tiles] = carry;
+}
+__global__ void k_scan_add(long long* a, int n, const long long* sums, int tiles) {
+    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i < n) a[i] += sums[i / kScanTile];
+    if (i == 0) a[n] = sums[tiles];
+}
+
+// Plain form: one launch per step and chunk.
+__global__ void k_batch_raster(BatchState B, int s) {
+    batch_raster(B, s, blockIdx.x * (long long)blockDim.x + threadIdx.x, (long long)gridDim.x * blockDim.x);
+}
+__global__ void k_batch_gather(BatchState B, int s) {
+    batch_gather(B, s, false, blockIdx.x * (long long)blockDim.x + threadIdx.x, (long long)gridDim.x * blockDim.x);
+}
+__global__ void __launch_bounds__(kChunk) k_batch_solve(BatchState B, int s) {
     extern __shared__ __align__(16) unsigned bsm[];
-    __shared__ unsigned acc[2][kBatchAcc];
-    constexpr int kHalf = kChunk / 2;
-    const int half = threadIdx.x / kHalf;
-    const NetGroup G{int(threadIdx.x % kHalf), kHalf, 1 + half};
-    const int gi = half * gridDim.x + blockIdx.x, ng = 2 * gridDim.x;
-    // Raster groups of the overlapped step: every CTA but the solving one.
-    const bool solo = gridDim.x == 1;
-    const int rgi = solo ? gi : half * (gridDim.x - 1) + blockIdx.x - 1, rng = solo ? ng : 2 * (gridDim.x - 1);
-    PhaseClock clk;
+    if (*reinterpret_cast<volatile int*>(B.error)) return;
+    const SolveSmem S = solve_smem(bsm, B.W);
+    const int C = 32 * B.W;
+    for (int k = threadIdx.x; k < C; k += blockDim.x) S.cnt[k] = B.count[k];
+    if (S.per_warp)
+        for (int k = threadIdx.x; k < (kChunk / 32) * C; k += blockDim.x) S.wh[k] = 0;
+    for (int k = threadIdx.x; k < B.W; k += blockDim.x) S.full[k] = B.fullmask[k];
+    __syncthreads();
+    if (!batch_solve(B, s, false, S)) return;
+    for (int k = threadIdx.x; k < C; k += blockDim.x) B.count[k] = S.cnt[k];
+    for (int k = threadIdx.x; k < B.W; k += blockDim.x) B.fullmask[k] = S.full[k];
+}
+__global__ void k_batch_publish(BatchState B, int s) {
+    if (*reinterpret_cast<volatile int*>(B.error)) return;
+    batch_publish(B, s, blockIdx.x * (long long)blockDim.x + threadIdx.x, (long long)gridDim.x * blockDim.x);
+}
+
+// Persistent batching: CTAs of kPersistThreads threads, one per SM, at least
+// two.  CTA 0 is the solver and has its SM to itself (its first kChunk
+// threads solve, the rest leave): for chunk r it waits until the other CTAs
+// (G of them, one shared barrier counter) have gathered chunk r, solves it,
+// and releases `solved` = r + 1.  The other CTAs run, per round r:
+//   A: wait for chunk r-1's colours, publish chunk r-1         | barrier
+//   B: gather chunk r+1 (cellmask as of chunk r-1, chunk r
+//      through the previous-chunk bits)                        | barrier
+//   C: raster chunk r+2 (its buffer was cleared in A)
+// The barrier after B(r) is what the solver waits for before chunk r+1
+// (counter (2 + 2(r+1)) * G); C overlaps the solve of chunk r.
+constexpr int kPersistThreads = 2 * kChunk;
+__global__ void __launch_bounds__(kPersistThreads, 1) k_batch_persistent(BatchState B, GridSync S, Tables T) {
+    extern __shared__ __align__(16) unsigned bsm[];
+    __shared__ int go;
+    const int chunks = (B.n + kChunk - 1) / kChunk;
+    const unsigned G = gridDim.x - 1;
+    if (blockIdx.x == 0) {
+        if (threadIdx.x >= kChunk) return;
+        PhaseClock clk{0, 0};
+        clk.start(S);
+        const SolveSmem M = solve_smem(bsm, B.W);
+        const int C = 32 * B.W;
+        for (int k = threadIdx.x; k < C; k += kChunk) M.cnt[k] = B.count[k];
+        if (M.per_warp)
+            for (int k = threadIdx.x; k < (kChunk / 32) * C; k += kChunk) M.wh[k] = 0;
+        for (int k = threadIdx.x; k < B.W; k += kChunk) M.full[k] = B.fullmask[k];
+        for (int r = 0; r < chunks; ++r) {
+            if (threadIdx.x == 0) go = wait_at_least(S.count, (2u + 2u * r) * G, S.timeout_ns, T, true);
+            solve_sync();
+            if (!go) return;
+            clk.mark(S, 8);
+            if (!batch_solve(B, r * kChunk, r > 0, M)) return;
+            __threadfence();
+            solve_sync();
+            if (threadIdx.x == 0) asm volatile("st.release.gpu.u32 [%0], %1;" ::"l"(B.solved), "r"(unsigned(r + 1)) : "memory");
+            clk.mark(S, 2);
+        }
+        for (int k = threadIdx.x; k < C; k += kChunk) B.count[k] = M.cnt[k];
+        for (int k = threadIdx.x; k < B.W; k += kChunk) B.fullmask[k] = M.full[k];
+        return;
+    }
+    PhaseClock clk{0, 1};
     clk.start(S);
-    for (int j = gi; j < min(kChunk, B.n); j += ng) batch_raster(B, 0, j, G);
-    if (!grid_sync(S, T)) return;
-    clk.mark(S, 0);
-    for (int s = 0; s < B.n; s += kChunk) {
-        const int m = min(kChunk, B.n - s);
-        for (int j = gi; j < m; j += ng) batch_forbid_preds(B, s, j, acc[half], G);
-        if (!grid_sync(S, T)) return;
+    const long long t = (blockIdx.x - 1) * (long long)blockDim.x + threadIdx.x, nt = (long long)G * blockDim.x;
+    batch_raster(B, 0, t, nt);
+    if (chunks > 1) batch_raster(B, kChunk, t, nt);
+    if (!grid_sync_of(S, T, G)) return;
+    batch_gather(B, 0, false, t, nt);
+    if (!grid_sync_of(S, T, G)) return;
+    clk.mark(S, 1);
+    for (int r = 0; r < chunks; ++r) {
+        if (r >= 1) {
+            if (threadIdx.x == 0) go = wait_at_least(B.solved, unsigned(r), S.timeout_ns, T, true);
+            __syncthreads();
+            if (!go) return;
+            clk.mark(S, 9);
+            batch_publish(B, (r - 1) * kChunk, t, nt);
+        }
+        if (!grid_sync_of(S, T, G)) return;
+        clk.mark(S, 0);
+        if (r + 1 < chunks) batch_gather(B, (r + 1) * kChunk, true, t, nt);
+        if (!grid_sync_of(S, T, G)) return;
         clk.mark(S, 1);
-        const int s2 = s + kChunk, m2 = s2 < B.n ? min(kChunk, B.n - s2) : 0;
-        if (blockIdx.x == 0) batch_phase3(B, s, bsm);
-        if (blockIdx.x != 0 || solo)
-            for (int j = rgi; j < m2; j += rng) batch_raster(B, s2, j, G);
-        if (!grid_sync(S, T)) return;
-        clk.mark(S, 2);
-        if (*reinterpret_cast<volatile int*>(B.error)) return;
-        for (int j = gi; j < m; j += ng) batch_phase4(B, s, j, G);
-        if (!grid_sync(S, T)) return;
-        clk.mark(S, 3);
+        if (r + 2 < chunks) batch_raster(B, (r + 2) * kChunk, t, nt);
+        clk.mark(S, 10);
+    }
+    if (chunks > 0) {
+        if (threadIdx.x == 0) go = wait_at_least(B.solved, unsigned(chunks), S.timeout_ns, T, true);
+        __syncthreads();
+        if (!go) return;
+        batch_publish(B, (chunks - 1) * kChunk, t, nt);
     }
 }
 
@@ -825,10 +941,17 @@ struct grb_ctx {
     int work_cap = 0;
     unsigned* sync = nullptr;   // [count, generation]
     // batching buffers
-    unsigned *cellmask = nullptr, *localmask = nullptr, *localmask2 = nullptr, *fmask = nullptr, *pred = nullptr,
-             *fullmask = nullptr;
+    unsigned *cellmask = nullptr, *fmask = nullptr, *fullmask = nullptr;
+    unsigned* lmask[3] = {nullptr, nullptr, nullptr};  // chunk-local masks
+    unsigned *pred = nullptr, *prevp = nullptr, *bsolved = nullptr;
+    bool lmask_dirty = false;          // a run stopped before clearing them
     int *bcount = nullptr, *ncolors = nullptr, *batch_of = nullptr, *brank = nullptr, *order = nullptr;
     int bW = 0, bn_cap = 0;
+    // flat mark / query-point lists by order position
+    long long *mark_off = nullptr, *pt_off = nullptr, *scan_sums = nullptr;
+    unsigned *mark_cell = nullptr, *pt_cell = nullptr;
+    unsigned short *mark_jj = nullptr, *pt_jj = nullptr;
+    long long mark_cap = 0, pt_cap = 0;
     // FLT stage (grb_upload_geometry / grb_upload_flt)
     std::vector<void*> geom_bufs;     // batching geometry replacing the uploaded one
     std::vector<void*> flt_bufs;
@@ -871,8 +994,8 @@ struct grb_ctx {
     // timing
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     bool profiling = false;
-    unsigned long long* d_phase = nullptr;     // [8] persistent-kernel phase clocks
-    double phase_ms[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    unsigned long long* d_phase = nullptr;     // [kPhaseSlots] persistent-kernel phase clocks
+    double phase_ms[kPhaseSlots] = {};
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev_pool;
     std::vector<int> ev_slot;                  // phase slot of each recorded pair
     size_t ev_used = 0;
@@ -1022,9 +1145,9 @@ int prof_collect(grb_ctx* c) {
     }
     c->ev_used = 0;
     if (c->d_phase) {
-        unsigned long long ns[8];
+        unsigned long long ns[kPhaseSlots];
         GRB_CUDA(c, cudaMemcpy(ns, c->d_phase, sizeof(ns), cudaMemcpyDeviceToHost));
-        for (int k = 0; k < 8; ++k) c->phase_ms[k] += ns[k] * 1e-6;
+        for (int k = 0; k < kPhaseSlots; ++k) c->phase_ms[k] += ns[k] * 1e-6;
         GRB_CUDA(c, cudaMemset(c->d_phase, 0, sizeof(ns)));
     }
     return GRB_OK;
@@ -1521,7 +1644,7 @@ int grb_create(const grb_grid* g, int32_t device, grb_ctx** out) {
     GRB_CUDA(cp, cudaMemcpy(yl, g->y_edge_len, sizeof(int) * (T.Y - 1), cudaMemcpyHostToDevice));
     GRB_CUDA(cp, cudaMemcpy(cap, g->capacity, sizeof(float) * cells, cudaMemcpyHostToDevice));
     GRB_CUDA(cp, cudaMemset(T.error, 0, 2 * sizeof(int)));
-    GRB_CUDA(cp, cudaFuncSetAttribute(k_batch_phase3, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    GRB_CUDA(cp, cudaFuncSetAttribute(k_batch_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
     GRB_CUDA(cp, cudaFuncSetAttribute(k_batch_persistent, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
     GRB_CUDA(cp, cudaFuncSetAttribute(k_lshape_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
     GRB_CUDA(cp, cudaFuncSetAttribute(k_lshape_bucketed, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
@@ -1547,8 +1670,10 @@ void grb_destroy(grb_ctx* c) {
     free_all(c->flt_bufs);
     free_all(c->owned);
     for (void* p : {(void*)c->check, (void*)c->bucket_ids, (void*)c->bucket_off, (void*)c->ids, (void*)c->batch_off, (void*)c->gscratch, (void*)c->work, (void*)c->cellmask,
-                    (void*)c->localmask, (void*)c->localmask2, (void*)c->fmask, (void*)c->pred, (void*)c->fullmask, (void*)c->bcount,
-                    (void*)c->ncolors, (void*)c->batch_of, (void*)c->brank, (void*)c->order})
+                    (void*)c->lmask[0], (void*)c->lmask[1], (void*)c->lmask[2], (void*)c->fmask, (void*)c->pred, (void*)c->prevp,
+                    (void*)c->bsolved, (void*)c->fullmask, (void*)c->bcount, (void*)c->ncolors, (void*)c->batch_of, (void*)c->brank,
+                    (void*)c->order, (void*)c->mark_off, (void*)c->pt_off, (void*)c->scan_sums, (void*)c->mark_cell,
+                    (void*)c->pt_cell, (void*)c->mark_jj, (void*)c->pt_jj})
         if (p) cudaFree(p);
     if (c->ev0) cudaEventDestroy(c->ev0);
     if (c->ev1) cudaEventDestroy(c->ev1);
@@ -2012,74 +2137,156 @@ int grb_get_plan(grb_ctx* c, int32_t* ids, int32_t* batch_off, int32_t* n, int32
     return GRB_OK;
 }
 
-int grb_plan_batches(grb_ctx* c, const int32_t* order, int32_t n, int32_t limit, int32_t sparsity, int32_t mode,
-                     int32_t* batch_of, int32_t* n_batches) {
-    if (!c || n < 0 || limit < 1 || sparsity < 1 || (n && !order)) return c ? fail(c, GRB_EINVAL, "bad batching arguments") : GRB_EINVAL;
-    GRB_CUDA(c, cudaSetDevice(c->device));
-    for (int i = 0; i < n; ++i)
-        if (order[i] < 0 || order[i] >= c->n_nets) return fail(c, GRB_EINVAL, "net id out of range");
-    const size_t xy = size_t(c->T.XY);
-    int W = std::max(c->bW, 8);
-    int rc = ensure_plan_capacity(c, n, n);
-    if (rc) return rc;
+// Copies the order and builds its flat mark and query-point lists
+// (k_flat_count, two scans, k_flat_fill); refuses net ids outside the
+// uploaded nets.
+static int build_flat_lists(grb_ctx* c, const int32_t* order, BatchState& B) {
+    const int n = B.n;
+    const int tiles = (n + kScanTile - 1) / kScanTile;
     if (c->bn_cap < n || !c->order) {
-        for (int** p : {&c->batch_of, &c->brank, &c->order}) { if (*p) cudaFree(*p); *p = nullptr; }
+        for (void** p : {(void**)&c->batch_of, (void**)&c->brank, (void**)&c->order, (void**)&c->mark_off,
+                         (void**)&c->pt_off, (void**)&c->scan_sums}) {
+            if (*p) cudaFree(*p);
+            *p = nullptr;
+        }
+        c->bn_cap = 0;
         const size_t m = std::max(n, 1);
-        if (cudaMalloc(&c->batch_of, 4 * m) || cudaMalloc(&c->brank, 4 * m) || cudaMalloc(&c->order, 4 * m)) {
+        const size_t t = size_t(tiles) + 1;
+        if (cudaMalloc(&c->batch_of, 4 * m) || cudaMalloc(&c->brank, 4 * m) || cudaMalloc(&c->order, 4 * m) ||
+            cudaMalloc(&c->mark_off, 8 * (m + 1)) || cudaMalloc(&c->pt_off, 8 * (m + 1)) ||
+            cudaMalloc(&c->scan_sums, 16 * t)) {
             cudaGetLastError();
             return fail(c, GRB_ENOMEM, "batching buffers");
         }
         c->bn_cap = n;
     }
-    if (!c->localmask) {
-        if (cudaMalloc(&c->localmask, xy * kChunkWords * 4) || cudaMalloc(&c->localmask2, xy * kChunkWords * 4) ||
-            cudaMalloc(&c->pred, size_t(kChunk) * kChunkWords * 4) ||
+    if (n) GRB_CUDA(c, cudaMemcpyAsync(c->order, order, sizeof(int) * n, cudaMemcpyHostToDevice, c->stream));
+    B.order = c->order;
+    B.batch_of = c->batch_of;
+    B.rank = c->brank;
+    B.mark_off = c->mark_off;
+    B.pt_off = c->pt_off;
+    const int grid = c->sms * 8;
+    if (n) k_flat_count<<<grid, 256, 0, c->stream>>>(B, c->n_nets);
+    long long* sums[2] = {c->scan_sums, c->scan_sums + tiles + 1};
+    long long* arr[2] = {c->mark_off, c->pt_off};
+    for (int k = 0; k < 2; ++k) {
+        if (n) k_scan_tiles<<<tiles, 256, 0, c->stream>>>(arr[k], n, sums[k]);
+        k_scan_sums<<<1, 1024, 0, c->stream>>>(sums[k], tiles);
+        k_scan_add<<<n / 256 + 1, 256, 0, c->stream>>>(arr[k], n, sums[k], tiles);
+    }
+    c->launches += (n ? 1 : 0) + 2 * (n ? 3 : 2);
+    GRB_CUDA(c, cudaGetLastError());
+    long long tot[2] = {0, 0};
+    int err[2] = {0, 0};
+    GRB_CUDA(c, cudaMemcpyAsync(tot, c->mark_off + n, 8, cudaMemcpyDeviceToHost, c->stream));
+    GRB_CUDA(c, cudaMemcpyAsync(tot + 1, c->pt_off + n, 8, cudaMemcpyDeviceToHost, c->stream));
+    GRB_CUDA(c, cudaMemcpyAsync(err, c->T.error, 2 * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    GRB_CUDA(c, cudaStreamSynchronize(c->stream));
+    if (err[0] == kEInval) {
+        GRB_CUDA(c, cudaMemsetAsync(c->T.error, 0, 2 * sizeof(int), c->stream));
+        GRB_CUDA(c, cudaStreamSynchronize(c->stream));
+        return fail(c, GRB_EINVAL, "net id out of range (order position " + std::to_string(err[1]) + ")");
+    }
+    if (err[0]) return check_device_error(c);
+    auto grow = [&](long long need, long long& cap, unsigned*& cell, unsigned short*& jj) {
+        if (need <= cap) return true;
+        if (cell) cudaFree(cell);
+        if (jj) cudaFree(jj);
+        cell = nullptr;
+        jj = nullptr;
+        cap = 0;
+        const long long want = need + need / 8 + 1024;
+        if (cudaMalloc(&cell, 4 * size_t(want)) || cudaMalloc(&jj, 2 * size_t(want))) {
+            cudaGetLastError();
+            return false;
+        }
+        cap = want;
+        return true;
+    };
+    if (!grow(tot[0], c->mark_cap, c->mark_cell, c->mark_jj) || !grow(tot[1], c->pt_cap, c->pt_cell, c->pt_jj))
+        return fail(c, GRB_ENOMEM, "batching mark lists");
+    B.mark_cell = c->mark_cell; B.mark_jj = c->mark_jj;
+    B.pt_cell = c->pt_cell; B.pt_jj = c->pt_jj;
+    if (n) {
+        k_flat_fill<<<grid, 256, 0, c->stream>>>(B);
+        c->launches += 1;
+        GRB_CUDA(c, cudaGetLastError());
+    }
+    return GRB_OK;
+}
+
+int grb_plan_batches(grb_ctx* c, const int32_t* order, int32_t n, int32_t limit, int32_t sparsity, int32_t mode,
+                     int32_t* batch_of, int32_t* n_batches) {
+    if (!c || n < 0 || limit < 1 || sparsity < 1 || (n && !order)) return c ? fail(c, GRB_EINVAL, "bad batching arguments") : GRB_EINVAL;
+    if (mode != GRB_MODE_PLAIN && mode != GRB_MODE_GRAPH && mode != GRB_MODE_PERSISTENT)
+        return fail(c, GRB_EINVAL, "unknown mode");
+    GRB_CUDA(c, cudaSetDevice(c->device));
+    const size_t xy = size_t(c->T.XY);
+    const size_t lm_bytes = xy * kChunkWords * 4;
+    const size_t pq_bytes = 2 * size_t(kChunk) * kChunkWords * 4;
+    int W = std::max(c->bW, 8);
+    int rc = ensure_plan_capacity(c, n, n);
+    if (rc) return rc;
+    if (!c->lmask[0]) {
+        if (cudaMalloc(&c->lmask[0], lm_bytes) || cudaMalloc(&c->lmask[1], lm_bytes) || cudaMalloc(&c->lmask[2], lm_bytes) ||
+            cudaMalloc(&c->pred, pq_bytes) || cudaMalloc(&c->prevp, pq_bytes) || cudaMalloc(&c->bsolved, 4) ||
             cudaMalloc(&c->ncolors, 4)) {
             cudaGetLastError();
             return fail(c, GRB_ENOMEM, "batching buffers");
         }
-        GRB_CUDA(c, cudaMemsetAsync(c->localmask, 0, xy * kChunkWords * 4, c->stream));
-        GRB_CUDA(c, cudaMemsetAsync(c->localmask2, 0, xy * kChunkWords * 4, c->stream));
+        c->lmask_dirty = true;
     }
-    GRB_CUDA(c, cudaMemcpyAsync(c->order, order, sizeof(int) * n, cudaMemcpyHostToDevice, c->stream));
+    BatchState B{};
+    B.X = c->T.X; B.Y = c->T.Y; B.n = n; B.limit = limit; B.sparsity = sparsity;
+    B.point_off = c->point_off; B.points = c->points;
+    B.hseg_off = c->hseg_off; B.hsegs = c->hsegs; B.vseg_off = c->vseg_off; B.vsegs = c->vsegs;
+    B.error = c->T.error; B.error_info = c->T.error_info;
     GRB_CUDA(c, cudaEventRecord(c->ev0, c->stream));
+    if ((rc = build_flat_lists(c, order, B))) return rc;
     for (int attempt = 0; attempt < 6; ++attempt) {
         if (W != c->bW || !c->cellmask) {
             for (unsigned** p : {&c->cellmask, &c->fmask, &c->fullmask}) { if (*p) cudaFree(*p); *p = nullptr; }
             if (c->bcount) cudaFree(c->bcount);
             c->bcount = nullptr;
-            if (cudaMalloc(&c->cellmask, xy * W * 4) || cudaMalloc(&c->fmask, size_t(kChunk) * W * 4) ||
+            c->bW = 0;
+            if (cudaMalloc(&c->cellmask, xy * W * 4) || cudaMalloc(&c->fmask, 2 * size_t(kChunk) * W * 4) ||
                 cudaMalloc(&c->fullmask, W * 4) || cudaMalloc(&c->bcount, size_t(32) * W * 4)) {
                 cudaGetLastError();
                 return fail(c, GRB_ENOMEM, "colour masks");
             }
             c->bW = W;
         }
+        const size_t smem = solve_smem_bytes(W);
+        if (smem > 200 * 1024) return fail(c, GRB_ELIMIT, "too many batch colours");
+        if (c->lmask_dirty) {
+            for (unsigned* lm : c->lmask) GRB_CUDA(c, cudaMemsetAsync(lm, 0, lm_bytes, c->stream));
+            c->lmask_dirty = false;
+        }
         GRB_CUDA(c, cudaMemsetAsync(c->cellmask, 0, xy * W * 4, c->stream));
+        GRB_CUDA(c, cudaMemsetAsync(c->fmask, 0, 2 * size_t(kChunk) * W * 4, c->stream));
+        GRB_CUDA(c, cudaMemsetAsync(c->pred, 0, pq_bytes, c->stream));
+        GRB_CUDA(c, cudaMemsetAsync(c->prevp, 0, pq_bytes, c->stream));
         GRB_CUDA(c, cudaMemsetAsync(c->fullmask, 0, W * 4, c->stream));
         GRB_CUDA(c, cudaMemsetAsync(c->bcount, 0, size_t(32) * W * 4, c->stream));
         GRB_CUDA(c, cudaMemsetAsync(c->ncolors, 0, 4, c->stream));
-        BatchState B{};
-        B.X = c->T.X; B.Y = c->T.Y; B.n = n; B.limit = limit; B.sparsity = sparsity; B.W = W;
-        B.order = c->order;
-        B.point_off = c->point_off; B.points = c->points;
-        B.hseg_off = c->hseg_off; B.hsegs = c->hsegs; B.vseg_off = c->vseg_off; B.vsegs = c->vsegs;
-        B.cellmask = c->cellmask; B.localmask = c->localmask; B.localmask2 = c->localmask2;
-        B.fmask = c->fmask; B.pred = c->pred;
+        GRB_CUDA(c, cudaMemsetAsync(c->bsolved, 0, 4, c->stream));
+        B.W = W;
+        B.cellmask = c->cellmask;
+        for (int k = 0; k < 3; ++k) B.localmask[k] = c->lmask[k];
+        B.fmask = c->fmask; B.pred = c->pred; B.prevp = c->prevp;
         B.fullmask = c->fullmask; B.count = c->bcount; B.n_colors = c->ncolors;
-        B.batch_of = c->batch_of; B.rank = c->brank;
-        B.error = c->T.error; B.error_info = c->T.error_info;
-        const size_t smem = phase3_smem_bytes(W);
-        if (smem > 200 * 1024 || W + kChunkWords > kBatchAcc) return fail(c, GRB_ELIMIT, "too many batch colours");
-        if (mode == GRB_MODE_PERSISTENT) {
-            int per_sm = 0;
-            GRB_CUDA(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_persistent, kChunk, smem));
-            if (per_sm < 1) return fail(c, GRB_EINVAL, "batching kernel does not fit on an SM");
+        B.solved = c->bsolved;
+        c->lmask_dirty = true;  // until the run completes
+        int per_sm = 0;
+        if (mode == GRB_MODE_PERSISTENT)
+            GRB_CUDA(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_persistent, kPersistThreads, smem));
+        if (mode == GRB_MODE_PERSISTENT && per_sm * c->sms >= 2) {
             GRB_CUDA(c, cudaMemsetAsync(c->sync, 0, 2 * sizeof(unsigned), c->stream));
-            GridSync S{c->sync, c->sync + 1, kBarrierTimeoutNs, c->profiling ? c->d_phase : nullptr};
+            GridSync S{c->sync, c->sync + 1, kBarrierTimeoutNs, c->profiling ? c->d_phase : nullptr, 0};
             Tables T = c->T;
             void* args[] = {&B, &S, &T};
-            GRB_CUDA(c, cudaLaunchCooperativeKernel((void*)k_batch_persistent, dim3(per_sm * c->sms), dim3(kChunk), args, smem, c->stream));
+            GRB_CUDA(c, cudaLaunchCooperativeKernel((void*)k_batch_persistent, dim3(per_sm * c->sms), dim3(kPersistThreads), args, smem, c->stream));
             c->launches += 1;
         } else {
             const int grid = c->sms * 4;
@@ -2089,13 +2296,13 @@ int grb_plan_batches(grb_ctx* c, const int32_t* order, int32_t n, int32_t limit,
                 k_batch_raster<<<grid, 256, 0, c->stream>>>(B, s);
                 prof_end(c, e);
                 if ((rc = prof_begin(c, 1, &e))) return rc;
-                k_batch_forbid_preds<<<grid, 256, 0, c->stream>>>(B, s);
+                k_batch_gather<<<grid, 256, 0, c->stream>>>(B, s);
                 prof_end(c, e);
                 if ((rc = prof_begin(c, 2, &e))) return rc;
-                k_batch_phase3<<<1, kChunk, smem, c->stream>>>(B, s);
+                k_batch_solve<<<1, kChunk, smem, c->stream>>>(B, s);
                 prof_end(c, e);
                 if ((rc = prof_begin(c, 3, &e))) return rc;
-                k_batch_phase4<<<grid, 256, 0, c->stream>>>(B, s);
+                k_batch_publish<<<grid, 256, 0, c->stream>>>(B, s);
                 prof_end(c, e);
                 c->launches += 4;
             }
@@ -2105,14 +2312,14 @@ int grb_plan_batches(grb_ctx* c, const int32_t* order, int32_t n, int32_t limit,
         GRB_CUDA(c, cudaMemcpyAsync(err, c->T.error, 2 * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
         GRB_CUDA(c, cudaStreamSynchronize(c->stream));
         if (err[0] == kELimit) {
-            // Not enough colour words: clear the chunk-local masks and retry wider.
+            // Not enough colour words: retry wider (the chunk-local masks are
+            // cleared at the start of the retry).
             GRB_CUDA(c, cudaMemsetAsync(c->T.error, 0, 2 * sizeof(int), c->stream));
-            GRB_CUDA(c, cudaMemsetAsync(c->localmask, 0, xy * kChunkWords * 4, c->stream));
-            GRB_CUDA(c, cudaMemsetAsync(c->localmask2, 0, xy * kChunkWords * 4, c->stream));
             W *= 2;
             continue;
         }
         if (err[0]) return check_device_error(c);
+        c->lmask_dirty = false;
         int nb = 0;
         GRB_CUDA(c, cudaMemcpy(&nb, c->ncolors, 4, cudaMemcpyDeviceToHost));
         k_plan_offsets<<<1, 1, 0, c->stream>>>(B, c->batch_off);
@@ -2512,11 +2719,11 @@ int grb_set_profiling(grb_ctx* c, int32_t on) {
     if (!c) return GRB_EINVAL;
     GRB_CUDA(c, cudaSetDevice(c->device));
     if (on && !c->d_phase) {
-        if (cudaMalloc(&c->d_phase, 8 * sizeof(unsigned long long)) != cudaSuccess) {
+        if (cudaMalloc(&c->d_phase, kPhaseSlots * sizeof(unsigned long long)) != cudaSuccess) {
             cudaGetLastError();
             return fail(c, GRB_ENOMEM, "profiling buffer");
         }
-        GRB_CUDA(c, cudaMemset(c->d_phase, 0, 8 * sizeof(unsigned long long)));
+        GRB_CUDA(c, cudaMemset(c->d_phase, 0, kPhaseSlots * sizeof(unsigned long long)));
     }
     c->profiling = on != 0;
     return GRB_OK;
@@ -2524,7 +2731,7 @@ int grb_set_profiling(grb_ctx* c, int32_t on) {
 
 int grb_phase_times(grb_ctx* c, double* ms, int32_t n, int32_t reset) {
     if (!c || !ms || n < 0) return GRB_EINVAL;
-    for (int k = 0; k < n && k < 8; ++k) ms[k] = c->phase_ms[k];
+    for (int k = 0; k < n && k < kPhaseSlots; ++k) ms[k] = c->phase_ms[k];
     if (reset) for (double& v : c->phase_ms) v = 0;
     return GRB_OK;
 }

@@ -301,15 +301,18 @@ class Router:
         self._check(self._lib.grb_get_stats(self._ctx, C.byref(st)))
         return _stats_dict(st)
 
-    PHASES = ("batch_forbid_raster", "batch_preds", "batch_solve", "batch_publish", "refresh_cells", "dp", "commit",
-              "refresh_prefix")
+    # Batching: plain form raster / gather / solve / publish; persistent form
+    # publish / gather / solve, plus the waits and the raster it overlaps
+    # with the solve.  L-shape stage: the next four.
+    PHASES = ("batch_raster", "batch_gather", "batch_solve", "batch_publish", "refresh_cells", "dp", "commit",
+              "refresh_prefix", "batch_solver_wait", "batch_worker_wait", "batch_raster_overlap", "unused")
 
     def set_profiling(self, on: bool = True):
         self._check(self._lib.grb_set_profiling(self._ctx, int(bool(on))))
 
     def phase_times(self, reset: bool = True) -> dict:
-        out = np.zeros(8, np.float64)
-        self._check(self._lib.grb_phase_times(self._ctx, _p(out), 8, int(reset)))
+        out = np.zeros(len(self.PHASES), np.float64)
+        self._check(self._lib.grb_phase_times(self._ctx, _p(out), len(out), int(reset)))
         return dict(zip(self.PHASES, out.tolist()))
 
     def sync(self):
