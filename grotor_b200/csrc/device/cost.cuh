@@ -29,22 +29,47 @@ __device__ __forceinline__ double of_cost_scaled(double scale, float capacity, f
     return 0;
 }
 
-__device__ __forceinline__ double incremental_of_cost(const Tables& T, int c, int l, double incre) {
-    const float cap = T.capacity[c];
-    const float dem = static_cast<float>(T.demand[c]) * 0.5f;
+// Overflow-cost increment of adding `incre` to a cell with capacity cap and
+// demand dem_half half-units, on a layer with overflow weight sc.
+__device__ __forceinline__ double incremental_of_cost(double scale, float cap, int dem_half, double sc,
+                                                      double incre) {
+    const float dem = static_cast<float>(dem_half) * 0.5f;
     const float with = static_cast<float>(static_cast<double>(dem) + incre + 0.0);
     const float without = static_cast<float>(static_cast<double>(dem) + 0.0);
-    return fmin(1e12, (of_cost_scaled(T.of_scale, cap, with) - of_cost_scaled(T.of_scale, cap, without)) *
-                          T.short_costs[l]);
+    return fmin(1e12, (of_cost_scaled(scale, cap, with) - of_cost_scaled(scale, cap, without)) * sc);
+}
+
+// What the costs of cell c depend on: its capacity and demand, those of the
+// previous cell along its track, its edge length and its layer's weight.
+struct CellInputs {
+    float cap0, cap1;
+    int dem0, dem1;
+    int pos, len, elen;
+    double sc;
+};
+
+__device__ __forceinline__ CellInputs load_cell(const Tables& T, int c) {
+    CellInputs in;
+    const int l = c / T.XY, rem = c - l * T.XY, x = rem / T.Y, y = rem - x * T.Y;
+    const bool ay = along_y(T, l);
+    const int stride = ay ? 1 : T.Y;
+    in.pos = ay ? y : x;
+    in.len = ay ? T.Y : T.X;
+    in.cap0 = T.capacity[c];
+    in.dem0 = T.demand[c];
+    in.cap1 = in.pos > 0 ? T.capacity[c - stride] : 0.f;
+    in.dem1 = in.pos > 0 ? T.demand[c - stride] : 0;
+    in.elen = in.pos < in.len - 1 ? (ay ? T.ylen[in.pos] : T.xlen[in.pos]) : 0;
+    in.sc = T.short_costs[l];
+    return in;
 }
 
 // update_single_wcost_ispd24 (full_update.cuh:34-51); the length term is the
 // fused multiply-add the compiler forms for `w += unit * len`.
-__device__ __forceinline__ float wire_cost_at(const Tables& T, int c) {
-    const int l = c / T.XY, rem = c - l * T.XY, x = rem / T.Y, y = rem - x * T.Y;
-    float w = static_cast<float>(incremental_of_cost(T, c, l, 1.0));
-    if (!along_y(T, l) && x < T.X - 1) w = static_cast<float>(fma(T.unit_wire, static_cast<double>(T.xlen[x]), static_cast<double>(w)));
-    if (along_y(T, l) && y < T.Y - 1) w = static_cast<float>(fma(T.unit_wire, static_cast<double>(T.ylen[y]), static_cast<double>(w)));
+__device__ __forceinline__ float wire_cost_of(const Tables& T, const CellInputs& in) {
+    float w = static_cast<float>(incremental_of_cost(T.of_scale, in.cap0, in.dem0, in.sc, 1.0));
+    if (in.pos < in.len - 1)
+        w = static_cast<float>(fma(T.unit_wire, static_cast<double>(in.elen), static_cast<double>(w)));
     // The GGR build keeps integer DP edges non-negative and below its sentinel
     // (full_update.cuh:47-50).
     if (T.int_wire) w = static_cast<float>(static_cast<long long>(fminf(fmaxf(w, 0.f), 1.e7f)));
@@ -53,27 +78,24 @@ __device__ __forceinline__ float wire_cost_at(const Tables& T, int c) {
 
 // update_single_vcost_ispd24 (full_update.cuh:58-83); cross points are zero
 // on a single GPU (preprocess.hpp:1757).
-__device__ __forceinline__ float via_cost_at(const Tables& T, int c) {
-    const int l = c / T.XY, rem = c - l * T.XY, x = rem / T.Y, y = rem - x * T.Y;
+__device__ __forceinline__ float via_cost_of(const Tables& T, const CellInputs& in) {
     float v;
-    if (along_y(T, l)) {
-        if (y == 0) v = static_cast<float>(incremental_of_cost(T, c, l, 1.0));
-        else if (y == T.Y - 1) v = static_cast<float>(incremental_of_cost(T, c - 1, l, 1.0));
-        else v = static_cast<float>(incremental_of_cost(T, c, l, 0.5) + incremental_of_cost(T, c - 1, l, 0.5));
-    } else {
-        if (x == 0) v = static_cast<float>(incremental_of_cost(T, c, l, 1.0));
-        else if (x == T.X - 1) v = static_cast<float>(incremental_of_cost(T, c - T.Y, l, 1.0));
-        else v = static_cast<float>(incremental_of_cost(T, c, l, 0.5) + incremental_of_cost(T, c - T.Y, l, 0.5));
-    }
+    if (in.pos == 0) v = static_cast<float>(incremental_of_cost(T.of_scale, in.cap0, in.dem0, in.sc, 1.0));
+    else if (in.pos == in.len - 1) v = static_cast<float>(incremental_of_cost(T.of_scale, in.cap1, in.dem1, in.sc, 1.0));
+    else
+        v = static_cast<float>(incremental_of_cost(T.of_scale, in.cap0, in.dem0, in.sc, 0.5) +
+                               incremental_of_cost(T.of_scale, in.cap1, in.dem1, in.sc, 0.5));
     return static_cast<float>(static_cast<double>(v) + T.unit_via);
 }
 
 // Recompute every dirty cell.  A warp loads 32 bitmap words at a time, ranks
-// their dirty cells with a warp prefix sum and computes them 32 at a time, one
-// cell per lane (a dirty word typically holds only a few dirty cells).  Wire
-// costs where the wire bit is set, via costs where the via bit is set (a
-// wire-dirty cell is always via-dirty).  Both words are cleared.
-// `warp`/`nwarps` number the calling warps across the launch.
+// their dirty cells with a warp prefix sum and takes them kRounds * 32
+// at a time, kRounds cells per lane whose inputs are all loaded before any
+// cost is computed or stored (kRounds trades registers for loads in flight).  Wire costs where the wire bit is set, via
+// costs where the via bit is set (a wire-dirty cell is always via-dirty).
+// Both words are cleared.  `warp`/`nwarps` number the calling warps across
+// the launch.
+template <int kRounds>
 __device__ __forceinline__ void refresh_dirty_cells(const Tables& T, int warp, int nwarps, int lane) {
     // The next window's bitmap words are loaded while this one is processed.
     int nw = warp * 32 + lane;
@@ -93,28 +115,45 @@ __device__ __forceinline__ void refresh_dirty_cells(const Tables& T, int warp, i
             if (lane >= d) incl += o;
         }
         const int total = __shfl_sync(0xffffffffu, incl, 31);
-        for (int r = 0; r < total; r += 32) {
-            const int k = r + lane;
-            // Owner lane: first lane whose inclusive count exceeds k.
-            int lo = 0;
+        for (int r = 0; r < total; r += 32 * kRounds) {
+            int cell[kRounds];
+            bool wire[kRounds];
 #pragma unroll
-            for (int step = 16; step; step >>= 1) {
-                const int v = __shfl_sync(0xffffffffu, incl, lo + step - 1);
-                if (v <= k) lo += step;
-            }
-            const int owner_incl = __shfl_sync(0xffffffffu, incl, lo);
-            const int owner_n = __shfl_sync(0xffffffffu, n, lo);
-            const unsigned ov = __shfl_sync(0xffffffffu, vb, lo), ow = __shfl_sync(0xffffffffu, wb, lo);
-            if (k < total) {
-                const int nth = k - (owner_incl - owner_n);  // 0-based rank inside the owner's word
-                unsigned m = ov;
-                for (int q = 0; q < nth; ++q) m &= m - 1;  // drop the nth lowest set bits
-                const int bit = __ffs(m) - 1;
-                const int c = (base + lo) * 32 + bit;
-                if (c < T.cells) {
-                    if ((ow >> bit) & 1u) T.wcost[c] = wire_cost_at(T, c);
-                    T.vcost[c] = via_cost_at(T, c);
+            for (int q = 0; q < kRounds; ++q) {
+                const int k = r + q * 32 + lane;
+                // Owner lane: first lane whose inclusive count exceeds k.
+                int lo = 0;
+#pragma unroll
+                for (int step = 16; step; step >>= 1) {
+                    const int v = __shfl_sync(0xffffffffu, incl, lo + step - 1);
+                    if (v <= k) lo += step;
                 }
+                const int owner_incl = __shfl_sync(0xffffffffu, incl, lo);
+                const int owner_n = __shfl_sync(0xffffffffu, n, lo);
+                const unsigned ov = __shfl_sync(0xffffffffu, vb, lo), ow = __shfl_sync(0xffffffffu, wb, lo);
+                cell[q] = -1;
+                wire[q] = false;
+                if (k < total) {
+                    const int nth = k - (owner_incl - owner_n);  // 0-based rank inside the owner's word
+                    unsigned m = ov;
+                    for (int j = 0; j < nth; ++j) m &= m - 1;  // drop the nth lowest set bits
+                    const int bit = __ffs(m) - 1;
+                    const int c = (base + lo) * 32 + bit;
+                    if (c < T.cells) {
+                        cell[q] = c;
+                        wire[q] = (ow >> bit) & 1u;
+                    }
+                }
+            }
+            CellInputs in[kRounds];
+#pragma unroll
+            for (int q = 0; q < kRounds; ++q)
+                if (cell[q] >= 0) in[q] = load_cell(T, cell[q]);
+#pragma unroll
+            for (int q = 0; q < kRounds; ++q) {
+                if (cell[q] < 0) continue;
+                if (wire[q]) T.wcost[cell[q]] = wire_cost_of(T, in[q]);
+                T.vcost[cell[q]] = via_cost_of(T, in[q]);
             }
         }
         if (vb) T.dirty_via[w] = 0u;

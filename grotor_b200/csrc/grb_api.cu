@@ -37,7 +37,7 @@ constexpr int kPhaseSlots = 12;  // grb_phase_times entries
 __global__ void k_refresh_cells(Tables T) {
     const int lane = threadIdx.x & 31;
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nwarps = (gridDim.x * blockDim.x) >> 5;
-    refresh_dirty_cells(T, warp, nwarps, lane);
+    refresh_dirty_cells<4>(T, warp, nwarps, lane);
 }
 
 // Prefix rebuild of dirty groups: pass 1 and pass 2 over (group, chunk) work
@@ -186,7 +186,7 @@ __global__ void __launch_bounds__(kPersistentThreads, 2) k_lshape_persistent(Tab
         const int stamp = stamp0 + b + 1;
         // refresh_cost (incremental_update.cuh:98-132).
         if (blockIdx.x == 0) collect_dirty_groups(T);
-        refresh_dirty_cells(T, gwarp, nwarps, lane);
+        refresh_dirty_cells<2>(T, gwarp, nwarps, lane);
         if (!grid_sync(S, T)) return;
         clk.mark(S, 4);
         const int items = *reinterpret_cast<volatile int*>(T.group_count) * T.tree_chunks;
@@ -268,7 +268,7 @@ __global__ void __launch_bounds__(kPersistentThreads, 2) k_flt_persistent(Tables
             clk.mark(S, 6);
         }
         if (blockIdx.x == 0) collect_dirty_groups(T);
-        refresh_dirty_cells(T, gwarp, nwarps, lane);
+        refresh_dirty_cells<2>(T, gwarp, nwarps, lane);
         if (!grid_sync(S, T)) return;
         clk.mark(S, 4);
         const int items = *reinterpret_cast<volatile int*>(T.group_count) * T.tree_chunks;
@@ -343,7 +343,7 @@ __global__ void __launch_bounds__(kPersistentThreads, 2) k_zshape_persistent(Tab
         const int lo = P.batch_off[b], cnt = P.batch_off[b + 1] - lo;
         const int stamp = stamp0 + b + 1;
         if (blockIdx.x == 0) collect_dirty_groups(T);
-        refresh_dirty_cells(T, gwarp, nwarps, lane);
+        refresh_dirty_cells<2>(T, gwarp, nwarps, lane);
         if (!grid_sync(S, T)) return;
         clk.mark(S, 4);
         const int items = *reinterpret_cast<volatile int*>(T.group_count) * T.tree_chunks;
