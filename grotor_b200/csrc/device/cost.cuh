@@ -181,6 +181,13 @@ __host__ __device__ __forceinline__ size_t prefix_smem_bytes(int max_len) {
     return size_t(prefix_tree_entries(max_len)) * 32 * sizeof(double);
 }
 
+// Per-warp shared scratch of the passes: a 32 x 32 chunk of doubles (rows
+// padded to 33 entries so row and column accesses are conflict-free).
+constexpr int kXposeStride = kChunkPos + 1;
+__host__ __device__ __forceinline__ size_t prefix_xpose_bytes() {
+    return size_t(kTrackGroup) * kXposeStride * sizeof(double);
+}
+
 struct GroupGeom {
     int l, len, nch, base, stride;
     bool live;
@@ -203,9 +210,35 @@ __device__ __forceinline__ GroupGeom group_geom(const Tables& T, int g, int lane
 }
 
 // The shifted input s[i] = w[i-1] of chunk c (0 outside the track); wire
-// costs are floats, widened when used.
-__device__ __forceinline__ void load_chunk(const Tables& T, const GroupGeom& G, int c, float (&x)[kChunkPos]) {
+// costs are floats, widened when used.  Along-x tracks: at each position the
+// 32 lanes read 32 consecutive cells.  Along-y tracks are runs of consecutive
+// cells, one per lane; with scratch `xs` the warp reads them run by run (32
+// consecutive floats per instruction) and transposes through shared memory.
+__device__ __forceinline__ void load_chunk(const Tables& T, const GroupGeom& G, int c, float (&x)[kChunkPos],
+                                           int lane, float* xs) {
     const int i0 = c * kChunkPos;
+    if (xs && G.stride == 1) {
+        const int i = i0 + lane;
+        // Rows in groups of 16, every load of a group issued before its
+        // shared-memory stores.
+#pragma unroll
+        for (int r0 = 0; r0 < kTrackGroup; r0 += 16) {
+            float v[16];
+#pragma unroll
+            for (int r = 0; r < 16; ++r) {
+                const int base = __shfl_sync(0xffffffffu, G.base, r0 + r);
+                const int live = __shfl_sync(0xffffffffu, int(G.live), r0 + r);
+                v[r] = (live && i > 0 && i < G.len) ? T.wcost[base + i - 1] : 0.0f;
+            }
+#pragma unroll
+            for (int r = 0; r < 16; ++r) xs[(r0 + r) * kXposeStride + lane] = v[r];
+        }
+        __syncwarp();
+#pragma unroll
+        for (int k = 0; k < kChunkPos; ++k) x[k] = xs[lane * kXposeStride + k];
+        __syncwarp();
+        return;
+    }
 #pragma unroll
     for (int k = 0; k < kChunkPos; ++k) {
         const int i = i0 + k;
@@ -214,10 +247,11 @@ __device__ __forceinline__ void load_chunk(const Tables& T, const GroupGeom& G, 
 }
 
 // Pass 1 for work item (g, c): the chunk total of every lane's track.
-__device__ __forceinline__ void prefix_pass1(const Tables& T, int g, int c, int lane) {
+// `xs`: the warp's scratch (prefix_xpose_bytes), or null.
+__device__ __forceinline__ void prefix_pass1(const Tables& T, int g, int c, int lane, void* xs) {
     const GroupGeom G = group_geom(T, g, lane);
     float x[kChunkPos];
-    load_chunk(T, G, c, x);
+    load_chunk(T, G, c, x, lane, static_cast<float*>(xs));
     double tot[6];
     double acc = 0;
 #pragma unroll
@@ -264,8 +298,10 @@ __device__ __forceinline__ void prefix_tree(const Tables& T, int g, double* tree
     }
 }
 
-// Pass 2 for work item (g, c): final prefix values of the chunk.
-__device__ __forceinline__ void prefix_pass2(const Tables& T, int g, int c, int lane) {
+// Pass 2 for work item (g, c): final prefix values of the chunk.  Along-y
+// tracks with scratch `xs`: the values go through shared memory and are
+// written run by run (32 consecutive doubles per instruction).
+__device__ __forceinline__ void prefix_pass2(const Tables& T, int g, int c, int lane, void* xs) {
     const GroupGeom G = group_geom(T, g, lane);
     const double* gt = T.ptree + size_t(g) * T.tree_stride * 32;
     double add[8];
@@ -280,7 +316,9 @@ __device__ __forceinline__ void prefix_pass2(const Tables& T, int g, int c, int 
         }
     }
     float x[kChunkPos];
-    load_chunk(T, G, c, x);
+    load_chunk(T, G, c, x, lane, static_cast<float*>(xs));
+    const bool rows = xs && G.stride == 1;
+    double* ds = static_cast<double*>(xs);
     double tot[6];
     const int i0 = c * kChunkPos;
 #pragma unroll
@@ -306,7 +344,25 @@ __device__ __forceinline__ void prefix_pass2(const Tables& T, int g, int c, int 
         for (int e = 0; e < 8; ++e)
             if ((c >> e) & 1) acc = acc + add[e];
         const int i = i0 + k;
-        if (G.live && i < G.len) T.presum[G.base + i * G.stride] = acc;
+        if (rows) ds[lane * kXposeStride + k] = acc;
+        else if (G.live && i < G.len) T.presum[G.base + i * G.stride] = acc;
+    }
+    if (rows) {
+        __syncwarp();
+        const int i = i0 + lane;
+#pragma unroll
+        for (int r0 = 0; r0 < kTrackGroup; r0 += 16) {
+            double v[16];
+#pragma unroll
+            for (int r = 0; r < 16; ++r) v[r] = ds[(r0 + r) * kXposeStride + lane];
+#pragma unroll
+            for (int r = 0; r < 16; ++r) {
+                const int base = __shfl_sync(0xffffffffu, G.base, r0 + r);
+                const int live = __shfl_sync(0xffffffffu, int(G.live), r0 + r);
+                if (live && i < G.len) T.presum[base + i] = v[r];
+            }
+        }
+        __syncwarp();
     }
 }
 

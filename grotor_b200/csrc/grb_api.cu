@@ -44,12 +44,14 @@ __global__ void k_refresh_cells(Tables T) {
 // items, one warp each; the tree with one CTA per group.
 __global__ void k_collect_groups(Tables T) { collect_dirty_groups(T); }
 __global__ void __launch_bounds__(256, 2) k_prefix_pass1(Tables T) {
+    extern __shared__ __align__(16) char xsm[];
+    void* xs = xsm + (threadIdx.x >> 5) * prefix_xpose_bytes();
     const int lane = threadIdx.x & 31;
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nwarps = (gridDim.x * blockDim.x) >> 5;
     const int items = *T.group_count * T.tree_chunks;
     for (int item = warp; item < items; item += nwarps) {
         int g, c;
-        if (prefix_item(T, item, g, c)) prefix_pass1(T, g, c, lane);
+        if (prefix_item(T, item, g, c)) prefix_pass1(T, g, c, lane, xs);
     }
 }
 __global__ void __launch_bounds__(kRefreshThreads) k_prefix_tree(Tables T) {
@@ -57,12 +59,14 @@ __global__ void __launch_bounds__(kRefreshThreads) k_prefix_tree(Tables T) {
     for (int k = blockIdx.x; k < *T.group_count; k += gridDim.x) prefix_tree(T, T.group_list[k], tree);
 }
 __global__ void __launch_bounds__(256, 2) k_prefix_pass2(Tables T) {
+    extern __shared__ __align__(16) char xsm[];
+    void* xs = xsm + (threadIdx.x >> 5) * prefix_xpose_bytes();
     const int lane = threadIdx.x & 31;
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nwarps = (gridDim.x * blockDim.x) >> 5;
     const int items = *T.group_count * T.tree_chunks;
     for (int item = warp; item < items; item += nwarps) {
         int g, c;
-        if (prefix_item(T, item, g, c)) prefix_pass2(T, g, c, lane);
+        if (prefix_item(T, item, g, c)) prefix_pass2(T, g, c, lane, xs);
     }
 }
 
@@ -192,7 +196,7 @@ __global__ void __launch_bounds__(kPersistentThreads, 2) k_lshape_persistent(Tab
         const int items = *reinterpret_cast<volatile int*>(T.group_count) * T.tree_chunks;
         for (int item = gwarp; item < items; item += nwarps) {
             int g, c;
-            if (prefix_item(T, item, g, c)) prefix_pass1(T, g, c, lane);
+            if (prefix_item(T, item, g, c)) prefix_pass1(T, g, c, lane, smem + warp * prefix_xpose_bytes());
         }
         if (!grid_sync(S, T)) return;
         for (int k = blockIdx.x; k < *reinterpret_cast<volatile int*>(T.group_count); k += gridDim.x)
@@ -200,7 +204,7 @@ __global__ void __launch_bounds__(kPersistentThreads, 2) k_lshape_persistent(Tab
         if (!grid_sync(S, T)) return;
         for (int item = gwarp; item < items; item += nwarps) {
             int g, c;
-            if (prefix_item(T, item, g, c)) prefix_pass2(T, g, c, lane);
+            if (prefix_item(T, item, g, c)) prefix_pass2(T, g, c, lane, smem + warp * prefix_xpose_bytes());
         }
         if (!grid_sync(S, T)) return;
         clk.mark(S, 7);
@@ -274,7 +278,7 @@ __global__ void __launch_bounds__(kPersistentThreads, 2) k_flt_persistent(Tables
         const int items = *reinterpret_cast<volatile int*>(T.group_count) * T.tree_chunks;
         for (int item = gwarp; item < items; item += nwarps) {
             int g, c;
-            if (prefix_item(T, item, g, c)) prefix_pass1(T, g, c, lane);
+            if (prefix_item(T, item, g, c)) prefix_pass1(T, g, c, lane, smem + warp * prefix_xpose_bytes());
         }
         if (!grid_sync(S, T)) return;
         for (int k = blockIdx.x; k < *reinterpret_cast<volatile int*>(T.group_count); k += gridDim.x)
@@ -282,7 +286,7 @@ __global__ void __launch_bounds__(kPersistentThreads, 2) k_flt_persistent(Tables
         if (!grid_sync(S, T)) return;
         for (int item = gwarp; item < items; item += nwarps) {
             int g, c;
-            if (prefix_item(T, item, g, c)) prefix_pass2(T, g, c, lane);
+            if (prefix_item(T, item, g, c)) prefix_pass2(T, g, c, lane, smem + warp * prefix_xpose_bytes());
         }
         if (!grid_sync(S, T)) return;
         clk.mark(S, 7);
@@ -349,7 +353,7 @@ __global__ void __launch_bounds__(kPersistentThreads, 2) k_zshape_persistent(Tab
         const int items = *reinterpret_cast<volatile int*>(T.group_count) * T.tree_chunks;
         for (int item = gwarp; item < items; item += nwarps) {
             int g, c;
-            if (prefix_item(T, item, g, c)) prefix_pass1(T, g, c, lane);
+            if (prefix_item(T, item, g, c)) prefix_pass1(T, g, c, lane, smem + warp * prefix_xpose_bytes());
         }
         if (!grid_sync(S, T)) return;
         for (int k = blockIdx.x; k < *reinterpret_cast<volatile int*>(T.group_count); k += gridDim.x)
@@ -357,7 +361,7 @@ __global__ void __launch_bounds__(kPersistentThreads, 2) k_zshape_persistent(Tab
         if (!grid_sync(S, T)) return;
         for (int item = gwarp; item < items; item += nwarps) {
             int g, c;
-            if (prefix_item(T, item, g, c)) prefix_pass2(T, g, c, lane);
+            if (prefix_item(T, item, g, c)) prefix_pass2(T, g, c, lane, smem + warp * prefix_xpose_bytes());
         }
         if (!grid_sync(S, T)) return;
         clk.mark(S, 7);
@@ -1162,9 +1166,9 @@ int refresh_plain(grb_ctx* c) {
     k_refresh_cells<<<c->sms * 8, 256, 0, c->stream>>>(T);
     prof_end(c, e);
     if ((rc = prof_begin(c, 7, &e))) return rc;
-    k_prefix_pass1<<<c->sms * 8, 256, 0, c->stream>>>(T);
+    k_prefix_pass1<<<c->sms * 8, 256, 8 * prefix_xpose_bytes(), c->stream>>>(T);
     k_prefix_tree<<<c->sms * 2, kRefreshThreads, prefix_smem_bytes(std::max(T.X, T.Y)), c->stream>>>(T);
-    k_prefix_pass2<<<c->sms * 8, 256, 0, c->stream>>>(T);
+    k_prefix_pass2<<<c->sms * 8, 256, 8 * prefix_xpose_bytes(), c->stream>>>(T);
     prof_end(c, e);
     c->launches += 5;
     GRB_CUDA(c, cudaGetLastError());
@@ -1297,7 +1301,8 @@ int ensure_work(grb_ctx* c);
 
 int z_stage_persistent(grb_ctx* c, int stamp0) {
     if (c->n_batches == 0) return GRB_OK;
-    const size_t smem = prefix_smem_bytes(std::max(c->T.X, c->T.Y));
+    const size_t smem = std::max(prefix_smem_bytes(std::max(c->T.X, c->T.Y)),
+                                 size_t(kPersistentThreads / 32) * prefix_xpose_bytes());
     GRB_CUDA(c, cudaFuncSetAttribute(k_zshape_persistent, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
     int per_sm = 0;
     GRB_CUDA(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_zshape_persistent, kPersistentThreads, smem));
@@ -1467,7 +1472,8 @@ int ensure_work(grb_ctx* c) {
 
 int flt_stage_persistent(grb_ctx* c, int stamp0, int remove) {
     if (c->n_batches == 0) return GRB_OK;
-    const size_t smem = prefix_smem_bytes(std::max(c->T.X, c->T.Y));
+    const size_t smem = std::max(prefix_smem_bytes(std::max(c->T.X, c->T.Y)),
+                                 size_t(kPersistentThreads / 32) * prefix_xpose_bytes());
     GRB_CUDA(c, cudaFuncSetAttribute(k_flt_persistent, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
     int per_sm = 0;
     GRB_CUDA(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_flt_persistent, kPersistentThreads, smem));
@@ -1524,7 +1530,7 @@ int stage_persistent(grb_ctx* c, int stamp0) {
     const size_t ab = arena_bytes(c->T.L, nmax);
     const int wpb = kPersistentThreads / 32;
     const size_t prefix_smem = prefix_smem_bytes(std::max(c->T.X, c->T.Y));  // prefix_tree
-    const size_t smem = std::max(ab * wpb, prefix_smem);
+    const size_t smem = std::max(std::max(ab * wpb, prefix_smem), size_t(wpb) * prefix_xpose_bytes());
     GRB_CUDA(c, cudaFuncSetAttribute(k_lshape_persistent, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
     int per_sm = 0;
     GRB_CUDA(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_lshape_persistent, kPersistentThreads, smem));
@@ -1648,6 +1654,8 @@ int grb_create(const grb_grid* g, int32_t device, grb_ctx** out) {
     GRB_CUDA(cp, cudaFuncSetAttribute(k_batch_persistent, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
     GRB_CUDA(cp, cudaFuncSetAttribute(k_lshape_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
     GRB_CUDA(cp, cudaFuncSetAttribute(k_lshape_bucketed, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    GRB_CUDA(cp, cudaFuncSetAttribute(k_prefix_pass1, cudaFuncAttributeMaxDynamicSharedMemorySize, int(8 * prefix_xpose_bytes())));
+    GRB_CUDA(cp, cudaFuncSetAttribute(k_prefix_pass2, cudaFuncAttributeMaxDynamicSharedMemorySize, int(8 * prefix_xpose_bytes())));
     GRB_CUDA(cp, cudaFuncSetAttribute(k_prefix_tree, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       int(prefix_smem_bytes(std::max(T.X, T.Y)))));
     const int r = grb_reset(cp);
