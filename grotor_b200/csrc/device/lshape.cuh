@@ -87,23 +87,49 @@ __device__ void lshape_net(const Tables& T, const Plan& P, int id, int stamp, co
     const int* nd = P.nodes + off;
     const int* par = P.parents + off;
 
-    // 1. Gather every cost the DP reads.
-    for (int q = lane; q < N * L; q += 32) {
-        const int i = q / L, l = q - i * L;
-        const int node = nd[i], r = node % XY, x = r / Y, y = r - x * Y;
-        A.vN[q] = T.vcost[l * XY + r];
-        if (i > 0) {
-            const int pr = nd[par[i]] % XY, px = pr / Y, py = pr - px * Y;
-            const int minx = min(x, px), maxx = max(x, px), miny = min(y, py), maxy = max(y, py);
-            const bool ay = along_y(T, l);
-            if (x == px || y == py) {
-                const bool valid = ay ? (x == px) : (y == py);
-                A.w1[q] = valid ? wire_cost(T, l, minx, maxx, miny, maxy) : 0.0;
-            } else {
-                A.w1[q] = ay ? wire_cost(T, l, x, x, miny, maxy) : wire_cost(T, l, minx, maxx, y, y);
-                A.w2[q] = ay ? wire_cost(T, l, px, px, miny, maxy) : wire_cost(T, l, minx, maxx, py, py);
-                A.vA[q] = T.vcost[cell_index(T, l, x, py)];
-                A.vB[q] = T.vcost[cell_index(T, l, px, y)];
+    // 1. Gather every cost the DP reads.  Each lane takes two (node, layer)
+    // items per pass and issues all their loads before any arena store.
+    for (int q0 = lane; q0 < N * L; q0 += 64) {
+        float vn[2], va[2], vb[2];
+        double w1[2], w2[2];
+        int kind[2];  // 0: none, 1: node only, 2: straight edge, 3: L-shaped edge
+#pragma unroll
+        for (int u = 0; u < 2; ++u) {
+            const int q = q0 + 32 * u;
+            kind[u] = 0;
+            vn[u] = va[u] = vb[u] = 0.f;
+            w1[u] = w2[u] = 0.0;
+            if (q >= N * L) continue;
+            const int i = q / L, l = q - i * L;
+            const int node = nd[i], r = node % XY, x = r / Y, y = r - x * Y;
+            vn[u] = T.vcost[l * XY + r];
+            kind[u] = 1;
+            if (i > 0) {
+                const int pr = nd[par[i]] % XY, px = pr / Y, py = pr - px * Y;
+                const int minx = min(x, px), maxx = max(x, px), miny = min(y, py), maxy = max(y, py);
+                const bool ay = along_y(T, l);
+                if (x == px || y == py) {
+                    const bool valid = ay ? (x == px) : (y == py);
+                    w1[u] = valid ? wire_cost(T, l, minx, maxx, miny, maxy) : 0.0;
+                    kind[u] = 2;
+                } else {
+                    w1[u] = ay ? wire_cost(T, l, x, x, miny, maxy) : wire_cost(T, l, minx, maxx, y, y);
+                    w2[u] = ay ? wire_cost(T, l, px, px, miny, maxy) : wire_cost(T, l, minx, maxx, py, py);
+                    va[u] = T.vcost[cell_index(T, l, x, py)];
+                    vb[u] = T.vcost[cell_index(T, l, px, y)];
+                    kind[u] = 3;
+                }
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < 2; ++u) {
+            const int q = q0 + 32 * u;
+            if (kind[u] >= 1) A.vN[q] = vn[u];
+            if (kind[u] >= 2) A.w1[q] = w1[u];
+            if (kind[u] == 3) {
+                A.w2[q] = w2[u];
+                A.vA[q] = va[u];
+                A.vB[q] = vb[u];
             }
         }
     }
