@@ -57,6 +57,7 @@ struct BatchState {
     unsigned short* pt_jj;
     unsigned* cellmask;         // [X*Y][W]
     unsigned* localmask[3];     // [X*Y][kChunkWords], chunk k in buffer k % 3
+    unsigned* ptchunk;          // [X*Y] bit k % 32: the cell is a query point of chunk k
     unsigned* fmask;            // [2][W][kChunk] forbidden colours, by chunk parity
     unsigned* pred;             // [2][kChunkWords][kChunk] predecessors inside the chunk
     unsigned* prevp;            // [2][kChunkWords][kChunk] marking nets of the previous chunk
@@ -164,15 +165,49 @@ __device__ __forceinline__ void flat_fill(const BatchState& B, int p) {
 
 __device__ __forceinline__ unsigned* chunk_mask(const BatchState& B, int chunk) { return B.localmask[chunk % 3]; }
 
-// Step 1: the chunk at order position s rasters its marks.  Threads t of nt.
-__device__ __forceinline__ void batch_raster(const BatchState& B, int s, long long t, long long nt) {
+// Query-point bits of the chunk at s: bit (chunk % 32) of every query point
+// cell of the chunk is set (set) or cleared.
+__device__ __forceinline__ void batch_point_bits(const BatchState& B, int s, bool set, long long t, long long nt) {
     const int m = min(kChunk, B.n - s);
-    unsigned* lm = chunk_mask(B, s / kChunk);
+    const unsigned bit = 1u << ((s / kChunk) & 31);
+    const long long a = B.pt_off[s], b = B.pt_off[s + m];
+    for (long long k = a + t; k < b; k += nt) {
+        unsigned* w = B.ptchunk + __ldg(B.pt_cell + k);
+        if (set) red_or(w, bit);
+        else asm volatile("red.relaxed.gpu.global.and.b32 [%0], %1;" ::"l"(w), "r"(~bit) : "memory");
+    }
+}
+
+// Step 1: the chunk at order position s rasters its marks.  Only a cell that
+// is a query point of this chunk or (with `next`) of the next one is ever read
+// back, so the raster keeps the marks whose cell has one of those query-point
+// bits; the bits live in a 4-byte-per-cell array that stays in L2, the
+// chunk-local masks do not.  Threads t of nt.
+__device__ __forceinline__ void batch_raster(const BatchState& B, int s, bool next, long long t, long long nt) {
+    const int m = min(kChunk, B.n - s), chunk = s / kChunk;
+    const unsigned want = (1u << (chunk & 31)) | (next ? 1u << ((chunk + 1) & 31) : 0u);
+    unsigned* lm = chunk_mask(B, chunk);
     const long long a = B.mark_off[s], b = B.mark_off[s + m];
     for (long long k = a + t; k < b; k += nt) {
         const unsigned q = __ldg(B.mark_cell + k);
         const int jj = __ldg(B.mark_jj + k);
-        red_or(lm + size_t(q) * kChunkWords + (jj >> 5), 1u << (jj & 31));
+        if (__ldcg(B.ptchunk + q) & want) red_or(lm + size_t(q) * kChunkWords + (jj >> 5), 1u << (jj & 31));
+    }
+}
+
+// The chunk-local mask of the chunk at s is nonzero only at query points of
+// this chunk and (with `next`) the next one: zero the whole 64-byte record of
+// each of those cells.
+__device__ __forceinline__ void batch_clear(const BatchState& B, int s, bool next, long long t, long long nt) {
+    unsigned* lm = chunk_mask(B, s / kChunk);
+    const long long a = B.pt_off[s];
+    const long long b = B.pt_off[min(s + (next ? 2 : 1) * kChunk, B.n)];
+    const long long items = (b - a) * 4;
+    for (long long k = t; k < items; k += nt) {
+        const long long pi = a + k / 4;
+        const int part = int(k & 3);
+        uint4* rec = reinterpret_cast<uint4*>(lm + size_t(__ldg(B.pt_cell + pi)) * kChunkWords);
+        rec[part] = make_uint4(0u, 0u, 0u, 0u);
     }
 }
 
@@ -213,17 +248,15 @@ __device__ __forceinline__ void batch_gather(const BatchState& B, int s, bool lo
     }
 }
 
-// Step 4: the chunk at s publishes its colours and clears its chunk-local mask.
+// Step 4: the chunk at s publishes its colours.
 __device__ __forceinline__ void batch_publish(const BatchState& B, int s, long long t, long long nt) {
     const int m = min(kChunk, B.n - s);
-    unsigned* lm = chunk_mask(B, s / kChunk);
     const long long a = B.mark_off[s], b = B.mark_off[s + m];
     for (long long k = a + t; k < b; k += nt) {
         const unsigned q = __ldg(B.mark_cell + k);
         const int jj = __ldg(B.mark_jj + k);
         const int c = __ldcg(B.batch_of + s + jj);
         red_or(B.cellmask + size_t(q) * B.W + (c >> 5), 1u << (c & 31));
-        lm[size_t(q) * kChunkWords + (jj >> 5)] = 0u;
     }
 }
 

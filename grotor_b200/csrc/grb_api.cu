@@ -701,9 +701,10 @@ __global__ void k_scan_add(long long* a, int n, const long long* sums, int tiles
 }
 
 // Plain form: one launch per step and chunk.
-__global__ void k_batch_raster(BatchState B, int s) {
-    batch_raster(B, s, blockIdx.x * (long long)blockDim.x + threadIdx.x, (long long)gridDim.x * blockDim.x);
-}
+__device__ __forceinline__ long long launch_thread() { return blockIdx.x * (long long)blockDim.x + threadIdx.x; }
+__device__ __forceinline__ long long launch_threads() { return (long long)gridDim.x * blockDim.x; }
+__global__ void k_batch_point_bits(BatchState B, int s) { batch_point_bits(B, s, true, launch_thread(), launch_threads()); }
+__global__ void k_batch_raster(BatchState B, int s) { batch_raster(B, s, false, launch_thread(), launch_threads()); }
 __global__ void k_batch_gather(BatchState B, int s) {
     batch_gather(B, s, false, blockIdx.x * (long long)blockDim.x + threadIdx.x, (long long)gridDim.x * blockDim.x);
 }
@@ -721,22 +722,32 @@ __global__ void __launch_bounds__(kChunk) k_batch_solve(BatchState B, int s) {
     for (int k = threadIdx.x; k < C; k += blockDim.x) B.count[k] = S.cnt[k];
     for (int k = threadIdx.x; k < B.W; k += blockDim.x) B.fullmask[k] = S.full[k];
 }
+// Publish chunk s, empty its chunk-local mask and query-point bits, and set
+// the next chunk's query-point bits.
 __global__ void k_batch_publish(BatchState B, int s) {
     if (*reinterpret_cast<volatile int*>(B.error)) return;
-    batch_publish(B, s, blockIdx.x * (long long)blockDim.x + threadIdx.x, (long long)gridDim.x * blockDim.x);
+    const long long t = launch_thread(), nt = launch_threads();
+    batch_publish(B, s, t, nt);
+    batch_clear(B, s, false, t, nt);
+    batch_point_bits(B, s, false, t, nt);
+    if (s + kChunk < B.n) batch_point_bits(B, s + kChunk, true, t, nt);
 }
 
 // Persistent batching: CTAs of kPersistThreads threads, one per SM, at least
 // two.  CTA 0 is the solver and has its SM to itself (its first kChunk
 // threads solve, the rest leave): for chunk r it waits until the other CTAs
 // (G of them, one shared barrier counter) have gathered chunk r, solves it,
-// and releases `solved` = r + 1.  The other CTAs run, per round r:
-//   A: wait for chunk r-1's colours, publish chunk r-1         | barrier
+// and releases `solved` = r + 1.  The other CTAs set the query-point bits of
+// chunks 0-3 | raster chunks 0 and 1 | gather chunk 0 | and then run, per
+// round r:
+//   A: wait for chunk r-1's colours, publish chunk r-1, empty
+//      its chunk-local mask                                    | barrier
 //   B: gather chunk r+1 (cellmask as of chunk r-1, chunk r
 //      through the previous-chunk bits)                        | barrier
-//   C: raster chunk r+2 (its buffer was cleared in A)
+//   C: raster chunk r+2 (its buffer was emptied in A), set the
+//      query-point bits of chunk r+4, clear those of chunk r-1
 // The barrier after B(r) is what the solver waits for before chunk r+1
-// (counter (2 + 2(r+1)) * G); C overlaps the solve of chunk r.
+// (counter (3 + 2(r+1)) * G); C overlaps the solve of chunk r.
 constexpr int kPersistThreads = 2 * kChunk;
 __global__ void __launch_bounds__(kPersistThreads, 1) k_batch_persistent(BatchState B, GridSync S, Tables T) {
     extern __shared__ __align__(16) unsigned bsm[];
@@ -754,7 +765,7 @@ __global__ void __launch_bounds__(kPersistThreads, 1) k_batch_persistent(BatchSt
             for (int k = threadIdx.x; k < (kChunk / 32) * C; k += kChunk) M.wh[k] = 0;
         for (int k = threadIdx.x; k < B.W; k += kChunk) M.full[k] = B.fullmask[k];
         for (int r = 0; r < chunks; ++r) {
-            if (threadIdx.x == 0) go = wait_at_least(S.count, (2u + 2u * r) * G, S.timeout_ns, T, true);
+            if (threadIdx.x == 0) go = wait_at_least(S.count, (3u + 2u * r) * G, S.timeout_ns, T, true);
             solve_sync();
             if (!go) return;
             clk.mark(S, 8);
@@ -771,8 +782,9 @@ __global__ void __launch_bounds__(kPersistThreads, 1) k_batch_persistent(BatchSt
     PhaseClock clk{0, 1};
     clk.start(S);
     const long long t = (blockIdx.x - 1) * (long long)blockDim.x + threadIdx.x, nt = (long long)G * blockDim.x;
-    batch_raster(B, 0, t, nt);
-    if (chunks > 1) batch_raster(B, kChunk, t, nt);
+    for (int k = 0; k < 4 && k < chunks; ++k) batch_point_bits(B, k * kChunk, true, t, nt);
+    if (!grid_sync_of(S, T, G)) return;
+    for (int k = 0; k < 2 && k < chunks; ++k) batch_raster(B, k * kChunk, true, t, nt);
     if (!grid_sync_of(S, T, G)) return;
     batch_gather(B, 0, false, t, nt);
     if (!grid_sync_of(S, T, G)) return;
@@ -784,13 +796,16 @@ __global__ void __launch_bounds__(kPersistThreads, 1) k_batch_persistent(BatchSt
             if (!go) return;
             clk.mark(S, 9);
             batch_publish(B, (r - 1) * kChunk, t, nt);
+            batch_clear(B, (r - 1) * kChunk, true, t, nt);
         }
         if (!grid_sync_of(S, T, G)) return;
         clk.mark(S, 0);
         if (r + 1 < chunks) batch_gather(B, (r + 1) * kChunk, true, t, nt);
         if (!grid_sync_of(S, T, G)) return;
         clk.mark(S, 1);
-        if (r + 2 < chunks) batch_raster(B, (r + 2) * kChunk, t, nt);
+        if (r + 2 < chunks) batch_raster(B, (r + 2) * kChunk, true, t, nt);
+        if (r + 4 < chunks) batch_point_bits(B, (r + 4) * kChunk, true, t, nt);
+        if (r >= 1) batch_point_bits(B, (r - 1) * kChunk, false, t, nt);
         clk.mark(S, 10);
     }
     if (chunks > 0) {
@@ -798,6 +813,8 @@ __global__ void __launch_bounds__(kPersistThreads, 1) k_batch_persistent(BatchSt
         __syncthreads();
         if (!go) return;
         batch_publish(B, (chunks - 1) * kChunk, t, nt);
+        batch_clear(B, (chunks - 1) * kChunk, true, t, nt);
+        batch_point_bits(B, (chunks - 1) * kChunk, false, t, nt);
     }
 }
 
@@ -947,6 +964,7 @@ struct grb_ctx {
     // batching buffers
     unsigned *cellmask = nullptr, *fmask = nullptr, *fullmask = nullptr;
     unsigned* lmask[3] = {nullptr, nullptr, nullptr};  // chunk-local masks
+    unsigned* ptchunk = nullptr;                        // [X*Y] query-point bits by chunk % 32
     unsigned *pred = nullptr, *prevp = nullptr, *bsolved = nullptr;
     bool lmask_dirty = false;          // a run stopped before clearing them
     int *bcount = nullptr, *ncolors = nullptr, *batch_of = nullptr, *brank = nullptr, *order = nullptr;
@@ -1678,7 +1696,7 @@ void grb_destroy(grb_ctx* c) {
     free_all(c->flt_bufs);
     free_all(c->owned);
     for (void* p : {(void*)c->check, (void*)c->bucket_ids, (void*)c->bucket_off, (void*)c->ids, (void*)c->batch_off, (void*)c->gscratch, (void*)c->work, (void*)c->cellmask,
-                    (void*)c->lmask[0], (void*)c->lmask[1], (void*)c->lmask[2], (void*)c->fmask, (void*)c->pred, (void*)c->prevp,
+                    (void*)c->lmask[0], (void*)c->lmask[1], (void*)c->lmask[2], (void*)c->ptchunk, (void*)c->fmask, (void*)c->pred, (void*)c->prevp,
                     (void*)c->bsolved, (void*)c->fullmask, (void*)c->bcount, (void*)c->ncolors, (void*)c->batch_of, (void*)c->brank,
                     (void*)c->order, (void*)c->mark_off, (void*)c->pt_off, (void*)c->scan_sums, (void*)c->mark_cell,
                     (void*)c->pt_cell, (void*)c->mark_jj, (void*)c->pt_jj})
@@ -2238,6 +2256,7 @@ int grb_plan_batches(grb_ctx* c, const int32_t* order, int32_t n, int32_t limit,
     if (rc) return rc;
     if (!c->lmask[0]) {
         if (cudaMalloc(&c->lmask[0], lm_bytes) || cudaMalloc(&c->lmask[1], lm_bytes) || cudaMalloc(&c->lmask[2], lm_bytes) ||
+            cudaMalloc(&c->ptchunk, xy * 4) ||
             cudaMalloc(&c->pred, pq_bytes) || cudaMalloc(&c->prevp, pq_bytes) || cudaMalloc(&c->bsolved, 4) ||
             cudaMalloc(&c->ncolors, 4)) {
             cudaGetLastError();
@@ -2269,6 +2288,7 @@ int grb_plan_batches(grb_ctx* c, const int32_t* order, int32_t n, int32_t limit,
         if (smem > 200 * 1024) return fail(c, GRB_ELIMIT, "too many batch colours");
         if (c->lmask_dirty) {
             for (unsigned* lm : c->lmask) GRB_CUDA(c, cudaMemsetAsync(lm, 0, lm_bytes, c->stream));
+            GRB_CUDA(c, cudaMemsetAsync(c->ptchunk, 0, xy * 4, c->stream));
             c->lmask_dirty = false;
         }
         GRB_CUDA(c, cudaMemsetAsync(c->cellmask, 0, xy * W * 4, c->stream));
@@ -2282,6 +2302,7 @@ int grb_plan_batches(grb_ctx* c, const int32_t* order, int32_t n, int32_t limit,
         B.W = W;
         B.cellmask = c->cellmask;
         for (int k = 0; k < 3; ++k) B.localmask[k] = c->lmask[k];
+        B.ptchunk = c->ptchunk;
         B.fmask = c->fmask; B.pred = c->pred; B.prevp = c->prevp;
         B.fullmask = c->fullmask; B.count = c->bcount; B.n_colors = c->ncolors;
         B.solved = c->bsolved;
@@ -2298,6 +2319,8 @@ int grb_plan_batches(grb_ctx* c, const int32_t* order, int32_t n, int32_t limit,
             c->launches += 1;
         } else {
             const int grid = c->sms * 4;
+            if (n) k_batch_point_bits<<<grid, 256, 0, c->stream>>>(B, 0);
+            c->launches += n ? 1 : 0;
             for (int s = 0; s < n; s += kChunk) {
                 cudaEvent_t e;
                 if ((rc = prof_begin(c, 0, &e))) return rc;
