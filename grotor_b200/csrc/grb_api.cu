@@ -741,13 +741,13 @@ __global__ void k_batch_publish(BatchState B, int s) {
 // chunks 0-3 | raster chunks 0 and 1 | gather chunk 0 | and then run, per
 // round r:
 //   A: wait for chunk r-1's colours, publish chunk r-1, empty
-//      its chunk-local mask                                    | barrier
+//      its chunk-local mask, set the query-point bits of chunk
+//      r+4 and clear those of chunk r-1                        | barrier
 //   B: gather chunk r+1 (cellmask as of chunk r-1, chunk r
-//      through the previous-chunk bits)                        | barrier
-//   C: raster chunk r+2 (its buffer was emptied in A), set the
-//      query-point bits of chunk r+4, clear those of chunk r-1
+//      through the previous-chunk bits) and raster chunk r+2
+//      (its buffer was emptied in A)                           | barrier
 // The barrier after B(r) is what the solver waits for before chunk r+1
-// (counter (3 + 2(r+1)) * G); C overlaps the solve of chunk r.
+// (counter (3 + 2(r+1)) * G).
 constexpr int kPersistThreads = 2 * kChunk;
 __global__ void __launch_bounds__(kPersistThreads, 1) k_batch_persistent(BatchState B, GridSync S, Tables T) {
     extern __shared__ __align__(16) unsigned bsm[];
@@ -797,16 +797,15 @@ __global__ void __launch_bounds__(kPersistThreads, 1) k_batch_persistent(BatchSt
             clk.mark(S, 9);
             batch_publish(B, (r - 1) * kChunk, t, nt);
             batch_clear(B, (r - 1) * kChunk, true, t, nt);
+            batch_point_bits(B, (r - 1) * kChunk, false, t, nt);
         }
+        if (r + 4 < chunks) batch_point_bits(B, (r + 4) * kChunk, true, t, nt);
         if (!grid_sync_of(S, T, G)) return;
         clk.mark(S, 0);
         if (r + 1 < chunks) batch_gather(B, (r + 1) * kChunk, true, t, nt);
+        if (r + 2 < chunks) batch_raster(B, (r + 2) * kChunk, true, t, nt);
         if (!grid_sync_of(S, T, G)) return;
         clk.mark(S, 1);
-        if (r + 2 < chunks) batch_raster(B, (r + 2) * kChunk, true, t, nt);
-        if (r + 4 < chunks) batch_point_bits(B, (r + 4) * kChunk, true, t, nt);
-        if (r >= 1) batch_point_bits(B, (r - 1) * kChunk, false, t, nt);
-        clk.mark(S, 10);
     }
     if (chunks > 0) {
         if (threadIdx.x == 0) go = wait_at_least(B.solved, unsigned(chunks), S.timeout_ns, T, true);
