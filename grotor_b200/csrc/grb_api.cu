@@ -989,6 +989,12 @@ struct grb_ctx {
     std::vector<void*> z_bufs;
     ZTrees Z{};
     int4* z_box = nullptr;            // per net (minx, maxx, miny, maxy)
+    // bounding-box refinement scratch (grb_plan_bbox_batches), grow-only
+    std::vector<void*> box_bufs;
+    unsigned long long *box_ka = nullptr, *box_kb = nullptr;
+    int *box_pend = nullptr, *box_tmp = nullptr, *box_bsize = nullptr, *box_bofs = nullptr;
+    int *box_rounds = nullptr, *box_first = nullptr, *box_off = nullptr;
+    int box_cap_n = 0, box_cap_g = 0;
     int z_n = -1;
     std::vector<int> h_z_node_off;
     int z_version = 0;
@@ -1690,6 +1696,7 @@ void grb_destroy(grb_ctx* c) {
     if (c->z_graph) cudaGraphExecDestroy(c->z_graph);
     free_all(c->soft_bufs);
     free_all(c->z_bufs);
+    free_all(c->box_bufs);
     free_all(c->net_bufs);
     free_all(c->geom_bufs);
     free_all(c->flt_bufs);
@@ -1932,15 +1939,25 @@ int grb_plan_bbox_batches(grb_ctx* c, const int32_t* bbox, int32_t max_batch, in
         if (dalloc(c, &box, c->n_nets, tmpb)) return GRB_ENOMEM;
         GRB_CUDA(c, cudaMemcpyAsync(box, bbox, sizeof(int4) * c->n_nets, cudaMemcpyHostToDevice, c->stream));
     }
-    unsigned long long *ka, *kb;
-    int *pend, *tmp, *bsize, *bofs, *rounds, *first, *off_new;
-    int rc = 0;
-    rc |= dalloc(c, &ka, n, tmpb); rc |= dalloc(c, &kb, n, tmpb);
-    rc |= dalloc(c, &pend, n, tmpb); rc |= dalloc(c, &tmp, n, tmpb);
-    rc |= dalloc(c, &bsize, n, tmpb); rc |= dalloc(c, &bofs, n, tmpb);
-    rc |= dalloc(c, &rounds, G, tmpb); rc |= dalloc(c, &first, G, tmpb);
-    rc |= dalloc(c, &off_new, n + 1, tmpb);
-    if (rc) { free_all(tmpb); return GRB_ENOMEM; }
+    // Scratch kept in the context (grow-only): allocating and freeing it on
+    // every call costs more than the refinement itself.
+    if (n > c->box_cap_n || G > c->box_cap_g) {
+        free_all(c->box_bufs);
+        c->box_cap_n = c->box_cap_g = 0;
+        const int cn = std::max(n, c->box_cap_n), cg = std::max(G, c->box_cap_g);
+        int rc = 0;
+        rc |= dalloc(c, &c->box_ka, cn, c->box_bufs); rc |= dalloc(c, &c->box_kb, cn, c->box_bufs);
+        rc |= dalloc(c, &c->box_pend, cn, c->box_bufs); rc |= dalloc(c, &c->box_tmp, cn, c->box_bufs);
+        rc |= dalloc(c, &c->box_bsize, cn, c->box_bufs); rc |= dalloc(c, &c->box_bofs, cn, c->box_bufs);
+        rc |= dalloc(c, &c->box_rounds, cg, c->box_bufs); rc |= dalloc(c, &c->box_first, cg, c->box_bufs);
+        rc |= dalloc(c, &c->box_off, cn + 1, c->box_bufs);
+        if (rc) { free_all(c->box_bufs); free_all(tmpb); return GRB_ENOMEM; }
+        c->box_cap_n = cn;
+        c->box_cap_g = cg;
+    }
+    unsigned long long *ka = c->box_ka, *kb = c->box_kb;
+    int *pend = c->box_pend, *tmp = c->box_tmp, *bsize = c->box_bsize, *bofs = c->box_bofs;
+    int *rounds = c->box_rounds, *first = c->box_first, *off_new = c->box_off;
     auto run = [&]() -> int {
         k_bbox_refine<<<G, kBoxThreads, 0, c->stream>>>(c->ids, c->batch_off, box, ka, kb, pend, tmp, bsize, rounds,
                                                         max_batch);
