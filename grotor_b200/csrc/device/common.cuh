@@ -70,12 +70,13 @@ struct Plan {
     const int* bucket_off;
 };
 
-// Size buckets of the routing DP: tree nodes <= 4, <= 8, <= 16, more.
+// Size buckets of the routing DP: tree nodes <= 2 (routed one net per lane),
+// <= 8, <= 16, more (one net per warp).
 constexpr int kDpBuckets = 4;
 __host__ __device__ __forceinline__ int dp_bucket(int nodes) {
-    return nodes <= 4 ? 0 : nodes <= 8 ? 1 : nodes <= 16 ? 2 : 3;
+    return nodes <= 2 ? 0 : nodes <= 8 ? 1 : nodes <= 16 ? 2 : 3;
 }
-__host__ __device__ __forceinline__ int dp_bucket_nodes(int b) { return b == 0 ? 4 : b == 1 ? 8 : 16; }
+__host__ __device__ __forceinline__ int dp_bucket_nodes(int b) { return b == 0 ? 2 : b == 1 ? 8 : 16; }
 
 // Launch shape chosen per size bucket (grb_autotune): nets per CTA of the
 // per-batch DP launch, nets taken per work-queue grab in the persistent form.

@@ -278,4 +278,204 @@ __device__ void lshape_net(const Tables& T, const Plan& P, int id, int stamp, co
     if (fuse_wires) commit_net_wires(T, P, id, stamp, 1, lane);
 }
 
+// Nets of one or two tree nodes, one net per lane: the lanes of a warp route
+// up to 32 such nets at once (most nets of a design), where lshape_net would
+// spend a whole warp, mostly idle, on each.  Same arithmetic, comparisons,
+// tie-breaks and emission order as lshape_net on the same net, so the routes
+// are identical.  Scratch: lane-interleaved per-warp shared memory of
+// pair_scratch_bytes().  id < 0: the lane has no net.
+constexpr int kPairD = 3 * kMaxLayers;  // doubles per lane: cur, w1, w2 (then diag)
+constexpr int kPairF = 3 * kMaxLayers;  // 4-byte words per lane: vA (then root vN), vB, vN (then choices)
+constexpr int kPairH = kMaxLayers;      // shorts per lane: best range through each layer
+__host__ __device__ __forceinline__ size_t pair_scratch_bytes() {
+    return size_t(32) * (kPairD * 8 + kPairF * 4 + kPairH * 2);
+}
+
+__device__ __forceinline__ void lshape_net_pair(const Tables& T, const Plan& P, int id, int stamp, char* scratch,
+                                                int lane, bool commit) {
+    if (id < 0) return;
+    double* sd = reinterpret_cast<double*>(scratch);
+    float* sf = reinterpret_cast<float*>(scratch + size_t(32) * kPairD * 8);
+    int* si = reinterpret_cast<int*>(sf);
+    unsigned short* sh = reinterpret_cast<unsigned short*>(scratch + size_t(32) * (kPairD * 8 + kPairF * 4));
+    auto cur = [&](int l) -> double& { return sd[l * 32 + lane]; };
+    auto w1 = [&](int l) -> double& { return sd[(kMaxLayers + l) * 32 + lane]; };
+    auto w2 = [&](int l) -> double& { return sd[(2 * kMaxLayers + l) * 32 + lane]; };    // then diag
+    auto vA = [&](int l) -> float& { return sf[l * 32 + lane]; };                           // then root vN
+    auto vB = [&](int l) -> float& { return sf[(kMaxLayers + l) * 32 + lane]; };
+    auto vN = [&](int l) -> float& { return sf[(2 * kMaxLayers + l) * 32 + lane]; };
+    auto pdiag = [&](int l) -> int& { return si[(2 * kMaxLayers + l) * 32 + lane]; };       // after vN
+    auto cfrom = [&](int l) -> unsigned short& { return sh[l * 32 + lane]; };
+    const int L = T.L, Y = T.Y, XY = T.XY;
+    const int off = P.node_off[id], N = P.node_off[id + 1] - off;
+    const int n0 = P.nodes[off], r0 = n0 % XY, x0 = r0 / Y, y0 = r0 - x0 * Y, fix0 = n0 / XY;
+    int x1 = 0, y1 = 0;
+    bool straight = false;
+    if (N == 2) {
+        const int n1 = P.nodes[off + 1], r1 = n1 % XY, fix1 = n1 / XY;
+        x1 = r1 / Y;
+        y1 = r1 - x1 * Y;
+        straight = x1 == x0 || y1 == y0;
+        const int minx = min(x1, x0), maxx = max(x1, x0), miny = min(y1, y0), maxy = max(y1, y0);
+        // Step 1 for node 1 (the child), kHalfLayers layers at a time: every
+        // load of a group is issued before its stores.
+        constexpr int kHalfLayers = kMaxLayers / 2;
+#pragma unroll
+        for (int l0 = 0; l0 < kMaxLayers; l0 += kHalfLayers) {
+            float vn[kHalfLayers], va[kHalfLayers], vb[kHalfLayers];
+            double a[kHalfLayers], b[kHalfLayers];
+#pragma unroll
+            for (int u = 0; u < kHalfLayers; ++u) {
+                const int l = l0 + u;
+                vn[u] = va[u] = vb[u] = 0.f;
+                a[u] = b[u] = 0.0;
+                if (l >= L) continue;
+                const bool ay = along_y(T, l);
+                vn[u] = T.vcost[l * XY + r1];
+                if (straight) {
+                    const bool valid = ay ? (x1 == x0) : (y1 == y0);
+                    a[u] = valid ? wire_cost(T, l, minx, maxx, miny, maxy) : 0.0;
+                } else {
+                    a[u] = ay ? wire_cost(T, l, x1, x1, miny, maxy) : wire_cost(T, l, minx, maxx, y1, y1);
+                    b[u] = ay ? wire_cost(T, l, x0, x0, miny, maxy) : wire_cost(T, l, minx, maxx, y0, y0);
+                    va[u] = T.vcost[cell_index(T, l, x1, y0)];
+                    vb[u] = T.vcost[cell_index(T, l, x0, y1)];
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < kHalfLayers; ++u) {
+                const int l = l0 + u;
+                if (l >= L) continue;
+                vN(l) = vn[u];
+                w1(l) = a[u];
+                w2(l) = b[u];
+                vA(l) = va[u];
+                vB(l) = vb[u];
+            }
+        }
+        // Steps 2 and 3a: the child's via stacks, and its best range through
+        // each layer, first minimum in (lo, hi) order.
+        for (int l = 0; l < L; ++l) {
+            cur(l) = kInf;
+            cfrom(l) = 0;
+        }
+        for (int lo = 0; lo < L; ++lo) {
+            double acc = 0;
+            for (int hi = lo; hi < L; ++hi) {
+                if (hi > lo) acc = acc + static_cast<double>(vN(hi - 1));
+                const double v = (fix1 < L && (lo > fix1 || hi < fix1)) ? kInf : acc;
+                for (int l = lo; l <= hi; ++l)
+                    if (v < cur(l)) {
+                        cur(l) = v;
+                        cfrom(l) = static_cast<unsigned short>(lo * L + hi);
+                    }
+            }
+        }
+        // Step 3b: best cost of reaching the parent on each layer.
+        for (int pl = 0; pl < L; ++pl) {
+            double best = kInf;
+            int pb = 0;
+            if (straight) {
+                const bool valid = along_y(T, pl) ? (x1 == x0) : (y1 == y0);
+                if (valid) {
+                    best = cur(pl) + w1(pl);
+                    pb = cfrom(pl) * L * L + pl * L + pl;
+                }
+            } else {
+                for (int cl = (pl & 1) ^ 1; cl < L; cl += 2) {
+                    const double cost = cur(cl) + w1(cl);
+                    double cost2 = 0;
+                    const bool ay = along_y(T, cl);
+                    for (int l = min(cl, pl) + 1; l < max(cl, pl); ++l)
+                        cost2 += static_cast<double>(ay ? vA(l) : vB(l));
+                    cost2 += w2(pl);
+                    if (cost + cost2 < best) {
+                        best = cost + cost2;
+                        pb = cfrom(cl) * L * L + cl * L + pl;
+                    }
+                }
+            }
+            w2(pl) = best;   // w2(pl) is not read again
+            pdiag(pl) = pb;  // vN of the child is not read again
+        }
+    }
+    // The root's via-cost column (vA of the child is not read again).
+    {
+        float v[kMaxLayers];
+#pragma unroll
+        for (int l = 0; l < kMaxLayers; ++l) v[l] = l < L ? T.vcost[l * XY + r0] : 0.f;
+#pragma unroll
+        for (int l = 0; l < kMaxLayers; ++l)
+            if (l < L) vA(l) = v[l];
+    }
+    // Steps 2, 3c, 3d and 4 for the root: its via stacks plus, for a child,
+    // the range minimum of the diagonal; the first minimal range.
+    int choice = 0, bestpath = 0;
+    {
+        double best = 0;
+        for (int lo = 0; lo < L; ++lo) {
+            double acc = 0, c = 0;
+            int path = 0;
+            if (N == 2) {
+                c = w2(lo);
+                path = pdiag(lo);
+            }
+            for (int hi = lo; hi < L; ++hi) {
+                if (hi > lo) acc = acc + static_cast<double>(vA(hi - 1));
+                double v = (fix0 < L && (lo > fix0 || hi < fix0)) ? kInf : acc;
+                if (N == 2) {
+                    if (hi > lo && !(c <= w2(hi))) {
+                        c = w2(hi);
+                        path = pdiag(hi);
+                    }
+                    v += c;
+                }
+                if ((lo == 0 && hi == 0) || v < best) {
+                    best = v;
+                    choice = lo * L + hi;
+                    bestpath = path;
+                }
+            }
+        }
+        if (!(best < kInf)) set_error(T, kEInval, id);
+    }
+    // Step 5: segments in node order.
+    int* out = P.routes + P.route_off[id];
+    const long long cap = P.route_off[id + 1] - P.route_off[id];
+    const int minl0 = choice / L, maxl0 = choice % L;
+    int words = minl0 < maxl0 ? 2 : 0;
+    int minl1 = 0, maxl1 = 0, cl = 0, pl = 0;
+    if (N == 2) {
+        const int r1 = bestpath / (L * L);
+        minl1 = r1 / L;
+        maxl1 = r1 % L;
+        cl = bestpath / L % L;
+        pl = bestpath % L;
+        words += (minl1 < maxl1 ? 2 : 0) + (straight ? 2 : 6);
+    }
+    if (1 + words > cap) {
+        set_error(T, kELimit, id);
+        return;
+    }
+    int* w = out + 1;
+    if (minl0 < maxl0) { *w++ = cell_index(T, minl0, x0, y0); *w++ = cell_index(T, maxl0, x0, y0); }
+    if (N == 2) {
+        if (minl1 < maxl1) { *w++ = cell_index(T, minl1, x1, y1); *w++ = cell_index(T, maxl1, x1, y1); }
+        if (straight) {
+            *w++ = cell_index(T, cl, min(x1, x0), min(y1, y0));
+            *w++ = cell_index(T, cl, max(x1, x0), max(y1, y0));
+        } else if (along_y(T, cl)) {
+            *w++ = cell_index(T, cl, x1, y1);   *w++ = cell_index(T, cl, x1, y0);
+            *w++ = cell_index(T, cl, x1, y0);   *w++ = cell_index(T, pl, x1, y0);
+            *w++ = cell_index(T, pl, x1, y0);   *w++ = cell_index(T, pl, x0, y0);
+        } else {
+            *w++ = cell_index(T, cl, x1, y1);   *w++ = cell_index(T, cl, x0, y1);
+            *w++ = cell_index(T, cl, x0, y1);   *w++ = cell_index(T, pl, x0, y1);
+            *w++ = cell_index(T, pl, x0, y1);   *w++ = cell_index(T, pl, x0, y0);
+        }
+    }
+    out[0] = 1 + words;
+    if (commit) commit_thread_wires(T, P, id, stamp, 1);
+}
+
 }  // namespace grb

@@ -122,6 +122,12 @@ __global__ void k_lshape_bucketed(Tables T, Plan P, int b, int stamp, BucketLaun
     if (warp >= BL.per[bk]) return;
     const int lo = P.bucket_off[b * (kDpBuckets + 1) + bk], hi = P.bucket_off[b * (kDpBuckets + 1) + bk + 1];
     const int k = (int(blockIdx.x) - BL.block_off[bk]) * BL.per[bk] + warp;
+    if (bk == 0) {
+        // Nets of one or two nodes: 32 per warp, one per lane.
+        const int q = lo + 32 * k + lane;
+        lshape_net_pair(T, P, q < hi ? P.bucket_ids[q] : -1, stamp, smem + size_t(warp) * BL.arena[0], lane, false);
+        return;
+    }
     if (lo + k >= hi) return;
     const int id = P.bucket_ids[lo + k];
     const int N = P.node_off[id + 1] - P.node_off[id];
@@ -210,7 +216,9 @@ __global__ void __launch_bounds__(kPersistentThreads, 2) k_lshape_persistent(Tab
         clk.mark(S, 7);
         // Route every net of the batch and commit its wires: size buckets from
         // the largest down (long nets start first), nets taken from the
-        // bucket's work queue `per_grab` at a time.
+        // bucket's work queue `per_grab` at a time.  (In this kernel the
+        // smallest nets are the filler that evens out the warps' finish
+        // times, so they too take a warp each.)
         const int lo = P.batch_off[b], cnt = P.batch_off[b + 1] - lo;
         const Arena A = warp_arena(smem, arena_b, warp, T.L, nmax);
         for (int bk = kDpBuckets - 1; bk >= 0; --bk) {
@@ -1213,8 +1221,11 @@ int launch_buckets(grb_ctx* c, int b, int stamp, int only) {
         BL.per[bk] = c->tune.per_cta[bk];
         BL.nmax[bk] = bk < kDpBuckets - 1 ? std::min(dp_bucket_nodes(bk), std::max(c->max_nodes, 1)) : 0;
         BL.arena[bk] = BL.nmax[bk] ? int(arena_bytes(c->T.L, BL.nmax[bk])) : 0;
+        if (bk == 0) BL.arena[0] = int(std::max<size_t>(BL.arena[0], pair_scratch_bytes()));
         if (cnt <= 0) continue;
-        const int nb = (cnt + BL.per[bk] - 1) / BL.per[bk];
+        // Bucket 0: each warp takes 32 nets (one per lane).
+        const int per_block = BL.per[bk] * (bk == 0 ? 32 : 1);
+        const int nb = (cnt + per_block - 1) / per_block;
         blocks += nb;
         threads = std::max(threads, 32 * BL.per[bk]);
         smem = std::max(smem, size_t(BL.per[bk]) * BL.arena[bk]);

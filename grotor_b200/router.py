@@ -217,7 +217,7 @@ class Router:
 
     def autotune(self, plain: bool = True, persistent: bool = True) -> dict:
         """Pick nets-per-CTA (per-batch DP launch) and nets-per-grab (persistent
-        work queue) by size bucket (<= 4, <= 8, <= 16, > 16 tree nodes) on the
+        work queue) by size bucket (<= 2, <= 8, <= 16, > 16 tree nodes) on the
         current plan; leaves the context reset."""
         per_cta = np.zeros(4, np.int32)
         per_grab = np.zeros(4, np.int32)

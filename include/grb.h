@@ -152,7 +152,7 @@ int grb_ripup_classify(grb_ctx* ctx, int32_t threshold, uint8_t* is_of);
 int grb_ripup_classify_noalloc(grb_ctx* ctx, int32_t threshold, uint8_t* is_of);
 
 /* Autotuner (no counterpart in the reference).  Nets of every batch are
- * scheduled by size bucket (tree nodes <= 4, <= 8, <= 16, more; the
+ * scheduled by size bucket (tree nodes <= 2, <= 8, <= 16, more; the
  * persistent form takes the largest bucket first).  what & 1 times the
  * per-batch DP launch of each bucket on the plan's largest batches for 1, 2,
  * 4 and 8 nets per CTA (arena sized to the bucket); what & 2 runs the
