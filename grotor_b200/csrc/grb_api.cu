@@ -1137,9 +1137,11 @@ Plan make_plan2(const grb_ctx* c) {
 
 int dp_nmax(const grb_ctx* c) { return std::min(c->max_nodes, 16); }
 
-// Global scratch for nets with more nodes than fit a shared-memory arena.
-int ensure_gscratch(grb_ctx* c, int slots) {
-    if (c->max_nodes <= dp_nmax(c)) return GRB_OK;
+
+// Global scratch for nets with more nodes than fit a shared-memory arena of
+// `nmax` nodes.
+int ensure_gscratch(grb_ctx* c, int slots, int nmax) {
+    if (c->max_nodes <= nmax) return GRB_OK;
     const size_t need = size_t(slots) * arena_bytes(c->T.L, c->max_nodes);
     if (need <= c->gscratch_bytes) return GRB_OK;
     if (c->gscratch) cudaFree(c->gscratch);
@@ -1234,7 +1236,7 @@ int launch_buckets(grb_ctx* c, int b, int stamp, int only) {
     BL.block_off[kDpBuckets] = blocks;
     if (!blocks) return GRB_OK;
     if (gslots) {
-        const int rc = ensure_gscratch(c, gslots);
+        const int rc = ensure_gscratch(c, gslots, dp_nmax(c));
         if (rc) return rc;
     }
     const size_t arena_slot = arena_bytes(c->T.L, std::max(c->max_nodes, 1));
@@ -1532,7 +1534,7 @@ int stage_graph(grb_ctx* c, int stamp0) {
         // Scratch must exist before capture (no allocation while capturing).
         int maxcnt = 0;
         for (int b = 0; b < c->n_batches; ++b) maxcnt = std::max(maxcnt, c->h_batch_off[b + 1] - c->h_batch_off[b]);
-        int rc = ensure_gscratch(c, maxcnt + 8);
+        int rc = ensure_gscratch(c, maxcnt + 8, dp_nmax(c));
         if (!rc) rc = ensure_buckets(c);
         if (rc) return rc;
         const int64_t before = c->launches;
@@ -1571,7 +1573,7 @@ int stage_persistent(grb_ctx* c, int stamp0) {
     if (per_sm < 1) return fail(c, GRB_EINVAL, "persistent kernel does not fit on an SM");
     const int blocks = per_sm * c->sms;
     const size_t slot = arena_bytes(c->T.L, std::max(c->max_nodes, 1));
-    int rc = ensure_gscratch(c, blocks * wpb);
+    int rc = ensure_gscratch(c, blocks * wpb, nmax);
     if (rc) return rc;
     if ((rc = ensure_buckets(c))) return rc;
     const int counters = c->n_batches * kDpBuckets;
