@@ -62,6 +62,31 @@ __device__ __forceinline__ void add_via_demand(const Tables& T, int c, int half)
     mark_edge_dirty(T, c);
 }
 
+// Demand of the via stack at (x, y) (ra = x*Y + y) between layers low and
+// high: every layer whose cell no wire of this batch stamped adds K at a track
+// end, else K/2 to the two edges it lands between.  All timestamps of the
+// stack are loaded before the first update.
+__device__ __forceinline__ void via_stack_demand(const Tables& T, int ra, int x, int y, int low, int high, int stamp,
+                                                 int K) {
+    int ts[kMaxLayers];
+#pragma unroll
+    for (int u = 0; u < kMaxLayers; ++u) ts[u] = low + u < high ? T.ts[(low + u) * T.XY + ra] : stamp;
+#pragma unroll
+    for (int u = 0; u < kMaxLayers; ++u) {
+        const int layer = low + u;
+        if (layer >= high || ts[u] >= stamp) continue;
+        const int c = layer * T.XY + ra;
+        const bool ay = along_y(T, layer);
+        const int pos = ay ? y : x, len = ay ? T.Y : T.X, stride = ay ? 1 : T.Y;
+        if (!pos) add_via_demand(T, c, 2 * K);
+        else if (pos == len - 1) add_via_demand(T, c - stride, 2 * K);
+        else {
+            add_via_demand(T, c - stride, K);
+            add_via_demand(T, c, K);
+        }
+    }
+}
+
 // One warp commits the via segments of net `id` (lanes over segments).
 __device__ __forceinline__ void commit_net_vias(const Tables& T, const Plan& P, int id, int stamp, int K,
                                                 int lane) {
@@ -75,18 +100,7 @@ __device__ __forceinline__ void commit_net_vias(const Tables& T, const Plan& P, 
         if (low == high) continue;
         const int ra = a - la * T.XY, x = ra / T.Y, y = ra - x * T.Y;
         vias += high - low;
-        for (int layer = low; layer < high; ++layer) {
-            const int c = layer * T.XY + x * T.Y + y;
-            if (T.ts[c] >= stamp) continue;
-            const bool ay = along_y(T, layer);
-            const int pos = ay ? y : x, len = ay ? T.Y : T.X, stride = ay ? 1 : T.Y;
-            if (!pos) add_via_demand(T, c, 2 * K);
-            else if (pos == len - 1) add_via_demand(T, c - stride, 2 * K);
-            else {
-                add_via_demand(T, c - stride, K);
-                add_via_demand(T, c, K);
-            }
-        }
+        via_stack_demand(T, ra, x, y, low, high, stamp, K);
     }
     for (int s = 16; s; s >>= 1) vias += __shfl_down_sync(0xffffffffu, vias, s);
     if (lane == 0 && vias) atomicAdd(T.vias, static_cast<unsigned long long>(vias * K));
@@ -143,18 +157,7 @@ __device__ __forceinline__ void commit_thread_vias(const Tables& T, const Plan& 
         if (low == high) continue;
         const int ra = a - la * T.XY, x = ra / T.Y, y = ra - x * T.Y;
         vias += high - low;
-        for (int layer = low; layer < high; ++layer) {
-            const int c = layer * T.XY + x * T.Y + y;
-            if (T.ts[c] >= stamp) continue;
-            const bool ay = along_y(T, layer);
-            const int pos = ay ? y : x, len = ay ? T.Y : T.X, stride = ay ? 1 : T.Y;
-            if (!pos) add_via_demand(T, c, 2 * K);
-            else if (pos == len - 1) add_via_demand(T, c - stride, 2 * K);
-            else {
-                add_via_demand(T, c - stride, K);
-                add_via_demand(T, c, K);
-            }
-        }
+        via_stack_demand(T, ra, x, y, low, high, stamp, K);
     }
     if (vias) atomicAdd(T.vias, static_cast<unsigned long long>(vias * K));
 }
