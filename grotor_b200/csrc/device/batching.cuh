@@ -213,6 +213,8 @@ __device__ __forceinline__ void batch_clear(const BatchState& B, int s, bool nex
 
 // Step 2: per query point, OR the cell's colours, the earlier nets' bits of
 // this chunk and (lookback) the previous chunk's bits into the net's column.
+// Each item is a 16-byte group of one record (W is a multiple of 4; a
+// chunk-local record is 16 words).
 __device__ __forceinline__ void batch_gather(const BatchState& B, int s, bool lookback, long long t, long long nt) {
     const int chunk = s / kChunk, m = min(kChunk, B.n - s), W = B.W;
     const unsigned* lm = chunk_mask(B, chunk);
@@ -220,31 +222,42 @@ __device__ __forceinline__ void batch_gather(const BatchState& B, int s, bool lo
     unsigned* F = B.fmask + size_t(chunk & 1) * W * kChunk;
     unsigned* P = B.pred + size_t(chunk & 1) * kChunkWords * kChunk;
     unsigned* Q = B.prevp + size_t(chunk & 1) * kChunkWords * kChunk;
-    const int per = W + kChunkWords * (lookback ? 2 : 1);
+    const int gw = W / 4, gl = kChunkWords / 4;
+    const int per = gw + gl * (lookback ? 2 : 1);
     const long long a = B.pt_off[s], b = B.pt_off[s + m];
     const long long items = (b - a) * per;
     for (long long k = t; k < items; k += nt) {
         const long long pi = k / per;
-        const int w = int(k - pi * per);
+        const int g = int(k - pi * per);
         const unsigned q = __ldg(B.pt_cell + a + pi);
         const int jj = __ldg(B.pt_jj + a + pi);
-        unsigned v;
+        uint4 v;
         unsigned* dst;
-        if (w < W) {
-            v = __ldcg(B.cellmask + size_t(q) * W + w);
-            dst = F + size_t(w) * kChunk + jj;
-        } else if (w < W + kChunkWords) {
-            const int pw = w - W;
-            if (pw > (jj >> 5)) continue;
-            v = __ldcg(lm + size_t(q) * kChunkWords + pw);
-            if (pw == (jj >> 5)) v &= (1u << (jj & 31)) - 1u;
-            dst = P + pw * kChunk + jj;
+        int w0;
+        if (g < gw) {
+            w0 = 4 * g;
+            v = __ldcg(reinterpret_cast<const uint4*>(B.cellmask + size_t(q) * W) + g);
+            dst = F;
+        } else if (g < gw + gl) {
+            w0 = 4 * (g - gw);
+            if (w0 > (jj >> 5)) continue;
+            v = __ldcg(reinterpret_cast<const uint4*>(lm + size_t(q) * kChunkWords) + (g - gw));
+            const unsigned own = (1u << (jj & 31)) - 1u;  // earlier nets of the own word
+            const int ow = (jj >> 5) - w0;
+            if (ow == 0) { v.x &= own; v.y = v.z = v.w = 0u; }
+            else if (ow == 1) { v.y &= own; v.z = v.w = 0u; }
+            else if (ow == 2) { v.z &= own; v.w = 0u; }
+            else if (ow == 3) v.w &= own;
+            dst = P;
         } else {
-            const int qw = w - W - kChunkWords;
-            v = __ldcg(lp + size_t(q) * kChunkWords + qw);
-            dst = Q + qw * kChunk + jj;
+            w0 = 4 * (g - gw - gl);
+            v = __ldcg(reinterpret_cast<const uint4*>(lp + size_t(q) * kChunkWords) + (g - gw - gl));
+            dst = Q;
         }
-        if (v) red_or(dst, v);
+        if (v.x) red_or(dst + size_t(w0) * kChunk + jj, v.x);
+        if (v.y) red_or(dst + size_t(w0 + 1) * kChunk + jj, v.y);
+        if (v.z) red_or(dst + size_t(w0 + 2) * kChunk + jj, v.z);
+        if (v.w) red_or(dst + size_t(w0 + 3) * kChunk + jj, v.w);
     }
 }
 
