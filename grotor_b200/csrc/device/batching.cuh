@@ -55,7 +55,8 @@ struct BatchState {
     long long* pt_off;          // [n+1]
     unsigned* pt_cell;          // query points
     unsigned short* pt_jj;
-    unsigned* cellmask;         // [X*Y][W]
+    unsigned* cellmask;         // [W][X*Y]: word w of every cell contiguous, so the
+                                // colour ORs of consecutive cells share sectors
     unsigned* localmask[3];     // [X*Y][kChunkWords], chunk k in buffer k % 3
     unsigned* ptchunk;          // [X*Y] bit k % 32: the cell is a query point of chunk k
     unsigned* fmask;            // [2][W][kChunk] forbidden colours, by chunk parity
@@ -236,7 +237,11 @@ __device__ __forceinline__ void batch_gather(const BatchState& B, int s, bool lo
         int w0;
         if (g < gw) {
             w0 = 4 * g;
-            v = __ldcg(reinterpret_cast<const uint4*>(B.cellmask + size_t(q) * W) + g);
+            const size_t XY = size_t(B.X) * B.Y;
+            v.x = __ldcg(B.cellmask + (4 * g) * XY + q);
+            v.y = __ldcg(B.cellmask + (4 * g + 1) * XY + q);
+            v.z = __ldcg(B.cellmask + (4 * g + 2) * XY + q);
+            v.w = __ldcg(B.cellmask + (4 * g + 3) * XY + q);
             dst = F;
         } else if (g < gw + gl) {
             w0 = 4 * (g - gw);
@@ -269,7 +274,7 @@ __device__ __forceinline__ void batch_publish(const BatchState& B, int s, long l
         const unsigned q = __ldg(B.mark_cell + k);
         const int jj = __ldg(B.mark_jj + k);
         const int c = __ldcg(B.batch_of + s + jj);
-        red_or(B.cellmask + size_t(q) * B.W + (c >> 5), 1u << (c & 31));
+        red_or(B.cellmask + size_t(c >> 5) * B.X * B.Y + q, 1u << (c & 31));
     }
 }
 
