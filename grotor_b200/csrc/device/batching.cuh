@@ -39,8 +39,10 @@
 
 namespace grb {
 
-constexpr int kChunk = 512;     // nets per chunk (== threads of the solve CTA)
-constexpr int kChunkWords = kChunk / 32;
+// Nets per chunk: CH = 512 or 1024 (== threads of the solve CTA), a template
+// parameter of every per-chunk step; storage is sized for the larger.
+constexpr int kChunkMax = 1024;
+constexpr int kChunkMaxWords = kChunkMax / 32;
 
 struct BatchState {
     int X, Y, n, limit, sparsity, W;   // W: colour words per cell
@@ -57,11 +59,11 @@ struct BatchState {
     unsigned short* pt_jj;
     unsigned* cellmask;         // [W][X*Y]: word w of every cell contiguous, so the
                                 // colour ORs of consecutive cells share sectors
-    unsigned* localmask[3];     // [X*Y][kChunkWords], chunk k in buffer k % 3
+    unsigned* localmask[3];     // [X*Y][CH/32], chunk k in buffer k % 3
     unsigned* ptchunk;          // [X*Y] bit k % 32: the cell is a query point of chunk k
-    unsigned* fmask;            // [2][W][kChunk] forbidden colours, by chunk parity
-    unsigned* pred;             // [2][kChunkWords][kChunk] predecessors inside the chunk
-    unsigned* prevp;            // [2][kChunkWords][kChunk] marking nets of the previous chunk
+    unsigned* fmask;            // [2][W][CH] forbidden colours, by chunk parity
+    unsigned* pred;             // [2][CH/32][CH] predecessors inside the chunk
+    unsigned* prevp;            // [2][CH/32][CH] marking nets of the previous chunk
     unsigned* fullmask;         // [W]
     int* count;                 // [32*W]
     int* n_colors;              // [1]
@@ -135,7 +137,8 @@ __device__ __forceinline__ void flat_count(const BatchState& B, int p) {
 __device__ __forceinline__ void flat_fill(const BatchState& B, int p) {
     const int lane = threadIdx.x & 31;
     const int id = B.order[p];
-    const unsigned short jj = static_cast<unsigned short>(p % kChunk);
+    // Position inside a chunk of kChunkMax; reduced mod CH where read.
+    const unsigned short jj = static_cast<unsigned short>(p % kChunkMax);
     long long o = B.mark_off[p];
     auto put = [&](int cell, int k, int) {
         B.mark_cell[o + k] = static_cast<unsigned>(cell);
@@ -168,9 +171,10 @@ __device__ __forceinline__ unsigned* chunk_mask(const BatchState& B, int chunk) 
 
 // Query-point bits of the chunk at s: bit (chunk % 32) of every query point
 // cell of the chunk is set (set) or cleared.
+template <int CH>
 __device__ __forceinline__ void batch_point_bits(const BatchState& B, int s, bool set, long long t, long long nt) {
-    const int m = min(kChunk, B.n - s);
-    const unsigned bit = 1u << ((s / kChunk) & 31);
+    const int m = min(CH, B.n - s);
+    const unsigned bit = 1u << ((s / CH) & 31);
     const long long a = B.pt_off[s], b = B.pt_off[s + m];
     for (long long k = a + t; k < b; k += nt) {
         unsigned* w = B.ptchunk + __ldg(B.pt_cell + k);
@@ -184,46 +188,50 @@ __device__ __forceinline__ void batch_point_bits(const BatchState& B, int s, boo
 // back, so the raster keeps the marks whose cell has one of those query-point
 // bits; the bits live in a 4-byte-per-cell array that stays in L2, the
 // chunk-local masks do not.  Threads t of nt.
+template <int CH>
 __device__ __forceinline__ void batch_raster(const BatchState& B, int s, bool next, long long t, long long nt) {
-    const int m = min(kChunk, B.n - s), chunk = s / kChunk;
+    const int m = min(CH, B.n - s), chunk = s / CH;
     const unsigned want = (1u << (chunk & 31)) | (next ? 1u << ((chunk + 1) & 31) : 0u);
     unsigned* lm = chunk_mask(B, chunk);
     const long long a = B.mark_off[s], b = B.mark_off[s + m];
     for (long long k = a + t; k < b; k += nt) {
         const unsigned q = __ldg(B.mark_cell + k);
-        const int jj = __ldg(B.mark_jj + k);
-        if (__ldcg(B.ptchunk + q) & want) red_or(lm + size_t(q) * kChunkWords + (jj >> 5), 1u << (jj & 31));
+        const int jj = __ldg(B.mark_jj + k) & (CH - 1);
+        if (__ldcg(B.ptchunk + q) & want) red_or(lm + size_t(q) * (CH / 32) + (jj >> 5), 1u << (jj & 31));
     }
 }
 
 // The chunk-local mask of the chunk at s is nonzero only at query points of
-// this chunk and (with `next`) the next one: zero the whole 64-byte record of
-// each of those cells.
+// this chunk and (with `next`) the next one: zero the whole record of each of
+// those cells.
+template <int CH>
 __device__ __forceinline__ void batch_clear(const BatchState& B, int s, bool next, long long t, long long nt) {
-    unsigned* lm = chunk_mask(B, s / kChunk);
+    unsigned* lm = chunk_mask(B, s / CH);
     const long long a = B.pt_off[s];
-    const long long b = B.pt_off[min(s + (next ? 2 : 1) * kChunk, B.n)];
-    const long long items = (b - a) * 4;
+    const long long b = B.pt_off[min(s + (next ? 2 : 1) * CH, B.n)];
+    constexpr int kParts = (CH / 32) / 4;  // 16-byte groups of a record
+    const long long items = (b - a) * kParts;
     for (long long k = t; k < items; k += nt) {
-        const long long pi = a + k / 4;
-        const int part = int(k & 3);
-        uint4* rec = reinterpret_cast<uint4*>(lm + size_t(__ldg(B.pt_cell + pi)) * kChunkWords);
+        const long long pi = a + k / kParts;
+        const int part = int(k % kParts);
+        uint4* rec = reinterpret_cast<uint4*>(lm + size_t(__ldg(B.pt_cell + pi)) * (CH / 32));
         rec[part] = make_uint4(0u, 0u, 0u, 0u);
     }
 }
 
 // Step 2: per query point, OR the cell's colours, the earlier nets' bits of
 // this chunk and (lookback) the previous chunk's bits into the net's column.
-// Each item is a 16-byte group of one record (W is a multiple of 4; a
-// chunk-local record is 16 words).
+// Each item is a 16-byte group of one record (W and (CH / 32) are
+// multiples of 4).
+template <int CH>
 __device__ __forceinline__ void batch_gather(const BatchState& B, int s, bool lookback, long long t, long long nt) {
-    const int chunk = s / kChunk, m = min(kChunk, B.n - s), W = B.W;
+    const int chunk = s / CH, m = min(CH, B.n - s), W = B.W;
     const unsigned* lm = chunk_mask(B, chunk);
     const unsigned* lp = lookback ? chunk_mask(B, chunk - 1) : nullptr;
-    unsigned* F = B.fmask + size_t(chunk & 1) * W * kChunk;
-    unsigned* P = B.pred + size_t(chunk & 1) * kChunkWords * kChunk;
-    unsigned* Q = B.prevp + size_t(chunk & 1) * kChunkWords * kChunk;
-    const int gw = W / 4, gl = kChunkWords / 4;
+    unsigned* F = B.fmask + size_t(chunk & 1) * W * CH;
+    unsigned* P = B.pred + size_t(chunk & 1) * (CH / 32) * CH;
+    unsigned* Q = B.prevp + size_t(chunk & 1) * (CH / 32) * CH;
+    const int gw = W / 4, gl = (CH / 32) / 4;
     const int per = gw + gl * (lookback ? 2 : 1);
     const long long a = B.pt_off[s], b = B.pt_off[s + m];
     const long long items = (b - a) * per;
@@ -231,7 +239,7 @@ __device__ __forceinline__ void batch_gather(const BatchState& B, int s, bool lo
         const long long pi = k / per;
         const int g = int(k - pi * per);
         const unsigned q = __ldg(B.pt_cell + a + pi);
-        const int jj = __ldg(B.pt_jj + a + pi);
+        const int jj = __ldg(B.pt_jj + a + pi) & (CH - 1);
         uint4 v;
         unsigned* dst;
         int w0;
@@ -246,7 +254,7 @@ __device__ __forceinline__ void batch_gather(const BatchState& B, int s, bool lo
         } else if (g < gw + gl) {
             w0 = 4 * (g - gw);
             if (w0 > (jj >> 5)) continue;
-            v = __ldcg(reinterpret_cast<const uint4*>(lm + size_t(q) * kChunkWords) + (g - gw));
+            v = __ldcg(reinterpret_cast<const uint4*>(lm + size_t(q) * (CH / 32)) + (g - gw));
             const unsigned own = (1u << (jj & 31)) - 1u;  // earlier nets of the own word
             const int ow = (jj >> 5) - w0;
             if (ow == 0) { v.x &= own; v.y = v.z = v.w = 0u; }
@@ -256,23 +264,24 @@ __device__ __forceinline__ void batch_gather(const BatchState& B, int s, bool lo
             dst = P;
         } else {
             w0 = 4 * (g - gw - gl);
-            v = __ldcg(reinterpret_cast<const uint4*>(lp + size_t(q) * kChunkWords) + (g - gw - gl));
+            v = __ldcg(reinterpret_cast<const uint4*>(lp + size_t(q) * (CH / 32)) + (g - gw - gl));
             dst = Q;
         }
-        if (v.x) red_or(dst + size_t(w0) * kChunk + jj, v.x);
-        if (v.y) red_or(dst + size_t(w0 + 1) * kChunk + jj, v.y);
-        if (v.z) red_or(dst + size_t(w0 + 2) * kChunk + jj, v.z);
-        if (v.w) red_or(dst + size_t(w0 + 3) * kChunk + jj, v.w);
+        if (v.x) red_or(dst + size_t(w0) * CH + jj, v.x);
+        if (v.y) red_or(dst + size_t(w0 + 1) * CH + jj, v.y);
+        if (v.z) red_or(dst + size_t(w0 + 2) * CH + jj, v.z);
+        if (v.w) red_or(dst + size_t(w0 + 3) * CH + jj, v.w);
     }
 }
 
 // Step 4: the chunk at s publishes its colours.
+template <int CH>
 __device__ __forceinline__ void batch_publish(const BatchState& B, int s, long long t, long long nt) {
-    const int m = min(kChunk, B.n - s);
+    const int m = min(CH, B.n - s);
     const long long a = B.mark_off[s], b = B.mark_off[s + m];
     for (long long k = a + t; k < b; k += nt) {
         const unsigned q = __ldg(B.mark_cell + k);
-        const int jj = __ldg(B.mark_jj + k);
+        const int jj = __ldg(B.mark_jj + k) & (CH - 1);
         const int c = __ldcg(B.batch_of + s + jj);
         red_or(B.cellmask + size_t(c >> 5) * B.X * B.Y + q, 1u << (c & 31));
     }
@@ -280,12 +289,12 @@ __device__ __forceinline__ void batch_publish(const BatchState& B, int s, long l
 
 // Shared memory of the solving CTA (kept across chunks in the persistent form).
 struct SolveSmem {
-    unsigned* U;     // [W][kChunk] colours a net may not take (published, full, previous chunk)
-    unsigned* P;     // [kChunkWords][kChunk] predecessor bits
-    int* col;        // [kChunk] colour of each net of the chunk
-    int* colp;       // [kChunk] colours of the previous chunk
+    unsigned* U;     // [W][CH] colours a net may not take (published, full, previous chunk)
+    unsigned* P;     // [(CH / 32)][CH] predecessor bits
+    int* col;        // [CH] colour of each net of the chunk
+    int* colp;       // [CH] colours of the previous chunk
     int* cnt;        // [32W] nets per colour so far
-    int* wh;         // [kChunk/32][32W] per-warp colour counts (zero between uses), or
+    int* wh;         // [CH/32][32W] per-warp colour counts (zero between uses), or
                      // for W > kWarpCountWords a [32W] running count
     bool per_warp;   // wh holds per-warp counts
     unsigned* full;  // [W] colours whose batch is full
@@ -295,44 +304,59 @@ struct SolveSmem {
 // barriers); beyond it, warps add their counts in turn (one barrier per warp).
 constexpr int kWarpCountWords = 32;
 
+// Shared memory a solving CTA may use (the per-warp colour counts are dropped
+// for the running count when they do not fit).
+constexpr size_t kSolveSmemLimit = 220 * 1024;
+template <int CH>
+__host__ __device__ __forceinline__ size_t solve_smem_base(int W) {
+    const size_t C = 32 * size_t(W);
+    return size_t(CH) * W * 4 + size_t(CH) * (CH / 32) * 4 + 2 * size_t(CH) * 4 + C * 4 + size_t(W) * 4;
+}
+template <int CH>
+__host__ __device__ __forceinline__ bool solve_per_warp(int W) {
+    return W <= kWarpCountWords && solve_smem_base<CH>(W) + (CH / 32) * 32 * size_t(W) * 4 <= kSolveSmemLimit;
+}
+template <int CH>
 __host__ __device__ __forceinline__ size_t solve_smem_bytes(int W) {
     const size_t C = 32 * size_t(W);
-    const size_t wh = W <= kWarpCountWords ? (kChunk / 32) * C : C;
-    return size_t(kChunk) * W * 4 + size_t(kChunk) * kChunkWords * 4 + 2 * size_t(kChunk) * 4 + C * 4 + wh * 4 +
+    const size_t wh = solve_per_warp<CH>(W) ? (CH / 32) * C : C;
+    return size_t(CH) * W * 4 + size_t(CH) * (CH / 32) * 4 + 2 * size_t(CH) * 4 + C * 4 + wh * 4 +
            size_t(W) * 4;
 }
 
+template <int CH>
 __device__ __forceinline__ SolveSmem solve_smem(unsigned* base, int W) {
     const int C = 32 * W;
     SolveSmem S;
     S.U = base;
-    S.P = S.U + size_t(kChunk) * W;
-    S.col = reinterpret_cast<int*>(S.P + size_t(kChunk) * kChunkWords);
-    S.colp = S.col + kChunk;
-    S.cnt = S.colp + kChunk;
+    S.P = S.U + size_t(CH) * W;
+    S.col = reinterpret_cast<int*>(S.P + size_t(CH) * (CH / 32));
+    S.colp = S.col + CH;
+    S.cnt = S.colp + CH;
     S.wh = S.cnt + C;
-    S.per_warp = W <= kWarpCountWords;
-    S.full = reinterpret_cast<unsigned*>(S.wh + (S.per_warp ? (kChunk / 32) * C : C));
+    S.per_warp = solve_per_warp<CH>(W);
+    S.full = reinterpret_cast<unsigned*>(S.wh + (S.per_warp ? (CH / 32) * C : C));
     return S;
 }
 
 // The smallest colour c >= c0 net `tid` may take: not in U, not held by a
 // predecessor (pmask: which predecessor words are nonzero).  C if none.
+template <int CH>
 __device__ __forceinline__ int first_fit(const SolveSmem& S, int tid, int W, unsigned pmask, int c0) {
     int c = c0;
     while (true) {
         int w = c >> 5;
         if (w >= W) return 32 * W;
-        unsigned used = S.U[w * kChunk + tid] | ((1u << (c & 31)) - 1u);
+        unsigned used = S.U[w * CH + tid] | ((1u << (c & 31)) - 1u);
         while (used == 0xffffffffu) {
             if (++w >= W) return 32 * W;
-            used = S.U[w * kChunk + tid];
+            used = S.U[w * CH + tid];
         }
         c = w * 32 + __ffs(~used) - 1;
         bool hit = false;
         for (unsigned pm = pmask; pm && !hit; pm &= pm - 1) {
             const int pw = __ffs(pm) - 1;
-            unsigned bits = S.P[pw * kChunk + tid];
+            unsigned bits = S.P[pw * CH + tid];
             while (bits) {
                 const int i = pw * 32 + __ffs(bits) - 1;
                 bits &= bits - 1;
@@ -344,29 +368,32 @@ __device__ __forceinline__ int first_fit(const SolveSmem& S, int tid, int W, uns
     }
 }
 
-// The solve runs on threads 0..kChunk-1 of its CTA and synchronises them
+// The solve runs on threads 0..CH-1 of its CTA and synchronises them
 // with named barrier 1 (the CTA may hold more threads, which do not take part).
-__device__ __forceinline__ void solve_sync() { asm volatile("bar.sync 1, %0;" ::"n"(kChunk) : "memory"); }
+template <int CH>
+__device__ __forceinline__ void solve_sync() { asm volatile("bar.sync 1, %0;" ::"n"(CH) : "memory"); }
+template <int CH>
 __device__ __forceinline__ bool solve_sync_or(bool v) {
     int r;
     asm volatile(
         "{\n .reg .pred p, q;\n setp.ne.s32 p, %1, 0;\n bar.red.or.pred q, 1, %2, p;\n selp.s32 %0, 1, 0, q;\n}"
-        : "=r"(r) : "r"(int(v)), "n"(kChunk) : "memory");
+        : "=r"(r) : "r"(int(v)), "n"(CH) : "memory");
     return r != 0;
 }
 
-// Step 3 (threads 0..kChunk-1 of a CTA): first-fit of the chunk at order
+// Step 3 (threads 0..CH-1 of a CTA): first-fit of the chunk at order
 // position s.  S.cnt and S.full hold the state of the chunks before it;
 // with `lookback`, S.colp holds the previous chunk's colours.  The chunk's
-// tables are read once and cleared for reuse by chunk s + 2 * kChunk.
+// tables are read once and cleared for reuse by chunk s + 2 * CH.
 // Returns false on colour overflow (kELimit recorded).
+template <int CH>
 __device__ __forceinline__ bool batch_solve(const BatchState& B, int s, bool lookback, const SolveSmem& S) {
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int chunk = s / kChunk, m = min(kChunk, B.n - s);
+    const int chunk = s / CH, m = min(CH, B.n - s);
     const int W = B.W, C = 32 * W;
-    unsigned* Fg = B.fmask + size_t(chunk & 1) * W * kChunk;
-    unsigned* Pg = B.pred + size_t(chunk & 1) * kChunkWords * kChunk;
-    unsigned* Qg = B.prevp + size_t(chunk & 1) * kChunkWords * kChunk;
+    unsigned* Fg = B.fmask + size_t(chunk & 1) * W * CH;
+    unsigned* Pg = B.pred + size_t(chunk & 1) * (CH / 32) * CH;
+    unsigned* Qg = B.prevp + size_t(chunk & 1) * (CH / 32) * CH;
     __shared__ int first_bad, overflow;
     if (tid == 0) overflow = 0;
     unsigned pmask = 0;
@@ -377,43 +404,43 @@ __device__ __forceinline__ bool batch_solve(const BatchState& B, int s, bool loo
         for (int w0 = 0; w0 < W; w0 += 8) {
             unsigned v[8];
 #pragma unroll
-            for (int k = 0; k < 8; ++k) v[k] = w0 + k < W ? __ldcg(Fg + size_t(w0 + k) * kChunk + tid) : 0u;
+            for (int k = 0; k < 8; ++k) v[k] = w0 + k < W ? __ldcg(Fg + size_t(w0 + k) * CH + tid) : 0u;
 #pragma unroll
             for (int k = 0; k < 8; ++k) {
                 if (w0 + k >= W) break;
-                if (v[k]) Fg[size_t(w0 + k) * kChunk + tid] = 0u;
-                S.U[(w0 + k) * kChunk + tid] = v[k] | S.full[w0 + k];
+                if (v[k]) Fg[size_t(w0 + k) * CH + tid] = 0u;
+                S.U[(w0 + k) * CH + tid] = v[k] | S.full[w0 + k];
             }
         }
         {
-            unsigned v[kChunkWords];
+            unsigned v[(CH / 32)];
 #pragma unroll
-            for (int w = 0; w < kChunkWords; ++w) v[w] = w <= (tid >> 5) ? __ldcg(Pg + w * kChunk + tid) : 0u;
+            for (int w = 0; w < (CH / 32); ++w) v[w] = w <= (tid >> 5) ? __ldcg(Pg + w * CH + tid) : 0u;
 #pragma unroll
-            for (int w = 0; w < kChunkWords; ++w) {
-                S.P[w * kChunk + tid] = v[w];
-                if (v[w]) { Pg[w * kChunk + tid] = 0u; pmask |= 1u << w; }
+            for (int w = 0; w < (CH / 32); ++w) {
+                S.P[w * CH + tid] = v[w];
+                if (v[w]) { Pg[w * CH + tid] = 0u; pmask |= 1u << w; }
             }
         }
         if (lookback) {
-            unsigned v[kChunkWords];
+            unsigned v[(CH / 32)];
 #pragma unroll
-            for (int w = 0; w < kChunkWords; ++w) v[w] = __ldcg(Qg + w * kChunk + tid);
+            for (int w = 0; w < (CH / 32); ++w) v[w] = __ldcg(Qg + w * CH + tid);
 #pragma unroll
-            for (int w = 0; w < kChunkWords; ++w) {
+            for (int w = 0; w < (CH / 32); ++w) {
                 unsigned bits = v[w];
-                if (bits) Qg[w * kChunk + tid] = 0u;
+                if (bits) Qg[w * CH + tid] = 0u;
                 while (bits) {
                     const int c = S.colp[w * 32 + __ffs(bits) - 1];
                     bits &= bits - 1;
-                    S.U[(c >> 5) * kChunk + tid] |= 1u << (c & 31);
+                    S.U[(c >> 5) * CH + tid] |= 1u << (c & 31);
                 }
             }
         }
-        c0 = first_fit(S, tid, W, 0u, 0);
+        c0 = first_fit<CH>(S, tid, W, 0u, 0);
     }
     S.col[tid] = -1;
-    solve_sync();
+    solve_sync<CH>();
     int fixed = 0;  // nets below `fixed` are final
     int rank = 0;
     while (true) {
@@ -421,13 +448,13 @@ __device__ __forceinline__ bool batch_solve(const BatchState& B, int s, bool loo
         while (true) {
             int mine = tid < m ? S.col[tid] : -1;
             if (tid < m && tid >= fixed) {
-                mine = first_fit(S, tid, W, pmask, c0);
+                mine = first_fit<CH>(S, tid, W, pmask, c0);
                 if (mine >= C) { overflow = 1; mine = C - 1; }
             }
-            solve_sync();
+            solve_sync<CH>();
             const bool changed = tid < m && S.col[tid] != mine;
             if (tid < m) S.col[tid] = mine;
-            if (!solve_sync_or(changed)) break;
+            if (!solve_sync_or<CH>(changed)) break;
         }
         if (overflow) break;
         // Position of every net inside its batch, in chunk order: colour
@@ -439,25 +466,25 @@ __device__ __forceinline__ bool batch_solve(const BatchState& B, int s, bool loo
         const int within = __popc(peers & ((1u << lane) - 1u));
         if (S.per_warp) {
             if (leader) S.wh[warp * C + c] = __popc(peers);
-            solve_sync();
+            solve_sync<CH>();
             if (tid < m) {
                 int r = S.cnt[c] + within;
                 for (int w = 0; w < warp; ++w) r += S.wh[w * C + c];
                 rank = r;
                 if (r >= B.limit) atomicMin(&first_bad, tid);
             }
-            solve_sync();
+            solve_sync<CH>();
             if (leader) S.wh[warp * C + c] = 0;
         } else {
-            for (int k = tid; k < C; k += kChunk) S.wh[k] = S.cnt[k];
-            solve_sync();
+            for (int k = tid; k < C; k += CH) S.wh[k] = S.cnt[k];
+            solve_sync<CH>();
             for (int w = 0; w < (m + 31) / 32; ++w) {
                 if (warp == w && tid < m) {
                     rank = S.wh[c] + within;
                     if (leader) S.wh[c] += __popc(peers);
                     if (rank >= B.limit) atomicMin(&first_bad, tid);
                 }
-                solve_sync();
+                solve_sync<CH>();
             }
         }
         const int bad = first_bad;
@@ -469,11 +496,11 @@ __device__ __forceinline__ bool batch_solve(const BatchState& B, int s, bool loo
         const int fc = S.col[bad];
         if (tid == 0) S.full[fc >> 5] |= 1u << (fc & 31);
         if (tid >= bad && tid < m) {
-            S.U[(fc >> 5) * kChunk + tid] |= 1u << (fc & 31);
-            c0 = first_fit(S, tid, W, 0u, c0);
+            S.U[(fc >> 5) * CH + tid] |= 1u << (fc & 31);
+            c0 = first_fit<CH>(S, tid, W, 0u, c0);
         }
         fixed = bad;
-        solve_sync();
+        solve_sync<CH>();
     }
     if (overflow) {
         if (tid == 0) batch_error(B, kELimit, s);
@@ -489,7 +516,7 @@ __device__ __forceinline__ bool batch_solve(const BatchState& B, int s, bool loo
     }
     for (int o = 16; o; o >>= 1) top = max(top, __shfl_xor_sync(0xffffffffu, top, o));
     if (lane == 0 && top) atomicMax(B.n_colors, top);
-    solve_sync();
+    solve_sync<CH>();
     return true;
 }
 

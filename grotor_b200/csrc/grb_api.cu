@@ -711,38 +711,43 @@ __global__ void k_scan_add(long long* a, int n, const long long* sums, int tiles
 // Plain form: one launch per step and chunk.
 __device__ __forceinline__ long long launch_thread() { return blockIdx.x * (long long)blockDim.x + threadIdx.x; }
 __device__ __forceinline__ long long launch_threads() { return (long long)gridDim.x * blockDim.x; }
-__global__ void k_batch_point_bits(BatchState B, int s) { batch_point_bits(B, s, true, launch_thread(), launch_threads()); }
-__global__ void k_batch_raster(BatchState B, int s) { batch_raster(B, s, false, launch_thread(), launch_threads()); }
+template <int CH>
+__global__ void k_batch_point_bits(BatchState B, int s) { batch_point_bits<CH>(B, s, true, launch_thread(), launch_threads()); }
+template <int CH>
+__global__ void k_batch_raster(BatchState B, int s) { batch_raster<CH>(B, s, false, launch_thread(), launch_threads()); }
+template <int CH>
 __global__ void k_batch_gather(BatchState B, int s) {
-    batch_gather(B, s, false, blockIdx.x * (long long)blockDim.x + threadIdx.x, (long long)gridDim.x * blockDim.x);
+    batch_gather<CH>(B, s, false, blockIdx.x * (long long)blockDim.x + threadIdx.x, (long long)gridDim.x * blockDim.x);
 }
-__global__ void __launch_bounds__(kChunk) k_batch_solve(BatchState B, int s) {
+template <int CH>
+__global__ void __launch_bounds__(CH) k_batch_solve(BatchState B, int s) {
     extern __shared__ __align__(16) unsigned bsm[];
     if (*reinterpret_cast<volatile int*>(B.error)) return;
-    const SolveSmem S = solve_smem(bsm, B.W);
+    const SolveSmem S = solve_smem<CH>(bsm, B.W);
     const int C = 32 * B.W;
     for (int k = threadIdx.x; k < C; k += blockDim.x) S.cnt[k] = B.count[k];
     if (S.per_warp)
-        for (int k = threadIdx.x; k < (kChunk / 32) * C; k += blockDim.x) S.wh[k] = 0;
+        for (int k = threadIdx.x; k < (CH / 32) * C; k += blockDim.x) S.wh[k] = 0;
     for (int k = threadIdx.x; k < B.W; k += blockDim.x) S.full[k] = B.fullmask[k];
     __syncthreads();
-    if (!batch_solve(B, s, false, S)) return;
+    if (!batch_solve<CH>(B, s, false, S)) return;
     for (int k = threadIdx.x; k < C; k += blockDim.x) B.count[k] = S.cnt[k];
     for (int k = threadIdx.x; k < B.W; k += blockDim.x) B.fullmask[k] = S.full[k];
 }
 // Publish chunk s, empty its chunk-local mask and query-point bits, and set
 // the next chunk's query-point bits.
+template <int CH>
 __global__ void k_batch_publish(BatchState B, int s) {
     if (*reinterpret_cast<volatile int*>(B.error)) return;
     const long long t = launch_thread(), nt = launch_threads();
-    batch_publish(B, s, t, nt);
-    batch_clear(B, s, false, t, nt);
-    batch_point_bits(B, s, false, t, nt);
-    if (s + kChunk < B.n) batch_point_bits(B, s + kChunk, true, t, nt);
+    batch_publish<CH>(B, s, t, nt);
+    batch_clear<CH>(B, s, false, t, nt);
+    batch_point_bits<CH>(B, s, false, t, nt);
+    if (s + CH < B.n) batch_point_bits<CH>(B, s + CH, true, t, nt);
 }
 
 // Persistent batching: CTAs of kPersistThreads threads, one per SM, at least
-// two.  CTA 0 is the solver and has its SM to itself (its first kChunk
+// two.  CTA 0 is the solver and has its SM to itself (its first CH
 // threads solve, the rest leave): for chunk r it waits until the other CTAs
 // (G of them, one shared barrier counter) have gathered chunk r, solves it,
 // and releases `solved` = r + 1.  The other CTAs set the query-point bits of
@@ -756,45 +761,46 @@ __global__ void k_batch_publish(BatchState B, int s) {
 //      (its buffer was emptied in A)                           | barrier
 // The barrier after B(r) is what the solver waits for before chunk r+1
 // (counter (3 + 2(r+1)) * G).
-constexpr int kPersistThreads = 2 * kChunk;
+constexpr int kPersistThreads = kChunkMax;
+template <int CH>
 __global__ void __launch_bounds__(kPersistThreads, 1) k_batch_persistent(BatchState B, GridSync S, Tables T) {
     extern __shared__ __align__(16) unsigned bsm[];
     __shared__ int go;
-    const int chunks = (B.n + kChunk - 1) / kChunk;
+    const int chunks = (B.n + CH - 1) / CH;
     const unsigned G = gridDim.x - 1;
     if (blockIdx.x == 0) {
-        if (threadIdx.x >= kChunk) return;
+        if (threadIdx.x >= CH) return;
         PhaseClock clk{0, 0};
         clk.start(S);
-        const SolveSmem M = solve_smem(bsm, B.W);
+        const SolveSmem M = solve_smem<CH>(bsm, B.W);
         const int C = 32 * B.W;
-        for (int k = threadIdx.x; k < C; k += kChunk) M.cnt[k] = B.count[k];
+        for (int k = threadIdx.x; k < C; k += CH) M.cnt[k] = B.count[k];
         if (M.per_warp)
-            for (int k = threadIdx.x; k < (kChunk / 32) * C; k += kChunk) M.wh[k] = 0;
-        for (int k = threadIdx.x; k < B.W; k += kChunk) M.full[k] = B.fullmask[k];
+            for (int k = threadIdx.x; k < (CH / 32) * C; k += CH) M.wh[k] = 0;
+        for (int k = threadIdx.x; k < B.W; k += CH) M.full[k] = B.fullmask[k];
         for (int r = 0; r < chunks; ++r) {
             if (threadIdx.x == 0) go = wait_at_least(S.count, (3u + 2u * r) * G, S.timeout_ns, T, true);
-            solve_sync();
+            solve_sync<CH>();
             if (!go) return;
             clk.mark(S, 8);
-            if (!batch_solve(B, r * kChunk, r > 0, M)) return;
+            if (!batch_solve<CH>(B, r * CH, r > 0, M)) return;
             __threadfence();
-            solve_sync();
+            solve_sync<CH>();
             if (threadIdx.x == 0) asm volatile("st.release.gpu.u32 [%0], %1;" ::"l"(B.solved), "r"(unsigned(r + 1)) : "memory");
             clk.mark(S, 2);
         }
-        for (int k = threadIdx.x; k < C; k += kChunk) B.count[k] = M.cnt[k];
-        for (int k = threadIdx.x; k < B.W; k += kChunk) B.fullmask[k] = M.full[k];
+        for (int k = threadIdx.x; k < C; k += CH) B.count[k] = M.cnt[k];
+        for (int k = threadIdx.x; k < B.W; k += CH) B.fullmask[k] = M.full[k];
         return;
     }
     PhaseClock clk{0, 1};
     clk.start(S);
     const long long t = (blockIdx.x - 1) * (long long)blockDim.x + threadIdx.x, nt = (long long)G * blockDim.x;
-    for (int k = 0; k < 4 && k < chunks; ++k) batch_point_bits(B, k * kChunk, true, t, nt);
+    for (int k = 0; k < 4 && k < chunks; ++k) batch_point_bits<CH>(B, k * CH, true, t, nt);
     if (!grid_sync_of(S, T, G)) return;
-    for (int k = 0; k < 2 && k < chunks; ++k) batch_raster(B, k * kChunk, true, t, nt);
+    for (int k = 0; k < 2 && k < chunks; ++k) batch_raster<CH>(B, k * CH, true, t, nt);
     if (!grid_sync_of(S, T, G)) return;
-    batch_gather(B, 0, false, t, nt);
+    batch_gather<CH>(B, 0, false, t, nt);
     if (!grid_sync_of(S, T, G)) return;
     clk.mark(S, 1);
     for (int r = 0; r < chunks; ++r) {
@@ -803,15 +809,15 @@ __global__ void __launch_bounds__(kPersistThreads, 1) k_batch_persistent(BatchSt
             __syncthreads();
             if (!go) return;
             clk.mark(S, 9);
-            batch_publish(B, (r - 1) * kChunk, t, nt);
-            batch_clear(B, (r - 1) * kChunk, true, t, nt);
-            batch_point_bits(B, (r - 1) * kChunk, false, t, nt);
+            batch_publish<CH>(B, (r - 1) * CH, t, nt);
+            batch_clear<CH>(B, (r - 1) * CH, true, t, nt);
+            batch_point_bits<CH>(B, (r - 1) * CH, false, t, nt);
         }
-        if (r + 4 < chunks) batch_point_bits(B, (r + 4) * kChunk, true, t, nt);
+        if (r + 4 < chunks) batch_point_bits<CH>(B, (r + 4) * CH, true, t, nt);
         if (!grid_sync_of(S, T, G)) return;
         clk.mark(S, 0);
-        if (r + 1 < chunks) batch_gather(B, (r + 1) * kChunk, true, t, nt);
-        if (r + 2 < chunks) batch_raster(B, (r + 2) * kChunk, true, t, nt);
+        if (r + 1 < chunks) batch_gather<CH>(B, (r + 1) * CH, true, t, nt);
+        if (r + 2 < chunks) batch_raster<CH>(B, (r + 2) * CH, true, t, nt);
         if (!grid_sync_of(S, T, G)) return;
         clk.mark(S, 1);
     }
@@ -819,9 +825,9 @@ __global__ void __launch_bounds__(kPersistThreads, 1) k_batch_persistent(BatchSt
         if (threadIdx.x == 0) go = wait_at_least(B.solved, unsigned(chunks), S.timeout_ns, T, true);
         __syncthreads();
         if (!go) return;
-        batch_publish(B, (chunks - 1) * kChunk, t, nt);
-        batch_clear(B, (chunks - 1) * kChunk, true, t, nt);
-        batch_point_bits(B, (chunks - 1) * kChunk, false, t, nt);
+        batch_publish<CH>(B, (chunks - 1) * CH, t, nt);
+        batch_clear<CH>(B, (chunks - 1) * CH, true, t, nt);
+        batch_point_bits<CH>(B, (chunks - 1) * CH, false, t, nt);
     }
 }
 
@@ -1613,6 +1619,47 @@ int ensure_plan_capacity(grb_ctx* c, int n, int nb) {
     return GRB_OK;
 }
 
+// Runs the batching of B (chunks of CH nets) in the requested form.
+template <int CH>
+static int launch_batching(grb_ctx* c, BatchState& B, int mode, size_t smem) {
+    const int n = B.n;
+    int rc = GRB_OK;
+    int per_sm = 0;
+    if (mode == GRB_MODE_PERSISTENT)
+        GRB_CUDA(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_persistent<CH>, kPersistThreads, smem));
+    if (mode == GRB_MODE_PERSISTENT && per_sm * c->sms >= 2) {
+        GRB_CUDA(c, cudaMemsetAsync(c->sync, 0, 2 * sizeof(unsigned), c->stream));
+        GridSync S{c->sync, c->sync + 1, kBarrierTimeoutNs, c->profiling ? c->d_phase : nullptr, 0};
+        Tables T = c->T;
+        void* args[] = {&B, &S, &T};
+        GRB_CUDA(c, cudaLaunchCooperativeKernel((void*)k_batch_persistent<CH>, dim3(per_sm * c->sms), dim3(kPersistThreads),
+                                                args, smem, c->stream));
+        c->launches += 1;
+        return GRB_OK;
+    }
+    const int grid = c->sms * 4;
+    if (n) k_batch_point_bits<CH><<<grid, 256, 0, c->stream>>>(B, 0);
+    c->launches += n ? 1 : 0;
+    for (int s = 0; s < n; s += CH) {
+        cudaEvent_t e;
+        if ((rc = prof_begin(c, 0, &e))) return rc;
+        k_batch_raster<CH><<<grid, 256, 0, c->stream>>>(B, s);
+        prof_end(c, e);
+        if ((rc = prof_begin(c, 1, &e))) return rc;
+        k_batch_gather<CH><<<grid, 256, 0, c->stream>>>(B, s);
+        prof_end(c, e);
+        if ((rc = prof_begin(c, 2, &e))) return rc;
+        k_batch_solve<CH><<<1, CH, smem, c->stream>>>(B, s);
+        prof_end(c, e);
+        if ((rc = prof_begin(c, 3, &e))) return rc;
+        k_batch_publish<CH><<<grid, 256, 0, c->stream>>>(B, s);
+        prof_end(c, e);
+        c->launches += 4;
+    }
+    GRB_CUDA(c, cudaGetLastError());
+    return GRB_OK;
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------------------
@@ -1686,8 +1733,10 @@ int grb_create(const grb_grid* g, int32_t device, grb_ctx** out) {
     GRB_CUDA(cp, cudaMemcpy(yl, g->y_edge_len, sizeof(int) * (T.Y - 1), cudaMemcpyHostToDevice));
     GRB_CUDA(cp, cudaMemcpy(cap, g->capacity, sizeof(float) * cells, cudaMemcpyHostToDevice));
     GRB_CUDA(cp, cudaMemset(T.error, 0, 2 * sizeof(int)));
-    GRB_CUDA(cp, cudaFuncSetAttribute(k_batch_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
-    GRB_CUDA(cp, cudaFuncSetAttribute(k_batch_persistent, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    GRB_CUDA(cp, cudaFuncSetAttribute(k_batch_solve<kChunkMax>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kSolveSmemLimit)));
+    GRB_CUDA(cp, cudaFuncSetAttribute(k_batch_solve<kChunkMax / 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kSolveSmemLimit)));
+    GRB_CUDA(cp, cudaFuncSetAttribute(k_batch_persistent<kChunkMax>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kSolveSmemLimit)));
+    GRB_CUDA(cp, cudaFuncSetAttribute(k_batch_persistent<kChunkMax / 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kSolveSmemLimit)));
     GRB_CUDA(cp, cudaFuncSetAttribute(k_lshape_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
     GRB_CUDA(cp, cudaFuncSetAttribute(k_lshape_bucketed, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
     GRB_CUDA(cp, cudaFuncSetAttribute(k_prefix_pass1, cudaFuncAttributeMaxDynamicSharedMemorySize, int(8 * prefix_xpose_bytes())));
@@ -2278,8 +2327,8 @@ int grb_plan_batches(grb_ctx* c, const int32_t* order, int32_t n, int32_t limit,
         return fail(c, GRB_EINVAL, "unknown mode");
     GRB_CUDA(c, cudaSetDevice(c->device));
     const size_t xy = size_t(c->T.XY);
-    const size_t lm_bytes = xy * kChunkWords * 4;
-    const size_t pq_bytes = 2 * size_t(kChunk) * kChunkWords * 4;
+    const size_t lm_bytes = xy * kChunkMaxWords * 4;
+    const size_t pq_bytes = 2 * size_t(kChunkMax) * kChunkMaxWords * 4;
     int W = std::max(c->bW, 8);
     int rc = ensure_plan_capacity(c, n, n);
     if (rc) return rc;
@@ -2306,22 +2355,25 @@ int grb_plan_batches(grb_ctx* c, const int32_t* order, int32_t n, int32_t limit,
             if (c->bcount) cudaFree(c->bcount);
             c->bcount = nullptr;
             c->bW = 0;
-            if (cudaMalloc(&c->cellmask, xy * W * 4) || cudaMalloc(&c->fmask, 2 * size_t(kChunk) * W * 4) ||
+            if (cudaMalloc(&c->cellmask, xy * W * 4) || cudaMalloc(&c->fmask, 2 * size_t(kChunkMax) * W * 4) ||
                 cudaMalloc(&c->fullmask, W * 4) || cudaMalloc(&c->bcount, size_t(32) * W * 4)) {
                 cudaGetLastError();
                 return fail(c, GRB_ENOMEM, "colour masks");
             }
             c->bW = W;
         }
-        const size_t smem = solve_smem_bytes(W);
-        if (smem > 200 * 1024) return fail(c, GRB_ELIMIT, "too many batch colours");
+        // Chunks of kChunkMax nets while the solver's shared memory fits,
+        // else of half as many.
+        const int CH = solve_smem_bytes<kChunkMax>(W) <= kSolveSmemLimit ? kChunkMax : kChunkMax / 2;
+        const size_t smem = CH == kChunkMax ? solve_smem_bytes<kChunkMax>(W) : solve_smem_bytes<kChunkMax / 2>(W);
+        if (smem > kSolveSmemLimit) return fail(c, GRB_ELIMIT, "too many batch colours");
         if (c->lmask_dirty) {
             for (unsigned* lm : c->lmask) GRB_CUDA(c, cudaMemsetAsync(lm, 0, lm_bytes, c->stream));
             GRB_CUDA(c, cudaMemsetAsync(c->ptchunk, 0, xy * 4, c->stream));
             c->lmask_dirty = false;
         }
         GRB_CUDA(c, cudaMemsetAsync(c->cellmask, 0, xy * W * 4, c->stream));
-        GRB_CUDA(c, cudaMemsetAsync(c->fmask, 0, 2 * size_t(kChunk) * W * 4, c->stream));
+        GRB_CUDA(c, cudaMemsetAsync(c->fmask, 0, 2 * size_t(kChunkMax) * W * 4, c->stream));
         GRB_CUDA(c, cudaMemsetAsync(c->pred, 0, pq_bytes, c->stream));
         GRB_CUDA(c, cudaMemsetAsync(c->prevp, 0, pq_bytes, c->stream));
         GRB_CUDA(c, cudaMemsetAsync(c->fullmask, 0, W * 4, c->stream));
@@ -2336,38 +2388,9 @@ int grb_plan_batches(grb_ctx* c, const int32_t* order, int32_t n, int32_t limit,
         B.fullmask = c->fullmask; B.count = c->bcount; B.n_colors = c->ncolors;
         B.solved = c->bsolved;
         c->lmask_dirty = true;  // until the run completes
-        int per_sm = 0;
-        if (mode == GRB_MODE_PERSISTENT)
-            GRB_CUDA(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_persistent, kPersistThreads, smem));
-        if (mode == GRB_MODE_PERSISTENT && per_sm * c->sms >= 2) {
-            GRB_CUDA(c, cudaMemsetAsync(c->sync, 0, 2 * sizeof(unsigned), c->stream));
-            GridSync S{c->sync, c->sync + 1, kBarrierTimeoutNs, c->profiling ? c->d_phase : nullptr, 0};
-            Tables T = c->T;
-            void* args[] = {&B, &S, &T};
-            GRB_CUDA(c, cudaLaunchCooperativeKernel((void*)k_batch_persistent, dim3(per_sm * c->sms), dim3(kPersistThreads), args, smem, c->stream));
-            c->launches += 1;
-        } else {
-            const int grid = c->sms * 4;
-            if (n) k_batch_point_bits<<<grid, 256, 0, c->stream>>>(B, 0);
-            c->launches += n ? 1 : 0;
-            for (int s = 0; s < n; s += kChunk) {
-                cudaEvent_t e;
-                if ((rc = prof_begin(c, 0, &e))) return rc;
-                k_batch_raster<<<grid, 256, 0, c->stream>>>(B, s);
-                prof_end(c, e);
-                if ((rc = prof_begin(c, 1, &e))) return rc;
-                k_batch_gather<<<grid, 256, 0, c->stream>>>(B, s);
-                prof_end(c, e);
-                if ((rc = prof_begin(c, 2, &e))) return rc;
-                k_batch_solve<<<1, kChunk, smem, c->stream>>>(B, s);
-                prof_end(c, e);
-                if ((rc = prof_begin(c, 3, &e))) return rc;
-                k_batch_publish<<<grid, 256, 0, c->stream>>>(B, s);
-                prof_end(c, e);
-                c->launches += 4;
-            }
-            GRB_CUDA(c, cudaGetLastError());
-        }
+        if ((rc = CH == kChunkMax ? launch_batching<kChunkMax>(c, B, mode, smem)
+                                  : launch_batching<kChunkMax / 2>(c, B, mode, smem)))
+            return rc;
         int err[2] = {0, 0};
         GRB_CUDA(c, cudaMemcpyAsync(err, c->T.error, 2 * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
         GRB_CUDA(c, cudaStreamSynchronize(c->stream));
