@@ -194,10 +194,21 @@ __device__ __forceinline__ void batch_raster(const BatchState& B, int s, bool ne
     const unsigned want = (1u << (chunk & 31)) | (next ? 1u << ((chunk + 1) & 31) : 0u);
     unsigned* lm = chunk_mask(B, chunk);
     const long long a = B.mark_off[s], b = B.mark_off[s + m];
-    for (long long k = a + t; k < b; k += nt) {
-        const unsigned q = __ldg(B.mark_cell + k);
-        const int jj = __ldg(B.mark_jj + k) & (CH - 1);
-        if (__ldcg(B.ptchunk + q) & want) red_or(lm + size_t(q) * (CH / 32) + (jj >> 5), 1u << (jj & 31));
+    // Four marks per thread and pass, every load of a pass issued first.
+    for (long long k0 = a + t; k0 < b; k0 += 4 * nt) {
+        unsigned q[4], bits[4];
+        int jj[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const long long k = k0 + u * nt;
+            q[u] = k < b ? __ldg(B.mark_cell + k) : 0u;
+            jj[u] = k < b ? (__ldg(B.mark_jj + k) & (CH - 1)) : -1;
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) bits[u] = jj[u] >= 0 ? __ldcg(B.ptchunk + q[u]) : 0u;
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+            if (bits[u] & want) red_or(lm + size_t(q[u]) * (CH / 32) + (jj[u] >> 5), 1u << (jj[u] & 31));
     }
 }
 
@@ -443,6 +454,8 @@ __device__ __forceinline__ bool batch_solve(const BatchState& B, int s, bool loo
     solve_sync<CH>();
     int fixed = 0;  // nets below `fixed` are final
     int rank = 0;
+    bool counted = false;  // this chunk's nets are in S.cnt already
+    __shared__ int tight;
     while (true) {
         // Jacobi sweeps until the colouring is a fixed point.
         while (true) {
@@ -476,20 +489,33 @@ __device__ __forceinline__ bool batch_solve(const BatchState& B, int s, bool loo
             solve_sync<CH>();
             if (leader) S.wh[warp * C + c] = 0;
         } else {
-            for (int k = tid; k < C; k += CH) S.wh[k] = S.cnt[k];
+            // Per-colour totals first: while no batch reaches the limit, no
+            // position inside a batch is needed here (the rank pass after the
+            // run assigns them); else warps add their counts in turn.
+            if (tid == 0) tight = 0;
             solve_sync<CH>();
-            for (int w = 0; w < (m + 31) / 32; ++w) {
-                if (warp == w && tid < m) {
-                    rank = S.wh[c] + within;
-                    if (leader) S.wh[c] += __popc(peers);
-                    if (rank >= B.limit) atomicMin(&first_bad, tid);
-                }
+            if (leader && atomicAdd(S.cnt + c, __popc(peers)) + __popc(peers) > B.limit) tight = 1;
+            solve_sync<CH>();
+            if (!tight) {
+                counted = true;
+            } else {
+                if (leader) atomicSub(S.cnt + c, __popc(peers));
                 solve_sync<CH>();
+                for (int k = tid; k < C; k += CH) S.wh[k] = S.cnt[k];
+                solve_sync<CH>();
+                for (int w = 0; w < (m + 31) / 32; ++w) {
+                    if (warp == w && tid < m) {
+                        rank = S.wh[c] + within;
+                        if (leader) S.wh[c] += __popc(peers);
+                        if (rank >= B.limit) atomicMin(&first_bad, tid);
+                    }
+                    solve_sync<CH>();
+                }
             }
         }
         const int bad = first_bad;
         if (bad >= m) {
-            if (leader) atomicAdd(S.cnt + c, __popc(peers));
+            if (leader && !counted) atomicAdd(S.cnt + c, __popc(peers));
             break;
         }
         // Net `bad` finds its colour full; so does every later net.
@@ -510,7 +536,6 @@ __device__ __forceinline__ bool batch_solve(const BatchState& B, int s, bool loo
     if (tid < m) {
         const int c = S.col[tid];
         B.batch_of[s + tid] = c;
-        B.rank[s + tid] = rank;
         S.colp[tid] = c;
         top = c + 1;
     }

@@ -831,6 +831,51 @@ __global__ void __launch_bounds__(kPersistThreads, 1) k_batch_persistent(BatchSt
     }
 }
 
+// Position of every net inside its batch: the number of earlier order
+// positions with the same colour.  A stable counting pass over tiles of
+// kRankTile positions: per-tile colour counts, their exclusive scan per
+// colour over the tiles, then the ranks inside each tile (warps in turn).
+constexpr int kRankTile = 1024;
+__global__ void __launch_bounds__(kRankTile) k_rank_counts(const int* batch_of, int n, int C, int* tile_cnt) {
+    extern __shared__ int hist[];  // [C]
+    for (int k = threadIdx.x; k < C; k += blockDim.x) hist[k] = 0;
+    __syncthreads();
+    const long long p = blockIdx.x * (long long)kRankTile + threadIdx.x;
+    if (p < n) atomicAdd(hist + batch_of[p], 1);
+    __syncthreads();
+    for (int k = threadIdx.x; k < C; k += blockDim.x) tile_cnt[size_t(blockIdx.x) * C + k] = hist[k];
+}
+__global__ void k_rank_scan(int* tile_cnt, int tiles, int C) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= C) return;
+    int acc = 0;
+    for (int t = 0; t < tiles; ++t) {
+        const int v = tile_cnt[size_t(t) * C + c];
+        tile_cnt[size_t(t) * C + c] = acc;
+        acc += v;
+    }
+}
+__global__ void __launch_bounds__(kRankTile) k_rank_assign(const int* batch_of, int n, int C, const int* tile_base,
+                                                           int* rank) {
+    extern __shared__ int run[];  // [C] counts of the tile's earlier warps
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int k = threadIdx.x; k < C; k += blockDim.x) run[k] = 0;
+    __syncthreads();
+    const long long p = blockIdx.x * (long long)kRankTile + threadIdx.x;
+    const int c = p < n ? batch_of[p] : -1 - lane;  // distinct dummies for idle lanes
+    const unsigned peers = __match_any_sync(0xffffffffu, c);
+    const int within = __popc(peers & ((1u << lane) - 1u));
+    const bool leader = p < n && lane == __ffs(peers) - 1;
+    for (int w = 0; w < kRankTile / 32; ++w) {
+        if (warp == w) {
+            if (p < n) rank[p] = tile_base[size_t(blockIdx.x) * C + c] + run[c] + within;
+            __syncwarp();
+            if (leader) run[c] += __popc(peers);
+        }
+        __syncthreads();
+    }
+}
+
 // Batch offsets in execution order (reversed colours) and the flattened ids.
 __global__ void k_plan_offsets(BatchState B, int* batch_off) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
@@ -981,6 +1026,8 @@ struct grb_ctx {
     unsigned *pred = nullptr, *prevp = nullptr, *bsolved = nullptr;
     bool lmask_dirty = false;          // a run stopped before clearing them
     int *bcount = nullptr, *ncolors = nullptr, *batch_of = nullptr, *brank = nullptr, *order = nullptr;
+    int* rank_tiles = nullptr;         // [tiles][colours] scratch of the rank pass
+    size_t rank_cap = 0;
     int bW = 0, bn_cap = 0;
     // flat mark / query-point lists by order position
     long long *mark_off = nullptr, *pt_off = nullptr, *scan_sums = nullptr;
@@ -1766,7 +1813,7 @@ void grb_destroy(grb_ctx* c) {
     for (void* p : {(void*)c->check, (void*)c->bucket_ids, (void*)c->bucket_off, (void*)c->ids, (void*)c->batch_off, (void*)c->gscratch, (void*)c->work, (void*)c->cellmask,
                     (void*)c->lmask[0], (void*)c->lmask[1], (void*)c->lmask[2], (void*)c->ptchunk, (void*)c->fmask, (void*)c->pred, (void*)c->prevp,
                     (void*)c->bsolved, (void*)c->fullmask, (void*)c->bcount, (void*)c->ncolors, (void*)c->batch_of, (void*)c->brank,
-                    (void*)c->order, (void*)c->mark_off, (void*)c->pt_off, (void*)c->scan_sums, (void*)c->mark_cell,
+                    (void*)c->order, (void*)c->rank_tiles, (void*)c->mark_off, (void*)c->pt_off, (void*)c->scan_sums, (void*)c->mark_cell,
                     (void*)c->pt_cell, (void*)c->mark_jj, (void*)c->pt_jj})
         if (p) cudaFree(p);
     if (c->ev0) cudaEventDestroy(c->ev0);
@@ -2403,6 +2450,25 @@ int grb_plan_batches(grb_ctx* c, const int32_t* order, int32_t n, int32_t limit,
         }
         if (err[0]) return check_device_error(c);
         c->lmask_dirty = false;
+        if (n) {
+            const int C = 32 * W, tiles = (n + kRankTile - 1) / kRankTile;
+            const size_t need = size_t(tiles) * C;
+            if (need > c->rank_cap) {
+                if (c->rank_tiles) cudaFree(c->rank_tiles);
+                c->rank_tiles = nullptr;
+                c->rank_cap = 0;
+                if (cudaMalloc(&c->rank_tiles, 4 * need) != cudaSuccess) {
+                    cudaGetLastError();
+                    return fail(c, GRB_ENOMEM, "batch rank scratch");
+                }
+                c->rank_cap = need;
+            }
+            k_rank_counts<<<tiles, kRankTile, 4 * C, c->stream>>>(c->batch_of, n, C, c->rank_tiles);
+            k_rank_scan<<<(C + 127) / 128, 128, 0, c->stream>>>(c->rank_tiles, tiles, C);
+            k_rank_assign<<<tiles, kRankTile, 4 * C, c->stream>>>(c->batch_of, n, C, c->rank_tiles, c->brank);
+            c->launches += 3;
+            GRB_CUDA(c, cudaGetLastError());
+        }
         int nb = 0;
         GRB_CUDA(c, cudaMemcpy(&nb, c->ncolors, 4, cudaMemcpyDeviceToHost));
         k_plan_offsets<<<1, 1, 0, c->stream>>>(B, c->batch_off);
