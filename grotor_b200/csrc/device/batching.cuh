@@ -11,12 +11,16 @@
 // same lists):
 //   * once per run, every net's marked cells and query points are written to
 //     flat lists in order-position order (k_flat_*), tagged with the net's
-//     position inside its chunk of kChunk nets, so each per-chunk step below is
-//     one balanced, coalesced pass over a contiguous range;
-//   * cellmask[cell] holds one bit per batch ("colour") already marking the cell;
-//   * nets are processed in chunks of kChunk in order; per chunk:
-//       1. raster: every mark ORs its net's bit into the chunk-local mask of
-//          the cell (triple-buffered by chunk index);
+//     position inside a chunk, so each per-chunk step below is one balanced,
+//     coalesced pass over a contiguous range;
+//   * cellmask holds one bit per batch ("colour") already marking each cell,
+//     plane-major (colour word w of all cells contiguous);
+//   * nets are processed in chunks of CH (1024, or 512 when the solver's
+//     shared memory for the colour words would not fit) in order; per chunk:
+//       1. raster: every mark on a query point of this chunk or of the next
+//          one (per-cell chunk bits, L2-resident, filter the rest) ORs its
+//          net's bit into the chunk-local mask of the cell (triple-buffered by
+//          chunk index);
 //       2. gather: every query point ORs, into its net's column of the chunk
 //          tables, the cell's colours (forbidden batches of earlier chunks),
 //          the chunk-local bits of earlier nets of the chunk (predecessors),
@@ -24,11 +28,12 @@
 //       3. solve: one CTA solves first-fit inside the chunk by Jacobi
 //          iteration over the predecessor DAG (converges to the unique
 //          sequential solution), then applies batch capacities in order;
-//       4. publish: every mark ORs its net's colour into cellmask and clears
-//          the chunk-local mask.
-//   Plain form: one launch per step per chunk.  Persistent form: one
+//       4. publish: every mark ORs its net's colour into cellmask; the
+//          chunk-local mask is emptied at the chunk's query points.
+//   Positions inside the batches come from a stable counting pass after the
+//   run.  Plain form: one launch per step per chunk.  Persistent form: one
 //   cooperative kernel in which CTA 0 solves chunk r while the other CTAs
-//   publish chunk r-1, raster chunk r+1 and gather chunk r+1; the gather
+//   publish chunk r-1, gather chunk r+1 and raster chunk r+2; the gather
 //   reads cellmask as of chunk r-1 and takes chunk r's colours through the
 //   previous-chunk bits, which the solver resolves from the colours it keeps
 //   in shared memory.  The solver and the other CTAs hand chunks over through
