@@ -32,6 +32,8 @@ struct Arena {
     float* vN;             // [nmax][L] via cost at the node
     unsigned short* from;  // [nmax][TT] choice*L*L + curl*L + parl
     int* range;            // [nmax] chosen range lo*L+hi
+    int* xy;               // [nmax] node coordinate x << 16 | y (grids are at most 8192 wide)
+    int* lay;              // [nmax] node layer (L: Steiner point)
     double* cur;           // [L]
     double* diag;          // [L]
     double* mcp;           // [TT]
@@ -47,7 +49,7 @@ __host__ __device__ __forceinline__ size_t arena_bytes(int L, int nmax) {
     b += 2 * L * 8 + TT * 8;
     b += nmax * TT * 2;
     b = (b + 7) & ~size_t(7);
-    b += nmax * 4 + 2 * L * 4;
+    b += nmax * 4 + 2 * L * 4 + 2 * size_t(nmax) * 4;
     return (b + 15) & ~size_t(15);
 }
 
@@ -69,7 +71,9 @@ __device__ __forceinline__ Arena carve_arena(char* base, int L, int nmax) {
     p = reinterpret_cast<char*>((reinterpret_cast<uintptr_t>(p) + 7) & ~uintptr_t(7));
     A.range = reinterpret_cast<int*>(p); p += nmax * 4;
     A.cur_from = reinterpret_cast<int*>(p); p += L * 4;
-    A.pdiag = reinterpret_cast<int*>(p);
+    A.pdiag = reinterpret_cast<int*>(p); p += L * 4;
+    A.xy = reinterpret_cast<int*>(p); p += nmax * 4;
+    A.lay = reinterpret_cast<int*>(p);
     return A;
 }
 
@@ -87,6 +91,14 @@ __device__ void lshape_net(const Tables& T, const Plan& P, int id, int stamp, co
     const int* nd = P.nodes + off;
     const int* par = P.parents + off;
 
+    // 0. Node coordinates, once per net (the divisions by the runtime grid
+    // sizes are not repeated per layer and step).
+    for (int q = lane; q < N; q += 32) {
+        const int node = nd[q], l = node / XY, r = node - l * XY, x = r / Y;
+        A.xy[q] = (x << 16) | (r - x * Y);
+        A.lay[q] = l;
+    }
+    __syncwarp();
     // 1. Gather every cost the DP reads.  Each lane takes two (node, layer)
     // items per pass and issues all their loads before any arena store.
     for (int q0 = lane; q0 < N * L; q0 += 64) {
@@ -101,11 +113,11 @@ __device__ void lshape_net(const Tables& T, const Plan& P, int id, int stamp, co
             w1[u] = w2[u] = 0.0;
             if (q >= N * L) continue;
             const int i = q / L, l = q - i * L;
-            const int node = nd[i], r = node % XY, x = r / Y, y = r - x * Y;
+            const int x = A.xy[i] >> 16, y = A.xy[i] & 0xffff, r = x * Y + y;
             vn[u] = T.vcost[l * XY + r];
             kind[u] = 1;
             if (i > 0) {
-                const int pr = nd[par[i]] % XY, px = pr / Y, py = pr - px * Y;
+                const int pxy = A.xy[par[i]], px = pxy >> 16, py = pxy & 0xffff;
                 const int minx = min(x, px), maxx = max(x, px), miny = min(y, py), maxy = max(y, py);
                 const bool ay = along_y(T, l);
                 if (x == px || y == py) {
@@ -137,7 +149,7 @@ __device__ void lshape_net(const Tables& T, const Plan& P, int id, int stamp, co
     // 2. Via stacks at every node (lshape_thread.cuh:40-50).
     for (int q = lane; q < N * L; q += 32) {
         const int i = q / L, lo = q - i * L;
-        const int fixed = nd[i] / XY;
+        const int fixed = A.lay[i];
         double acc = 0;
         for (int hi = lo; hi < L; ++hi) {
             if (hi > lo) acc = acc + static_cast<double>(A.vN[i * L + hi - 1]);
@@ -164,8 +176,8 @@ __device__ void lshape_net(const Tables& T, const Plan& P, int id, int stamp, co
         __syncwarp();
         if (lane < L) {
             const int pl = lane;
-            const int node = nd[i] % XY, x = node / Y, y = node - x * Y;
-            const int pn = nd[p] % XY, px = pn / Y, py = pn - px * Y;
+            const int x = A.xy[i] >> 16, y = A.xy[i] & 0xffff;
+            const int px = A.xy[p] >> 16, py = A.xy[p] & 0xffff;
             double best = kInf;
             int pb = 0;
             if (x == px || y == py) {
@@ -230,13 +242,11 @@ __device__ void lshape_net(const Tables& T, const Plan& P, int id, int stamp, co
         const int i = b0 + lane;
         int words = 0, x = 0, y = 0, px = 0, py = 0, cl = 0, pl = 0, minl = 0, maxl = 0;
         if (i < N) {
-            const int node = nd[i] % XY;
-            x = node / Y; y = node - x * Y;
+            x = A.xy[i] >> 16; y = A.xy[i] & 0xffff;
             minl = A.range[i] / L; maxl = A.range[i] % L;
             words = minl < maxl ? 2 : 0;
             if (i) {
-                const int pn = nd[par[i]] % XY;
-                px = pn / Y; py = pn - px * Y;
+                px = A.xy[par[i]] >> 16; py = A.xy[par[i]] & 0xffff;
                 const int pr = A.range[par[i]];
                 const int f = A.from[i * TT + tri(L, pr / L, pr % L)];
                 cl = f / L % L; pl = f % L;
