@@ -180,6 +180,36 @@ __global__ void k_commit_vias(Tables T, Plan P, int b, int stamp, int K) {
     for (int k = warp; k < cnt; k += warps) commit_net_vias(T, P, P.ids[lo + k], stamp, K, lane);
 }
 
+// refresh_cost (incremental_update.cuh:98-132) inside a persistent stage
+// kernel: dirty cells | prefix pass 1 | trees | pass 2, each phase ended by a
+// grid barrier.  `smem`: the block's dynamic shared memory (per-warp pass
+// scratch, or the tree of the group a block builds).  False when a barrier
+// gave up.
+__device__ __forceinline__ bool refresh_persistent(const Tables& T, GridSync& S, PhaseClock& clk, int gwarp,
+                                                   int nwarps, int lane, char* smem) {
+    void* xs = smem + (threadIdx.x >> 5) * prefix_xpose_bytes();
+    if (blockIdx.x == 0) collect_dirty_groups(T);
+    refresh_dirty_cells<2>(T, gwarp, nwarps, lane);
+    if (!grid_sync(S, T)) return false;
+    clk.mark(S, 4);
+    const int items = *reinterpret_cast<volatile int*>(T.group_count) * T.tree_chunks;
+    for (int item = gwarp; item < items; item += nwarps) {
+        int g, c;
+        if (prefix_item(T, item, g, c)) prefix_pass1(T, g, c, lane, xs);
+    }
+    if (!grid_sync(S, T)) return false;
+    for (int k = blockIdx.x; k < *reinterpret_cast<volatile int*>(T.group_count); k += gridDim.x)
+        prefix_tree(T, T.group_list[k], reinterpret_cast<double*>(smem));
+    if (!grid_sync(S, T)) return false;
+    for (int item = gwarp; item < items; item += nwarps) {
+        int g, c;
+        if (prefix_item(T, item, g, c)) prefix_pass2(T, g, c, lane, xs);
+    }
+    if (!grid_sync(S, T)) return false;
+    clk.mark(S, 7);
+    return true;
+}
+
 // Persistent stage: every batch of the plan in one cooperative launch.
 // Per batch: recompute dirty cells (block 0 also lists the dirty prefix
 // groups) -> prefix pass 1 -> prefix trees -> prefix pass 2 -> route and commit
@@ -189,31 +219,11 @@ __global__ void __launch_bounds__(kPersistentThreads, 2) k_lshape_persistent(Tab
     extern __shared__ __align__(16) char smem[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int gwarp = warp * gridDim.x + blockIdx.x, nwarps = gridDim.x * (blockDim.x >> 5);
-    double* tree = reinterpret_cast<double*>(smem);
     PhaseClock clk;
     clk.start(S);
     for (int b = 0; b < P.n_batches; ++b) {
         const int stamp = stamp0 + b + 1;
-        // refresh_cost (incremental_update.cuh:98-132).
-        if (blockIdx.x == 0) collect_dirty_groups(T);
-        refresh_dirty_cells<2>(T, gwarp, nwarps, lane);
-        if (!grid_sync(S, T)) return;
-        clk.mark(S, 4);
-        const int items = *reinterpret_cast<volatile int*>(T.group_count) * T.tree_chunks;
-        for (int item = gwarp; item < items; item += nwarps) {
-            int g, c;
-            if (prefix_item(T, item, g, c)) prefix_pass1(T, g, c, lane, smem + warp * prefix_xpose_bytes());
-        }
-        if (!grid_sync(S, T)) return;
-        for (int k = blockIdx.x; k < *reinterpret_cast<volatile int*>(T.group_count); k += gridDim.x)
-            prefix_tree(T, T.group_list[k], tree);
-        if (!grid_sync(S, T)) return;
-        for (int item = gwarp; item < items; item += nwarps) {
-            int g, c;
-            if (prefix_item(T, item, g, c)) prefix_pass2(T, g, c, lane, smem + warp * prefix_xpose_bytes());
-        }
-        if (!grid_sync(S, T)) return;
-        clk.mark(S, 7);
+        if (!refresh_persistent(T, S, clk, gwarp, nwarps, lane, smem)) return;
         // Route every net of the batch and commit its wires: size buckets from
         // the largest down (long nets start first), nets taken from the
         // bucket's work queue `per_grab` at a time.  (In this kernel the
@@ -266,7 +276,6 @@ __global__ void __launch_bounds__(kPersistentThreads, 2) k_flt_persistent(Tables
     extern __shared__ __align__(16) char smem[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int gwarp = warp * gridDim.x + blockIdx.x, nwarps = gridDim.x * (blockDim.x >> 5);
-    double* tree = reinterpret_cast<double*>(smem);
     PhaseClock clk;
     clk.start(S);
     for (int b = 0; b < P2.n_batches; ++b) {
@@ -279,25 +288,7 @@ __global__ void __launch_bounds__(kPersistentThreads, 2) k_flt_persistent(Tables
             if (!grid_sync(S, T)) return;
             clk.mark(S, 6);
         }
-        if (blockIdx.x == 0) collect_dirty_groups(T);
-        refresh_dirty_cells<2>(T, gwarp, nwarps, lane);
-        if (!grid_sync(S, T)) return;
-        clk.mark(S, 4);
-        const int items = *reinterpret_cast<volatile int*>(T.group_count) * T.tree_chunks;
-        for (int item = gwarp; item < items; item += nwarps) {
-            int g, c;
-            if (prefix_item(T, item, g, c)) prefix_pass1(T, g, c, lane, smem + warp * prefix_xpose_bytes());
-        }
-        if (!grid_sync(S, T)) return;
-        for (int k = blockIdx.x; k < *reinterpret_cast<volatile int*>(T.group_count); k += gridDim.x)
-            prefix_tree(T, T.group_list[k], tree);
-        if (!grid_sync(S, T)) return;
-        for (int item = gwarp; item < items; item += nwarps) {
-            int g, c;
-            if (prefix_item(T, item, g, c)) prefix_pass2(T, g, c, lane, smem + warp * prefix_xpose_bytes());
-        }
-        if (!grid_sync(S, T)) return;
-        clk.mark(S, 7);
+        if (!refresh_persistent(T, S, clk, gwarp, nwarps, lane, smem)) return;
         while (true) {
             int k = 0;
             if (lane == 0) k = atomicAdd(work + b, 1);
@@ -346,7 +337,6 @@ __global__ void __launch_bounds__(kPersistentThreads, 2) k_zshape_persistent(Tab
     extern __shared__ __align__(16) char smem[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int gwarp = warp * gridDim.x + blockIdx.x, nwarps = gridDim.x * (blockDim.x >> 5);
-    double* tree = reinterpret_cast<double*>(smem);
     __shared__ int cand[kZCand];
     __shared__ int znet;
     PhaseClock clk;
@@ -354,25 +344,7 @@ __global__ void __launch_bounds__(kPersistentThreads, 2) k_zshape_persistent(Tab
     for (int b = 0; b < P.n_batches; ++b) {
         const int lo = P.batch_off[b], cnt = P.batch_off[b + 1] - lo;
         const int stamp = stamp0 + b + 1;
-        if (blockIdx.x == 0) collect_dirty_groups(T);
-        refresh_dirty_cells<2>(T, gwarp, nwarps, lane);
-        if (!grid_sync(S, T)) return;
-        clk.mark(S, 4);
-        const int items = *reinterpret_cast<volatile int*>(T.group_count) * T.tree_chunks;
-        for (int item = gwarp; item < items; item += nwarps) {
-            int g, c;
-            if (prefix_item(T, item, g, c)) prefix_pass1(T, g, c, lane, smem + warp * prefix_xpose_bytes());
-        }
-        if (!grid_sync(S, T)) return;
-        for (int k = blockIdx.x; k < *reinterpret_cast<volatile int*>(T.group_count); k += gridDim.x)
-            prefix_tree(T, T.group_list[k], tree);
-        if (!grid_sync(S, T)) return;
-        for (int item = gwarp; item < items; item += nwarps) {
-            int g, c;
-            if (prefix_item(T, item, g, c)) prefix_pass2(T, g, c, lane, smem + warp * prefix_xpose_bytes());
-        }
-        if (!grid_sync(S, T)) return;
-        clk.mark(S, 7);
+        if (!refresh_persistent(T, S, clk, gwarp, nwarps, lane, smem)) return;
         while (true) {  // one CTA per net
             if (threadIdx.x == 0) znet = atomicAdd(work + b, 1);
             __syncthreads();
