@@ -196,7 +196,9 @@ __device__ __forceinline__ void zedge(const Tables& T, const ZTrees& Z, int j, i
         // positions of the node's row/column (the reference scans them in
         // order keeping strict improvements), found by a block reduction of
         // (value, position) pairs.
-        __shared__ int red_v[32], red_b[32];
+        // Each warp's first minimum per layer goes to shared memory; after one
+        // barrier, thread i combines layer i over the warps.
+        __shared__ int red_v[32][kMaxLayers], red_b[32][kMaxLayers];
         for (int i = 1; i < LAYER; ++i) {
             const bool ay = ((i & 1) ^ D) != 0;
             const int cur = static_cast<int>(ay ? i * NN + tox * Z.N + toy : i * NN + toy * Z.N + tox);
@@ -212,19 +214,22 @@ __device__ __forceinline__ void zedge(const Tables& T, const ZTrees& Z, int j, i
                 const int ov = __shfl_down_sync(0xffffffffu, bv, o), ob = __shfl_down_sync(0xffffffffu, bb, o);
                 if (ob >= 0 && (bb < 0 || ov < bv || (ov == bv && ob < bb))) { bv = ov; bb = ob; }
             }
-            if ((lane & 31) == 0) { red_v[lane >> 5] = bv; red_b[lane >> 5] = bb; }
-            __syncthreads();
-            if (lane == 0) {
-                for (int w = 1; w < (nth + 31) / 32; ++w) {
-                    const int ov = red_v[w], ob = red_b[w];
-                    if (ob >= 0 && (bb < 0 || ov < bv || (ov == bv && ob < bb))) { bv = ov; bb = ob; }
-                }
-                if (bb >= 0 && bv < mj[cur]) {
-                    const int last = static_cast<int>(ay ? i * NN + tox * Z.N + bb : i * NN + toy * Z.N + bb);
-                    mj[cur] = bv; pj[cur] = p4[last]; p2j[cur] = p5[last];
-                }
+            if ((lane & 31) == 0) { red_v[lane >> 5][i] = bv; red_b[lane >> 5][i] = bb; }
+        }
+        __syncthreads();
+        if (lane >= 1 && lane < LAYER) {
+            const int i = lane;
+            const bool ay = ((i & 1) ^ D) != 0;
+            const int cur = static_cast<int>(ay ? i * NN + tox * Z.N + toy : i * NN + toy * Z.N + tox);
+            int bv = red_v[0][i], bb = red_b[0][i];
+            for (int w = 1; w < (nth + 31) / 32; ++w) {
+                const int ov = red_v[w][i], ob = red_b[w][i];
+                if (ob >= 0 && (bb < 0 || ov < bv || (ov == bv && ob < bb))) { bv = ov; bb = ob; }
             }
-            __syncthreads();
+            if (bb >= 0 && bv < mj[cur]) {
+                const int last = static_cast<int>(ay ? i * NN + tox * Z.N + bb : i * NN + toy * Z.N + bb);
+                mj[cur] = bv; pj[cur] = p4[last]; p2j[cur] = p5[last];
+            }
         }
     } else if (fromx == tox) {
         for (int i = 1 + lane; i < LAYER; i += nth) {
