@@ -87,20 +87,57 @@ __device__ __forceinline__ void via_stack_demand(const Tables& T, int ra, int x,
     }
 }
 
-// One warp commits the via segments of net `id` (lanes over segments).
-__device__ __forceinline__ void commit_net_vias(const Tables& T, const Plan& P, int id, int stamp, int K,
-                                                int lane) {
-    const int* r = net_routes(P, id);
-    const int words = r[0];
+// Route segment (a, b): if it is a via, commit its stack and return the
+// number of layers it crosses, else 0.
+__device__ __forceinline__ int via_segment(const Tables& T, int a, int b, int stamp, int K) {
+    const int la = a / T.XY, lb = b / T.XY;
+    const int low = min(la, lb), high = max(la, lb);
+    if (low == high) return 0;
+    const int ra = a - la * T.XY, x = ra / T.Y, y = ra - x * T.Y;
+    via_stack_demand(T, ra, x, y, low, high, stamp, K);
+    return high - low;
+}
+
+// One warp commits the via segments of the nets ids[first], ids[first +
+// step], ... below ids[cnt] (routes of plan P), lanes over each net's
+// segments.  The warp loads the ids and route offsets of 32 of
+// its nets at once, and each net's first 32 segments (those inside its route
+// capacity) while the previous net's via stacks are committed, so a net costs
+// about one memory round trip instead of four.
+__device__ __forceinline__ void commit_vias_strided(const Tables& T, const Plan& P, const int* ids, int cnt,
+                                                    int first, int step, int stamp, int K, int lane) {
     long long vias = 0;
-    for (int i = 1 + 2 * lane; i < words; i += 64) {
-        const int a = r[i], b = r[i + 1];
-        const int la = a / T.XY, lb = b / T.XY;
-        const int low = min(la, lb), high = max(la, lb);
-        if (low == high) continue;
-        const int ra = a - la * T.XY, x = ra / T.Y, y = ra - x * T.Y;
-        vias += high - low;
-        via_stack_demand(T, ra, x, y, low, high, stamp, K);
+    for (int g0 = first; g0 < cnt; g0 += 32 * step) {
+        const int mine = g0 + lane * step;
+        long long off = 0, cap = 0;
+        if (mine < cnt) {
+            const int id = ids[mine];
+            off = P.route_off[id];
+            cap = P.route_off[id + 1] - off;
+        }
+        const int nn = min(32, (cnt - 1 - g0) / step + 1);
+        const int i0 = 1 + 2 * lane;
+        // Net j's word count and lane's first segment (if inside capacity).
+        int words = 0, a = 0, b = 0;
+        {
+            const int* r = P.routes + __shfl_sync(0xffffffffu, off, 0);
+            const long long c = __shfl_sync(0xffffffffu, cap, 0);
+            words = r[0];
+            if (i0 + 1 < c) { a = r[i0]; b = r[i0 + 1]; }
+        }
+        for (int j = 0; j < nn; ++j) {
+            const int* r = P.routes + __shfl_sync(0xffffffffu, off, j);
+            const long long c = __shfl_sync(0xffffffffu, cap, j);
+            const int cw = words, ca = a, cb = b;
+            if (j + 1 < nn) {
+                const int* rn = P.routes + __shfl_sync(0xffffffffu, off, j + 1);
+                const long long nc = __shfl_sync(0xffffffffu, cap, j + 1);
+                words = rn[0];
+                if (i0 + 1 < nc) { a = rn[i0]; b = rn[i0 + 1]; }
+            }
+            if (i0 < cw) vias += i0 + 1 < c ? via_segment(T, ca, cb, stamp, K) : via_segment(T, r[i0], r[i0 + 1], stamp, K);
+            for (int i = i0 + 64; i < cw; i += 64) vias += via_segment(T, r[i], r[i + 1], stamp, K);
+        }
     }
     for (int s = 16; s; s >>= 1) vias += __shfl_down_sync(0xffffffffu, vias, s);
     if (lane == 0 && vias) atomicAdd(T.vias, static_cast<unsigned long long>(vias * K));

@@ -88,6 +88,23 @@ __device__ __forceinline__ float via_cost_of(const Tables& T, const CellInputs& 
     return static_cast<float>(static_cast<double>(v) + T.unit_via);
 }
 
+// Position of the n-th (0-based) set bit of m, which has more than n set
+// bits: a binary search over halves, quarters, ... by population count, the
+// same few instructions for every lane whatever n is.
+__device__ __forceinline__ int nth_set_bit(unsigned m, int n) {
+    int pos = 0;
+#pragma unroll
+    for (int w = 16; w; w >>= 1) {
+        const unsigned low = m & ((1u << w) - 1u);
+        const int c = __popc(low);
+        const bool up = n >= c;
+        n = up ? n - c : n;
+        pos = up ? pos + w : pos;
+        m = up ? m >> w : low;
+    }
+    return pos;
+}
+
 // Recompute every dirty cell.  A warp loads 32 bitmap words at a time, ranks
 // their dirty cells with a warp prefix sum and takes them kRounds * 32
 // at a time, kRounds cells per lane whose inputs are all loaded before any
@@ -135,9 +152,7 @@ __device__ __forceinline__ void refresh_dirty_cells(const Tables& T, int warp, i
                 wire[q] = false;
                 if (k < total) {
                     const int nth = k - (owner_incl - owner_n);  // 0-based rank inside the owner's word
-                    unsigned m = ov;
-                    for (int j = 0; j < nth; ++j) m &= m - 1;  // drop the nth lowest set bits
-                    const int bit = __ffs(m) - 1;
+                    const int bit = nth_set_bit(ov, nth);
                     const int c = (base + lo) * 32 + bit;
                     if (c < T.cells) {
                         cell[q] = c;

@@ -177,7 +177,7 @@ __global__ void k_commit_vias(Tables T, Plan P, int b, int stamp, int K) {
     const int lane = threadIdx.x & 31;
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, warps = (gridDim.x * blockDim.x) >> 5;
     const int lo = P.batch_off[b], cnt = P.batch_off[b + 1] - lo;
-    for (int k = warp; k < cnt; k += warps) commit_net_vias(T, P, P.ids[lo + k], stamp, K, lane);
+    commit_vias_strided(T, P, P.ids + lo, cnt, warp, warps, stamp, K, lane);
 }
 
 // refresh_cost (incremental_update.cuh:98-132) inside a persistent stage
@@ -251,7 +251,7 @@ __global__ void __launch_bounds__(kPersistentThreads, 2) k_lshape_persistent(Tab
         if (!grid_sync(S, T)) return;
         clk.mark(S, 5);
         // Via demand sees every wire timestamp of the batch.
-        for (int k = gwarp; k < cnt; k += nwarps) commit_net_vias(T, P, P.ids[lo + k], stamp, 1, lane);
+        commit_vias_strided(T, P, P.ids + lo, cnt, gwarp, nwarps, stamp, 1, lane);
         if (!grid_sync(S, T)) return;
         clk.mark(S, 6);
     }
@@ -284,7 +284,7 @@ __global__ void __launch_bounds__(kPersistentThreads, 2) k_flt_persistent(Tables
         if (remove) {
             for (int k = gwarp; k < cnt; k += nwarps) commit_net_wires(T, P1, P2.ids[lo + k], stamp - 1, -1, lane);
             if (!grid_sync(S, T)) return;
-            for (int k = gwarp; k < cnt; k += nwarps) commit_net_vias(T, P1, P2.ids[lo + k], stamp - 1, -1, lane);
+            commit_vias_strided(T, P1, P2.ids + lo, cnt, gwarp, nwarps, stamp - 1, -1, lane);
             if (!grid_sync(S, T)) return;
             clk.mark(S, 6);
         }
@@ -298,7 +298,7 @@ __global__ void __launch_bounds__(kPersistentThreads, 2) k_flt_persistent(Tables
         }
         if (!grid_sync(S, T)) return;
         clk.mark(S, 5);
-        for (int k = gwarp; k < cnt; k += nwarps) commit_net_vias(T, P2, P2.ids[lo + k], stamp, 1, lane);
+        commit_vias_strided(T, P2, P2.ids + lo, cnt, gwarp, nwarps, stamp, 1, lane);
         if (!grid_sync(S, T)) return;
         clk.mark(S, 6);
     }
@@ -355,7 +355,7 @@ __global__ void __launch_bounds__(kPersistentThreads, 2) k_zshape_persistent(Tab
         }
         if (!grid_sync(S, T)) return;
         clk.mark(S, 5);
-        for (int k = gwarp; k < cnt; k += nwarps) commit_net_vias(T, P, P.ids[lo + k], stamp, 1, lane);
+        commit_vias_strided(T, P, P.ids + lo, cnt, gwarp, nwarps, stamp, 1, lane);
         if (!grid_sync(S, T)) return;
         clk.mark(S, 6);
     }
