@@ -388,7 +388,6 @@ __device__ __forceinline__ int ztrace(const Tables& T, const ZTrees& Z, int nb, 
     return status;
 }
 
-// Route net `id` with one warp; with `commit`, also its wire demand.
 // Route net `id` with the whole CTA (thread t of nth); with `commit`, also its
 // wire demand (warp 0).  `cand`: 2 * LAYER * LAYER ints of shared memory.
 __device__ __forceinline__ void zshape_net(const Tables& T, const ZTrees& Z, const Plan& P, int id, int stamp,
