@@ -92,10 +92,6 @@ __device__ __forceinline__ void set_error(const Tables& T, int code, int info) {
     if (atomicCAS(T.error, 0, code) == 0) *T.error_info = info;
 }
 
-__device__ __forceinline__ bool bit_test(const unsigned* bits, int i) { return (bits[i >> 5] >> (i & 31)) & 1u; }
-
-__device__ __forceinline__ int track_length(const Tables& T, int l) { return along_y(T, l) ? T.Y : T.X; }
-
 // Dirty marking uses fire-and-forget atomics (no return value): the refresh
 // finds the work by scanning the bitmaps, which are small (one bit per cell).
 // Fire-and-forget reductions: the result is never read, so the instruction
