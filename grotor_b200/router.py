@@ -305,7 +305,7 @@ class Router:
     # publish / gather / solve, plus the waits and the raster it overlaps
     # with the solve.  L-shape stage: the next four.
     PHASES = ("batch_raster", "batch_gather", "batch_solve", "batch_publish", "refresh_cells", "dp", "commit",
-              "refresh_prefix", "batch_solver_wait", "batch_worker_wait", "batch_raster_overlap", "unused")
+              "refresh_prefix", "batch_solver_wait", "batch_worker_wait", "unused10", "unused11")
 
     def set_profiling(self, on: bool = True):
         self._check(self._lib.grb_set_profiling(self._ctx, int(bool(on))))

@@ -295,13 +295,14 @@ int64_t grb_kernel_launches(grb_ctx* ctx);
  * group with CUDA events and the persistent kernels time each phase between
  * grid barriers (global timer, thread 0 of one block).  grb_phase_times
  * returns accumulated milliseconds per phase (up to 12 entries):
- * batching [0] raster (persistent: publish), [1] gather of forbidden colours
- * and predecessors, [2] in-chunk solve, [3] publish (plain form only);
- * L-shape stage [4] dirty-cell cost recompute, [5] DP (persistent: + wire
- * commit), [6] commit (persistent: vias), [7] prefix-table rebuild;
- * persistent batching [8] solver waiting for a gathered chunk, [9] other
- * blocks waiting for a solved chunk, [10] raster overlapped with the solve;
- * [11] unused.  The reference prints its stage timings as BATCH_TIMING /
+ * batching [0] raster (persistent: publish of the previous chunk), [1]
+ * gather of forbidden colours and predecessors (persistent: gather of the
+ * next chunk and raster of the one after), [2] in-chunk solve, [3] publish
+ * (plain form only); stages [4] dirty-cell cost recompute, [5] DP
+ * (persistent: + wire commit), [6] commit (persistent: vias), [7]
+ * prefix-table rebuild; persistent batching [8] solver waiting for a
+ * gathered chunk, [9] other blocks waiting for a solved chunk; [10] and [11]
+ * unused.  The reference prints its stage timings as BATCH_TIMING /
  * DAG_TIMING records (router_state.hpp:259-264). */
 int grb_set_profiling(grb_ctx* ctx, int32_t on);
 int grb_phase_times(grb_ctx* ctx, double* ms, int32_t n, int32_t reset);
