@@ -27,7 +27,7 @@ using namespace grb;
 // ---------------------------------------------------------------------------
 namespace {
 
-constexpr int kRefreshThreads = 256;       // refresh_group needs 8 warps
+constexpr int kRefreshThreads = 256;       // threads of a prefix-tree CTA
 constexpr int kPersistentThreads = 256;
 constexpr int kDpThreads = 128;
 constexpr unsigned long long kBarrierTimeoutNs = 20ull * 1000 * 1000 * 1000;
