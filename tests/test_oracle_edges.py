@@ -1,7 +1,8 @@
-"""Edge cases of the oracle's first-fit batching that hold whatever the
-conflict rule: an empty order, a single net, the batch-size limit, and the
-first-fit shape of the result (a net opens at most one new batch, and never
-skips one)."""
+"""Edge cases of the oracle.  First-fit batching, whatever the conflict rule:
+an empty order, a single net, the batch-size limit, and the first-fit shape
+of the result (a net opens at most one new batch, and never skips one).
+Rip-up classification at threshold extremes, and the congestion view of an
+empty grid."""
 import numpy as np
 import pytest
 
@@ -46,3 +47,50 @@ def test_first_fit_shape_and_limit(design, limit):
         assert b <= opened + 1
         opened = max(opened, int(b))
     assert np.bincount(bo, minlength=nb).max() <= limit
+
+
+def _routed(d):
+    from grotor_b200.router import plan_from_batches
+    from helpers import orc_grid
+    n = d.nets
+    bo, nb = _batches(d, d.order, 1000000)
+    ids, off = plan_from_batches(d.order, bo, nb)
+    r = oracle.lshape_stage(orc_grid(d.grid), ids, off, n.node_off, n.nodes, n.parents, n.route_off, threads=2)
+    assert r["status"] == 0
+    return orc_grid(d.grid), r
+
+
+def _wire_length(d, routes, i):
+    from helpers import net_routes
+    g = d.grid
+    XY = g.X * g.Y
+    rr = net_routes(routes, d.nets.route_off, i)
+    total = 0
+    for k in range(1, len(rr), 2):
+        a, b = int(rr[k]), int(rr[k + 1])
+        if a // XY == b // XY:
+            total += abs(a % XY // g.Y - b % XY // g.Y) + abs(a % g.Y - b % g.Y)
+    return total
+
+
+def test_ripup_threshold_extremes(design):
+    """A net is ripped up when more than 10 unit edges of its wires carry
+    overflow (congestion.cuh:114-136): with a threshold below every demand
+    every edge counts, so exactly the nets longer than 10 edges are taken;
+    with a threshold above every demand none is."""
+    g, r = _routed(design)
+    none = oracle.ripup_classify(g, r["demand_half"], 10**6, design.nets.route_off, r["routes"])
+    assert not none.any()
+    every = oracle.ripup_classify(g, r["demand_half"], -10**6, design.nets.route_off, r["routes"])
+    want = np.array([_wire_length(design, r["routes"], i) > 10 for i in range(design.nets.n)], np.uint8)
+    assert want.any() and not want.all()
+    np.testing.assert_array_equal(every, want)
+
+
+def test_congestion_view_without_demand(design):
+    """No demand and non-negative capacities: no congested position and all
+    running sums zero."""
+    g, _ = _routed(design)
+    cong, xs, ys = oracle.congestion_view(g, np.zeros(g.cells, np.int32))
+    assert not cong.any()
+    assert not xs.any() and not ys.any()
