@@ -94,3 +94,18 @@ def test_congestion_view_without_demand(design):
     cong, xs, ys = oracle.congestion_view(g, np.zeros(g.cells, np.int32))
     assert not cong.any()
     assert not xs.any() and not ys.any()
+
+
+def test_plan_from_batches_reverses_and_keeps_order(design):
+    """The execution plan runs the last first-fit batch first
+    (lshape.cuh:70-77); inside a batch the nets keep their order."""
+    from grotor_b200.router import plan_from_batches
+    bo, nb = _batches(design, design.order, 37)
+    ids, off = plan_from_batches(design.order, bo, nb)
+    assert off[0] == 0 and off[-1] == len(design.order) and len(off) == nb + 1
+    assert sorted(ids.tolist()) == sorted(design.order.tolist())
+    for k in range(nb):
+        want = [int(n) for n, b in zip(design.order, bo) if b == nb - 1 - k]
+        assert ids[off[k]:off[k + 1]].tolist() == want
+    e_ids, e_off = plan_from_batches(np.zeros(0, np.int32), np.zeros(0, np.int32), 0)
+    assert len(e_ids) == 0 and e_off.tolist() == [0]
