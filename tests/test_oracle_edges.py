@@ -1,8 +1,8 @@
 """Edge cases of the oracle.  First-fit batching, whatever the conflict rule:
 an empty order, a single net, the batch-size limit, and the first-fit shape
 of the result (a net opens at most one new batch, and never skips one).
-Rip-up classification at threshold extremes, and the congestion view of an
-empty grid."""
+Rip-up classification at threshold extremes, the congestion view of an
+empty grid, and the execution plan built from a first-fit result."""
 import numpy as np
 import pytest
 
