@@ -10,10 +10,21 @@ stage-runtime definition, README.md:139).  The plain per-batch-launch form and
 the CUDA-graph form run on the same GPU afterwards for the comparison the
 metric names, and their routes are checked identical.
 
+After the timed region, on rank 0 of a single-GPU run, the CPU leg runs the
+reference's own CPU first-fit batching (built from its sources into
+oracle/_ref/) on the whole order and the CPU restatement of its DAG code on the
+whole plan (all host cores): their time is ``cpu_baseline``, and their results
+are the checker of the GPU's -- ``parity`` records that the GPU's batches
+equal the reference's and that every route word, the demand, the timestamps
+and the statistics equal the restatement's (which evaluates the cost model's
+exponential through the device's own values, grb_cost_exp, so its costs are
+bit-identical).
+
 ``--impl reference`` times the reference's own CPU implementation of the path
-on the host cores instead (its CPU first-fit batching, built from its sources
-into oracle/_ref/, plus the CPU restatement of its DAG code on all cores) on a
-bounded sample of the same workload.
+on the host cores instead (the same two programs) on a bounded stride sample
+of the same workload per step, plus one run of the reference's batching over
+the whole order; it never loads the routing library (the workload generator is
+a library of its own).
 
 Multi-GPU: the path does not shard (batches depend on each other through
 demand), so ``--gpus N`` runs N independent replicas (seed + rank); timing is
@@ -27,7 +38,6 @@ import os
 import subprocess
 import sys
 import tempfile
-import threading
 import time
 
 import numpy as np
@@ -54,7 +64,8 @@ def parse_args():
     ap.add_argument("--workload", default=WORKLOAD)
     ap.add_argument("--no-compare", action="store_true", help="skip the plain / graph executor comparison")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
-    ap.add_argument("--cpu-nets", type=int, default=0, help="CPU baseline sample size (0: automatic)")
+    ap.add_argument("--cpu-nets", type=int, default=0,
+                    help="nets per step of --impl reference (a stride sample; 0: 30,000)")
     ap.add_argument("--no-tune", action="store_true", help="skip grb_autotune (default launch shapes)")
     ap.add_argument("--executor", default="persistent", choices=["persistent", "plain", "graph"],
                     help="executor of the timed step (the headline is the persistent one)")
@@ -178,6 +189,48 @@ def barrier(pg):
         torch.cuda.synchronize()
 
 
+def host_cores() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def cpu_model() -> str:
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def workload_config(name, grid, n_nets, n_batches):
+    """The `config` of both arms' JSON lines (identical for the same workload)."""
+    return {"workload": name, "grid": [grid.X, grid.Y, grid.L + 1], "nets": int(n_nets), "batches": int(n_batches),
+            "batch_limit": BATCH_LIMIT,
+            "l2": "inputs larger than L2 (cost/prefix/demand tables %.0f MB)" % (grid.cells * 32 / 1e6)}
+
+
+def ref_batching(grid, order, geom):
+    """The reference's own CPU first-fit batching (oracle/_ref/ref_harness,
+    generate_batches_rsmt on one core) over `order`; returns (batch_of per
+    order position, milliseconds it reports), or None when not built."""
+    harness = os.path.join(ROOT, "oracle", "_ref", "ref_harness")
+    if not os.path.exists(harness):
+        return None
+    with tempfile.TemporaryDirectory() as w:
+        np.array([grid.L, grid.X, grid.Y, grid.DIR], np.int32).tofile(os.path.join(w, "meta.i32"))
+        np.asarray(order, np.int32).tofile(os.path.join(w, "order.i32"))
+        for name in ("point_off", "points", "hseg_off", "hsegs", "vseg_off", "vsegs"):
+            np.asarray(getattr(geom, name), np.int32).tofile(os.path.join(w, f"{name}.i32"))
+        res = subprocess.run([harness, "batch", w, str(BATCH_LIMIT), "1"], capture_output=True, text=True,
+                             check=True)
+        ms = float(res.stdout.split("elapsed_ms=")[1].split()[0])
+        return np.fromfile(os.path.join(w, "ref_batch_of.i32"), np.int32), ms
+
+
 def stride_sample(design, target):
     """Every k-th net of the stage order (sizes representative of the design)."""
     order = design.order
@@ -223,19 +276,11 @@ def cpu_stage(design, n_sample, threads):
     ids = ids[np.argsort(pos[ids], kind="stable")]
     sub = sub_nets(design, ids)
     order = np.arange(len(ids), dtype=np.int32)
-    harness = os.path.join(ROOT, "oracle", "_ref", "ref_harness")
     kind = "port"
     t0 = time.perf_counter()
-    if os.path.exists(harness):
-        with tempfile.TemporaryDirectory() as w:
-            np.array([g.L, g.X, g.Y, g.DIR], np.int32).tofile(os.path.join(w, "meta.i32"))
-            order.tofile(os.path.join(w, "order.i32"))
-            for name in ("point_off", "points", "hseg_off", "hsegs", "vseg_off", "vsegs"):
-                np.asarray(getattr(sub, name), np.int32).tofile(os.path.join(w, f"{name}.i32"))
-            res = subprocess.run([harness, "batch", w, str(BATCH_LIMIT), "1"], capture_output=True, text=True,
-                                 check=True)
-            batch_ms = float(res.stdout.split("elapsed_ms=")[1].split()[0])
-            bo = np.fromfile(os.path.join(w, "ref_batch_of.i32"), np.int32)
+    rb = ref_batching(g, order, sub)
+    if rb is not None:
+        bo, batch_ms = rb
         kind = "reference"
     else:
         tb = time.perf_counter()
@@ -350,11 +395,8 @@ def run_grotor(args):
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": args.workload, "grid": [design.grid.X, design.grid.Y, design.grid.L + 1],
-                   "nets": n_nets, "batches": int(stats_p["n_batches"]), "batch_limit": BATCH_LIMIT,
-                   "executor": args.executor, "parallelism": f"replicas{world}",
-                   "l2": "inputs larger than L2 (cost/prefix/demand tables %.0f MB)" % (
-                       design.grid.cells * 32 / 1e6)},
+        "config": workload_config(args.workload, design.grid, n_nets, stats_p["n_batches"]),
+        "executor": args.executor, "parallelism": f"replicas{world}",
         "stage": {"batching_ms": float(np.mean(bt)), "dag_ms": float(np.mean(dt)),
                   "wirelength": stats_p["wirelength"], "vias": stats_p["vias"]},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
@@ -411,27 +453,80 @@ def run_grotor(args):
         comp["routes_identical"] = identical
         result["executors"] = comp
 
-    result["config"]["autotune"] = tune
+    result["autotune"] = tune
+    if rank == 0 and world == 1 and not args.no_cpu:
+        # Untimed: the GPU's batch of every order position, for the checker.
+        gpu_batch_of, _ = r.generate_batches_rsmt(order, BATCH_LIMIT, 1, args.executor)
+        base, parity = cpu_leg(design, args.workload, gpu_batch_of, ids, off, routes_p, tables_p, stats_p)
+        result["cpu_baseline"] = base
+        result["parity"] = parity
     if rank == 0 and world == 1 and not args.no_extra:
         r.close()
         r = None
         result["zshape"] = zshape_measure(args)
         result["softmin"] = softmin_measure(args)
-    if rank == 0 and world == 1 and not args.no_cpu:
-        threads = os.cpu_count() or 1
-        target = args.cpu_nets or 60000
-        sec, info = cpu_stage(design, target, threads)
-        result["cpu_baseline"] = {"value": info["nets"] / sec, "unit": UNIT, "cores": threads, "kind": info["kind"],
-                                  "sample": (f"every {max(1, n_nets // target)}-th net of {args.workload} in stage "
-                                             f"order ({info['nets']} nets, {info['batches']} batches): reference "
-                                             f"CPU batching {info['batching_ms']:.0f} ms on 1 core + CPU DAG "
-                                             f"restatement {info['dag_ms']:.0f} ms on {threads} threads")}
     if r is not None:
         r.close()
     if pg is not None:
         pg.destroy_process_group()
     if rank == 0:
         print(json.dumps(result), flush=True)
+
+
+def cpu_leg(design, workload, gpu_batch_of, ids, off, routes, tables, stats):
+    """The CPU baseline on the whole workload, which is also the checker of the
+    GPU run: the reference's own CPU batching over the whole order (one core,
+    its design), then the CPU restatement of its DAG code over the whole plan
+    on every host core, with the device's values of the cost model's
+    exponential.  Returns (cpu_baseline, parity)."""
+    import ctypes as C
+
+    import oracle
+    from grotor_b200 import _abi
+    g, n = design.grid, design.nets
+    cores = host_cores()
+    t0 = time.perf_counter()
+    rb = ref_batching(g, design.order, n)
+    if rb is not None:
+        ref_bo, batch_ms, kind = rb[0], rb[1], "reference"
+    else:
+        tb = time.perf_counter()
+        ref_bo, _ = oracle.batches(g.X, g.Y, design.order, n.point_off, n.points, n.hseg_off, n.hsegs, n.vseg_off,
+                                   n.vsegs, BATCH_LIMIT, 1)
+        batch_ms, kind = (time.perf_counter() - tb) * 1e3, "port"
+    og = oracle.OrcGrid(g.L, g.X, g.Y, g.DIR, g.unit_wire, g.unit_via, g.short_costs, g.x_edge_len, g.y_edge_len,
+                        g.capacity)
+    x = oracle.exp_args(og, int(tables["demand_half"].max()) + 8)
+    y = np.empty_like(x)
+    assert _abi.load().grb_cost_exp(0, x.ctypes.data_as(C.c_void_p), len(x), y.ctypes.data_as(C.c_void_p)) == 0
+    oracle.set_exp_table(x, y)
+    td = time.perf_counter()
+    orc = oracle.lshape_stage(og, ids, off, n.node_off, n.nodes, n.parents, n.route_off, threads=cores)
+    dag_ms = (time.perf_counter() - td) * 1e3
+    misses = oracle.exp_table_misses()
+    oracle.set_exp_table()
+    log(f"cpu leg: batching {batch_ms:.0f} ms ({kind}), DAG {dag_ms:.0f} ms on {cores} cores, "
+        f"{time.perf_counter() - t0:.0f} s in all")
+    sec = (batch_ms + dag_ms) / 1e3
+    base = {"value": n.n / sec, "unit": UNIT, "cores": cores, "kind": kind, "cpu_model": cpu_model(),
+            "batching_ms": batch_ms, "dag_ms": dag_ms,
+            "sample": (f"the whole workload ({n.n} nets, {int(ref_bo.max()) + 1} batches): the reference's CPU "
+                       f"first-fit batching on 1 core (its own code, oracle/_ref) + the CPU restatement of its DAG "
+                       f"code on {cores} threads")}
+    checks = {
+        "batches_equal_reference_cpu": bool(np.array_equal(ref_bo, gpu_batch_of)),
+        "routes_equal_oracle": bool(np.array_equal(orc["routes"], routes)),
+        "demand_equal_oracle": bool(np.array_equal(orc["demand_half"], tables["demand_half"])),
+        "timestamps_equal_oracle": bool(np.array_equal(orc["timestamp"], tables["timestamp"])),
+        "wirelength_equal_oracle": orc["wirelength"] == stats["wirelength"],
+        "vias_equal_oracle": orc["vias"] == stats["vias"],
+        "exp_table_misses": int(misses),
+    }
+    ok = all(v for k, v in checks.items() if k != "exp_table_misses") and misses == 0 and orc["status"] == 0
+    parity = {"result": "identical" if ok else "DIFFERS", **checks,
+              "how": ("GPU batches vs the reference's own CPU batching over the whole order; GPU stage vs the CPU "
+                      "restatement on the same plan with the device's exponential values")}
+    return base, parity
 
 
 # --------------------------------------------------------------------------- other stages
@@ -531,13 +626,31 @@ def softmin_measure(args, workload="softmin_320x320x10", taus=(1.0, 0.1, 0.01), 
 
 # --------------------------------------------------------------------------- reference arm
 def run_reference(args):
+    """The reference's own CPU implementation of the path: its CPU first-fit
+    batching (oracle/_ref, one core by design) and the CPU restatement of its
+    DAG code (all host cores).  Per step a stride sample of the workload's nets
+    (sized so the run ends within minutes); the reference's batching over the
+    whole order is timed once besides.  Loads the workload generator and the
+    restatement, never the routing library."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
     from grotor_b200.synth import WORKLOADS, Design
     design = Design(WORKLOADS[args.workload])
-    threads = os.cpu_count() or 1
+    threads = host_cores()
     target = args.cpu_nets or 30000
+    rb = ref_batching(design.grid, design.order, design.nets)
+    if rb is not None:
+        full_bo, full_ms = rb
+    else:
+        import oracle
+        g, n = design.grid, design.nets
+        t = time.perf_counter()
+        full_bo, _ = oracle.batches(g.X, g.Y, design.order, n.point_off, n.points, n.hseg_off, n.hsegs,
+                                    n.vseg_off, n.vsegs, BATCH_LIMIT, 1)
+        full_ms = (time.perf_counter() - t) * 1e3
+    n_batches = int(full_bo.max()) + 1 if len(full_bo) else 0
+    log(f"reference batching over the whole order: {full_ms:.0f} ms, {n_batches} batches")
     times, info = [], None
     for i in range(args.warmup + args.steps):
         sec, info = cpu_stage(design, target, threads)
@@ -547,15 +660,18 @@ def run_reference(args):
     value = info["nets"] / float(np.mean(times))
     sample = (f"every {max(1, design.n_subnets // target)}-th net of {args.workload} in stage order "
               f"({info['nets']} nets, {info['batches']} batches): reference CPU batching (its own code, 1 core) "
-              f"+ CPU restatement of its DAG code on {threads} threads")
+              f"+ CPU restatement of its DAG code on {threads} threads; the sample has fewer batches than the "
+              f"whole design, so its per-net batching is cheaper (whole order: {full_ms:.0f} ms for "
+              f"{design.n_subnets} nets)")
     result = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": int(os.environ.get("WORLD_SIZE", "1")),
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": float(np.mean(times)) * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": args.workload, "grid": [design.grid.X, design.grid.Y, design.grid.L + 1],
-                   "nets": design.n_subnets, "batch_limit": BATCH_LIMIT, "parallelism": "host"},
-        "impl": "reference",
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": info["kind"], "sample": sample},
+        "config": workload_config(args.workload, design.grid, design.n_subnets, n_batches),
+        "parallelism": "host", "impl": "reference",
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": info["kind"],
+                         "cpu_model": cpu_model(), "sample": sample},
+        "full_order_batching_ms": full_ms,
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(result), flush=True)

@@ -1,7 +1,11 @@
 """ctypes mirror of include/grb.h and include/grb_synth.h.
 
-The shared library ``libgrb.so`` is built in-tree by ``grotor_b200.build``.
-Loading fails loudly when it is missing: the package has no CPU fallback.
+The shared library ``libgrb.so`` (the routing path) is built in-tree by
+``grotor_b200.build``; loading fails loudly when it is missing: the package has
+no CPU fallback.  The seeded workload generator of include/grb_synth.h is a
+separate host-only library, ``libgrb_synth.so``, so a process that only needs
+synthetic designs (the CPU reference arm of bench.py) never loads the routing
+library.
 """
 from __future__ import annotations
 
@@ -10,6 +14,7 @@ import os
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libgrb.so")
+SYNTH_PATH = os.path.join(_HERE, "libgrb_synth.so")
 
 GRB_OK, GRB_EINVAL, GRB_ENOMEM, GRB_ECUDA, GRB_ETIMEDOUT, GRB_ELIMIT = range(6)
 MODE_PLAIN, MODE_GRAPH, MODE_PERSISTENT = 0, 1, 2
@@ -91,6 +96,7 @@ SIGNATURES = {
     "grb_plan_bbox_batches": (C.c_int, [P, P, C.c_int32, C.POINTER(C.c_int32)]),
     "grb_zshape_stage": (C.c_int, [P, C.c_int32, C.POINTER(GrbStats)]),
     "grb_congestion_view": (C.c_int, [P, P, P, P]),
+    "grb_cost_exp": (C.c_int, [C.c_int32, P, C.c_int32, P]),
     "grb_read_tables": (C.c_int, [P, P, P, P, P, P]),
     "grb_read_routes": (C.c_int, [P, P]),
     "grb_get_stats": (C.c_int, [P, C.POINTER(GrbStats)]),
@@ -99,7 +105,12 @@ SIGNATURES = {
     "grb_kernel_launches": (C.c_int64, [P]),
     "grb_set_profiling": (C.c_int, [P, C.c_int32]),
     "grb_phase_times": (C.c_int, [P, P, C.c_int32, C.c_int32]),
-    # grb_synth.h
+    # grb_prof.h
+    "grb_stage_traffic": (C.c_int, [P, C.c_int32, P, P, P, P, P, P, P, P, P, P, P, P, C.c_int32, P]),
+}
+
+# include/grb_synth.h (libgrb_synth.so)
+SYNTH_SIGNATURES = {
     "grb_synth_generate": (P, [C.POINTER(GrbSynthParams)]),
     "grb_design_free": (None, [P]),
     "grb_design_error": (C.c_char_p, [P]),
@@ -111,23 +122,29 @@ SIGNATURES = {
     "grb_design_subnet_info": (C.c_int, [P, C.POINTER(P), C.POINTER(P), C.POINTER(P)]),
     "grb_design_order": (C.c_int, [P, P]),
     "grb_design_pins": (C.c_int, [P, C.POINTER(P), C.POINTER(P), C.POINTER(C.c_int32)]),
-    # grb_prof.h
-    "grb_stage_traffic": (C.c_int, [P, C.c_int32, P, P, P, P, P, P, P, P, P, P, P, P, C.c_int32, P]),
 }
 
-_lib = None
+_libs = {}
 
 
-def load() -> C.CDLL:
-    """Load libgrb.so (raises if it has not been built)."""
-    global _lib
-    if _lib is None:
-        if not os.path.exists(LIB_PATH):
-            raise ImportError(f"grotor_b200 native library missing: {LIB_PATH} (run grotor_b200.build.build())")
-        lib = C.CDLL(LIB_PATH)
-        for name, (res, args) in SIGNATURES.items():
+def _open(path: str, signatures: dict) -> C.CDLL:
+    if path not in _libs:
+        if not os.path.exists(path):
+            raise ImportError(f"grotor_b200 native library missing: {path} (run grotor_b200.build.build())")
+        lib = C.CDLL(path)
+        for name, (res, args) in signatures.items():
             f = getattr(lib, name)
             f.restype = res
             f.argtypes = args
-        _lib = lib
-    return _lib
+        _libs[path] = lib
+    return _libs[path]
+
+
+def load() -> C.CDLL:
+    """Load libgrb.so, the routing path (raises if it has not been built)."""
+    return _open(LIB_PATH, SIGNATURES)
+
+
+def load_synth() -> C.CDLL:
+    """Load libgrb_synth.so, the workload generator (host code only)."""
+    return _open(SYNTH_PATH, SYNTH_SIGNATURES)

@@ -1,6 +1,6 @@
 // commit.cuh -- demand commit and rip-up of routed nets.
 //
-// Semantics of the reference's batch commit (demand.cuh:410-493): wires first
+// Semantics of the reference's batch commit (demand.cuh:236-319): wires first
 // (each unit edge gets K, its timestamp becomes the batch stamp, both segment
 // endpoints are stamped), then -- after every wire of the batch is in -- vias:
 // each via layer whose cell was not stamped by a wire of this batch adds K to

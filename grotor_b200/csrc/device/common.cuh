@@ -12,7 +12,7 @@
 namespace grb {
 
 constexpr double kInf = 1e22;   // router_state.hpp:271
-constexpr int kMaxLayers = 10;  // lshape_warp.cuh:314 asserts L <= 10
+constexpr int kMaxLayers = 10;  // lshape_warp.cuh:115 asserts L <= 10
 constexpr int kTrackGroup = 32; // tracks per prefix group (one per lane)
 
 enum : int {

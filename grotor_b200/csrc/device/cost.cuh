@@ -20,12 +20,17 @@
 
 namespace grb {
 
+// The exponential of the cost model: CUDA's __expf on a float argument, the
+// reference's choice (full_update.cuh:12-13).  grb_cost_exp evaluates the same
+// function for checkers.
+__device__ __forceinline__ float cost_exp(float a) { return __expf(a); }
+
 __device__ __forceinline__ double of_cost_scaled(double scale, float capacity, float demand) {
     if (capacity > 0.001) {
         const float diff = demand - capacity;
-        return __expf(fmin(0.5 * diff, scale * 0.5 * diff));
+        return cost_exp(static_cast<float>(fmin(0.5 * diff, scale * 0.5 * diff)));
     }
-    if (demand > 0) return __expf(fmin(1.5 * demand, scale * 1.5 * demand));
+    if (demand > 0) return cost_exp(static_cast<float>(fmin(1.5 * demand, scale * 1.5 * demand)));
     return 0;
 }
 

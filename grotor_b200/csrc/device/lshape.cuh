@@ -1,7 +1,7 @@
 // lshape.cuh -- L-shape pattern routing with layer assignment, one warp per net.
 //
 // Semantics are those of the reference's tree DP (lshape_thread.cuh:18-171,
-// lshape_warp.cuh:8-446): per tree node a table dist[low][high] over layer
+// lshape_warp.cuh:8-247): per tree node a table dist[low][high] over layer
 // ranges (via stack cost inside the range, INF where a pin's layer falls
 // outside); children are merged into their parent in descending node order;
 // an edge is a straight wire or an L with a via stack at the corner; strict '<'
@@ -234,7 +234,7 @@ __device__ void lshape_net(const Tables& T, const Plan& P, int id, int stamp, co
         }
     }
     __syncwarp();
-    // 5. Segment emission in node order (lshape_warp.cuh:414-439).
+    // 5. Segment emission in node order (lshape_warp.cuh:215-240).
     int* out = P.routes + P.route_off[id];
     const long long cap = P.route_off[id + 1] - P.route_off[id];
     int next = 1;

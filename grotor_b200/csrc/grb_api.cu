@@ -943,6 +943,11 @@ __global__ void k_float_line_prefix(float* v, int lines, int len, int line_strid
     }
 }
 
+// The cost model's exponential for n values (grb_cost_exp).
+__global__ void k_cost_exp(const float* x, int n, float* y) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) y[i] = cost_exp(x[i]);
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------------------
@@ -951,7 +956,8 @@ __global__ void k_float_line_prefix(float* v, int lines, int len, int line_strid
 // The rip-up classification needs one int per grid cell (overflow marks, then
 // their prefix along each track) and one flag per net.  For callers that must
 // not allocate device memory this scratch lives in one file-scope array that
-// every GPU loading the library holds until the process exits (about 20 MiB).
+// every GPU loading the library holds until the process exits:
+// (4,194,304 + 262,144) ints = 17,825,792 bytes = 17.0 MiB.
 constexpr int kNoAllocCells = 4 << 20;  // at most 4,194,304 grid cells (L*X*Y)
 constexpr int kNoAllocNets = 1 << 20;   // at most 1,048,576 nets
 constexpr int kNoAllocWords = kNoAllocCells + kNoAllocNets / 4;
@@ -1286,7 +1292,7 @@ int route_plain(grb_ctx* c, int b, int stamp) {
 int commit_plain(grb_ctx* c, int b, int stamp, int K) {
     const int cnt = c->h_batch_off[b + 1] - c->h_batch_off[b];
     if (cnt <= 0) return GRB_OK;
-    const int blocks = std::min((cnt + 3) / 4, 1056);  // demand.cuh:490
+    const int blocks = std::min((cnt + 3) / 4, 1056);  // demand.cuh:316
     cudaEvent_t e;
     const int prc = prof_begin(c, 6, &e);
     if (prc) return prc;
@@ -2710,7 +2716,8 @@ int grb_ripup_classify(grb_ctx* c, int32_t threshold, uint8_t* is_of) {
 
 // Device address of g_noalloc_scratch on the current device.  Host code only
 // holds a host-side stand-in for the array's name, so the address is looked up
-// once per device, with that device current, and cached.
+// once per device, with that device current, and cached until the process
+// exits (a device reset by the host application invalidates it).
 static int noalloc_scratch(grb_ctx* c, int** out) {
     static std::mutex lock;
     static std::vector<int*> cache;
@@ -2753,6 +2760,23 @@ int grb_ripup_classify_noalloc(grb_ctx* c, int32_t threshold, uint8_t* is_of) {
     GRB_CUDA(c, cudaGetLastError());
     if (c->n_nets) GRB_CUDA(c, cudaMemcpyAsync(is_of, flags, c->n_nets, cudaMemcpyDeviceToHost, c->stream));
     GRB_CUDA(c, cudaStreamSynchronize(c->stream));
+    return GRB_OK;
+}
+
+int grb_cost_exp(int32_t device, const float* x, int32_t n, float* y) {
+    if (n < 0 || (n > 0 && (!x || !y))) return GRB_EINVAL;
+    if (n == 0) return GRB_OK;
+    if (cudaSetDevice(device) != cudaSuccess) { cudaGetLastError(); return GRB_ECUDA; }
+    float* d = nullptr;
+    if (cudaMalloc(&d, sizeof(float) * 2 * size_t(n)) != cudaSuccess) { cudaGetLastError(); return GRB_ENOMEM; }
+    cudaError_t e = cudaMemcpy(d, x, sizeof(float) * n, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) {
+        k_cost_exp<<<std::min((n + 255) / 256, 4096), 256>>>(d, n, d + n);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpy(y, d + n, sizeof(float) * n, cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    if (e != cudaSuccess) { cudaGetLastError(); return GRB_ECUDA; }
     return GRB_OK;
 }
 

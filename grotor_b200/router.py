@@ -6,7 +6,7 @@ and exposes the reference's hot-path seams under their reference names:
 * ``generate_batches_rsmt``  -- cudb::generate_batches_rsmt (generate_batches_cpu.hpp:7)
 * ``refresh_cost``           -- graph::refresh_cost (incremental_update.cuh:98)
 * ``route_batch``            -- the Lshape_route_warp launch (lshape.cuh:168)
-* ``commit_batch_demand``    -- graph::commit_batch_demand (demand.cuh:487)
+* ``commit_batch_demand``    -- graph::commit_batch_demand (demand.cuh:313)
 * ``lshape_route``           -- Lshape_route::Lshape_route's hot loop (lshape.cuh:153-179)
 * ``ripup``                  -- graph::ripup (congestion.cuh:114)
 

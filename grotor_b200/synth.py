@@ -1,4 +1,4 @@
-"""Seeded synthetic designs (wrapper of include/grb_synth.h).
+"""Seeded synthetic designs (wrapper of include/grb_synth.h, libgrb_synth.so).
 
 Five workloads follow the reference benchmark plan (GCell grid, capacity
 model, pin-count and bounding-box distributions); ``scaled`` variants keep a
@@ -70,7 +70,7 @@ class Design:
     """A generated design plus its routing topology (host arrays)."""
 
     def __init__(self, params: SynthParams, max_subnet_pins: int = 12, threads: int = 0):
-        self._lib = _abi.load()
+        self._lib = _abi.load_synth()
         self.params = params
         s = _abi.GrbSynthParams(**{f: getattr(params, f) for f, _ in _abi.GrbSynthParams._fields_})
         self._d = C.c_void_p(self._lib.grb_synth_generate(C.byref(s)))

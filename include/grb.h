@@ -15,7 +15,7 @@
  *  - Tree nodes are 3-D cell ids; Steiner nodes use layer L (preprocess.hpp:131).
  *  - Route words per net: [count, a0, b0, a1, b1, ...] where count is one past
  *    the last used word, exactly the reference's route record
- *    (lshape_warp.cuh:414-439); a pair with equal layers is a wire, otherwise a
+ *    (lshape_warp.cuh:215-240); a pair with equal layers is a wire, otherwise a
  *    via stack.
  *  - Demand is int32 half-units (wire edge +2, split via landing +1 each side);
  *    demand_half * 0.5f equals the reference's float demand bit-for-bit.
@@ -94,7 +94,7 @@ const char* grb_last_error(const grb_ctx* ctx);
 void* grb_stream(grb_ctx* ctx);
 
 /* Zero demand, timestamps, statistics and routes; mark every cost dirty
- * (the state of a freshly built database; lshape_benchmark.cuh:276-290). */
+ * (the state of a freshly built database; experiments/lshape_benchmark.cuh:86-99). */
 int grb_reset(grb_ctx* ctx);
 
 /* Upload per-net topology and geometry (host buffers; replaces the uploads in
@@ -119,10 +119,10 @@ int grb_get_plan(grb_ctx* ctx, int32_t* ids, int32_t* batch_off, int32_t* n, int
 int grb_refresh_cost(grb_ctx* ctx);
 
 /* Route batch `b` of the plan with L-shape patterns (Lshape_route_warp,
- * lshape_warp.cuh:304-446); writes routes only. */
+ * lshape_warp.cuh:105-247); writes routes only. */
 int grb_route_batch(grb_ctx* ctx, int32_t b, int32_t stamp);
 
-/* graph::commit_batch_demand (demand.cuh:487-493): K = +1 commits, K = -1
+/* graph::commit_batch_demand (demand.cuh:313-319): K = +1 commits, K = -1
  * rips up the batch's routes. */
 int grb_commit_batch(grb_ctx* ctx, int32_t b, int32_t stamp, int32_t K);
 
@@ -142,10 +142,13 @@ int grb_ripup_classify(grb_ctx* ctx, int32_t threshold, uint8_t* is_of);
  * device-wide synchronisation cudaMalloc/cudaFree bring.  This entry point
  * allocates nothing: its scratch (one int per grid cell, one flag per net) is a
  * fixed array inside the library that every GPU loading the library holds until
- * the process exits (about 20 MiB).  Limits: at most 4,194,304 grid cells
- * (L*X*Y) and 1,048,576 nets; larger designs get GRB_ELIMIT.  The first call on
- * a device looks up the array's device address with that device current, so it
- * should come before any stream capture.  All calls share the one array (its
+ * the process exits: (4,194,304 + 262,144) ints = 17.0 MiB.  Limits: at most
+ * 4,194,304 grid cells (L*X*Y) and 1,048,576 nets; larger designs get
+ * GRB_ELIMIT.  The first call on a device looks up the array's device address
+ * with that device current, so it should come before any stream capture; the
+ * address is kept until the process exits, so a caller that resets the device
+ * (cudaDeviceReset, which destroys the primary context) must not call this
+ * entry point again in that process.  All calls share the one array (its
  * contents are those of the last call, and every word is rewritten before use),
  * so calls that overlap on the GPU -- two contexts or streams on the same
  * device at once -- race; serialise them.  Results equal grb_ripup_classify's. */
@@ -273,6 +276,15 @@ int grb_softmin_backward(grb_ctx* ctx, int32_t dtype, double tau, const void* ca
 
 /* Congestion view for the FLT topology builder (congestion.cuh:60-112). */
 int grb_congestion_view(grb_ctx* ctx, uint8_t* congestion, float* xsum, float* ysum);
+
+/* The cost model's exponential as the cost kernels evaluate it on `device`
+ * (CUDA's __expf on a float argument, the reference's choice in
+ * full_update.cuh:12-13): y[i] = exp(x[i]) for n host values (no counterpart
+ * in the reference).  For checkers that restate the cost model on the host and
+ * must reproduce the device's cost tables bit for bit: given these values for
+ * the arguments the model can produce, a host restatement needs no copy of the
+ * device's exponential.  Needs no context; allocates and synchronises. */
+int grb_cost_exp(int32_t device, const float* x, int32_t n, float* y);
 
 /* Read device tables (any pointer may be NULL). */
 int grb_read_tables(grb_ctx* ctx, float* wcost, float* vcost, double* presum, int32_t* demand_half,

@@ -6,6 +6,7 @@
 #include "grb_oracle.h"
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -25,23 +26,60 @@ struct Grid {
     bool along_y(int l) const { return ((l & 1) ^ DIR) != 0; }
 };
 
+// The exponential of the cost model.  The reference evaluates CUDA's __expf;
+// the host expf stands in for it (tolerance-level agreement), unless a table
+// of the device's own values has been set (orc_set_exp_table): then every
+// argument is looked up there and the cost tables come out bit-identical to
+// the device's.  Arguments missing from a set table fall back to expf and are
+// counted (orc_exp_table_misses), so a checker can prove the table was complete.
+struct ExpTable {
+    std::vector<float> x, y;  // x ascending
+    std::atomic<long long> misses{0};
+};
+ExpTable g_exp;
+
+float cost_exp(float a) {
+    if (!g_exp.x.empty()) {
+        const auto it = std::lower_bound(g_exp.x.begin(), g_exp.x.end(), a);
+        if (it != g_exp.x.end() && *it == a) return g_exp.y[it - g_exp.x.begin()];
+        g_exp.misses.fetch_add(1, std::memory_order_relaxed);
+    }
+    return expf(a);
+}
+
 // full_update.cuh:9-14 (of_cost_scaled).  The reference passes capacity and
 // demand as float; the difference is a float subtraction, scaled in double, and
-// the argument of the exponential is narrowed to float.  The host expf stands in
-// for CUDA's __expf (tolerance-level agreement, see header).
-double of_cost_scaled(double scale, float capacity, float demand) {
+// the argument of the exponential is narrowed to float.  Returns false where
+// no exponential is evaluated (zero capacity and no demand).
+bool of_cost_arg(double scale, float capacity, float demand, float* arg) {
     if (capacity > 0.001) {
         const float diff = demand - capacity;
         const double a = 0.5 * static_cast<double>(diff);
         const double b = scale * 0.5 * static_cast<double>(diff);
-        return static_cast<double>(expf(static_cast<float>(std::min(a, b))));
+        *arg = static_cast<float>(std::min(a, b));
+        return true;
     }
     if (demand > 0) {
         const double a = 1.5 * static_cast<double>(demand);
         const double b = scale * 1.5 * static_cast<double>(demand);
-        return static_cast<double>(expf(static_cast<float>(std::min(a, b))));
+        *arg = static_cast<float>(std::min(a, b));
+        return true;
     }
-    return 0;
+    return false;
+}
+
+double of_cost_scaled(double scale, float capacity, float demand) {
+    float a;
+    return of_cost_arg(scale, capacity, demand, &a) ? static_cast<double>(cost_exp(a)) : 0.0;
+}
+
+// The demands incremental_of_cost passes to of_cost_scaled for a cell of
+// demand h half-units: without and with each increment the cost model adds.
+void cost_demands(int h, float out[3]) {
+    const float dem = static_cast<float>(h) * 0.5f;
+    out[0] = static_cast<float>(static_cast<double>(dem) + 0.0);
+    out[1] = static_cast<float>(static_cast<double>(dem) + 1.0 + 0.0);
+    out[2] = static_cast<float>(static_cast<double>(dem) + 0.5 + 0.0);
 }
 
 // full_update.cuh:23-32 (incremental_of_cost).
@@ -115,6 +153,39 @@ void sklansky_track(int n, Load load, Store store) {
 
 extern "C" {
 
+int64_t orc_exp_args(const orc_grid* g, int32_t max_demand_half, float* out, int64_t cap) {
+    std::vector<float> caps(g->capacity, g->capacity + size_t(g->L) * g->X * g->Y);
+    std::sort(caps.begin(), caps.end());
+    caps.erase(std::unique(caps.begin(), caps.end()), caps.end());
+    std::vector<float> args;
+    for (float c : caps)
+        for (int h = 0; h <= max_demand_half; ++h) {
+            float dem[3];
+            cost_demands(h, dem);
+            for (float d : dem) {
+                float a;
+                if (of_cost_arg(g->of_cost_scale, c, d, &a)) args.push_back(a);
+            }
+        }
+    std::sort(args.begin(), args.end());
+    args.erase(std::unique(args.begin(), args.end()), args.end());
+    const int64_t n = int64_t(args.size());
+    if (out) std::copy(args.begin(), args.begin() + std::min(n, cap), out);
+    return n;
+}
+
+void orc_set_exp_table(int64_t n, const float* x, const float* y) {
+    std::vector<std::pair<float, float>> v(size_t(std::max<int64_t>(n, 0)));
+    for (int64_t i = 0; i < n; ++i) v[i] = {x[i], y[i]};
+    std::sort(v.begin(), v.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
+    g_exp.x.resize(v.size());
+    g_exp.y.resize(v.size());
+    for (size_t i = 0; i < v.size(); ++i) { g_exp.x[i] = v[i].first; g_exp.y[i] = v[i].second; }
+    g_exp.misses.store(0);
+}
+
+int64_t orc_exp_table_misses(void) { return g_exp.misses.load(); }
+
 void orc_cost_full(const orc_grid* g, const int32_t* demand_half, float* wcost, float* vcost) {
     Grid G(g);
     const int cells = G.L * G.X * G.Y;
@@ -164,7 +235,7 @@ void orc_presum_logstep(const orc_grid* g, const float* wcost, double* presum) {
 }
 
 // lshape_thread.cuh:18-171 (Lshape_route_cuda), one net at a time; the warp
-// kernel lshape_warp.cuh:304-446 is equal to it by construction (children of a
+// kernel lshape_warp.cuh:105-247 is equal to it by construction (children of a
 // parent are merged in descending node order in both).
 int orc_lshape_batch(const orc_grid* g, const float* vcost, const double* presum,
                      int32_t n, const int32_t* ids, const int32_t* node_off,
@@ -294,7 +365,7 @@ int orc_lshape_batch(const orc_grid* g, const float* vcost, const double* presum
 }  // extern "C"
 
 namespace {
-// demand.cuh:410-493 (commit_batch_wires then commit_batch_vias).  `touched`,
+// demand.cuh:236-319 (commit_batch_wires then commit_batch_vias).  `touched`,
 // when given, receives every edge cell whose demand changed.
 void commit_impl(const orc_grid* g, int32_t n, const int32_t* ids,
                  const int64_t* route_off, const int32_t* routes,

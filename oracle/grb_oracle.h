@@ -9,8 +9,10 @@
  * Every function restates the reference's algorithm from its source (file:line
  * cited at each definition, paths relative to the GRotor project root).  Cost
  * values use the host's expf where the reference uses CUDA's __expf, so costs
- * agree with the GPU within 1e-6 relative; every other step (prefix addition
- * order, DP comparisons, tie-breaks, demand, batching) is exact.  Parity of the
+ * agree with the GPU within 1e-6 relative -- or bit for bit once a table of
+ * the device's own exponential values is installed (orc_set_exp_table); every
+ * other step (prefix addition order, DP comparisons, tie-breaks, demand,
+ * batching) is exact.  Parity of the
  * restatement is pinned against outputs of the reference itself (see
  * tests/golden/ and oracle/ref_harness.cu).
  *
@@ -36,6 +38,19 @@ typedef struct orc_grid {
     const float* capacity;       /* [L*X*Y] */
     int32_t integer_wire;        /* 1: GGR build's wire costs, clamped to [0, 1e7] and truncated (full_update.cuh:47-50) */
 } orc_grid;
+
+/* The cost model's exponential (full_update.cuh:9-14).  By default the host's
+ * expf stands in for the device's __expf, which agrees within 1e-6 relative.
+ * orc_exp_args writes, ascending and without repeats, every argument the cost
+ * model can pass to the exponential on this grid for cell demands of 0 ..
+ * max_demand_half half-units (at most `cap` of them; returns the count).
+ * orc_set_exp_table installs the device's values y[i] = exp(x[i]) for such
+ * arguments (n = 0 removes the table); with it every cost value equals the
+ * device's bit for bit.  Arguments missing from an installed table use expf
+ * and are counted by orc_exp_table_misses (reset by orc_set_exp_table). */
+int64_t orc_exp_args(const orc_grid* g, int32_t max_demand_half, float* out, int64_t cap);
+void orc_set_exp_table(int64_t n, const float* x, const float* y);
+int64_t orc_exp_table_misses(void);
 
 /* Full cost recompute: wcost/vcost from capacity and demand. */
 void orc_cost_full(const orc_grid* g, const int32_t* demand_half, float* wcost, float* vcost);

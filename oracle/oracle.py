@@ -13,7 +13,7 @@ _LIB = os.path.join(_HERE, "liboracle.so")
 __all__ = [
     "build", "load", "OrcGrid", "cost_full", "presum", "presum_logstep", "lshape_batch",
     "commit_batch", "batches", "ripup_classify", "congestion_view", "lshape_stage", "flt_stage", "zshape_stage",
-    "bbox_batches",
+    "bbox_batches", "exp_args", "set_exp_table", "exp_table_misses",
 ]
 
 
@@ -66,6 +66,10 @@ def _declare(lib):
     lib.orc_zshape_stage.restype = C.c_int
     lib.orc_bbox_batches.argtypes = [C.c_int32, C.c_int32, C.c_int32, P, P, C.c_int32, P, P]
     lib.orc_bbox_batches.restype = C.c_int32
+    lib.orc_exp_args.argtypes = [P, C.c_int32, P, C.c_int64]
+    lib.orc_exp_args.restype = C.c_int64
+    lib.orc_set_exp_table.argtypes = [C.c_int64, P, P]
+    lib.orc_exp_table_misses.restype = C.c_int64
 
 
 class _COrcFlt(C.Structure):
@@ -260,3 +264,29 @@ def bbox_batches(X, Y, group, bbox, max_batch=250):
     nb = lib.orc_bbox_batches(int(X), int(Y), len(group), _p(group), _p(_c(bbox, np.int32)), int(max_batch),
                               _p(ids), _p(off))
     return [ids[off[k]:off[k + 1]].tolist() for k in range(nb)]
+
+
+def exp_args(g: OrcGrid, max_demand_half: int) -> np.ndarray:
+    """Every argument the cost model can pass to the exponential on this grid
+    for cell demands up to max_demand_half half-units (ascending, unique)."""
+    lib = load()
+    n = lib.orc_exp_args(g.ref, int(max_demand_half), None, 0)
+    out = np.empty(n, np.float32)
+    lib.orc_exp_args(g.ref, int(max_demand_half), _p(out), n)
+    return out
+
+
+def set_exp_table(x=None, y=None) -> None:
+    """Install the device's exponential values y = exp(x) (None removes them)."""
+    lib = load()
+    if x is None:
+        lib.orc_set_exp_table(0, None, None)
+        return
+    x = _c(x, np.float32)
+    y = _c(y, np.float32)
+    assert x.shape == y.shape
+    lib.orc_set_exp_table(len(x), _p(x), _p(y))
+
+
+def exp_table_misses() -> int:
+    return int(load().orc_exp_table_misses())

@@ -5,8 +5,11 @@
 #                   the Z-shape pipeline of the reference's grotor_ggr build)
 #   evaluator    -- the reference's scoring program (resources/evaluator.cpp)
 #   POWV9.dat, POST9.dat -- FLUTE lookup tables the reference reads at run time
-# Usage: make -C oracle -f ref.mk [REF=/path/to/GRotor]
-REF ?= /root/reference
+# Usage: make -C oracle -f ref.mk REF=/path/to/GRotor
+# (REF has no default: the caller names the reference checkout.)
+ifeq ($(REF),)
+$(error REF=<path to the GRotor sources> is required)
+endif
 NVCC ?= nvcc
 HOSTCXX ?= /usr/bin/g++
 OUT := _ref

@@ -18,7 +18,7 @@
 //   batch <dir> <limit> <sparsity>  CPU: time generate_batches_rsmt on a dumped
 //                                   geometry (X, Y, order, points, segments).
 //   flt   <cap> <net> <dir> <lut>   GPU: the reference default pipeline up to and
-//                                   through its FLT stage (pipeline.hpp:263-305):
+//                                   through its FLT stage (pipeline.hpp:86-137):
 //                                   L-shape, congestion view, rip-up, the host FLT
 //                                   DAG builder; dumps the DAGs, the FLT batching
 //                                   geometry and batches and the state before the
@@ -172,7 +172,7 @@ int run_route(const std::string& cap, const std::string& net, const std::string&
         cudb::RouterState state;
         state.batch_sparsity_override = 1;
         state.report_score = false;
-        // pipeline.hpp:247-276, stage one only.
+        // pipeline.hpp:36-67, stage one only.
         cudb::build_cuda_database(state);
         graph::initialize_incremental_cost(state);
         auto& view = state.device;
@@ -202,7 +202,7 @@ int run_route(const std::string& cap, const std::string& net, const std::string&
         dump(dir, "ref_presum", presum);
         std::vector<double> st{stats.total_wirelength, double(stats.total_via_count)};
         dump(dir, "ref_stats", st);
-        graph::finish_nets(state, all);  // pipeline.hpp:283-291
+        graph::finish_nets(state, all);  // pipeline.hpp:71-77
         auto records = graph::collect_output_nets(std::move(nets2output));
         nets2output = {};
         graph::output_nets(state, std::move(records));
@@ -312,7 +312,7 @@ int run_flt(const std::string& cap, const std::string& net, const std::string& d
         dump(dir, tag + "_stats", st);
     };
     dump_state("flt_before");
-    // pipeline.hpp:263-285: mode, congestion view, rip-up, phase-two offsets.
+    // pipeline.hpp:86-106: mode, congestion view, rip-up, phase-two offsets.
     if (state.nets.size() > 5000000) mode = 1;
     if (state.nets.size() > 20000000) mode = 2;
     graph::extract_congestionView<<<BLOCK_NUM(view.X * view.Y), THREAD_NUM>>>(view);
@@ -570,7 +570,7 @@ int run_write(const std::string& cap, const std::string& net, const std::string&
     for (int i = 0; i < int(db::nets.size()); ++i)
         if (db::nets[i].pins.size() == 1) nets2output.push(i);
     // Lshape_route leaves nets2route in plan order and finish_nets publishes in
-    // that order (lshape.cuh:70-77, pipeline.hpp:286): use the plan if given.
+    // that order (lshape.cuh:70-77, pipeline.hpp:77): use the plan if given.
     std::vector<int> all(state.nets.size());
     std::iota(all.begin(), all.end(), 0);
     if (std::filesystem::exists(dir + "/ids.i32")) all = load<int>(dir + "/ids.i32");

@@ -179,3 +179,32 @@ def route_geometry(r: np.ndarray, X: int, Y: int):
         else:
             edges += [l * XY + x * Y + ya for x in range(min(xa, xb), max(xa, xb))]
     return sorted(edges), sorted(vias)
+
+
+class device_exp_table:
+    """Context manager: install in the oracle the device's own values of the
+    cost model's exponential (grb_cost_exp on cuda:0) for every argument the
+    cost model can produce on `og` up to `max_demand_half`, so the oracle's
+    cost tables are bit-identical to the device's; removed on exit.  `misses`
+    is the number of exponentials the oracle evaluated outside the table."""
+
+    def __init__(self, og, max_demand_half):
+        self.og, self.hmax, self.misses = og, int(max_demand_half), None
+
+    def __enter__(self):
+        import ctypes as C
+
+        import oracle
+        from grotor_b200 import _abi
+        x = oracle.exp_args(self.og, self.hmax)
+        y = np.empty_like(x)
+        rc = _abi.load().grb_cost_exp(0, x.ctypes.data_as(C.c_void_p), len(x), y.ctypes.data_as(C.c_void_p))
+        assert rc == 0, f"grb_cost_exp failed ({rc})"
+        oracle.set_exp_table(x, y)
+        return self
+
+    def __exit__(self, *exc):
+        import oracle
+        self.misses = oracle.exp_table_misses()
+        oracle.set_exp_table()
+        return False

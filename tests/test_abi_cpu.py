@@ -9,9 +9,9 @@ import numpy as np
 from helpers import ROOT
 
 
-def _declared():
+def _declared(headers):
     names = set()
-    for h in os.listdir(os.path.join(ROOT, "include")):
+    for h in headers:
         text = open(os.path.join(ROOT, "include", h)).read()
         text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
         names |= set(re.findall(r"\b(grb_[a-z_0-9]+)\s*\(", text))
@@ -19,14 +19,26 @@ def _declared():
 
 
 def test_every_declared_symbol_is_exported():
+    """grb.h and grb_prof.h are the routing library's ABI (libgrb.so),
+    grb_synth.h the workload generator's (libgrb_synth.so)."""
     from grotor_b200 import _abi
+    headers = sorted(os.listdir(os.path.join(ROOT, "include")))
+    assert headers == ["grb.h", "grb_prof.h", "grb_synth.h"]
     lib = _abi.load()
-    declared = _declared()
+    declared = _declared(["grb.h", "grb_prof.h"])
     assert len(declared) > 20
     missing = [n for n in sorted(declared) if not hasattr(lib, n)]
     assert not missing, missing
     # and the Python mirror binds every one of them
     assert declared <= set(_abi.SIGNATURES), sorted(declared - set(_abi.SIGNATURES))
+    synth = _abi.load_synth()
+    declared_synth = _declared(["grb_synth.h"])
+    assert len(declared_synth) >= 10
+    missing = [n for n in sorted(declared_synth) if not hasattr(synth, n)]
+    assert not missing, missing
+    assert declared_synth <= set(_abi.SYNTH_SIGNATURES)
+    # the generator is not part of the routing library
+    assert not any(hasattr(lib, n) for n in declared_synth)
 
 
 def test_invalid_arguments_return_codes():

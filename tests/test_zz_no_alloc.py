@@ -46,6 +46,38 @@ def test_matches_allocating_entry_point_twice(routed):
     assert flagged > 0  # the comparison covered flagged nets
 
 
+@pytest.fixture(scope="module")
+def routed_at_limit():
+    """A design of exactly 4,194,304 cells (4 routing layers of 1024 x 1024),
+    the largest the fixed array takes, with close to a million nets and low
+    capacities: the per-net flags then start right after the last cell word
+    the classification uses."""
+    from grotor_b200 import Router
+    from grotor_b200.synth import SynthParams, Design
+    d = Design(SynthParams(1024, 1024, 5, 880000, 1, 3, seed=78))
+    assert d.grid.cells == 4 << 20 and 800000 < d.n_subnets <= 1 << 20
+    r = Router(d.grid)
+    r.upload_nets(d.nets)
+    r.generate_batches_rsmt(d.order, 1000000)
+    r.lshape_route("persistent")
+    yield r
+    r.close()
+
+
+def test_matches_allocating_entry_point_at_the_size_limit(routed_at_limit):
+    from grotor_b200 import _abi
+    lib = _abi.load()
+    r = routed_at_limit
+    for thr in (0, -1):
+        want = r.ripup(thr)
+        assert want.sum() > 0
+        for _ in range(2):
+            got = np.zeros_like(want)
+            rc = lib.grb_ripup_classify_noalloc(r._ctx, thr, got.ctypes.data_as(C.c_void_p))
+            assert rc == 0, lib.grb_last_error(r._ctx).decode()
+            np.testing.assert_array_equal(got, want)
+
+
 def test_refuses_designs_beyond_its_limit():
     from grotor_b200 import GrbError, GridArrays, Router
     from grotor_b200._abi import GRB_ELIMIT
