@@ -18,6 +18,7 @@ SYNTH_PATH = os.path.join(_HERE, "libgrb_synth.so")
 
 GRB_OK, GRB_EINVAL, GRB_ENOMEM, GRB_ECUDA, GRB_ETIMEDOUT, GRB_ELIMIT = range(6)
 MODE_PLAIN, MODE_GRAPH, MODE_PERSISTENT = 0, 1, 2
+GRB_TAIL_RIPUP, GRB_TAIL_VIEW = 1, 2
 ERROR_NAMES = {1: "GRB_EINVAL", 2: "GRB_ENOMEM", 3: "GRB_ECUDA", 4: "GRB_ETIMEDOUT", 5: "GRB_ELIMIT"}
 
 P = C.c_void_p
@@ -97,12 +98,15 @@ SIGNATURES = {
     "grb_zshape_stage": (C.c_int, [P, C.c_int32, C.POINTER(GrbStats)]),
     "grb_congestion_view": (C.c_int, [P, P, P, P]),
     "grb_cost_exp": (C.c_int, [C.c_int32, P, C.c_int32, P]),
+    "grb_set_stage_tail": (C.c_int, [P, C.c_int32, C.c_int32]),
+    "grb_read_stage_tail": (C.c_int, [P, P, P, P, P]),
     "grb_read_tables": (C.c_int, [P, P, P, P, P, P]),
     "grb_read_routes": (C.c_int, [P, P]),
     "grb_get_stats": (C.c_int, [P, C.POINTER(GrbStats)]),
     "grb_set_stats": (C.c_int, [P, C.c_double, C.c_int64]),
     "grb_sync": (C.c_int, [P]),
     "grb_kernel_launches": (C.c_int64, [P]),
+    "grb_set_wait_limit": (C.c_int, [P, C.c_double]),
     "grb_set_profiling": (C.c_int, [P, C.c_int32]),
     "grb_phase_times": (C.c_int, [P, P, C.c_int32, C.c_int32]),
     # grb_prof.h

@@ -57,9 +57,11 @@ __device__ __forceinline__ void commit_net_wires(const Tables& T, const Plan& P,
     if (lane == 0 && length != 0.0) atomicAdd(T.wirelength, length * K);
 }
 
-__device__ __forceinline__ void add_via_demand(const Tables& T, int c, int half) {
+// Via demand on cell c, position pos of track `track` of layer l.
+__device__ __forceinline__ void add_via_demand(const Tables& T, int c, int half, int l, int track, int pos, int len,
+                                               int stride) {
     red_add(T.demand + c, half);
-    mark_edge_dirty(T, c);
+    mark_edge_dirty(T, c, l, track, pos, len, stride);
 }
 
 // Demand of the via stack at (x, y) (ra = x*Y + y) between layers low and
@@ -77,12 +79,12 @@ __device__ __forceinline__ void via_stack_demand(const Tables& T, int ra, int x,
         if (layer >= high || ts[u] >= stamp) continue;
         const int c = layer * T.XY + ra;
         const bool ay = along_y(T, layer);
-        const int pos = ay ? y : x, len = ay ? T.Y : T.X, stride = ay ? 1 : T.Y;
-        if (!pos) add_via_demand(T, c, 2 * K);
-        else if (pos == len - 1) add_via_demand(T, c - stride, 2 * K);
+        const int pos = ay ? y : x, len = ay ? T.Y : T.X, stride = ay ? 1 : T.Y, track = ay ? x : y;
+        if (!pos) add_via_demand(T, c, 2 * K, layer, track, pos, len, stride);
+        else if (pos == len - 1) add_via_demand(T, c - stride, 2 * K, layer, track, pos - 1, len, stride);
         else {
-            add_via_demand(T, c - stride, K);
-            add_via_demand(T, c, K);
+            add_via_demand(T, c - stride, K, layer, track, pos - 1, len, stride);
+            add_via_demand(T, c, K, layer, track, pos, len, stride);
         }
     }
 }

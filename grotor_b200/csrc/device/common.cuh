@@ -14,6 +14,7 @@ namespace grb {
 constexpr double kInf = 1e22;   // router_state.hpp:271
 constexpr int kMaxLayers = 10;  // lshape_warp.cuh:115 asserts L <= 10
 constexpr int kTrackGroup = 32; // tracks per prefix group (one per lane)
+constexpr int kNoCapRow = 255;  // cap_id of a cell whose capacity has no table row
 
 enum : int {
     kOk = 0, kEInval = 1, kENoMem = 2, kECuda = 3, kETimedOut = 4, kELimit = 5,
@@ -33,14 +34,24 @@ struct Tables {
     float* wcost;
     float* vcost;
     double* presum;
-    unsigned* dirty_wire;  // one bit per cell
-    unsigned* dirty_via;   // one bit per cell
+    unsigned* dirty_wire;  // one bit per cell: wire cost to recompute
+    unsigned* dirty_via;   // one bit per cell: via cost to recompute
     int words;             // bitmap words
     int int_wire;          // 1: wire costs clamped to [0, 1e7] and truncated (GGR build)
-    // Prefix groups: kTrackGroup adjacent tracks of one layer.
+    // Cost-term table: row (l, k) holds, for demands h < of_dmax half-units,
+    // the terms of a cell of capacity value k on layer l (cost.cuh
+    // cell_terms_at); one row per layer and distinct capacity value (cap_id[c]
+    // = k of cell c, kNoCapRow where the design has too many values).
+    const unsigned char* cap_id;
+    const double2* of_table;
+    int of_rows;           // capacity values (rows per layer)
+    int of_stride;         // entries per row
+    int of_dmax;           // demands below this come from the table
+    // Prefix groups: kTrackGroup adjacent tracks of one layer.  A group's
+    // prefix is rebuilt from the first 32-position chunk where a wire cost of
+    // one of its tracks changed.
     int group_base[kMaxLayers + 1];
-    unsigned* group_flag;  // [n_groups], nonzero = some track of the group changed
-    int* group_first;      // [n_groups] first 32-position chunk whose wire cost changed (INT_MAX: none)
+    int* group_first;      // [n_groups] first chunk with a demand change (INT_MAX: none)
     int* first_list;       // [n_groups] group_first of each listed dirty group
     int n_groups;
     int* group_list;       // [n_groups] dirty groups of the current refresh
@@ -92,8 +103,6 @@ __device__ __forceinline__ void set_error(const Tables& T, int code, int info) {
     if (atomicCAS(T.error, 0, code) == 0) *T.error_info = info;
 }
 
-// Dirty marking uses fire-and-forget atomics (no return value): the refresh
-// finds the work by scanning the bitmaps, which are small (one bit per cell).
 // Fire-and-forget reductions: the result is never read, so the instruction
 // carries no return value and the issuing thread does not wait for L2.
 __device__ __forceinline__ void red_or(unsigned* p, unsigned v) {
@@ -102,33 +111,30 @@ __device__ __forceinline__ void red_or(unsigned* p, unsigned v) {
 __device__ __forceinline__ void red_add(int* p, int v) {
     asm volatile("red.relaxed.gpu.global.add.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
+__device__ __forceinline__ void red_min(int* p, int v) {
+    asm volatile("red.relaxed.gpu.global.min.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
 
 __device__ __forceinline__ void set_bits(unsigned* bits, int word, unsigned mask) {
     if (mask) red_or(bits + word, mask);
 }
 
-__device__ __forceinline__ void red_min(int* p, int v) {
-    asm volatile("red.relaxed.gpu.global.min.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
-}
-
-// A wire cost of track `track` at position `pos` changed: the group's prefix
-// must be rebuilt from that position's 32-position chunk on.
+// A wire cost of track `track` of layer l at position `pos` changed: the
+// group's prefix must be rebuilt from that position's 32-position chunk on.
 __device__ __forceinline__ void mark_group_dirty(const Tables& T, int l, int track, int pos) {
-    const int g = T.group_base[l] + track / kTrackGroup;
-    T.group_flag[g] = 1u;
-    red_min(T.group_first + g, pos >> 5);
+    red_min(T.group_first + T.group_base[l] + track / kTrackGroup, pos >> 5);
 }
 
-// A demand change on edge cell c invalidates its wire cost, its own via cost
-// and the via cost of the next cell along the track (fenwick.cuh:27-38).
-__device__ __forceinline__ void mark_edge_dirty(const Tables& T, int c) {
-    const int l = c / T.XY, rem = c - l * T.XY, x = rem / T.Y, y = rem - x * T.Y;
-    const bool ay = along_y(T, l);
-    const int pos = ay ? y : x, len = ay ? T.Y : T.X, stride = ay ? 1 : T.Y;
+// A demand change on edge cell c (position pos of track `track` of layer l,
+// track length len, stride along the track) invalidates its wire cost, its
+// own via cost and the via cost of the next cell along the track
+// (fenwick.cuh:27-38).
+__device__ __forceinline__ void mark_edge_dirty(const Tables& T, int c, int l, int track, int pos, int len,
+                                                int stride) {
     set_bits(T.dirty_wire, c >> 5, 1u << (c & 31));
     set_bits(T.dirty_via, c >> 5, 1u << (c & 31));
     if (pos + 1 < len) set_bits(T.dirty_via, (c + stride) >> 5, 1u << ((c + stride) & 31));
-    mark_group_dirty(T, l, ay ? x : y, pos);
+    mark_group_dirty(T, l, track, pos);
 }
 
 // Mark cells [first, last] of a bitmap with one atomic per word

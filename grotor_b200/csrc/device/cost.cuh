@@ -34,63 +34,95 @@ __device__ __forceinline__ double of_cost_scaled(double scale, float capacity, f
     return 0;
 }
 
-// Overflow-cost increment of adding `incre` to a cell with capacity cap and
-// demand dem_half half-units, on a layer with overflow weight sc.
-__device__ __forceinline__ double incremental_of_cost(double scale, float cap, int dem_half, double sc,
-                                                      double incre) {
+// Cost terms of one cell: the overflow increments of adding a whole unit
+// and half a unit of demand (incremental_of_cost with incre 1.0 and 0.5, in
+// its arithmetic; the exponential of the current demand is shared).
+__device__ __forceinline__ void cell_terms(const Tables& T, float cap, int dem_half, double sc, double& one,
+                                           double& half) {
     const float dem = static_cast<float>(dem_half) * 0.5f;
-    const float with = static_cast<float>(static_cast<double>(dem) + incre + 0.0);
-    const float without = static_cast<float>(static_cast<double>(dem) + 0.0);
-    return fmin(1e12, (of_cost_scaled(scale, cap, with) - of_cost_scaled(scale, cap, without)) * sc);
+    const float w1 = static_cast<float>(static_cast<double>(dem) + 1.0 + 0.0);
+    const float wh = static_cast<float>(static_cast<double>(dem) + 0.5 + 0.0);
+    const float w0 = static_cast<float>(static_cast<double>(dem) + 0.0);
+    const double o0 = of_cost_scaled(T.of_scale, cap, w0);
+    one = fmin(1e12, (of_cost_scaled(T.of_scale, cap, w1) - o0) * sc);
+    half = fmin(1e12, (of_cost_scaled(T.of_scale, cap, wh) - o0) * sc);
 }
 
-// What the costs of cell c depend on: its capacity and demand, those of the
-// previous cell along its track, its edge length and its layer's weight.
-struct CellInputs {
-    float cap0, cap1;
-    int dem0, dem1;
-    int pos, len, elen;
-    double sc;
-};
-
-__device__ __forceinline__ CellInputs load_cell(const Tables& T, int c) {
-    CellInputs in;
-    const int l = c / T.XY, rem = c - l * T.XY, x = rem / T.Y, y = rem - x * T.Y;
-    const bool ay = along_y(T, l);
-    const int stride = ay ? 1 : T.Y;
-    in.pos = ay ? y : x;
-    in.len = ay ? T.Y : T.X;
-    in.cap0 = T.capacity[c];
-    in.dem0 = T.demand[c];
-    in.cap1 = in.pos > 0 ? T.capacity[c - stride] : 0.f;
-    in.dem1 = in.pos > 0 ? T.demand[c - stride] : 0;
-    in.elen = in.pos < in.len - 1 ? (ay ? T.ylen[in.pos] : T.xlen[in.pos]) : 0;
-    in.sc = T.short_costs[l];
-    return in;
+// The terms the cost kernels use per cell: `wof`, the overflow increment of
+// a whole unit rounded to float (what the wire cost and the end-of-track via
+// cost start from) and `half`, the increment of half a unit (double, what an
+// interior via cost sums).
+__device__ __forceinline__ double2 terms_of(double one, double half) {
+    return make_double2(static_cast<double>(static_cast<float>(one)), half);
 }
 
-// update_single_wcost_ispd24 (full_update.cuh:34-51); the length term is the
-// fused multiply-add the compiler forms for `w += unit * len`.
-__device__ __forceinline__ float wire_cost_of(const Tables& T, const CellInputs& in) {
-    float w = static_cast<float>(incremental_of_cost(T.of_scale, in.cap0, in.dem0, in.sc, 1.0));
-    if (in.pos < in.len - 1)
-        w = static_cast<float>(fma(T.unit_wire, static_cast<double>(in.elen), static_cast<double>(w)));
+// Computed from capacity and demand (out of line: the table below covers
+// almost every cell, and the refresh's unrolled loops stay small).
+__device__ __noinline__ double2 cell_terms_computed(const Tables& T, int c, int dem_half, double sc) {
+    double one, half;
+    cell_terms(T, T.capacity[c], dem_half, sc, one, half);
+    return terms_of(one, half);
+}
+
+// The terms of cell c (capacity row cid, demand dem_half half-units) on a
+// layer of weight sc.  The demands the cost model evaluates are h/2, h/2 + 1/2
+// and h/2 + 1 (exactly (h+1)/2 and (h+2)/2 in float), so for a capacity with a
+// table row and a demand in range the terms are precomputed per (layer,
+// capacity, demand) by the same functions: the same bits.
+__device__ __forceinline__ double2 cell_terms_at(const Tables& T, int l, int c, unsigned cid, int dem_half,
+                                                 double sc) {
+    if (cid != kNoCapRow && dem_half >= 0 && dem_half < T.of_dmax)
+        return __ldg(T.of_table + (size_t(l) * T.of_rows + cid) * T.of_stride + dem_half);
+    return cell_terms_computed(T, c, dem_half, sc);
+}
+
+// update_single_wcost_ispd24 (full_update.cuh:34-51) from the cell's terms;
+// the length term is the fused multiply-add the compiler forms for
+// `w += unit * len`.  elen: the edge length (ignored at the track's end).
+__device__ __forceinline__ float wire_cost_of(const Tables& T, double wof, int pos, int len, int elen) {
+    float w = static_cast<float>(wof);
+    if (pos < len - 1) w = static_cast<float>(fma(T.unit_wire, static_cast<double>(elen), wof));
     // The GGR build keeps integer DP edges non-negative and below its sentinel
     // (full_update.cuh:47-50).
     if (T.int_wire) w = static_cast<float>(static_cast<long long>(fminf(fmaxf(w, 0.f), 1.e7f)));
     return w;
 }
 
-// update_single_vcost_ispd24 (full_update.cuh:58-83); cross points are zero
-// on a single GPU (preprocess.hpp:1757).
-__device__ __forceinline__ float via_cost_of(const Tables& T, const CellInputs& in) {
+// update_single_vcost_ispd24 (full_update.cuh:58-83) from the terms of the
+// cell and of the previous cell along its track; cross points are zero on a
+// single GPU (preprocess.hpp:1757).
+__device__ __forceinline__ float via_cost_of(const Tables& T, const double2& t, const double2& prev, int pos,
+                                             int len) {
     float v;
-    if (in.pos == 0) v = static_cast<float>(incremental_of_cost(T.of_scale, in.cap0, in.dem0, in.sc, 1.0));
-    else if (in.pos == in.len - 1) v = static_cast<float>(incremental_of_cost(T.of_scale, in.cap1, in.dem1, in.sc, 1.0));
-    else
-        v = static_cast<float>(incremental_of_cost(T.of_scale, in.cap0, in.dem0, in.sc, 0.5) +
-                               incremental_of_cost(T.of_scale, in.cap1, in.dem1, in.sc, 0.5));
+    if (pos == 0) v = static_cast<float>(t.x);
+    else if (pos == len - 1) v = static_cast<float>(prev.x);
+    else v = static_cast<float>(t.y + prev.y);
     return static_cast<float>(static_cast<double>(v) + T.unit_via);
+}
+
+// What the costs of cell c depend on: its own terms and those of the
+// previous cell along its track (capacity row and demand of each), its
+// position, the track length and the edge length.
+struct CellInputs {
+    unsigned cid0, cid1;
+    int dem0, dem1;
+    int l, pos, len, elen, stride;
+};
+
+__device__ __forceinline__ CellInputs load_cell(const Tables& T, int c) {
+    CellInputs in;
+    const int l = c / T.XY, rem = c - l * T.XY, x = rem / T.Y, y = rem - x * T.Y;
+    const bool ay = along_y(T, l);
+    in.l = l;
+    in.stride = ay ? 1 : T.Y;
+    in.pos = ay ? y : x;
+    in.len = ay ? T.Y : T.X;
+    in.cid0 = T.cap_id[c];
+    in.dem0 = T.demand[c];
+    in.cid1 = in.pos > 0 ? T.cap_id[c - in.stride] : 0u;
+    in.dem1 = in.pos > 0 ? T.demand[c - in.stride] : 0;
+    in.elen = in.pos < in.len - 1 ? (ay ? T.ylen[in.pos] : T.xlen[in.pos]) : 0;
+    return in;
 }
 
 // Position of the n-th (0-based) set bit of m, which has more than n set
@@ -110,13 +142,15 @@ __device__ __forceinline__ int nth_set_bit(unsigned m, int n) {
     return pos;
 }
 
-// Recompute every dirty cell.  A warp loads 32 bitmap words at a time, ranks
-// their dirty cells with a warp prefix sum and takes them kRounds * 32
-// at a time, kRounds cells per lane whose inputs are all loaded before any
-// cost is computed or stored (kRounds trades registers for loads in flight).  Wire costs where the wire bit is set, via
-// costs where the via bit is set (a wire-dirty cell is always via-dirty).
-// Both words are cleared.  `warp`/`nwarps` number the calling warps across
-// the launch.
+// update_dirty_costs / update_dirty_wire_cost (incremental_update.cuh:44-96):
+// recompute every dirty cell.  A warp loads 32 bitmap words at a time, ranks
+// their dirty cells with a warp prefix sum and takes them kRounds * 32 at a
+// time, kRounds cells per lane whose inputs are all loaded before any cost is
+// computed or stored (kRounds trades registers for loads in flight).  Wire
+// costs where the wire bit is set, via costs where the via bit is set (a
+// wire-dirty cell is always via-dirty); the terms come from the cost-term
+// table.  Both words are cleared.  `warp`/`nwarps` number the calling warps
+// across the launch.
 template <int kRounds>
 __device__ __forceinline__ void refresh_dirty_cells(const Tables& T, int warp, int nwarps, int lane) {
     // The next window's bitmap words are loaded while this one is processed.
@@ -172,8 +206,14 @@ __device__ __forceinline__ void refresh_dirty_cells(const Tables& T, int warp, i
 #pragma unroll
             for (int q = 0; q < kRounds; ++q) {
                 if (cell[q] < 0) continue;
-                if (wire[q]) T.wcost[cell[q]] = wire_cost_of(T, in[q]);
-                T.vcost[cell[q]] = via_cost_of(T, in[q]);
+                const int c = cell[q];
+                const double sc = T.short_costs[in[q].l];
+                const double2 t0 = cell_terms_at(T, in[q].l, c, in[q].cid0, in[q].dem0, sc);
+                const double2 t1 = in[q].pos > 0
+                                       ? cell_terms_at(T, in[q].l, c - in[q].stride, in[q].cid1, in[q].dem1, sc)
+                                       : make_double2(0.0, 0.0);
+                if (wire[q]) T.wcost[c] = wire_cost_of(T, t0.x, in[q].pos, in[q].len, in[q].elen);
+                T.vcost[c] = via_cost_of(T, t0, t1, in[q].pos, in[q].len);
             }
         }
         if (vb) T.dirty_via[w] = 0u;
@@ -266,12 +306,10 @@ __device__ __forceinline__ void load_chunk(const Tables& T, const GroupGeom& G, 
     }
 }
 
-// Pass 1 for work item (g, c): the chunk total of every lane's track.
-// `xs`: the warp's scratch (prefix_xpose_bytes), or null.
-__device__ __forceinline__ void prefix_pass1(const Tables& T, int g, int c, int lane, void* xs) {
-    const GroupGeom G = group_geom(T, g, lane);
-    float x[kChunkPos];
-    load_chunk(T, G, c, x, lane, static_cast<float*>(xs));
+// The pairwise total of a chunk's prefix inputs: the reference association
+// over the chunk (k = 31 has all five low bits set, so the final accumulator
+// is the total of the aligned 32-block).
+__device__ __forceinline__ double chunk_total(const float (&x)[kChunkPos]) {
     double tot[6];
     double acc = 0;
 #pragma unroll
@@ -291,8 +329,17 @@ __device__ __forceinline__ void prefix_pass1(const Tables& T, int g, int c, int 
 #pragma unroll
         for (int d = 0; d < 6; ++d) if (d <= t) tot[d] = fresh[d];
     }
-    // k = 31 has all five low bits set: acc is the pairwise total of the chunk.
-    T.ptree[(size_t(g) * T.tree_stride + c) * 32 + lane] = acc;
+    return acc;
+}
+
+// Pass 1 for work item (g, c): the chunk total of every lane's track (wire
+// costs must be current).  `xs`: the warp's scratch (prefix_xpose_bytes), or
+// null.
+__device__ __forceinline__ void prefix_pass1(const Tables& T, int g, int c, int lane, void* xs) {
+    const GroupGeom G = group_geom(T, g, lane);
+    float x[kChunkPos];
+    load_chunk(T, G, c, x, lane, static_cast<float*>(xs));
+    T.ptree[(size_t(g) * T.tree_stride + c) * 32 + lane] = chunk_total(x);
 }
 
 // Tree of aligned block totals for group g (one CTA, `tree` = shared memory
@@ -318,25 +365,15 @@ __device__ __forceinline__ void prefix_tree(const Tables& T, int g, double* tree
     }
 }
 
-// Pass 2 for work item (g, c): final prefix values of the chunk.  Along-y
-// tracks with scratch `xs`: the values go through shared memory and are
-// written run by run (32 consecutive doubles per instruction).
-__device__ __forceinline__ void prefix_pass2(const Tables& T, int g, int c, int lane, void* xs) {
-    const GroupGeom G = group_geom(T, g, lane);
-    const double* gt = T.ptree + size_t(g) * T.tree_stride * 32;
-    double add[8];
-    {
-        int off = 0, cnt = G.nch;
-#pragma unroll
-        for (int e = 0; e < 8; ++e) {
-            add[e] = 0.0;
-            if (cnt >= 1 && ((c >> e) & 1)) add[e] = gt[(off + (c >> e) - 1) * 32 + lane];
-            off += cnt;
-            cnt >>= 1;
-        }
-    }
-    float x[kChunkPos];
-    load_chunk(T, G, c, x, lane, static_cast<float*>(xs));
+// Final prefix values of chunk c from its prefix inputs x and the totals
+// add[e] of the aligned blocks of 2^e chunks below it (for the set bits e of
+// c; 0 elsewhere): per element, lowest bit first, the blocks inside the chunk
+// then the chunk-level blocks.  Along-y tracks with scratch `xs`: the values
+// go through shared memory and are written run by run (32 consecutive
+// doubles per instruction).
+__device__ __forceinline__ void chunk_prefix_store(const Tables& T, const GroupGeom& G, int c,
+                                                   const float (&x)[kChunkPos], const double (&add)[8], int lane,
+                                                   void* xs) {
     const bool rows = xs && G.stride == 1;
     double* ds = static_cast<double*>(xs);
     double tot[6];
@@ -386,18 +423,40 @@ __device__ __forceinline__ void prefix_pass2(const Tables& T, int g, int c, int 
     }
 }
 
-// Move the dirty-group flags into group_list and clear them (one CTA).  The
-// commits that follow mark the flags again for the next refresh.
+// Pass 2 for work item (g, c): final prefix values of the chunk, its inputs
+// re-read from the wire costs and the chunk-level totals from the tree.
+__device__ __forceinline__ void prefix_pass2(const Tables& T, int g, int c, int lane, void* xs) {
+    const GroupGeom G = group_geom(T, g, lane);
+    const double* gt = T.ptree + size_t(g) * T.tree_stride * 32;
+    double add[8];
+    {
+        int off = 0, cnt = G.nch;
+#pragma unroll
+        for (int e = 0; e < 8; ++e) {
+            add[e] = 0.0;
+            if (cnt >= 1 && ((c >> e) & 1)) add[e] = gt[(off + (c >> e) - 1) * 32 + lane];
+            off += cnt;
+            cnt >>= 1;
+        }
+    }
+    float x[kChunkPos];
+    load_chunk(T, G, c, x, lane, static_cast<float*>(xs));
+    chunk_prefix_store(T, G, c, x, add, lane, xs);
+}
+
+// Move the dirty groups (group_first below INT_MAX) into group_list and mark
+// them clean (one CTA).  The commits that follow mark them again for the next
+// refresh.
 __device__ __forceinline__ void collect_dirty_groups(const Tables& T) {
     __shared__ int count;
     if (threadIdx.x == 0) count = 0;
     __syncthreads();
     for (int g = threadIdx.x; g < T.n_groups; g += blockDim.x) {
-        if (T.group_flag[g]) {
+        const int first = T.group_first[g];
+        if (first != 0x7fffffff) {
             const int k = atomicAdd(&count, 1);
             T.group_list[k] = g;
-            T.first_list[k] = T.group_first[g];
-            T.group_flag[g] = 0u;
+            T.first_list[k] = first;
             T.group_first[g] = 0x7fffffff;
         }
     }

@@ -34,11 +34,13 @@ struct Arena {
     int* range;            // [nmax] chosen range lo*L+hi
     int* xy;               // [nmax] node coordinate x << 16 | y (grids are at most 8192 wide)
     int* lay;              // [nmax] node layer (L: Steiner point)
-    double* cur;           // [L]
-    double* diag;          // [L]
-    double* mcp;           // [TT]
-    int* cur_from;         // [L]
-    int* pdiag;            // [L]
+    int* dep;              // [nmax] node depth (root 0)
+    // Per-lane scratch of a level pass: lane = slot * L + layer for up to
+    // 32 / L nodes at once.
+    double* cur;           // [32] best range through each layer (of the slot's node)
+    double* diag;          // [32] best parent-layer cost
+    int* cur_from;         // [32]
+    int* pdiag;            // [32]
 };
 
 __host__ __device__ __forceinline__ size_t arena_bytes(int L, int nmax) {
@@ -46,10 +48,10 @@ __host__ __device__ __forceinline__ size_t arena_bytes(int L, int nmax) {
     size_t b = 0;
     b += nmax * TT * 8 + 2 * size_t(nmax) * L * 8 + 3 * size_t(nmax) * L * 4;
     b = (b + 7) & ~size_t(7);
-    b += 2 * L * 8 + TT * 8;
+    b += 2 * 32 * 8;
     b += nmax * TT * 2;
     b = (b + 7) & ~size_t(7);
-    b += nmax * 4 + 2 * L * 4 + 2 * size_t(nmax) * 4;
+    b += nmax * 4 + 2 * 32 * 4 + 3 * size_t(nmax) * 4;
     return (b + 15) & ~size_t(15);
 }
 
@@ -64,16 +66,16 @@ __device__ __forceinline__ Arena carve_arena(char* base, int L, int nmax) {
     A.vB = reinterpret_cast<float*>(p); p += size_t(nmax) * L * 4;
     A.vN = reinterpret_cast<float*>(p); p += size_t(nmax) * L * 4;
     p = reinterpret_cast<char*>((reinterpret_cast<uintptr_t>(p) + 7) & ~uintptr_t(7));
-    A.cur = reinterpret_cast<double*>(p); p += L * 8;
-    A.diag = reinterpret_cast<double*>(p); p += L * 8;
-    A.mcp = reinterpret_cast<double*>(p); p += TT * 8;
+    A.cur = reinterpret_cast<double*>(p); p += 32 * 8;
+    A.diag = reinterpret_cast<double*>(p); p += 32 * 8;
     A.from = reinterpret_cast<unsigned short*>(p); p += size_t(nmax) * TT * 2;
     p = reinterpret_cast<char*>((reinterpret_cast<uintptr_t>(p) + 7) & ~uintptr_t(7));
     A.range = reinterpret_cast<int*>(p); p += nmax * 4;
-    A.cur_from = reinterpret_cast<int*>(p); p += L * 4;
-    A.pdiag = reinterpret_cast<int*>(p); p += L * 4;
+    A.cur_from = reinterpret_cast<int*>(p); p += 32 * 4;
+    A.pdiag = reinterpret_cast<int*>(p); p += 32 * 4;
     A.xy = reinterpret_cast<int*>(p); p += nmax * 4;
-    A.lay = reinterpret_cast<int*>(p);
+    A.lay = reinterpret_cast<int*>(p); p += nmax * 4;
+    A.dep = reinterpret_cast<int*>(p);
     return A;
 }
 
@@ -93,11 +95,17 @@ __device__ void lshape_net(const Tables& T, const Plan& P, int id, int stamp, co
 
     // 0. Node coordinates, once per net (the divisions by the runtime grid
     // sizes are not repeated per layer and step).
+    int dmax = 0;
     for (int q = lane; q < N; q += 32) {
         const int node = nd[q], l = node / XY, r = node - l * XY, x = r / Y;
         A.xy[q] = (x << 16) | (r - x * Y);
         A.lay[q] = l;
+        int d = 0;
+        for (int v = q; v > 0; v = par[v]) ++d;  // parents precede children
+        A.dep[q] = d;
+        dmax = max(dmax, d);
     }
+    for (int s = 16; s; s >>= 1) dmax = max(dmax, __shfl_xor_sync(0xffffffffu, dmax, s));
     __syncwarp();
     // 1. Gather every cost the DP reads.  Each lane takes two (node, layer)
     // items per pass and issues all their loads before any arena store.
@@ -157,83 +165,130 @@ __device__ void lshape_net(const Tables& T, const Plan& P, int id, int stamp, co
         }
     }
     __syncwarp();
-    // 3. Children in descending node order (lshape_thread.cuh:51-115).
-    for (int i = N - 1; i >= 1; --i) {
-        const int p = par[i];
-        const double* di = A.dist + i * TT;
-        if (lane < L) {
-            const int l = lane;
-            double best = kInf;
-            int bf = 0;
-            for (int lo = 0; lo <= l; ++lo)
-                for (int hi = l; hi < L; ++hi) {
-                    const double v = di[tri(L, lo, hi)];
-                    if (v < best) { best = v; bf = lo * L + hi; }
+    // 3. Children into parents (lshape_thread.cuh:51-115), one depth at a
+    // time from the deepest: the nodes of a depth have complete tables, so
+    // up to 32 / L of them are processed at once (lane = slot * L + layer);
+    // then every node of the depth, in descending node order, adds its table
+    // into its parent.  A parent receives its children (all one depth below
+    // it) in descending order, exactly the sequential loop's additions.
+    const int S = max(1, 32 / L);
+    const int slot = lane / L, sl = lane - slot * L;
+    for (int d = dmax; d >= 1; --d) {
+        for (int base = 0; base < N; base += 32) {
+            const int q = base + lane;
+            unsigned at = __ballot_sync(0xffffffffu, q < N && A.dep[q] == d);
+            while (at) {
+                // The next S nodes of this depth in this window.
+                int mine = -1;
+                {
+                    unsigned m = at;
+                    for (int k = 0; k < S && m; ++k) {
+                        const int b = __ffs(m) - 1;
+                        m &= m - 1;
+                        if (k == slot) mine = base + b;
+                    }
+                    at = m;
                 }
-            A.cur[l] = best;
-            A.cur_from[l] = bf;
-        }
-        __syncwarp();
-        if (lane < L) {
-            const int pl = lane;
-            const int x = A.xy[i] >> 16, y = A.xy[i] & 0xffff;
-            const int px = A.xy[p] >> 16, py = A.xy[p] & 0xffff;
-            double best = kInf;
-            int pb = 0;
-            if (x == px || y == py) {
-                const bool valid = along_y(T, pl) ? (x == px) : (y == py);
-                if (valid) {
-                    best = A.cur[pl] + A.w1[i * L + pl];
-                    pb = A.cur_from[pl] * L * L + pl * L + pl;
+                const bool act = slot < S && mine >= 0;
+                const int i = mine;
+                if (act) {
+                    const double* di = A.dist + i * TT;
+                    const int l = sl;
+                    double best = kInf;
+                    int bf = 0;
+                    for (int lo = 0; lo <= l; ++lo)
+                        for (int hi = l; hi < L; ++hi) {
+                            const double v = di[tri(L, lo, hi)];
+                            if (v < best) { best = v; bf = lo * L + hi; }
+                        }
+                    A.cur[lane] = best;
+                    A.cur_from[lane] = bf;
                 }
-            } else {
-                for (int cl = (pl & 1) ^ 1; cl < L; cl += 2) {
-                    const double cost = A.cur[cl] + A.w1[i * L + cl];
-                    double cost2 = 0;
-                    const float* v = along_y(T, cl) ? A.vA + i * L : A.vB + i * L;
-                    for (int l = min(cl, pl) + 1; l < max(cl, pl); ++l) cost2 += static_cast<double>(v[l]);
-                    cost2 += A.w2[i * L + pl];
-                    if (cost + cost2 < best) {
-                        best = cost + cost2;
-                        pb = A.cur_from[cl] * L * L + cl * L + pl;
+                __syncwarp();
+                if (act) {
+                    const int pl = sl, p = par[i], s0 = slot * L;
+                    const int x = A.xy[i] >> 16, y = A.xy[i] & 0xffff;
+                    const int px = A.xy[p] >> 16, py = A.xy[p] & 0xffff;
+                    double best = kInf;
+                    int pb = 0;
+                    if (x == px || y == py) {
+                        const bool valid = along_y(T, pl) ? (x == px) : (y == py);
+                        if (valid) {
+                            best = A.cur[s0 + pl] + A.w1[i * L + pl];
+                            pb = A.cur_from[s0 + pl] * L * L + pl * L + pl;
+                        }
+                    } else {
+                        for (int cl = (pl & 1) ^ 1; cl < L; cl += 2) {
+                            const double cost = A.cur[s0 + cl] + A.w1[i * L + cl];
+                            double cost2 = 0;
+                            const float* v = along_y(T, cl) ? A.vA + i * L : A.vB + i * L;
+                            for (int l = min(cl, pl) + 1; l < max(cl, pl); ++l) cost2 += static_cast<double>(v[l]);
+                            cost2 += A.w2[i * L + pl];
+                            if (cost + cost2 < best) {
+                                best = cost + cost2;
+                                pb = A.cur_from[s0 + cl] * L * L + cl * L + pl;
+                            }
+                        }
+                    }
+                    A.diag[lane] = best;
+                    A.pdiag[lane] = pb;
+                }
+                __syncwarp();
+                if (act) {
+                    // The node's contribution to its parent replaces its own
+                    // table (read above, not needed again).
+                    const int lo = sl, s0 = slot * L;
+                    double c = A.diag[s0 + lo];
+                    int path = A.pdiag[s0 + lo];
+                    for (int hi = lo; hi < L; ++hi) {
+                        if (hi > lo && !(c <= A.diag[s0 + hi])) { c = A.diag[s0 + hi]; path = A.pdiag[s0 + hi]; }
+                        const int t = tri(L, lo, hi);
+                        A.dist[i * TT + t] = c;
+                        A.from[i * TT + t] = static_cast<unsigned short>(path);
                     }
                 }
-            }
-            A.diag[pl] = best;
-            A.pdiag[pl] = pb;
-        }
-        __syncwarp();
-        if (lane < L) {
-            const int lo = lane;
-            double c = A.diag[lo];
-            int path = A.pdiag[lo];
-            for (int hi = lo; hi < L; ++hi) {
-                if (hi > lo && !(c <= A.diag[hi])) { c = A.diag[hi]; path = A.pdiag[hi]; }
-                const int t = tri(L, lo, hi);
-                A.mcp[t] = c;
-                A.from[i * TT + t] = static_cast<unsigned short>(path);
+                __syncwarp();
             }
         }
-        __syncwarp();
-        for (int t = lane; t < TT; t += 32) A.dist[p * TT + t] += A.mcp[t];
-        __syncwarp();
+        for (int i = N - 1; i >= 1; --i) {
+            if (A.dep[i] != d) continue;
+            const int p = par[i];
+            for (int t = lane; t < TT; t += 32) A.dist[p * TT + t] += A.dist[i * TT + t];
+            __syncwarp();
+        }
     }
-    // 4. Root range and traceback (lshape_thread.cuh:117-127).
-    if (lane == 0) {
-        int choice = 0, best_t = 0;
-        for (int lo = 0; lo < L; ++lo)
-            for (int hi = lo; hi < L; ++hi) {
-                const int t = tri(L, lo, hi);
-                if (A.dist[t] < A.dist[best_t]) { best_t = t; choice = lo * L + hi; }
-            }
-        A.range[0] = choice;
-        if (!(A.dist[best_t] < kInf)) set_error(T, kEInval, id);
-        for (int i = 1; i < N; ++i) {
-            const int pr = A.range[par[i]];
-            A.range[i] = A.from[i * TT + tri(L, pr / L, pr % L)] / (L * L);
+    // 4. Root range (lshape_thread.cuh:117-120): the first minimum in loop
+    // order (lo, then hi), i.e. the smallest triangular index among equal
+    // values -- a warp argmin; then the traceback one depth at a time.
+    {
+        double bv = __longlong_as_double(0x7ff0000000000000ll);  // +infinity: every finite entry is below it
+        int bt = 1 << 30;
+        for (int t = lane; t < TT; t += 32) {
+            const double v = A.dist[t];
+            if (v < bv) { bv = v; bt = t; }
+        }
+        for (int s = 16; s; s >>= 1) {
+            const double ov = __shfl_xor_sync(0xffffffffu, bv, s);
+            const int ot = __shfl_xor_sync(0xffffffffu, bt, s);
+            if (ov < bv || (ov == bv && ot < bt)) { bv = ov; bt = ot; }
+        }
+        if (lane == 0) {
+            if (bt >= TT) bt = 0;  // no entry below infinity: the sequential loop keeps index 0
+            int lo = 0;
+            while (lo + 1 < L && tri(L, lo + 1, lo + 1) <= bt) ++lo;
+            A.range[0] = lo * L + (lo + bt - tri(L, lo, lo));
+            if (!(bv < kInf)) set_error(T, kEInval, id);
         }
     }
     __syncwarp();
+    for (int d = 1; d <= dmax; ++d) {
+        for (int i = lane; i < N; i += 32) {
+            if (i == 0 || A.dep[i] != d) continue;
+            const int pr = A.range[par[i]];
+            A.range[i] = A.from[i * TT + tri(L, pr / L, pr % L)] / (L * L);
+        }
+        __syncwarp();
+    }
     // 5. Segment emission in node order (lshape_warp.cuh:215-240).
     int* out = P.routes + P.route_off[id];
     const long long cap = P.route_off[id + 1] - P.route_off[id];

@@ -8,11 +8,13 @@
 #include <memory>
 #include <mutex>
 #include <string>
+#include <unordered_map>
 #include <vector>
 
 #include "../../include/grb.h"
 #include "device/batching.cuh"
 #include "device/commit.cuh"
+#include "device/congestion.cuh"
 #include "device/common.cuh"
 #include "device/cost.cuh"
 #include "device/flt.cuh"
@@ -31,7 +33,8 @@ constexpr int kRefreshThreads = 256;       // threads of a prefix-tree CTA
 constexpr int kPersistentThreads = 256;
 constexpr int kDpThreads = 128;
 constexpr unsigned long long kBarrierTimeoutNs = 20ull * 1000 * 1000 * 1000;
-constexpr int kPhaseSlots = 12;  // grb_phase_times entries
+constexpr int kPhaseSlots = 20;  // grb_phase_times entries
+constexpr int kNetTimeSlot = 12;  // per size bucket: summed net time [12..15], longest net [16..19]
 
 // update_dirty_costs (incremental_update.cuh:62-96): recompute dirty cells.
 __global__ void k_refresh_cells(Tables T) {
@@ -79,7 +82,7 @@ __global__ void k_mark_all_dirty(Tables T) {
         T.dirty_wire[i] = m;
         T.dirty_via[i] = m;
     }
-    if (i < T.n_groups) { T.group_flag[i] = 1u; T.group_first[i] = 0; }
+    if (i < T.n_groups) T.group_first[i] = 0;
 }
 
 __device__ __forceinline__ Arena warp_arena(char* smem, size_t arena_b, int warp, int L, int nmax) {
@@ -181,10 +184,10 @@ __global__ void k_commit_vias(Tables T, Plan P, int b, int stamp, int K) {
 }
 
 // refresh_cost (incremental_update.cuh:98-132) inside a persistent stage
-// kernel: dirty cells | prefix pass 1 | trees | pass 2, each phase ended by a
-// grid barrier.  `smem`: the block's dynamic shared memory (per-warp pass
-// scratch, or the tree of the group a block builds).  False when a barrier
-// gave up.
+// kernel: dirty cells (block 0 also lists the dirty groups) | prefix pass 1 |
+// trees | pass 2, each phase ended by a grid barrier.  `smem`: the block's
+// dynamic shared memory (per-warp pass scratch, or the tree of the group a
+// block builds).  False when a barrier gave up.
 __device__ __forceinline__ bool refresh_persistent(const Tables& T, GridSync& S, PhaseClock& clk, int gwarp,
                                                    int nwarps, int lane, char* smem) {
     void* xs = smem + (threadIdx.x >> 5) * prefix_xpose_bytes();
@@ -215,7 +218,7 @@ __device__ __forceinline__ bool refresh_persistent(const Tables& T, GridSync& S,
 // groups) -> prefix pass 1 -> prefix trees -> prefix pass 2 -> route and commit
 // wires -> commit vias, separated by bounded grid barriers.
 __global__ void __launch_bounds__(kPersistentThreads, 2) k_lshape_persistent(Tables T, Plan P, GridSync S,
-        int stamp0, int nmax, size_t arena_b, char* gscratch, size_t gslot, int* work, DpTune tune) {
+        int stamp0, int nmax, size_t arena_b, char* gscratch, size_t gslot, int* work, DpTune tune, StageTail tail) {
     extern __shared__ __align__(16) char smem[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int gwarp = warp * gridDim.x + blockIdx.x, nwarps = gridDim.x * (blockDim.x >> 5);
@@ -242,9 +245,15 @@ __global__ void __launch_bounds__(kPersistentThreads, 2) k_lshape_persistent(Tab
                 for (int q = blo + k; q < min(blo + k + g, bhi); ++q) {
                     const int id = P.bucket_ids[q];
                     const int N = P.node_off[id + 1] - P.node_off[id];
+                    const unsigned long long t0 = S.phase_ns && lane == 0 ? global_ns() : 0ull;
                     if (N <= nmax) lshape_net(T, P, id, stamp, A, lane, true);
                     else if (gscratch) lshape_net(T, P, id, stamp, carve_arena(gscratch + size_t(gwarp) * gslot, T.L, N), lane, true);
                     else if (lane == 0) set_error(T, kELimit, id);
+                    if (S.phase_ns && lane == 0) {  // profiling: warp time of every net, by size bucket
+                        const unsigned long long dt = global_ns() - t0;
+                        atomicAdd(S.phase_ns + kNetTimeSlot + bk, dt);
+                        atomicMax(S.phase_ns + kNetTimeSlot + kDpBuckets + bk, dt);
+                    }
                 }
             }
         }
@@ -255,6 +264,9 @@ __global__ void __launch_bounds__(kPersistentThreads, 2) k_lshape_persistent(Tab
         if (!grid_sync(S, T)) return;
         clk.mark(S, 6);
     }
+    // Rip-up classification and congestion view of the final demand, in the
+    // same launch (no host round trip between the stage and them).
+    if (tail.flags) stage_tail_persistent(T, P, tail, S);
 }
 
 // --- FLT stage kernels (flt.cuh) --------------------------------------------
@@ -863,84 +875,37 @@ __global__ void k_plan_scatter(BatchState B, const int* batch_off, int* ids) {
 }
 
 // --- rip-up classification and congestion view -----------------------------
+// Rip-up classification and congestion view (device/congestion.cuh).
 __global__ void k_mark_overflow(Tables T, int threshold, int* of_sum) {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= T.cells) return;
-    const int l = c / T.XY, rem = c - l * T.XY, x = rem / T.Y, y = rem - x * T.Y;
-    const bool edge = along_y(T, l) ? (y + 1 < T.Y) : (x + 1 < T.X);
-    of_sum[c] = (edge && T.capacity[c] + threshold <= static_cast<float>(T.demand[c]) * 0.5f) ? 1 : 0;
+    if (c < T.cells) overflow_mark(T, threshold, of_sum, c);
 }
-// Exclusive integer prefix along each track (prefix_scan.cuh:42-72; integer
-// sums are order-free).  One thread per track.
-__global__ void k_int_prefix(Tables T, int* v) {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    int l = 0, acc = 0;
-    int base = t;
-    for (; l < T.L; ++l) {
-        const int tracks = along_y(T, l) ? T.X : T.Y;
-        if (base < tracks) break;
-        base -= tracks;
-    }
-    if (l >= T.L) return;
-    const bool ay = along_y(T, l);
-    const int len = ay ? T.Y : T.X, stride = ay ? 1 : T.Y;
-    const int c0 = ay ? cell_index(T, l, base, 0) : cell_index(T, l, 0, base);
-    for (int k = 0; k < len; ++k) {
-        const int c = c0 + k * stride, x = v[c];
-        v[c] = acc;
-        acc += x;
-    }
-}
+__global__ void k_int_prefix(Tables T, int* v) { overflow_prefix_track(T, v, blockIdx.x * blockDim.x + threadIdx.x); }
 __global__ void k_overflow_nets(Tables T, Plan P, int n, const int* of_sum, unsigned char* is_of) {
     const int id = blockIdx.x * blockDim.x + threadIdx.x;
-    if (id >= n) return;
-    const int* r = P.routes + P.route_off[id];
-    int count = 0;
-    unsigned char flag = 0;
-    if (P.route_off[id + 1] > P.route_off[id]) {
-        for (int i = 1; i < r[0]; i += 2) {
-            const int a = r[i], b = r[i + 1], l = a / T.XY, ra = a % T.XY, rb = b % T.XY;
-            const int x0 = ra / T.Y, y0 = ra % T.Y, x1 = rb / T.Y, y1 = rb % T.Y;
-            if (x0 != x1) count += of_sum[cell_index(T, l, max(x0, x1), y0)] - of_sum[cell_index(T, l, min(x0, x1), y0)];
-            if (y0 != y1) count += of_sum[cell_index(T, l, x0, max(y0, y1))] - of_sum[cell_index(T, l, x0, min(y0, y1))];
-            if (count > 10) { flag = 1; break; }
-        }
-    }
-    is_of[id] = flag;
+    if (id < n) overflow_net(T, P, of_sum, is_of, id);
 }
 __global__ void k_congestion(Tables T, unsigned char* cong, float* xsum, float* ysum) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= T.XY) return;
-    double worst = 0.0;
-    for (int l = 0; l < T.L; ++l) {
-        const int e = l * T.XY + i;
-        worst = fmax(worst, static_cast<double>(static_cast<float>(T.demand[e]) * 0.5f - T.capacity[e]));
-    }
-    cong[i] = worst > 0.0;
-    xsum[i] = static_cast<float>(worst);
-    ysum[i] = static_cast<float>(worst);
+    if (i < T.XY) congestion_cell(T, cong, xsum, ysum, i);
 }
-// Float prefix of one line in the reference's log-step association
-// (congestion.cuh:81-112), one thread per line.
 __global__ void k_float_line_prefix(float* v, int lines, int len, int line_stride, int elem_stride) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= lines) return;
-    float* a = v + size_t(t) * line_stride;
-    float tot[32];
-    float prev = 0.f;
-    for (int i = 0; i < len; ++i) {
-        const float cur = a[size_t(i) * elem_stride];
-        float acc = i ? prev : 0.f;
-        prev = cur;
-        float fresh[32];
-        fresh[0] = acc;
-        int d = 0;
-        while ((i >> d) & 1) { acc = acc + tot[d]; ++d; fresh[d] = acc; }
-        for (int j = 0; j <= d; ++j) tot[j] = fresh[j];
-        for (int e = d + 1; (i >> e) != 0; ++e)
-            if ((i >> e) & 1) acc = acc + tot[e];
-        a[size_t(i) * elem_stride] = acc;
-    }
+    if (t < lines) congestion_line_prefix(v + size_t(t) * line_stride, len, elem_stride);
+}
+
+// Cost-term table (Tables::of_table): entry ((l, k), h) = the terms of a
+// cell of capacity caps[k] and demand h half-units on layer l, by the same
+// functions the kernels would evaluate.
+constexpr int kOfDmax = 512;  // demands below 512 half-units come from the table
+__global__ void k_build_of_table(Tables T, const float* caps) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= T.L * T.of_rows * T.of_stride) return;
+    const int row = i / T.of_stride, h = i - row * T.of_stride;
+    const int l = row / T.of_rows, k = row - l * T.of_rows;
+    double one, half;
+    cell_terms(T, caps[k], h, T.short_costs[l], one, half);
+    const_cast<double2*>(T.of_table)[i] = terms_of(one, half);
 }
 
 // The cost model's exponential for n values (grb_cost_exp).
@@ -973,7 +938,6 @@ struct grb_ctx {
     std::string error;
     Tables T{};
     std::vector<void*> owned;
-    int words = 0;          // bitmap words
     int stamp = 0;
     int64_t launches = 0;
     // net store
@@ -1060,12 +1024,20 @@ struct grb_ctx {
     // timing
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     bool profiling = false;
+    unsigned long long wait_ns = kBarrierTimeoutNs;  // limit of every device-side wait (grb_set_wait_limit)
     unsigned long long* d_phase = nullptr;     // [kPhaseSlots] persistent-kernel phase clocks
     double phase_ms[kPhaseSlots] = {};
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev_pool;
     std::vector<int> ev_slot;                  // phase slot of each recorded pair
     size_t ev_used = 0;
     double batching_ms = 0, dag_ms = 0;
+    // stage tail (grb_set_stage_tail): buffers grow on demand
+    int tail_flags = 0, tail_threshold = 0, tail_nets = 0, tail_valid = 0;
+    int* tail_of_sum = nullptr;
+    unsigned char* tail_is_of = nullptr;
+    int tail_is_of_cap = 0;
+    unsigned char* tail_cong = nullptr;
+    float *tail_xsum = nullptr, *tail_ysum = nullptr;
 };
 
 namespace {
@@ -1215,7 +1187,12 @@ int prof_collect(grb_ctx* c) {
     if (c->d_phase) {
         unsigned long long ns[kPhaseSlots];
         GRB_CUDA(c, cudaMemcpy(ns, c->d_phase, sizeof(ns), cudaMemcpyDeviceToHost));
-        for (int k = 0; k < kPhaseSlots; ++k) c->phase_ms[k] += ns[k] * 1e-6;
+        for (int k = 0; k < kPhaseSlots; ++k) {
+            if (k >= kNetTimeSlot + kDpBuckets && k < kNetTimeSlot + 2 * kDpBuckets)
+                c->phase_ms[k] = std::max(c->phase_ms[k], ns[k] * 1e-6);  // longest net: a maximum
+            else
+                c->phase_ms[k] += ns[k] * 1e-6;
+        }
         GRB_CUDA(c, cudaMemset(c->d_phase, 0, sizeof(ns)));
     }
     return GRB_OK;
@@ -1304,6 +1281,56 @@ int commit_plain(grb_ctx* c, int b, int stamp, int K) {
     return GRB_OK;
 }
 
+// The stage tail's device view (buffers sized for the current design).
+StageTail make_tail(grb_ctx* c) {
+    StageTail t{};
+    t.flags = c->tail_flags;
+    t.threshold = c->tail_threshold;
+    t.n_nets = c->n_nets;
+    t.of_sum = c->tail_of_sum;
+    t.is_of = c->tail_is_of;
+    t.cong = c->tail_cong;
+    t.xsum = c->tail_xsum;
+    t.ysum = c->tail_ysum;
+    return t;
+}
+
+// Grow the tail's per-net flags to the uploaded nets (before any launch).
+int ensure_tail(grb_ctx* c) {
+    if (!(c->tail_flags & kTailRipup) || c->n_nets <= c->tail_is_of_cap) return GRB_OK;
+    if (c->tail_is_of) cudaFree(c->tail_is_of);
+    c->tail_is_of = nullptr;
+    c->tail_is_of_cap = 0;
+    if (cudaMalloc(&c->tail_is_of, c->n_nets) != cudaSuccess) { cudaGetLastError(); return fail(c, GRB_ENOMEM, "rip-up flags"); }
+    c->tail_is_of_cap = c->n_nets;
+    return GRB_OK;
+}
+
+// The stage tail as separate launches after the last batch (plain and graph
+// forms).
+int launch_tail(grb_ctx* c) {
+    if (!c->tail_flags) return GRB_OK;
+    const StageTail t = make_tail(c);
+    const Tables& T = c->T;
+    if (t.flags & kTailRipup) {
+        int tracks = 0;
+        for (int l = 0; l < T.L; ++l) tracks += (((l & 1) ^ T.DIR) ? T.X : T.Y);
+        k_mark_overflow<<<(T.cells + 255) / 256, 256, 0, c->stream>>>(T, t.threshold, t.of_sum);
+        k_int_prefix<<<(tracks + 127) / 128, 128, 0, c->stream>>>(T, t.of_sum);
+        if (c->n_nets)
+            k_overflow_nets<<<(c->n_nets + 255) / 256, 256, 0, c->stream>>>(T, make_plan(c), c->n_nets, t.of_sum, t.is_of);
+        c->launches += c->n_nets ? 3 : 2;
+    }
+    if (t.flags & kTailView) {
+        k_congestion<<<(T.XY + 255) / 256, 256, 0, c->stream>>>(T, t.cong, t.xsum, t.ysum);
+        k_float_line_prefix<<<(T.X + 127) / 128, 128, 0, c->stream>>>(t.ysum, T.X, T.Y, T.Y, 1);  // per x, along y
+        k_float_line_prefix<<<(T.Y + 127) / 128, 128, 0, c->stream>>>(t.xsum, T.Y, T.X, 1, T.Y);  // per y, along x
+        c->launches += 3;
+    }
+    GRB_CUDA(c, cudaGetLastError());
+    return GRB_OK;
+}
+
 int stage_plain(grb_ctx* c, int stamp0) {
     for (int b = 0; b < c->n_batches; ++b) {
         const int stamp = stamp0 + b + 1;
@@ -1380,7 +1407,7 @@ int z_stage_persistent(grb_ctx* c, int stamp0) {
     Tables T = c->T;
     ZTrees Z = c->Z;
     Plan P = make_plan(c);
-    GridSync S{c->sync, c->sync + 1, kBarrierTimeoutNs, c->profiling ? c->d_phase : nullptr};
+    GridSync S{c->sync, c->sync + 1, c->wait_ns, c->profiling ? c->d_phase : nullptr};
     void* args[] = {&T, &Z, &P, &S, &stamp0, &c->work};
     GRB_CUDA(c, cudaLaunchCooperativeKernel((void*)k_zshape_persistent, dim3(per_sm * c->sms), dim3(kPersistentThreads),
                                             args, smem, c->stream));
@@ -1551,7 +1578,7 @@ int flt_stage_persistent(grb_ctx* c, int stamp0, int remove) {
     Tables T = c->T;
     Flt F = c->F;
     Plan P1 = make_plan(c), P2 = make_plan2(c);
-    GridSync S{c->sync, c->sync + 1, kBarrierTimeoutNs, c->profiling ? c->d_phase : nullptr};
+    GridSync S{c->sync, c->sync + 1, c->wait_ns, c->profiling ? c->d_phase : nullptr};
     void* args[] = {&T, &F, &P1, &P2, &S, &stamp0, &remove, &c->work};
     GRB_CUDA(c, cudaLaunchCooperativeKernel((void*)k_flt_persistent, dim3(per_sm * c->sms), dim3(kPersistentThreads),
                                             args, smem, c->stream));
@@ -1618,10 +1645,12 @@ int stage_persistent(grb_ctx* c, int stamp0) {
     GRB_CUDA(c, cudaMemsetAsync(c->sync, 0, 2 * sizeof(unsigned), c->stream));
     Tables T = c->T;
     Plan P = make_plan(c);
-    GridSync S{c->sync, c->sync + 1, kBarrierTimeoutNs, c->profiling ? c->d_phase : nullptr};
+    GridSync S{c->sync, c->sync + 1, c->wait_ns, c->profiling ? c->d_phase : nullptr};
     char* gs = c->gscratch;
     DpTune tune = c->tune;
-    void* args[] = {&T, &P, &S, &stamp0, (void*)&nmax, (void*)&ab, &gs, (void*)&slot, &c->work, &tune};
+    if ((rc = ensure_tail(c))) return rc;
+    StageTail tail = make_tail(c);
+    void* args[] = {&T, &P, &S, &stamp0, (void*)&nmax, (void*)&ab, &gs, (void*)&slot, &c->work, &tune, &tail};
     GRB_CUDA(c, cudaLaunchCooperativeKernel((void*)k_lshape_persistent, dim3(blocks), dim3(kPersistentThreads), args, smem, c->stream));
     c->launches += 1;
     return GRB_OK;
@@ -1654,7 +1683,7 @@ static int launch_batching(grb_ctx* c, BatchState& B, int mode, size_t smem) {
         GRB_CUDA(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_persistent<CH>, kPersistThreads, smem));
     if (mode == GRB_MODE_PERSISTENT && per_sm * c->sms >= 2) {
         GRB_CUDA(c, cudaMemsetAsync(c->sync, 0, 2 * sizeof(unsigned), c->stream));
-        GridSync S{c->sync, c->sync + 1, kBarrierTimeoutNs, c->profiling ? c->d_phase : nullptr, 0};
+        GridSync S{c->sync, c->sync + 1, c->wait_ns, c->profiling ? c->d_phase : nullptr, 0};
         Tables T = c->T;
         void* args[] = {&B, &S, &T};
         GRB_CUDA(c, cudaLaunchCooperativeKernel((void*)k_batch_persistent<CH>, dim3(per_sm * c->sms), dim3(kPersistThreads),
@@ -1713,8 +1742,7 @@ int grb_create(const grb_grid* g, int32_t device, grb_ctx** out) {
     T.unit_wire = g->unit_length_wire_cost; T.unit_via = g->unit_via_cost;
     T.of_scale = g->of_cost_scale;
     const size_t cells = T.cells;
-    c->words = int((cells + 31) / 32);
-    T.words = c->words;
+    T.words = int((cells + 31) / 32);
     int ng = 0;
     for (int l = 0; l < T.L; ++l) {
         T.group_base[l] = ng;
@@ -1736,9 +1764,8 @@ int grb_create(const grb_grid* g, int32_t device, grb_ctx** out) {
     rc |= dalloc(cp, &T.wcost, cells, cp->owned);
     rc |= dalloc(cp, &T.vcost, cells, cp->owned);
     rc |= dalloc(cp, &T.presum, cells, cp->owned);
-    rc |= dalloc(cp, &T.dirty_wire, c->words, cp->owned);
-    rc |= dalloc(cp, &T.dirty_via, c->words, cp->owned);
-    rc |= dalloc(cp, &T.group_flag, ng, cp->owned);
+    rc |= dalloc(cp, &T.dirty_wire, T.words, cp->owned);
+    rc |= dalloc(cp, &T.dirty_via, T.words, cp->owned);
     rc |= dalloc(cp, &T.group_first, ng, cp->owned);
     rc |= dalloc(cp, &T.first_list, ng, cp->owned);
     rc |= dalloc(cp, &T.group_list, ng, cp->owned);
@@ -1746,6 +1773,7 @@ int grb_create(const grb_grid* g, int32_t device, grb_ctx** out) {
     T.tree_chunks = prefix_chunks(std::max(T.X, T.Y));
     T.tree_stride = prefix_tree_entries(std::max(T.X, T.Y));
     rc |= dalloc(cp, &T.ptree, size_t(ng) * T.tree_stride * 32, cp->owned);
+
     rc |= dalloc(cp, &T.wirelength, 1, cp->owned);
     rc |= dalloc(cp, &T.vias, 1, cp->owned);
     rc |= dalloc(cp, &T.error, 2, cp->owned);
@@ -1758,6 +1786,53 @@ int grb_create(const grb_grid* g, int32_t device, grb_ctx** out) {
     GRB_CUDA(cp, cudaMemcpy(yl, g->y_edge_len, sizeof(int) * (T.Y - 1), cudaMemcpyHostToDevice));
     GRB_CUDA(cp, cudaMemcpy(cap, g->capacity, sizeof(float) * cells, cudaMemcpyHostToDevice));
     GRB_CUDA(cp, cudaMemset(T.error, 0, 2 * sizeof(int)));
+    {
+        // Distinct capacity values (at most kNoCapRow of them get table rows;
+        // with more, every cost is computed) and each cell's row.
+        std::vector<unsigned char> cid(cells);
+        std::vector<float> caps;
+        std::unordered_map<uint32_t, int> row;
+        uint32_t last = 0;
+        int last_row = -1;
+        for (size_t i = 0; i < cells; ++i) {
+            uint32_t bits;
+            std::memcpy(&bits, g->capacity + i, 4);
+            if (last_row < 0 || bits != last) {
+                auto it = row.find(bits);
+                if (it == row.end()) {
+                    if (int(caps.size()) >= kNoCapRow) { caps.clear(); break; }
+                    it = row.emplace(bits, int(caps.size())).first;
+                    caps.push_back(g->capacity[i]);
+                }
+                last = bits;
+                last_row = it->second;
+            }
+            cid[i] = static_cast<unsigned char>(last_row);
+        }
+        if (caps.empty()) std::fill(cid.begin(), cid.end(), static_cast<unsigned char>(kNoCapRow));
+        unsigned char* d_cid = nullptr;
+        double2* d_table = nullptr;
+        float* d_caps = nullptr;
+        const int rows = std::max<int>(int(caps.size()), 1);
+        T.of_dmax = caps.empty() ? 0 : kOfDmax;
+        T.of_rows = rows;
+        T.of_stride = kOfDmax;
+        if (dalloc(cp, &d_cid, cells, cp->owned) ||
+            dalloc(cp, &d_table, size_t(T.L) * rows * T.of_stride, cp->owned) || dalloc(cp, &d_caps, rows, cp->owned)) {
+            free_all(cp->owned);
+            return GRB_ENOMEM;
+        }
+        T.cap_id = d_cid;
+        T.of_table = d_table;
+        GRB_CUDA(cp, cudaMemcpy(d_cid, cid.data(), cells, cudaMemcpyHostToDevice));
+        if (!caps.empty()) {
+            GRB_CUDA(cp, cudaMemcpy(d_caps, caps.data(), sizeof(float) * caps.size(), cudaMemcpyHostToDevice));
+            const int n = T.L * rows * T.of_stride;
+            k_build_of_table<<<(n + 255) / 256, 256>>>(T, d_caps);
+            GRB_CUDA(cp, cudaGetLastError());
+            GRB_CUDA(cp, cudaDeviceSynchronize());
+        }
+    }
     GRB_CUDA(cp, cudaFuncSetAttribute(k_batch_solve<kChunkMax>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kSolveSmemLimit)));
     GRB_CUDA(cp, cudaFuncSetAttribute(k_batch_solve<kChunkMax / 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kSolveSmemLimit)));
     GRB_CUDA(cp, cudaFuncSetAttribute(k_batch_persistent<kChunkMax>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kSolveSmemLimit)));
@@ -1778,6 +1853,9 @@ void grb_destroy(grb_ctx* c) {
     if (!c) return;
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
+    for (void* p : {(void*)c->tail_of_sum, (void*)c->tail_is_of, (void*)c->tail_cong, (void*)c->tail_xsum,
+                    (void*)c->tail_ysum})
+        if (p) cudaFree(p);
     if (c->graph) cudaGraphExecDestroy(c->graph);
     if (c->flt_graph) cudaGraphExecDestroy(c->flt_graph);
     if (c->z_graph) cudaGraphExecDestroy(c->z_graph);
@@ -1814,7 +1892,7 @@ int grb_reset(grb_ctx* c) {
     GRB_CUDA(c, cudaMemsetAsync(T.wirelength, 0, sizeof(double), c->stream));
     GRB_CUDA(c, cudaMemsetAsync(T.vias, 0, sizeof(unsigned long long), c->stream));
     if (c->routes) GRB_CUDA(c, cudaMemsetAsync(c->routes, 0, sizeof(int) * std::max<long long>(c->route_words, 1), c->stream));
-    const int n = std::max(c->words, T.n_groups);
+    const int n = std::max(T.words, T.n_groups);
     k_mark_all_dirty<<<(n + 255) / 256, 256, 0, c->stream>>>(T);
     c->launches += 1;
     GRB_CUDA(c, cudaGetLastError());
@@ -1917,7 +1995,7 @@ int grb_set_wire_cost_mode(grb_ctx* c, int32_t integer_wire) {
     GRB_CUDA(c, cudaSetDevice(c->device));
     c->T.int_wire = integer_wire ? 1 : 0;
     // Every wire cost changes: the next refresh recomputes all cells and tracks.
-    const int n = std::max(c->words, c->T.n_groups);
+    const int n = std::max(c->T.words, c->T.n_groups);
     k_mark_all_dirty<<<(n + 255) / 256, 256, 0, c->stream>>>(c->T);
     c->launches += 1;
     GRB_CUDA(c, cudaGetLastError());
@@ -2496,13 +2574,17 @@ int grb_lshape_stage(grb_ctx* c, int32_t mode, grb_stats* stats) {
     const int stamp0 = c->stamp;
     GRB_CUDA(c, cudaEventRecord(c->ev0, c->stream));
     int rc;
+    c->tail_valid = 0;
+    if ((rc = ensure_tail(c))) return rc;
     if (mode == GRB_MODE_PLAIN) rc = stage_plain(c, stamp0);
     else if (mode == GRB_MODE_GRAPH) rc = stage_graph(c, stamp0);
     else if (mode == GRB_MODE_PERSISTENT) rc = stage_persistent(c, stamp0);
     else return fail(c, GRB_EINVAL, "unknown mode");
+    if (!rc && mode != GRB_MODE_PERSISTENT) rc = launch_tail(c);
     if (rc) return rc;
     GRB_CUDA(c, cudaEventRecord(c->ev1, c->stream));
     c->stamp = stamp0 + c->n_batches;
+    if (c->tail_flags) { c->tail_valid = 1; c->tail_nets = c->n_nets; }
     rc = check_device_error(c);
     if (rc) return rc;
     float ms = 0;
@@ -2763,6 +2845,46 @@ int grb_ripup_classify_noalloc(grb_ctx* c, int32_t threshold, uint8_t* is_of) {
     return GRB_OK;
 }
 
+int grb_set_stage_tail(grb_ctx* c, int32_t flags, int32_t threshold) {
+    if (!c) return GRB_EINVAL;
+    if (flags & ~(kTailRipup | kTailView)) return fail(c, GRB_EINVAL, "unknown stage tail flags");
+    GRB_CUDA(c, cudaSetDevice(c->device));
+    const size_t cells = c->T.cells, xy = c->T.XY;
+    if ((flags & kTailRipup) && !c->tail_of_sum && cudaMalloc(&c->tail_of_sum, 4 * cells) != cudaSuccess) {
+        cudaGetLastError();
+        c->tail_of_sum = nullptr;
+        return fail(c, GRB_ENOMEM, "rip-up marks");
+    }
+    if ((flags & kTailView) && !c->tail_cong) {
+        if (cudaMalloc(&c->tail_cong, xy) || cudaMalloc(&c->tail_xsum, 4 * xy) || cudaMalloc(&c->tail_ysum, 4 * xy)) {
+            cudaGetLastError();
+            for (void* p : {(void*)c->tail_cong, (void*)c->tail_xsum, (void*)c->tail_ysum}) if (p) cudaFree(p);
+            c->tail_cong = nullptr; c->tail_xsum = c->tail_ysum = nullptr;
+            return fail(c, GRB_ENOMEM, "congestion view buffers");
+        }
+    }
+    c->tail_flags = flags;
+    c->tail_threshold = threshold;
+    c->tail_valid = 0;
+    return ensure_tail(c);
+}
+
+int grb_read_stage_tail(grb_ctx* c, uint8_t* is_of, uint8_t* congestion, float* xsum, float* ysum) {
+    if (!c) return GRB_EINVAL;
+    if (!c->tail_valid) return fail(c, GRB_EINVAL, "no L-shape stage has run with a stage tail since it was set");
+    if (is_of && !(c->tail_flags & kTailRipup)) return fail(c, GRB_EINVAL, "the stage tail has no rip-up classification");
+    if ((congestion || xsum || ysum) && !(c->tail_flags & kTailView))
+        return fail(c, GRB_EINVAL, "the stage tail has no congestion view");
+    GRB_CUDA(c, cudaSetDevice(c->device));
+    const size_t xy = c->T.XY;
+    if (is_of && c->tail_nets) GRB_CUDA(c, cudaMemcpyAsync(is_of, c->tail_is_of, c->tail_nets, cudaMemcpyDeviceToHost, c->stream));
+    if (congestion) GRB_CUDA(c, cudaMemcpyAsync(congestion, c->tail_cong, xy, cudaMemcpyDeviceToHost, c->stream));
+    if (xsum) GRB_CUDA(c, cudaMemcpyAsync(xsum, c->tail_xsum, 4 * xy, cudaMemcpyDeviceToHost, c->stream));
+    if (ysum) GRB_CUDA(c, cudaMemcpyAsync(ysum, c->tail_ysum, 4 * xy, cudaMemcpyDeviceToHost, c->stream));
+    GRB_CUDA(c, cudaStreamSynchronize(c->stream));
+    return GRB_OK;
+}
+
 int grb_cost_exp(int32_t device, const float* x, int32_t n, float* y) {
     if (n < 0 || (n > 0 && (!x || !y))) return GRB_EINVAL;
     if (n == 0) return GRB_OK;
@@ -2859,6 +2981,14 @@ int grb_sync(grb_ctx* c) {
 }
 
 int64_t grb_kernel_launches(grb_ctx* c) { return c ? c->launches : 0; }
+
+int grb_set_wait_limit(grb_ctx* c, double seconds) {
+    if (!c) return GRB_EINVAL;
+    if (!(seconds > 0) || seconds > 3600) return fail(c, GRB_EINVAL, "wait limit must be in (0, 3600] seconds");
+    c->wait_ns = static_cast<unsigned long long>(seconds * 1e9);
+    if (c->wait_ns == 0) c->wait_ns = 1;
+    return GRB_OK;
+}
 
 int grb_set_profiling(grb_ctx* c, int32_t on) {
     if (!c) return GRB_EINVAL;

@@ -271,6 +271,25 @@ class Router:
         self._check(self._lib.grb_congestion_view(self._ctx, _p(cong), _p(xs), _p(ys)))
         return cong, xs, ys
 
+    def set_stage_tail(self, ripup: bool = True, view: bool = True, threshold: int = 0):
+        """Compute the rip-up classification and/or the congestion view of the
+        final demand at the end of every following lshape_route (inside the
+        persistent kernel, no host round trip); read with stage_tail()."""
+        flags = (_abi.GRB_TAIL_RIPUP if ripup else 0) | (_abi.GRB_TAIL_VIEW if view else 0)
+        self._check(self._lib.grb_set_stage_tail(self._ctx, flags, int(threshold)))
+        self._tail = flags
+
+    def stage_tail(self):
+        """(is_of, (congestion, xsum, ysum)) of the last stage's tail (None for
+        parts not computed)."""
+        flags = getattr(self, "_tail", 0)
+        xy = self.grid.X * self.grid.Y
+        is_of = np.zeros(self.nets.n if self.nets else 0, np.uint8) if flags & _abi.GRB_TAIL_RIPUP else None
+        view = (np.empty(xy, np.uint8), np.empty(xy, np.float32), np.empty(xy, np.float32)) \
+            if flags & _abi.GRB_TAIL_VIEW else None
+        self._check(self._lib.grb_read_stage_tail(self._ctx, _p(is_of), *(_p(v) for v in (view or (None,) * 3))))
+        return is_of, view
+
     # -- readback ----------------------------------------------------------------
     def read_tables(self) -> dict:
         n = self.grid.cells
@@ -304,8 +323,14 @@ class Router:
     # Batching: plain form raster / gather / solve / publish; persistent form
     # publish / gather / solve, plus the waits and the raster it overlaps
     # with the solve.  L-shape stage: the next four.
-    PHASES = ("batch_raster", "batch_gather", "batch_solve", "batch_publish", "refresh_cells", "dp", "commit",
-              "refresh_prefix", "batch_solver_wait", "batch_worker_wait", "unused10", "unused11")
+    PHASES = ("batch_raster", "batch_gather", "batch_solve", "batch_publish", "cost_pass1", "dp", "commit",
+              "prefix_tree_pass2", "batch_solver_wait", "batch_worker_wait", "unused10", "unused11",
+              "net_ms_bucket0", "net_ms_bucket1", "net_ms_bucket2", "net_ms_bucket3",
+              "longest_net_ms_bucket0", "longest_net_ms_bucket1", "longest_net_ms_bucket2", "longest_net_ms_bucket3")
+
+    def set_wait_limit(self, seconds: float):
+        """Limit of every device-side wait of the persistent kernels."""
+        self._check(self._lib.grb_set_wait_limit(self._ctx, float(seconds)))
 
     def set_profiling(self, on: bool = True):
         self._check(self._lib.grb_set_profiling(self._ctx, int(bool(on))))

@@ -274,6 +274,24 @@ int grb_softmin_forward(grb_ctx* ctx, int32_t dtype, double tau, const void* cap
 int grb_softmin_backward(grb_ctx* ctx, int32_t dtype, double tau, const void* capacity, const void* unit_wire,
                          double unit_via, double grad_total, void* dcap, void* dunit_wire, double* dunit_via);
 
+/* Stage tail: the rip-up classification (flags bit 0, GRB_TAIL_RIPUP, with
+ * graph::ripup's threshold) and the congestion view (bit 1, GRB_TAIL_VIEW) of
+ * the final demand, computed by every following grb_lshape_stage right after
+ * its last batch -- in the persistent executor inside the same kernel, with
+ * no host round trip between the stage and them (the reference runs both
+ * right after its L-shape stage, pipeline.hpp:86-93, each with a host
+ * synchronisation; the rip-up flags it then downloads, flt.cuh:58-60, are
+ * read here with grb_read_stage_tail).  flags = 0 turns the tail off.
+ * Allocates its buffers here (one int per cell, one byte per net, a byte and
+ * two floats per 2-D cell). */
+#define GRB_TAIL_RIPUP 1
+#define GRB_TAIL_VIEW 2
+int grb_set_stage_tail(grb_ctx* ctx, int32_t flags, int32_t threshold);
+/* Copy the last stage tail's results to the host: is_of[n] (as
+ * grb_ripup_classify), congestion/xsum/ysum[X*Y] (as grb_congestion_view);
+ * any pointer may be NULL. */
+int grb_read_stage_tail(grb_ctx* ctx, uint8_t* is_of, uint8_t* congestion, float* xsum, float* ysum);
+
 /* Congestion view for the FLT topology builder (congestion.cuh:60-112). */
 int grb_congestion_view(grb_ctx* ctx, uint8_t* congestion, float* xsum, float* ysum);
 
@@ -303,18 +321,28 @@ int grb_sync(grb_ctx* ctx);
  * every kernel node); used for launch accounting by callers. */
 int64_t grb_kernel_launches(grb_ctx* ctx);
 
+/* Limit of every device-side wait of the persistent kernels (grid barriers
+ * and the batching kernel's hand-over counters), in seconds; 20 by default.
+ * A wait that runs out records GRB_ETIMEDOUT, every block of the kernel
+ * returns, and the call that launched it reports GRB_ETIMEDOUT.  The
+ * context's tables are then in an unspecified state: grb_reset (and a new
+ * plan) before the next stage.  (The reference has no device waits.) */
+int grb_set_wait_limit(grb_ctx* ctx, double seconds);
+
 /* Profiling (off by default).  When on, the plain form brackets each launch
  * group with CUDA events and the persistent kernels time each phase between
  * grid barriers (global timer, thread 0 of one block).  grb_phase_times
- * returns accumulated milliseconds per phase (up to 12 entries):
+ * returns accumulated milliseconds per phase (up to 20 entries):
  * batching [0] raster (persistent: publish of the previous chunk), [1]
  * gather of forbidden colours and predecessors (persistent: gather of the
  * next chunk and raster of the one after), [2] in-chunk solve, [3] publish
- * (plain form only); stages [4] dirty-cell cost recompute, [5] DP
- * (persistent: + wire commit), [6] commit (persistent: vias), [7]
- * prefix-table rebuild; persistent batching [8] solver waiting for a
- * gathered chunk, [9] other blocks waiting for a solved chunk; [10] and [11]
- * unused.  The reference prints its stage timings as BATCH_TIMING /
+ * (plain form only); stages [4] cost recompute of the dirty chunks with
+ * prefix pass 1, [5] DP (persistent: + wire commit), [6] commit
+ * (persistent: vias), [7] prefix trees and pass 2; persistent batching [8]
+ * solver waiting for a gathered chunk, [9] other blocks waiting for a solved
+ * chunk; [10] and [11] unused; persistent L-shape stage, per size bucket k of
+ * the DP (tree nodes <= 2, <= 8, <= 16, more): [12+k] warp time summed over
+ * its nets, [16+k] the longest single net (a maximum, not a sum).  The reference prints its stage timings as BATCH_TIMING /
  * DAG_TIMING records (router_state.hpp:259-264). */
 int grb_set_profiling(grb_ctx* ctx, int32_t on);
 int grb_phase_times(grb_ctx* ctx, double* ms, int32_t n, int32_t reset);

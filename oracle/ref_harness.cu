@@ -318,6 +318,19 @@ int run_flt(const std::string& cap, const std::string& net, const std::string& d
     graph::extract_congestionView<<<BLOCK_NUM(view.X * view.Y), THREAD_NUM>>>(view);
     graph::extract_congestionView_xsum<<<view.Y, THREAD_NUM, sizeof(float) * view.X>>>(view);
     graph::extract_congestionView_ysum<<<view.X, THREAD_NUM, sizeof(float) * view.Y>>>(view);
+    {
+        // The congestion view the host FLT builder reads (congestion.cuh:60-112).
+        const size_t xy = size_t(view.X) * view.Y;
+        std::vector<unsigned char> cong(xy);
+        std::vector<float> xsum(xy), ysum(xy);
+        grotor::cuda_check(cudaMemcpy(cong.data(), view.congestion, xy, cudaMemcpyDeviceToHost), "congestion");
+        grotor::cuda_check(cudaMemcpy(xsum.data(), view.congestion_xsum, 4 * xy, cudaMemcpyDeviceToHost), "xsum");
+        grotor::cuda_check(cudaMemcpy(ysum.data(), view.congestion_ysum, 4 * xy, cudaMemcpyDeviceToHost), "ysum");
+        std::vector<int> cong_i(cong.begin(), cong.end());
+        dump(dir, "flt_congestion", cong_i);
+        dump(dir, "flt_xsum", xsum);
+        dump(dir, "flt_ysum", ysum);
+    }
     auto overflow_nets = graph::ripup(state, 0);
     dump(dir, "flt_of_nets", overflow_nets.first);
     int pin_count = 0;

@@ -14,6 +14,7 @@ multisets themselves are compared exactly on the GPU (test_gpu_flt.py).
 import numpy as np
 import pytest
 
+import oracle
 from helpers import (flt_by_net, float_demand_to_half, golden_grid, golden_nets, load_golden, orc_grid,
                      ref_routes2_of, route_geometry, segment_multiset)
 
@@ -86,3 +87,20 @@ def test_flt_stage_equals_reference(name):
         assert route_geometry(ours, X, Y) == route_geometry(ref, X, Y), f"net {net}"
         same_segments += segment_multiset(ours) == segment_multiset(ref)
     assert same_segments >= 0.95 * len(g["flt_nets"])
+
+
+def test_congestion_view_equals_reference():
+    """The oracle's congestion view (congestion.cuh:60-112) of the reference's
+    demand after its L-shape stage equals the view the reference itself
+    computed for its FLT topology builder, bit for bit: the per-cell flag and
+    both row/column float prefixes (whose association the restatement
+    follows)."""
+    g = load_golden("ref_flt_48x48x10_1500")
+    if "flt_congestion" not in g:
+        pytest.skip("fixture lacks the reference congestion view")
+    og = orc_grid(golden_grid(g))
+    cong, xs, ys = oracle.congestion_view(og, float_demand_to_half(g["flt_before_demand"]))
+    np.testing.assert_array_equal(cong, g["flt_congestion"].astype(np.uint8))
+    np.testing.assert_array_equal(xs.view(np.int32), g["flt_xsum"].view(np.int32))
+    np.testing.assert_array_equal(ys.view(np.int32), g["flt_ysum"].view(np.int32))
+    assert cong.sum() > 0 and np.count_nonzero(xs) > 0
