@@ -86,9 +86,14 @@ __device__ __forceinline__ double wire_cost(const Tables& T, int l, int xmin, in
 
 // Route one net.  All 32 lanes of the warp call this with the same id.
 // Returns false (and records kELimit) if the net's route storage is too small.
-__device__ void lshape_net(const Tables& T, const Plan& P, int id, int stamp, const Arena& A, int lane,
-                           bool fuse_wires) {
-    const int L = T.L, Y = T.Y, XY = T.XY, TT = tri_count(L);
+// LC: the number of routing layers when known at compile time (the loops
+// over layers then unroll into independent loads and predicated compares, in
+// the same order), 0 for any layer count.
+template <int LC>
+__device__ __forceinline__ void lshape_net_l(const Tables& T, const Plan& P, int id, int stamp, const Arena& A,
+                                             int lane, bool fuse_wires) {
+    const int L = LC > 0 ? LC : T.L, Y = T.Y, XY = T.XY, TT = tri_count(L);
+    constexpr int LL = LC > 0 ? LC : kMaxLayers;  // static bound of the layer loops
     const int off = P.node_off[id], N = P.node_off[id + 1] - off;
     const int* nd = P.nodes + off;
     const int* par = P.parents + off;
@@ -159,7 +164,9 @@ __device__ void lshape_net(const Tables& T, const Plan& P, int id, int stamp, co
         const int i = q / L, lo = q - i * L;
         const int fixed = A.lay[i];
         double acc = 0;
-        for (int hi = lo; hi < L; ++hi) {
+#pragma unroll
+        for (int hi = 0; hi < LL; ++hi) {
+            if (hi < lo || hi >= L) continue;
             if (hi > lo) acc = acc + static_cast<double>(A.vN[i * L + hi - 1]);
             A.dist[i * TT + tri(L, lo, hi)] = (fixed < L && (lo > fixed || hi < fixed)) ? kInf : acc;
         }
@@ -196,8 +203,11 @@ __device__ void lshape_net(const Tables& T, const Plan& P, int id, int stamp, co
                     const int l = sl;
                     double best = kInf;
                     int bf = 0;
-                    for (int lo = 0; lo <= l; ++lo)
-                        for (int hi = l; hi < L; ++hi) {
+#pragma unroll
+                    for (int lo = 0; lo < LL; ++lo)
+#pragma unroll
+                        for (int hi = lo; hi < LL; ++hi) {
+                            if (lo > l || hi < l || hi >= L) continue;
                             const double v = di[tri(L, lo, hi)];
                             if (v < best) { best = v; bf = lo * L + hi; }
                         }
@@ -218,11 +228,16 @@ __device__ void lshape_net(const Tables& T, const Plan& P, int id, int stamp, co
                             pb = A.cur_from[s0 + pl] * L * L + pl * L + pl;
                         }
                     } else {
-                        for (int cl = (pl & 1) ^ 1; cl < L; cl += 2) {
+#pragma unroll
+                        for (int cl = 0; cl < LL; ++cl) {
+                            if (((cl ^ pl) & 1) == 0 || cl >= L) continue;  // the other parity, ascending
                             const double cost = A.cur[s0 + cl] + A.w1[i * L + cl];
                             double cost2 = 0;
                             const float* v = along_y(T, cl) ? A.vA + i * L : A.vB + i * L;
-                            for (int l = min(cl, pl) + 1; l < max(cl, pl); ++l) cost2 += static_cast<double>(v[l]);
+                            const int a = min(cl, pl), b = max(cl, pl);
+#pragma unroll
+                            for (int l = 0; l < LL; ++l)
+                                if (l > a && l < b) cost2 += static_cast<double>(v[l]);
                             cost2 += A.w2[i * L + pl];
                             if (cost + cost2 < best) {
                                 best = cost + cost2;
@@ -240,7 +255,9 @@ __device__ void lshape_net(const Tables& T, const Plan& P, int id, int stamp, co
                     const int lo = sl, s0 = slot * L;
                     double c = A.diag[s0 + lo];
                     int path = A.pdiag[s0 + lo];
-                    for (int hi = lo; hi < L; ++hi) {
+#pragma unroll
+                    for (int hi = 0; hi < LL; ++hi) {
+                        if (hi < lo || hi >= L) continue;
                         if (hi > lo && !(c <= A.diag[s0 + hi])) { c = A.diag[s0 + hi]; path = A.pdiag[s0 + hi]; }
                         const int t = tri(L, lo, hi);
                         A.dist[i * TT + t] = c;
@@ -343,6 +360,14 @@ __device__ void lshape_net(const Tables& T, const Plan& P, int id, int stamp, co
     if (fuse_wires) commit_net_wires(T, P, id, stamp, 1, lane);
 }
 
+// Route one net: the layer loops unrolled for the 9 routing layers of the
+// reference's 10-layer designs, generic otherwise.
+__device__ __forceinline__ void lshape_net(const Tables& T, const Plan& P, int id, int stamp, const Arena& A,
+                                           int lane, bool fuse_wires) {
+    if (T.L == 9) lshape_net_l<9>(T, P, id, stamp, A, lane, fuse_wires);
+    else lshape_net_l<0>(T, P, id, stamp, A, lane, fuse_wires);
+}
+
 // Nets of one or two tree nodes, one net per lane: the lanes of a warp route
 // up to 32 such nets at once (most nets of a design), where lshape_net would
 // spend a whole warp, mostly idle, on each.  Same arithmetic, comparisons,
@@ -356,8 +381,9 @@ __host__ __device__ __forceinline__ size_t pair_scratch_bytes() {
     return size_t(32) * (kPairD * 8 + kPairF * 4 + kPairH * 2);
 }
 
-__device__ __forceinline__ void lshape_net_pair(const Tables& T, const Plan& P, int id, int stamp, char* scratch,
-                                                int lane, bool commit) {
+template <int LC>
+__device__ __forceinline__ void lshape_net_pair_l(const Tables& T, const Plan& P, int id, int stamp, char* scratch,
+                                                  int lane, bool commit) {
     if (id < 0) return;
     double* sd = reinterpret_cast<double*>(scratch);
     float* sf = reinterpret_cast<float*>(scratch + size_t(32) * kPairD * 8);
@@ -371,7 +397,7 @@ __device__ __forceinline__ void lshape_net_pair(const Tables& T, const Plan& P, 
     auto vN = [&](int l) -> float& { return sf[(2 * kMaxLayers + l) * 32 + lane]; };
     auto pdiag = [&](int l) -> int& { return si[(2 * kMaxLayers + l) * 32 + lane]; };       // after vN
     auto cfrom = [&](int l) -> unsigned short& { return sh[l * 32 + lane]; };
-    const int L = T.L, Y = T.Y, XY = T.XY;
+    const int L = LC > 0 ? LC : T.L, Y = T.Y, XY = T.XY;
     const int off = P.node_off[id], N = P.node_off[id + 1] - off;
     const int n0 = P.nodes[off], r0 = n0 % XY, x0 = r0 / Y, y0 = r0 - x0 * Y, fix0 = n0 / XY;
     int x1 = 0, y1 = 0;
@@ -420,15 +446,19 @@ __device__ __forceinline__ void lshape_net_pair(const Tables& T, const Plan& P, 
         }
         // Steps 2 and 3a: the child's via stacks, and its best range through
         // each layer, first minimum in (lo, hi) order.
+#pragma unroll
         for (int l = 0; l < L; ++l) {
             cur(l) = kInf;
             cfrom(l) = 0;
         }
+#pragma unroll
         for (int lo = 0; lo < L; ++lo) {
             double acc = 0;
+#pragma unroll
             for (int hi = lo; hi < L; ++hi) {
                 if (hi > lo) acc = acc + static_cast<double>(vN(hi - 1));
                 const double v = (fix1 < L && (lo > fix1 || hi < fix1)) ? kInf : acc;
+#pragma unroll
                 for (int l = lo; l <= hi; ++l)
                     if (v < cur(l)) {
                         cur(l) = v;
@@ -437,6 +467,7 @@ __device__ __forceinline__ void lshape_net_pair(const Tables& T, const Plan& P, 
             }
         }
         // Step 3b: best cost of reaching the parent on each layer.
+#pragma unroll
         for (int pl = 0; pl < L; ++pl) {
             double best = kInf;
             int pb = 0;
@@ -447,10 +478,12 @@ __device__ __forceinline__ void lshape_net_pair(const Tables& T, const Plan& P, 
                     pb = cfrom(pl) * L * L + pl * L + pl;
                 }
             } else {
+#pragma unroll
                 for (int cl = (pl & 1) ^ 1; cl < L; cl += 2) {
                     const double cost = cur(cl) + w1(cl);
                     double cost2 = 0;
                     const bool ay = along_y(T, cl);
+#pragma unroll
                     for (int l = min(cl, pl) + 1; l < max(cl, pl); ++l)
                         cost2 += static_cast<double>(ay ? vA(l) : vB(l));
                     cost2 += w2(pl);
@@ -478,6 +511,7 @@ __device__ __forceinline__ void lshape_net_pair(const Tables& T, const Plan& P, 
     int choice = 0, bestpath = 0;
     {
         double best = 0;
+#pragma unroll
         for (int lo = 0; lo < L; ++lo) {
             double acc = 0, c = 0;
             int path = 0;
@@ -485,6 +519,7 @@ __device__ __forceinline__ void lshape_net_pair(const Tables& T, const Plan& P, 
                 c = w2(lo);
                 path = pdiag(lo);
             }
+#pragma unroll
             for (int hi = lo; hi < L; ++hi) {
                 if (hi > lo) acc = acc + static_cast<double>(vA(hi - 1));
                 double v = (fix0 < L && (lo > fix0 || hi < fix0)) ? kInf : acc;
@@ -541,6 +576,14 @@ __device__ __forceinline__ void lshape_net_pair(const Tables& T, const Plan& P, 
     }
     out[0] = 1 + words;
     if (commit) commit_thread_wires(T, P, id, stamp, 1);
+}
+
+// One or two tree nodes per lane: unrolled for 9 routing layers, generic
+// otherwise.
+__device__ __forceinline__ void lshape_net_pair(const Tables& T, const Plan& P, int id, int stamp, char* scratch,
+                                                int lane, bool commit) {
+    if (T.L == 9) lshape_net_pair_l<9>(T, P, id, stamp, scratch, lane, commit);
+    else lshape_net_pair_l<0>(T, P, id, stamp, scratch, lane, commit);
 }
 
 }  // namespace grb

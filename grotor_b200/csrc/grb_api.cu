@@ -237,6 +237,26 @@ __global__ void __launch_bounds__(kPersistentThreads, 2) k_lshape_persistent(Tab
         for (int bk = kDpBuckets - 1; bk >= 0; --bk) {
             const int blo = P.bucket_off[b * (kDpBuckets + 1) + bk], bhi = P.bucket_off[b * (kDpBuckets + 1) + bk + 1];
             const int g = tune.per_grab[bk];
+            if (bk == 0 && g >= 32) {
+                // Nets of one or two nodes, one per lane (lane-interleaved
+                // scratch in the warp's arena), g per grab.
+                while (true) {
+                    int k = 0;
+                    if (lane == 0) k = atomicAdd(work + b * kDpBuckets + bk, g);
+                    k = __shfl_sync(0xffffffffu, k, 0);
+                    if (blo + k >= bhi) break;
+                    const unsigned long long t0 = S.phase_ns && lane == 0 ? global_ns() : 0ull;
+                    for (int q = blo + k + lane; q < min(blo + k + g, bhi); q += 32)
+                        lshape_net_pair(T, P, P.bucket_ids[q], stamp, smem + size_t(warp) * arena_b, lane, true);
+                    __syncwarp();
+                    if (S.phase_ns && lane == 0) {
+                        const unsigned long long dt = global_ns() - t0;
+                        atomicAdd(S.phase_ns + kNetTimeSlot + bk, dt);
+                        atomicMax(S.phase_ns + kNetTimeSlot + kDpBuckets + bk, dt);
+                    }
+                }
+                continue;
+            }
             while (true) {
                 int k = 0;
                 if (lane == 0) k = atomicAdd(work + b * kDpBuckets + bk, g);
@@ -1621,7 +1641,8 @@ int stage_graph(grb_ctx* c, int stamp0) {
 int stage_persistent(grb_ctx* c, int stamp0) {
     if (c->n_batches == 0) return GRB_OK;
     const int nmax = dp_nmax(c);
-    const size_t ab = arena_bytes(c->T.L, nmax);
+    // A warp's arena also holds the lane-per-net scratch of the smallest nets.
+    const size_t ab = std::max(arena_bytes(c->T.L, nmax), (pair_scratch_bytes() + 15) & ~size_t(15));
     const int wpb = kPersistentThreads / 32;
     const size_t prefix_smem = prefix_smem_bytes(std::max(c->T.X, c->T.Y));  // prefix_tree
     const size_t smem = std::max(std::max(ab * wpb, prefix_smem), size_t(wpb) * prefix_xpose_bytes());
@@ -2743,10 +2764,14 @@ int grb_autotune(grb_ctx* c, int32_t what, int32_t* per_cta, int32_t* per_grab) 
     if (what & 2) {
         // Persistent form: whole-stage runs from a reset state for each
         // candidate set of nets per grab (small buckets take more per grab).
-        const int cands[4][kDpBuckets] = {{1, 1, 1, 1}, {2, 1, 1, 1}, {4, 2, 1, 1}, {8, 4, 2, 1}};
+        // per_grab[0] >= 32: nets of one or two nodes one per lane, that many
+        // per grab.
+        constexpr int kCands = 6;
+        const int cands[kCands][kDpBuckets] = {{1, 1, 1, 1}, {2, 1, 1, 1}, {4, 2, 1, 1}, {8, 4, 2, 1},
+                                               {32, 2, 1, 1}, {64, 4, 2, 1}};
         float best = 1e30f;
         int pick = 0;
-        for (int k = 0; k < 4; ++k) {
+        for (int k = 0; k < kCands; ++k) {
             for (int q = 0; q < kDpBuckets; ++q) c->tune.per_grab[q] = cands[k][q];
             if ((rc = grb_reset(c))) { c->profiling = prof; return rc; }
             GRB_CUDA(c, cudaEventRecord(c->ev0, c->stream));

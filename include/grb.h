@@ -160,7 +160,8 @@ int grb_ripup_classify_noalloc(grb_ctx* ctx, int32_t threshold, uint8_t* is_of);
  * per-batch DP launch of each bucket on the plan's largest batches for 1, 2,
  * 4 and 8 nets per CTA (arena sized to the bucket); what & 2 runs the
  * persistent stage from a reset state for candidate nets-per-grab sets of its
- * work queue.  The choices stay in the context (and are copied to the
+ * work queue (a nets-per-grab of 32 or more for the smallest bucket routes
+ * those nets one per lane).  The choices stay in the context (and are copied to the
  * optional per_cta[4] / per_grab[4]).  Needs nets and a plan; leaves the
  * context reset (grb_reset).  Routes do not depend on the choices. */
 int grb_autotune(grb_ctx* ctx, int32_t what, int32_t* per_cta, int32_t* per_grab);

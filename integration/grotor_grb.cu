@@ -1,0 +1,348 @@
+// grotor_grb.cu -- the reference router's default pipeline with its routing
+// hot path on grotor_b200.
+//
+// This is the reference-side driver a maintainer of the reference router adds
+// to adopt grotor_b200: the program below is the reference's own `main`
+// (src/main.cu:22-179) and `grotor::route` (src/pipeline.hpp:14-157), compiled
+// against the reference's headers (include path only; nothing is copied), with
+// the hot path of its two routing stages replaced by calls into libgrb (the C
+// ABI of include/grb.h):
+//
+//   * stage one, Lshape_route (src/routing/lshape.cuh:21-197): the reference's
+//     host code builds the FLUTE trees and the HPWL order as before; first-fit
+//     batching (generate_batches_cpu_timed), the per-batch cost refresh, the
+//     L-shape DP and the demand commit run in grb_plan_batches +
+//     grb_lshape_stage, whose stage tail also computes the congestion view and
+//     the rip-up classification the pipeline needs next (pipeline.hpp:86-93);
+//   * stage two, Lshape_route_detour::route_detour (src/routing/flt.cuh:
+//     186-192): the reference's host FLT DAG builder (process_net,
+//     flt.cuh:8-46) runs unchanged on the congestion view; batching and the
+//     DAG execution loop of route_prepared_topology (flt.cuh:75-182) run in
+//     grb_plan_batches + grb_upload_flt + grb_flt_stage.
+//
+// Everything else -- CAP/NET parsing (db::read), net splitting
+// (prepare_routing_nets), FLUTE, the FLT DAG builder, finish_nets and the .out
+// writer (output_nets) -- is the reference's code, so the same input gives
+// the same .out (stage-one nets byte for byte; for stage-two nets the
+// reference's own segment order is not defined, so the segments of each net
+// are compared as a set).
+//
+// Usage: grotor_grb -cap FILE -net FILE -out FILE [--lut-dir DIR]
+//                   [--executor persistent|plain|graph] [--stop-after lshape|routing]
+#include "pipeline.hpp"
+
+#include <filesystem>
+
+#include "grb.h"
+
+namespace drop_in {
+
+void check(int rc, grb_ctx* ctx, const char* what) {
+    if (rc) throw std::runtime_error(std::string(what) + ": " + (ctx ? grb_last_error(ctx) : "error ") +
+                                     " (code " + std::to_string(rc) + ")");
+}
+
+// The grid tables of build_cuda_database (preprocess.hpp:1625-1786).
+struct Grid {
+    std::vector<double> short_costs;
+    std::vector<int32_t> xlen, ylen;
+    std::vector<float> capacity;
+    grb_grid g{};
+};
+
+Grid make_grid(const cudb::RouterState& state) {
+    Grid G;
+    const int L = state.device.L, X = state.device.X, Y = state.device.Y;
+    for (int l = 0; l < L; ++l) G.short_costs.push_back(db::unit_length_short_costs[l + 1]);
+    for (int x = 0; x + 1 < X; ++x) G.xlen.push_back(db::x_edge_len[x]);
+    for (int y = 0; y + 1 < Y; ++y) G.ylen.push_back(db::y_edge_len[y]);
+    G.capacity.resize(size_t(L) * X * Y);
+    for (int l = 0; l < L; ++l)
+        for (int x = 0; x < X; ++x)
+            for (int y = 0; y < Y; ++y) G.capacity[(size_t(l) * X + x) * Y + y] = float(db::capacity[l + 1][x][y]);
+    G.g.L = L;
+    G.g.X = X;
+    G.g.Y = Y;
+    G.g.DIR = db::layers[1].dir;
+    G.g.unit_length_wire_cost = db::unit_length_wire_cost;
+    G.g.unit_via_cost = db::unit_via_cost;
+    G.g.of_cost_scale = 1.0;  // router_state.hpp:37 on one GPU
+    G.g.unit_length_short_costs = G.short_costs.data();
+    G.g.x_edge_len = G.xlen.data();
+    G.g.y_edge_len = G.ylen.data();
+    G.g.capacity = G.capacity.data();
+    return G;
+}
+
+// Every net's tree in the depth-first order of Lshape_route (node 0 = root,
+// parents before children; lshape.cuh:85-103), its batching geometry
+// (net::points and the RSMT segments), and its route words at the reference's
+// own offsets (pin_cnt_sum_cpu * ROUTE_PER_PIN, router_state.hpp:31) -- all by
+// net id.
+struct Nets {
+    std::vector<int32_t> node_off{0}, nodes, parents, point_off{0}, points, hseg_off{0}, hsegs, vseg_off{0}, vsegs;
+    std::vector<int64_t> route_off;
+    grb_nets n{};
+};
+
+Nets flatten_nets(const cudb::RouterState& state) {
+    Nets F;
+    const auto& nets = state.nets;
+    const int count = int(nets.size());
+    for (int id = 0; id < count; ++id) {
+        const auto& graph = nets[id].rsmt;
+        const size_t base = F.nodes.size();
+        const size_t size = graph.empty() ? 0 : graph.back().size();
+        F.nodes.resize(base + size);
+        F.parents.resize(base + size);
+        int next = 0;
+        std::function<void(int, int, int)> dfs = [&](int x, int par, int par_node) {
+            const int idx = next++;
+            F.nodes[base + idx] = graph.back()[x];
+            F.parents[base + idx] = par_node;
+            for (int e : graph[x]) if (e != par) dfs(e, x, idx);
+        };
+        if (size) dfs(0, -1, -1);
+        F.node_off.push_back(int32_t(F.nodes.size()));
+        for (int p : nets[id].points) F.points.push_back(p);
+        F.point_off.push_back(int32_t(F.points.size()));
+        for (const auto& s : nets[id].rsmt_h_segments) { F.hsegs.push_back(s.first); F.hsegs.push_back(s.second); }
+        F.hseg_off.push_back(int32_t(F.hsegs.size() / 2));
+        for (const auto& s : nets[id].rsmt_v_segments) { F.vsegs.push_back(s.first); F.vsegs.push_back(s.second); }
+        F.vseg_off.push_back(int32_t(F.vsegs.size() / 2));
+    }
+    for (int id = 0; id <= count; ++id)
+        F.route_off.push_back(int64_t(state.pin_cnt_sum_cpu[id]) * int64_t(state.device.ROUTE_PER_PIN));
+    F.n.n = count;
+    F.n.node_off = F.node_off.data();
+    F.n.nodes = F.nodes.data();
+    F.n.parents = F.parents.data();
+    F.n.route_off = F.route_off.data();
+    F.n.point_off = F.point_off.data();
+    F.n.points = F.points.data();
+    F.n.hseg_off = F.hseg_off.data();
+    F.n.hsegs = F.hsegs.data();
+    F.n.vseg_off = F.vseg_off.data();
+    F.n.vsegs = F.vsegs.data();
+    return F;
+}
+
+int32_t executor_mode(const std::string& name) {
+    if (name == "persistent") return GRB_MODE_PERSISTENT;
+    if (name == "plain") return GRB_MODE_PLAIN;
+    if (name == "graph") return GRB_MODE_GRAPH;
+    throw std::invalid_argument("--executor expects persistent, plain or graph");
+}
+
+// Stage one: Lshape_route (lshape.cuh:21-197) with batching, cost refresh,
+// DAG and commit on grotor_b200.  Leaves nets2route in the plan order, as
+// the reference does, and the phase-one routes in state.routes_cpu.
+void lshape_stage(cudb::RouterState& state, grb_ctx* ctx, std::vector<int>& nets2route, int32_t mode,
+                  int64_t initial_vias, bool tail) {
+    auto& nets = state.nets;
+#pragma omp parallel for num_threads(8)
+    for (int i = 0; i < int(nets2route.size()); ++i) nets[nets2route[i]].construct_rsmt(state, false);
+    std::sort(nets2route.begin(), nets2route.end(), [&](int l, int r) { return nets[l].hpwl > nets[r].hpwl; });
+    Nets F = flatten_nets(state);
+    check(grb_upload_nets(ctx, &F.n), ctx, "grb_upload_nets");
+    check(grb_set_stats(ctx, 0.0, initial_vias), ctx, "grb_set_stats");
+    int32_t nb = 0;
+    check(grb_plan_batches(ctx, nets2route.data(), int32_t(nets2route.size()), 1000000, state.batch_sparsity_override,
+                           mode == GRB_MODE_PERSISTENT ? GRB_MODE_PERSISTENT : GRB_MODE_PLAIN, nullptr, &nb),
+          ctx, "grb_plan_batches");
+    check(grb_set_stage_tail(ctx, tail ? (GRB_TAIL_RIPUP | GRB_TAIL_VIEW) : 0, 0), ctx, "grb_set_stage_tail");
+    grb_stats st{};
+    check(grb_lshape_stage(ctx, mode, &st), ctx, "grb_lshape_stage");
+    std::vector<int32_t> batch_off(nb + 1);
+    int32_t n = 0, nb2 = 0;
+    check(grb_get_plan(ctx, nets2route.data(), batch_off.data(), &n, &nb2), ctx, "grb_get_plan");
+    const size_t words = size_t(state.device.ROUTE_PER_PIN) * state.device.PIN_NUM + 1;
+    state.routes_cpu.reset(new int[words]());
+    check(grb_read_routes(ctx, state.routes_cpu.get()), ctx, "grb_read_routes");
+    printf("DAG_TIMING stage=lshape batch_index=-1 elapsed_ms=%.6f nets=%zu batches=%d executor=grotor_b200\n",
+           st.dag_ms, nets2route.size(), nb);
+    printf("BATCH_TIMING backend=grotor_b200 elapsed_ms=%.6f nets=%zu batches=%d used_for_routing=1\n",
+           st.batching_ms, nets2route.size(), nb);
+}
+
+// Stage two: Lshape_route_detour::route_detour (flt.cuh:186-192).  The
+// congestion view comes from the stage tail; the host DAG builder is the
+// reference's; batching and route_prepared_topology's batch loop run on
+// grotor_b200.  Leaves the phase-two routes in state.routes_phase2_cpu.
+void flt_stage(cudb::RouterState& state, grb_ctx* ctx, std::vector<int>& nets2route, int32_t mode,
+               std::vector<unsigned char>& cong, std::vector<float>& xsum, std::vector<float>& ysum) {
+    if (nets2route.empty()) return;
+    auto& nets = state.nets;
+    // prepare_detour_topology (flt.cuh:48-73) with the view in host memory.
+    std::sort(nets2route.begin(), nets2route.end(), [&](int l, int r) { return nets[l].hpwl > nets[r].hpwl; });
+    std::unique_ptr<bool[]> view(new bool[cong.size()]);
+    for (size_t i = 0; i < cong.size(); ++i) view[i] = cong[i] != 0;
+    state.packing.congestionView_cpu = view.get();
+    state.packing.congestionView_xsum_cpu = xsum.data();
+    state.packing.congestionView_ysum_cpu = ysum.data();
+    for (int id : nets2route) if (nets[id].rsmt.empty()) nets[id].construct_rsmt(state);
+    state.flt_topology.begin(nets2route, nets.size(), 8);
+    grotor::batching::prepare_geometry(state, nets2route, 8);
+    Lshape_route_detour::multithreaded_processing(state, nets2route);
+    state.packing.congestionView_cpu = nullptr;
+    state.packing.congestionView_xsum_cpu = state.packing.congestionView_ysum_cpu = nullptr;
+    // The FLT DAGs (flt::Topology spans) and batching geometry, by net id.
+    const int count = int(nets.size());
+    std::vector<int> slot_of(count, -1);
+    for (size_t s = 0; s < nets2route.size(); ++s) slot_of[nets2route[s]] = int(s);
+    std::vector<int32_t> node_off{0}, coord, depth, children, parent_end, edge_off{0}, edge_parent, edge_slot;
+    std::vector<int32_t> point_off{0}, points, hseg_off{0}, hsegs, vseg_off{0}, vsegs;
+    std::vector<int64_t> route2_off{0};
+    const auto& topo = state.flt_topology;
+    for (int id = 0; id < count; ++id) {
+        const int s = slot_of[id];
+        if (s >= 0) {
+            const auto& span = topo.spans[s];
+            const auto& arena = topo.arenas[span.lane];
+            for (int i = 0; i < span.nodes; ++i) {
+                const auto& nd = arena.nodes[span.node_begin + i];
+                coord.push_back(nd.coordinate);
+                depth.push_back(nd.depth);
+                children.push_back(nd.children);
+                parent_end.push_back(nd.parent_end);
+            }
+            for (int i = 0; i < span.edges; ++i) {
+                const auto& e = arena.edges[span.edge_begin + i];
+                edge_parent.push_back(e.parent);
+                edge_slot.push_back(e.source_slot);
+            }
+        }
+        node_off.push_back(int32_t(coord.size()));
+        edge_off.push_back(int32_t(edge_parent.size()));
+        const auto& n = nets[id];
+        for (int p : n.points) points.push_back(p);
+        point_off.push_back(int32_t(points.size()));
+        for (const auto& sg : n.rsmt_h_segments) { hsegs.push_back(sg.first); hsegs.push_back(sg.second); }
+        hseg_off.push_back(int32_t(hsegs.size() / 2));
+        for (const auto& sg : n.rsmt_v_segments) { vsegs.push_back(sg.first); vsegs.push_back(sg.second); }
+        vseg_off.push_back(int32_t(vsegs.size() / 2));
+        const int64_t words = s >= 0 ? int64_t(n.pins.size()) * int64_t(state.device.ROUTE_PER_PIN_PHASE2) : 0;
+        route2_off.push_back(route2_off.back() + words);
+    }
+    state.flt_topology.clear();
+    check(grb_upload_geometry(ctx, point_off.data(), points.data(), hseg_off.data(), hsegs.data(), vseg_off.data(),
+                              vsegs.data()),
+          ctx, "grb_upload_geometry");
+    int32_t nb = 0;
+    check(grb_plan_batches(ctx, nets2route.data(), int32_t(nets2route.size()), 300000, state.batch_sparsity_override,
+                           mode == GRB_MODE_PERSISTENT ? GRB_MODE_PERSISTENT : GRB_MODE_PLAIN, nullptr, &nb),
+          ctx, "grb_plan_batches (FLT)");
+    grb_flt_dags d{node_off.data(), coord.data(), depth.data(), children.data(), parent_end.data(),
+                   edge_off.data(), edge_parent.data(), edge_slot.data(), route2_off.data()};
+    check(grb_upload_flt(ctx, &d), ctx, "grb_upload_flt");
+    grb_stats st{};
+    check(grb_flt_stage(ctx, 1, mode, &st), ctx, "grb_flt_stage");
+    const size_t words = size_t(state.device.ROUTE_PER_PIN_PHASE2) * state.device.PIN_NUM_PHASE2 + 1;
+    state.routes_phase2_cpu.reset(new int[std::max<size_t>(words, size_t(route2_off.back()) + 1)]());
+    check(grb_read_routes2(ctx, state.routes_phase2_cpu.get()), ctx, "grb_read_routes2");
+    printf("DAG_TIMING stage=detour batch_index=-1 elapsed_ms=%.6f nets=%zu batches=%d executor=grotor_b200\n",
+           st.dag_ms, nets2route.size(), nb);
+}
+
+// grotor::route (pipeline.hpp:14-157).  The output order is the reference's:
+// single-pin nets, then (after stage one) the nets without overflow, then the
+// rerouted ones.
+void route(cudb::RouterState& state, int32_t mode, bool stop_after_lshape) {
+    cudb::prepare_routing_nets(state);
+    int64_t initial_vias = 0;  // one via per metal1 pin (preprocess.hpp:1716-1718)
+    for (auto& dbnet : db::nets)
+        for (int pin : dbnet.pins) initial_vias += pin < state.device.X * state.device.Y;
+    for (int i = 0; i < int(db::nets.size()); ++i)
+        if (db::nets[i].pins.size() == 1) nets2output.push(i);
+    Grid G = make_grid(state);
+    grb_ctx* ctx = nullptr;
+    check(grb_create(&G.g, 0, &ctx), nullptr, "grb_create");
+    std::unique_ptr<grb_ctx, void (*)(grb_ctx*)> owner(ctx, grb_destroy);
+    std::vector<int> all_nets(state.nets.size());
+    std::iota(all_nets.begin(), all_nets.end(), 0);
+    lshape_stage(state, ctx, all_nets, mode, initial_vias, !stop_after_lshape);
+    if (stop_after_lshape) {
+        graph::finish_nets(state, all_nets);
+        graph::output_nets(state, graph::collect_output_nets(std::move(nets2output)));
+        nets2output = {};
+        return;
+    }
+    // pipeline.hpp:86-106: classification, phase-two offsets (the global
+    // `mode` of runtime.hpp:29 selects the DAG builder's variant for large
+    // designs).
+    if (state.nets.size() > 5000000) ::mode = 1;
+    if (state.nets.size() > 20000000) ::mode = 2;
+    const size_t xy = size_t(state.device.X) * state.device.Y;
+    std::vector<unsigned char> is_of(state.nets.size()), cong(xy);
+    std::vector<float> xsum(xy), ysum(xy);
+    check(grb_read_stage_tail(ctx, is_of.data(), cong.data(), xsum.data(), ysum.data()), ctx, "grb_read_stage_tail");
+    std::vector<int> of_nets, no_of_nets;
+    for (int i = 0; i < int(is_of.size()); ++i) (is_of[i] ? of_nets : no_of_nets).push_back(i);
+    graph::finish_nets(state, no_of_nets);
+    int pin_count = 0;
+    for (int id : of_nets) {
+        state.pin_cnt_sum_phase2_cpu[id] = pin_count;
+        pin_count += int(state.nets[id].pins.size());
+        state.ripup_flag_cpu[id] = 1;
+    }
+    state.device.PIN_NUM_PHASE2 = pin_count;
+    // The nets without overflow are written before stage two, as the
+    // reference's output task does.
+    graph::output_nets(state, graph::collect_output_nets(std::move(nets2output)));
+    nets2output = {};
+    std::vector<int> rerouted = of_nets;
+    flt_stage(state, ctx, rerouted, mode, cong, xsum, ysum);
+    graph::finish_nets(state, of_nets);
+    graph::output_nets(state, graph::collect_output_nets(std::move(nets2output)));
+    nets2output = {};
+}
+
+}  // namespace drop_in
+
+int main(int argc, char** argv) {
+    try {
+        std::string cap, net, output, lut_dir = ".", executor = "persistent";
+        bool stop_after_lshape = false;
+        if (argc < 7 || argc % 2 != 1)
+            throw std::invalid_argument("Usage: grotor_grb -cap FILE -net FILE -out FILE [--lut-dir DIR] "
+                                        "[--executor persistent|plain|graph] [--stop-after lshape|routing]");
+        for (int i = 1; i < argc; i += 2) {
+            const std::string option = argv[i], value = argv[i + 1];
+            if (option == "-cap") cap = value;
+            else if (option == "-net") net = value;
+            else if (option == "-out") output = value;
+            else if (option == "--lut-dir") lut_dir = value;
+            else if (option == "--executor") executor = value;
+            else if (option == "--stop-after") {
+                if (value != "lshape" && value != "routing") throw std::invalid_argument("--stop-after expects lshape or routing");
+                stop_after_lshape = value == "lshape";
+            } else throw std::invalid_argument("Unknown option: " + option);
+        }
+        if (cap.empty() || net.empty() || output.empty()) throw std::invalid_argument("-cap, -net and -out are required");
+        const int32_t mode = drop_in::executor_mode(executor);
+        program_start = std::chrono::high_resolution_clock::now();
+        db::read(cap.data(), net.data());
+        const auto caller_directory = std::filesystem::current_path();
+        std::filesystem::current_path(lut_dir);
+        flute::readLUT();
+        std::filesystem::current_path(caller_directory);
+        out_file = fopen(output.c_str(), "w");
+        if (!out_file) throw std::runtime_error("Cannot open output: " + output);
+        if (setvbuf(out_file, nullptr, _IONBF, 0)) throw std::runtime_error("Cannot configure routing output");
+        {
+            cudb::RouterState state;
+            state.batch_sparsity_override = 1;
+            state.report_score = false;
+            drop_in::route(state, mode, stop_after_lshape);
+        }
+        const int close_status = fclose(out_file);
+        out_file = nullptr;
+        if (close_status) throw std::runtime_error("Failed to close routing output");
+        printf("GROTOR_COMPLETE wall_seconds=%.6f\n", elapsed_time());
+        return EXIT_SUCCESS;
+    } catch (const std::exception& error) {
+        if (out_file) fclose(out_file);
+        fprintf(stderr, "grotor_grb error: %s\n", error.what());
+        return EXIT_FAILURE;
+    }
+}
