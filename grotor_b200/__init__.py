@@ -9,6 +9,6 @@ missing; there is no CPU fallback.  (The package import itself loads nothing,
 so the seeded workload generator, ``grotor_b200.synth``, can be used by a
 process that must not load the routing library.)
 """
-from .router import GrbError, GridArrays, NetArrays, Router, plan_from_batches  # noqa: F401
+from .router import GrbError, GridArrays, NetArrays, Router, TreeArrays, plan_from_batches  # noqa: F401
 
-__all__ = ["GrbError", "GridArrays", "NetArrays", "Router", "plan_from_batches"]
+__all__ = ["GrbError", "GridArrays", "NetArrays", "Router", "TreeArrays", "plan_from_batches"]

@@ -39,6 +39,10 @@ class GrbNets(C.Structure):
     ]
 
 
+class GrbTrees(C.Structure):
+    _fields_ = [("n", C.c_int32), ("node_off", P), ("pos", P), ("adj_off", P), ("adj", P), ("route_off", P)]
+
+
 class GrbStats(C.Structure):
     _fields_ = [
         ("total_wirelength", C.c_double), ("total_via_count", C.c_int64), ("n_batches", C.c_int32),
@@ -75,6 +79,9 @@ SIGNATURES = {
     "grb_stream": (P, [P]),
     "grb_reset": (C.c_int, [P]),
     "grb_upload_nets": (C.c_int, [P, C.POINTER(GrbNets)]),
+    "grb_build_topology": (C.c_int, [P, C.POINTER(GrbTrees)]),
+    "grb_topology_sizes": (C.c_int, [P, P]),
+    "grb_read_topology": (C.c_int, [P] + [P] * 9),
     "grb_plan_batches": (C.c_int, [P, P, C.c_int32, C.c_int32, C.c_int32, C.c_int32, P, C.POINTER(C.c_int32)]),
     "grb_set_plan": (C.c_int, [P, P, C.c_int32, P, C.c_int32]),
     "grb_get_plan": (C.c_int, [P, P, P, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),

@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <climits>
 #include <cstdio>
 #include <cstring>
 #include <memory>
@@ -20,6 +21,7 @@
 #include "device/flt.cuh"
 #include "device/lshape.cuh"
 #include "device/softmin.cuh"
+#include "device/topology.cuh"
 #include "device/zshape.cuh"
 
 using namespace grb;
@@ -633,6 +635,16 @@ __global__ void k_validate_nets(NetCheck C) {
     }
 }
 
+// --- topology construction (topology.cuh) -----------------------------------
+__global__ void k_topo_count(TopoBuild B) {
+    const int id = blockIdx.x * blockDim.x + threadIdx.x;
+    if (id < B.n) topo_count(B, id);
+}
+__global__ void k_topo_fill(TopoBuild B) {
+    const int id = blockIdx.x * blockDim.x + threadIdx.x;
+    if (id < B.n) topo_fill(B, id);
+}
+
 // --- batching kernels -------------------------------------------------------
 // Flat lists: per-position counts (warp per position), exclusive scans, fill.
 __global__ void k_flat_count(BatchState B, int n_nets) {
@@ -999,6 +1011,8 @@ struct grb_ctx {
     // FLT stage (grb_upload_geometry / grb_upload_flt)
     std::vector<void*> geom_bufs;     // batching geometry replacing the uploaded one
     std::vector<void*> flt_bufs;
+    std::vector<void*> topo_bufs;     // grb_build_topology: uploaded trees, counts, DFS stack
+    long long topo_sizes[4] = {-1, 0, 0, 0};  // nodes, points, h-, v-segments of the net store (-1: none)
     Flt F{};
     long long route2_words = 0;
     int flt_n = -1;                   // nets covered by the uploaded DAGs
@@ -1886,6 +1900,7 @@ void grb_destroy(grb_ctx* c) {
     free_all(c->net_bufs);
     free_all(c->geom_bufs);
     free_all(c->flt_bufs);
+    free_all(c->topo_bufs);
     free_all(c->owned);
     for (void* p : {(void*)c->check, (void*)c->bucket_ids, (void*)c->bucket_off, (void*)c->ids, (void*)c->batch_off, (void*)c->gscratch, (void*)c->work, (void*)c->cellmask,
                     (void*)c->lmask[0], (void*)c->lmask[1], (void*)c->lmask[2], (void*)c->ptchunk, (void*)c->fmask, (void*)c->pred, (void*)c->prevp,
@@ -1921,6 +1936,69 @@ int grb_reset(grb_ctx* c) {
     return GRB_OK;
 }
 
+// Device buffers of the net store, reused while every array still fits
+// (need: nets, nodes, route words, points, h-segments, v-segments).
+static int net_buffers(grb_ctx* c, const long long need[6]) {
+    bool fits = !c->net_bufs.empty() && c->geom_bufs.empty();
+    for (int k = 0; k < 6 && fits; ++k) fits = need[k] <= c->net_cap[k];
+    if (fits) return GRB_OK;
+    GRB_CUDA(c, cudaStreamSynchronize(c->stream));
+    free_all(c->net_bufs);
+    free_all(c->geom_bufs);
+    free_all(c->flt_bufs);
+    c->flt_n = -1;
+    const long long n = need[0], nn = need[1], rw = need[2], np = need[3], nh = need[4], nv = need[5];
+    int rc = 0;
+    rc |= dalloc(c, &c->node_off, n + 1, c->net_bufs);
+    rc |= dalloc(c, &c->nodes, nn, c->net_bufs);
+    rc |= dalloc(c, &c->parents, nn, c->net_bufs);
+    rc |= dalloc(c, &c->route_off, n + 1, c->net_bufs);
+    rc |= dalloc(c, &c->routes, rw, c->net_bufs);
+    rc |= dalloc(c, &c->point_off, n + 1, c->net_bufs);
+    rc |= dalloc(c, &c->points, np, c->net_bufs);
+    rc |= dalloc(c, &c->hseg_off, n + 1, c->net_bufs);
+    rc |= dalloc(c, &c->hsegs, 2 * size_t(nh), c->net_bufs);
+    rc |= dalloc(c, &c->vseg_off, n + 1, c->net_bufs);
+    rc |= dalloc(c, &c->vsegs, 2 * size_t(nv), c->net_bufs);
+    if (rc) { free_all(c->net_bufs); return fail(c, GRB_ENOMEM, "net buffers"); }
+    for (int k = 0; k < 6; ++k) c->net_cap[k] = need[k];
+    return GRB_OK;
+}
+
+// Device-side check of the net store just written (every index a stage kernel
+// will dereference); the net count becomes the context's on success.
+static int validate_net_store(grb_ctx* c, int n, int nn, long long rw, int np, int nh, int nv) {
+    int status[3] = {0, 0, 0};
+    if (!c->check) {
+        if (cudaMalloc(&c->check, 3 * sizeof(int)) != cudaSuccess) { cudaGetLastError(); return fail(c, GRB_ENOMEM, "validation status"); }
+    }
+    GRB_CUDA(c, cudaMemsetAsync(c->check, 0, 3 * sizeof(int), c->stream));
+    NetCheck C{c->node_off, c->nodes, c->parents, c->route_off, c->point_off, c->points, c->hseg_off, c->hsegs,
+               c->vseg_off, c->vsegs, n, nn, np, nh, nv, c->T.XY, c->T.L, rw, c->check};
+    k_validate_nets<<<c->sms * 4, 256, 0, c->stream>>>(C);
+    c->launches += 1;
+    GRB_CUDA(c, cudaGetLastError());
+    GRB_CUDA(c, cudaMemcpyAsync(status, c->check, 3 * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    GRB_CUDA(c, cudaStreamSynchronize(c->stream));
+    c->flt_n = -1;  // FLT DAGs and Z-shape trees refer to the previous nets
+    c->z_n = -1;
+    if (status[0]) {
+        static const char* what[] = {"", "offsets must be non-decreasing and within the arrays", "tree node outside the grid",
+                                     "parents must precede children", "batching geometry outside the grid"};
+        c->n_nets = 0;  // no net id is accepted until a valid upload
+        c->topo_sizes[0] = -1;
+        return fail(c, GRB_EINVAL, std::string(what[status[0]]) + " (item " + std::to_string(status[1]) + ")");
+    }
+    c->n_nets = n;
+    c->max_nodes = status[2];
+    c->route_words = rw;
+    c->topo_sizes[0] = nn;
+    c->topo_sizes[1] = np;
+    c->topo_sizes[2] = nh;
+    c->topo_sizes[3] = nv;
+    return GRB_OK;
+}
+
 int grb_upload_nets(grb_ctx* c, const grb_nets* nets) {
     if (!c || !nets || nets->n < 0 || !nets->node_off || !nets->route_off) return c ? fail(c, GRB_EINVAL, "bad nets") : GRB_EINVAL;
     GRB_CUDA(c, cudaSetDevice(c->device));
@@ -1938,31 +2016,8 @@ int grb_upload_nets(grb_ctx* c, const grb_nets* nets) {
     if (nn < 0 || rw < 0 || np < 0 || nh < 0 || nv < 0) return fail(c, GRB_EINVAL, "negative totals");
     if ((nn && (!nets->nodes || !nets->parents)) || (np && !nets->points) || (nh && !nets->hsegs) || (nv && !nets->vsegs))
         return fail(c, GRB_EINVAL, "net arrays missing");
-    // Reuse the device buffers when every array still fits.
     const long long need[6] = {n, nn, rw, np, nh, nv};
-    bool fits = !c->net_bufs.empty() && c->geom_bufs.empty();
-    for (int k = 0; k < 6 && fits; ++k) fits = need[k] <= c->net_cap[k];
-    if (!fits) {
-        GRB_CUDA(c, cudaStreamSynchronize(c->stream));
-        free_all(c->net_bufs);
-        free_all(c->geom_bufs);
-        free_all(c->flt_bufs);
-        c->flt_n = -1;
-        int rc = 0;
-        rc |= dalloc(c, &c->node_off, n + 1, c->net_bufs);
-        rc |= dalloc(c, &c->nodes, nn, c->net_bufs);
-        rc |= dalloc(c, &c->parents, nn, c->net_bufs);
-        rc |= dalloc(c, &c->route_off, n + 1, c->net_bufs);
-        rc |= dalloc(c, &c->routes, rw, c->net_bufs);
-        rc |= dalloc(c, &c->point_off, n + 1, c->net_bufs);
-        rc |= dalloc(c, &c->points, np, c->net_bufs);
-        rc |= dalloc(c, &c->hseg_off, n + 1, c->net_bufs);
-        rc |= dalloc(c, &c->hsegs, 2 * size_t(nh), c->net_bufs);
-        rc |= dalloc(c, &c->vseg_off, n + 1, c->net_bufs);
-        rc |= dalloc(c, &c->vsegs, 2 * size_t(nv), c->net_bufs);
-        if (rc) { free_all(c->net_bufs); return GRB_ENOMEM; }
-        for (int k = 0; k < 6; ++k) c->net_cap[k] = need[k];
-    }
+    if (int rc = net_buffers(c, need)) return rc;
     auto h2d = [&](void* dst, const void* src, size_t bytes) {
         return src && bytes ? cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, c->stream) : cudaSuccess;
     };
@@ -1980,34 +2035,133 @@ int grb_upload_nets(grb_ctx* c, const grb_nets* nets) {
     if (nets->vseg_off) GRB_CUDA(c, h2d(c->vseg_off, nets->vseg_off, sizeof(int) * (n + 1)));
     else GRB_CUDA(c, cudaMemsetAsync(c->vseg_off, 0, sizeof(int) * (n + 1), c->stream));
     GRB_CUDA(c, h2d(c->vsegs, nets->vsegs, sizeof(int) * 2 * nv));
-    // Device-side validation; host buffers may be pageable and short-lived: the
-    // copies complete before return.
-    int status[3] = {0, 0, 0};
-    if (!c->check) {
-        if (cudaMalloc(&c->check, 3 * sizeof(int)) != cudaSuccess) { cudaGetLastError(); return fail(c, GRB_ENOMEM, "validation status"); }
+    // Host buffers may be pageable and short-lived: the validation's
+    // synchronisation completes the copies before return.
+    return validate_net_store(c, n, nn, rw, np, nh, nv);
+}
+
+int grb_build_topology(grb_ctx* c, const grb_trees* t) {
+    if (!c || !t || t->n < 0 || !t->node_off || !t->route_off || !t->adj_off)
+        return c ? fail(c, GRB_EINVAL, "bad trees") : GRB_EINVAL;
+    GRB_CUDA(c, cudaSetDevice(c->device));
+    const int n = t->n;
+    if (t->node_off[0] != 0 || t->route_off[0] != 0 || t->adj_off[0] != 0)
+        return fail(c, GRB_EINVAL, "offsets must start at 0");
+    const long long nn = t->node_off[n], rw = t->route_off[n];
+    if (nn < 0 || nn > (1ll << 30) || rw < 0) return fail(c, GRB_EINVAL, "bad totals");
+    const long long na = t->adj_off[nn];
+    if (na < 0 || (nn && !t->pos) || (na && !t->adj)) return fail(c, GRB_EINVAL, "tree arrays missing");
+    // Uploaded trees, per-net counts and the DFS stack (freed after the build).
+    free_all(c->topo_bufs);
+    int *d_node_off = nullptr, *d_pos = nullptr, *d_adj_off = nullptr, *d_adj = nullptr, *d_stack = nullptr,
+        *d_status = nullptr;
+    long long *d_cnt = nullptr, *d_sums = nullptr;
+    const int tiles = (n + kScanTile - 1) / kScanTile;
+    int rc = 0;
+    rc |= dalloc(c, &d_node_off, n + 1, c->topo_bufs);
+    rc |= dalloc(c, &d_pos, std::max(nn, 1ll), c->topo_bufs);
+    rc |= dalloc(c, &d_adj_off, nn + 1, c->topo_bufs);
+    rc |= dalloc(c, &d_adj, std::max(na, 1ll), c->topo_bufs);
+    rc |= dalloc(c, &d_stack, 4 * std::max(nn, 1ll), c->topo_bufs);
+    rc |= dalloc(c, &d_status, 2, c->topo_bufs);
+    rc |= dalloc(c, &d_cnt, 3 * (size_t(n) + 1), c->topo_bufs);
+    rc |= dalloc(c, &d_sums, 3 * (size_t(tiles) + 1), c->topo_bufs);
+    if (rc) { free_all(c->topo_bufs); return fail(c, GRB_ENOMEM, "topology scratch"); }
+    auto h2d = [&](void* dst, const void* src, size_t bytes) {
+        return bytes ? cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, c->stream) : cudaSuccess;
+    };
+    GRB_CUDA(c, h2d(d_node_off, t->node_off, sizeof(int) * (n + 1)));
+    GRB_CUDA(c, h2d(d_pos, t->pos, sizeof(int) * nn));
+    GRB_CUDA(c, h2d(d_adj_off, t->adj_off, sizeof(int) * (nn + 1)));
+    GRB_CUDA(c, h2d(d_adj, t->adj, sizeof(int) * na));
+    GRB_CUDA(c, cudaMemsetAsync(d_status, 0, 2 * sizeof(int), c->stream));
+    TopoBuild B{n, c->T.X, c->T.Y, c->T.L, nn, na, d_node_off, d_pos, d_adj_off, d_adj,
+                {d_cnt, d_cnt + n + 1, d_cnt + 2 * (n + 1)}};
+    B.stack = d_stack;
+    B.seen = d_stack + 3 * nn;
+    B.status = d_status;
+    const int grid = std::max(1, (n + 255) / 256);
+    if (n) k_topo_count<<<grid, 256, 0, c->stream>>>(B);
+    for (int k = 0; k < 3; ++k) {
+        long long* sums = d_sums + k * (tiles + 1);
+        if (n) k_scan_tiles<<<tiles, 256, 0, c->stream>>>(B.cnt[k], n, sums);
+        k_scan_sums<<<1, 1024, 0, c->stream>>>(sums, tiles);
+        k_scan_add<<<n / 256 + 1, 256, 0, c->stream>>>(B.cnt[k], n, sums, tiles);
     }
-    GRB_CUDA(c, cudaMemsetAsync(c->check, 0, 3 * sizeof(int), c->stream));
-    NetCheck C{c->node_off, c->nodes, c->parents, c->route_off, c->point_off, c->points, c->hseg_off, c->hsegs,
-               c->vseg_off, c->vsegs, n, nn, np, nh, nv, c->T.XY, c->T.L, rw, c->check};
-    k_validate_nets<<<c->sms * 4, 256, 0, c->stream>>>(C);
-    c->launches += 1;
+    c->launches += (n ? 1 : 0) + 3 * (n ? 3 : 2);
     GRB_CUDA(c, cudaGetLastError());
-    GRB_CUDA(c, cudaMemcpyAsync(status, c->check, 3 * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    long long tot[3] = {0, 0, 0};
+    int status[2] = {0, 0};
+    for (int k = 0; k < 3; ++k)
+        GRB_CUDA(c, cudaMemcpyAsync(tot + k, B.cnt[k] + n, sizeof(long long), cudaMemcpyDeviceToHost, c->stream));
+    GRB_CUDA(c, cudaMemcpyAsync(status, d_status, sizeof(status), cudaMemcpyDeviceToHost, c->stream));
     GRB_CUDA(c, cudaStreamSynchronize(c->stream));
+    static const char* what[] = {"", "tree adjacency outside its net", "tree node outside the grid",
+                                 "adjacency is not a tree on the net's nodes"};
     if (status[0]) {
-        static const char* what[] = {"", "offsets must be non-decreasing and within the arrays", "tree node outside the grid",
-                                     "parents must precede children", "batching geometry outside the grid"};
-        c->n_nets = 0;  // no net id is accepted until a valid upload
-        c->flt_n = -1;
-        c->z_n = -1;
-        return fail(c, GRB_EINVAL, std::string(what[status[0]]) + " (item " + std::to_string(status[1]) + ")");
+        free_all(c->topo_bufs);
+        c->n_nets = 0;
+        return fail(c, GRB_EINVAL, std::string(what[status[0]]) + " (net " + std::to_string(status[1]) + ")");
     }
-    const long long maxn = status[2];
-    c->n_nets = n;
-    c->max_nodes = int(maxn);
-    c->route_words = rw;
-    c->flt_n = -1;  // FLT DAGs and Z-shape trees refer to the previous nets
-    c->z_n = -1;
+    if (tot[0] > INT_MAX || 2 * tot[1] > INT_MAX || 2 * tot[2] > INT_MAX) {
+        free_all(c->topo_bufs);
+        return fail(c, GRB_EINVAL, "geometry exceeds 2^31 entries");
+    }
+    const long long need[6] = {n, nn, rw, tot[0], tot[1], tot[2]};
+    if (int e = net_buffers(c, need)) { free_all(c->topo_bufs); return e; }
+    GRB_CUDA(c, cudaMemcpyAsync(c->node_off, d_node_off, sizeof(int) * (n + 1), cudaMemcpyDeviceToDevice, c->stream));
+    GRB_CUDA(c, h2d(c->route_off, t->route_off, sizeof(long long) * (n + 1)));
+    GRB_CUDA(c, cudaMemsetAsync(c->routes, 0, sizeof(int) * std::max<long long>(rw, 1), c->stream));
+    B.nodes = c->nodes;
+    B.parents = c->parents;
+    B.point_off = c->point_off; B.points = c->points;
+    B.hseg_off = c->hseg_off; B.hsegs = c->hsegs;
+    B.vseg_off = c->vseg_off; B.vsegs = c->vsegs;
+    if (n) {
+        GRB_CUDA(c, cudaMemsetAsync(B.seen, 0, sizeof(int) * std::max(nn, 1ll), c->stream));
+        k_topo_fill<<<grid, 256, 0, c->stream>>>(B);
+        c->launches += 1;
+    } else {
+        GRB_CUDA(c, cudaMemsetAsync(c->point_off, 0, sizeof(int), c->stream));
+        GRB_CUDA(c, cudaMemsetAsync(c->hseg_off, 0, sizeof(int), c->stream));
+        GRB_CUDA(c, cudaMemsetAsync(c->vseg_off, 0, sizeof(int), c->stream));
+    }
+    GRB_CUDA(c, cudaGetLastError());
+    GRB_CUDA(c, cudaMemcpyAsync(status, d_status, sizeof(status), cudaMemcpyDeviceToHost, c->stream));
+    GRB_CUDA(c, cudaStreamSynchronize(c->stream));
+    free_all(c->topo_bufs);
+    if (status[0]) {
+        c->n_nets = 0;
+        return fail(c, GRB_EINVAL, std::string(what[status[0]]) + " (net " + std::to_string(status[1]) + ")");
+    }
+    return validate_net_store(c, n, int(nn), rw, int(tot[0]), int(tot[1]), int(tot[2]));
+}
+
+int grb_topology_sizes(grb_ctx* c, int64_t* sizes) {
+    if (!c || !sizes) return c ? fail(c, GRB_EINVAL, "null") : GRB_EINVAL;
+    for (int k = 0; k < 4; ++k) sizes[k] = c->topo_sizes[k];
+    return GRB_OK;
+}
+
+int grb_read_topology(grb_ctx* c, int32_t* node_off, int32_t* nodes, int32_t* parents, int32_t* point_off,
+                      int32_t* points, int32_t* hseg_off, int32_t* hsegs, int32_t* vseg_off, int32_t* vsegs) {
+    if (!c) return GRB_EINVAL;
+    if (c->topo_sizes[0] < 0) return fail(c, GRB_EINVAL, "no nets");
+    GRB_CUDA(c, cudaSetDevice(c->device));
+    const size_t n1 = size_t(c->n_nets) + 1;
+    auto d2h = [&](void* dst, const void* src, size_t bytes) {
+        return dst && bytes ? cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, c->stream) : cudaSuccess;
+    };
+    GRB_CUDA(c, d2h(node_off, c->node_off, 4 * n1));
+    GRB_CUDA(c, d2h(nodes, c->nodes, 4 * size_t(c->topo_sizes[0])));
+    GRB_CUDA(c, d2h(parents, c->parents, 4 * size_t(c->topo_sizes[0])));
+    GRB_CUDA(c, d2h(point_off, c->point_off, 4 * n1));
+    GRB_CUDA(c, d2h(points, c->points, 4 * size_t(c->topo_sizes[1])));
+    GRB_CUDA(c, d2h(hseg_off, c->hseg_off, 4 * n1));
+    GRB_CUDA(c, d2h(hsegs, c->hsegs, 8 * size_t(c->topo_sizes[2])));
+    GRB_CUDA(c, d2h(vseg_off, c->vseg_off, 4 * n1));
+    GRB_CUDA(c, d2h(vsegs, c->vsegs, 8 * size_t(c->topo_sizes[3])));
+    GRB_CUDA(c, cudaStreamSynchronize(c->stream));
     return GRB_OK;
 }
 

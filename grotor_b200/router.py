@@ -95,6 +95,26 @@ class NetArrays:
         return _abi.GrbNets(self.n, *[_p(a) for a in self._keep])
 
 
+@dataclass
+class TreeArrays:
+    """Steiner trees of every net (grb_trees): node positions with their
+    layer (L = Steiner point) and each node's adjacency list."""
+    node_off: np.ndarray
+    pos: np.ndarray
+    adj_off: np.ndarray
+    adj: np.ndarray
+    route_off: np.ndarray
+
+    @property
+    def n(self) -> int:
+        return len(self.node_off) - 1
+
+    def struct(self) -> _abi.GrbTrees:
+        self._keep = [_c(self.node_off, np.int32), _c(self.pos, np.int32), _c(self.adj_off, np.int32),
+                      _c(self.adj, np.int32), _c(self.route_off, np.int64)]
+        return _abi.GrbTrees(self.n, *[_p(a) for a in self._keep])
+
+
 class Router:
     """One routing context on one GPU (owns device memory and a CUDA stream)."""
 
@@ -107,6 +127,8 @@ class Router:
         if rc:
             raise GrbError(rc, "grb_create failed")
         self.nets: NetArrays | None = None
+        self._n = 0            # nets in the context's store
+        self._route_words = 0  # route words of the store
 
     # -- lifecycle ---------------------------------------------------------
     def close(self):
@@ -145,6 +167,35 @@ class Router:
         s = nets.struct()
         self._check(self._lib.grb_upload_nets(self._ctx, C.byref(s)))
         self.nets = nets
+        self._n = nets.n
+        self._route_words = int(nets.route_off[-1])
+
+    def build_topology(self, trees: "TreeArrays"):
+        """Build every net's DP tree and batching geometry on the device from
+        its Steiner tree (grb_build_topology)."""
+        s = trees.struct()
+        self._check(self._lib.grb_build_topology(self._ctx, C.byref(s)))
+        self.nets = None
+        self._n = trees.n
+        self._route_words = int(trees.route_off[-1])
+
+    def _n_nets(self) -> int:
+        return self._n
+
+    def read_topology(self) -> dict:
+        """The context's net store: trees in DFS order and batching geometry."""
+        sizes = np.zeros(4, np.int64)
+        self._check(self._lib.grb_topology_sizes(self._ctx, _p(sizes)))
+        n1 = self._n_nets() + 1
+        nn, npt, nh, nv = (int(v) for v in sizes)
+        out = {"node_off": np.empty(n1, np.int32), "nodes": np.empty(nn, np.int32),
+               "parents": np.empty(nn, np.int32), "point_off": np.empty(n1, np.int32),
+               "points": np.empty(npt, np.int32), "hseg_off": np.empty(n1, np.int32),
+               "hsegs": np.empty(2 * nh, np.int32), "vseg_off": np.empty(n1, np.int32),
+               "vsegs": np.empty(2 * nv, np.int32)}
+        self._check(self._lib.grb_read_topology(self._ctx, *(_p(out[k]) for k in (
+            "node_off", "nodes", "parents", "point_off", "points", "hseg_off", "hsegs", "vseg_off", "vsegs"))))
+        return out
 
     # -- batching ------------------------------------------------------------
     def generate_batches_rsmt(self, order, limit: int = 1000000, sparsity: int = 1, mode="persistent"):
@@ -250,7 +301,7 @@ class Router:
         return _stats_dict(st)
 
     def ripup(self, threshold: int = 0) -> np.ndarray:
-        out = np.zeros(self.nets.n if self.nets else 0, np.uint8)
+        out = np.zeros(self._n, np.uint8)
         self._check(self._lib.grb_ripup_classify(self._ctx, int(threshold), _p(out)))
         return out
 
@@ -259,7 +310,7 @@ class Router:
         (for callers under a fixed device-memory budget or in loops that must
         not allocate); see grb_ripup_classify_noalloc in include/grb.h for the
         size limits and the rule that overlapping calls race."""
-        out = np.zeros(self.nets.n if self.nets else 0, np.uint8)
+        out = np.zeros(self._n, np.uint8)
         self._check(self._lib.grb_ripup_classify_noalloc(self._ctx, int(threshold), _p(out)))
         return out
 
@@ -284,7 +335,7 @@ class Router:
         parts not computed)."""
         flags = getattr(self, "_tail", 0)
         xy = self.grid.X * self.grid.Y
-        is_of = np.zeros(self.nets.n if self.nets else 0, np.uint8) if flags & _abi.GRB_TAIL_RIPUP else None
+        is_of = np.zeros(self._n, np.uint8) if flags & _abi.GRB_TAIL_RIPUP else None
         view = (np.empty(xy, np.uint8), np.empty(xy, np.float32), np.empty(xy, np.float32)) \
             if flags & _abi.GRB_TAIL_VIEW else None
         self._check(self._lib.grb_read_stage_tail(self._ctx, _p(is_of), *(_p(v) for v in (view or (None,) * 3))))
@@ -304,7 +355,7 @@ class Router:
         """All route words (route_off order).  ``out`` may be a caller-owned
         int32 buffer of at least that many words (pinned host memory makes the
         copy run at full PCIe rate)."""
-        words = int(self.nets.route_off[-1]) if self.nets is not None else 0
+        words = self._route_words
         if out is None:
             out = np.zeros(words, np.int32)
         elif out.dtype != np.int32 or not out.flags.c_contiguous or out.size < words:

@@ -148,3 +148,45 @@ def _arr(ptr, ctype, count):
         return np.zeros(0, np.dtype(ctype))
     addr = ptr.value if isinstance(ptr, C.c_void_p) else ptr
     return np.ctypeslib.as_array(C.cast(addr, C.POINTER(ctype)), shape=(count,))
+
+
+def steiner_trees(nets: NetArrays, shuffle_seed: int | None = None):
+    """The nets' trees in the form FLUTE leaves them (grb_trees): node
+    positions and adjacency lists, from the depth-first arrays.
+
+    Without a seed every node lists its parent first and then its children by
+    index, so the depth-first flattening from node 0 gives the arrays back.
+    With a seed the nodes of every net are relabelled (node 0 included, which
+    re-roots the tree) and every adjacency list is shuffled."""
+    from .router import TreeArrays
+    node_off = np.asarray(nets.node_off, np.int64)
+    n, nn = len(node_off) - 1, int(node_off[-1])
+    net_of = np.repeat(np.arange(n, dtype=np.int64), np.diff(node_off))
+    local = np.arange(nn, dtype=np.int64) - node_off[net_of]
+    parents = np.asarray(nets.parents, np.int64)
+    if shuffle_seed is None:
+        new_of_old = np.arange(nn, dtype=np.int64)
+    else:
+        rng = np.random.default_rng(shuffle_seed)
+        order = np.lexsort((rng.random(nn), net_of))
+        new_of_old = np.empty(nn, np.int64)
+        new_of_old[order] = np.arange(nn, dtype=np.int64)
+    pos = np.empty(nn, np.int32)
+    pos[new_of_old] = np.asarray(nets.nodes, np.int32)
+    child = np.flatnonzero(local > 0)
+    par = node_off[net_of[child]] + parents[child]
+    a, b = new_of_old[child], new_of_old[par]
+    src = np.concatenate([a, b])
+    dst = np.concatenate([b, a])
+    if shuffle_seed is None:
+        # Parent entries first (key -1), then children by their index.
+        key = np.concatenate([np.full(len(a), -1, np.int64), a])
+        perm = np.lexsort((key, src))
+    else:
+        perm = np.lexsort((rng.random(len(src)), src))
+    src, dst = src[perm], dst[perm]
+    adj_off = np.zeros(nn + 1, np.int64)
+    np.add.at(adj_off, src + 1, 1)
+    adj_off = np.cumsum(adj_off).astype(np.int32)
+    adj = (dst - node_off[net_of[dst]]).astype(np.int32)
+    return TreeArrays(np.asarray(nets.node_off, np.int32), pos, adj_off, adj, np.asarray(nets.route_off, np.int64))

@@ -101,6 +101,34 @@ int grb_reset(grb_ctx* ctx);
  * Lshape_route, lshape.cuh:126-138, and the batching inputs). */
 int grb_upload_nets(grb_ctx* ctx, const grb_nets* nets);
 
+/* Every net's Steiner tree as FLUTE leaves it in net::rsmt after
+ * construct_rsmt (preprocess.hpp:72-93 and 124-126): the node positions
+ * (layer * X*Y + x*Y + y; layer L marks a Steiner point) and each node's
+ * adjacency list (net-local node indices, in net::rsmt order). */
+typedef struct grb_trees {
+    int32_t n;
+    const int32_t* node_off;   /* [n+1] */
+    const int32_t* pos;        /* [node_off[n]] */
+    const int32_t* adj_off;    /* [node_off[n]+1] offsets into adj */
+    const int32_t* adj;        /* neighbours, net-local indices */
+    const int64_t* route_off;  /* [n+1] as in grb_nets */
+} grb_trees;
+
+/* Topology construction on the device: from the trees, every net's DP tree
+ * (the depth-first flattening of Lshape_route, lshape.cuh:85-98) and batching
+ * geometry (net::points, rsmt_h_segments, rsmt_v_segments of construct_rsmt,
+ * preprocess.hpp:95-123) are built on the GPU, in the same order as the
+ * reference's host code; the context then holds the same nets as after
+ * grb_upload_nets of the host-built arrays.  GRB_EINVAL if a net's adjacency
+ * is not a tree on its nodes or a position is outside the grid. */
+int grb_build_topology(grb_ctx* ctx, const grb_trees* trees);
+/* Sizes of the context's net store: nodes, points, h-segments, v-segments. */
+int grb_topology_sizes(grb_ctx* ctx, int64_t* sizes);
+/* Copy the net store out (node_off, point_off, hseg_off, vseg_off: n+1
+ * entries; segments as pairs); any pointer may be NULL. */
+int grb_read_topology(grb_ctx* ctx, int32_t* node_off, int32_t* nodes, int32_t* parents, int32_t* point_off,
+                      int32_t* points, int32_t* hseg_off, int32_t* hsegs, int32_t* vseg_off, int32_t* vsegs);
+
 /* Exact first-fit batching of nets `order[0..n)` with at most `limit` nets per
  * batch (cudb::generate_batches_rsmt, generate_batches_cpu.hpp:7-73, and its
  * RT-core replacements).  The result becomes the context's plan in execution

@@ -9,11 +9,14 @@
 // ABI of include/grb.h):
 //
 //   * stage one, Lshape_route (src/routing/lshape.cuh:21-197): the reference's
-//     host code builds the FLUTE trees and the HPWL order as before; first-fit
-//     batching (generate_batches_cpu_timed), the per-batch cost refresh, the
-//     L-shape DP and the demand commit run in grb_plan_batches +
-//     grb_lshape_stage, whose stage tail also computes the congestion view and
-//     the rip-up classification the pipeline needs next (pipeline.hpp:86-93);
+//     host code builds the FLUTE trees and the HPWL order as before; the
+//     trees' batching geometry and depth-first flattening (construct_rsmt's
+//     geometry, lshape.cuh:85-98) are built on the device by
+//     grb_build_topology; first-fit batching (generate_batches_cpu_timed),
+//     the per-batch cost refresh, the L-shape DP and the demand commit run in
+//     grb_plan_batches + grb_lshape_stage, whose stage tail also computes the
+//     congestion view and the rip-up classification the pipeline needs next
+//     (pipeline.hpp:86-93);
 //   * stage two, Lshape_route_detour::route_detour (src/routing/flt.cuh:
 //     186-192): the reference's host FLT DAG builder (process_net,
 //     flt.cuh:8-46) runs unchanged on the congestion view; batching and the
@@ -74,56 +77,41 @@ Grid make_grid(const cudb::RouterState& state) {
     return G;
 }
 
-// Every net's tree in the depth-first order of Lshape_route (node 0 = root,
-// parents before children; lshape.cuh:85-103), its batching geometry
-// (net::points and the RSMT segments), and its route words at the reference's
-// own offsets (pin_cnt_sum_cpu * ROUTE_PER_PIN, router_state.hpp:31) -- all by
-// net id.
-struct Nets {
-    std::vector<int32_t> node_off{0}, nodes, parents, point_off{0}, points, hseg_off{0}, hsegs, vseg_off{0}, vsegs;
+// Every net's Steiner tree as FLUTE leaves it in net::rsmt (node positions
+// with their layer, then each node's adjacency list; preprocess.hpp:72-93,
+// 124-126) and its route words at the reference's own offsets
+// (pin_cnt_sum_cpu * ROUTE_PER_PIN, router_state.hpp:31) -- all by net id.
+// grb_build_topology turns them into the depth-first trees of Lshape_route
+// (lshape.cuh:85-98) and the batching geometry of construct_rsmt
+// (preprocess.hpp:95-123) on the device.
+struct Trees {
+    std::vector<int32_t> node_off{0}, pos, adj_off{0}, adj;
     std::vector<int64_t> route_off;
-    grb_nets n{};
+    grb_trees t{};
 };
 
-Nets flatten_nets(const cudb::RouterState& state) {
-    Nets F;
+Trees flatten_trees(const cudb::RouterState& state) {
+    Trees F;
     const auto& nets = state.nets;
     const int count = int(nets.size());
     for (int id = 0; id < count; ++id) {
         const auto& graph = nets[id].rsmt;
-        const size_t base = F.nodes.size();
         const size_t size = graph.empty() ? 0 : graph.back().size();
-        F.nodes.resize(base + size);
-        F.parents.resize(base + size);
-        int next = 0;
-        std::function<void(int, int, int)> dfs = [&](int x, int par, int par_node) {
-            const int idx = next++;
-            F.nodes[base + idx] = graph.back()[x];
-            F.parents[base + idx] = par_node;
-            for (int e : graph[x]) if (e != par) dfs(e, x, idx);
-        };
-        if (size) dfs(0, -1, -1);
-        F.node_off.push_back(int32_t(F.nodes.size()));
-        for (int p : nets[id].points) F.points.push_back(p);
-        F.point_off.push_back(int32_t(F.points.size()));
-        for (const auto& s : nets[id].rsmt_h_segments) { F.hsegs.push_back(s.first); F.hsegs.push_back(s.second); }
-        F.hseg_off.push_back(int32_t(F.hsegs.size() / 2));
-        for (const auto& s : nets[id].rsmt_v_segments) { F.vsegs.push_back(s.first); F.vsegs.push_back(s.second); }
-        F.vseg_off.push_back(int32_t(F.vsegs.size() / 2));
+        for (size_t i = 0; i < size; ++i) {
+            F.pos.push_back(graph.back()[i]);
+            F.adj.insert(F.adj.end(), graph[i].begin(), graph[i].end());
+            F.adj_off.push_back(int32_t(F.adj.size()));
+        }
+        F.node_off.push_back(int32_t(F.pos.size()));
     }
     for (int id = 0; id <= count; ++id)
         F.route_off.push_back(int64_t(state.pin_cnt_sum_cpu[id]) * int64_t(state.device.ROUTE_PER_PIN));
-    F.n.n = count;
-    F.n.node_off = F.node_off.data();
-    F.n.nodes = F.nodes.data();
-    F.n.parents = F.parents.data();
-    F.n.route_off = F.route_off.data();
-    F.n.point_off = F.point_off.data();
-    F.n.points = F.points.data();
-    F.n.hseg_off = F.hseg_off.data();
-    F.n.hsegs = F.hsegs.data();
-    F.n.vseg_off = F.vseg_off.data();
-    F.n.vsegs = F.vsegs.data();
+    F.t.n = count;
+    F.t.node_off = F.node_off.data();
+    F.t.pos = F.pos.data();
+    F.t.adj_off = F.adj_off.data();
+    F.t.adj = F.adj.data();
+    F.t.route_off = F.route_off.data();
     return F;
 }
 
@@ -140,11 +128,16 @@ int32_t executor_mode(const std::string& name) {
 void lshape_stage(cudb::RouterState& state, grb_ctx* ctx, std::vector<int>& nets2route, int32_t mode,
                   int64_t initial_vias, bool tail) {
     auto& nets = state.nets;
+    const auto topology_start = std::chrono::steady_clock::now();
+    // FLUTE only (construct_rsmt's rsmt_only form); the geometry and the
+    // depth-first trees are built on the device.
 #pragma omp parallel for num_threads(8)
-    for (int i = 0; i < int(nets2route.size()); ++i) nets[nets2route[i]].construct_rsmt(state, false);
+    for (int i = 0; i < int(nets2route.size()); ++i) nets[nets2route[i]].construct_rsmt(state, true);
+    Trees F = flatten_trees(state);
+    check(grb_build_topology(ctx, &F.t), ctx, "grb_build_topology");
+    printf("TOPOLOGY_TIMING stage=lshape elapsed_ms=%.6f geometry_fused=0 executor=grotor_b200\n",
+           std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - topology_start).count());
     std::sort(nets2route.begin(), nets2route.end(), [&](int l, int r) { return nets[l].hpwl > nets[r].hpwl; });
-    Nets F = flatten_nets(state);
-    check(grb_upload_nets(ctx, &F.n), ctx, "grb_upload_nets");
     check(grb_set_stats(ctx, 0.0, initial_vias), ctx, "grb_set_stats");
     int32_t nb = 0;
     check(grb_plan_batches(ctx, nets2route.data(), int32_t(nets2route.size()), 1000000, state.batch_sparsity_override,
@@ -175,6 +168,13 @@ void flt_stage(cudb::RouterState& state, grb_ctx* ctx, std::vector<int>& nets2ro
     auto& nets = state.nets;
     // prepare_detour_topology (flt.cuh:48-73) with the view in host memory.
     std::sort(nets2route.begin(), nets2route.end(), [&](int l, int r) { return nets[l].hpwl > nets[r].hpwl; });
+    // The FLT builder keeps a net's stage-one RSMT segments (it runs with
+    // construct_segments = false, flt.cuh:20); stage one built them on the
+    // device, so the rerouted nets get them on the host here, from the same
+    // trees (construct_rsmt is a pure function of net::rsmt and the pins).
+#pragma omp parallel for num_threads(8)
+    for (int i = 0; i < int(nets2route.size()); ++i)
+        if (!nets[nets2route[i]].rsmt.empty()) nets[nets2route[i]].construct_rsmt(state, false);
     std::unique_ptr<bool[]> view(new bool[cong.size()]);
     for (size_t i = 0; i < cong.size(); ++i) view[i] = cong[i] != 0;
     state.packing.congestionView_cpu = view.get();
@@ -242,6 +242,8 @@ void flt_stage(cudb::RouterState& state, grb_ctx* ctx, std::vector<int>& nets2ro
     check(grb_read_routes2(ctx, state.routes_phase2_cpu.get()), ctx, "grb_read_routes2");
     printf("DAG_TIMING stage=detour batch_index=-1 elapsed_ms=%.6f nets=%zu batches=%d executor=grotor_b200\n",
            st.dag_ms, nets2route.size(), nb);
+    printf("BATCH_TIMING stage=detour backend=grotor_b200 elapsed_ms=%.6f nets=%zu batches=%d used_for_routing=1\n",
+           st.batching_ms, nets2route.size(), nb);
 }
 
 // grotor::route (pipeline.hpp:14-157).  The output order is the reference's:
@@ -290,8 +292,9 @@ void route(cudb::RouterState& state, int32_t mode, bool stop_after_lshape) {
     // reference's output task does.
     graph::output_nets(state, graph::collect_output_nets(std::move(nets2output)));
     nets2output = {};
-    std::vector<int> rerouted = of_nets;
-    flt_stage(state, ctx, rerouted, mode, cong, xsum, ysum);
+    // Stage two sorts of_nets in place (flt.cuh:52), and the reference
+    // publishes the rerouted nets in that order (pipeline.hpp:137,143).
+    flt_stage(state, ctx, of_nets, mode, cong, xsum, ysum);
     graph::finish_nets(state, of_nets);
     graph::output_nets(state, graph::collect_output_nets(std::move(nets2output)));
     nets2output = {};

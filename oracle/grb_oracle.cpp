@@ -6,6 +6,7 @@
 #include "grb_oracle.h"
 
 #include <algorithm>
+#include <functional>
 #include <atomic>
 #include <cmath>
 #include <cstring>
@@ -1264,6 +1265,75 @@ int32_t orc_bbox_batches(int32_t X, int32_t Y, int32_t n, const int32_t* group, 
         off[++nb] = out;
     }
     return nb;
+}
+
+// construct_rsmt's geometry (preprocess.hpp:95-123) and Lshape_route's
+// recursive depth-first flattening (lshape.cuh:85-98), net by net.
+int orc_build_topology(int32_t X, int32_t Y, int32_t n, const int32_t* node_off, const int32_t* pos,
+                       const int32_t* adj_off, const int32_t* adj, int32_t* nodes, int32_t* parents,
+                       int32_t* point_off, int32_t* points, int32_t* hseg_off, int32_t* hsegs,
+                       int32_t* vseg_off, int32_t* vsegs, int64_t* totals) {
+    const int XY = X * Y;
+    int np = 0, nh = 0, nv = 0;
+    point_off[0] = hseg_off[0] = vseg_off[0] = 0;
+    for (int id = 0; id < n; ++id) {
+        const int base = node_off[id], N = node_off[id + 1] - base;
+        // Adjacency must stay inside the net.
+        for (int i = 0; i < N; ++i)
+            for (int k = adj_off[base + i]; k < adj_off[base + i + 1]; ++k)
+                if (adj[k] < 0 || adj[k] >= N) return -(id + 1);
+        auto p2 = [&](int i) { return pos[base + i] % XY; };
+        for (int i = 0; i < N; ++i) points[np++] = p2(i);
+        for (int i = 0; i < N; ++i) {
+            const int xi = p2(i) / Y, yi = p2(i) % Y;
+            for (int k = adj_off[base + i]; k < adj_off[base + i + 1]; ++k) {
+                const int j = adj[k];
+                if (j >= i) continue;
+                const int xj = p2(j) / Y, yj = p2(j) % Y;
+                const int minx = std::min(xi, xj), maxx = std::max(xi, xj), miny = std::min(yi, yj),
+                          maxy = std::max(yi, yj);
+                if (xi != xj && yi != yj) {
+                    hsegs[2 * nh] = minx * Y + miny; hsegs[2 * nh + 1] = maxx * Y + miny; ++nh;
+                    hsegs[2 * nh] = minx * Y + maxy; hsegs[2 * nh + 1] = maxx * Y + maxy; ++nh;
+                    vsegs[2 * nv] = minx * Y + miny; vsegs[2 * nv + 1] = minx * Y + maxy; ++nv;
+                    vsegs[2 * nv] = maxx * Y + miny; vsegs[2 * nv + 1] = maxx * Y + maxy; ++nv;
+                    points[np++] = xi * Y + yj;
+                    points[np++] = xj * Y + yi;
+                } else if (xi != xj) {
+                    hsegs[2 * nh] = minx * Y + miny; hsegs[2 * nh + 1] = maxx * Y + miny; ++nh;
+                    points[np++] = minx * Y + miny;
+                    points[np++] = maxx * Y + miny;
+                } else if (yi != yj) {
+                    vsegs[2 * nv] = minx * Y + miny; vsegs[2 * nv + 1] = minx * Y + maxy; ++nv;
+                    points[np++] = minx * Y + miny;
+                    points[np++] = minx * Y + maxy;
+                }
+            }
+        }
+        point_off[id + 1] = np;
+        hseg_off[id + 1] = nh;
+        vseg_off[id + 1] = nv;
+        // Recursive preorder; a node reached twice means the adjacency is
+        // not a tree.
+        int next = 0;
+        bool bad = false;
+        std::vector<char> seen(N, 0);
+        std::function<void(int, int, int)> dfs = [&](int x, int par, int par_node) {
+            if (bad || seen[x]) { bad = true; return; }
+            seen[x] = 1;
+            const int idx = next++;
+            nodes[base + idx] = pos[base + x];
+            parents[base + idx] = par_node;
+            for (int k = adj_off[base + x]; k < adj_off[base + x + 1]; ++k)
+                if (adj[k] != par) dfs(adj[k], x, idx);
+        };
+        if (N) dfs(0, -1, -1);
+        if (bad || next != N) return -(id + 1);
+    }
+    totals[0] = np;
+    totals[1] = nh;
+    totals[2] = nv;
+    return 0;
 }
 
 }  // extern "C"

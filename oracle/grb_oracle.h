@@ -163,6 +163,22 @@ int orc_zshape_stage(const orc_grid* g, const orc_ztrees* trees, int32_t n_batch
 int32_t orc_bbox_batches(int32_t X, int32_t Y, int32_t n, const int32_t* group, const int32_t* bbox,
                          int32_t max_batch, int32_t* ids, int32_t* off);
 
+/* Topology of every net from its Steiner tree: the batching geometry of
+ * net::construct_rsmt (preprocess.hpp:95-123: the nodes' 2-D cells, then per
+ * tree edge (i, j < i) in adjacency order two corner or end points and its
+ * h / v segments) and the depth-first flattening of Lshape_route
+ * (lshape.cuh:85-98: preorder from node 0, neighbours in adjacency order,
+ * parent's preorder index).  pos: layer*X*Y + x*Y + y per node (layer L =
+ * Steiner point); adj_off/adj: each node's neighbours (net-local indices).
+ * Output buffers hold at most node_off[n] nodes, 3*node_off[n] points and
+ * 2*node_off[n] segments of each kind; totals[0..2] receive the point, h- and
+ * v-segment counts.  Returns 0, or -(net+1) for a net whose adjacency is not
+ * a tree on its nodes. */
+int orc_build_topology(int32_t X, int32_t Y, int32_t n, const int32_t* node_off, const int32_t* pos,
+                       const int32_t* adj_off, const int32_t* adj, int32_t* nodes, int32_t* parents,
+                       int32_t* point_off, int32_t* points, int32_t* hseg_off, int32_t* hsegs,
+                       int32_t* vseg_off, int32_t* vsegs, int64_t* totals);
+
 #ifdef __cplusplus
 }
 #endif

@@ -13,7 +13,7 @@ _LIB = os.path.join(_HERE, "liboracle.so")
 __all__ = [
     "build", "load", "OrcGrid", "cost_full", "presum", "presum_logstep", "lshape_batch",
     "commit_batch", "batches", "ripup_classify", "congestion_view", "lshape_stage", "flt_stage", "zshape_stage",
-    "bbox_batches", "exp_args", "set_exp_table", "exp_table_misses",
+    "bbox_batches", "exp_args", "set_exp_table", "exp_table_misses", "build_topology",
 ]
 
 
@@ -58,6 +58,8 @@ def _declare(lib):
     lib.orc_batches.restype = C.c_int32
     lib.orc_ripup_classify.argtypes = [P, P, C.c_int32, C.c_int32, P, P, P]
     lib.orc_congestion_view.argtypes = [P, P, P, P, P]
+    lib.orc_build_topology.argtypes = [C.c_int32, C.c_int32, C.c_int32] + [P] * 13
+    lib.orc_build_topology.restype = C.c_int
     lib.orc_lshape_stage.argtypes = [P, C.c_int32, P, P, P, P, P, P, P, P, P, P, P, P, C.c_int32]
     lib.orc_lshape_stage.restype = C.c_int
     lib.orc_flt_stage.argtypes = [P, P, C.c_int32, P, P, P, P, P, P, C.c_int32, P, P, P, P, P, C.c_int32]
@@ -290,3 +292,27 @@ def set_exp_table(x=None, y=None) -> None:
 
 def exp_table_misses() -> int:
     return int(load().orc_exp_table_misses())
+
+
+def build_topology(X, Y, node_off, pos, adj_off, adj):
+    """Per-net DP trees and batching geometry from Steiner trees
+    (orc_build_topology); returns a dict of the flat arrays."""
+    lib = load()
+    node_off = _c(node_off, np.int32)
+    n = len(node_off) - 1
+    nn = int(node_off[-1])
+    out = {"node_off": node_off.copy(), "nodes": np.zeros(nn, np.int32), "parents": np.zeros(nn, np.int32),
+           "point_off": np.zeros(n + 1, np.int32), "points": np.zeros(3 * nn, np.int32),
+           "hseg_off": np.zeros(n + 1, np.int32), "hsegs": np.zeros(4 * nn, np.int32),
+           "vseg_off": np.zeros(n + 1, np.int32), "vsegs": np.zeros(4 * nn, np.int32)}
+    totals = np.zeros(3, np.int64)
+    rc = lib.orc_build_topology(int(X), int(Y), n, _p(node_off), _p(_c(pos, np.int32)), _p(_c(adj_off, np.int32)),
+                                _p(_c(adj, np.int32)), _p(out["nodes"]), _p(out["parents"]), _p(out["point_off"]),
+                                _p(out["points"]), _p(out["hseg_off"]), _p(out["hsegs"]), _p(out["vseg_off"]),
+                                _p(out["vsegs"]), _p(totals))
+    if rc:
+        raise ValueError(f"net {-rc - 1}: adjacency is not a tree on its nodes")
+    out["points"] = out["points"][:totals[0]]
+    out["hsegs"] = out["hsegs"][:2 * totals[1]]
+    out["vsegs"] = out["vsegs"][:2 * totals[2]]
+    return out

@@ -119,8 +119,17 @@ int run_topo(const std::string& cap, const std::string& net, const std::string& 
     // Per-net DFS flattening exactly as lshape.cuh:85-103.
     std::vector<int> node_off{0}, nodes, parents, point_off{0}, points, hseg_off{0}, hsegs, vseg_off{0}, vsegs;
     std::vector<int> hpwl(n), original(n), pin_count(n);
+    // The trees themselves (net::rsmt after construct_rsmt: node positions
+    // with their layer, then each node's adjacency list), for the topology
+    // construction's parity.
+    std::vector<int> rsmt_pos, rsmt_adj_off{0}, rsmt_adj;
     for (int id = 0; id < n; ++id) {
         auto& graph = nets[id].rsmt;
+        for (size_t i = 0; i + 1 < graph.size(); ++i) {
+            rsmt_pos.push_back(graph.back()[i]);
+            rsmt_adj.insert(rsmt_adj.end(), graph[i].begin(), graph[i].end());
+            rsmt_adj_off.push_back(rsmt_adj.size());
+        }
         const size_t base = nodes.size();
         nodes.resize(base + graph.back().size());
         parents.resize(base + graph.back().size());
@@ -151,6 +160,7 @@ int run_topo(const std::string& cap, const std::string& net, const std::string& 
         for (int pin : dbnet.pins) pin_vias[0] += pin < state.device.X * state.device.Y;
     dump(dir, "pin_vias", pin_vias);
     dump(dir, "node_off", node_off); dump(dir, "nodes", nodes); dump(dir, "parents", parents);
+    dump(dir, "rsmt_pos", rsmt_pos); dump(dir, "rsmt_adj_off", rsmt_adj_off); dump(dir, "rsmt_adj", rsmt_adj);
     dump(dir, "point_off", point_off); dump(dir, "points", points);
     dump(dir, "hseg_off", hseg_off); dump(dir, "hsegs", hsegs);
     dump(dir, "vseg_off", vseg_off); dump(dir, "vsegs", vsegs);

@@ -57,7 +57,8 @@ Z_FIXTURES = {"ref_z_48x48x10_1500", "ref_z_40x56x10_800"}
 HARNESS_GGR = os.path.join(REF, "ref_harness_ggr")
 TOPO_KEYS = ["meta", "short_costs", "unit_costs", "x_edge_len", "y_edge_len", "capacity", "pin_acc_num",
              "node_off", "nodes", "parents", "point_off", "points", "hseg_off", "hsegs", "vseg_off", "vsegs",
-             "hpwl", "original", "pin_count", "order", "batch_of", "ids", "batch_off", "pin_vias"]
+             "hpwl", "original", "pin_count", "order", "batch_of", "ids", "batch_off", "pin_vias",
+             "rsmt_pos", "rsmt_adj_off", "rsmt_adj"]
 EXT = {"i32": np.int32, "i64": np.int64, "f32": np.float32, "f64": np.float64}
 
 
