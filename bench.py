@@ -33,6 +33,7 @@ the max over ranks.
 from __future__ import annotations
 
 import argparse
+import ctypes as C
 import json
 import os
 import subprocess
@@ -406,7 +407,6 @@ def run_grotor(args):
 
     # Roofline of the two kernels of the persistent form.
     lib = r._lib
-    import ctypes as C
     out = np.zeros(4, np.float64)
     gs = design.grid.struct()
     P = lambda a: np.ascontiguousarray(a).ctypes.data_as(C.c_void_p)  # noqa: E731
@@ -479,8 +479,6 @@ def cpu_leg(design, workload, gpu_batch_of, ids, off, routes, tables, stats):
     its design), then the CPU restatement of its DAG code over the whole plan
     on every host core, with the device's values of the cost model's
     exponential.  Returns (cpu_baseline, parity)."""
-    import ctypes as C
-
     import oracle
     from grotor_b200 import _abi
     g, n = design.grid, design.nets
@@ -582,6 +580,24 @@ def zshape_measure(args, workload="large_800x800x10", steps=3, warmup=2):
                      "first_fit_ms": float(np.mean(first)), "dag_ms": float(np.mean(dag)), "batches": int(nb),
                      "wirelength": st["wirelength"], "vias": st["vias"], "status": status}
     out["speedup_persistent_vs_plain"] = out["plain"]["ms_per_step"] / out["persistent"]["ms_per_step"]
+    # Roofline of the stage kernel: the model's bytes (grb_zshape_traffic:
+    # refresh, DP reads of every net's box rows and columns, commit) over the
+    # stage's device time, for each executor (same plan, same routes).
+    ids, off = r.plan()
+    routes = r.read_routes()
+    traffic = np.zeros(3, np.float64)
+    gs = d.grid.struct()
+    Pp = lambda a: np.ascontiguousarray(a).ctypes.data_as(C.c_void_p)  # noqa: E731
+    rc = r._lib.grb_zshape_traffic(C.byref(gs), len(off) - 1, Pp(off), Pp(ids), Pp(z["node_off"]), Pp(z["coord"]),
+                                   Pp(z["child"]), Pp(route_off), Pp(routes), Pp(traffic))
+    assert rc == 0
+    peak, kind = measured_peak()
+    out["algorithmic_bytes"] = {"refresh": traffic[0], "dp": traffic[1], "commit": traffic[2]}
+    for mode in ("persistent", "plain"):
+        ach = traffic.sum() / (out[mode]["dag_ms"] / 1e3) / 1e9
+        out[mode]["roofline"] = {"kernel": "k_zshape_persistent" if mode == "persistent" else "per-batch launches",
+                                 "bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
+                                 "peak_source": f"{kind} hbm_gbs"}
     r.close()
     return out
 
@@ -601,6 +617,27 @@ def softmin_measure(args, workload="softmin_320x320x10", taus=(1.0, 0.1, 0.01), 
     r.lshape_route("persistent")
     g = d.grid
     out = {"workload": workload, "nets": int(d.n_subnets), "dtype": "f32"}
+    # Byte model of one forward and one adjoint (T = 4 bytes, f32): cost tables
+    # (capacity, unit wire cost and demand read, wire and via cost written),
+    # track prefix (read + write), the DAG's read set (grb_dag_reads: distinct
+    # prefix and via-cost entries per net, 8 B per tree node), net costs; the
+    # adjoint repeats tables, prefix and reads, adds read-modify-write of the
+    # adjoint entries, the suffix pass, the chain rule to capacity and unit
+    # wire cost and the via-cost sum.
+    reads = np.zeros(3, np.float64)
+    gs = g.struct()
+    Pp = lambda a: np.ascontiguousarray(a).ctypes.data_as(C.c_void_p)  # noqa: E731
+    n = d.nets
+    assert r._lib.grb_dag_reads(C.byref(gs), n.n, None, Pp(n.node_off), Pp(n.nodes), Pp(n.parents), Pp(reads)) == 0
+    T, cells = 4.0, float(g.L * g.X * g.Y)
+    tables, prefix = cells * (3 * T + 4 + 2 * T), cells * 2 * T
+    dag = T * (reads[0] + reads[1]) + 8.0 * reads[2]
+    fwd_bytes = tables + prefix + dag + T * n.n
+    bwd_bytes = tables + prefix + 2 * cells * T + dag + 2 * T * (reads[0] + reads[1]) + cells * 2 * T + \
+        cells * 6 * T + cells * T
+    peak, kind = measured_peak()
+    out["algorithmic_bytes"] = {"forward": fwd_bytes, "backward": bwd_bytes, "dag_prefix_entries": reads[0],
+                                "dag_via_entries": reads[1], "tree_nodes": reads[2]}
     for tau in taus:
         cap = torch.tensor(np.asarray(g.capacity, np.float32), device="cuda").requires_grad_(True)
         uw = torch.full_like(cap, float(g.unit_wire)).requires_grad_(True)
@@ -618,8 +655,15 @@ def softmin_measure(args, workload="softmin_320x320x10", taus=(1.0, 0.1, 0.01), 
             if k:
                 fw.append((t1 - t0) * 1e3)
                 bw.append((t2 - t1) * 1e3)
-        out[f"tau_{tau:g}"] = {"forward_ms": float(np.mean(fw)), "backward_ms": float(np.mean(bw)),
-                               "total_cost": float(F.item())}
+        fa = fwd_bytes / (np.mean(fw) / 1e3) / 1e9
+        ba = bwd_bytes / (np.mean(bw) / 1e3) / 1e9
+        out[f"tau_{tau:g}"] = {
+            "forward_ms": float(np.mean(fw)), "backward_ms": float(np.mean(bw)), "total_cost": float(F.item()),
+            "roofline_forward": {"kernel": "k_soft_forward (+ tables, prefix)", "bound": "hbm", "achieved": fa,
+                                 "peak": peak, "unit": "GB/s", "frac": fa / peak, "peak_source": f"{kind} hbm_gbs"},
+            "roofline_backward": {"kernel": "k_soft_backward (+ tables, prefix, suffix, chain)", "bound": "hbm",
+                                  "achieved": ba, "peak": peak, "unit": "GB/s", "frac": ba / peak,
+                                  "peak_source": f"{kind} hbm_gbs"}}
     r.close()
     return out
 

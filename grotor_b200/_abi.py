@@ -118,6 +118,9 @@ SIGNATURES = {
     "grb_phase_times": (C.c_int, [P, P, C.c_int32, C.c_int32]),
     # grb_prof.h
     "grb_stage_traffic": (C.c_int, [P, C.c_int32, P, P, P, P, P, P, P, P, P, P, P, P, C.c_int32, P]),
+    "grb_zshape_traffic": (C.c_int, [P, C.c_int32, P, P, P, P, P, P, P, P]),
+    "grb_flt_traffic": (C.c_int, [P, C.c_int32, P, P, P, P, P, P, C.c_int32, P]),
+    "grb_dag_reads": (C.c_int, [P, C.c_int32, P, P, P, P, P]),
 }
 
 # include/grb_synth.h (libgrb_synth.so)

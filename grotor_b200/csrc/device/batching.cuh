@@ -357,31 +357,27 @@ __device__ __forceinline__ SolveSmem solve_smem(unsigned* base, int W) {
 
 // The smallest colour c >= c0 net `tid` may take: not in U, not held by a
 // predecessor (pmask: which predecessor words are nonzero).  C if none.
+// Word by word from c0's: the word's forbidden bits are U's plus the colours
+// of the predecessors that fall in it (one pass over the predecessors per
+// word, whatever the number of colours the net has to skip).
 template <int CH>
 __device__ __forceinline__ int first_fit(const SolveSmem& S, int tid, int W, unsigned pmask, int c0) {
-    int c = c0;
-    while (true) {
-        int w = c >> 5;
-        if (w >= W) return 32 * W;
-        unsigned used = S.U[w * CH + tid] | ((1u << (c & 31)) - 1u);
-        while (used == 0xffffffffu) {
-            if (++w >= W) return 32 * W;
-            used = S.U[w * CH + tid];
-        }
-        c = w * 32 + __ffs(~used) - 1;
-        bool hit = false;
-        for (unsigned pm = pmask; pm && !hit; pm &= pm - 1) {
+    for (int w = c0 >> 5; w < W; ++w) {
+        unsigned used = S.U[w * CH + tid];
+        if (w == (c0 >> 5)) used |= (1u << (c0 & 31)) - 1u;
+        if (used == 0xffffffffu) continue;
+        for (unsigned pm = pmask; pm; pm &= pm - 1) {
             const int pw = __ffs(pm) - 1;
             unsigned bits = S.P[pw * CH + tid];
             while (bits) {
-                const int i = pw * 32 + __ffs(bits) - 1;
+                const int ci = S.col[pw * 32 + __ffs(bits) - 1];
                 bits &= bits - 1;
-                if (S.col[i] == c) { hit = true; break; }
+                if ((ci >> 5) == w) used |= 1u << (ci & 31);  // ci = -1 (not yet coloured) is in no word
             }
         }
-        if (!hit) return c;
-        ++c;
+        if (used != 0xffffffffu) return w * 32 + __ffs(~used) - 1;
     }
+    return 32 * W;
 }
 
 // The solve runs on threads 0..CH-1 of its CTA and synchronises them

@@ -11,9 +11,12 @@
 // wires (straight, or split at the best sampled mid-edge layer change) and
 // each node's via stack.
 //
-// B200 form: one warp per net (the reference uses a 128-thread CTA); lanes
-// take the nodes of one depth level, __syncwarp separates levels; the packed
-// keys live in a per-stage workspace in HBM (mostly L2-resident per batch).
+// B200 form: the layer-change tables of all the batch's edges are one
+// grid-wide pass, a thread per (edge, from-layer, to-layer) entry (the
+// reference launches a thread per (edge, from-layer)); then one warp per net
+// (the reference uses a 128-thread CTA); lanes take the nodes of one depth
+// level, __syncwarp separates levels; the packed keys live in a per-stage
+// workspace in HBM (mostly L2-resident per batch).
 // Node numbering is net-local: candidates for a slot always belong to one
 // net, so the batch-global numbering of the reference orders them the same.
 // Segments are appended in level order, ascending node index within a level,
@@ -56,6 +59,10 @@ struct Flt {
     double* ce;                    // [edges*81] layer-change cost
     int* bc;                       // [edges*81] layer-change position
     int* routes2;
+    // per plan position: first edge slot (exclusive prefix of the plan's
+    // edges, [plan+1]); per edge slot: its plan position
+    const int* eprefix;
+    const int* emap;
 };
 
 __device__ __forceinline__ double flt_wire(const Tables& T, int l, int xmin, int xmax, int ymin, int ymax) {
@@ -75,44 +82,62 @@ __device__ __forceinline__ double flt_cost(unsigned long long p) {
     return static_cast<double>(__int_as_float(i));
 }
 
-// precompute_cost_edge (flt_cost.cuh:50-130) for global edge `e` and
-// from-layer `fl`.  Rows the solve never reads (wrong direction, or an edge of
-// Manhattan length <= 4, where only straight wires are offered) stay INF.
-__device__ __forceinline__ void flt_edge_row(const Tables& T, const Flt& F, int nb, int e, int fl) {
+// precompute_cost_edge (flt_cost.cuh:50-130), one entry: global edge `e`,
+// from-layer `fl`, to-layer `tl`.  Entries the solve never reads (wrong
+// direction, an edge of Manhattan length <= 4, where only straight wires are
+// offered, or a to-layer of the other parity) are INF.  The sampled
+// positions are scanned in increasing order and the first minimum is kept.
+__device__ __forceinline__ void flt_edge_cell(const Tables& T, const Flt& F, int nb, int e, int fl, int tl) {
     const int to = nb + F.eparent[e], from = nb + F.eslot[e] / 10;
     const int ct = F.coord[to], cf = F.coord[from];
     const int tox = ct / T.Y % T.X, toy = ct % T.Y, fromx = cf / T.Y % T.X, fromy = cf % T.Y;
-    double* ce = F.ce + size_t(e) * 81 + fl * 9;
-    int* bc = F.bc + size_t(e) * 81 + fl * 9;
+    double* ce = F.ce + size_t(e) * 81 + fl * 9 + tl;
+    int* bc = F.bc + size_t(e) * 81 + fl * 9 + tl;
     const bool ay = along_y(T, fl);
     const int distance = abs(tox - fromx) + abs(toy - fromy);
-    if ((!ay && fromy != toy) || (ay && fromx != tox) || distance <= 4) {
-        for (int tl = 0; tl < 9; ++tl) { ce[tl] = kInf; bc[tl] = -1; }
+    if ((!ay && fromy != toy) || (ay && fromx != tox) || distance <= 4 || (tl & 1) != (fl & 1)) {
+        *ce = kInf;
+        *bc = -1;
         return;
     }
     const int dd = distance / min(distance, 20);
     const bool vertical = fromx == tox;
     const int start = vertical ? min(fromy, toy) : min(fromx, tox);
     const int end = vertical ? max(fromy, toy) : max(fromx, tox);
-    for (int tl = 0; tl < 9; ++tl) {
-        if ((tl & 1) != (fl & 1)) { ce[tl] = kInf; bc[tl] = -1; continue; }
-        double best = kInf;
-        int pos = -1;
-        for (int sp = start + dd; sp < end; sp += dd) {
-            const int sx = vertical ? fromx : sp, sy = vertical ? sp : fromy;
-            double via = 0;
-            for (int ll = min(fl, tl); ll < max(fl, tl); ++ll) via += T.vcost[cell_index(T, ll, sx, sy)];
-            double c = via;
-            if (vertical)
-                c += (flt_wire(T, fl, fromx, fromx, min(fromy, sy), max(fromy, sy)) +
-                      flt_wire(T, tl, tox, tox, min(toy, sy), max(toy, sy)));
-            else
-                c += (flt_wire(T, fl, min(fromx, sx), max(fromx, sx), fromy, fromy) +
-                      flt_wire(T, tl, min(tox, sx), max(tox, sx), toy, toy));
-            if (c < best) { best = c; pos = sp; }
-        }
-        ce[tl] = best;
-        bc[tl] = pos;
+    const int lo = min(fl, tl), hi = max(fl, tl);
+    double best = kInf;
+    int pos = -1;
+    for (int sp = start + dd; sp < end; sp += dd) {
+        const int sx = vertical ? fromx : sp, sy = vertical ? sp : fromy;
+        double via = 0;
+        for (int ll = lo; ll < hi; ++ll) via += T.vcost[cell_index(T, ll, sx, sy)];
+        double c = via;
+        if (vertical)
+            c += (flt_wire(T, fl, fromx, fromx, min(fromy, sy), max(fromy, sy)) +
+                  flt_wire(T, tl, tox, tox, min(toy, sy), max(toy, sy)));
+        else
+            c += (flt_wire(T, fl, min(fromx, sx), max(fromx, sx), fromy, fromy) +
+                  flt_wire(T, tl, min(tox, sx), max(tox, sx), toy, toy));
+        if (c < best) { best = c; pos = sp; }
+    }
+    *ce = best;
+    *bc = pos;
+}
+
+// The layer-change tables of every edge of batch b, one (edge, from-layer,
+// to-layer) entry per thread over threads t, t + nt, ...: the reference's
+// precompute_cost_edge launch over the batch's edges (flt.cuh:152), with the
+// to-layer loop spread too.  Edge slot s of the plan belongs to plan position
+// emap[s]; eprefix[k] is the first slot of position k.
+__device__ __forceinline__ void flt_edges_batch(const Tables& T, const Flt& F, const Plan& P, int b, long long t,
+                                                long long nt) {
+    const int lo = P.batch_off[b], hi = P.batch_off[b + 1];
+    const long long s0 = F.eprefix[lo], items = (static_cast<long long>(F.eprefix[hi]) - s0) * 81;
+    for (long long q = t; q < items; q += nt) {
+        const int s = static_cast<int>(s0 + q / 81), r = static_cast<int>(q % 81);
+        const int k = F.emap[s];
+        const int id = P.ids[k];
+        flt_edge_cell(T, F, F.node_off[id], F.edge_off[id] + (s - F.eprefix[k]), r / 9, r % 9);
     }
 }
 
@@ -269,9 +294,8 @@ __device__ __forceinline__ int flt_trace_node(const Tables& T, const Flt& F, int
 __device__ __forceinline__ void flt_net(const Tables& T, const Flt& F, const Plan& P2, int id, int stamp, int lane,
                                         bool commit) {
     const int nb = F.node_off[id], N = F.node_off[id + 1] - nb;
-    const int eb = F.edge_off[id], E = F.edge_off[id + 1] - eb;
+    const int eb = F.edge_off[id];
     if (N <= 0) return;
-    for (int k = lane; k < E * 9; k += 32) flt_edge_row(T, F, nb, eb + k / 9, k % 9);
     for (int k = lane; k < N * kFltLayers; k += 32) F.costs[size_t(nb) * kFltLayers + k] = kInf;
     const int cb = F.child_off[nb], cn = F.child_off[nb + N - 1] + F.children[nb + N - 1] - cb;
     for (int k = lane; k < cn * kFltLayers; k += 32) F.packed[size_t(cb) * kFltLayers + k] = kFltInit;

@@ -45,25 +45,16 @@ __device__ __forceinline__ int zadd(int a, int b) {
 __device__ __forceinline__ int zidx(const ZTrees& Z, int i, int x, int y) {
     return static_cast<int>(i * Z.NN + (((i & 1) ^ Z.D) ? x * Z.N + y : y * Z.N + x));
 }
-// WireCosts (zshape.cuh:8-19): prefix value at a plane index.
-__device__ __forceinline__ double zsum(const Tables& T, const ZTrees& Z, int index) {
-    const int layer = static_cast<int>(index / Z.NN) - 1;
-    if (layer < 0 || layer >= T.L) return 0;
-    const int a = index / Z.N % Z.N, b = index % Z.N;
-    const bool ay = along_y(T, layer);
-    return T.presum[cell_index(T, layer, ay ? a : b, ay ? b : a)];
+// ViaCosts (zshape.cuh:20-31) and boundedWireCost over WireCosts
+// (zshape.cuh:8-19, 32-35) for plane layer i (1..L, routing layer i-1) at grid
+// positions.  The reference decodes (layer, x, y) from a plane index; the
+// loops here know the positions and read the same cells directly.
+__device__ __forceinline__ int zvia_at(const Tables& T, int i, int x, int y) {
+    return static_cast<int>(fminf(fmaxf(T.vcost[cell_index(T, i - 1, x, y)], 1.f), 1.e6f));
 }
-// ViaCosts (zshape.cuh:20-31).
-__device__ __forceinline__ int zvia(const Tables& T, const ZTrees& Z, int index) {
-    const int layer = static_cast<int>(index / Z.NN) - 1;
-    if (layer < 0 || layer >= T.L) return kZInf;
-    const int a = index / Z.N % Z.N, b = index % Z.N;
-    const bool ay = along_y(T, layer);
-    return static_cast<int>(fminf(fmaxf(T.vcost[cell_index(T, layer, ay ? a : b, ay ? b : a)], 1.f), 1.e6f));
-}
-// boundedWireCost (zshape.cuh:32-35).
-__device__ __forceinline__ int zwire(const Tables& T, const ZTrees& Z, int a, int b) {
-    return static_cast<int>(fmin(fabs(zsum(T, Z, a) - zsum(T, Z, b)), static_cast<double>(kZInf / 2)));
+__device__ __forceinline__ int zwire_at(const Tables& T, int i, int x0, int y0, int x1, int y1) {
+    return static_cast<int>(fmin(fabs(T.presum[cell_index(T, i - 1, x0, y0)] - T.presum[cell_index(T, i - 1, x1, y1)]),
+                                 static_cast<double>(kZInf / 2)));
 }
 
 // viaSweep (zshape.cuh:42-61) on plane 4 at 2-D position (x, y): up, then
@@ -81,7 +72,7 @@ __device__ __noinline__ void zvia_sweep(const Tables& T, const ZTrees& Z, int x,
             const int c = zidx(Z, i, x, y);
             mv[i] = m[c];
             pv[i] = p[c];
-            vc[i] = zvia(T, Z, c);
+            vc[i] = zvia_at(T, i, x, y);
             q[i] = i;
         }
     }
@@ -144,7 +135,7 @@ __device__ __forceinline__ void zedge(const Tables& T, const ZTrees& Z, int j, i
                 for (int b = miny + lane; b <= maxy; b += nth) {
                     if (b == fromy) continue;
                     const int cur = static_cast<int>(i * NN + fromx * Z.N + b);
-                    m4[cur] = zadd(map0[last], zwire(T, Z, last, cur));
+                    m4[cur] = zadd(map0[last], zwire_at(T, i, fromx, fromy, fromx, b));
                     p4[cur] = last;
                 }
             } else {
@@ -152,7 +143,7 @@ __device__ __forceinline__ void zedge(const Tables& T, const ZTrees& Z, int j, i
                 for (int b = minx + lane; b <= maxx; b += nth) {
                     if (b == fromx) continue;
                     const int cur = static_cast<int>(i * NN + fromy * Z.N + b);
-                    m4[cur] = zadd(map0[last], zwire(T, Z, last, cur));
+                    m4[cur] = zadd(map0[last], zwire_at(T, i, fromx, fromy, b, fromy));
                     p4[cur] = last;
                 }
             }
@@ -172,13 +163,13 @@ __device__ __forceinline__ void zedge(const Tables& T, const ZTrees& Z, int j, i
             if ((i & 1) ^ D) {
                 for (int b = minx + lane; b <= maxx; b += nth) {
                     const int last = static_cast<int>(i * NN + b * Z.N + fromy), cur = static_cast<int>(i * NN + b * Z.N + toy);
-                    const int v = zadd(m4[last], zwire(T, Z, last, cur));
+                    const int v = zadd(m4[last], zwire_at(T, i, b, fromy, b, toy));
                     if (v < m4[cur]) { m4[cur] = v; p4[cur] = p4[last]; }
                 }
             } else {
                 for (int b = miny + lane; b <= maxy; b += nth) {
                     const int last = static_cast<int>(i * NN + b * Z.N + fromx), cur = static_cast<int>(i * NN + b * Z.N + tox);
-                    const int v = zadd(m4[last], zwire(T, Z, last, cur));
+                    const int v = zadd(m4[last], zwire_at(T, i, fromx, b, tox, b));
                     if (v < m4[cur]) { m4[cur] = v; p4[cur] = p4[last]; }
                 }
             }
@@ -201,13 +192,12 @@ __device__ __forceinline__ void zedge(const Tables& T, const ZTrees& Z, int j, i
         __shared__ int red_v[32][kMaxLayers], red_b[32][kMaxLayers];
         for (int i = 1; i < LAYER; ++i) {
             const bool ay = ((i & 1) ^ D) != 0;
-            const int cur = static_cast<int>(ay ? i * NN + tox * Z.N + toy : i * NN + toy * Z.N + tox);
             const int lo = ay ? miny : minx, hi = ay ? maxy : maxx, skip = ay ? toy : tox;
             int bv = 0, bb = -1;
             for (int b = lo + lane; b <= hi; b += nth) {
                 if (b == skip) continue;
                 const int last = static_cast<int>(ay ? i * NN + tox * Z.N + b : i * NN + toy * Z.N + b);
-                const int v = zadd(m4[last], zwire(T, Z, last, cur));
+                const int v = zadd(m4[last], ay ? zwire_at(T, i, tox, b, tox, toy) : zwire_at(T, i, b, toy, tox, toy));
                 if (bb < 0 || v < bv) { bv = v; bb = b; }
             }
             for (int o = 16; o; o >>= 1) {
@@ -235,7 +225,7 @@ __device__ __forceinline__ void zedge(const Tables& T, const ZTrees& Z, int j, i
         for (int i = 1 + lane; i < LAYER; i += nth) {
             if ((i & 1) ^ D) {
                 const int last = static_cast<int>(i * NN + fromx * Z.N + fromy), cur = static_cast<int>(i * NN + tox * Z.N + toy);
-                const int v = zadd(map0[last], zwire(T, Z, last, cur));
+                const int v = zadd(map0[last], zwire_at(T, i, fromx, fromy, tox, toy));
                 if (mj[cur] > v) { mj[cur] = v; pj[cur] = last; }
             } else {
                 mj[i * NN + toy * Z.N + tox] = kZInf;
@@ -245,7 +235,7 @@ __device__ __forceinline__ void zedge(const Tables& T, const ZTrees& Z, int j, i
         for (int i = 1 + lane; i < LAYER; i += nth) {
             if ((!(i & 1)) ^ D) {
                 const int last = static_cast<int>(i * NN + fromy * Z.N + fromx), cur = static_cast<int>(i * NN + toy * Z.N + tox);
-                const int v = zadd(map0[last], zwire(T, Z, last, cur));
+                const int v = zadd(map0[last], zwire_at(T, i, fromx, fromy, tox, toy));
                 if (mj[cur] > v) { mj[cur] = v; pj[cur] = last; }
             } else {
                 mj[i * NN + tox * Z.N + toy] = kZInf;
@@ -268,7 +258,7 @@ __device__ __forceinline__ void znode_dp_warp(const Tables& T, const ZTrees& Z, 
     const int idx_l = lane < LAYER ? zidx(Z, lane, tox, toy) : 0;
     int pv[3];
     for (int j = 0; j < 3; ++j) pv[j] = (lane < LAYER && ch[j] != -1) ? Z.map[(j + 1) * Z.LNN + idx_l] : 0;
-    const int vc = lane < LAYER ? zvia(T, Z, idx_l) : 0;
+    const int vc = lane < LAYER ? (lane >= 1 ? zvia_at(T, lane, tox, toy) : kZInf) : 0;
     const int lower = lane;
     int viaSum = 0, minCost = kZInf, bestpos[3] = {0, 0, 0};
     int costs[3] = {ch[0] == -1 ? 0 : kZInf, ch[1] == -1 ? 0 : kZInf, ch[2] == -1 ? 0 : kZInf};

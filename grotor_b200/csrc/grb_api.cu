@@ -302,9 +302,15 @@ __global__ void __launch_bounds__(kFltThreads) k_flt_batch(Tables T, Flt F, Plan
     if (k < cnt) flt_net(T, F, P2, P2.ids[lo + k], stamp, lane, true);
 }
 
+// Layer-change tables of batch b's edges (flt_edges_batch).
+__global__ void k_flt_edges(Tables T, Flt F, Plan P2, int b) {
+    flt_edges_batch(T, F, P2, b, blockIdx.x * (long long)blockDim.x + threadIdx.x, (long long)gridDim.x * blockDim.x);
+}
+
 // Persistent FLT stage: per batch, [remove stage-one wires -> remove their
-// vias ->] refresh cells -> prefix pass 1 -> trees -> pass 2 -> FLT nets and
-// wires -> vias, separated by bounded grid barriers (flt.cuh:141-168 order).
+// vias ->] refresh cells -> prefix pass 1 -> trees -> pass 2 -> layer-change
+// tables of the batch's edges -> FLT nets and wires -> vias, separated by
+// bounded grid barriers (flt.cuh:141-168 order).
 __global__ void __launch_bounds__(kPersistentThreads, 2) k_flt_persistent(Tables T, Flt F, Plan P1, Plan P2,
         GridSync S, int stamp0, int remove, int* work) {
     extern __shared__ __align__(16) char smem[];
@@ -323,6 +329,10 @@ __global__ void __launch_bounds__(kPersistentThreads, 2) k_flt_persistent(Tables
             clk.mark(S, 6);
         }
         if (!refresh_persistent(T, S, clk, gwarp, nwarps, lane, smem)) return;
+        flt_edges_batch(T, F, P2, b, blockIdx.x * (long long)blockDim.x + threadIdx.x,
+                        (long long)gridDim.x * blockDim.x);
+        if (!grid_sync(S, T)) return;
+        clk.mark(S, 10);
         while (true) {
             int k = 0;
             if (lane == 0) k = atomicAdd(work + b, 1);
@@ -1017,6 +1027,11 @@ struct grb_ctx {
     long long route2_words = 0;
     int flt_n = -1;                   // nets covered by the uploaded DAGs
     std::vector<int> h_flt_node_off;
+    std::vector<int> h_flt_edge_off;
+    int* flt_eprefix = nullptr;       // [plan+1] first edge slot of each plan position
+    int* flt_emap = nullptr;          // plan position of each edge slot
+    long long flt_emap_cap = 0;
+    int flt_emap_plan = -1, flt_emap_flt = -1;  // plan / DAG versions the map was built for
     std::vector<long long> h_route2_off;
     int flt_version = 0;
     cudaGraphExec_t flt_graph = nullptr;
@@ -1549,6 +1564,8 @@ int flt_stage_plain(grb_ctx* c, int stamp0, int remove) {
         }
         if ((rc = refresh_plain(c))) return rc;
         if ((rc = prof_begin(c, 5, &e))) return rc;
+        k_flt_edges<<<c->sms * 8, 256, 0, c->stream>>>(c->T, c->F, P2, b);
+        c->launches += 1;
         k_flt_batch<<<(cnt + kFltThreads / 32 - 1) / (kFltThreads / 32), kFltThreads, 0, c->stream>>>(c->T, c->F, P2, b,
                                                                                                       stamp);
         prof_end(c, e);
@@ -1901,6 +1918,8 @@ void grb_destroy(grb_ctx* c) {
     free_all(c->geom_bufs);
     free_all(c->flt_bufs);
     free_all(c->topo_bufs);
+    if (c->flt_eprefix) cudaFree(c->flt_eprefix);
+    if (c->flt_emap) cudaFree(c->flt_emap);
     free_all(c->owned);
     for (void* p : {(void*)c->check, (void*)c->bucket_ids, (void*)c->bucket_off, (void*)c->ids, (void*)c->batch_off, (void*)c->gscratch, (void*)c->work, (void*)c->cellmask,
                     (void*)c->lmask[0], (void*)c->lmask[1], (void*)c->lmask[2], (void*)c->ptchunk, (void*)c->fmask, (void*)c->pred, (void*)c->prevp,
@@ -2486,6 +2505,7 @@ int grb_upload_flt(grb_ctx* c, const grb_flt_dags* d) {
     c->route2_words = rw;
     c->flt_n = n;
     c->h_flt_node_off.assign(d->node_off, d->node_off + n + 1);
+    c->h_flt_edge_off.assign(d->edge_off, d->edge_off + n + 1);
     c->h_route2_off.assign(d->route2_off, d->route2_off + n + 1);
     ++c->flt_version;
     return GRB_OK;
@@ -2780,6 +2800,40 @@ int grb_flt_stage(grb_ctx* c, int32_t remove_phase_one, int32_t mode, grb_stats*
     }
     for (int id : ids)
         if (c->h_flt_node_off[id + 1] == c->h_flt_node_off[id]) return fail(c, GRB_EINVAL, "plan net " + std::to_string(id) + " has no FLT DAG");
+    if (c->flt_emap_plan != c->plan_version || c->flt_emap_flt != c->flt_version) {
+        // Edge slots of the plan: each plan position's edges, in plan order.
+        std::vector<int> eprefix(size_t(c->plan_n) + 1, 0);
+        for (int k = 0; k < c->plan_n; ++k) {
+            const long long e = eprefix[k] + (long long)c->h_flt_edge_off[ids[k] + 1] - c->h_flt_edge_off[ids[k]];
+            if (e > INT_MAX / 81) return fail(c, GRB_EINVAL, "too many FLT edges in one plan");
+            eprefix[k + 1] = int(e);
+        }
+        const long long slots = eprefix[c->plan_n];
+        std::vector<int> emap(std::max(slots, 1ll));
+        for (int k = 0; k < c->plan_n; ++k)
+            std::fill(emap.begin() + eprefix[k], emap.begin() + eprefix[k + 1], k);
+        if (c->flt_emap_cap < std::max<long long>(slots, c->plan_n + 1)) {
+            if (c->flt_eprefix) cudaFree(c->flt_eprefix);
+            if (c->flt_emap) cudaFree(c->flt_emap);
+            c->flt_eprefix = c->flt_emap = nullptr;
+            c->flt_emap_cap = 0;
+            const long long cap = std::max<long long>(slots, c->plan_n + 1);
+            if (cudaMalloc(&c->flt_eprefix, sizeof(int) * cap) != cudaSuccess ||
+                cudaMalloc(&c->flt_emap, sizeof(int) * cap) != cudaSuccess) {
+                cudaGetLastError();
+                return fail(c, GRB_ENOMEM, "FLT edge map");
+            }
+            c->flt_emap_cap = cap;
+        }
+        GRB_CUDA(c, cudaMemcpyAsync(c->flt_eprefix, eprefix.data(), sizeof(int) * eprefix.size(), cudaMemcpyHostToDevice,
+                                    c->stream));
+        GRB_CUDA(c, cudaMemcpyAsync(c->flt_emap, emap.data(), sizeof(int) * slots, cudaMemcpyHostToDevice, c->stream));
+        GRB_CUDA(c, cudaStreamSynchronize(c->stream));
+        c->flt_emap_plan = c->plan_version;
+        c->flt_emap_flt = c->flt_version;
+    }
+    c->F.eprefix = c->flt_eprefix;
+    c->F.emap = c->flt_emap;
     const int remove = remove_phase_one ? 1 : 0;
     const int stamp0 = c->stamp;
     GRB_CUDA(c, cudaEventRecord(c->ev0, c->stream));

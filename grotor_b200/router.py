@@ -375,7 +375,7 @@ class Router:
     # publish / gather / solve, plus the waits and the raster it overlaps
     # with the solve.  L-shape stage: the next four.
     PHASES = ("batch_raster", "batch_gather", "batch_solve", "batch_publish", "cost_pass1", "dp", "commit",
-              "prefix_tree_pass2", "batch_solver_wait", "batch_worker_wait", "unused10", "unused11",
+              "prefix_tree_pass2", "batch_solver_wait", "batch_worker_wait", "flt_edge_tables", "unused11",
               "net_ms_bucket0", "net_ms_bucket1", "net_ms_bucket2", "net_ms_bucket3",
               "longest_net_ms_bucket0", "longest_net_ms_bucket1", "longest_net_ms_bucket2", "longest_net_ms_bucket3")
 

@@ -32,13 +32,19 @@
 //
 // Usage: grotor_grb -cap FILE -net FILE -out FILE [--lut-dir DIR]
 //                   [--executor persistent|plain|graph] [--stop-after lshape|routing]
+//                   [--report-traffic 0|1]
 #include "pipeline.hpp"
 
 #include <filesystem>
 
 #include "grb.h"
+#include "grb_prof.h"
 
 namespace drop_in {
+
+// --report-traffic 1: print the FLT stage's algorithmic bytes (grb_flt_traffic)
+// beside its timing, for its roofline.
+bool report_traffic = false;
 
 void check(int rc, grb_ctx* ctx, const char* what) {
     if (rc) throw std::runtime_error(std::string(what) + ": " + (ctx ? grb_last_error(ctx) : "error ") +
@@ -162,7 +168,7 @@ void lshape_stage(cudb::RouterState& state, grb_ctx* ctx, std::vector<int>& nets
 // congestion view comes from the stage tail; the host DAG builder is the
 // reference's; batching and route_prepared_topology's batch loop run on
 // grotor_b200.  Leaves the phase-two routes in state.routes_phase2_cpu.
-void flt_stage(cudb::RouterState& state, grb_ctx* ctx, std::vector<int>& nets2route, int32_t mode,
+void flt_stage(cudb::RouterState& state, grb_ctx* ctx, const grb_grid& grid, std::vector<int>& nets2route, int32_t mode,
                std::vector<unsigned char>& cong, std::vector<float>& xsum, std::vector<float>& ysum) {
     if (nets2route.empty()) return;
     auto& nets = state.nets;
@@ -244,6 +250,18 @@ void flt_stage(cudb::RouterState& state, grb_ctx* ctx, std::vector<int>& nets2ro
            st.dag_ms, nets2route.size(), nb);
     printf("BATCH_TIMING stage=detour backend=grotor_b200 elapsed_ms=%.6f nets=%zu batches=%d used_for_routing=1\n",
            st.batching_ms, nets2route.size(), nb);
+    if (report_traffic) {
+        std::vector<int32_t> plan(nets2route.size()), plan_off(size_t(nb) + 1);
+        int32_t pn = 0, pb = 0;
+        check(grb_get_plan(ctx, plan.data(), plan_off.data(), &pn, &pb), ctx, "grb_get_plan");
+        std::vector<int64_t> route_off(size_t(count) + 1);
+        for (int id = 0; id <= count; ++id)
+            route_off[id] = int64_t(state.pin_cnt_sum_cpu[id]) * int64_t(state.device.ROUTE_PER_PIN);
+        double bytes[3] = {0, 0, 0};
+        check(grb_flt_traffic(&grid, pb, plan_off.data(), plan.data(), &d, route_off.data(), state.routes_cpu.get(),
+                              state.routes_phase2_cpu.get(), 1, bytes), ctx, "grb_flt_traffic");
+        printf("FLT_TRAFFIC refresh_bytes=%.0f dp_bytes=%.0f commit_bytes=%.0f\n", bytes[0], bytes[1], bytes[2]);
+    }
 }
 
 // grotor::route (pipeline.hpp:14-157).  The output order is the reference's:
@@ -294,7 +312,7 @@ void route(cudb::RouterState& state, int32_t mode, bool stop_after_lshape) {
     nets2output = {};
     // Stage two sorts of_nets in place (flt.cuh:52), and the reference
     // publishes the rerouted nets in that order (pipeline.hpp:137,143).
-    flt_stage(state, ctx, of_nets, mode, cong, xsum, ysum);
+    flt_stage(state, ctx, G.g, of_nets, mode, cong, xsum, ysum);
     graph::finish_nets(state, of_nets);
     graph::output_nets(state, graph::collect_output_nets(std::move(nets2output)));
     nets2output = {};
@@ -308,7 +326,8 @@ int main(int argc, char** argv) {
         bool stop_after_lshape = false;
         if (argc < 7 || argc % 2 != 1)
             throw std::invalid_argument("Usage: grotor_grb -cap FILE -net FILE -out FILE [--lut-dir DIR] "
-                                        "[--executor persistent|plain|graph] [--stop-after lshape|routing]");
+                                        "[--executor persistent|plain|graph] [--stop-after lshape|routing] "
+                                        "[--report-traffic 0|1]");
         for (int i = 1; i < argc; i += 2) {
             const std::string option = argv[i], value = argv[i + 1];
             if (option == "-cap") cap = value;
@@ -316,6 +335,7 @@ int main(int argc, char** argv) {
             else if (option == "-out") output = value;
             else if (option == "--lut-dir") lut_dir = value;
             else if (option == "--executor") executor = value;
+            else if (option == "--report-traffic") drop_in::report_traffic = value == "1";
             else if (option == "--stop-after") {
                 if (value != "lshape" && value != "routing") throw std::invalid_argument("--stop-after expects lshape or routing");
                 stop_after_lshape = value == "lshape";

@@ -10,7 +10,8 @@ Records: BATCH_TIMING / DAG_TIMING per stage (the reference's stage metric is
 batching ms + DAG ms), TOPOLOGY_TIMING (stage one: FLUTE and the nets'
 topology; the stock program's also covers its host geometry and DFS),
 GROTOR_COMPLETE (wall seconds of the whole program, reading and writing
-included).
+included); for the first executor, FLT_TRAFFIC (the FLT stage's algorithmic
+bytes, grb_flt_traffic) and from it the stage kernel's roofline.
 
 Usage:  python integration/stage_timing.py [--workloads medium_320x320x10,large_800x800x10]
                                            [--executors persistent,plain] [--out FILE]
@@ -40,10 +41,13 @@ def records(text: str) -> dict:
     batch_stage = "lshape"
     for line in text.splitlines():
         tag, _, rest = line.partition(" ")
-        if tag not in ("BATCH_TIMING", "DAG_TIMING", "TOPOLOGY_TIMING", "GROTOR_COMPLETE", "PIPELINE_TIMING"):
+        if tag not in ("BATCH_TIMING", "DAG_TIMING", "TOPOLOGY_TIMING", "GROTOR_COMPLETE", "PIPELINE_TIMING",
+                       "FLT_TRAFFIC"):
             continue
         kv = dict(p.split("=", 1) for p in rest.split() if "=" in p)
-        if tag == "GROTOR_COMPLETE":
+        if tag == "FLT_TRAFFIC":
+            out["detour"]["algorithmic_bytes"] = {k: float(v) for k, v in kv.items()}
+        elif tag == "GROTOR_COMPLETE":
             out["wall_s"] = float(kv["wall_seconds"])
         elif tag == "PIPELINE_TIMING":
             out["pipeline"] = {k: float(v) for k, v in kv.items()}
@@ -62,7 +66,23 @@ def records(text: str) -> dict:
         r = out[st]
         if "batching_ms" in r and "dag_ms" in r:
             r["stage_ms"] = r["batching_ms"] + r["dag_ms"]
+    d = out["detour"]
+    if "algorithmic_bytes" in d and d.get("dag_ms"):
+        # Roofline of the FLT stage kernel (refresh + layer-change tables +
+        # DAG solve + commit in one launch): the model's bytes over its time.
+        peak, kind = measured_peak()
+        ach = sum(d["algorithmic_bytes"].values()) / (d["dag_ms"] / 1e3) / 1e9
+        d["roofline"] = {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
+                         "peak_source": f"{kind} hbm_gbs"}
     return out
+
+
+def measured_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
 
 
 def parse_out(path):
@@ -111,7 +131,8 @@ def measure(workload, executors, log):
         res["reference"]["scores"] = ref_scores
         for ex in executors:
             mine = os.path.join(w, f"{ex}.out")
-            text, t = run([DRIVER, "-cap", cap, "-net", net, "-out", mine, "--lut-dir", REF_DIR, "--executor", ex])
+            text, t = run([DRIVER, "-cap", cap, "-net", net, "-out", mine, "--lut-dir", REF_DIR, "--executor", ex,
+                           "--report-traffic", "1" if ex == executors[0] else "0"])
             log(f"{workload}: drop-in ({ex}) in {t:.1f} s")
             got = parse_out(mine)
             same_order = [a for a, _ in ref_nets] == [b for b, _ in got]
