@@ -43,6 +43,14 @@ class GrbTrees(C.Structure):
     _fields_ = [("n", C.c_int32), ("node_off", P), ("pos", P), ("adj_off", P), ("adj", P), ("route_off", P)]
 
 
+class GrbOutRecords(C.Structure):
+    _fields_ = [("n", C.c_int32), ("name_off", P), ("names", P), ("pin_off", P), ("pins", P), ("extra_off", P),
+                ("extra", P), ("sub_off", P), ("subnets", P), ("sub_phase2", P)]
+
+
+OUT_SINK = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_int64, C.c_void_p)
+
+
 class GrbStats(C.Structure):
     _fields_ = [
         ("total_wirelength", C.c_double), ("total_via_count", C.c_int64), ("n_batches", C.c_int32),
@@ -95,6 +103,8 @@ SIGNATURES = {
     "grb_upload_flt": (C.c_int, [P, C.POINTER(GrbFltDags)]),
     "grb_flt_stage": (C.c_int, [P, C.c_int32, C.c_int32, C.POINTER(GrbStats)]),
     "grb_read_routes2": (C.c_int, [P, P]),
+    "grb_format_out": (C.c_int, [P, C.POINTER(GrbOutRecords), C.POINTER(C.c_int64)]),
+    "grb_drain_out": (C.c_int, [P, OUT_SINK, P]),
     "grb_set_wire_cost_mode": (C.c_int, [P, C.c_int32]),
     "grb_autotune": (C.c_int, [P, C.c_int32, P, P]),
     "grb_softmin_forward": (C.c_int, [P, C.c_int32, C.c_double, P, P, C.c_double, P, C.POINTER(C.c_double)]),
@@ -109,6 +119,7 @@ SIGNATURES = {
     "grb_read_stage_tail": (C.c_int, [P, P, P, P, P]),
     "grb_read_tables": (C.c_int, [P, P, P, P, P, P]),
     "grb_read_routes": (C.c_int, [P, P]),
+    "grb_write_routes": (C.c_int, [P, P]),
     "grb_get_stats": (C.c_int, [P, C.POINTER(GrbStats)]),
     "grb_set_stats": (C.c_int, [P, C.c_double, C.c_int64]),
     "grb_sync": (C.c_int, [P]),

@@ -50,8 +50,7 @@ struct Soft {
     T* P;                // [cells] exclusive prefix of wc along each track
     T* dP;               // [cells] adjoint of P
     T* dvc;              // [cells] adjoint of vc
-    T* slot;             // per-thread scratch, 2 * slot_nodes * L * L values each
-    int slot_nodes;
+    T* slot;             // scratch: 2 * L * L values per node (range tables, adjoints)
     T* net_cost;         // [n_nets] soft root value of each net
 };
 

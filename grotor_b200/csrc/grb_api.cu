@@ -19,6 +19,7 @@
 #include "device/common.cuh"
 #include "device/cost.cuh"
 #include "device/flt.cuh"
+#include "device/outfmt.cuh"
 #include "device/lshape.cuh"
 #include "device/softmin.cuh"
 #include "device/topology.cuh"
@@ -547,20 +548,24 @@ __global__ void k_soft_prefix(Tables Tb, Soft<T> S) {
         acc += S.wc[base + q * stride];
     }
 }
+// One thread per net; a net's range tables (and their adjoints) sit in the
+// scratch at twice its first node's index times L*L, so every net of the
+// design runs at once.
 template <class T>
 __global__ void __launch_bounds__(kSoftThreads) k_soft_forward(Tables Tb, Soft<T> S, Plan P, int n) {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x, nt = gridDim.x * blockDim.x;
-    T* dist = S.slot + size_t(t) * 2 * S.slot_nodes * Tb.L * Tb.L;
-    for (int id = t; id < n; id += nt)
-        S.net_cost[id] = P.node_off[id + 1] > P.node_off[id] ? soft_net_forward<T>(Tb, S, P, id, dist) : T(0);
+    const int id = blockIdx.x * blockDim.x + threadIdx.x;
+    if (id >= n) return;
+    T* dist = S.slot + size_t(2) * P.node_off[id] * Tb.L * Tb.L;
+    S.net_cost[id] = P.node_off[id + 1] > P.node_off[id] ? soft_net_forward<T>(Tb, S, P, id, dist) : T(0);
 }
 template <class T>
 __global__ void __launch_bounds__(kSoftThreads) k_soft_backward(Tables Tb, Soft<T> S, Plan P, int n, T g) {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x, nt = gridDim.x * blockDim.x;
-    T* dist = S.slot + size_t(t) * 2 * S.slot_nodes * Tb.L * Tb.L;
-    T* gd = dist + size_t(S.slot_nodes) * Tb.L * Tb.L;
-    for (int id = t; id < n; id += nt)
-        if (P.node_off[id + 1] > P.node_off[id]) soft_net_backward<T>(Tb, S, P, id, dist, gd, g);
+    const int id = blockIdx.x * blockDim.x + threadIdx.x;
+    if (id >= n) return;
+    const int N = P.node_off[id + 1] - P.node_off[id];
+    T* dist = S.slot + size_t(2) * P.node_off[id] * Tb.L * Tb.L;
+    T* gd = dist + size_t(N) * Tb.L * Tb.L;
+    if (N > 0) soft_net_backward<T>(Tb, S, P, id, dist, gd, g);
 }
 // dwc[j] = sum over later track positions of dP (presum[i] = sum_{j<i} wc[j]).
 template <class T>
@@ -653,6 +658,16 @@ __global__ void k_topo_count(TopoBuild B) {
 __global__ void k_topo_fill(TopoBuild B) {
     const int id = blockIdx.x * blockDim.x + threadIdx.x;
     if (id < B.n) topo_fill(B, id);
+}
+
+// --- .out text (outfmt.cuh): one warp per record ---------------------------
+__global__ void k_out_count(OutRecords R) {
+    const int r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (r < R.n) out_count(R, r, threadIdx.x & 31);
+}
+__global__ void k_out_write(OutRecords R) {
+    const int r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (r < R.n) out_write(R, r, threadIdx.x & 31);
 }
 
 // --- batching kernels -------------------------------------------------------
@@ -1022,6 +1037,14 @@ struct grb_ctx {
     std::vector<void*> geom_bufs;     // batching geometry replacing the uploaded one
     std::vector<void*> flt_bufs;
     std::vector<void*> topo_bufs;     // grb_build_topology: uploaded trees, counts, DFS stack
+    // .out text (grb_format_out / grb_drain_out)
+    std::vector<void*> out_bufs;      // uploaded records and per-record byte offsets
+    char* out_text = nullptr;
+    long long out_text_cap = 0, out_bytes = 0;
+    bool out_pending = false;         // formatted text not yet drained
+    cudaStream_t out_stream = nullptr;
+    cudaEvent_t out_ready = nullptr, out_chunk_ev[2] = {nullptr, nullptr};
+    char* out_host[2] = {nullptr, nullptr};  // pinned chunk buffers
     long long topo_sizes[4] = {-1, 0, 0, 0};  // nodes, points, h-, v-segments of the net store (-1: none)
     Flt F{};
     long long route2_words = 0;
@@ -1465,12 +1488,10 @@ int z_stage_persistent(grb_ctx* c, int stamp0) {
 }
 
 // --- soft-min executors ------------------------------------------------------
-int soft_threads(const grb_ctx* c) { return c->sms * kSoftThreads; }
-
 int soft_workspace(grb_ctx* c) {
     const size_t cells = c->T.cells;
-    const int nodes = std::max(c->max_nodes, 1);
-    const size_t slot = size_t(soft_threads(c)) * 2 * nodes * c->T.L * c->T.L * sizeof(double);
+    // Range tables and adjoints of every node: 2 * nodes * L * L values.
+    const size_t slot = 2 * size_t(std::max(c->topo_sizes[0], 1ll)) * c->T.L * c->T.L * sizeof(double);
     if (c->soft_cells && c->soft_slot_bytes >= slot) return GRB_OK;
     GRB_CUDA(c, cudaStreamSynchronize(c->stream));
     free_all(c->soft_bufs);
@@ -1494,7 +1515,6 @@ Soft<T> soft_view(grb_ctx* c, double tau, const void* cap, const void* uw, doubl
     S.tau = static_cast<T>(tau);
     S.wc = a; S.vc = a + cells; S.P = a + 2 * cells; S.dP = a + 3 * cells; S.dvc = a + 4 * cells;
     S.slot = reinterpret_cast<T*>(c->soft_slot);
-    S.slot_nodes = std::max(c->max_nodes, 1);
     S.net_cost = net_cost;
     return S;
 }
@@ -1507,8 +1527,8 @@ int soft_forward(grb_ctx* c, double tau, const void* cap, const void* uw, double
     const int M = std::max(Tb.X, Tb.Y);
     k_soft_tables<T><<<(Tb.cells + 255) / 256, 256, 0, c->stream>>>(Tb, S);
     k_soft_prefix<T><<<(Tb.L * M + 127) / 128, 128, 0, c->stream>>>(Tb, S);
-    const int th = std::min(soft_threads(c), std::max(n, 1));
-    k_soft_forward<T><<<(th + kSoftThreads - 1) / kSoftThreads, kSoftThreads, 0, c->stream>>>(Tb, S, make_plan(c), n);
+    k_soft_forward<T><<<std::max(1, (n + kSoftThreads - 1) / kSoftThreads), kSoftThreads, 0, c->stream>>>(
+        Tb, S, make_plan(c), n);
     k_soft_sum<T><<<1, 1024, 0, c->stream>>>(net_cost, n, c->soft_scalar);
     c->launches += 4;
     GRB_CUDA(c, cudaGetLastError());
@@ -1530,9 +1550,8 @@ int soft_backward(grb_ctx* c, double tau, const void* cap, const void* uw, doubl
     k_soft_prefix<T><<<(Tb.L * M + 127) / 128, 128, 0, c->stream>>>(Tb, S);
     GRB_CUDA(c, cudaMemsetAsync(S.dP, 0, sizeof(T) * cells, c->stream));
     GRB_CUDA(c, cudaMemsetAsync(S.dvc, 0, sizeof(T) * cells, c->stream));
-    const int th = std::min(soft_threads(c), std::max(n, 1));
-    k_soft_backward<T><<<(th + kSoftThreads - 1) / kSoftThreads, kSoftThreads, 0, c->stream>>>(Tb, S, make_plan(c), n,
-                                                                                              static_cast<T>(g));
+    k_soft_backward<T><<<std::max(1, (n + kSoftThreads - 1) / kSoftThreads), kSoftThreads, 0, c->stream>>>(
+        Tb, S, make_plan(c), n, static_cast<T>(g));
     k_soft_suffix<T><<<(Tb.L * M + 127) / 128, 128, 0, c->stream>>>(Tb, S, dwc);
     k_soft_chain<T><<<(Tb.cells + 255) / 256, 256, 0, c->stream>>>(Tb, S, dwc, dcap, duw);
     k_soft_sum<T><<<1, 1024, 0, c->stream>>>(S.dvc, int(cells), c->soft_scalar + 1);
@@ -1918,6 +1937,14 @@ void grb_destroy(grb_ctx* c) {
     free_all(c->geom_bufs);
     free_all(c->flt_bufs);
     free_all(c->topo_bufs);
+    if (c->out_stream) cudaStreamSynchronize(c->out_stream);
+    free_all(c->out_bufs);
+    if (c->out_text) cudaFree(c->out_text);
+    for (char* h : c->out_host)
+        if (h) cudaFreeHost(h);
+    for (cudaEvent_t e : {c->out_ready, c->out_chunk_ev[0], c->out_chunk_ev[1]})
+        if (e) cudaEventDestroy(e);
+    if (c->out_stream) cudaStreamDestroy(c->out_stream);
     if (c->flt_eprefix) cudaFree(c->flt_eprefix);
     if (c->flt_emap) cudaFree(c->flt_emap);
     free_all(c->owned);
@@ -2154,6 +2181,145 @@ int grb_build_topology(grb_ctx* c, const grb_trees* t) {
         return fail(c, GRB_EINVAL, std::string(what[status[0]]) + " (net " + std::to_string(status[1]) + ")");
     }
     return validate_net_store(c, n, int(nn), rw, int(tot[0]), int(tot[1]), int(tot[2]));
+}
+
+// Chunk of the text copied to the host per sink call.
+constexpr long long kOutChunk = 64ll << 20;
+
+int grb_format_out(grb_ctx* c, const grb_out_records* rec, int64_t* bytes) {
+    if (!c || !rec || rec->n < 0 || !rec->name_off || !rec->pin_off || !rec->extra_off || !rec->sub_off || !bytes)
+        return c ? fail(c, GRB_EINVAL, "bad output records") : GRB_EINVAL;
+    if (c->out_pending) return fail(c, GRB_EINVAL, "the previous text has not been drained (grb_drain_out)");
+    GRB_CUDA(c, cudaSetDevice(c->device));
+    const int n = rec->n;
+    if (rec->name_off[0] != 0 || rec->pin_off[0] != 0 || rec->extra_off[0] != 0 || rec->sub_off[0] != 0)
+        return fail(c, GRB_EINVAL, "offsets must start at 0");
+    const long long nc = rec->name_off[n], np = rec->pin_off[n], ne = rec->extra_off[n], ns = rec->sub_off[n];
+    if (nc < 0 || np < 0 || ne < 0 || ns < 0) return fail(c, GRB_EINVAL, "negative totals");
+    for (int r = 0; r < n; ++r)
+        if (rec->name_off[r + 1] < rec->name_off[r] || rec->pin_off[r + 1] < rec->pin_off[r] ||
+            rec->extra_off[r + 1] < rec->extra_off[r] || rec->sub_off[r + 1] < rec->sub_off[r])
+            return fail(c, GRB_EINVAL, "offsets must be non-decreasing");
+    if ((nc && !rec->names) || (np && !rec->pins) || (ne && !rec->extra) || (ns && (!rec->subnets || !rec->sub_phase2)))
+        return fail(c, GRB_EINVAL, "record arrays missing");
+    if (ns && !c->routes) return fail(c, GRB_EINVAL, "no nets uploaded");
+    // The drain (possibly on another host thread, beside stage work on the
+    // context's stream) allocates and frees nothing: stream, events and the
+    // pinned chunk buffers are made here.
+    if (!c->out_stream) {
+        GRB_CUDA(c, cudaStreamCreateWithFlags(&c->out_stream, cudaStreamNonBlocking));
+        GRB_CUDA(c, cudaEventCreateWithFlags(&c->out_ready, cudaEventDisableTiming));
+        // Blocking events: the draining thread sleeps instead of spinning on a
+        // core the caller's pipeline may need.
+        for (cudaEvent_t& e : c->out_chunk_ev)
+            GRB_CUDA(c, cudaEventCreateWithFlags(&e, cudaEventDisableTiming | cudaEventBlockingSync));
+    }
+    for (char*& h : c->out_host)
+        if (!h && cudaMallocHost(&h, size_t(kOutChunk)) != cudaSuccess) {
+            cudaGetLastError();
+            return fail(c, GRB_ENOMEM, "pinned output buffers");
+        }
+    free_all(c->out_bufs);
+    long long* d_name_off = nullptr, *d_bytes = nullptr, *d_sums = nullptr;
+    char* d_names = nullptr;
+    int *d_pin_off = nullptr, *d_pins = nullptr, *d_extra_off = nullptr, *d_extra = nullptr, *d_sub_off = nullptr,
+        *d_subnets = nullptr, *d_status = nullptr;
+    unsigned char* d_phase2 = nullptr;
+    const int tiles = (n + kScanTile - 1) / kScanTile;
+    int rc = 0;
+    rc |= dalloc(c, &d_name_off, n + 1, c->out_bufs);
+    rc |= dalloc(c, &d_names, std::max(nc, 1ll), c->out_bufs);
+    rc |= dalloc(c, &d_pin_off, n + 1, c->out_bufs);
+    rc |= dalloc(c, &d_pins, std::max(np, 1ll), c->out_bufs);
+    rc |= dalloc(c, &d_extra_off, n + 1, c->out_bufs);
+    rc |= dalloc(c, &d_extra, std::max(ne, 1ll), c->out_bufs);
+    rc |= dalloc(c, &d_sub_off, n + 1, c->out_bufs);
+    rc |= dalloc(c, &d_subnets, std::max(ns, 1ll), c->out_bufs);
+    rc |= dalloc(c, &d_phase2, std::max(ns, 1ll), c->out_bufs);
+    rc |= dalloc(c, &d_bytes, n + 1, c->out_bufs);
+    rc |= dalloc(c, &d_sums, tiles + 1, c->out_bufs);
+    rc |= dalloc(c, &d_status, 2, c->out_bufs);
+    if (rc) { free_all(c->out_bufs); return fail(c, GRB_ENOMEM, "output records"); }
+    auto h2d = [&](void* dst, const void* src, size_t b) {
+        return b ? cudaMemcpyAsync(dst, src, b, cudaMemcpyHostToDevice, c->stream) : cudaSuccess;
+    };
+    GRB_CUDA(c, h2d(d_name_off, rec->name_off, 8 * (size_t(n) + 1)));
+    GRB_CUDA(c, h2d(d_names, rec->names, size_t(nc)));
+    GRB_CUDA(c, h2d(d_pin_off, rec->pin_off, 4 * (size_t(n) + 1)));
+    GRB_CUDA(c, h2d(d_pins, rec->pins, 4 * size_t(np)));
+    GRB_CUDA(c, h2d(d_extra_off, rec->extra_off, 4 * (size_t(n) + 1)));
+    GRB_CUDA(c, h2d(d_extra, rec->extra, 4 * size_t(ne)));
+    GRB_CUDA(c, h2d(d_sub_off, rec->sub_off, 4 * (size_t(n) + 1)));
+    GRB_CUDA(c, h2d(d_subnets, rec->subnets, 4 * size_t(ns)));
+    GRB_CUDA(c, h2d(d_phase2, rec->sub_phase2, size_t(ns)));
+    GRB_CUDA(c, cudaMemsetAsync(d_status, 0, 2 * sizeof(int), c->stream));
+    OutRecords R{n, c->T.X, c->T.Y, d_name_off, d_names, d_pin_off, d_pins, d_extra_off, d_extra, d_sub_off,
+                 d_subnets, d_phase2, c->route_off, c->routes, c->F.route2_off, c->F.routes2, d_bytes, nullptr,
+                 d_status, c->n_nets};
+    if (!c->F.routes2) R.route2_off = nullptr;
+    const int blocks = std::max(1, (n + 7) / 8);  // 8 warps per CTA
+    if (n) k_out_count<<<blocks, 256, 0, c->stream>>>(R);
+    if (n) k_scan_tiles<<<tiles, 256, 0, c->stream>>>(d_bytes, n, d_sums);
+    k_scan_sums<<<1, 1024, 0, c->stream>>>(d_sums, tiles);
+    k_scan_add<<<n / 256 + 1, 256, 0, c->stream>>>(d_bytes, n, d_sums, tiles);
+    c->launches += (n ? 2 : 0) + 2;
+    GRB_CUDA(c, cudaGetLastError());
+    long long total = 0;
+    int status[2] = {0, 0};
+    GRB_CUDA(c, cudaMemcpyAsync(&total, d_bytes + n, sizeof(long long), cudaMemcpyDeviceToHost, c->stream));
+    GRB_CUDA(c, cudaMemcpyAsync(status, d_status, sizeof(status), cudaMemcpyDeviceToHost, c->stream));
+    GRB_CUDA(c, cudaStreamSynchronize(c->stream));
+    if (status[0]) {
+        free_all(c->out_bufs);
+        return fail(c, GRB_EINVAL, "record " + std::to_string(status[1]) + ": subnet id or its route words invalid");
+    }
+    if (total > c->out_text_cap) {
+        if (c->out_text) cudaFree(c->out_text);
+        c->out_text = nullptr;
+        c->out_text_cap = 0;
+        if (cudaMalloc(&c->out_text, size_t(std::max(total, 1ll))) != cudaSuccess) {
+            cudaGetLastError();
+            free_all(c->out_bufs);
+            return fail(c, GRB_ENOMEM, "output text");
+        }
+        c->out_text_cap = total;
+    }
+    R.text = c->out_text;
+    if (n) k_out_write<<<blocks, 256, 0, c->stream>>>(R);
+    c->launches += n ? 1 : 0;
+    GRB_CUDA(c, cudaGetLastError());
+    GRB_CUDA(c, cudaEventRecord(c->out_ready, c->stream));
+    c->out_bytes = total;
+    c->out_pending = true;
+    *bytes = total;
+    return GRB_OK;
+}
+
+int grb_drain_out(grb_ctx* c, grb_out_sink sink, void* user) {
+    if (!c || !sink) return c ? fail(c, GRB_EINVAL, "no sink") : GRB_EINVAL;
+    if (!c->out_pending) return GRB_OK;
+    GRB_CUDA(c, cudaSetDevice(c->device));
+    GRB_CUDA(c, cudaStreamWaitEvent(c->out_stream, c->out_ready, 0));
+    const long long total = c->out_bytes;
+    const long long chunks = (total + kOutChunk - 1) / kOutChunk;
+    auto issue = [&](long long k) {
+        const long long off = k * kOutChunk, len = std::min(kOutChunk, total - off);
+        cudaError_t e = cudaMemcpyAsync(c->out_host[k & 1], c->out_text + off, size_t(len), cudaMemcpyDeviceToHost,
+                                        c->out_stream);
+        if (e == cudaSuccess) e = cudaEventRecord(c->out_chunk_ev[k & 1], c->out_stream);
+        return e;
+    };
+    if (chunks) GRB_CUDA(c, issue(0));
+    int rc = GRB_OK;
+    for (long long k = 0; k < chunks; ++k) {
+        GRB_CUDA(c, cudaEventSynchronize(c->out_chunk_ev[k & 1]));
+        if (k + 1 < chunks) GRB_CUDA(c, issue(k + 1));  // the other buffer was consumed at step k - 1
+        const long long len = std::min(kOutChunk, total - k * kOutChunk);
+        if (sink(c->out_host[k & 1], len, user) != 0) { rc = fail(c, GRB_EINVAL, "the output sink failed"); break; }
+    }
+    // (every copy has been waited for through its chunk event)
+    c->out_pending = false;
+    return rc;
 }
 
 int grb_topology_sizes(grb_ctx* c, int64_t* sizes) {
@@ -3177,6 +3343,15 @@ int grb_read_routes(grb_ctx* c, int32_t* routes) {
     if (!c || !routes) return GRB_EINVAL;
     GRB_CUDA(c, cudaSetDevice(c->device));
     if (c->route_words) GRB_CUDA(c, cudaMemcpyAsync(routes, c->routes, sizeof(int) * c->route_words, cudaMemcpyDeviceToHost, c->stream));
+    GRB_CUDA(c, cudaStreamSynchronize(c->stream));
+    return GRB_OK;
+}
+
+int grb_write_routes(grb_ctx* c, const int32_t* routes) {
+    if (!c || !routes) return c ? fail(c, GRB_EINVAL, "null routes") : GRB_EINVAL;
+    GRB_CUDA(c, cudaSetDevice(c->device));
+    if (c->route_words)
+        GRB_CUDA(c, cudaMemcpyAsync(c->routes, routes, sizeof(int) * c->route_words, cudaMemcpyHostToDevice, c->stream));
     GRB_CUDA(c, cudaStreamSynchronize(c->stream));
     return GRB_OK;
 }

@@ -197,6 +197,42 @@ class Router:
             "node_off", "nodes", "parents", "point_off", "points", "hseg_off", "hsegs", "vseg_off", "vsegs"))))
         return out
 
+    def write_out(self, names, pins, extra, subnets, phase2=None) -> bytes:
+        """The .out text of output records (graph::output_nets), formatted on
+        the device from the context's routes (grb_format_out) and drained to
+        the host (grb_drain_out).  Per record: its name, its 3-D pins, its
+        extra route pairs (flat 3-D positions) and its subnet ids, with
+        per-subnet phase-two flags (default 0)."""
+        def csr(lists, dtype):
+            off = np.zeros(len(lists) + 1, np.int32)
+            off[1:] = np.cumsum([len(v) for v in lists])
+            flat = np.concatenate([np.asarray(v, dtype) for v in lists]) if lists else np.zeros(0, dtype)
+            return off, np.ascontiguousarray(flat, dtype)
+        raw = [n.encode() if isinstance(n, str) else bytes(n) for n in names]
+        name_off = np.zeros(len(raw) + 1, np.int64)
+        name_off[1:] = np.cumsum([len(b) for b in raw])
+        name_buf = np.frombuffer(b"".join(raw) or b"\0", np.uint8)
+        pin_off, pin_flat = csr(pins, np.int32)
+        extra_off, extra_flat = csr(extra, np.int32)
+        sub_off, sub_flat = csr(subnets, np.int32)
+        if phase2 is None:
+            phase2 = [np.zeros(len(v), np.uint8) for v in subnets]
+        _, ph_flat = csr(phase2, np.uint8)
+        rec = _abi.GrbOutRecords(len(raw), _p(name_off), _p(name_buf), _p(pin_off), _p(pin_flat), _p(extra_off),
+                                 _p(extra_flat), _p(sub_off), _p(sub_flat), _p(ph_flat))
+        nbytes = C.c_int64(0)
+        self._check(self._lib.grb_format_out(self._ctx, C.byref(rec), C.byref(nbytes)))
+        parts = []
+
+        def sink(data, size, _user):
+            parts.append(C.string_at(data, size))
+            return 0
+        cb = _abi.OUT_SINK(sink)
+        self._check(self._lib.grb_drain_out(self._ctx, cb, None))
+        text = b"".join(parts)
+        assert len(text) == nbytes.value
+        return text
+
     # -- batching ------------------------------------------------------------
     def generate_batches_rsmt(self, order, limit: int = 1000000, sparsity: int = 1, mode="persistent"):
         """Exact first-fit batching; installs the reversed, flattened plan and

@@ -238,6 +238,45 @@ int grb_upload_flt(grb_ctx* ctx, const grb_flt_dags* dags);
  * phase-two routes.  mode: GRB_MODE_PLAIN, GRAPH or PERSISTENT. */
 int grb_flt_stage(grb_ctx* ctx, int32_t remove_phase_one, int32_t mode, grb_stats* stats);
 
+/* ---- .out writer (graph::output_nets, output.hpp:79-112) ---------------- */
+/* Output records in output order, as graph::collect_output_nets hands them to
+ * the writer (output.hpp:16-26): per record its name, its pins (3-D positions;
+ * a pin on layer 0 is written as a via to layer 1), extra route pairs (3-D
+ * positions, two per segment) and subnets (net ids of the context), each with
+ * its rip-up flag (RouterState::ripup_flag_cpu: 1 selects the phase-two
+ * routes). */
+typedef struct grb_out_records {
+    int32_t n;
+    const int64_t* name_off;       /* [n+1] into names */
+    const char* names;
+    const int32_t* pin_off;        /* [n+1] */
+    const int32_t* pins;
+    const int32_t* extra_off;      /* [n+1] */
+    const int32_t* extra;
+    const int32_t* sub_off;        /* [n+1] */
+    const int32_t* subnets;
+    const uint8_t* sub_phase2;
+} grb_out_records;
+
+/* Receives the text in order; returns 0 to go on. */
+typedef int (*grb_out_sink)(const char* data, int64_t bytes, void* user);
+
+/* Format the records' .out text on the device -- exactly the bytes
+ * graph::output_nets writes through grotor::RouteWriter (output_writer.hpp:
+ * 29-43) from the context's current routes (stage one, and phase two for
+ * flagged subnets) -- and leave it for grb_drain_out.  Returns its size in
+ * *bytes.  The formatting is queued on the context's stream; the routes it
+ * reads are those of the work queued before it. */
+int grb_format_out(grb_ctx* ctx, const grb_out_records* records, int64_t* bytes);
+
+/* Hand the formatted text to `sink` in order, in chunks of 64 MiB: chunk k+1
+ * is copied (on the context's copy stream) while the sink consumes chunk k.
+ * May run on another host thread while the calling thread queues further
+ * stage work on the same context (the drain allocates nothing and touches no
+ * other state); one text at a time: grb_format_out refuses while one is
+ * pending. */
+int grb_drain_out(grb_ctx* ctx, grb_out_sink sink, void* user);
+
 /* Copy all phase-two route words (route2_off[n] words) to the host. */
 int grb_read_routes2(grb_ctx* ctx, int32_t* routes2);
 
@@ -338,6 +377,11 @@ int grb_read_tables(grb_ctx* ctx, float* wcost, float* vcost, double* presum, in
                     int32_t* timestamp);
 /* Copy all route words (route_off[n] words) to the host. */
 int grb_read_routes(grb_ctx* ctx, int32_t* routes);
+/* Replace all route words (route_off[n] words) from the host: routes a caller
+ * edited after a stage (the GGR pipeline's promote_congested_segments and
+ * canonicalize_routes, zshape_topology.hpp:122-248) for grb_format_out.
+ * Demand and timestamps are left as they are. */
+int grb_write_routes(grb_ctx* ctx, const int32_t* routes);
 int grb_get_stats(grb_ctx* ctx, grb_stats* stats);
 /* Set the statistics counters (the reference uploads RouterState::statistics,
  * whose via count starts at the number of metal1 pins, preprocess.hpp:1716-1718

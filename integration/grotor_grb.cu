@@ -21,14 +21,19 @@
 //     186-192): the reference's host FLT DAG builder (process_net,
 //     flt.cuh:8-46) runs unchanged on the congestion view; batching and the
 //     DAG execution loop of route_prepared_topology (flt.cuh:75-182) run in
-//     grb_plan_batches + grb_upload_flt + grb_flt_stage.
+//     grb_plan_batches + grb_upload_flt + grb_flt_stage;
+//   * the .out writer, graph::output_nets (src/output.hpp:79-112): the text of
+//     each part of the file is formatted on the device from the device's
+//     routes (grb_format_out) and drained into the file by a host task
+//     (grb_drain_out) that overlaps the next stage, where the reference's
+//     output task (pipeline.hpp:20-35) formats on the host.
 //
 // Everything else -- CAP/NET parsing (db::read), net splitting
-// (prepare_routing_nets), FLUTE, the FLT DAG builder, finish_nets and the .out
-// writer (output_nets) -- is the reference's code, so the same input gives
-// the same .out (stage-one nets byte for byte; for stage-two nets the
-// reference's own segment order is not defined, so the segments of each net
-// are compared as a set).
+// (prepare_routing_nets), FLUTE, the FLT DAG builder, finish_nets and
+// collect_output_nets -- is the reference's code, so the same input gives the
+// same .out (stage-one nets byte for byte; for stage-two nets the reference's
+// own segment order is not defined, so the segments of each net are compared
+// as a set).
 //
 // Usage: grotor_grb -cap FILE -net FILE -out FILE [--lut-dir DIR]
 //                   [--executor persistent|plain|graph] [--stop-after lshape|routing]
@@ -36,8 +41,9 @@
 #include "pipeline.hpp"
 
 #include <filesystem>
+#include <future>
 
-#include "grb.h"
+#include "drop_in.cuh"
 #include "grb_prof.h"
 
 namespace drop_in {
@@ -46,91 +52,9 @@ namespace drop_in {
 // beside its timing, for its roofline.
 bool report_traffic = false;
 
-void check(int rc, grb_ctx* ctx, const char* what) {
-    if (rc) throw std::runtime_error(std::string(what) + ": " + (ctx ? grb_last_error(ctx) : "error ") +
-                                     " (code " + std::to_string(rc) + ")");
-}
-
-// The grid tables of build_cuda_database (preprocess.hpp:1625-1786).
-struct Grid {
-    std::vector<double> short_costs;
-    std::vector<int32_t> xlen, ylen;
-    std::vector<float> capacity;
-    grb_grid g{};
-};
-
-Grid make_grid(const cudb::RouterState& state) {
-    Grid G;
-    const int L = state.device.L, X = state.device.X, Y = state.device.Y;
-    for (int l = 0; l < L; ++l) G.short_costs.push_back(db::unit_length_short_costs[l + 1]);
-    for (int x = 0; x + 1 < X; ++x) G.xlen.push_back(db::x_edge_len[x]);
-    for (int y = 0; y + 1 < Y; ++y) G.ylen.push_back(db::y_edge_len[y]);
-    G.capacity.resize(size_t(L) * X * Y);
-    for (int l = 0; l < L; ++l)
-        for (int x = 0; x < X; ++x)
-            for (int y = 0; y < Y; ++y) G.capacity[(size_t(l) * X + x) * Y + y] = float(db::capacity[l + 1][x][y]);
-    G.g.L = L;
-    G.g.X = X;
-    G.g.Y = Y;
-    G.g.DIR = db::layers[1].dir;
-    G.g.unit_length_wire_cost = db::unit_length_wire_cost;
-    G.g.unit_via_cost = db::unit_via_cost;
-    G.g.of_cost_scale = 1.0;  // router_state.hpp:37 on one GPU
-    G.g.unit_length_short_costs = G.short_costs.data();
-    G.g.x_edge_len = G.xlen.data();
-    G.g.y_edge_len = G.ylen.data();
-    G.g.capacity = G.capacity.data();
-    return G;
-}
-
-// Every net's Steiner tree as FLUTE leaves it in net::rsmt (node positions
-// with their layer, then each node's adjacency list; preprocess.hpp:72-93,
-// 124-126) and its route words at the reference's own offsets
-// (pin_cnt_sum_cpu * ROUTE_PER_PIN, router_state.hpp:31) -- all by net id.
-// grb_build_topology turns them into the depth-first trees of Lshape_route
-// (lshape.cuh:85-98) and the batching geometry of construct_rsmt
-// (preprocess.hpp:95-123) on the device.
-struct Trees {
-    std::vector<int32_t> node_off{0}, pos, adj_off{0}, adj;
-    std::vector<int64_t> route_off;
-    grb_trees t{};
-};
-
-Trees flatten_trees(const cudb::RouterState& state) {
-    Trees F;
-    const auto& nets = state.nets;
-    const int count = int(nets.size());
-    for (int id = 0; id < count; ++id) {
-        const auto& graph = nets[id].rsmt;
-        const size_t size = graph.empty() ? 0 : graph.back().size();
-        for (size_t i = 0; i < size; ++i) {
-            F.pos.push_back(graph.back()[i]);
-            F.adj.insert(F.adj.end(), graph[i].begin(), graph[i].end());
-            F.adj_off.push_back(int32_t(F.adj.size()));
-        }
-        F.node_off.push_back(int32_t(F.pos.size()));
-    }
-    for (int id = 0; id <= count; ++id)
-        F.route_off.push_back(int64_t(state.pin_cnt_sum_cpu[id]) * int64_t(state.device.ROUTE_PER_PIN));
-    F.t.n = count;
-    F.t.node_off = F.node_off.data();
-    F.t.pos = F.pos.data();
-    F.t.adj_off = F.adj_off.data();
-    F.t.adj = F.adj.data();
-    F.t.route_off = F.route_off.data();
-    return F;
-}
-
-int32_t executor_mode(const std::string& name) {
-    if (name == "persistent") return GRB_MODE_PERSISTENT;
-    if (name == "plain") return GRB_MODE_PLAIN;
-    if (name == "graph") return GRB_MODE_GRAPH;
-    throw std::invalid_argument("--executor expects persistent, plain or graph");
-}
-
 // Stage one: Lshape_route (lshape.cuh:21-197) with batching, cost refresh,
 // DAG and commit on grotor_b200.  Leaves nets2route in the plan order, as
-// the reference does, and the phase-one routes in state.routes_cpu.
+// the reference does.
 void lshape_stage(cudb::RouterState& state, grb_ctx* ctx, std::vector<int>& nets2route, int32_t mode,
                   int64_t initial_vias, bool tail) {
     auto& nets = state.nets;
@@ -155,9 +79,11 @@ void lshape_stage(cudb::RouterState& state, grb_ctx* ctx, std::vector<int>& nets
     std::vector<int32_t> batch_off(nb + 1);
     int32_t n = 0, nb2 = 0;
     check(grb_get_plan(ctx, nets2route.data(), batch_off.data(), &n, &nb2), ctx, "grb_get_plan");
-    const size_t words = size_t(state.device.ROUTE_PER_PIN) * state.device.PIN_NUM + 1;
-    state.routes_cpu.reset(new int[words]());
-    check(grb_read_routes(ctx, state.routes_cpu.get()), ctx, "grb_read_routes");
+    if (report_traffic) {  // the .out is written from the device's routes; the host copy feeds the byte model
+        const size_t words = size_t(state.device.ROUTE_PER_PIN) * state.device.PIN_NUM + 1;
+        state.routes_cpu.reset(new int[words]());
+        check(grb_read_routes(ctx, state.routes_cpu.get()), ctx, "grb_read_routes");
+    }
     printf("DAG_TIMING stage=lshape batch_index=-1 elapsed_ms=%.6f nets=%zu batches=%d executor=grotor_b200\n",
            st.dag_ms, nets2route.size(), nb);
     printf("BATCH_TIMING backend=grotor_b200 elapsed_ms=%.6f nets=%zu batches=%d used_for_routing=1\n",
@@ -167,7 +93,7 @@ void lshape_stage(cudb::RouterState& state, grb_ctx* ctx, std::vector<int>& nets
 // Stage two: Lshape_route_detour::route_detour (flt.cuh:186-192).  The
 // congestion view comes from the stage tail; the host DAG builder is the
 // reference's; batching and route_prepared_topology's batch loop run on
-// grotor_b200.  Leaves the phase-two routes in state.routes_phase2_cpu.
+// grotor_b200.
 void flt_stage(cudb::RouterState& state, grb_ctx* ctx, const grb_grid& grid, std::vector<int>& nets2route, int32_t mode,
                std::vector<unsigned char>& cong, std::vector<float>& xsum, std::vector<float>& ysum) {
     if (nets2route.empty()) return;
@@ -243,9 +169,11 @@ void flt_stage(cudb::RouterState& state, grb_ctx* ctx, const grb_grid& grid, std
     check(grb_upload_flt(ctx, &d), ctx, "grb_upload_flt");
     grb_stats st{};
     check(grb_flt_stage(ctx, 1, mode, &st), ctx, "grb_flt_stage");
-    const size_t words = size_t(state.device.ROUTE_PER_PIN_PHASE2) * state.device.PIN_NUM_PHASE2 + 1;
-    state.routes_phase2_cpu.reset(new int[std::max<size_t>(words, size_t(route2_off.back()) + 1)]());
-    check(grb_read_routes2(ctx, state.routes_phase2_cpu.get()), ctx, "grb_read_routes2");
+    if (report_traffic) {
+        const size_t words = size_t(state.device.ROUTE_PER_PIN_PHASE2) * state.device.PIN_NUM_PHASE2 + 1;
+        state.routes_phase2_cpu.reset(new int[std::max<size_t>(words, size_t(route2_off.back()) + 1)]());
+        check(grb_read_routes2(ctx, state.routes_phase2_cpu.get()), ctx, "grb_read_routes2");
+    }
     printf("DAG_TIMING stage=detour batch_index=-1 elapsed_ms=%.6f nets=%zu batches=%d executor=grotor_b200\n",
            st.dag_ms, nets2route.size(), nb);
     printf("BATCH_TIMING stage=detour backend=grotor_b200 elapsed_ms=%.6f nets=%zu batches=%d used_for_routing=1\n",
@@ -272,19 +200,22 @@ void route(cudb::RouterState& state, int32_t mode, bool stop_after_lshape) {
     int64_t initial_vias = 0;  // one via per metal1 pin (preprocess.hpp:1716-1718)
     for (auto& dbnet : db::nets)
         for (int pin : dbnet.pins) initial_vias += pin < state.device.X * state.device.Y;
-    for (int i = 0; i < int(db::nets.size()); ++i)
-        if (db::nets[i].pins.size() == 1) nets2output.push(i);
     Grid G = make_grid(state);
     grb_ctx* ctx = nullptr;
     check(grb_create(&G.g, 0, &ctx), nullptr, "grb_create");
     std::unique_ptr<grb_ctx, void (*)(grb_ctx*)> owner(ctx, grb_destroy);
+    Output out{ctx};
+    // Single-pin nets first (pipeline.hpp:57-59), written while stage one runs.
+    for (int i = 0; i < int(db::nets.size()); ++i)
+        if (db::nets[i].pins.size() == 1) nets2output.push(i);
+    out.start(state);
     std::vector<int> all_nets(state.nets.size());
     std::iota(all_nets.begin(), all_nets.end(), 0);
     lshape_stage(state, ctx, all_nets, mode, initial_vias, !stop_after_lshape);
     if (stop_after_lshape) {
         graph::finish_nets(state, all_nets);
-        graph::output_nets(state, graph::collect_output_nets(std::move(nets2output)));
-        nets2output = {};
+        out.start(state);
+        out.wait();
         return;
     }
     // pipeline.hpp:86-106: classification, phase-two offsets (the global
@@ -306,16 +237,16 @@ void route(cudb::RouterState& state, int32_t mode, bool stop_after_lshape) {
         state.ripup_flag_cpu[id] = 1;
     }
     state.device.PIN_NUM_PHASE2 = pin_count;
-    // The nets without overflow are written before stage two, as the
-    // reference's output task does.
-    graph::output_nets(state, graph::collect_output_nets(std::move(nets2output)));
-    nets2output = {};
+    // The nets without overflow are written while stage two runs, as the
+    // reference's output task does (pipeline.hpp:108-109).
+    out.start(state);
     // Stage two sorts of_nets in place (flt.cuh:52), and the reference
     // publishes the rerouted nets in that order (pipeline.hpp:137,143).
     flt_stage(state, ctx, G.g, of_nets, mode, cong, xsum, ysum);
     graph::finish_nets(state, of_nets);
-    graph::output_nets(state, graph::collect_output_nets(std::move(nets2output)));
-    nets2output = {};
+    out.start(state);
+    out.wait();
+    printf("OUTPUT_TIMING format_ms=%.3f output_wait_ms=%.3f executor=grotor_b200\n", out.format_ms, out.wait_ms);
 }
 
 }  // namespace drop_in

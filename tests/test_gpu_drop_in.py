@@ -9,7 +9,9 @@ L-shape stage), as a set for nets rerouted by stage two (the reference's FLT
 stage appends segments with atomics, so their order is not defined) -- and
 the reference evaluator's scores (wirelength, via, overflow and total cost,
 open and incomplete nets) identical.  Runs on a congested design (many FLT
-nets) and on the seeded 320x320x10 design with 120,000 nets.
+nets) and on the seeded 320x320x10 design with 120,000 nets.  The GGR
+pipeline's drop-in (integration/grotor_grb_ggr) against the reference's own
+GGR build: the whole .out byte for byte.
 """
 import os
 import subprocess
@@ -24,12 +26,18 @@ pytestmark = pytest.mark.gpu
 REF_DIR = os.path.join(ROOT, "oracle", "_ref")
 STOCK = os.path.join(REF_DIR, "grotor")
 DRIVER = os.path.join(ROOT, "integration", "_build", "grotor_grb")
+STOCK_GGR = os.path.join(REF_DIR, "grotor_ggr")
+DRIVER_GGR = os.path.join(ROOT, "integration", "_build", "grotor_grb_ggr")
 EVALUATOR = os.path.join(REF_DIR, "evaluator")
 
 DESIGNS = {
     "congested_48x48x10_1500": ("small_64x64x5", dict(n_nets=1500, cap_layers=10, seed=13, X=48, Y=48, cap_lo=1,
                                                      cap_hi=4)),
     "medium_320x320x10": ("medium_320x320x10", {}),
+}
+GGR_DESIGNS = {
+    "ggr_48x48x10_1500": ("small_64x64x5", dict(n_nets=1500, cap_layers=10, seed=13, X=48, Y=48)),
+    "ggr_160x160x10_20k": ("medium_320x320x10", dict(n_nets=20000, X=160, Y=160, big_lo=80, big_hi=160, seed=21)),
 }
 
 
@@ -85,3 +93,28 @@ def test_drop_in_matches_stock_reference(name, tmp_path):
         assert open(ref_out, "rb").read() == open(mine, "rb").read()
     assert scores(cap, net, ref_out) == scores(cap, net, mine)
     print(f"{name}: {len(a)} nets, {reordered} with stage-two segments in another order")
+
+
+@pytest.mark.parametrize("name", list(GGR_DESIGNS))
+def test_ggr_drop_in_matches_stock_reference(name, tmp_path):
+    """The GGR pipeline (the reference's grotor_ggr build, pipeline_ggr.hpp):
+    first-fit groups, bounding-box batches and the Z-shape stage on
+    grotor_b200, the reference's post-processing, the device writer; the .out
+    must be byte-identical to the stock GGR program's, with identical scores."""
+    if not (os.path.exists(STOCK_GGR) and os.path.exists(DRIVER_GGR)):
+        pytest.skip("stock GGR reference or GGR drop-in driver not built (oracle/ref.mk, integration/Makefile)")
+    from grotor_b200.synth import WORKLOADS, Design
+    wl, over = GGR_DESIGNS[name]
+    cap, net = str(tmp_path / "d.cap"), str(tmp_path / "d.net")
+    Design(replace(WORKLOADS[wl], **over)).write(cap, net)
+    ref_out, mine = str(tmp_path / "ref.out"), str(tmp_path / "mine.out")
+    r = subprocess.run([STOCK_GGR, "-cap", cap, "-net", net, "-out", ref_out, "--lut-dir", REF_DIR, "--report-score",
+                        "0"], capture_output=True, text=True, timeout=900)
+    assert r.returncode == 0, r.stderr[-3000:]
+    for ex in ("persistent", "plain"):
+        m = subprocess.run([DRIVER_GGR, "-cap", cap, "-net", net, "-out", mine, "--lut-dir", REF_DIR, "--executor", ex],
+                           capture_output=True, text=True, timeout=900)
+        assert m.returncode == 0, m.stderr[-3000:]
+        a, b = open(ref_out, "rb").read(), open(mine, "rb").read()
+        assert a == b, f"{ex}: .out differs ({len(a)} vs {len(b)} bytes)"
+    assert scores(cap, net, ref_out) == scores(cap, net, mine)
