@@ -103,6 +103,12 @@ SIGNATURES = {
     "grb_upload_flt": (C.c_int, [P, C.POINTER(GrbFltDags)]),
     "grb_flt_stage": (C.c_int, [P, C.c_int32, C.c_int32, C.POINTER(GrbStats)]),
     "grb_read_routes2": (C.c_int, [P, P]),
+    "grb_write_routes2": (C.c_int, [P, P]),
+    "grb_remove_routes": (C.c_int, [P, P, C.c_int32, P]),
+    "grb_ripup_classify_phase2": (C.c_int, [P, C.c_int32, P, P]),
+    "grb_routing_score": (C.c_int, [P, C.POINTER(C.c_double)]),
+    "grb_checkpoint": (C.c_int, [P]),
+    "grb_restore": (C.c_int, [P]),
     "grb_format_out": (C.c_int, [P, C.POINTER(GrbOutRecords), C.POINTER(C.c_int64)]),
     "grb_drain_out": (C.c_int, [P, OUT_SINK, P]),
     "grb_set_wire_cost_mode": (C.c_int, [P, C.c_int32]),

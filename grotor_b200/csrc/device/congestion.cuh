@@ -45,12 +45,10 @@ __device__ __forceinline__ int overflow_tracks(const Tables& T) {
 
 // mark_overflow_nets (congestion.cuh:22-58): net `id` is flagged when its
 // wires cross more than 10 overflowing edges.
-__device__ __forceinline__ void overflow_net(const Tables& T, const Plan& P, const int* of_sum, unsigned char* is_of,
-                                             int id) {
-    const int* r = P.routes + P.route_off[id];
+__device__ __forceinline__ unsigned char overflow_route(const Tables& T, const int* r, bool has, const int* of_sum) {
     int count = 0;
     unsigned char flag = 0;
-    if (P.route_off[id + 1] > P.route_off[id]) {
+    if (has) {
         for (int i = 1; i < r[0]; i += 2) {
             const int a = r[i], b = r[i + 1], l = a / T.XY, ra = a % T.XY, rb = b % T.XY;
             const int x0 = ra / T.Y, y0 = ra % T.Y, x1 = rb / T.Y, y1 = rb % T.Y;
@@ -59,7 +57,11 @@ __device__ __forceinline__ void overflow_net(const Tables& T, const Plan& P, con
             if (count > 10) { flag = 1; break; }
         }
     }
-    is_of[id] = flag;
+    return flag;
+}
+__device__ __forceinline__ void overflow_net(const Tables& T, const Plan& P, const int* of_sum, unsigned char* is_of,
+                                             int id) {
+    is_of[id] = overflow_route(T, P.routes + P.route_off[id], P.route_off[id + 1] > P.route_off[id], of_sum);
 }
 
 // extract_congestionView (congestion.cuh:60-80) for 2-D cell i: the worst

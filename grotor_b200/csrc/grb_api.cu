@@ -21,6 +21,7 @@
 #include "device/flt.cuh"
 #include "device/outfmt.cuh"
 #include "device/lshape.cuh"
+#include "device/maze.cuh"
 #include "device/softmin.cuh"
 #include "device/topology.cuh"
 #include "device/zshape.cuh"
@@ -660,6 +661,20 @@ __global__ void k_topo_fill(TopoBuild B) {
     if (id < B.n) topo_fill(B, id);
 }
 
+// --- maze stage (maze.cuh) ---------------------------------------------------
+struct RemoveList {
+    const int* ids;
+    const unsigned char* phase2;
+    int n;
+};
+__global__ void k_maze_remove(Tables T, Plan P, Plan P2, RemoveList R) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= R.n) return;
+    const int id = R.ids[k];
+    maze_remove_route(T, R.phase2[k] ? P2.routes + P2.route_off[id] : P.routes + P.route_off[id]);
+}
+__global__ void __launch_bounds__(kScoreThreads) k_maze_score(Tables T, double* partials) { maze_score_partial(T, partials); }
+
 // --- .out text (outfmt.cuh): one warp per record ---------------------------
 __global__ void k_out_count(OutRecords R) {
     const int r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -942,6 +957,15 @@ __global__ void k_overflow_nets(Tables T, Plan P, int n, const int* of_sum, unsi
     const int id = blockIdx.x * blockDim.x + threadIdx.x;
     if (id < n) overflow_net(T, P, of_sum, is_of, id);
 }
+// The same with each net's current route: phase two where phase2[id] is set
+// (mark_overflow_nets, congestion.cuh:30-45).
+__global__ void k_overflow_nets2(Tables T, Plan P, Plan P2, int n, const int* of_sum, const unsigned char* phase2,
+                                 unsigned char* is_of) {
+    const int id = blockIdx.x * blockDim.x + threadIdx.x;
+    if (id >= n) return;
+    const Plan& Q = phase2[id] ? P2 : P;
+    is_of[id] = overflow_route(T, Q.routes + Q.route_off[id], Q.route_off[id + 1] > Q.route_off[id], of_sum);
+}
 __global__ void k_congestion(Tables T, unsigned char* cong, float* xsum, float* ysum) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < T.XY) congestion_cell(T, cong, xsum, ysum, i);
@@ -1037,6 +1061,11 @@ struct grb_ctx {
     std::vector<void*> geom_bufs;     // batching geometry replacing the uploaded one
     std::vector<void*> flt_bufs;
     std::vector<void*> topo_bufs;     // grb_build_topology: uploaded trees, counts, DFS stack
+    // maze stage (grb_remove_routes, grb_routing_score, grb_checkpoint)
+    int* ckpt_demand = nullptr;       // demand snapshot
+    double ckpt_wirelength = 0;
+    unsigned long long ckpt_vias = 0;
+    double* score_partials = nullptr;
     // .out text (grb_format_out / grb_drain_out)
     std::vector<void*> out_bufs;      // uploaded records and per-record byte offsets
     char* out_text = nullptr;
@@ -1947,6 +1976,8 @@ void grb_destroy(grb_ctx* c) {
     if (c->out_stream) cudaStreamDestroy(c->out_stream);
     if (c->flt_eprefix) cudaFree(c->flt_eprefix);
     if (c->flt_emap) cudaFree(c->flt_emap);
+    if (c->ckpt_demand) cudaFree(c->ckpt_demand);
+    if (c->score_partials) cudaFree(c->score_partials);
     free_all(c->owned);
     for (void* p : {(void*)c->check, (void*)c->bucket_ids, (void*)c->bucket_off, (void*)c->ids, (void*)c->batch_off, (void*)c->gscratch, (void*)c->work, (void*)c->cellmask,
                     (void*)c->lmask[0], (void*)c->lmask[1], (void*)c->lmask[2], (void*)c->ptchunk, (void*)c->fmask, (void*)c->pred, (void*)c->prevp,
@@ -2320,6 +2351,92 @@ int grb_drain_out(grb_ctx* c, grb_out_sink sink, void* user) {
     // (every copy has been waited for through its chunk event)
     c->out_pending = false;
     return rc;
+}
+
+int grb_remove_routes(grb_ctx* c, const int32_t* ids, int32_t n, const uint8_t* phase2) {
+    if (!c || n < 0 || (n && (!ids || !phase2))) return c ? fail(c, GRB_EINVAL, "bad removal list") : GRB_EINVAL;
+    if (!c->routes) return fail(c, GRB_EINVAL, "no nets uploaded");
+    GRB_CUDA(c, cudaSetDevice(c->device));
+    if (n == 0) return GRB_OK;
+    for (int k = 0; k < n; ++k) {
+        if (ids[k] < 0 || ids[k] >= c->n_nets) return fail(c, GRB_EINVAL, "net id out of range (item " + std::to_string(k) + ")");
+        if (phase2[k] && (c->flt_n != c->n_nets || c->h_route2_off[ids[k] + 1] == c->h_route2_off[ids[k]]))
+            return fail(c, GRB_EINVAL, "net " + std::to_string(ids[k]) + " has no phase-two routes");
+    }
+    int* d_ids = nullptr;
+    unsigned char* d_ph = nullptr;
+    if (cudaMalloc(&d_ids, sizeof(int) * n) != cudaSuccess || cudaMalloc(&d_ph, size_t(n)) != cudaSuccess) {
+        cudaGetLastError();
+        if (d_ids) cudaFree(d_ids);
+        return fail(c, GRB_ENOMEM, "removal list");
+    }
+    GRB_CUDA(c, cudaMemcpyAsync(d_ids, ids, sizeof(int) * n, cudaMemcpyHostToDevice, c->stream));
+    GRB_CUDA(c, cudaMemcpyAsync(d_ph, phase2, size_t(n), cudaMemcpyHostToDevice, c->stream));
+    Plan P = make_plan(c);
+    Plan P2 = c->F.routes2 ? make_plan2(c) : P;
+    k_maze_remove<<<(n + 127) / 128, 128, 0, c->stream>>>(c->T, P, P2, RemoveList{d_ids, d_ph, n});
+    c->launches += 1;
+    GRB_CUDA(c, cudaGetLastError());
+    GRB_CUDA(c, cudaStreamSynchronize(c->stream));
+    cudaFree(d_ids);
+    cudaFree(d_ph);
+    return check_device_error(c);
+}
+
+int grb_routing_score(grb_ctx* c, double* score) {
+    if (!c || !score) return c ? fail(c, GRB_EINVAL, "null score") : GRB_EINVAL;
+    GRB_CUDA(c, cudaSetDevice(c->device));
+    if (!c->score_partials && cudaMalloc(&c->score_partials, sizeof(double) * kScoreBlocks) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(c, GRB_ENOMEM, "score partials");
+    }
+    k_maze_score<<<kScoreBlocks, kScoreThreads, 0, c->stream>>>(c->T, c->score_partials);
+    c->launches += 1;
+    GRB_CUDA(c, cudaGetLastError());
+    std::vector<double> host(kScoreBlocks);
+    GRB_CUDA(c, cudaMemcpyAsync(host.data(), c->score_partials, sizeof(double) * kScoreBlocks, cudaMemcpyDeviceToHost,
+                                c->stream));
+    double wl = 0;
+    unsigned long long vias = 0;
+    GRB_CUDA(c, cudaMemcpyAsync(&wl, c->T.wirelength, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    GRB_CUDA(c, cudaMemcpyAsync(&vias, c->T.vias, sizeof(vias), cudaMemcpyDeviceToHost, c->stream));
+    GRB_CUDA(c, cudaStreamSynchronize(c->stream));
+    double s = wl * c->T.unit_wire + static_cast<double>(static_cast<long long>(vias)) * c->T.unit_via;
+    for (double v : host) s += v;
+    *score = s;
+    return GRB_OK;
+}
+
+int grb_checkpoint(grb_ctx* c) {
+    if (!c) return GRB_EINVAL;
+    GRB_CUDA(c, cudaSetDevice(c->device));
+    if (!c->ckpt_demand && cudaMalloc(&c->ckpt_demand, sizeof(int) * size_t(c->T.cells)) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(c, GRB_ENOMEM, "checkpoint");
+    }
+    GRB_CUDA(c, cudaMemcpyAsync(c->ckpt_demand, c->T.demand, sizeof(int) * size_t(c->T.cells), cudaMemcpyDeviceToDevice,
+                                c->stream));
+    GRB_CUDA(c, cudaMemcpyAsync(&c->ckpt_wirelength, c->T.wirelength, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    GRB_CUDA(c, cudaMemcpyAsync(&c->ckpt_vias, c->T.vias, sizeof(unsigned long long), cudaMemcpyDeviceToHost, c->stream));
+    GRB_CUDA(c, cudaStreamSynchronize(c->stream));
+    return GRB_OK;
+}
+
+int grb_restore(grb_ctx* c) {
+    if (!c) return GRB_EINVAL;
+    if (!c->ckpt_demand) return fail(c, GRB_EINVAL, "no checkpoint");
+    GRB_CUDA(c, cudaSetDevice(c->device));
+    GRB_CUDA(c, cudaMemcpyAsync(c->T.demand, c->ckpt_demand, sizeof(int) * size_t(c->T.cells), cudaMemcpyDeviceToDevice,
+                                c->stream));
+    GRB_CUDA(c, cudaMemcpyAsync(c->T.wirelength, &c->ckpt_wirelength, sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    GRB_CUDA(c, cudaMemcpyAsync(c->T.vias, &c->ckpt_vias, sizeof(unsigned long long), cudaMemcpyHostToDevice, c->stream));
+    // Every cost is recomputed at the next refresh (the reference clears
+    // costs_initialized, maze_quality.cuh:100).
+    k_mark_all_dirty<<<(c->T.cells + 255) / 256, 256, 0, c->stream>>>(c->T);
+    c->launches += 1;
+    GRB_CUDA(c, cudaGetLastError());
+    GRB_CUDA(c, cudaStreamSynchronize(c->stream));
+    return GRB_OK;
 }
 
 int grb_topology_sizes(grb_ctx* c, int64_t* sizes) {
@@ -3169,28 +3286,52 @@ int grb_autotune(grb_ctx* c, int32_t what, int32_t* per_cta, int32_t* per_grab) 
     return GRB_OK;
 }
 
+static int ripup_classify(grb_ctx* c, int32_t threshold, const uint8_t* phase2, uint8_t* is_of);
+
 int grb_ripup_classify(grb_ctx* c, int32_t threshold, uint8_t* is_of) {
+    return ripup_classify(c, threshold, nullptr, is_of);
+}
+
+int grb_ripup_classify_phase2(grb_ctx* c, int32_t threshold, const uint8_t* phase2, uint8_t* is_of) {
+    if (!c || !phase2) return c ? fail(c, GRB_EINVAL, "null flags") : GRB_EINVAL;
+    for (int id = 0; id < c->n_nets; ++id)
+        if (phase2[id] && (c->flt_n != c->n_nets || c->h_route2_off[id + 1] == c->h_route2_off[id]))
+            return fail(c, GRB_EINVAL, "net " + std::to_string(id) + " has no phase-two routes");
+    return ripup_classify(c, threshold, phase2, is_of);
+}
+
+static int ripup_classify(grb_ctx* c, int32_t threshold, const uint8_t* phase2, uint8_t* is_of) {
     if (!c || !is_of) return GRB_EINVAL;
     GRB_CUDA(c, cudaSetDevice(c->device));
     int* of_sum = nullptr;
     unsigned char* flags = nullptr;
-    if (cudaMalloc(&of_sum, sizeof(int) * size_t(c->T.cells)) || cudaMalloc(&flags, std::max(c->n_nets, 1))) {
+    unsigned char* d_phase2 = nullptr;
+    if (cudaMalloc(&of_sum, sizeof(int) * size_t(c->T.cells)) || cudaMalloc(&flags, std::max(c->n_nets, 1)) ||
+        (phase2 && cudaMalloc(&d_phase2, std::max(c->n_nets, 1)))) {
         cudaGetLastError();
         if (of_sum) cudaFree(of_sum);
+        if (flags) cudaFree(flags);
         return fail(c, GRB_ENOMEM, "rip-up buffers");
     }
+    if (phase2 && c->n_nets)
+        GRB_CUDA(c, cudaMemcpyAsync(d_phase2, phase2, size_t(c->n_nets), cudaMemcpyHostToDevice, c->stream));
     int tracks = 0;
     for (int l = 0; l < c->T.L; ++l) tracks += (((l & 1) ^ c->T.DIR) ? c->T.X : c->T.Y);
     k_mark_overflow<<<(c->T.cells + 255) / 256, 256, 0, c->stream>>>(c->T, threshold, of_sum);
     k_int_prefix<<<(tracks + 127) / 128, 128, 0, c->stream>>>(c->T, of_sum);
     Plan P = make_plan(c);
-    if (c->n_nets) k_overflow_nets<<<(c->n_nets + 255) / 256, 256, 0, c->stream>>>(c->T, P, c->n_nets, of_sum, flags);
+    if (c->n_nets && phase2)
+        k_overflow_nets2<<<(c->n_nets + 255) / 256, 256, 0, c->stream>>>(c->T, P, make_plan2(c), c->n_nets, of_sum,
+                                                                           d_phase2, flags);
+    else if (c->n_nets)
+        k_overflow_nets<<<(c->n_nets + 255) / 256, 256, 0, c->stream>>>(c->T, P, c->n_nets, of_sum, flags);
     c->launches += 3;
     cudaError_t e = cudaGetLastError();
     if (e == cudaSuccess) e = cudaMemcpyAsync(is_of, flags, c->n_nets, cudaMemcpyDeviceToHost, c->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
     cudaFree(of_sum);
     cudaFree(flags);
+    if (d_phase2) cudaFree(d_phase2);
     if (e != cudaSuccess) return cuda_fail(c, e, "rip-up classification");
     return GRB_OK;
 }
@@ -3352,6 +3493,17 @@ int grb_write_routes(grb_ctx* c, const int32_t* routes) {
     GRB_CUDA(c, cudaSetDevice(c->device));
     if (c->route_words)
         GRB_CUDA(c, cudaMemcpyAsync(c->routes, routes, sizeof(int) * c->route_words, cudaMemcpyHostToDevice, c->stream));
+    GRB_CUDA(c, cudaStreamSynchronize(c->stream));
+    return GRB_OK;
+}
+
+int grb_write_routes2(grb_ctx* c, const int32_t* routes2) {
+    if (!c || !routes2) return c ? fail(c, GRB_EINVAL, "null routes") : GRB_EINVAL;
+    if (c->flt_n != c->n_nets || c->flt_n < 0) return fail(c, GRB_EINVAL, "no phase-two route storage uploaded");
+    GRB_CUDA(c, cudaSetDevice(c->device));
+    if (c->route2_words)
+        GRB_CUDA(c, cudaMemcpyAsync(c->F.routes2, routes2, sizeof(int) * c->route2_words, cudaMemcpyHostToDevice,
+                                    c->stream));
     GRB_CUDA(c, cudaStreamSynchronize(c->stream));
     return GRB_OK;
 }

@@ -238,6 +238,34 @@ int grb_upload_flt(grb_ctx* ctx, const grb_flt_dags* dags);
  * phase-two routes.  mode: GRB_MODE_PLAIN, GRAPH or PERSISTENT. */
 int grb_flt_stage(grb_ctx* ctx, int32_t remove_phase_one, int32_t mode, grb_stats* stats);
 
+/* ---- Maze stage of the CUGR2 pipeline (pipeline_cugr2.hpp:90-117) -------- */
+/* maze::remove_routes (maze.cuh:24-64): remove the current routes of nets
+ * ids[0..n) -- the phase-two words where phase2[k] is set, the stage-one
+ * words otherwise -- from the demand and the statistics: each wire unit edge
+ * -1, each via layer whose cell none of the net's own wires covers -1 at a
+ * track end, else -1/2 on the two edges it lands between; the statistics
+ * lose the net's edge lengths and via layers. */
+int grb_remove_routes(grb_ctx* ctx, const int32_t* ids, int32_t n, const uint8_t* phase2);
+
+/* graph::ripup's classification (congestion.cuh:8-58,114-136) on each net's
+ * current route: the phase-two words for nets with phase2[id] set (the
+ * reference's ripup_flag), the stage-one words otherwise. */
+int grb_ripup_classify_phase2(grb_ctx* ctx, int32_t threshold, const uint8_t* phase2, uint8_t* is_of);
+
+/* maze::routing_score (maze_quality.cuh:28-43): wirelength * unit wire cost +
+ * vias * unit via cost + the overflow cost of every edge cell, reduced in a
+ * fixed order (1024 blocks of 256 threads, a halving tree per block, the
+ * partials in order), so equal states give equal scores bit for bit. */
+int grb_routing_score(grb_ctx* ctx, double* score);
+
+/* maze::Checkpoint (maze_quality.cuh:55-104), device part: grb_checkpoint
+ * saves the demand and the statistics, grb_restore puts them back and
+ * marks every cost for recomputation at the next refresh.  The route words
+ * and rip-up flags are the caller's (the reference keeps them in host copies
+ * too, pipeline_cugr2.hpp:14-61). */
+int grb_checkpoint(grb_ctx* ctx);
+int grb_restore(grb_ctx* ctx);
+
 /* ---- .out writer (graph::output_nets, output.hpp:79-112) ---------------- */
 /* Output records in output order, as graph::collect_output_nets hands them to
  * the writer (output.hpp:16-26): per record its name, its pins (3-D positions;
@@ -279,6 +307,12 @@ int grb_drain_out(grb_ctx* ctx, grb_out_sink sink, void* user);
 
 /* Copy all phase-two route words (route2_off[n] words) to the host. */
 int grb_read_routes2(grb_ctx* ctx, int32_t* routes2);
+/* Replace all phase-two route words (route2_off[n] words of the last
+ * grb_upload_flt) from the host: the routes of nets with phase-two storage
+ * but no DAG in this stage, carried over from an earlier stage
+ * (reserve_reroute_storage, pipeline_cugr2.hpp:14-63), or restored after a
+ * rejected stage. */
+int grb_write_routes2(grb_ctx* ctx, const int32_t* routes2);
 
 /* ---- Z-shape stage (the reference's GGR pipeline, pipeline_ggr.hpp:8-144) */
 

@@ -52,44 +52,6 @@ namespace drop_in {
 // beside its timing, for its roofline.
 bool report_traffic = false;
 
-// Stage one: Lshape_route (lshape.cuh:21-197) with batching, cost refresh,
-// DAG and commit on grotor_b200.  Leaves nets2route in the plan order, as
-// the reference does.
-void lshape_stage(cudb::RouterState& state, grb_ctx* ctx, std::vector<int>& nets2route, int32_t mode,
-                  int64_t initial_vias, bool tail) {
-    auto& nets = state.nets;
-    const auto topology_start = std::chrono::steady_clock::now();
-    // FLUTE only (construct_rsmt's rsmt_only form); the geometry and the
-    // depth-first trees are built on the device.
-#pragma omp parallel for num_threads(8)
-    for (int i = 0; i < int(nets2route.size()); ++i) nets[nets2route[i]].construct_rsmt(state, true);
-    Trees F = flatten_trees(state);
-    check(grb_build_topology(ctx, &F.t), ctx, "grb_build_topology");
-    printf("TOPOLOGY_TIMING stage=lshape elapsed_ms=%.6f geometry_fused=0 executor=grotor_b200\n",
-           std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - topology_start).count());
-    std::sort(nets2route.begin(), nets2route.end(), [&](int l, int r) { return nets[l].hpwl > nets[r].hpwl; });
-    check(grb_set_stats(ctx, 0.0, initial_vias), ctx, "grb_set_stats");
-    int32_t nb = 0;
-    check(grb_plan_batches(ctx, nets2route.data(), int32_t(nets2route.size()), 1000000, state.batch_sparsity_override,
-                           mode == GRB_MODE_PERSISTENT ? GRB_MODE_PERSISTENT : GRB_MODE_PLAIN, nullptr, &nb),
-          ctx, "grb_plan_batches");
-    check(grb_set_stage_tail(ctx, tail ? (GRB_TAIL_RIPUP | GRB_TAIL_VIEW) : 0, 0), ctx, "grb_set_stage_tail");
-    grb_stats st{};
-    check(grb_lshape_stage(ctx, mode, &st), ctx, "grb_lshape_stage");
-    std::vector<int32_t> batch_off(nb + 1);
-    int32_t n = 0, nb2 = 0;
-    check(grb_get_plan(ctx, nets2route.data(), batch_off.data(), &n, &nb2), ctx, "grb_get_plan");
-    if (report_traffic) {  // the .out is written from the device's routes; the host copy feeds the byte model
-        const size_t words = size_t(state.device.ROUTE_PER_PIN) * state.device.PIN_NUM + 1;
-        state.routes_cpu.reset(new int[words]());
-        check(grb_read_routes(ctx, state.routes_cpu.get()), ctx, "grb_read_routes");
-    }
-    printf("DAG_TIMING stage=lshape batch_index=-1 elapsed_ms=%.6f nets=%zu batches=%d executor=grotor_b200\n",
-           st.dag_ms, nets2route.size(), nb);
-    printf("BATCH_TIMING backend=grotor_b200 elapsed_ms=%.6f nets=%zu batches=%d used_for_routing=1\n",
-           st.batching_ms, nets2route.size(), nb);
-}
-
 // Stage two: Lshape_route_detour::route_detour (flt.cuh:186-192).  The
 // congestion view comes from the stage tail; the host DAG builder is the
 // reference's; batching and route_prepared_topology's batch loop run on
@@ -97,88 +59,15 @@ void lshape_stage(cudb::RouterState& state, grb_ctx* ctx, std::vector<int>& nets
 void flt_stage(cudb::RouterState& state, grb_ctx* ctx, const grb_grid& grid, std::vector<int>& nets2route, int32_t mode,
                std::vector<unsigned char>& cong, std::vector<float>& xsum, std::vector<float>& ysum) {
     if (nets2route.empty()) return;
-    auto& nets = state.nets;
-    // prepare_detour_topology (flt.cuh:48-73) with the view in host memory.
-    std::sort(nets2route.begin(), nets2route.end(), [&](int l, int r) { return nets[l].hpwl > nets[r].hpwl; });
-    // The FLT builder keeps a net's stage-one RSMT segments (it runs with
-    // construct_segments = false, flt.cuh:20); stage one built them on the
-    // device, so the rerouted nets get them on the host here, from the same
-    // trees (construct_rsmt is a pure function of net::rsmt and the pins).
-#pragma omp parallel for num_threads(8)
-    for (int i = 0; i < int(nets2route.size()); ++i)
-        if (!nets[nets2route[i]].rsmt.empty()) nets[nets2route[i]].construct_rsmt(state, false);
-    std::unique_ptr<bool[]> view(new bool[cong.size()]);
-    for (size_t i = 0; i < cong.size(); ++i) view[i] = cong[i] != 0;
-    state.packing.congestionView_cpu = view.get();
-    state.packing.congestionView_xsum_cpu = xsum.data();
-    state.packing.congestionView_ysum_cpu = ysum.data();
-    for (int id : nets2route) if (nets[id].rsmt.empty()) nets[id].construct_rsmt(state);
-    state.flt_topology.begin(nets2route, nets.size(), 8);
-    grotor::batching::prepare_geometry(state, nets2route, 8);
-    Lshape_route_detour::multithreaded_processing(state, nets2route);
-    state.packing.congestionView_cpu = nullptr;
-    state.packing.congestionView_xsum_cpu = state.packing.congestionView_ysum_cpu = nullptr;
-    // The FLT DAGs (flt::Topology spans) and batching geometry, by net id.
-    const int count = int(nets.size());
-    std::vector<int> slot_of(count, -1);
-    for (size_t s = 0; s < nets2route.size(); ++s) slot_of[nets2route[s]] = int(s);
-    std::vector<int32_t> node_off{0}, coord, depth, children, parent_end, edge_off{0}, edge_parent, edge_slot;
-    std::vector<int32_t> point_off{0}, points, hseg_off{0}, hsegs, vseg_off{0}, vsegs;
-    std::vector<int64_t> route2_off{0};
-    const auto& topo = state.flt_topology;
-    for (int id = 0; id < count; ++id) {
-        const int s = slot_of[id];
-        if (s >= 0) {
-            const auto& span = topo.spans[s];
-            const auto& arena = topo.arenas[span.lane];
-            for (int i = 0; i < span.nodes; ++i) {
-                const auto& nd = arena.nodes[span.node_begin + i];
-                coord.push_back(nd.coordinate);
-                depth.push_back(nd.depth);
-                children.push_back(nd.children);
-                parent_end.push_back(nd.parent_end);
-            }
-            for (int i = 0; i < span.edges; ++i) {
-                const auto& e = arena.edges[span.edge_begin + i];
-                edge_parent.push_back(e.parent);
-                edge_slot.push_back(e.source_slot);
-            }
-        }
-        node_off.push_back(int32_t(coord.size()));
-        edge_off.push_back(int32_t(edge_parent.size()));
-        const auto& n = nets[id];
-        for (int p : n.points) points.push_back(p);
-        point_off.push_back(int32_t(points.size()));
-        for (const auto& sg : n.rsmt_h_segments) { hsegs.push_back(sg.first); hsegs.push_back(sg.second); }
-        hseg_off.push_back(int32_t(hsegs.size() / 2));
-        for (const auto& sg : n.rsmt_v_segments) { vsegs.push_back(sg.first); vsegs.push_back(sg.second); }
-        vseg_off.push_back(int32_t(vsegs.size() / 2));
-        const int64_t words = s >= 0 ? int64_t(n.pins.size()) * int64_t(state.device.ROUTE_PER_PIN_PHASE2) : 0;
-        route2_off.push_back(route2_off.back() + words);
-    }
-    state.flt_topology.clear();
-    check(grb_upload_geometry(ctx, point_off.data(), points.data(), hseg_off.data(), hsegs.data(), vseg_off.data(),
-                              vsegs.data()),
-          ctx, "grb_upload_geometry");
-    int32_t nb = 0;
-    check(grb_plan_batches(ctx, nets2route.data(), int32_t(nets2route.size()), 300000, state.batch_sparsity_override,
-                           mode == GRB_MODE_PERSISTENT ? GRB_MODE_PERSISTENT : GRB_MODE_PLAIN, nullptr, &nb),
-          ctx, "grb_plan_batches (FLT)");
-    grb_flt_dags d{node_off.data(), coord.data(), depth.data(), children.data(), parent_end.data(),
-                   edge_off.data(), edge_parent.data(), edge_slot.data(), route2_off.data()};
-    check(grb_upload_flt(ctx, &d), ctx, "grb_upload_flt");
-    grb_stats st{};
-    check(grb_flt_stage(ctx, 1, mode, &st), ctx, "grb_flt_stage");
+    detour_prepare(state, nets2route, cong, xsum, ysum);
+    FltRun run = flt_run(state, ctx, nets2route, mode, 1, state.device.ROUTE_PER_PIN_PHASE2, "detour");
     if (report_traffic) {
+        const int count = int(state.nets.size());
         const size_t words = size_t(state.device.ROUTE_PER_PIN_PHASE2) * state.device.PIN_NUM_PHASE2 + 1;
-        state.routes_phase2_cpu.reset(new int[std::max<size_t>(words, size_t(route2_off.back()) + 1)]());
+        state.routes_phase2_cpu.reset(new int[std::max<size_t>(words, size_t(run.route2_off.back()) + 1)]());
         check(grb_read_routes2(ctx, state.routes_phase2_cpu.get()), ctx, "grb_read_routes2");
-    }
-    printf("DAG_TIMING stage=detour batch_index=-1 elapsed_ms=%.6f nets=%zu batches=%d executor=grotor_b200\n",
-           st.dag_ms, nets2route.size(), nb);
-    printf("BATCH_TIMING stage=detour backend=grotor_b200 elapsed_ms=%.6f nets=%zu batches=%d used_for_routing=1\n",
-           st.batching_ms, nets2route.size(), nb);
-    if (report_traffic) {
+        const int32_t nb = run.nb;
+        const grb_flt_dags& d = run.d;
         std::vector<int32_t> plan(nets2route.size()), plan_off(size_t(nb) + 1);
         int32_t pn = 0, pb = 0;
         check(grb_get_plan(ctx, plan.data(), plan_off.data(), &pn, &pb), ctx, "grb_get_plan");
@@ -211,7 +100,7 @@ void route(cudb::RouterState& state, int32_t mode, bool stop_after_lshape) {
     out.start(state);
     std::vector<int> all_nets(state.nets.size());
     std::iota(all_nets.begin(), all_nets.end(), 0);
-    lshape_stage(state, ctx, all_nets, mode, initial_vias, !stop_after_lshape);
+    lshape_stage(state, ctx, all_nets, mode, initial_vias, !stop_after_lshape, report_traffic);
     if (stop_after_lshape) {
         graph::finish_nets(state, all_nets);
         out.start(state);

@@ -28,6 +28,8 @@ STOCK = os.path.join(REF_DIR, "grotor")
 DRIVER = os.path.join(ROOT, "integration", "_build", "grotor_grb")
 STOCK_GGR = os.path.join(REF_DIR, "grotor_ggr")
 DRIVER_GGR = os.path.join(ROOT, "integration", "_build", "grotor_grb_ggr")
+STOCK_CUGR2 = os.path.join(REF_DIR, "grotor_cugr2")
+DRIVER_CUGR2 = os.path.join(ROOT, "integration", "_build", "grotor_grb_cugr2")
 EVALUATOR = os.path.join(REF_DIR, "evaluator")
 
 DESIGNS = {
@@ -118,3 +120,39 @@ def test_ggr_drop_in_matches_stock_reference(name, tmp_path):
         a, b = open(ref_out, "rb").read(), open(mine, "rb").read()
         assert a == b, f"{ex}: .out differs ({len(a)} vs {len(b)} bytes)"
     assert scores(cap, net, ref_out) == scores(cap, net, mine)
+
+
+def stage_lines(text, tags):
+    return [ln.strip() for ln in text.splitlines() if ln.split(" ")[0] in tags and "executor=" not in ln]
+
+
+@pytest.mark.parametrize("name", list(DESIGNS))
+def test_cugr2_drop_in_matches_stock_reference(name, tmp_path):
+    """The CUGR2 pipeline (the reference's grotor_cugr2 build,
+    pipeline_cugr2.hpp): L-shape, rip-up, FLT detour and the maze stage with
+    its checkpoint and score gate on grotor_b200 around the reference's host
+    maze topology.  Same nets in the same order, every net's segments as a
+    set, identical scores; the maze stage's sizes and its score gate (both
+    scores, printed to 12 digits) as the stock program reports them."""
+    if not (os.path.exists(STOCK_CUGR2) and os.path.exists(DRIVER_CUGR2)):
+        pytest.skip("stock CUGR2 reference or CUGR2 drop-in driver not built (oracle/ref.mk, integration/Makefile)")
+    from grotor_b200.synth import WORKLOADS, Design
+    wl, over = DESIGNS[name]
+    cap, net = str(tmp_path / "d.cap"), str(tmp_path / "d.net")
+    Design(replace(WORKLOADS[wl], **over)).write(cap, net)
+    ref_out, mine = str(tmp_path / "ref.out"), str(tmp_path / "mine.out")
+    r = subprocess.run([STOCK_CUGR2, "-cap", cap, "-net", net, "-out", ref_out, "--lut-dir", REF_DIR, "--report-score",
+                        "0"], capture_output=True, text=True, timeout=900)
+    assert r.returncode == 0, r.stderr[-3000:]
+    tags = ("ROUTING_STAGE_BEGIN", "MAZE_QUALITY_GATE", "ROUTING_REMAINING_OVERFLOW", "REROUTE_STORAGE")
+    for ex in ("persistent", "plain"):
+        m = subprocess.run([DRIVER_CUGR2, "-cap", cap, "-net", net, "-out", mine, "--lut-dir", REF_DIR, "--executor",
+                            ex], capture_output=True, text=True, timeout=900)
+        assert m.returncode == 0, m.stderr[-3000:]
+        assert stage_lines(r.stdout, tags) == stage_lines(m.stdout, tags)
+        a, b = parse_out(ref_out), parse_out(mine)
+        assert [n for n, _ in a] == [n for n, _ in b], "net order differs"
+        for (n, sa), (_, sb) in zip(a, b):
+            assert sorted(sa) == sorted(sb), f"{ex}: net {n}: segments differ"
+        assert scores(cap, net, ref_out) == scores(cap, net, mine)
+    print(name, stage_lines(r.stdout, tags))
