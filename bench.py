@@ -465,6 +465,7 @@ def run_grotor(args):
         r = None
         result["zshape"] = zshape_measure(args)
         result["softmin"] = softmin_measure(args)
+        result["pipeline"] = pipeline_measure(args)
     if r is not None:
         r.close()
     if pg is not None:
@@ -600,6 +601,69 @@ def zshape_measure(args, workload="large_800x800x10", steps=3, warmup=2):
                                  "peak_source": f"{kind} hbm_gbs"}
     r.close()
     return out
+
+
+def pipeline_measure(args, workload="medium_320x320x10"):
+    """The default pipeline end to end through the drop-in driver
+    (integration/_build/grotor_grb: the reference's program flow on this
+    library, CAP/NET in, .out out) on the 'medium' design: stage one
+    (L-shape) and stage two (rip-up + FLT, configuration 3's composite) with
+    each stage's device time, nets/s and, for the FLT stage, its roofline from
+    the byte model (a separate run with --report-traffic 1, untimed)."""
+    driver = os.path.join(ROOT, "integration", "_build", "grotor_grb")
+    lut = os.path.dirname(driver)  # FLUTE's tables beside the driver (integration/Makefile)
+    if not os.path.exists(driver) or not os.path.exists(os.path.join(lut, "POWV9.dat")):
+        return {"unavailable": "drop-in driver or FLUTE tables not built (integration/Makefile)"}
+    from grotor_b200.synth import WORKLOADS, Design
+
+    def records(text):
+        out = {"lshape": {}, "detour": {}}
+        for line in text.splitlines():
+            tag, _, rest = line.partition(" ")
+            kv = dict(p.split("=", 1) for p in rest.split() if "=" in p)
+            if tag == "DAG_TIMING" and kv.get("batch_index") == "-1":
+                out[kv["stage"]].update(dag_ms=float(kv["elapsed_ms"]), nets=int(kv["nets"]), batches=int(kv["batches"]))
+            elif tag == "BATCH_TIMING":
+                out[kv.get("stage", "lshape")]["batching_ms"] = float(kv["elapsed_ms"])
+            elif tag == "TOPOLOGY_TIMING" and kv.get("stage") == "lshape":
+                out["lshape"]["topology_ms"] = float(kv["elapsed_ms"])
+            elif tag == "FLT_TRAFFIC":
+                out["detour"]["algorithmic_bytes"] = sum(float(v) for v in kv.values())
+            elif tag == "GROTOR_COMPLETE":
+                out["wall_s"] = float(kv["wall_seconds"])
+        for st in ("lshape", "detour"):
+            d = out[st]
+            if "dag_ms" in d and "batching_ms" in d:
+                d["stage_ms"] = d["dag_ms"] + d["batching_ms"]
+                d["nets_per_s"] = d["nets"] / (d["stage_ms"] / 1e3)
+        return out
+
+    res = {"workload": workload, "driver": "integration/_build/grotor_grb"}
+    with tempfile.TemporaryDirectory() as w:
+        cap, net = os.path.join(w, "d.cap"), os.path.join(w, "d.net")
+        Design(WORKLOADS[workload]).write(cap, net)
+        for ex in ("persistent", "plain"):
+            run = subprocess.run([driver, "-cap", cap, "-net", net, "-out", os.path.join(w, ex + ".out"), "--lut-dir",
+                                  lut, "--executor", ex], capture_output=True, text=True, timeout=900)
+            if run.returncode:
+                return {"unavailable": f"drop-in driver failed: {run.stderr[-300:]}"}
+            res[ex] = records(run.stdout)
+        res["outputs_identical"] = open(os.path.join(w, "persistent.out"), "rb").read() == \
+            open(os.path.join(w, "plain.out"), "rb").read()
+        run = subprocess.run([driver, "-cap", cap, "-net", net, "-out", os.devnull, "--lut-dir", lut, "--executor",
+                              "persistent", "--report-traffic", "1"], capture_output=True, text=True, timeout=900)
+    byt = records(run.stdout)["detour"].get("algorithmic_bytes") if run.returncode == 0 else None
+    peak, kind = measured_peak()
+    for ex in ("persistent", "plain"):
+        d = res[ex]["detour"]
+        if byt and d.get("dag_ms"):
+            ach = byt / (d["dag_ms"] / 1e3) / 1e9
+            d["roofline"] = {"kernel": "k_flt_persistent" if ex == "persistent" else "per-batch launches", "bound": "hbm",
+                             "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
+                             "algorithmic_bytes": byt, "peak_source": f"{kind} hbm_gbs"}
+    if res["plain"]["detour"].get("stage_ms") and res["persistent"]["detour"].get("stage_ms"):
+        res["flt_speedup_persistent_vs_plain"] = res["plain"]["detour"]["stage_ms"] / res["persistent"]["detour"]["stage_ms"]
+    return res
 
 
 def softmin_measure(args, workload="softmin_320x320x10", taus=(1.0, 0.1, 0.01), reps=3):

@@ -141,7 +141,11 @@ __device__ __forceinline__ void flt_edges_batch(const Tables& T, const Flt& F, c
     }
 }
 
-// solve_flt_node (flt_block.cuh:6-142) for net-local node `i`.
+// solve_flt_node (flt_block.cuh:6-142) for net-local node `i`.  The node's
+// inputs -- its children's candidate keys and the via costs of its column --
+// are loaded once, and its range costs and choices are kept in registers and
+// thread-local arrays until the end (in HBM they would cost a round trip per
+// read after a write); the loops and comparisons are the reference's.
 __device__ __forceinline__ void flt_solve_node(const Tables& T, const Flt& F, int nb, int eb, int i) {
     const int g = nb + i;
     const int c0 = F.coord[g];
@@ -150,17 +154,35 @@ __device__ __forceinline__ void flt_solve_node(const Tables& T, const Flt& F, in
     const int nc = F.children[g];
     unsigned long long* cbp = F.best + size_t(F.child_off[g]) * kFltLayers;
     const unsigned long long* cpk = F.packed + size_t(F.child_off[g]) * kFltLayers;
-    double* cst = F.costs + size_t(g) * kFltLayers;
+    double* cst_g = F.costs + size_t(g) * kFltLayers;
+    unsigned long long pk[kFltMaxChildren][kFltLayers];  // children's keys
+    for (int c = 0; c < nc; ++c) {
+        unsigned long long v[kFltLayers];
+#pragma unroll
+        for (int li = 0; li < kFltLayers; ++li) v[li] = cpk[c * kFltLayers + li];
+#pragma unroll
+        for (int li = 0; li < kFltLayers; ++li) pk[c][li] = v[li];
+    }
+    float vc[kFltLayers];  // via cost of routing layer li - 2 at the node
+#pragma unroll
+    for (int li = 2; li < kFltLayers; ++li) vc[li] = li - 2 < T.L ? T.vcost[cell_index(T, li - 2, x, y)] : 0.f;
+    double cst[kFltLayers];
+#pragma unroll
+    for (int li = 0; li < kFltLayers; ++li) cst[li] = kInf;  // as flt_net left them
+    unsigned long long chosen[kFltMaxChildren][kFltLayers];  // chosen child candidate per range top
+    unsigned written = 0;                                    // range tops whose choices were set
     double mcc[kFltMaxChildren];
     unsigned long long bp[kFltMaxChildren];
     for (int c = 0; c < kFltMaxChildren; ++c) bp[c] = 0;
     for (int low = 1; low <= flow; ++low) {
         for (int c = 0; c < nc; ++c) mcc[c] = kInf;
         double via = 0;
-        for (int li = low; li < T.L + 1; ++li) {
-            if (li > low) via += T.vcost[cell_index(T, li - 2, x, y)];
+#pragma unroll
+        for (int li = 1; li < kFltLayers; ++li) {
+            if (li < low || li >= T.L + 1) continue;
+            if (li > low) via += vc[li];
             for (int c = 0; c < nc; ++c) {
-                const unsigned long long pv = cpk[c * kFltLayers + li];
+                const unsigned long long pv = pk[c][li];
                 const double cc = flt_cost(pv);
                 if (cc < mcc[c]) { mcc[c] = cc; bp[c] = static_cast<unsigned long long>(static_cast<unsigned>(pv)) * kFltLayers + li; }
             }
@@ -169,17 +191,27 @@ __device__ __forceinline__ void flt_solve_node(const Tables& T, const Flt& F, in
                 for (int c = 0; c < nc; ++c) cost += mcc[c];
                 if (cost < kInf && cost < cst[li]) {
                     cst[li] = cost;
-                    for (int c = 0; c < nc; ++c) cbp[c * kFltLayers + li] = bp[c];
+                    for (int c = 0; c < nc; ++c) chosen[c][li] = bp[c];
+                    written |= 1u << li;
                 }
             }
         }
-        for (int li = T.L - 1; li >= low; --li) {
+#pragma unroll
+        for (int li = kFltLayers - 2; li >= 1; --li) {
+            if (li < low || li > T.L - 1) continue;
             if (cst[li + 1] < cst[li]) {
                 cst[li] = cst[li + 1];
-                for (int c = 0; c < nc; ++c) cbp[c * kFltLayers + li] = cbp[c * kFltLayers + li + 1];
+                for (int c = 0; c < nc; ++c) chosen[c][li] = chosen[c][li + 1];
+                written |= 1u << li;
             }
         }
     }
+#pragma unroll
+    for (int li = 0; li < kFltLayers; ++li) cst_g[li] = cst[li];
+    for (int c = 0; c < nc; ++c)
+#pragma unroll
+        for (int li = 0; li < kFltLayers; ++li)
+            if (written >> li & 1u) cbp[c * kFltLayers + li] = chosen[c][li];
     const int pb = i ? F.pend[g - 1] : 0, pe = F.pend[g];
     for (int e = eb + pb; e < eb + pe; ++e) {
         const int par = nb + F.eparent[e], slot = F.eslot[e] % 10;
@@ -189,6 +221,7 @@ __device__ __forceinline__ void flt_solve_node(const Tables& T, const Flt& F, in
         const bool far = abs(x - px) + abs(y - py) > 4;
         unsigned long long cache[kFltLayers];
         for (int t = 0; t < kFltLayers; ++t) cache[t] = kFltInit;
+#pragma unroll
         for (int layer = 1; layer < kFltLayers; ++layer) {
             const bool ay = ((layer & 1) ^ T.DIR) == 1;  // 1-based layer index
             if (ay && y != py) continue;

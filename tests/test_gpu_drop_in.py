@@ -126,7 +126,13 @@ def stage_lines(text, tags):
     return [ln.strip() for ln in text.splitlines() if ln.split(" ")[0] in tags and "executor=" not in ln]
 
 
-@pytest.mark.parametrize("name", list(DESIGNS))
+CUGR2_DESIGNS = dict(DESIGNS)
+# a design whose maze stage the score gate accepts (the others reject theirs)
+CUGR2_DESIGNS["maze_accepted_64x64x10_3000"] = ("small_64x64x5", dict(n_nets=3000, cap_layers=10, seed=2, X=64, Y=64,
+                                                                      cap_lo=5, cap_hi=9))
+
+
+@pytest.mark.parametrize("name", list(CUGR2_DESIGNS))
 def test_cugr2_drop_in_matches_stock_reference(name, tmp_path):
     """The CUGR2 pipeline (the reference's grotor_cugr2 build,
     pipeline_cugr2.hpp): L-shape, rip-up, FLT detour and the maze stage with
@@ -137,7 +143,7 @@ def test_cugr2_drop_in_matches_stock_reference(name, tmp_path):
     if not (os.path.exists(STOCK_CUGR2) and os.path.exists(DRIVER_CUGR2)):
         pytest.skip("stock CUGR2 reference or CUGR2 drop-in driver not built (oracle/ref.mk, integration/Makefile)")
     from grotor_b200.synth import WORKLOADS, Design
-    wl, over = DESIGNS[name]
+    wl, over = CUGR2_DESIGNS[name]
     cap, net = str(tmp_path / "d.cap"), str(tmp_path / "d.net")
     Design(replace(WORKLOADS[wl], **over)).write(cap, net)
     ref_out, mine = str(tmp_path / "ref.out"), str(tmp_path / "mine.out")
