@@ -466,6 +466,7 @@ def run_grotor(args):
         result["zshape"] = zshape_measure(args)
         result["softmin"] = softmin_measure(args)
         result["pipeline"] = pipeline_measure(args)
+        result["configs"] = configs_measure(args)
     if r is not None:
         r.close()
     if pg is not None:
@@ -600,6 +601,50 @@ def zshape_measure(args, workload="large_800x800x10", steps=3, warmup=2):
                                  "bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
                                  "peak_source": f"{kind} hbm_gbs"}
     r.close()
+    return out
+
+
+def configs_measure(args, workloads=("small_64x64x5", "medium_320x320x10", "large_800x800x10"), reps=3):
+    """The L-shape stage (batching + DAG) on the benchmark plan's other
+    configurations -- 'small' (64x64x5, 5,000 nets), 'medium' (320x320x10,
+    120K nets) and 'large' (800x800x10, 900K nets) -- in the persistent and
+    plain executors: mean device time over `reps` steps after one warm-up,
+    nets/s, and the routes of the two executors compared."""
+    import torch
+
+    from grotor_b200 import Router
+    from grotor_b200.synth import WORKLOADS, Design
+    out = {}
+    for wl in workloads:
+        d = Design(WORKLOADS[wl])
+        r = Router(d.grid)
+        r.upload_nets(d.nets)
+        stream = _stream(r)
+        res = {"nets": int(d.nets.n)}
+        routes = {}
+        for mode in ("persistent", "plain"):
+            times, bt, dt = [], [], []
+            for k in range(reps + 1):
+                torch.cuda.synchronize()
+                a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                a.record(stream)
+                r.reset()
+                _, nb = r.generate_batches_rsmt(d.order, BATCH_LIMIT, 1, mode)
+                st = r.lshape_route(mode)
+                b.record(stream)
+                torch.cuda.synchronize()
+                if k:
+                    times.append(a.elapsed_time(b))
+                    bt.append(st["batching_ms"])
+                    dt.append(st["dag_ms"])
+            routes[mode] = r.read_routes()
+            ms = float(np.mean(times))
+            res[mode] = {"ms_per_step": ms, "nets_per_s": d.nets.n / (ms / 1e3), "batching_ms": float(np.mean(bt)),
+                         "dag_ms": float(np.mean(dt)), "batches": int(nb)}
+        res["speedup_persistent_vs_plain"] = res["plain"]["ms_per_step"] / res["persistent"]["ms_per_step"]
+        res["routes_identical"] = bool(np.array_equal(routes["persistent"], routes["plain"]))
+        r.close()
+        out[wl] = res
     return out
 
 
