@@ -335,13 +335,10 @@ __global__ void __launch_bounds__(kPersistentThreads, 2) k_flt_persistent(Tables
                         (long long)gridDim.x * blockDim.x);
         if (!grid_sync(S, T)) return;
         clk.mark(S, 10);
-        while (true) {
-            int k = 0;
-            if (lane == 0) k = atomicAdd(work + b, 1);
-            k = __shfl_sync(0xffffffffu, k, 0);
-            if (k >= cnt) break;
-            flt_net(T, F, P2, P2.ids[lo + k], stamp, lane, true);
-        }
+        // Net k to global warp k: warp 0 of every block first, so a batch's
+        // nets (often fewer than the blocks) land on different SMs, each with
+        // its L1 to itself for the nets' thread-local arrays.
+        for (int k = gwarp; k < cnt; k += nwarps) flt_net(T, F, P2, P2.ids[lo + k], stamp, lane, true);
         if (!grid_sync(S, T)) return;
         clk.mark(S, 5);
         commit_vias_strided(T, P2, P2.ids + lo, cnt, gwarp, nwarps, stamp, 1, lane);
