@@ -82,62 +82,103 @@ __device__ __forceinline__ double flt_cost(unsigned long long p) {
     return static_cast<double>(__int_as_float(i));
 }
 
-// precompute_cost_edge (flt_cost.cuh:50-130), one entry: global edge `e`,
-// from-layer `fl`, to-layer `tl`.  Entries the solve never reads (wrong
-// direction, an edge of Manhattan length <= 4, where only straight wires are
-// offered, or a to-layer of the other parity) are INF.  The sampled
-// positions are scanned in increasing order and the first minimum is kept.
-__device__ __forceinline__ void flt_edge_cell(const Tables& T, const Flt& F, int nb, int e, int fl, int tl) {
+// precompute_cost_edge (flt_cost.cuh:50-130) for every (from-layer,
+// to-layer) entry of global edge `e`, one warp.  Entries the solve never
+// reads -- an edge with a bend or of Manhattan length <= 4 (only straight
+// wires are offered there), a from-layer across the edge's direction, a
+// to-layer of the other parity -- are INF with position -1.  Otherwise the
+// entry is the cheapest layer change over the sampled positions (every
+// dd-th position strictly inside the edge, dd = distance / min(distance,
+// 20)): the via stack between the layers there plus the wire from each end
+// to it on its layer, the via costs added from the lower layer up and the two
+// wires summed before they are added, the first minimum in increasing
+// position kept.  Lanes take the positions (32 at a time) and evaluate every
+// entry there; the first minimum comes from a warp reduction of (cost,
+// position) pairs.
+__device__ __forceinline__ void flt_edge_warp(const Tables& T, const Flt& F, int nb, int e, int lane) {
     const int to = nb + F.eparent[e], from = nb + F.eslot[e] / 10;
     const int ct = F.coord[to], cf = F.coord[from];
     const int tox = ct / T.Y % T.X, toy = ct % T.Y, fromx = cf / T.Y % T.X, fromy = cf % T.Y;
-    double* ce = F.ce + size_t(e) * 81 + fl * 9 + tl;
-    int* bc = F.bc + size_t(e) * 81 + fl * 9 + tl;
-    const bool ay = along_y(T, fl);
+    double* ce = F.ce + size_t(e) * 81;
+    int* bc = F.bc + size_t(e) * 81;
+    for (int k = lane; k < 81; k += 32) { ce[k] = kInf; bc[k] = -1; }
     const int distance = abs(tox - fromx) + abs(toy - fromy);
-    if ((!ay && fromy != toy) || (ay && fromx != tox) || distance <= 4 || (tl & 1) != (fl & 1)) {
-        *ce = kInf;
-        *bc = -1;
-        return;
-    }
-    const int dd = distance / min(distance, 20);
     const bool vertical = fromx == tox;
+    if (distance <= 4 || (!vertical && fromy != toy)) return;
+    __syncwarp();  // the fill above comes before the entries below
+    const int dd = distance / min(distance, 20);
     const int start = vertical ? min(fromy, toy) : min(fromx, tox);
     const int end = vertical ? max(fromy, toy) : max(fromx, tox);
-    const int lo = min(fl, tl), hi = max(fl, tl);
-    double best = kInf;
-    int pos = -1;
-    for (int sp = start + dd; sp < end; sp += dd) {
-        const int sx = vertical ? fromx : sp, sy = vertical ? sp : fromy;
-        double via = 0;
-        for (int ll = lo; ll < hi; ++ll) via += T.vcost[cell_index(T, ll, sx, sy)];
-        double c = via;
-        if (vertical)
-            c += (flt_wire(T, fl, fromx, fromx, min(fromy, sy), max(fromy, sy)) +
-                  flt_wire(T, tl, tox, tox, min(toy, sy), max(toy, sy)));
-        else
-            c += (flt_wire(T, fl, min(fromx, sx), max(fromx, sx), fromy, fromy) +
-                  flt_wire(T, tl, min(tox, sx), max(tox, sx), toy, toy));
-        if (c < best) { best = c; pos = sp; }
+    const int ns = start + dd < end ? (end - 1 - (start + dd)) / dd + 1 : 0;  // sampled positions
+    // Layers of the edge's direction (the only from- and to-layers with
+    // finite entries): l0, l0 + 2, ...
+    const int l0 = (vertical ? (T.DIR ^ 1) : T.DIR) & 1;
+    constexpr int KV = (kFltLayers + 1) / 2;
+    for (int fi = 0; fi < KV; ++fi) {
+        const int fl = l0 + 2 * fi;
+        if (fl >= 9 || fl >= T.L) break;
+        double bv[KV];
+        int bp[KV];
+#pragma unroll
+        for (int ti = 0; ti < KV; ++ti) { bv[ti] = kInf; bp[ti] = -1; }
+        const double pF = T.presum[cell_index(T, fl, fromx, fromy)];
+        for (int base = 0; base < ns; base += 32) {
+            const int s = base + lane;
+            if (s < ns) {
+                const int sp = start + dd + s * dd;
+                const int sx = vertical ? fromx : sp, sy = vertical ? sp : fromy;
+                float vc[kFltLayers];
+#pragma unroll
+                for (int ll = 0; ll < kFltLayers - 1; ++ll) vc[ll] = ll < T.L ? T.vcost[cell_index(T, ll, sx, sy)] : 0.f;
+                const double pf = T.presum[cell_index(T, fl, sx, sy)];
+                const double wf = vertical ? (sy > fromy ? pf - pF : pF - pf) : (sx > fromx ? pf - pF : pF - pf);
+#pragma unroll
+                for (int ti = 0; ti < KV; ++ti) {
+                    const int tl = l0 + 2 * ti;
+                    if (tl >= 9 || tl >= T.L) continue;
+                    const double pT = T.presum[cell_index(T, tl, tox, toy)];
+                    const double pt = T.presum[cell_index(T, tl, vertical ? tox : sp, vertical ? sp : toy)];
+                    const double wt = vertical ? (sy > toy ? pt - pT : pT - pt) : (sx > tox ? pt - pT : pT - pt);
+                    const int lo = min(fl, tl), hi = max(fl, tl);
+                    double via = 0;
+#pragma unroll
+                    for (int ll = 0; ll < kFltLayers - 1; ++ll)
+                        if (ll >= lo && ll < hi) via += vc[ll];  // in increasing order, as the reference adds
+                    double c = via;
+                    c += (wf + wt);
+                    if (c < bv[ti]) { bv[ti] = c; bp[ti] = sp; }
+                }
+            }
+        }
+#pragma unroll
+        for (int ti = 0; ti < KV; ++ti) {
+            const int tl = l0 + 2 * ti;
+            if (tl >= 9 || tl >= T.L) continue;
+            double v = bv[ti];
+            int p = bp[ti];
+            for (int o = 16; o; o >>= 1) {
+                const double ov = __shfl_down_sync(0xffffffffu, v, o);
+                const int op = __shfl_down_sync(0xffffffffu, p, o);
+                if (op >= 0 && (p < 0 || ov < v || (ov == v && op < p))) { v = ov; p = op; }
+            }
+            if (lane == 0 && p >= 0) { ce[fl * 9 + tl] = v; bc[fl * 9 + tl] = p; }
+        }
     }
-    *ce = best;
-    *bc = pos;
 }
 
-// The layer-change tables of every edge of batch b, one (edge, from-layer,
-// to-layer) entry per thread over threads t, t + nt, ...: the reference's
-// precompute_cost_edge launch over the batch's edges (flt.cuh:152), with the
-// to-layer loop spread too.  Edge slot s of the plan belongs to plan position
-// emap[s]; eprefix[k] is the first slot of position k.
-__device__ __forceinline__ void flt_edges_batch(const Tables& T, const Flt& F, const Plan& P, int b, long long t,
-                                                long long nt) {
+// The layer-change tables of every edge of batch b, one warp per edge over
+// warps w, w + nw, ...: the reference's precompute_cost_edge launch over the
+// batch's edges (flt.cuh:152).  Edge slot s of the plan belongs to plan
+// position emap[s]; eprefix[k] is the first slot of position k.
+__device__ __forceinline__ void flt_edges_batch(const Tables& T, const Flt& F, const Plan& P, int b, long long w,
+                                                long long nw, int lane) {
     const int lo = P.batch_off[b], hi = P.batch_off[b + 1];
-    const long long s0 = F.eprefix[lo], items = (static_cast<long long>(F.eprefix[hi]) - s0) * 81;
-    for (long long q = t; q < items; q += nt) {
-        const int s = static_cast<int>(s0 + q / 81), r = static_cast<int>(q % 81);
+    const long long s0 = F.eprefix[lo], items = static_cast<long long>(F.eprefix[hi]) - s0;
+    for (long long q = w; q < items; q += nw) {
+        const int s = static_cast<int>(s0 + q);
         const int k = F.emap[s];
         const int id = P.ids[k];
-        flt_edge_cell(T, F, F.node_off[id], F.edge_off[id] + (s - F.eprefix[k]), r / 9, r % 9);
+        flt_edge_warp(T, F, F.node_off[id], F.edge_off[id] + (s - F.eprefix[k]), lane);
     }
 }
 

@@ -306,7 +306,8 @@ __global__ void __launch_bounds__(kFltThreads) k_flt_batch(Tables T, Flt F, Plan
 
 // Layer-change tables of batch b's edges (flt_edges_batch).
 __global__ void k_flt_edges(Tables T, Flt F, Plan P2, int b) {
-    flt_edges_batch(T, F, P2, b, blockIdx.x * (long long)blockDim.x + threadIdx.x, (long long)gridDim.x * blockDim.x);
+    flt_edges_batch(T, F, P2, b, (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5,
+                    ((long long)gridDim.x * blockDim.x) >> 5, threadIdx.x & 31);
 }
 
 // Persistent FLT stage: per batch, [remove stage-one wires -> remove their
@@ -331,8 +332,7 @@ __global__ void __launch_bounds__(kPersistentThreads, 2) k_flt_persistent(Tables
             clk.mark(S, 6);
         }
         if (!refresh_persistent(T, S, clk, gwarp, nwarps, lane, smem)) return;
-        flt_edges_batch(T, F, P2, b, blockIdx.x * (long long)blockDim.x + threadIdx.x,
-                        (long long)gridDim.x * blockDim.x);
+        flt_edges_batch(T, F, P2, b, gwarp, nwarps, lane);
         if (!grid_sync(S, T)) return;
         clk.mark(S, 10);
         // Net k to global warp k: warp 0 of every block first, so a batch's
