@@ -190,3 +190,19 @@ def steiner_trees(nets: NetArrays, shuffle_seed: int | None = None):
     adj_off = np.cumsum(adj_off).astype(np.int32)
     adj = (dst - node_off[net_of[dst]]).astype(np.int32)
     return TreeArrays(np.asarray(nets.node_off, np.int32), pos, adj_off, adj, np.asarray(nets.route_off, np.int64))
+
+
+def _main(argv=None):
+    """``python -m grotor_b200.synth WORKLOAD CAP NET`` writes a workload's
+    design as the reference's .cap and .net input files."""
+    import argparse
+    ap = argparse.ArgumentParser(prog="python -m grotor_b200.synth")
+    ap.add_argument("workload", choices=sorted(WORKLOADS))
+    ap.add_argument("cap")
+    ap.add_argument("net")
+    args = ap.parse_args(argv)
+    Design(WORKLOADS[args.workload]).write(args.cap, args.net)
+
+
+if __name__ == "__main__":
+    _main()

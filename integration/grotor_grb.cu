@@ -81,11 +81,29 @@ void flt_stage(cudb::RouterState& state, grb_ctx* ctx, const grb_grid& grid, std
     }
 }
 
+// Host wall time of the program's phases (DROPIN_TIMING), from the clock
+// that GROTOR_COMPLETE reads.
+struct Phases {
+    std::chrono::high_resolution_clock::time_point last = program_start;
+    std::vector<std::pair<const char*, double>> ms;
+    void mark(const char* name) {
+        const auto now = std::chrono::high_resolution_clock::now();
+        ms.emplace_back(name, std::chrono::duration<double, std::milli>(now - last).count());
+        last = now;
+    }
+    void print() const {
+        printf("DROPIN_TIMING");
+        for (const auto& [name, v] : ms) printf(" %s_ms=%.3f", name, v);
+        printf("\n");
+    }
+};
+
 // grotor::route (pipeline.hpp:14-157).  The output order is the reference's:
 // single-pin nets, then (after stage one) the nets without overflow, then the
 // rerouted ones.
-void route(cudb::RouterState& state, int32_t mode, bool stop_after_lshape) {
+void route(cudb::RouterState& state, int32_t mode, bool stop_after_lshape, Phases& ph) {
     cudb::prepare_routing_nets(state);
+    ph.mark("prepare");
     int64_t initial_vias = 0;  // one via per metal1 pin (preprocess.hpp:1716-1718)
     for (auto& dbnet : db::nets)
         for (int pin : dbnet.pins) initial_vias += pin < state.device.X * state.device.Y;
@@ -93,6 +111,7 @@ void route(cudb::RouterState& state, int32_t mode, bool stop_after_lshape) {
     grb_ctx* ctx = nullptr;
     check(grb_create(&G.g, 0, &ctx), nullptr, "grb_create");
     std::unique_ptr<grb_ctx, void (*)(grb_ctx*)> owner(ctx, grb_destroy);
+    ph.mark("create");
     Output out{ctx};
     // Single-pin nets first (pipeline.hpp:57-59), written while stage one runs.
     for (int i = 0; i < int(db::nets.size()); ++i)
@@ -101,6 +120,7 @@ void route(cudb::RouterState& state, int32_t mode, bool stop_after_lshape) {
     std::vector<int> all_nets(state.nets.size());
     std::iota(all_nets.begin(), all_nets.end(), 0);
     lshape_stage(state, ctx, all_nets, mode, initial_vias, !stop_after_lshape, report_traffic);
+    ph.mark("lshape");
     if (stop_after_lshape) {
         graph::finish_nets(state, all_nets);
         out.start(state);
@@ -126,15 +146,19 @@ void route(cudb::RouterState& state, int32_t mode, bool stop_after_lshape) {
         state.ripup_flag_cpu[id] = 1;
     }
     state.device.PIN_NUM_PHASE2 = pin_count;
+    ph.mark("classification");
     // The nets without overflow are written while stage two runs, as the
     // reference's output task does (pipeline.hpp:108-109).
     out.start(state);
+    ph.mark("output_start");
     // Stage two sorts of_nets in place (flt.cuh:52), and the reference
     // publishes the rerouted nets in that order (pipeline.hpp:137,143).
     flt_stage(state, ctx, G.g, of_nets, mode, cong, xsum, ysum);
+    ph.mark("flt");
     graph::finish_nets(state, of_nets);
     out.start(state);
     out.wait();
+    ph.mark("output_finish");
     printf("OUTPUT_TIMING format_ms=%.3f output_wait_ms=%.3f executor=grotor_b200\n", out.format_ms, out.wait_ms);
 }
 
@@ -164,7 +188,9 @@ int main(int argc, char** argv) {
         if (cap.empty() || net.empty() || output.empty()) throw std::invalid_argument("-cap, -net and -out are required");
         const int32_t mode = drop_in::executor_mode(executor);
         program_start = std::chrono::high_resolution_clock::now();
+        drop_in::Phases ph;
         db::read(cap.data(), net.data());
+        ph.mark("read");
         const auto caller_directory = std::filesystem::current_path();
         std::filesystem::current_path(lut_dir);
         flute::readLUT();
@@ -172,15 +198,18 @@ int main(int argc, char** argv) {
         out_file = fopen(output.c_str(), "w");
         if (!out_file) throw std::runtime_error("Cannot open output: " + output);
         if (setvbuf(out_file, nullptr, _IONBF, 0)) throw std::runtime_error("Cannot configure routing output");
+        ph.mark("lut");
         {
             cudb::RouterState state;
             state.batch_sparsity_override = 1;
             state.report_score = false;
-            drop_in::route(state, mode, stop_after_lshape);
+            drop_in::route(state, mode, stop_after_lshape, ph);
         }
+        ph.mark("teardown");
         const int close_status = fclose(out_file);
         out_file = nullptr;
         if (close_status) throw std::runtime_error("Failed to close routing output");
+        ph.print();
         printf("GROTOR_COMPLETE wall_seconds=%.6f\n", elapsed_time());
         return EXIT_SUCCESS;
     } catch (const std::exception& error) {

@@ -91,6 +91,7 @@ void route_ggr(cudb::RouterState& state, int32_t mode) {
     std::unique_ptr<grb_ctx, void (*)(grb_ctx*)> owner(ctx, grb_destroy);
     auto& nets = state.nets;
     const int count = int(nets.size());
+    printf("ROUTING_STAGE_BEGIN stage=zshape nets=%d\n", count);  // pipeline_ggr.hpp:17
     std::vector<int> order(count);
     std::iota(order.begin(), order.end(), 0);
     const auto topology_start = std::chrono::steady_clock::now();
@@ -142,6 +143,7 @@ void route_ggr(cudb::RouterState& state, int32_t mode) {
     Output out{ctx};
     out.start(state);
     out.wait();
+    printf("ROUTING_STAGE_END stage=zshape\n");  // pipeline_ggr.hpp:159
 }
 
 }  // namespace drop_in

@@ -1,22 +1,31 @@
-"""The reference router's default pipeline (stage one: L-shape; rip-up; stage
-two: FLT) run end to end twice on the same CAP/NET -- the stock program
-(oracle/_ref/grotor, the reference's own src/main.cu, CPU batching) and the
-drop-in (integration/_build/grotor_grb: the same program with its routing hot
-path on grotor_b200) -- with each program's own stage records, wall time,
-.out agreement and the reference evaluator's scores.  Needs a GPU and both
-programs built (oracle/ref.mk, integration/Makefile).
+"""The reference router's pipelines run end to end twice on the same CAP/NET
+-- the stock program (oracle/_ref: the reference's own src/main.cu built as
+grotor, grotor_ggr and grotor_cugr2) and the drop-in (integration/_build: the
+same program with its routing hot path on grotor_b200) -- with each program's
+own stage records, wall time, .out agreement and the reference evaluator's
+scores.  Needs a GPU and the programs built (oracle/ref.mk,
+integration/Makefile).
+
+Pipelines: "default" (stage one: L-shape; rip-up; stage two: FLT),
+"ggr" (first-fit groups, bounding-box batches, Z-shape stage, the host
+post-processing) and "cugr2" (L-shape, rip-up, FLT detour, the maze stage
+with its score gate).
 
 Records: BATCH_TIMING / DAG_TIMING per stage (the reference's stage metric is
 batching ms + DAG ms), TOPOLOGY_TIMING (stage one: FLUTE and the nets'
 topology; the stock program's also covers its host geometry and DFS),
+MAZE_PHASE_TIMING / MAZE_SEARCH (the maze stage, host search included),
+PIPELINE_TIMING (the stock program's phases) / DROPIN_TIMING (the drop-in's
+phases, from program start),
 GROTOR_COMPLETE (wall seconds of the whole program, reading and writing
 included), OUTPUT_TIMING (the device .out writer: formatting, and the time
-the pipeline waited for the file); from one more run, FLT_TRAFFIC (the FLT
-stage's algorithmic bytes, grb_flt_traffic) and from it each executor's FLT
-stage roofline.
+the pipeline waited for the file); from one more run of the default
+pipeline, FLT_TRAFFIC (the FLT stage's algorithmic bytes, grb_flt_traffic)
+and from it each executor's FLT stage roofline.
 
 Usage:  python integration/stage_timing.py [--workloads medium_320x320x10,large_800x800x10]
-                                           [--executors persistent,plain] [--out FILE]
+                                           [--pipelines default,ggr,cugr2]
+                                           [--executors persistent,plain] [--repeat R] [--out FILE]
 """
 from __future__ import annotations
 
@@ -32,43 +41,65 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 sys.path.insert(0, ROOT)
 REF_DIR = os.path.join(ROOT, "oracle", "_ref")
-STOCK = os.path.join(REF_DIR, "grotor")
-DRIVER = os.path.join(HERE, "_build", "grotor_grb")
 EVALUATOR = os.path.join(REF_DIR, "evaluator")
+# pipeline -> (stock program, drop-in driver, stages in the order their
+# records appear when a program prints no ROUTING_STAGE_BEGIN)
+PIPELINES = {
+    "default": (os.path.join(REF_DIR, "grotor"), os.path.join(HERE, "_build", "grotor_grb"), ("lshape", "detour")),
+    "ggr": (os.path.join(REF_DIR, "grotor_ggr"), os.path.join(HERE, "_build", "grotor_grb_ggr"), ("zshape",)),
+    "cugr2": (os.path.join(REF_DIR, "grotor_cugr2"), os.path.join(HERE, "_build", "grotor_grb_cugr2"),
+              ("lshape", "detour", "maze")),
+}
 
 
-def records(text: str) -> dict:
-    """Stage records of one run: {'lshape': {...}, 'detour': {...}, ...}."""
-    out = {"lshape": {}, "detour": {}}
-    batch_stage = "lshape"
+def records(text: str, stages=("lshape", "detour")) -> dict:
+    """Stage records of one run: {'lshape': {...}, 'detour': {...}, ...}.  A
+    record is filed under the stage it names, else under the stage the last
+    ROUTING_STAGE_BEGIN opened, else under the next stage of `stages` (the
+    default program prints one BATCH_TIMING per batching call, stage one
+    first)."""
+    out = {st: {} for st in stages}
+    pending = list(stages)
+    current = None
     for line in text.splitlines():
         tag, _, rest = line.partition(" ")
         if tag not in ("BATCH_TIMING", "DAG_TIMING", "TOPOLOGY_TIMING", "GROTOR_COMPLETE", "PIPELINE_TIMING",
-                       "FLT_TRAFFIC", "OUTPUT_TIMING"):
+                       "FLT_TRAFFIC", "OUTPUT_TIMING", "DROPIN_TIMING", "ROUTING_STAGE_BEGIN", "MAZE_PHASE_TIMING",
+                       "MAZE_SEARCH", "MAZE_QUALITY_GATE"):
             continue
         kv = dict(p.split("=", 1) for p in rest.split() if "=" in p)
-        if tag == "OUTPUT_TIMING":
+        if tag == "ROUTING_STAGE_BEGIN":
+            current = kv["stage"]
+            out.setdefault(current, {})["stage_nets"] = int(kv["nets"])
+        elif tag == "OUTPUT_TIMING":
             out["output"] = {k: float(v) for k, v in kv.items() if k != "executor"}
         elif tag == "FLT_TRAFFIC":
             out["detour"]["algorithmic_bytes"] = {k: float(v) for k, v in kv.items()}
         elif tag == "GROTOR_COMPLETE":
             out["wall_s"] = float(kv["wall_seconds"])
-        elif tag == "PIPELINE_TIMING":
+        elif tag in ("PIPELINE_TIMING", "DROPIN_TIMING"):
             out["pipeline"] = {k: float(v) for k, v in kv.items()}
+        elif tag == "MAZE_PHASE_TIMING":
+            out.setdefault("maze", {})["phase_ms"] = float(kv["elapsed_ms"])
+        elif tag == "MAZE_SEARCH":
+            out.setdefault("maze", {})["search_ms"] = float(kv["elapsed_ms"])
+        elif tag == "MAZE_QUALITY_GATE":
+            out.setdefault("maze", {})["accepted"] = int(kv["accepted"])
         elif tag == "BATCH_TIMING":
-            # The stock program prints one record per batching call, stage one first.
-            stage = kv.get("stage", batch_stage)
-            out[stage]["batching_ms"] = float(kv["elapsed_ms"])
-            out[stage]["nets"] = int(kv["nets"])
-            out[stage]["batches"] = int(kv["batches"])
-            batch_stage = "detour"
+            stage = kv.get("stage") or current or (pending[0] if pending else "other")
+            if stage in pending:
+                pending.remove(stage)
+            r = out.setdefault(stage, {})
+            r["batching_ms"] = float(kv["elapsed_ms"])
+            r["nets"] = int(kv["nets"])
+            r["batches"] = int(kv["batches"])
         elif tag == "DAG_TIMING" and kv.get("batch_index") == "-1":
-            out[kv["stage"]]["dag_ms"] = float(kv["elapsed_ms"])
+            out.setdefault(kv["stage"], {})["dag_ms"] = float(kv["elapsed_ms"])
         elif tag == "TOPOLOGY_TIMING":
-            out[kv["stage"] if kv["stage"] in out else "detour"]["topology_ms"] = float(kv["elapsed_ms"])
-    for st in ("lshape", "detour"):
-        r = out[st]
-        if "batching_ms" in r and "dag_ms" in r:
+            stage = kv["stage"] if kv["stage"] in out else ("detour" if "detour" in out else kv["stage"])
+            out.setdefault(stage, {})["topology_ms"] = float(kv["elapsed_ms"])
+    for r in out.values():
+        if isinstance(r, dict) and "batching_ms" in r and "dag_ms" in r:
             r["stage_ms"] = r["batching_ms"] + r["dag_ms"]
     return out
 
@@ -122,56 +153,93 @@ def run(cmd):
     return res.stdout, time.perf_counter() - t
 
 
-def measure(workload, executors, log):
-    from grotor_b200.synth import WORKLOADS, Design
-    with tempfile.TemporaryDirectory() as w:
-        cap, net = os.path.join(w, "d.cap"), os.path.join(w, "d.net")
-        Design(WORKLOADS[workload]).write(cap, net)
-        ref_out = os.path.join(w, "ref.out")
-        text, t = run([STOCK, "-cap", cap, "-net", net, "-out", ref_out, "--lut-dir", REF_DIR, "--report-score", "0",
+def median_run(runs):
+    """The run with the median wall time, with every run's wall time."""
+    runs = sorted(runs, key=lambda r: r.get("wall_s", r["process_s"]))
+    pick = dict(runs[(len(runs) - 1) // 2])
+    pick["wall_s_runs"] = [r.get("wall_s") for r in runs]
+    return pick
+
+
+def measure_pipeline(pipeline, cap, net, w, executors, log, repeat=1):
+    """The stock program and the drop-in in each executor, `repeat` times in
+    turn; each program's record is its median-wall run.  Outputs are compared
+    on the first run."""
+    stock, driver, stages = PIPELINES[pipeline]
+    ref_out = os.path.join(w, f"{pipeline}_ref.out")
+    runs = {"reference": []}
+    runs.update({ex: [] for ex in executors})
+    res = {"pipeline": pipeline}
+    for rep in range(repeat):
+        text, t = run([stock, "-cap", cap, "-net", net, "-out", ref_out, "--lut-dir", REF_DIR, "--report-score", "0",
                        "--profile-stages", "1"])
-        res = {"workload": workload, "reference": dict(records(text), process_s=t)}
-        log(f"{workload}: stock reference in {t:.1f} s")
-        ref_nets = parse_out(ref_out)
-        ref_scores = scores(cap, net, ref_out)
-        res["reference"]["scores"] = ref_scores
+        runs["reference"].append(dict(records(text, stages), process_s=t))
+        log(f"{pipeline}: stock reference in {t:.1f} s")
+        if rep == 0:
+            ref_nets = parse_out(ref_out)
+            ref_bytes = open(ref_out, "rb").read()
+            ref_scores = scores(cap, net, ref_out)
         for ex in executors:
-            mine = os.path.join(w, f"{ex}.out")
-            text, t = run([DRIVER, "-cap", cap, "-net", net, "-out", mine, "--lut-dir", REF_DIR, "--executor", ex])
-            log(f"{workload}: drop-in ({ex}) in {t:.1f} s")
-            got = parse_out(mine)
-            same_order = [a for a, _ in ref_nets] == [b for b, _ in got]
-            same_sets = same_order and all(sorted(a) == sorted(b) for (_, a), (_, b) in zip(ref_nets, got))
-            sc = scores(cap, net, mine)
-            r = dict(records(text), process_s=t, net_order_equal=same_order, segments_equal=same_sets,
-                     scores_equal=sc == ref_scores)
-            res[f"grotor_b200_{ex}"] = r
+            mine = os.path.join(w, f"{pipeline}_{ex}.out")
+            text, t = run([driver, "-cap", cap, "-net", net, "-out", mine, "--lut-dir", REF_DIR, "--executor", ex])
+            log(f"{pipeline}: drop-in ({ex}) in {t:.1f} s")
+            r = dict(records(text, stages), process_s=t)
+            if rep == 0:
+                got = parse_out(mine)
+                same_order = [a for a, _ in ref_nets] == [b for b, _ in got]
+                same_sets = same_order and all(sorted(a) == sorted(b) for (_, a), (_, b) in zip(ref_nets, got))
+                sc = scores(cap, net, mine)
+                res[f"{ex}_equal"] = dict(net_order_equal=same_order, segments_equal=same_sets,
+                                          bytes_equal=open(mine, "rb").read() == ref_bytes,
+                                          scores_equal=sc == ref_scores)
+            runs[ex].append(r)
+    res["reference"] = dict(median_run(runs["reference"]), scores=ref_scores)
+    for ex in executors:
+        res[f"grotor_b200_{ex}"] = dict(median_run(runs[ex]), **res.pop(f"{ex}_equal"))
+    if pipeline == "default":
         # The byte model runs on the host after the stage: a separate run, so
         # that its time is in no timed record above.
-        text, _ = run([DRIVER, "-cap", cap, "-net", net, "-out", os.devnull, "--lut-dir", REF_DIR, "--executor",
+        text, _ = run([driver, "-cap", cap, "-net", net, "-out", os.devnull, "--lut-dir", REF_DIR, "--executor",
                        executors[0], "--report-traffic", "1"])
-        model = records(text)["detour"].get("algorithmic_bytes")
+        model = records(text, stages)["detour"].get("algorithmic_bytes")
         for ex in executors:
             d = res[f"grotor_b200_{ex}"]["detour"]
             if model and d.get("dag_ms"):
                 d["roofline"] = flt_roofline(d, model)
-        return res
+    return res
+
+
+def measure(workload, pipelines, executors, log, repeat=1):
+    from grotor_b200.synth import WORKLOADS, Design
+    with tempfile.TemporaryDirectory() as w:
+        cap, net = os.path.join(w, "d.cap"), os.path.join(w, "d.net")
+        Design(WORKLOADS[workload]).write(cap, net)
+        out = []
+        for p in pipelines:
+            r = measure_pipeline(p, cap, net, w, executors, lambda *a: log(f"{workload}:", *a), repeat)
+            out.append(dict(workload=workload, **r))
+        return out
 
 
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--workloads", default="medium_320x320x10,large_800x800x10")
+    ap.add_argument("--pipelines", default="default")
     ap.add_argument("--executors", default="persistent,plain")
+    ap.add_argument("--repeat", type=int, default=1, help="runs of each program, in turn (median wall kept)")
     ap.add_argument("--out", default=None)
     args = ap.parse_args()
-    for f in (STOCK, DRIVER, EVALUATOR):
-        if not os.path.exists(f):
-            sys.exit(f"{f} is not built (oracle/ref.mk, integration/Makefile)")
+    pipelines = args.pipelines.split(",")
+    for p in pipelines:
+        for f in PIPELINES[p][:2] + (EVALUATOR,):
+            if not os.path.exists(f):
+                sys.exit(f"{f} is not built (oracle/ref.mk, integration/Makefile)")
 
     def log(*a):
         print(*a, file=sys.stderr, flush=True)
 
-    results = [measure(wl, args.executors.split(","), log) for wl in args.workloads.split(",")]
+    results = [r for wl in args.workloads.split(",")
+               for r in measure(wl, pipelines, args.executors.split(","), log, args.repeat)]
     text = json.dumps(results, indent=1)
     print(text)
     if args.out:
