@@ -81,6 +81,7 @@ class GrbSynthParams(C.Structure):
 
 # Every exported entry point: name -> (restype, argtypes).
 SIGNATURES = {
+    "grb_init_device": (C.c_int, [C.c_int32]),
     "grb_create": (C.c_int, [C.POINTER(GrbGrid), C.c_int32, C.POINTER(P)]),
     "grb_destroy": (None, [P]),
     "grb_last_error": (C.c_char_p, [P]),

@@ -1818,6 +1818,27 @@ static int launch_batching(grb_ctx* c, BatchState& B, int mode, size_t smem) {
 // ---------------------------------------------------------------------------
 extern "C" {
 
+int grb_init_device(int32_t device) {
+    if (cudaSetDevice(device) != cudaSuccess || cudaFree(nullptr) != cudaSuccess) {
+        cudaGetLastError();
+        return GRB_ECUDA;
+    }
+    // Loading a kernel's code is deferred to its first use; these are the
+    // kernels every stage starts with.
+    const void* kernels[] = {(const void*)k_batch_persistent<kChunkMax>, (const void*)k_lshape_persistent,
+                             (const void*)k_flt_persistent, (const void*)k_zshape_persistent,
+                             (const void*)k_refresh_cells, (const void*)k_prefix_pass1, (const void*)k_prefix_pass2,
+                             (const void*)k_lshape_bucketed, (const void*)k_topo_fill, (const void*)k_out_write};
+    for (const void* k : kernels) {
+        cudaFuncAttributes a{};
+        if (cudaFuncGetAttributes(&a, k) != cudaSuccess) {
+            cudaGetLastError();
+            return GRB_ECUDA;
+        }
+    }
+    return GRB_OK;
+}
+
 int grb_create(const grb_grid* g, int32_t device, grb_ctx** out) {
     if (!out) return GRB_EINVAL;
     *out = nullptr;

@@ -85,6 +85,14 @@ typedef struct grb_stats {
     double dag_ms;             /* device time of the last stage */
 } grb_stats;
 
+/* Start CUDA on `device` and load the library's stage kernels, so that a
+ * caller can overlap this one-time cost with its input reading, as the
+ * reference's main does with cudaFree(nullptr) and cudaFuncGetAttributes in
+ * an asynchronous task while db::read and flute::readLUT run
+ * (src/main.cu:101-106).  Optional: grb_create does the same when it has not
+ * been called.  Safe to call from another thread than the context's. */
+int grb_init_device(int32_t device);
+
 /* Create a context on `device` and upload the grid (build_cuda_database,
  * preprocess.hpp:1625; initialize_incremental_cost, incremental_update.cuh:7). */
 int grb_create(const grb_grid* grid, int32_t device, grb_ctx** out);

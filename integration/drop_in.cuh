@@ -16,6 +16,24 @@
 
 namespace drop_in {
 
+// Host wall time of the program's phases (DROPIN_TIMING), from the clock
+// that GROTOR_COMPLETE reads.
+struct Phases {
+    std::chrono::high_resolution_clock::time_point last = program_start;
+    std::vector<std::pair<const char*, double>> ms;
+    void mark(const char* name) {
+        const auto now = std::chrono::high_resolution_clock::now();
+        ms.emplace_back(name, std::chrono::duration<double, std::milli>(now - last).count());
+        last = now;
+    }
+    void print() const {
+        printf("DROPIN_TIMING");
+        for (const auto& [name, v] : ms) printf(" %s_ms=%.3f", name, v);
+        printf("\n");
+    }
+};
+inline Phases phases;
+
 void check(int rc, grb_ctx* ctx, const char* what) {
     if (rc) throw std::runtime_error(std::string(what) + ": " + (ctx ? grb_last_error(ctx) : "error ") +
                                      " (code " + std::to_string(rc) + ")");
@@ -102,8 +120,10 @@ void lshape_stage(cudb::RouterState& state, grb_ctx* ctx, std::vector<int>& nets
     // depth-first trees are built on the device.
 #pragma omp parallel for num_threads(8)
     for (int i = 0; i < int(nets2route.size()); ++i) nets[nets2route[i]].construct_rsmt(state, true);
+    phases.mark("lshape_flute");
     Trees F = flatten_trees(state);
     check(grb_build_topology(ctx, &F.t), ctx, "grb_build_topology");
+    phases.mark("lshape_topology");
     printf("TOPOLOGY_TIMING stage=lshape elapsed_ms=%.6f geometry_fused=0 executor=grotor_b200\n",
            std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - topology_start).count());
     std::sort(nets2route.begin(), nets2route.end(), [&](int l, int r) { return nets[l].hpwl > nets[r].hpwl; });
@@ -115,6 +135,7 @@ void lshape_stage(cudb::RouterState& state, grb_ctx* ctx, std::vector<int>& nets
     check(grb_set_stage_tail(ctx, tail ? (GRB_TAIL_RIPUP | GRB_TAIL_VIEW) : 0, 0), ctx, "grb_set_stage_tail");
     grb_stats st{};
     check(grb_lshape_stage(ctx, mode, &st), ctx, "grb_lshape_stage");
+    phases.mark("lshape_stage");
     std::vector<int32_t> batch_off(nb + 1);
     int32_t n = 0, nb2 = 0;
     check(grb_get_plan(ctx, nets2route.data(), batch_off.data(), &n, &nb2), ctx, "grb_get_plan");
@@ -205,17 +226,20 @@ FltRun flt_run(cudb::RouterState& state, grb_ctx* ctx, std::vector<int>& nets2ro
         R.node_off.push_back(int32_t(R.coord.size()));
         R.edge_off.push_back(int32_t(R.edge_parent.size()));
         const auto& n = nets[id];
-        for (int p : n.points) points.push_back(p);
+        if (s >= 0) {  // only the listed nets are batched: the others' ranges stay empty
+            for (int p : n.points) points.push_back(p);
+            for (const auto& sg : n.rsmt_h_segments) { hsegs.push_back(sg.first); hsegs.push_back(sg.second); }
+            for (const auto& sg : n.rsmt_v_segments) { vsegs.push_back(sg.first); vsegs.push_back(sg.second); }
+        }
         point_off.push_back(int32_t(points.size()));
-        for (const auto& sg : n.rsmt_h_segments) { hsegs.push_back(sg.first); hsegs.push_back(sg.second); }
         hseg_off.push_back(int32_t(hsegs.size() / 2));
-        for (const auto& sg : n.rsmt_v_segments) { vsegs.push_back(sg.first); vsegs.push_back(sg.second); }
         vseg_off.push_back(int32_t(vsegs.size() / 2));
         const bool stored = s >= 0 || (keep && (*keep)[id]);  // `keep`: storage for earlier stages' routes too
         const int64_t words = stored ? int64_t(n.pins.size()) * words_per_pin : 0;
         R.route2_off.push_back(R.route2_off.back() + words);
     }
     state.flt_topology.clear();
+    phases.mark("flt_flatten");
     check(grb_upload_geometry(ctx, point_off.data(), points.data(), hseg_off.data(), hsegs.data(), vseg_off.data(),
                               vsegs.data()),
           ctx, "grb_upload_geometry");
@@ -226,7 +250,9 @@ FltRun flt_run(cudb::RouterState& state, grb_ctx* ctx, std::vector<int>& nets2ro
                        R.edge_off.data(), R.edge_parent.data(), R.edge_slot.data(), R.route2_off.data()};
     check(grb_upload_flt(ctx, &R.d), ctx, "grb_upload_flt");
     if (before_stage) before_stage(R);
+    phases.mark("flt_upload_plan");
     check(grb_flt_stage(ctx, remove, mode, &R.st), ctx, "grb_flt_stage");
+    phases.mark("flt_stage");
     printf("DAG_TIMING stage=%s batch_index=-1 elapsed_ms=%.6f nets=%zu batches=%d executor=grotor_b200\n", stage,
            R.st.dag_ms, nets2route.size(), R.nb);
     printf("BATCH_TIMING stage=%s backend=grotor_b200 elapsed_ms=%.6f nets=%zu batches=%d used_for_routing=1\n", stage,

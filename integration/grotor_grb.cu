@@ -60,6 +60,7 @@ void flt_stage(cudb::RouterState& state, grb_ctx* ctx, const grb_grid& grid, std
                std::vector<unsigned char>& cong, std::vector<float>& xsum, std::vector<float>& ysum) {
     if (nets2route.empty()) return;
     detour_prepare(state, nets2route, cong, xsum, ysum);
+    phases.mark("flt_prepare");
     FltRun run = flt_run(state, ctx, nets2route, mode, 1, state.device.ROUTE_PER_PIN_PHASE2, "detour");
     if (report_traffic) {
         const int count = int(state.nets.size());
@@ -81,27 +82,11 @@ void flt_stage(cudb::RouterState& state, grb_ctx* ctx, const grb_grid& grid, std
     }
 }
 
-// Host wall time of the program's phases (DROPIN_TIMING), from the clock
-// that GROTOR_COMPLETE reads.
-struct Phases {
-    std::chrono::high_resolution_clock::time_point last = program_start;
-    std::vector<std::pair<const char*, double>> ms;
-    void mark(const char* name) {
-        const auto now = std::chrono::high_resolution_clock::now();
-        ms.emplace_back(name, std::chrono::duration<double, std::milli>(now - last).count());
-        last = now;
-    }
-    void print() const {
-        printf("DROPIN_TIMING");
-        for (const auto& [name, v] : ms) printf(" %s_ms=%.3f", name, v);
-        printf("\n");
-    }
-};
-
 // grotor::route (pipeline.hpp:14-157).  The output order is the reference's:
 // single-pin nets, then (after stage one) the nets without overflow, then the
 // rerouted ones.
-void route(cudb::RouterState& state, int32_t mode, bool stop_after_lshape, Phases& ph) {
+void route(cudb::RouterState& state, int32_t mode, bool stop_after_lshape) {
+    Phases& ph = phases;
     cudb::prepare_routing_nets(state);
     ph.mark("prepare");
     int64_t initial_vias = 0;  // one via per metal1 pin (preprocess.hpp:1716-1718)
@@ -117,10 +102,11 @@ void route(cudb::RouterState& state, int32_t mode, bool stop_after_lshape, Phase
     for (int i = 0; i < int(db::nets.size()); ++i)
         if (db::nets[i].pins.size() == 1) nets2output.push(i);
     out.start(state);
+    ph.mark("output_first");
     std::vector<int> all_nets(state.nets.size());
     std::iota(all_nets.begin(), all_nets.end(), 0);
     lshape_stage(state, ctx, all_nets, mode, initial_vias, !stop_after_lshape, report_traffic);
-    ph.mark("lshape");
+    ph.mark("lshape_rest");
     if (stop_after_lshape) {
         graph::finish_nets(state, all_nets);
         out.start(state);
@@ -154,7 +140,7 @@ void route(cudb::RouterState& state, int32_t mode, bool stop_after_lshape, Phase
     // Stage two sorts of_nets in place (flt.cuh:52), and the reference
     // publishes the rerouted nets in that order (pipeline.hpp:137,143).
     flt_stage(state, ctx, G.g, of_nets, mode, cong, xsum, ysum);
-    ph.mark("flt");
+    ph.mark("flt_rest");
     graph::finish_nets(state, of_nets);
     out.start(state);
     out.wait();
@@ -188,7 +174,10 @@ int main(int argc, char** argv) {
         if (cap.empty() || net.empty() || output.empty()) throw std::invalid_argument("-cap, -net and -out are required");
         const int32_t mode = drop_in::executor_mode(executor);
         program_start = std::chrono::high_resolution_clock::now();
-        drop_in::Phases ph;
+        drop_in::Phases& ph = drop_in::phases;
+        ph.last = program_start;
+        // CUDA starts while the input is read (src/main.cu:101-106).
+        auto gpu_ready = std::async(std::launch::async, [] { return grb_init_device(0); });
         db::read(cap.data(), net.data());
         ph.mark("read");
         const auto caller_directory = std::filesystem::current_path();
@@ -199,11 +188,13 @@ int main(int argc, char** argv) {
         if (!out_file) throw std::runtime_error("Cannot open output: " + output);
         if (setvbuf(out_file, nullptr, _IONBF, 0)) throw std::runtime_error("Cannot configure routing output");
         ph.mark("lut");
+        drop_in::check(gpu_ready.get(), nullptr, "grb_init_device");
+        ph.mark("cuda_init_wait");
         {
             cudb::RouterState state;
             state.batch_sparsity_override = 1;
             state.report_score = false;
-            drop_in::route(state, mode, stop_after_lshape, ph);
+            drop_in::route(state, mode, stop_after_lshape);
         }
         ph.mark("teardown");
         const int close_status = fclose(out_file);

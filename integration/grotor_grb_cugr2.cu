@@ -263,6 +263,8 @@ int main(int argc, char** argv) {
         if (cap.empty() || net.empty() || output.empty()) throw std::invalid_argument("-cap, -net and -out are required");
         const int32_t mode = drop_in::executor_mode(executor);
         program_start = std::chrono::high_resolution_clock::now();
+        // CUDA starts while the input is read (src/main.cu:101-106).
+        auto gpu_ready = std::async(std::launch::async, [] { return grb_init_device(0); });
         db::read(cap.data(), net.data());
         const auto caller_directory = std::filesystem::current_path();
         std::filesystem::current_path(lut_dir);
@@ -271,6 +273,7 @@ int main(int argc, char** argv) {
         out_file = fopen(output.c_str(), "w");
         if (!out_file) throw std::runtime_error("Cannot open output: " + output);
         if (setvbuf(out_file, nullptr, _IONBF, 0)) throw std::runtime_error("Cannot configure routing output");
+        drop_in::check(gpu_ready.get(), nullptr, "grb_init_device");
         {
             cudb::RouterState state;
             state.batch_sparsity_override = 1;

@@ -42,36 +42,55 @@ struct ZTrees {
 ZTrees encode_trees(const cudb::RouterState& state) {
     ZTrees Z;
     const auto& view = state.device;
-    const std::vector<int> zero(state.nets.size(), 0);
-    for (int id = 0; id < int(state.nets.size()); ++id) {
-        const auto& nt = state.nets[id];
-        const auto enc = grotor::zshape::encode_batch({id}, state.nets, zero, view.X, view.Y, view.L);
-        const int* rec = enc.points.data() + enc.points[0];
-        const int cnt = rec[1];
-        const auto& graph = nt.rsmt;
-        const int nodes = int(graph.size()) - 1;
-        int root = 0;
-        for (int i = 0; i < nodes; ++i)
-            if (graph[i].size() == 1) { root = i; break; }
-        std::vector<int> ord, parent(nodes, -1), stack{root};
-        while (!stack.empty()) {
-            const int v = stack.back();
-            stack.pop_back();
-            ord.push_back(v);
-            for (auto it = graph[v].rbegin(); it != graph[v].rend(); ++it) {
-                if (*it == parent[v]) continue;
-                parent[*it] = v;
-                stack.push_back(*it);
+    const int count = int(state.nets.size());
+    const std::vector<int> zero(count, 0);
+    // Nets in contiguous parts, one per thread, each encoded into its own
+    // arrays; the parts are then joined in net order.
+    constexpr int kParts = 8;
+    struct Part { std::vector<int32_t> size, coord, child; };
+    std::vector<Part> parts(kParts);
+#pragma omp parallel for num_threads(kParts) schedule(static, 1)
+    for (int t = 0; t < kParts; ++t) {
+        Part& P = parts[t];
+        const int lo = int(int64_t(count) * t / kParts), hi = int(int64_t(count) * (t + 1) / kParts);
+        std::vector<int> ord, parent, stack;
+        for (int id = lo; id < hi; ++id) {
+            const auto& nt = state.nets[id];
+            const auto enc = grotor::zshape::encode_batch({id}, state.nets, zero, view.X, view.Y, view.L);
+            const int* rec = enc.points.data() + enc.points[0];
+            const int cnt = rec[1];
+            const auto& graph = nt.rsmt;
+            const int nodes = int(graph.size()) - 1;
+            int root = 0;
+            for (int i = 0; i < nodes; ++i)
+                if (graph[i].size() == 1) { root = i; break; }
+            ord.clear();
+            parent.assign(nodes, -1);
+            stack.assign(1, root);
+            while (!stack.empty()) {
+                const int v = stack.back();
+                stack.pop_back();
+                ord.push_back(v);
+                for (auto it = graph[v].rbegin(); it != graph[v].rend(); ++it) {
+                    if (*it == parent[v]) continue;
+                    parent[*it] = v;
+                    stack.push_back(*it);
+                }
             }
-        }
-        for (int k = 0; k < cnt; ++k) {
-            Z.coord.push_back(graph.back()[ord[k]]);
-            for (int j = 0; j < 3; ++j) {
-                const int c = rec[2 + 6 * k + 3 + j];
-                Z.child.push_back(c < 0 ? -1 : c / 6);
+            for (int k = 0; k < cnt; ++k) {
+                P.coord.push_back(graph.back()[ord[k]]);
+                for (int j = 0; j < 3; ++j) {
+                    const int c = rec[2 + 6 * k + 3 + j];
+                    P.child.push_back(c < 0 ? -1 : c / 6);
+                }
             }
+            P.size.push_back(cnt);
         }
-        Z.node_off.push_back(int32_t(Z.coord.size()));
+    }
+    for (const Part& P : parts) {
+        for (int n : P.size) Z.node_off.push_back(Z.node_off.back() + n);
+        Z.coord.insert(Z.coord.end(), P.coord.begin(), P.coord.end());
+        Z.child.insert(Z.child.end(), P.child.begin(), P.child.end());
     }
     Z.t.node_off = Z.node_off.data();
     Z.t.coord = Z.coord.data();
@@ -82,6 +101,7 @@ ZTrees encode_trees(const cudb::RouterState& state) {
 void route_ggr(cudb::RouterState& state, int32_t mode) {
     state.device.ROUTE_PER_PIN = 256;  // pipeline_ggr.hpp:9
     cudb::prepare_routing_nets(state);
+    phases.mark("prepare");
     int64_t initial_vias = 0;  // one via per metal1 pin (preprocess.hpp:1716-1718)
     for (auto& dbnet : db::nets)
         for (int pin : dbnet.pins) initial_vias += pin < state.device.X * state.device.Y;
@@ -89,6 +109,7 @@ void route_ggr(cudb::RouterState& state, int32_t mode) {
     grb_ctx* ctx = nullptr;
     check(grb_create(&G.g, 0, &ctx), nullptr, "grb_create");
     std::unique_ptr<grb_ctx, void (*)(grb_ctx*)> owner(ctx, grb_destroy);
+    phases.mark("create");
     auto& nets = state.nets;
     const int count = int(nets.size());
     printf("ROUTING_STAGE_BEGIN stage=zshape nets=%d\n", count);  // pipeline_ggr.hpp:17
@@ -97,10 +118,12 @@ void route_ggr(cudb::RouterState& state, int32_t mode) {
     const auto topology_start = std::chrono::steady_clock::now();
 #pragma omp parallel for num_threads(8)
     for (int i = 0; i < count; ++i) nets[i].construct_rsmt(state, true);
+    phases.mark("flute");
     Trees F = flatten_trees(state);
     check(grb_build_topology(ctx, &F.t), ctx, "grb_build_topology");
     ZTrees Z = encode_trees(state);
     check(grb_upload_zshape(ctx, &Z.t), ctx, "grb_upload_zshape");
+    phases.mark("topology");
     printf("TOPOLOGY_TIMING stage=zshape elapsed_ms=%.6f executor=grotor_b200\n",
            std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - topology_start).count());
     // pipeline_ggr.hpp:31-33: HPWL descending, larger id first on ties.
@@ -117,6 +140,7 @@ void route_ggr(cudb::RouterState& state, int32_t mode) {
     for (const auto& nt : nets) { bbox.push_back(nt.minx); bbox.push_back(nt.maxx); bbox.push_back(nt.miny); bbox.push_back(nt.maxy); }
     check(grb_plan_bbox_batches(ctx, bbox.data(), 250, &nb), ctx, "grb_plan_bbox_batches");
     grb_stats st{};
+    phases.mark("plan");
     const int zrc = grb_zshape_stage(ctx, mode, &st);
     if (zrc == GRB_ELIMIT) throw std::runtime_error(std::string("Z-shape DP failure or route storage overflow: ") + grb_last_error(ctx));
     check(zrc, ctx, "grb_zshape_stage");
@@ -129,6 +153,7 @@ void route_ggr(cudb::RouterState& state, int32_t mode) {
     const size_t words = size_t(state.device.ROUTE_PER_PIN) * state.device.PIN_NUM + 1;
     state.routes_cpu.reset(new int[words]());
     check(grb_read_routes(ctx, state.routes_cpu.get()), ctx, "grb_read_routes");
+    phases.mark("stage_download");
     const auto post_begin = std::chrono::steady_clock::now();
     const int promoted = grotor::zshape::promote_congested_segments(count, state.device.X, state.device.Y, state.device.L,
         state.device.ROUTE_PER_PIN, state.pin_cnt_sum_cpu, state.routes_cpu.get());
@@ -136,6 +161,7 @@ void route_ggr(cudb::RouterState& state, int32_t mode) {
                                         state.pin_cnt_sum_cpu, state.routes_cpu.get());
     printf("ZSHAPE_POSTPROCESS promoted_segments=%d elapsed_ms=%.6f\n", promoted,
            std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - post_begin).count());
+    phases.mark("postprocess");
     check(grb_write_routes(ctx, state.routes_cpu.get()), ctx, "grb_write_routes");
     for (int i = 0; i < int(db::nets.size()); ++i)
         if (db::nets[i].pins.size() == 1) nets2output.push(i);
@@ -143,6 +169,7 @@ void route_ggr(cudb::RouterState& state, int32_t mode) {
     Output out{ctx};
     out.start(state);
     out.wait();
+    phases.mark("output");
     printf("ROUTING_STAGE_END stage=zshape\n");  // pipeline_ggr.hpp:159
 }
 
@@ -166,7 +193,11 @@ int main(int argc, char** argv) {
         if (cap.empty() || net.empty() || output.empty()) throw std::invalid_argument("-cap, -net and -out are required");
         const int32_t mode = drop_in::executor_mode(executor);
         program_start = std::chrono::high_resolution_clock::now();
+        // CUDA starts while the input is read (src/main.cu:101-106).
+        auto gpu_ready = std::async(std::launch::async, [] { return grb_init_device(0); });
+        drop_in::phases.last = program_start;
         db::read(cap.data(), net.data());
+        drop_in::phases.mark("read");
         const auto caller_directory = std::filesystem::current_path();
         std::filesystem::current_path(lut_dir);
         flute::readLUT();
@@ -174,15 +205,20 @@ int main(int argc, char** argv) {
         out_file = fopen(output.c_str(), "w");
         if (!out_file) throw std::runtime_error("Cannot open output: " + output);
         if (setvbuf(out_file, nullptr, _IONBF, 0)) throw std::runtime_error("Cannot configure routing output");
+        drop_in::phases.mark("lut");
+        drop_in::check(gpu_ready.get(), nullptr, "grb_init_device");
+        drop_in::phases.mark("cuda_init_wait");
         {
             cudb::RouterState state;
             state.batch_sparsity_override = 1;
             state.report_score = false;
             drop_in::route_ggr(state, mode);
         }
+        drop_in::phases.mark("teardown");
         const int close_status = fclose(out_file);
         out_file = nullptr;
         if (close_status) throw std::runtime_error("Failed to close routing output");
+        drop_in::phases.print();
         printf("GROTOR_COMPLETE wall_seconds=%.6f\n", elapsed_time());
         return EXIT_SUCCESS;
     } catch (const std::exception& error) {
