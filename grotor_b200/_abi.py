@@ -103,6 +103,7 @@ SIGNATURES = {
     "grb_upload_geometry": (C.c_int, [P, P, P, P, P, P, P]),
     "grb_upload_flt": (C.c_int, [P, C.POINTER(GrbFltDags)]),
     "grb_flt_stage": (C.c_int, [P, C.c_int32, C.c_int32, C.POINTER(GrbStats)]),
+    "grb_set_flt_block_width": (C.c_int, [P, C.c_int32]),
     "grb_read_routes2": (C.c_int, [P, P]),
     "grb_write_routes2": (C.c_int, [P, P]),
     "grb_remove_routes": (C.c_int, [P, P, C.c_int32, P]),

@@ -14,15 +14,16 @@ namespace grb {
 
 __device__ __forceinline__ const int* net_routes(const Plan& P, int id) { return P.routes + P.route_off[id]; }
 
-// One warp commits the wire segments of net `id`; lanes split each segment's
+// One warp commits the wire segments of net `id` (of `parts` warps sharing a
+// net, warp `part` takes every parts-th segment); lanes split each segment's
 // unit edges.  Along-y segments cover consecutive cells, so their dirty bits
 // are set a bitmap word at a time (fenwick.cuh:51-78).
 __device__ __forceinline__ void commit_net_wires(const Tables& T, const Plan& P, int id, int stamp, int K,
-                                                 int lane) {
+                                                 int lane, int part = 0, int parts = 1) {
     const int* r = net_routes(P, id);
     const int words = r[0];
     double length = 0;
-    for (int i = 1; i < words; i += 2) {
+    for (int i = 1 + 2 * part; i < words; i += 2 * parts) {
         const int a = r[i], b = r[i + 1], layer = a / T.XY;
         if (layer != b / T.XY) continue;
         const int ra = a - layer * T.XY, rb = b - layer * T.XY;

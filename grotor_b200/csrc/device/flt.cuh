@@ -63,6 +63,10 @@ struct Flt {
     // edges, [plan+1]); per edge slot: its plan position
     const int* eprefix;
     const int* emap;
+    // per plan position, batch by batch: the batch's positions with its wide
+    // nets (a DAG level wider than a warp) first; per batch: its wide nets
+    const int* border;
+    const int* nwide;
 };
 
 __device__ __forceinline__ double flt_wire(const Tables& T, int l, int xmin, int xmax, int ymin, int ymax) {
@@ -411,6 +415,73 @@ __device__ __forceinline__ void flt_net(const Tables& T, const Flt& F, const Pla
     }
     __syncwarp();
     if (commit && !bad) commit_net_wires(T, P2, id, stamp, 1, lane);
+}
+
+// Route net `id` with the whole CTA: flt_net for nets whose DAG has a level
+// wider than a warp, the CTA's threads over a level's nodes.  The words go
+// out in the same order (level by level, ascending node index, each node's
+// wires before its via stack): a block scan of the words per node replaces
+// the warp scan.  All threads of the CTA call with the same id.
+__device__ __forceinline__ void flt_net_block(const Tables& T, const Flt& F, const Plan& P2, int id, int stamp,
+                                              bool commit) {
+    __shared__ int wsum[32];
+    const int tid = threadIdx.x, nth = blockDim.x, lane = tid & 31, warp = tid >> 5, nw = nth >> 5;
+    const int nb = F.node_off[id], N = F.node_off[id + 1] - nb;
+    const int eb = F.edge_off[id];
+    if (N <= 0) return;
+    for (int k = tid; k < N * kFltLayers; k += nth) F.costs[size_t(nb) * kFltLayers + k] = kInf;
+    const int cb = F.child_off[nb], cn = F.child_off[nb + N - 1] + F.children[nb + N - 1] - cb;
+    for (int k = tid; k < cn * kFltLayers; k += nth) F.packed[size_t(cb) * kFltLayers + k] = kFltInit;
+    __syncthreads();
+    const int* lev = F.level + F.lvl_off[id];
+    const int nl = F.lvl_off[id + 1] - F.lvl_off[id] - 1;
+    const int* ord = F.order + nb;
+    for (int d = nl - 1; d >= 0; --d) {
+        for (int k = lev[d] + tid; k < lev[d + 1]; k += nth) flt_solve_node(T, F, nb, eb, ord[k]);
+        __syncthreads();
+    }
+    int* r = F.routes2 + P2.route_off[id];
+    const long long cap = P2.route_off[id + 1] - P2.route_off[id];
+    long long count = 1;
+    bool bad = false;
+    for (int d = 0; d < nl; ++d) {
+        for (int base = lev[d]; base < lev[d + 1]; base += nth) {
+            int w[8];
+            int n = 0;
+            if (base + tid < lev[d + 1]) n = flt_trace_node(T, F, nb, eb, ord[base + tid], w);
+            const bool neg = n < 0;
+            n = max(n, 0);
+            int off = n;  // inclusive scan inside the warp
+            for (int s = 1; s < 32; s <<= 1) {
+                const int v = __shfl_up_sync(0xffffffffu, off, s);
+                if (lane >= s) off += v;
+            }
+            if (lane == 31) wsum[warp] = off;
+            if (__syncthreads_or(neg)) bad = true;
+            if (warp == 0) {  // inclusive scan of the warp totals
+                int v = lane < nw ? wsum[lane] : 0;
+                for (int s = 1; s < 32; s <<= 1) {
+                    const int u = __shfl_up_sync(0xffffffffu, v, s);
+                    if (lane >= s) v += u;
+                }
+                if (lane < nw) wsum[lane] = v;
+            }
+            __syncthreads();
+            const int total = wsum[nw - 1];
+            off += (warp ? wsum[warp - 1] : 0) - n;
+            if (count + total <= cap)
+                for (int k = 0; k < n; ++k) r[count + off + k] = w[k];
+            else bad = true;
+            count += total;
+            __syncthreads();  // wsum is reused by the next round
+        }
+    }
+    if (tid == 0) {
+        if (bad) { set_error(T, kELimit, id); r[0] = 1; }
+        else r[0] = int(count);
+    }
+    __syncthreads();
+    if (commit && !bad) commit_net_wires(T, P2, id, stamp, 1, lane, warp, nw);
 }
 
 }  // namespace grb

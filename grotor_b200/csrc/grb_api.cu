@@ -297,11 +297,16 @@ __global__ void __launch_bounds__(kPersistentThreads, 2) k_lshape_persistent(Tab
 constexpr int kFltThreads = 128;
 
 // One warp per net of batch b: layer-change tables, solve, trace, wires.
-__global__ void __launch_bounds__(kFltThreads) k_flt_batch(Tables T, Flt F, Plan P2, int b, int stamp) {
+// Blocks below `nw` take the batch's wide nets, a CTA each.
+__global__ void __launch_bounds__(kFltThreads) k_flt_batch(Tables T, Flt F, Plan P2, int b, int stamp, int nw) {
     const int lane = threadIdx.x & 31;
-    const int k = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lo = P2.batch_off[b], cnt = P2.batch_off[b + 1] - lo;
-    if (k < cnt) flt_net(T, F, P2, P2.ids[lo + k], stamp, lane, true);
+    if (int(blockIdx.x) < nw) {
+        flt_net_block(T, F, P2, P2.ids[F.border[lo + blockIdx.x]], stamp, true);
+        return;
+    }
+    const int k = nw + (((blockIdx.x - nw) * blockDim.x + threadIdx.x) >> 5);
+    if (k < cnt) flt_net(T, F, P2, P2.ids[F.border[lo + k]], stamp, lane, true);
 }
 
 // Layer-change tables of batch b's edges (flt_edges_batch).
@@ -335,10 +340,19 @@ __global__ void __launch_bounds__(kPersistentThreads, 2) k_flt_persistent(Tables
         flt_edges_batch(T, F, P2, b, gwarp, nwarps, lane);
         if (!grid_sync(S, T)) return;
         clk.mark(S, 10);
-        // Net k to global warp k: warp 0 of every block first, so a batch's
-        // nets (often fewer than the blocks) land on different SMs, each with
-        // its L1 to itself for the nets' thread-local arrays.
-        for (int k = gwarp; k < cnt; k += nwarps) flt_net(T, F, P2, P2.ids[lo + k], stamp, lane, true);
+        // The batch's wide nets a CTA each, from block 0; the others a warp
+        // each, to global warps in block-major order over the remaining blocks
+        // (warp 0 of every block first, so a batch's nets -- often fewer than
+        // the blocks -- land on different SMs, each with its L1 to itself for
+        // the nets' thread-local arrays).  With at least as many wide nets as
+        // blocks, every block takes wide nets in turn and then every warp the
+        // others.
+        const int nw = F.nwide[b], G = gridDim.x, wpb = blockDim.x >> 5;
+        for (int k = blockIdx.x; k < nw; k += G) flt_net_block(T, F, P2, P2.ids[F.border[lo + k]], stamp, true);
+        const int G2 = nw < G ? G - nw : G, b2 = nw < G ? int(blockIdx.x) - nw : int(blockIdx.x);
+        if (b2 >= 0)
+            for (int k = nw + warp * G2 + b2; k < cnt; k += G2 * wpb)
+                flt_net(T, F, P2, P2.ids[F.border[lo + k]], stamp, lane, true);
         if (!grid_sync(S, T)) return;
         clk.mark(S, 5);
         commit_vias_strided(T, P2, P2.ids + lo, cnt, gwarp, nwarps, stamp, 1, lane);
@@ -1082,9 +1096,16 @@ struct grb_ctx {
     long long flt_emap_cap = 0;
     int flt_emap_plan = -1, flt_emap_flt = -1;  // plan / DAG versions the map was built for
     std::vector<long long> h_route2_off;
+    std::vector<int> h_flt_width;     // per net: nodes of its widest DAG level
+    int flt_block_width = 32;         // wider nets are routed by a whole CTA (< 0: none)
+    int* flt_border = nullptr;        // plan positions, each batch's wide nets first
+    int* flt_nwide = nullptr;         // wide nets per batch
+    long long flt_border_cap = 0, flt_nwide_cap = 0;
+    long long flt_border_key[3] = {-1, -1, -1};  // plan, DAG versions and width it was built for
+    std::vector<int> h_flt_nwide;
     int flt_version = 0;
     cudaGraphExec_t flt_graph = nullptr;
-    long long flt_graph_key[4] = {-1, -1, -1, -1};
+    long long flt_graph_key[5] = {-1, -1, -1, -1, -1};
     int64_t flt_graph_kernels = 0;
     // Z-shape stage (grb_upload_zshape)
     std::vector<void*> z_bufs;
@@ -1611,8 +1632,9 @@ int flt_stage_plain(grb_ctx* c, int stamp0, int remove) {
         if ((rc = prof_begin(c, 5, &e))) return rc;
         k_flt_edges<<<c->sms * 8, 256, 0, c->stream>>>(c->T, c->F, P2, b);
         c->launches += 1;
-        k_flt_batch<<<(cnt + kFltThreads / 32 - 1) / (kFltThreads / 32), kFltThreads, 0, c->stream>>>(c->T, c->F, P2, b,
-                                                                                                      stamp);
+        const int nw = c->h_flt_nwide[b];
+        k_flt_batch<<<nw + (cnt - nw + kFltThreads / 32 - 1) / (kFltThreads / 32), kFltThreads, 0, c->stream>>>(
+            c->T, c->F, P2, b, stamp, nw);
         prof_end(c, e);
         if ((rc = prof_begin(c, 6, &e))) return rc;
         k_commit_vias<<<cblocks, 128, 0, c->stream>>>(c->T, P2, b, stamp, 1);
@@ -1624,8 +1646,8 @@ int flt_stage_plain(grb_ctx* c, int stamp0, int remove) {
 }
 
 int flt_stage_graph(grb_ctx* c, int stamp0, int remove) {
-    const long long key[4] = {c->plan_version, c->flt_version, stamp0, remove};
-    if (!c->flt_graph || !std::equal(key, key + 4, c->flt_graph_key)) {
+    const long long key[5] = {c->plan_version, c->flt_version, stamp0, remove, c->flt_block_width};
+    if (!c->flt_graph || !std::equal(key, key + 5, c->flt_graph_key)) {
         if (c->flt_graph) { cudaGraphExecDestroy(c->flt_graph); c->flt_graph = nullptr; }
         const int64_t before = c->launches;
         const bool prof = c->profiling;
@@ -1642,7 +1664,7 @@ int flt_stage_graph(grb_ctx* c, int stamp0, int remove) {
         if (ei != cudaSuccess) return cuda_fail(c, ei, "cudaGraphInstantiate");
         c->flt_graph_kernels = c->launches - before;
         c->launches = before;
-        std::copy(key, key + 4, c->flt_graph_key);
+        std::copy(key, key + 5, c->flt_graph_key);
     }
     GRB_CUDA(c, cudaGraphLaunch(c->flt_graph, c->stream));
     c->launches += c->flt_graph_kernels;
@@ -1994,6 +2016,8 @@ void grb_destroy(grb_ctx* c) {
     if (c->out_stream) cudaStreamDestroy(c->out_stream);
     if (c->flt_eprefix) cudaFree(c->flt_eprefix);
     if (c->flt_emap) cudaFree(c->flt_emap);
+    if (c->flt_border) cudaFree(c->flt_border);
+    if (c->flt_nwide) cudaFree(c->flt_nwide);
     if (c->ckpt_demand) cudaFree(c->ckpt_demand);
     if (c->score_partials) cudaFree(c->score_partials);
     free_all(c->owned);
@@ -2707,7 +2731,7 @@ int grb_upload_flt(grb_ctx* c, const grb_flt_dags* d) {
         return fail(c, GRB_EINVAL, "FLT DAG arrays missing");
     // Host validation (every index the kernels dereference) and the derived
     // per-node arrays: global child offsets, depth-sorted order, level offsets.
-    std::vector<int> child_off(size_t(nn) + 1), order(nn), eslot(ne), lvl_off(n + 1, 0), level;
+    std::vector<int> child_off(size_t(nn) + 1), order(nn), eslot(ne), lvl_off(n + 1, 0), level, width(n, 0);
     long long children = 0;
     for (int id = 0; id < n; ++id) {
         const int nb = d->node_off[id], N = d->node_off[id + 1] - nb;
@@ -2748,6 +2772,7 @@ int grb_upload_flt(grb_ctx* c, const grb_flt_dags* d) {
         }
         std::vector<int> cnt(maxd + 2, 0);
         for (int i = 0; i < N; ++i) ++cnt[d->depth[nb + i] + 1];
+        for (int q = 0; q <= maxd; ++q) width[id] = std::max(width[id], cnt[q + 1]);
         for (int q = 0; q <= maxd; ++q) cnt[q + 1] += cnt[q];
         for (int q = 0; q <= maxd + 1; ++q) level.push_back(cnt[q]);
         for (int i = 0; i < N; ++i) order[nb + cnt[d->depth[nb + i]]++] = i;  // stable by index
@@ -2808,6 +2833,7 @@ int grb_upload_flt(grb_ctx* c, const grb_flt_dags* d) {
     c->h_flt_node_off.assign(d->node_off, d->node_off + n + 1);
     c->h_flt_edge_off.assign(d->edge_off, d->edge_off + n + 1);
     c->h_route2_off.assign(d->route2_off, d->route2_off + n + 1);
+    c->h_flt_width = std::move(width);
     ++c->flt_version;
     return GRB_OK;
 }
@@ -3090,6 +3116,12 @@ int grb_lshape_stage(grb_ctx* c, int32_t mode, grb_stats* stats) {
     return stats ? grb_get_stats(c, stats) : GRB_OK;
 }
 
+int grb_set_flt_block_width(grb_ctx* c, int32_t width) {
+    if (!c) return GRB_EINVAL;
+    c->flt_block_width = width;
+    return GRB_OK;
+}
+
 int grb_flt_stage(grb_ctx* c, int32_t remove_phase_one, int32_t mode, grb_stats* stats) {
     if (!c) return GRB_EINVAL;
     if (c->flt_n != c->n_nets || c->flt_n < 0) return fail(c, GRB_EINVAL, "no FLT DAGs uploaded for the current nets");
@@ -3135,6 +3167,43 @@ int grb_flt_stage(grb_ctx* c, int32_t remove_phase_one, int32_t mode, grb_stats*
     }
     c->F.eprefix = c->flt_eprefix;
     c->F.emap = c->flt_emap;
+    const long long bkey[3] = {c->plan_version, c->flt_version, c->flt_block_width};
+    if (!std::equal(bkey, bkey + 3, c->flt_border_key)) {
+        // Each batch's positions with its wide nets first (a net's place inside
+        // its batch changes nothing: the nets of a batch are independent).
+        std::vector<int> border(std::max(c->plan_n, 1)), nwide(std::max(c->n_batches, 1), 0);
+        for (int b = 0; b < c->n_batches; ++b) {
+            int w = c->h_batch_off[b];
+            for (int pass = 0; pass < 2; ++pass)
+                for (int k = c->h_batch_off[b]; k < c->h_batch_off[b + 1]; ++k) {
+                    const bool wide = c->flt_block_width >= 0 && c->h_flt_width[ids[k]] > c->flt_block_width;
+                    if (wide == (pass == 0)) border[w++] = k;
+                    if (wide && pass == 0) ++nwide[b];
+                }
+        }
+        if (c->flt_border_cap < (long long)border.size() || c->flt_nwide_cap < (long long)nwide.size()) {
+            if (c->flt_border) cudaFree(c->flt_border);
+            if (c->flt_nwide) cudaFree(c->flt_nwide);
+            c->flt_border = c->flt_nwide = nullptr;
+            c->flt_border_cap = c->flt_nwide_cap = 0;
+            if (cudaMalloc(&c->flt_border, sizeof(int) * border.size()) != cudaSuccess ||
+                cudaMalloc(&c->flt_nwide, sizeof(int) * nwide.size()) != cudaSuccess) {
+                cudaGetLastError();
+                return fail(c, GRB_ENOMEM, "FLT net order");
+            }
+            c->flt_border_cap = (long long)border.size();
+            c->flt_nwide_cap = (long long)nwide.size();
+        }
+        GRB_CUDA(c, cudaMemcpyAsync(c->flt_border, border.data(), sizeof(int) * border.size(), cudaMemcpyHostToDevice,
+                                    c->stream));
+        GRB_CUDA(c, cudaMemcpyAsync(c->flt_nwide, nwide.data(), sizeof(int) * nwide.size(), cudaMemcpyHostToDevice,
+                                    c->stream));
+        GRB_CUDA(c, cudaStreamSynchronize(c->stream));
+        c->h_flt_nwide = std::move(nwide);
+        std::copy(bkey, bkey + 3, c->flt_border_key);
+    }
+    c->F.border = c->flt_border;
+    c->F.nwide = c->flt_nwide;
     const int remove = remove_phase_one ? 1 : 0;
     const int stamp0 = c->stamp;
     GRB_CUDA(c, cudaEventRecord(c->ev0, c->stream));

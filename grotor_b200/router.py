@@ -297,6 +297,11 @@ class Router:
         self._check(self._lib.grb_flt_stage(self._ctx, int(bool(remove_phase_one)), mode_id(mode), C.byref(st)))
         return _stats_dict(st)
 
+    def set_flt_block_width(self, width: int):
+        """Nets whose widest FLT DAG level holds more than `width` nodes are
+        routed by a whole CTA (default 32; negative: every net by one warp)."""
+        self._check(self._lib.grb_set_flt_block_width(self._ctx, int(width)))
+
     def read_routes2(self) -> np.ndarray:
         out = np.zeros(getattr(self, "_route2_words", 0), np.int32)
         self._check(self._lib.grb_read_routes2(self._ctx, _p(out)))

@@ -246,6 +246,12 @@ int grb_upload_flt(grb_ctx* ctx, const grb_flt_dags* dags);
  * phase-two routes.  mode: GRB_MODE_PLAIN, GRAPH or PERSISTENT. */
 int grb_flt_stage(grb_ctx* ctx, int32_t remove_phase_one, int32_t mode, grb_stats* stats);
 
+/* Nets whose widest FLT DAG level holds more than `width` nodes are solved
+ * and traced by a whole CTA (its threads over a level's nodes), the others by
+ * one warp each; routes, demand and statistics are the same either way.
+ * Default 32; a negative width routes every net with one warp. */
+int grb_set_flt_block_width(grb_ctx* ctx, int32_t width);
+
 /* ---- Maze stage of the CUGR2 pipeline (pipeline_cugr2.hpp:90-117) -------- */
 /* maze::remove_routes (maze.cuh:24-64): remove the current routes of nets
  * ids[0..n) -- the phase-two words where phase2[k] is set, the stage-one

@@ -34,6 +34,10 @@ struct Phases {
 };
 inline Phases phases;
 
+// FLT nets whose widest DAG level holds more nodes than this go to a whole
+// CTA (grb_set_flt_block_width; the library's default).
+inline int flt_block_width = 32;
+
 void check(int rc, grb_ctx* ctx, const char* what) {
     if (rc) throw std::runtime_error(std::string(what) + ": " + (ctx ? grb_last_error(ctx) : "error ") +
                                      " (code " + std::to_string(rc) + ")");
@@ -249,6 +253,7 @@ FltRun flt_run(cudb::RouterState& state, grb_ctx* ctx, std::vector<int>& nets2ro
     R.d = grb_flt_dags{R.node_off.data(), R.coord.data(), R.depth.data(), R.children.data(), R.parent_end.data(),
                        R.edge_off.data(), R.edge_parent.data(), R.edge_slot.data(), R.route2_off.data()};
     check(grb_upload_flt(ctx, &R.d), ctx, "grb_upload_flt");
+    check(grb_set_flt_block_width(ctx, flt_block_width), ctx, "grb_set_flt_block_width");
     if (before_stage) before_stage(R);
     phases.mark("flt_upload_plan");
     check(grb_flt_stage(ctx, remove, mode, &R.st), ctx, "grb_flt_stage");

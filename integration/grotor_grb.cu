@@ -37,6 +37,7 @@
 //
 // Usage: grotor_grb -cap FILE -net FILE -out FILE [--lut-dir DIR]
 //                   [--executor persistent|plain|graph] [--stop-after lshape|routing]
+//                   [--flt-block-width N]
 //                   [--report-traffic 0|1]
 #include "pipeline.hpp"
 
@@ -157,6 +158,7 @@ int main(int argc, char** argv) {
         if (argc < 7 || argc % 2 != 1)
             throw std::invalid_argument("Usage: grotor_grb -cap FILE -net FILE -out FILE [--lut-dir DIR] "
                                         "[--executor persistent|plain|graph] [--stop-after lshape|routing] "
+                                        "[--flt-block-width N] "
                                         "[--report-traffic 0|1]");
         for (int i = 1; i < argc; i += 2) {
             const std::string option = argv[i], value = argv[i + 1];
@@ -166,6 +168,7 @@ int main(int argc, char** argv) {
             else if (option == "--lut-dir") lut_dir = value;
             else if (option == "--executor") executor = value;
             else if (option == "--report-traffic") drop_in::report_traffic = value == "1";
+            else if (option == "--flt-block-width") drop_in::flt_block_width = std::stoi(value);
             else if (option == "--stop-after") {
                 if (value != "lshape" && value != "routing") throw std::invalid_argument("--stop-after expects lshape or routing");
                 stop_after_lshape = value == "lshape";

@@ -102,3 +102,31 @@ def test_flt_stage_equals_oracle(name):
         exact += np.array_equal(a[:a[0]], b[:b[0]])
     assert exact >= 0.95 * len(g["flt_nets"])
     r.close()
+
+
+@pytest.mark.parametrize("mode", ["plain", "persistent"])
+@pytest.mark.parametrize("name", NAMES)
+def test_flt_block_path_equals_warp_path(name, mode):
+    """Nets routed by a whole CTA (a DAG level wider than the threshold) give
+    the same route words, demand and statistics as one warp per net: every
+    net by one warp (-1), every net by a CTA (0), and a mix (2)."""
+    g = load_golden(name)
+    need_flt(g)
+    dags, _, route2_off = flt_by_net(g)
+    out = {}
+    for width in (-1, 0, 2):
+        r = router_after_lshape(g)
+        r.upload_flt(dags, route2_off)
+        r.set_plan(g["flt_batch_ids"], g["flt_batch_off"])
+        r.set_flt_block_width(width)
+        st = r.flt_route(mode, remove_phase_one=True)
+        out[width] = (r.read_routes2(), r.read_tables(), st)
+        r.close()
+    routes_w, tables_w, st_w = out[-1]
+    np.testing.assert_array_equal(tables_w["demand_half"], float_demand_to_half(g["flt_after_demand"]))
+    for width in (0, 2):
+        routes, tables, st = out[width]
+        np.testing.assert_array_equal(routes, routes_w)
+        np.testing.assert_array_equal(tables["demand_half"], tables_w["demand_half"])
+        np.testing.assert_array_equal(tables["timestamp"], tables_w["timestamp"])
+        assert (st["wirelength"], st["vias"], st["stamp"]) == (st_w["wirelength"], st_w["vias"], st_w["stamp"])
