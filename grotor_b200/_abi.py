@@ -127,6 +127,8 @@ SIGNATURES = {
     "grb_read_stage_tail": (C.c_int, [P, P, P, P, P]),
     "grb_read_tables": (C.c_int, [P, P, P, P, P, P]),
     "grb_read_routes": (C.c_int, [P, P]),
+    "grb_read_routes_used": (C.c_int, [P, P]),
+    "grb_write_routes_used": (C.c_int, [P, P]),
     "grb_write_routes": (C.c_int, [P, P]),
     "grb_get_stats": (C.c_int, [P, C.POINTER(GrbStats)]),
     "grb_set_stats": (C.c_int, [P, C.c_double, C.c_int64]),

@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <thread>
 #include <climits>
 #include <cstdio>
 #include <cstring>
@@ -775,6 +776,29 @@ __global__ void k_scan_add(long long* a, int n, const long long* sums, int tiles
     if (i == 0) a[n] = sums[tiles];
 }
 
+// Route words in use per net: the count word and the words below it,
+// clamped to the net's storage (at least the count word).
+__global__ void k_route_used(const int* routes, const long long* route_off, int n, long long* used) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const long long cap = route_off[i + 1] - route_off[i];
+    used[i] = cap > 0 ? max(1ll, min(static_cast<long long>(routes[route_off[i]]), cap)) : 0;
+}
+// One warp per net moves its words in use between the route storage and a
+// packed array (pos: exclusive prefix of the words in use).
+__global__ void k_route_move(const long long* route_off, const long long* pos, int n, int* routes, int* packed,
+                             int to_packed) {
+    const int lane = threadIdx.x & 31;
+    for (long long i = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5; i < n;
+         i += ((long long)gridDim.x * blockDim.x) >> 5) {
+        const long long a = pos[i], m = pos[i + 1] - a, r = route_off[i];
+        for (long long k = lane; k < m; k += 32) {
+            if (to_packed) packed[a + k] = routes[r + k];
+            else routes[r + k] = packed[a + k];
+        }
+    }
+}
+
 // Plain form: one launch per step and chunk.
 __device__ __forceinline__ long long launch_thread() { return blockIdx.x * (long long)blockDim.x + threadIdx.x; }
 __device__ __forceinline__ long long launch_threads() { return (long long)gridDim.x * blockDim.x; }
@@ -1096,6 +1120,11 @@ struct grb_ctx {
     long long flt_emap_cap = 0;
     int flt_emap_plan = -1, flt_emap_flt = -1;  // plan / DAG versions the map was built for
     std::vector<long long> h_route2_off;
+    std::vector<void*> used_bufs;     // grb_read/write_routes_used: positions, tile sums, packed words
+    long long used_n_cap = -1, used_words_cap = 0;
+    long long* used_pos = nullptr;
+    long long* used_sums = nullptr;
+    int* used_pack = nullptr;
     std::vector<int> h_flt_width;     // per net: nodes of its widest DAG level
     int flt_block_width = 32;         // wider nets are routed by a whole CTA (< 0: none)
     int* flt_border = nullptr;        // plan positions, each batch's wide nets first
@@ -1541,6 +1570,7 @@ int soft_workspace(grb_ctx* c) {
     const size_t slot = 2 * size_t(std::max(c->topo_sizes[0], 1ll)) * c->T.L * c->T.L * sizeof(double);
     if (c->soft_cells && c->soft_slot_bytes >= slot) return GRB_OK;
     GRB_CUDA(c, cudaStreamSynchronize(c->stream));
+    free_all(c->used_bufs);
     free_all(c->soft_bufs);
     int rc = 0;
     rc |= dalloc(c, &c->soft_cells, 6 * cells * sizeof(double), c->soft_bufs);
@@ -3571,6 +3601,113 @@ int grb_read_routes(grb_ctx* c, int32_t* routes) {
     if (!c || !routes) return GRB_EINVAL;
     GRB_CUDA(c, cudaSetDevice(c->device));
     if (c->route_words) GRB_CUDA(c, cudaMemcpyAsync(routes, c->routes, sizeof(int) * c->route_words, cudaMemcpyDeviceToHost, c->stream));
+    GRB_CUDA(c, cudaStreamSynchronize(c->stream));
+    return GRB_OK;
+}
+
+// Host side of the used-word transfers: device positions for n nets and a
+// packed buffer of `words` (grown as needed), and the host route offsets.
+static int used_buffers(grb_ctx* c, long long words) {
+    const int n = c->n_nets;
+    if (c->used_n_cap < n) {
+        free_all(c->used_bufs);
+        c->used_words_cap = 0;
+        c->used_pack = nullptr;
+        const int tiles = (n + kScanTile - 1) / kScanTile;
+        if (dalloc(c, &c->used_pos, size_t(n) + 1, c->used_bufs) || dalloc(c, &c->used_sums, size_t(tiles) + 1, c->used_bufs)) {
+            free_all(c->used_bufs);
+            c->used_n_cap = -1;
+            return fail(c, GRB_ENOMEM, "route transfer positions");
+        }
+        c->used_n_cap = n;
+    }
+    if (words > c->used_words_cap) {
+        if (c->used_pack) {
+            cudaFree(c->used_pack);
+            c->used_bufs.erase(std::find(c->used_bufs.begin(), c->used_bufs.end(), (void*)c->used_pack));
+            c->used_pack = nullptr;
+            c->used_words_cap = 0;
+        }
+        if (dalloc(c, &c->used_pack, size_t(std::max(words, 1ll)), c->used_bufs)) return fail(c, GRB_ENOMEM, "route transfer buffer");
+        c->used_words_cap = words;
+    }
+    return GRB_OK;
+}
+
+// Copy each net's words in use between `host` (at the route offsets) and
+// `packed` (at the positions), on `threads` host threads.
+static void used_scatter(int n, const long long* route_off, const long long* pos, int* host, int* packed,
+                         bool to_host) {
+    const int threads = int(std::min<long long>(8, std::max(1, n / 4096)));
+    auto part = [&](int t) {
+        const int lo = int((long long)n * t / threads), hi = int((long long)n * (t + 1) / threads);
+        for (int i = lo; i < hi; ++i) {
+            const size_t m = size_t(pos[i + 1] - pos[i]);
+            if (to_host) std::memcpy(host + route_off[i], packed + pos[i], m * sizeof(int));
+            else std::memcpy(packed + pos[i], host + route_off[i], m * sizeof(int));
+        }
+    };
+    std::vector<std::thread> pool;
+    for (int t = 1; t < threads; ++t) pool.emplace_back(part, t);
+    part(0);
+    for (auto& th : pool) th.join();
+}
+
+int grb_read_routes_used(grb_ctx* c, int32_t* routes) {
+    if (!c || !routes) return c ? fail(c, GRB_EINVAL, "null routes") : GRB_EINVAL;
+    GRB_CUDA(c, cudaSetDevice(c->device));
+    const int n = c->n_nets;
+    if (n <= 0) return GRB_OK;
+    int rc = used_buffers(c, 0);
+    if (rc) return rc;
+    const int tiles = (n + kScanTile - 1) / kScanTile;
+    k_route_used<<<(n + 255) / 256, 256, 0, c->stream>>>(c->routes, c->route_off, n, c->used_pos);
+    k_scan_tiles<<<tiles, 256, 0, c->stream>>>(c->used_pos, n, c->used_sums);
+    k_scan_sums<<<1, 1024, 0, c->stream>>>(c->used_sums, tiles);
+    k_scan_add<<<n / 256 + 1, 256, 0, c->stream>>>(c->used_pos, n, c->used_sums, tiles);
+    c->launches += 4;
+    GRB_CUDA(c, cudaGetLastError());
+    std::vector<long long> pos(size_t(n) + 1), off(size_t(n) + 1);
+    GRB_CUDA(c, cudaMemcpyAsync(pos.data(), c->used_pos, sizeof(long long) * (n + 1), cudaMemcpyDeviceToHost, c->stream));
+    GRB_CUDA(c, cudaMemcpyAsync(off.data(), c->route_off, sizeof(long long) * (n + 1), cudaMemcpyDeviceToHost, c->stream));
+    GRB_CUDA(c, cudaStreamSynchronize(c->stream));
+    const long long words = pos[n];
+    if ((rc = used_buffers(c, words))) return rc;
+    k_route_move<<<std::max(1, std::min((n + 7) / 8, c->sms * 16)), 256, 0, c->stream>>>(c->route_off, c->used_pos, n,
+                                                                                        c->routes, c->used_pack, 1);
+    c->launches += 1;
+    GRB_CUDA(c, cudaGetLastError());
+    std::vector<int> packed(size_t(std::max(words, 1ll)));
+    GRB_CUDA(c, cudaMemcpyAsync(packed.data(), c->used_pack, sizeof(int) * words, cudaMemcpyDeviceToHost, c->stream));
+    GRB_CUDA(c, cudaStreamSynchronize(c->stream));
+    used_scatter(n, off.data(), pos.data(), routes, packed.data(), true);
+    return GRB_OK;
+}
+
+int grb_write_routes_used(grb_ctx* c, const int32_t* routes) {
+    if (!c || !routes) return c ? fail(c, GRB_EINVAL, "null routes") : GRB_EINVAL;
+    GRB_CUDA(c, cudaSetDevice(c->device));
+    const int n = c->n_nets;
+    if (n <= 0) return GRB_OK;
+    std::vector<long long> pos(size_t(n) + 1), off(size_t(n) + 1);
+    GRB_CUDA(c, cudaMemcpyAsync(off.data(), c->route_off, sizeof(long long) * (n + 1), cudaMemcpyDeviceToHost, c->stream));
+    GRB_CUDA(c, cudaStreamSynchronize(c->stream));
+    pos[0] = 0;
+    for (int i = 0; i < n; ++i) {
+        const long long cap = off[i + 1] - off[i];
+        pos[i + 1] = pos[i] + (cap > 0 ? std::max(1ll, std::min<long long>(routes[off[i]], cap)) : 0);
+    }
+    const long long words = pos[n];
+    int rc = used_buffers(c, words);
+    if (rc) return rc;
+    std::vector<int> packed(size_t(std::max(words, 1ll)));
+    used_scatter(n, off.data(), pos.data(), const_cast<int32_t*>(routes), packed.data(), false);
+    GRB_CUDA(c, cudaMemcpyAsync(c->used_pack, packed.data(), sizeof(int) * words, cudaMemcpyHostToDevice, c->stream));
+    GRB_CUDA(c, cudaMemcpyAsync(c->used_pos, pos.data(), sizeof(long long) * (n + 1), cudaMemcpyHostToDevice, c->stream));
+    k_route_move<<<std::max(1, std::min((n + 7) / 8, c->sms * 16)), 256, 0, c->stream>>>(c->route_off, c->used_pos, n,
+                                                                                        c->routes, c->used_pack, 0);
+    c->launches += 1;
+    GRB_CUDA(c, cudaGetLastError());
     GRB_CUDA(c, cudaStreamSynchronize(c->stream));
     return GRB_OK;
 }

@@ -404,6 +404,23 @@ class Router:
         self._check(self._lib.grb_read_routes(self._ctx, _p(out)))
         return out
 
+    def read_routes_used(self, out: np.ndarray) -> np.ndarray:
+        """Each net's route words in use (its count word and the words below
+        it) into ``out`` (int32, route_off order); its other words are left as
+        they were."""
+        if out.dtype != np.int32 or not out.flags.c_contiguous or out.size < self._route_words:
+            raise ValueError(f"out must be a contiguous int32 array of at least {self._route_words} words")
+        self._check(self._lib.grb_read_routes_used(self._ctx, _p(out)))
+        return out
+
+    def write_routes_used(self, routes: np.ndarray):
+        """Each net's route words in use, read from ``routes`` (count word at
+        the net's offset), to the device; the device's other words are kept."""
+        routes = np.ascontiguousarray(routes, np.int32)
+        if routes.size < self._route_words:
+            raise ValueError(f"routes must hold at least {self._route_words} words")
+        self._check(self._lib.grb_write_routes_used(self._ctx, _p(routes)))
+
     def set_stats(self, wirelength: float = 0.0, vias: int = 0):
         self._check(self._lib.grb_set_stats(self._ctx, float(wirelength), int(vias)))
 

@@ -425,6 +425,19 @@ int grb_read_tables(grb_ctx* ctx, float* wcost, float* vcost, double* presum, in
                     int32_t* timestamp);
 /* Copy all route words (route_off[n] words) to the host. */
 int grb_read_routes(grb_ctx* ctx, int32_t* routes);
+/* Copy only the route words in use: for each net, its count word r[0] and
+ * the words below it (at least the count word), to the same offsets of
+ * `routes`; every other word of `routes` is left as it was.  A route holds a
+ * small part of its reserved storage (the GGR build reserves 256 words per pin,
+ * pipeline_ggr.hpp:9), so this moves a small part of what download_routes
+ * copies (router_state.hpp:215-222); host code that reads a route only below
+ * its count -- the GGR post-processing, zshape_topology.hpp:122-248, and the
+ * writer -- sees the same routes. */
+int grb_read_routes_used(grb_ctx* ctx, int32_t* routes);
+/* The reverse of grb_read_routes_used: for each net, the count word at its
+ * offset of `routes` (clamped to the net's storage) and the words below it are
+ * written to the device; the device's other words keep their values. */
+int grb_write_routes_used(grb_ctx* ctx, const int32_t* routes);
 /* Replace all route words (route_off[n] words) from the host: routes a caller
  * edited after a stage (the GGR pipeline's promote_congested_segments and
  * canonicalize_routes, zshape_topology.hpp:122-248) for grb_format_out.

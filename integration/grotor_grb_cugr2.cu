@@ -236,8 +236,10 @@ void route_cugr2(cudb::RouterState& state, int32_t mode) {
     printf("ROUTING_REMAINING_OVERFLOW nets=%zu\n", remaining);
     // pipeline_cugr2.hpp:123-128: the reference's writer on the downloaded routes.
     const size_t words = size_t(state.device.ROUTE_PER_PIN) * state.device.PIN_NUM + 1;
-    state.routes_cpu.reset(new int[words]());
-    check(grb_read_routes(ctx, state.routes_cpu.get()), ctx, "grb_read_routes");
+    // Only the words in use move (the writer reads a route below its count
+    // word), so the storage needs no clearing.
+    state.routes_cpu.reset(new int[words]);
+    check(grb_read_routes_used(ctx, state.routes_cpu.get()), ctx, "grb_read_routes_used");
     graph::finish_nets(state, all_nets);
     auto records = graph::collect_output_nets(std::move(nets2output));
     graph::output_nets(state, std::move(records));

@@ -18,8 +18,10 @@
 //     (grb_set_wire_cost_mode);
 //   * the host post-processing (promote_congested_segments,
 //     canonicalize_routes, zshape_topology.hpp:122-248) is the reference's
-//     code on the downloaded routes; the .out is then formatted on the device
-//     from the post-processed routes (grb_format_out / grb_drain_out).
+//     code on the downloaded routes (only their words in use move, each way:
+//     grb_read_routes_used, grb_write_routes_used); the .out is then
+//     formatted on the device from the post-processed routes (grb_format_out
+//     / grb_drain_out).
 //
 // Usage: grotor_grb_ggr -cap FILE -net FILE -out FILE [--lut-dir DIR]
 //                       [--executor persistent|plain|graph]
@@ -151,8 +153,10 @@ void route_ggr(cudb::RouterState& state, int32_t mode) {
     // pipeline_ggr.hpp:142-151: the reference's post-processing on the
     // downloaded routes, then the routes go back for the device writer.
     const size_t words = size_t(state.device.ROUTE_PER_PIN) * state.device.PIN_NUM + 1;
-    state.routes_cpu.reset(new int[words]());
-    check(grb_read_routes(ctx, state.routes_cpu.get()), ctx, "grb_read_routes");
+    // Only the words in use move (the post-processing and the writer read a
+    // route below its count word), so the storage needs no clearing.
+    state.routes_cpu.reset(new int[words]);
+    check(grb_read_routes_used(ctx, state.routes_cpu.get()), ctx, "grb_read_routes_used");
     phases.mark("stage_download");
     const auto post_begin = std::chrono::steady_clock::now();
     const int promoted = grotor::zshape::promote_congested_segments(count, state.device.X, state.device.Y, state.device.L,
@@ -162,7 +166,7 @@ void route_ggr(cudb::RouterState& state, int32_t mode) {
     printf("ZSHAPE_POSTPROCESS promoted_segments=%d elapsed_ms=%.6f\n", promoted,
            std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - post_begin).count());
     phases.mark("postprocess");
-    check(grb_write_routes(ctx, state.routes_cpu.get()), ctx, "grb_write_routes");
+    check(grb_write_routes_used(ctx, state.routes_cpu.get()), ctx, "grb_write_routes_used");
     for (int i = 0; i < int(db::nets.size()); ++i)
         if (db::nets[i].pins.size() == 1) nets2output.push(i);
     graph::finish_nets(state, order);

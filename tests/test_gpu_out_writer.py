@@ -67,3 +67,35 @@ def test_device_writer_equals_reference_writer():
     assert r.write_out(names[:3], pins[:3], extra[:3], subnets[:3]) == reference_text(
         g.X, g.Y, names[:3], pins[:3], extra[:3], subnets[:3], routes, n.route_off)
     r.close()
+
+
+def test_used_word_transfers():
+    """grb_read_routes_used moves each net's count word and the words below it
+    (and nothing else) to the host; grb_write_routes_used moves them back; a
+    net whose count word is 0 still has that word moved."""
+    from grotor_b200 import Router
+    from grotor_b200.synth import WORKLOADS, Design
+    d = Design(WORKLOADS["medium_320x320x10"].scaled(6000, seed=11))
+    r = Router(d.grid)
+    r.upload_nets(d.nets)
+    r.generate_batches_rsmt(d.order, 1000000)
+    r.lshape_route("persistent")
+    full = r.read_routes()
+    off = np.asarray(d.nets.route_off, np.int64)
+    used = np.zeros(full.size, bool)
+    for i in range(len(off) - 1):
+        if off[i + 1] > off[i]:
+            used[off[i]:off[i] + max(1, min(int(full[off[i]]), int(off[i + 1] - off[i])))] = True
+    assert not used.all()
+    got = r.read_routes_used(np.full(full.size, -7, np.int32))
+    np.testing.assert_array_equal(got[used], full[used])
+    assert (got[~used] == -7).all()
+    # Back to the device over a reset (routes zeroed): the words in use return,
+    # the others stay zero.
+    r.reset()
+    sent = np.where(used, full, 12345).astype(np.int32)
+    r.write_routes_used(sent)
+    back = r.read_routes()
+    np.testing.assert_array_equal(back[used], full[used])
+    assert (back[~used] == 0).all()
+    r.close()
