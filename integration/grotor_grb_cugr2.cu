@@ -129,6 +129,7 @@ void maze_view(cudb::RouterState& state, grb_ctx* ctx, const Grid& G, MazeView& 
 
 void route_cugr2(cudb::RouterState& state, int32_t mode) {
     cudb::prepare_routing_nets(state);
+    phases.mark("prepare");
     int64_t initial_vias = 0;  // one via per metal1 pin (preprocess.hpp:1716-1718)
     for (auto& dbnet : db::nets)
         for (int pin : dbnet.pins) initial_vias += pin < state.device.X * state.device.Y;
@@ -136,6 +137,7 @@ void route_cugr2(cudb::RouterState& state, int32_t mode) {
     grb_ctx* ctx = nullptr;
     check(grb_create(&G.g, 0, &ctx), nullptr, "grb_create");
     std::unique_ptr<grb_ctx, void (*)(grb_ctx*)> owner(ctx, grb_destroy);
+    phases.mark("create");
     for (int i = 0; i < int(db::nets.size()); ++i)
         if (db::nets[i].pins.size() == 1) nets2output.push(i);
     const int count = int(state.nets.size());
@@ -144,6 +146,7 @@ void route_cugr2(cudb::RouterState& state, int32_t mode) {
     printf("ROUTING_STAGE_BEGIN stage=lshape nets=%zu\n", all_nets.size());
     lshape_stage(state, ctx, all_nets, mode, initial_vias, true, true);
     printf("ROUTING_STAGE_END stage=lshape\n");
+    phases.mark("lshape_rest");
     if (state.nets.size() > 5000000) ::mode = 1;
     if (state.nets.size() > 20000000) ::mode = 2;
     const size_t xy = size_t(state.device.X) * state.device.Y;
@@ -153,12 +156,15 @@ void route_cugr2(cudb::RouterState& state, int32_t mode) {
     std::vector<int> detour;
     for (int i = 0; i < count; ++i) if (is_of[i]) detour.push_back(i);
     reserve_phase2(state, detour, 128);
+    phases.mark("classification");
     printf("ROUTING_STAGE_BEGIN stage=detour nets=%zu\n", detour.size());
     if (!detour.empty()) {
         detour_prepare(state, detour, cong, xsum, ysum);
+        phases.mark("flt_prepare");
         FltRun run = flt_run(state, ctx, detour, mode, 1, state.device.ROUTE_PER_PIN_PHASE2, "detour");
         collect_phase2(state, ctx, run, detour);
     }
+    phases.mark("detour_collect");
     printf("ROUTING_STAGE_END stage=detour\n");
 
     // pipeline_cugr2.hpp:90-117: the maze stage on the nets still overflowing
@@ -180,11 +186,14 @@ void route_cugr2(cudb::RouterState& state, int32_t mode) {
         const size_t words0 = size_t(stride0) * pins + 1;
         std::unique_ptr<int[]> routes0(new int[words0]);
         std::copy_n(state.routes_phase2_cpu.get(), words0, routes0.get());
+        phases.mark("maze_checkpoint");
         double before = 0;
         check(grb_routing_score(ctx, &before), ctx, "grb_routing_score");
         MazeView M;
         maze_view(state, ctx, G, M);
+        phases.mark("maze_view");
         grotor::maze::prepare_topology(state, maze_nets);
+        phases.mark("maze_search");
         std::vector<uint8_t> phase2(maze_nets.size());
         for (size_t k = 0; k < maze_nets.size(); ++k) phase2[k] = state.ripup_flag_cpu[maze_nets[k]] != 0;
         check(grb_remove_routes(ctx, maze_nets.data(), int32_t(maze_nets.size()), phase2.data()), ctx,
@@ -196,6 +205,7 @@ void route_cugr2(cudb::RouterState& state, int32_t mode) {
             stride = std::max(stride, (words + p - 1) / p);
         }
         reserve_phase2(state, maze_nets, stride);
+        phases.mark("maze_remove_reserve");
         // Every flagged net keeps phase-two storage on the device (the earlier
         // stage's routes are written into it), so the score, the final
         // classification and a restore see each net's current route.
@@ -207,6 +217,7 @@ void route_cugr2(cudb::RouterState& state, int32_t mode) {
                          state.ripup_flag_cpu);
         });
         collect_phase2(state, ctx, run, maze_nets);
+        phases.mark("maze_collect");
         double after = 0;
         check(grb_routing_score(ctx, &after), ctx, "grb_routing_score");
         const bool accepted = std::isfinite(after) && after < before;
@@ -221,6 +232,7 @@ void route_cugr2(cudb::RouterState& state, int32_t mode) {
         }
         printf("MAZE_QUALITY_GATE accepted=%d before_score=%.12g candidate_score=%.12g\n", int(accepted), before,
                after);
+        phases.mark("maze_gate");
         state.device.capacity = nullptr;
         state.device.demand = nullptr;
         state.device.x_edge_len = state.device.y_edge_len = nullptr;
@@ -240,9 +252,11 @@ void route_cugr2(cudb::RouterState& state, int32_t mode) {
     // word), so the storage needs no clearing.
     state.routes_cpu.reset(new int[words]);
     check(grb_read_routes_used(ctx, state.routes_cpu.get()), ctx, "grb_read_routes_used");
+    phases.mark("final_download");
     graph::finish_nets(state, all_nets);
     auto records = graph::collect_output_nets(std::move(nets2output));
     graph::output_nets(state, std::move(records));
+    phases.mark("output");
 }
 
 }  // namespace drop_in
@@ -267,7 +281,9 @@ int main(int argc, char** argv) {
         program_start = std::chrono::high_resolution_clock::now();
         // CUDA starts while the input is read (src/main.cu:101-106).
         auto gpu_ready = std::async(std::launch::async, [] { return grb_init_device(0); });
+        drop_in::phases.last = program_start;
         db::read(cap.data(), net.data());
+        drop_in::phases.mark("read");
         const auto caller_directory = std::filesystem::current_path();
         std::filesystem::current_path(lut_dir);
         flute::readLUT();
@@ -275,16 +291,20 @@ int main(int argc, char** argv) {
         out_file = fopen(output.c_str(), "w");
         if (!out_file) throw std::runtime_error("Cannot open output: " + output);
         if (setvbuf(out_file, nullptr, _IONBF, 0)) throw std::runtime_error("Cannot configure routing output");
+        drop_in::phases.mark("lut");
         drop_in::check(gpu_ready.get(), nullptr, "grb_init_device");
+        drop_in::phases.mark("cuda_init_wait");
         {
             cudb::RouterState state;
             state.batch_sparsity_override = 1;
             state.report_score = false;
             drop_in::route_cugr2(state, mode);
         }
+        drop_in::phases.mark("teardown");
         const int close_status = fclose(out_file);
         out_file = nullptr;
         if (close_status) throw std::runtime_error("Failed to close routing output");
+        drop_in::phases.print();
         printf("GROTOR_COMPLETE wall_seconds=%.6f\n", elapsed_time());
         return EXIT_SUCCESS;
     } catch (const std::exception& error) {
