@@ -18,7 +18,8 @@
 //     (grb_set_wire_cost_mode);
 //   * the host post-processing (promote_congested_segments,
 //     canonicalize_routes, zshape_topology.hpp:122-248) is the reference's
-//     code on the downloaded routes (only their words in use move, each way:
+//     code on the downloaded routes, canonicalize_routes on 8 threads over
+//     ranges of nets (only the routes' words in use move, each way:
 //     grb_read_routes_used, grb_write_routes_used); the .out is then
 //     formatted on the device from the post-processed routes (grb_format_out
 //     / grb_drain_out).
@@ -100,6 +101,29 @@ ZTrees encode_trees(const cudb::RouterState& state) {
     return Z;
 }
 
+// canonicalize_routes (zshape_topology.hpp:184-248) rewrites each net's route
+// from that route alone, so contiguous ranges of nets go to host threads, each
+// calling the reference's function with the offsets of its range (a net's
+// words stay where the whole-array call would put them).
+void canonicalize_parallel(cudb::RouterState& state, int count) {
+    constexpr int kParts = 8;
+    std::vector<std::exception_ptr> err(kParts);
+#pragma omp parallel for num_threads(kParts) schedule(static, 1)
+    for (int t = 0; t < kParts; ++t) {
+        const int lo = int(int64_t(count) * t / kParts), hi = int(int64_t(count) * (t + 1) / kParts);
+        if (lo >= hi) continue;
+        try {
+            const std::vector<int> offsets(state.pin_cnt_sum_cpu.begin() + lo, state.pin_cnt_sum_cpu.begin() + hi + 1);
+            grotor::zshape::canonicalize_routes(hi - lo, state.device.X, state.device.Y, state.device.ROUTE_PER_PIN,
+                                                offsets, state.routes_cpu.get());
+        } catch (...) {
+            err[t] = std::current_exception();
+        }
+    }
+    for (auto& e : err)
+        if (e) std::rethrow_exception(e);
+}
+
 void route_ggr(cudb::RouterState& state, int32_t mode) {
     state.device.ROUTE_PER_PIN = 256;  // pipeline_ggr.hpp:9
     cudb::prepare_routing_nets(state);
@@ -161,8 +185,8 @@ void route_ggr(cudb::RouterState& state, int32_t mode) {
     const auto post_begin = std::chrono::steady_clock::now();
     const int promoted = grotor::zshape::promote_congested_segments(count, state.device.X, state.device.Y, state.device.L,
         state.device.ROUTE_PER_PIN, state.pin_cnt_sum_cpu, state.routes_cpu.get());
-    grotor::zshape::canonicalize_routes(count, state.device.X, state.device.Y, state.device.ROUTE_PER_PIN,
-                                        state.pin_cnt_sum_cpu, state.routes_cpu.get());
+    phases.mark("postprocess_promote");
+    canonicalize_parallel(state, count);
     printf("ZSHAPE_POSTPROCESS promoted_segments=%d elapsed_ms=%.6f\n", promoted,
            std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - post_begin).count());
     phases.mark("postprocess");
