@@ -17,14 +17,15 @@
 //     plane-major (colour word w of all cells contiguous);
 //   * nets are processed in chunks of CH (1024, or 512 when the solver's
 //     shared memory for the colour words would not fit) in order; per chunk:
-//       1. raster: every mark on a query point of this chunk or of the next
-//          one (per-cell chunk bits, L2-resident, filter the rest) ORs its
-//          net's bit into the chunk-local mask of the cell (triple-buffered by
-//          chunk index);
+//       1. raster: every mark on a query point of this chunk or (persistent
+//          form) of the two chunks after it (per-cell chunk bits,
+//          L2-resident, filter the rest) ORs its net's bit into the
+//          chunk-local mask of the cell (five buffers by chunk index);
 //       2. gather: every query point ORs, into its net's column of the chunk
 //          tables, the cell's colours (forbidden batches of earlier chunks),
 //          the chunk-local bits of earlier nets of the chunk (predecessors),
-//          and -- in the lookback form -- the bits of the previous chunk's nets;
+//          and -- in the persistent form -- the bits of the previous chunk's
+//          nets and the colours of the nets two chunks back;
 //       3. solve: one CTA solves first-fit inside the chunk by Jacobi
 //          iteration over the predecessor DAG (converges to the unique
 //          sequential solution), then applies batch capacities in order;
@@ -32,13 +33,15 @@
 //          chunk-local mask is emptied at the chunk's query points.
 //   Positions inside the batches come from a stable counting pass after the
 //   run.  Plain form: one launch per step per chunk.  Persistent form: one
-//   cooperative kernel in which CTA 0 solves chunk r while the other CTAs
-//   publish chunk r-1, gather chunk r+1 and raster chunk r+2; the gather
-//   reads cellmask as of chunk r-1 and takes chunk r's colours through the
-//   previous-chunk bits, which the solver resolves from the colours it keeps
-//   in shared memory.  The solver and the other CTAs hand chunks over through
-//   two monotone counters (bounded waits), so the solve never waits for a
-//   publish.
+//   cooperative kernel in which CTA 0 solves chunk r while the other CTAs, in
+//   one phase and one grid barrier, publish chunk r-1, gather chunk r+1 and
+//   raster chunk r+2; the gather reads cellmask as of chunk r-2 at least (chunk
+//   r-1's publish runs beside it), resolves chunk r-1's nets through that
+//   chunk's local mask and its solved colours, and takes chunk r's colours
+//   through the previous-chunk bits, which the solver resolves from the colours
+//   it keeps in shared memory.  The solver and the other CTAs hand chunks over
+//   through two monotone counters (bounded waits), so the solve never waits
+//   for a publish.
 #pragma once
 #include "common.cuh"
 
@@ -64,7 +67,7 @@ struct BatchState {
     unsigned short* pt_jj;
     unsigned* cellmask;         // [W][X*Y]: word w of every cell contiguous, so the
                                 // colour ORs of consecutive cells share sectors
-    unsigned* localmask[3];     // [X*Y][CH/32], chunk k in buffer k % 3
+    unsigned* localmask[5];     // [X*Y][CH/32], chunk k in buffer k % 5
     unsigned* ptchunk;          // [X*Y] bit k % 32: the cell is a query point of chunk k
     unsigned* fmask;            // [2][W][CH] forbidden colours, by chunk parity
     unsigned* pred;             // [2][CH/32][CH] predecessors inside the chunk
@@ -172,7 +175,8 @@ __device__ __forceinline__ void flat_fill(const BatchState& B, int p) {
     }
 }
 
-__device__ __forceinline__ unsigned* chunk_mask(const BatchState& B, int chunk) { return B.localmask[chunk % 3]; }
+constexpr int kLocalMasks = 5;
+__device__ __forceinline__ unsigned* chunk_mask(const BatchState& B, int chunk) { return B.localmask[chunk % kLocalMasks]; }
 
 // Query-point bits of the chunk at s: bit (chunk % 32) of every query point
 // cell of the chunk is set (set) or cleared.
@@ -189,14 +193,15 @@ __device__ __forceinline__ void batch_point_bits(const BatchState& B, int s, boo
 }
 
 // Step 1: the chunk at order position s rasters its marks.  Only a cell that
-// is a query point of this chunk or (with `next`) of the next one is ever read
-// back, so the raster keeps the marks whose cell has one of those query-point
-// bits; the bits live in a 4-byte-per-cell array that stays in L2, the
-// chunk-local masks do not.  Threads t of nt.
+// is a query point of this chunk or of the `ahead` chunks after it is ever
+// read back, so the raster keeps the marks whose cell has one of those
+// query-point bits; the bits live in a 4-byte-per-cell array that stays in L2,
+// the chunk-local masks do not.  Threads t of nt.
 template <int CH>
-__device__ __forceinline__ void batch_raster(const BatchState& B, int s, bool next, long long t, long long nt) {
+__device__ __forceinline__ void batch_raster(const BatchState& B, int s, int ahead, long long t, long long nt) {
     const int m = min(CH, B.n - s), chunk = s / CH;
-    const unsigned want = (1u << (chunk & 31)) | (next ? 1u << ((chunk + 1) & 31) : 0u);
+    unsigned want = 0u;
+    for (int a = 0; a <= ahead; ++a) want |= 1u << ((chunk + a) & 31);
     unsigned* lm = chunk_mask(B, chunk);
     const long long a = B.mark_off[s], b = B.mark_off[s + m];
     // Four marks per thread and pass, every load of a pass issued first.
@@ -218,13 +223,13 @@ __device__ __forceinline__ void batch_raster(const BatchState& B, int s, bool ne
 }
 
 // The chunk-local mask of the chunk at s is nonzero only at query points of
-// this chunk and (with `next`) the next one: zero the whole record of each of
+// this chunk and the `ahead` chunks after it: zero the whole record of each of
 // those cells.
 template <int CH>
-__device__ __forceinline__ void batch_clear(const BatchState& B, int s, bool next, long long t, long long nt) {
+__device__ __forceinline__ void batch_clear(const BatchState& B, int s, int ahead, long long t, long long nt) {
     unsigned* lm = chunk_mask(B, s / CH);
     const long long a = B.pt_off[s];
-    const long long b = B.pt_off[min(s + (next ? 2 : 1) * CH, B.n)];
+    const long long b = B.pt_off[min(s + (ahead + 1) * CH, B.n)];
     constexpr int kParts = (CH / 32) / 4;  // 16-byte groups of a record
     const long long items = (b - a) * kParts;
     for (long long k = t; k < items; k += nt) {
@@ -235,20 +240,24 @@ __device__ __forceinline__ void batch_clear(const BatchState& B, int s, bool nex
     }
 }
 
-// Step 2: per query point, OR the cell's colours, the earlier nets' bits of
-// this chunk and (lookback) the previous chunk's bits into the net's column.
+// Step 2: per query point, OR into the net's columns the cell's colours, the
+// earlier nets' bits of this chunk and, with lookback >= 1, the bits of the
+// previous chunk's nets (resolved by the solver, which knows their colours);
+// with lookback 2 also the colours of the nets two chunks back that mark the
+// cell (that chunk is solved, its colours published or being published).
 // Each item is a 16-byte group of one record (W and (CH / 32) are
 // multiples of 4).
 template <int CH>
-__device__ __forceinline__ void batch_gather(const BatchState& B, int s, bool lookback, long long t, long long nt) {
+__device__ __forceinline__ void batch_gather(const BatchState& B, int s, int lookback, long long t, long long nt) {
     const int chunk = s / CH, m = min(CH, B.n - s), W = B.W;
     const unsigned* lm = chunk_mask(B, chunk);
-    const unsigned* lp = lookback ? chunk_mask(B, chunk - 1) : nullptr;
+    const unsigned* lp = lookback >= 1 ? chunk_mask(B, chunk - 1) : nullptr;
+    const unsigned* lp2 = lookback >= 2 ? chunk_mask(B, chunk - 2) : nullptr;
     unsigned* F = B.fmask + size_t(chunk & 1) * W * CH;
     unsigned* P = B.pred + size_t(chunk & 1) * (CH / 32) * CH;
     unsigned* Q = B.prevp + size_t(chunk & 1) * (CH / 32) * CH;
     const int gw = W / 4, gl = (CH / 32) / 4;
-    const int per = gw + gl * (lookback ? 2 : 1);
+    const int per = gw + gl * (1 + lookback);
     const long long a = B.pt_off[s], b = B.pt_off[s + m];
     const long long items = (b - a) * per;
     for (long long k = t; k < items; k += nt) {
@@ -278,10 +287,22 @@ __device__ __forceinline__ void batch_gather(const BatchState& B, int s, bool lo
             else if (ow == 2) { v.z &= own; v.w = 0u; }
             else if (ow == 3) v.w &= own;
             dst = P;
-        } else {
+        } else if (g < gw + 2 * gl) {
             w0 = 4 * (g - gw - gl);
             v = __ldcg(reinterpret_cast<const uint4*>(lp + size_t(q) * (CH / 32)) + (g - gw - gl));
             dst = Q;
+        } else {
+            w0 = 4 * (g - gw - 2 * gl);
+            v = __ldcg(reinterpret_cast<const uint4*>(lp2 + size_t(q) * (CH / 32)) + (g - gw - 2 * gl));
+            const unsigned vw[4] = {v.x, v.y, v.z, v.w};
+            const int* col2 = B.batch_of + size_t(chunk - 2) * CH;
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+                for (unsigned bits = vw[u]; bits; bits &= bits - 1) {
+                    const int c = __ldcg(col2 + (w0 + u) * 32 + __ffs(bits) - 1);
+                    red_or(F + size_t(c >> 5) * CH + jj, 1u << (c & 31));
+                }
+            continue;
         }
         if (v.x) red_or(dst + size_t(w0) * CH + jj, v.x);
         if (v.y) red_or(dst + size_t(w0 + 1) * CH + jj, v.y);

@@ -805,10 +805,10 @@ __device__ __forceinline__ long long launch_threads() { return (long long)gridDi
 template <int CH>
 __global__ void k_batch_point_bits(BatchState B, int s) { batch_point_bits<CH>(B, s, true, launch_thread(), launch_threads()); }
 template <int CH>
-__global__ void k_batch_raster(BatchState B, int s) { batch_raster<CH>(B, s, false, launch_thread(), launch_threads()); }
+__global__ void k_batch_raster(BatchState B, int s) { batch_raster<CH>(B, s, 0, launch_thread(), launch_threads()); }
 template <int CH>
 __global__ void k_batch_gather(BatchState B, int s) {
-    batch_gather<CH>(B, s, false, blockIdx.x * (long long)blockDim.x + threadIdx.x, (long long)gridDim.x * blockDim.x);
+    batch_gather<CH>(B, s, 0, blockIdx.x * (long long)blockDim.x + threadIdx.x, (long long)gridDim.x * blockDim.x);
 }
 template <int CH>
 __global__ void __launch_bounds__(CH) k_batch_solve(BatchState B, int s) {
@@ -832,7 +832,7 @@ __global__ void k_batch_publish(BatchState B, int s) {
     if (*reinterpret_cast<volatile int*>(B.error)) return;
     const long long t = launch_thread(), nt = launch_threads();
     batch_publish<CH>(B, s, t, nt);
-    batch_clear<CH>(B, s, false, t, nt);
+    batch_clear<CH>(B, s, 0, t, nt);
     batch_point_bits<CH>(B, s, false, t, nt);
     if (s + CH < B.n) batch_point_bits<CH>(B, s + CH, true, t, nt);
 }
@@ -842,16 +842,19 @@ __global__ void k_batch_publish(BatchState B, int s) {
 // threads solve, the rest leave): for chunk r it waits until the other CTAs
 // (G of them, one shared barrier counter) have gathered chunk r, solves it,
 // and releases `solved` = r + 1.  The other CTAs set the query-point bits of
-// chunks 0-3 | raster chunks 0 and 1 | gather chunk 0 | and then run, per
-// round r:
-//   A: wait for chunk r-1's colours, publish chunk r-1, empty
-//      its chunk-local mask, set the query-point bits of chunk
-//      r+4 and clear those of chunk r-1                        | barrier
-//   B: gather chunk r+1 (cellmask as of chunk r-1, chunk r
-//      through the previous-chunk bits) and raster chunk r+2
-//      (its buffer was emptied in A)                           | barrier
-// The barrier after B(r) is what the solver waits for before chunk r+1
-// (counter (3 + 2(r+1)) * G).
+// chunks 0-4 | raster chunks 0 and 1 | gather chunk 0 | and then run, per
+// round r, one phase and one barrier:
+//   wait for chunk r-1's colours; publish chunk r-1 and clear its query-point
+//   bits; empty chunk r-2's chunk-local mask; set the query-point bits of
+//   chunk r+5; gather chunk r+1 (cellmask as of chunk r-2 at least, chunk r-1
+//   through its chunk-local mask and its colours, chunk r through the
+//   previous-chunk bits the solver resolves); raster chunk r+2, keeping the
+//   marks on query points of chunks r+2 to r+4              | barrier
+// A chunk's local mask (five buffers, chunk k in buffer k % 5) is written by
+// its raster in round k-2, read by the gathers of chunks k, k+1 and k+2
+// (rounds k-1 to k+1) and emptied in round k+2, before the raster of chunk
+// k+5 in round k+3.  The barrier of round r is what the solver waits for
+// before chunk r+1 (counter (3 + (r + 1)) * G).
 constexpr int kPersistThreads = kChunkMax;
 template <int CH>
 __global__ void __launch_bounds__(kPersistThreads, 1) k_batch_persistent(BatchState B, GridSync S, Tables T) {
@@ -870,7 +873,7 @@ __global__ void __launch_bounds__(kPersistThreads, 1) k_batch_persistent(BatchSt
             for (int k = threadIdx.x; k < (CH / 32) * C; k += CH) M.wh[k] = 0;
         for (int k = threadIdx.x; k < B.W; k += CH) M.full[k] = B.fullmask[k];
         for (int r = 0; r < chunks; ++r) {
-            if (threadIdx.x == 0) go = wait_at_least(S.count, (3u + 2u * r) * G, S.timeout_ns, T, true);
+            if (threadIdx.x == 0) go = wait_at_least(S.count, (3u + unsigned(r)) * G, S.timeout_ns, T, true);
             solve_sync<CH>();
             if (!go) return;
             clk.mark(S, 8);
@@ -887,11 +890,11 @@ __global__ void __launch_bounds__(kPersistThreads, 1) k_batch_persistent(BatchSt
     PhaseClock clk{0, 1};
     clk.start(S);
     const long long t = (blockIdx.x - 1) * (long long)blockDim.x + threadIdx.x, nt = (long long)G * blockDim.x;
-    for (int k = 0; k < 4 && k < chunks; ++k) batch_point_bits<CH>(B, k * CH, true, t, nt);
+    for (int k = 0; k < 5 && k < chunks; ++k) batch_point_bits<CH>(B, k * CH, true, t, nt);
     if (!grid_sync_of(S, T, G)) return;
-    for (int k = 0; k < 2 && k < chunks; ++k) batch_raster<CH>(B, k * CH, true, t, nt);
+    for (int k = 0; k < 2 && k < chunks; ++k) batch_raster<CH>(B, k * CH, 2, t, nt);
     if (!grid_sync_of(S, T, G)) return;
-    batch_gather<CH>(B, 0, false, t, nt);
+    batch_gather<CH>(B, 0, 0, t, nt);
     if (!grid_sync_of(S, T, G)) return;
     clk.mark(S, 1);
     for (int r = 0; r < chunks; ++r) {
@@ -901,14 +904,12 @@ __global__ void __launch_bounds__(kPersistThreads, 1) k_batch_persistent(BatchSt
             if (!go) return;
             clk.mark(S, 9);
             batch_publish<CH>(B, (r - 1) * CH, t, nt);
-            batch_clear<CH>(B, (r - 1) * CH, true, t, nt);
             batch_point_bits<CH>(B, (r - 1) * CH, false, t, nt);
         }
-        if (r + 4 < chunks) batch_point_bits<CH>(B, (r + 4) * CH, true, t, nt);
-        if (!grid_sync_of(S, T, G)) return;
-        clk.mark(S, 0);
-        if (r + 1 < chunks) batch_gather<CH>(B, (r + 1) * CH, true, t, nt);
-        if (r + 2 < chunks) batch_raster<CH>(B, (r + 2) * CH, true, t, nt);
+        if (r >= 2) batch_clear<CH>(B, (r - 2) * CH, 2, t, nt);
+        if (r + 5 < chunks) batch_point_bits<CH>(B, (r + 5) * CH, true, t, nt);
+        if (r + 1 < chunks) batch_gather<CH>(B, (r + 1) * CH, min(r + 1, 2), t, nt);
+        if (r + 2 < chunks) batch_raster<CH>(B, (r + 2) * CH, 2, t, nt);
         if (!grid_sync_of(S, T, G)) return;
         clk.mark(S, 1);
     }
@@ -917,8 +918,8 @@ __global__ void __launch_bounds__(kPersistThreads, 1) k_batch_persistent(BatchSt
         __syncthreads();
         if (!go) return;
         batch_publish<CH>(B, (chunks - 1) * CH, t, nt);
-        batch_clear<CH>(B, (chunks - 1) * CH, true, t, nt);
         batch_point_bits<CH>(B, (chunks - 1) * CH, false, t, nt);
+        for (int k = max(chunks - 2, 0); k < chunks; ++k) batch_clear<CH>(B, k * CH, 2, t, nt);
     }
 }
 
@@ -1079,7 +1080,7 @@ struct grb_ctx {
     unsigned* sync = nullptr;   // [count, generation]
     // batching buffers
     unsigned *cellmask = nullptr, *fmask = nullptr, *fullmask = nullptr;
-    unsigned* lmask[3] = {nullptr, nullptr, nullptr};  // chunk-local masks
+    unsigned* lmask[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};  // chunk-local masks
     unsigned* ptchunk = nullptr;                        // [X*Y] query-point bits by chunk % 32
     unsigned *pred = nullptr, *prevp = nullptr, *bsolved = nullptr;
     bool lmask_dirty = false;          // a run stopped before clearing them
@@ -2052,7 +2053,8 @@ void grb_destroy(grb_ctx* c) {
     if (c->score_partials) cudaFree(c->score_partials);
     free_all(c->owned);
     for (void* p : {(void*)c->check, (void*)c->bucket_ids, (void*)c->bucket_off, (void*)c->ids, (void*)c->batch_off, (void*)c->gscratch, (void*)c->work, (void*)c->cellmask,
-                    (void*)c->lmask[0], (void*)c->lmask[1], (void*)c->lmask[2], (void*)c->ptchunk, (void*)c->fmask, (void*)c->pred, (void*)c->prevp,
+                    (void*)c->lmask[0], (void*)c->lmask[1], (void*)c->lmask[2], (void*)c->lmask[3], (void*)c->lmask[4],
+                    (void*)c->ptchunk, (void*)c->fmask, (void*)c->pred, (void*)c->prevp,
                     (void*)c->bsolved, (void*)c->fullmask, (void*)c->bcount, (void*)c->ncolors, (void*)c->batch_of, (void*)c->brank,
                     (void*)c->order, (void*)c->rank_tiles, (void*)c->mark_off, (void*)c->pt_off, (void*)c->scan_sums, (void*)c->mark_cell,
                     (void*)c->pt_cell, (void*)c->mark_jj, (void*)c->pt_jj})
@@ -2989,6 +2991,7 @@ int grb_plan_batches(grb_ctx* c, const int32_t* order, int32_t n, int32_t limit,
     if (rc) return rc;
     if (!c->lmask[0]) {
         if (cudaMalloc(&c->lmask[0], lm_bytes) || cudaMalloc(&c->lmask[1], lm_bytes) || cudaMalloc(&c->lmask[2], lm_bytes) ||
+            cudaMalloc(&c->lmask[3], lm_bytes) || cudaMalloc(&c->lmask[4], lm_bytes) ||
             cudaMalloc(&c->ptchunk, xy * 4) ||
             cudaMalloc(&c->pred, pq_bytes) || cudaMalloc(&c->prevp, pq_bytes) || cudaMalloc(&c->bsolved, 4) ||
             cudaMalloc(&c->ncolors, 4)) {
@@ -3037,7 +3040,7 @@ int grb_plan_batches(grb_ctx* c, const int32_t* order, int32_t n, int32_t limit,
         GRB_CUDA(c, cudaMemsetAsync(c->bsolved, 0, 4, c->stream));
         B.W = W;
         B.cellmask = c->cellmask;
-        for (int k = 0; k < 3; ++k) B.localmask[k] = c->lmask[k];
+        for (int k = 0; k < 5; ++k) B.localmask[k] = c->lmask[k];
         B.ptchunk = c->ptchunk;
         B.fmask = c->fmask; B.pred = c->pred; B.prevp = c->prevp;
         B.fullmask = c->fullmask; B.count = c->bcount; B.n_colors = c->ncolors;
