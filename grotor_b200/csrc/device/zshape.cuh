@@ -101,6 +101,36 @@ __device__ __noinline__ void zvia_sweep(const Tables& T, const ZTrees& Z, int x,
     }
 }
 
+// The (layer, position) items of an edge phase over plane layers 1..LAYER-1:
+// the layers along y ((i & 1) ^ D) come first, `ey` positions each, then the
+// others, `ex` positions each.  Flattening the layers into one index space
+// gives a layer's items to different threads: the reference's loop over the
+// layers (one dependent load chain per layer and thread) becomes a single pass.
+struct ZItems {
+    int ey, ex, ny, nx, iy, ix;  // extents, layer counts, first layer of each kind
+    __device__ int count() const { return ny * ey + nx * ex; }
+};
+__device__ __forceinline__ ZItems zitems(const ZTrees& Z, int ey, int ex) {
+    ZItems I;
+    I.ey = ey; I.ex = ex;
+    I.iy = 1 + Z.D;
+    I.ix = 2 - Z.D;
+    I.ny = I.iy <= Z.LAYER - 1 ? (Z.LAYER - 1 - I.iy) / 2 + 1 : 0;
+    I.nx = I.ix <= Z.LAYER - 1 ? (Z.LAYER - 1 - I.ix) / 2 + 1 : 0;
+    return I;
+}
+// Item k -> plane layer i, offset o along its box side, along-y flag.
+__device__ __forceinline__ void zitem(const ZItems& I, int k, int& i, int& o, bool& ay) {
+    const int ky = I.ny * I.ey;
+    ay = k < ky;
+    if (ay) { i = I.iy + 2 * (k / I.ey); o = k % I.ey; }
+    else { k -= ky; i = I.ix + 2 * (k / I.ex); o = k % I.ex; }
+}
+// Items a thread takes per pass, their loads issued together: 1 measured
+// fastest (1,387 ms for the persistent stage at the 900K-net design against
+// 1,421 with 2 and 1,502 with 4, which spill in the persistent kernel).
+constexpr int kZUnroll = 1;
+
 // Child slot j (1..3) of node (tox, toy): fill plane j at the node from the
 // child at (fromx, fromy) (zshape.cuh:87-237).
 __device__ __forceinline__ void zedge(const Tables& T, const ZTrees& Z, int j, int fromx, int fromy, int tox, int toy,
@@ -129,23 +159,37 @@ __device__ __forceinline__ void zedge(const Tables& T, const ZTrees& Z, int j, i
             }
         __syncthreads();
         // Straight runs out of the child along each layer's direction.
-        for (int i = 1; i < LAYER; ++i) {
-            if ((i & 1) ^ D) {
-                const int last = static_cast<int>(i * NN + fromx * Z.N + fromy);
-                for (int b = miny + lane; b <= maxy; b += nth) {
-                    if (b == fromy) continue;
-                    const int cur = static_cast<int>(i * NN + fromx * Z.N + b);
-                    m4[cur] = zadd(map0[last], zwire_at(T, i, fromx, fromy, fromx, b));
-                    p4[cur] = last;
+        {
+            const ZItems I = zitems(Z, maxy - miny + 1, maxx - minx + 1);
+            const int items = I.count();
+            for (int k0 = lane; k0 < items; k0 += kZUnroll * nth) {
+                int cur[kZUnroll], last[kZUnroll], base[kZUnroll], w[kZUnroll];
+                bool ok[kZUnroll];
+#pragma unroll
+                for (int u = 0; u < kZUnroll; ++u) {
+                    const int k = k0 + u * nth;
+                    ok[u] = false;
+                    if (k >= items) continue;
+                    int i, o;
+                    bool ay;
+                    zitem(I, k, i, o, ay);
+                    const int b = (ay ? miny : minx) + o;
+                    if (b == (ay ? fromy : fromx)) continue;
+                    ok[u] = true;
+                    if (ay) {
+                        last[u] = static_cast<int>(i * NN + fromx * Z.N + fromy);
+                        cur[u] = static_cast<int>(i * NN + fromx * Z.N + b);
+                        w[u] = zwire_at(T, i, fromx, fromy, fromx, b);
+                    } else {
+                        last[u] = static_cast<int>(i * NN + fromy * Z.N + fromx);
+                        cur[u] = static_cast<int>(i * NN + fromy * Z.N + b);
+                        w[u] = zwire_at(T, i, fromx, fromy, b, fromy);
+                    }
+                    base[u] = map0[last[u]];
                 }
-            } else {
-                const int last = static_cast<int>(i * NN + fromy * Z.N + fromx);
-                for (int b = minx + lane; b <= maxx; b += nth) {
-                    if (b == fromx) continue;
-                    const int cur = static_cast<int>(i * NN + fromy * Z.N + b);
-                    m4[cur] = zadd(map0[last], zwire_at(T, i, fromx, fromy, b, fromy));
-                    p4[cur] = last;
-                }
+#pragma unroll
+                for (int u = 0; u < kZUnroll; ++u)
+                    if (ok[u]) { m4[cur[u]] = zadd(base[u], w[u]); p4[cur[u]] = last[u]; }
             }
         }
         __syncthreads();
@@ -158,20 +202,41 @@ __device__ __forceinline__ void zedge(const Tables& T, const ZTrees& Z, int j, i
             }
         }
         __syncthreads();
-        // Cross the box to the node's row / column.
-        for (int i = 1; i < LAYER; ++i) {
-            if ((i & 1) ^ D) {
-                for (int b = minx + lane; b <= maxx; b += nth) {
-                    const int last = static_cast<int>(i * NN + b * Z.N + fromy), cur = static_cast<int>(i * NN + b * Z.N + toy);
-                    const int v = zadd(m4[last], zwire_at(T, i, b, fromy, b, toy));
-                    if (v < m4[cur]) { m4[cur] = v; p4[cur] = p4[last]; }
+        // Cross the box to the node's row / column (layers along y cross at
+        // every column of the box, the others at every row).
+        {
+            const ZItems I = zitems(Z, maxx - minx + 1, maxy - miny + 1);
+            const int items = I.count();
+            for (int k0 = lane; k0 < items; k0 += kZUnroll * nth) {
+                int cur[kZUnroll], last[kZUnroll], v[kZUnroll], mc[kZUnroll], pl[kZUnroll];
+                bool ok[kZUnroll];
+#pragma unroll
+                for (int u = 0; u < kZUnroll; ++u) {
+                    const int k = k0 + u * nth;
+                    ok[u] = k < items;
+                    if (!ok[u]) continue;
+                    int i, o;
+                    bool ay;
+                    zitem(I, k, i, o, ay);
+                    int w;
+                    if (ay) {
+                        const int b = minx + o;
+                        last[u] = static_cast<int>(i * NN + b * Z.N + fromy);
+                        cur[u] = static_cast<int>(i * NN + b * Z.N + toy);
+                        w = zwire_at(T, i, b, fromy, b, toy);
+                    } else {
+                        const int b = miny + o;
+                        last[u] = static_cast<int>(i * NN + b * Z.N + fromx);
+                        cur[u] = static_cast<int>(i * NN + b * Z.N + tox);
+                        w = zwire_at(T, i, fromx, b, tox, b);
+                    }
+                    v[u] = zadd(m4[last[u]], w);
+                    mc[u] = m4[cur[u]];
+                    pl[u] = p4[last[u]];
                 }
-            } else {
-                for (int b = miny + lane; b <= maxy; b += nth) {
-                    const int last = static_cast<int>(i * NN + b * Z.N + fromx), cur = static_cast<int>(i * NN + b * Z.N + tox);
-                    const int v = zadd(m4[last], zwire_at(T, i, fromx, b, tox, b));
-                    if (v < m4[cur]) { m4[cur] = v; p4[cur] = p4[last]; }
-                }
+#pragma unroll
+                for (int u = 0; u < kZUnroll; ++u)
+                    if (ok[u] && v[u] < mc[u]) { m4[cur[u]] = v[u]; p4[cur[u]] = pl[u]; }
             }
         }
         __syncthreads();
@@ -185,37 +250,45 @@ __device__ __forceinline__ void zedge(const Tables& T, const ZTrees& Z, int j, i
         __syncthreads();
         // Last run into the node: per layer, the first minimum over the
         // positions of the node's row/column (the reference scans them in
-        // order keeping strict improvements), found by a block reduction of
-        // (value, position) pairs.
-        // Each warp's first minimum per layer goes to shared memory; after one
-        // barrier, thread i combines layer i over the warps.
-        __shared__ int red_v[32][kMaxLayers], red_b[32][kMaxLayers];
-        for (int i = 1; i < LAYER; ++i) {
-            const bool ay = ((i & 1) ^ D) != 0;
-            const int lo = ay ? miny : minx, hi = ay ? maxy : maxx, skip = ay ? toy : tox;
-            int bv = 0, bb = -1;
-            for (int b = lo + lane; b <= hi; b += nth) {
-                if (b == skip) continue;
-                const int last = static_cast<int>(ay ? i * NN + tox * Z.N + b : i * NN + toy * Z.N + b);
-                const int v = zadd(m4[last], ay ? zwire_at(T, i, tox, b, tox, toy) : zwire_at(T, i, b, toy, tox, toy));
-                if (bb < 0 || v < bv) { bv = v; bb = b; }
+        // order keeping strict improvements), as the (value, position) minimum.
+        // A warp per layer (lanes over the positions, several loads in
+        // flight per lane); its result goes to shared memory, and after one
+        // barrier thread i applies layer i's.
+        __shared__ int red_v[kMaxLayers + 1], red_b[kMaxLayers + 1];
+        {
+            const int warp = lane >> 5, wl = lane & 31, nw = (nth + 31) / 32;
+            for (int i = 1 + warp; i < LAYER; i += nw) {
+                const bool ay = ((i & 1) ^ D) != 0;
+                const int lo = ay ? miny : minx, hi = ay ? maxy : maxx, skip = ay ? toy : tox;
+                int bv = 0, bb = -1;
+                for (int b0 = lo + wl; b0 <= hi; b0 += kZUnroll * 32) {
+                    int v[kZUnroll];
+                    bool ok[kZUnroll];
+#pragma unroll
+                    for (int u = 0; u < kZUnroll; ++u) {
+                        const int b = b0 + u * 32;
+                        ok[u] = b <= hi && b != skip;
+                        if (!ok[u]) continue;
+                        const int last = static_cast<int>(ay ? i * NN + tox * Z.N + b : i * NN + toy * Z.N + b);
+                        v[u] = zadd(m4[last], ay ? zwire_at(T, i, tox, b, tox, toy) : zwire_at(T, i, b, toy, tox, toy));
+                    }
+#pragma unroll
+                    for (int u = 0; u < kZUnroll; ++u)
+                        if (ok[u] && (bb < 0 || v[u] < bv)) { bv = v[u]; bb = b0 + u * 32; }
+                }
+                for (int o = 16; o; o >>= 1) {
+                    const int ov = __shfl_down_sync(0xffffffffu, bv, o), ob = __shfl_down_sync(0xffffffffu, bb, o);
+                    if (ob >= 0 && (bb < 0 || ov < bv || (ov == bv && ob < bb))) { bv = ov; bb = ob; }
+                }
+                if (wl == 0) { red_v[i] = bv; red_b[i] = bb; }
             }
-            for (int o = 16; o; o >>= 1) {
-                const int ov = __shfl_down_sync(0xffffffffu, bv, o), ob = __shfl_down_sync(0xffffffffu, bb, o);
-                if (ob >= 0 && (bb < 0 || ov < bv || (ov == bv && ob < bb))) { bv = ov; bb = ob; }
-            }
-            if ((lane & 31) == 0) { red_v[lane >> 5][i] = bv; red_b[lane >> 5][i] = bb; }
         }
         __syncthreads();
         if (lane >= 1 && lane < LAYER) {
             const int i = lane;
             const bool ay = ((i & 1) ^ D) != 0;
             const int cur = static_cast<int>(ay ? i * NN + tox * Z.N + toy : i * NN + toy * Z.N + tox);
-            int bv = red_v[0][i], bb = red_b[0][i];
-            for (int w = 1; w < (nth + 31) / 32; ++w) {
-                const int ov = red_v[w][i], ob = red_b[w][i];
-                if (ob >= 0 && (bb < 0 || ov < bv || (ov == bv && ob < bb))) { bv = ov; bb = ob; }
-            }
+            const int bv = red_v[i], bb = red_b[i];
             if (bb >= 0 && bv < mj[cur]) {
                 const int last = static_cast<int>(ay ? i * NN + tox * Z.N + bb : i * NN + toy * Z.N + bb);
                 mj[cur] = bv; pj[cur] = p4[last]; p2j[cur] = p5[last];
